@@ -1,0 +1,244 @@
+/*
+ * cloudsc_b200.h -- C ABI of the B200 (sm_100a) implementation of the OpenIFS
+ * prognostic cloud scheme CLOUDSC.
+ *
+ * The entry points keep the argument list of the reference subroutine
+ *   ifs-source/arpifs/phys_ec/cloudsc.F90:14-44   (SUBROUTINE CLOUDSC)
+ * in the same order, with the seven derived-type arguments (YDECLDP, YDECUMF,
+ * YDEPHLI, YDERAD, YDEPHY, YDVDF, YDSPP_CONFIG) collapsed into one POD struct,
+ * cloudsc_params, that the caller fills once (from the model's own YDECLDP and
+ * friends, or with cloudsc_b200_params_default).
+ *
+ * Conventions (identical to the Fortran reference):
+ *   - every array is column-major Fortran storage: element (jl,jk) of a
+ *     (KLON,KLEV) array is at (jk-1)*KLON + (jl-1); element (jl,jk,jm) of a
+ *     (KLON,KLEV,N) array is at ((jm-1)*KLEV + (jk-1))*KLON + (jl-1);
+ *     half-level arrays are (KLON,KLEV+1);
+ *   - KIDIA/KFDIA are 1-based; only columns KIDIA..KFDIA are written;
+ *   - LOGICAL arguments are 4-byte integers (non-zero = .TRUE.);
+ *   - REAL(KIND=JPRB) is double (the double-precision OpenIFS build);
+ *     the *_sp entry points take the single-precision build's REAL(4).
+ *
+ * Return codes: 0 = success; > 0 = number of negative-condensate warning events
+ * (the reference WRITEs a warning to NULOUT for each, cloudsc.F90:3794,3802);
+ * < 0 = one of the CLOUDSC_E_* errors below.  Nothing traps or aborts on the
+ * device.
+ */
+#ifndef CLOUDSC_B200_H
+#define CLOUDSC_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLOUDSC_NCLV 5 /* yoecldp.F90:102 NCLV; species index order below */
+#define CLOUDSC_NCLDQL 1
+#define CLOUDSC_NCLDQI 2
+#define CLOUDSC_NCLDQR 3
+#define CLOUDSC_NCLDQS 4
+#define CLOUDSC_NCLDQV 5
+
+#define CLOUDSC_OK 0
+#define CLOUDSC_E_NULL (-1)        /* a required array pointer is NULL          */
+#define CLOUDSC_E_SHAPE (-2)       /* KIDIA/KFDIA/KLON/KLEV/NCLDTOP inconsistent */
+#define CLOUDSC_E_UNSUPPORTED (-3) /* a parameter switch this build lacks is on  */
+#define CLOUDSC_E_CUDA (-4)        /* a CUDA runtime call failed                */
+#define CLOUDSC_E_PARAMS (-5)      /* no parameters uploaded / bad param struct */
+#define CLOUDSC_E_TOO_LARGE (-6)   /* request exceeds a fixed capacity          */
+
+#define CLOUDSC_PARAMS_MAGIC 0x434c4453u /* 'CLDS' */
+
+/*
+ * Every scalar CLOUDSC reads through its ASSOCIATE block (cloudsc.F90:612-682)
+ * plus the YOMCST/YOETHF constants of fcttre.func.h.  Field names are the
+ * reference names in lower case.  Integers are int32; logicals are int32.
+ */
+typedef struct cloudsc_params {
+  uint32_t magic;   /* CLOUDSC_PARAMS_MAGIC */
+  int32_t version;  /* 1 */
+  /* ---- YOMCST (yomcst.F90) ---- */
+  double rg, rd, rv, rcpd, retv, rtt, rlvtt, rlstt, rlmlt, rpi, ra;
+  /* ---- YOETHF (suphec.F90:231-254) ---- */
+  double r2es, r3les, r3ies, r4les, r4ies, r5les, r5ies, r5alvcp, r5alscp;
+  double ralvdcp, ralsdcp, ralfdcp, rtwat, rtice, rticecu;
+  double rtwat_rtice_r, rtwat_rticecu_r, rkoop1, rkoop2;
+  /* ---- TECLDP (yoecldp.F90, defaults from sucldp.F90:243-530) ---- */
+  double ramid, ramin, rlmin, rcldiff, rcldiff_convi, rclcrit_sea, rclcrit_land;
+  double rkconv, rprc1, rpecons, rprecrhmax, rvrfactor, rcovpmin, rtaumel;
+  double rkooptau, rssicefactor, rsnowlin1, rsnowlin2, rlcritsnow, rthomo;
+  double rvice, rvrain, rvsnow, rxfallspeedrain, rxfallspeedice, rnice, rccn;
+  double rcldtopcf, rdepliqrefrate, rdepliqrefdepth, riceinit, rdensref, rdenswat;
+  double rcl_overlapliqice, rcl_effrime, rcl_inhomogaut, rcl_inhomogacc;
+  double rcl_kkaac, rcl_kkbac, rcl_kkaau, rcl_kkbauq, rcl_kkbaun;
+  double rcl_kk_cloud_num_sea, rcl_kk_cloud_num_land, rcl_eff_racw;
+  double rcl_dr, rcl_x1r, rcl_x2r, rcl_lam1r, rcl_lam2r;
+  double rcl_const1r, rcl_const2r, rcl_const3r, rcl_const4r, rcl_const5r;
+  double rcl_const6r, rcl_const7r, rcl_const8r, rcl_const9r, rcl_const10r;
+  double rcl_cdenom1, rcl_cdenom2, rcl_cdenom3, rcl_ka273, rcl_fzrab;
+  double rcl_x1s, rcl_lam1s, rcl_lam2s;
+  double rcl_const1s, rcl_const2s, rcl_const3s, rcl_const4s, rcl_const5s;
+  double rcl_const6s, rcl_const7s, rcl_const8s;
+  double rcl_const1i, rcl_const2i, rcl_const3i, rcl_const4i, rcl_const5i;
+  double rcl_const6i, rcl_const7i;
+  double rcl_apb1, rcl_apb2, rcl_apb3;
+  double ricehi1, ricehi2;
+  int32_t ncldtop;
+  /* switches that select code paths; the values the B200 kernels implement
+   * are the reference defaults noted beside each (others -> CLOUDSC_E_UNSUPPORTED) */
+  int32_t laericeauto, laericesed, laerliqautolsp, laerliqcoll; /* all 0 (NAERCLD=0) */
+  int32_t lcloud_inhomog;                                       /* 0 */
+  int32_t lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint; /* 0 */
+  int32_t lcldbud_timeint;                                      /* any */
+  int32_t lcldbudget, lscmec;                                   /* 0 (diagnostic only) */
+  /* ---- TECUMF (sucumf.F90:203,228-229) ---- */
+  int32_t lmfdsnow;                                             /* any (default 1) */
+  double rmfadvw, rmfadvwdd;                                    /* any (default 0) */
+  /* ---- TERAD / TEPHY / TVDF / TSPP_CONFIG ---- */
+  double rcloud_frac_std;                                       /* suecrad.F90:745 */
+  int32_t lrad_cloud_inhomog;                                   /* 0 */
+  int32_t lbud23;                                               /* any (budgets off) */
+  double reisthsc;                                              /* unused when budgets off */
+  int32_t lspp;                                                 /* 0 */
+  int32_t pad_;
+} cloudsc_params;
+
+/*
+ * Fill *p with the reference defaults of SUCLDP/SUPHEC/YOMCST/SUCUMF/SUECRAD
+ * for physics time step tsphy (RSSICEFACTOR = MIN(TSPHY/RKOOPTAU,1),
+ * sucldp.F90:655) and cloud-top level ncldtop (sucldp.F90:631-634).
+ * Replaces: the SUCLDP call chain (ifs-source/arpifs/phys_ec/sucldp.F90:243-655).
+ */
+int cloudsc_b200_params_default(double tsphy, int32_t ncldtop, cloudsc_params *p);
+
+/*
+ * NCLDTOP from the standard-atmosphere full-level pressures stpre[0..klev-1]
+ * (Pa) and RCLDTOPP (su0phy.F90:1343, 100 Pa): the smallest level >= 2 whose
+ * pressure exceeds rcldtopp.  Replaces sucldp.F90:631-634.
+ */
+int32_t cloudsc_b200_ncldtop(int32_t klev, const double *stpre, double rcldtopp);
+
+/*
+ * Upload *p to every device this process uses (constant memory).  Must be
+ * called once before the first CLOUDSC call and again whenever the parameters
+ * change.  Thread-safe.  Replaces the derived-type arguments YDECLDP..YDSPP_CONFIG.
+ */
+int cloudsc_b200_setup(const cloudsc_params *p);
+
+/*
+ * Per-block drop-in: the full CLOUDSC argument list with HOST pointers.
+ * Replaces the call at ifs-source/arpifs/phys_ec/cloud_layer.F90:169-201
+ * (SUBROUTINE CLOUDSC, ifs-source/arpifs/phys_ec/cloudsc.F90:14-44).
+ * Copies the block to the GPU, runs the FP64 kernel, copies results back.
+ * Safe to call concurrently from several host threads (one stream and one
+ * device workspace per calling thread), as EC_PHYS_DRV does under OpenMP
+ * (ec_phys_drv.F90:438).  Arrays the default configuration does not read may be NULL:
+ * pvfa, pdyna..pdyns, phrsw, phrlw, pvervel, pgeom, pgaw, kctop, kpbltype,
+ * pgp2dspp, plcrit_aer, picrit_aer, pre_ice, pccn, pnice, pfsd, pextra.
+ */
+int cloudsc_b200_block(
+    const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
+    int32_t lddiag, double ptsphy, const double *pt, const double *pq,
+    const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfa, const double *pvfl,
+    const double *pvfi, const double *pdyna, const double *pdynl,
+    const double *pdyni, const double *pdynr, const double *pdyns,
+    const double *phrsw, const double *phrlw, const double *pvervel,
+    const double *pap, const double *paph, const double *pgeom, const double *plsm,
+    const double *pgaw, const int32_t *ldcum, const int32_t *kctop,
+    const int32_t *ktype, const int32_t *kpbltype, double *peis, const double *plu,
+    double *plude, const double *pludeli, const double *psnde, const double *pmfu,
+    const double *pmfd, const double *pgp2dspp, int32_t ldslphy, const double *pa,
+    const double *pclv, const double *plcrit_aer, const double *picrit_aer,
+    const double *pre_ice, const double *pccn, const double *pnice,
+    double *pcovptot, double *pfsd, double *prainfrac_toprfz, double *pfsqlf,
+    double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf,
+    double *pfsqsf, double *pfcqrng, double *pfcqsng, double *pfsqltur,
+    double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
+    double *pfhpsn, double *pextra, int32_t kfldx);
+
+/*
+ * Batched persistent launch: DEVICE pointers to arrays stored as
+ * (NPROMA, <dims>, NGPBLKS), the EC_PHYS_DRV storage (ec_phys_drv.F90:145-185);
+ * block ib (0-based) of an array with per-block size S starts at ib*S.
+ * Block ib covers columns 1..MIN(NPROMA, NGPTOT-ib*NPROMA) (ec_phys_drv.F90:441).
+ * One kernel launch processes every block on `stream` (a cudaStream_t, or
+ * NULL for the default stream); the call returns without synchronising.
+ * Argument order is that of CLOUDSC with KIDIA/KFDIA/KLON replaced by
+ * NPROMA/NGPBLKS/NGPTOT.  The optional `ncounters` device buffer (may be NULL)
+ * receives the number of negative-condensate warning events (uint32, added to).
+ * `precision` selects the arithmetic: 0 = FP64 (the reference's double
+ * build), 1 = FP32-mixed (FP32 microphysics, FP64 5x5 solve, saturation
+ * adjustment and budget sums).
+ */
+int cloudsc_b200_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks,
+    int32_t ngptot, double ptsphy, const double *pt, const double *pq,
+    const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi,
+    const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis,
+    const double *plu, double *plude, const double *pludeli, const double *psnde,
+    const double *pmfu, const double *pmfd, const double *pa, const double *pclv,
+    double *pcovptot, double *prainfrac_toprfz, double *pfsqlf, double *pfsqif,
+    double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur,
+    double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
+    uint32_t *ncounters, int32_t precision, void *stream);
+
+/*
+ * Batched call with HOST pointers (same arrays and order as
+ * cloudsc_b200_batched): blocks are processed in chunks of chunk_blocks
+ * (<= 0 selects 64), each chunk's host-to-device copy, kernel and
+ * device-to-host copy pipelined on three streams over three device buffers,
+ * so transfers overlap compute.  Host arrays should be page-locked for the
+ * copies to run asynchronously.  Synchronous: returns when all outputs are
+ * back in host memory.  Columns beyond NGPTOT in the last block are left
+ * untouched.  Replaces the whole EC_PHYS_DRV block loop over CLOUDSC
+ * (ec_phys_drv.F90:430-442) for callers that keep the state on the host.
+ */
+int cloudsc_b200_batched_host(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks,
+    int32_t ngptot, double ptsphy, const double *pt, const double *pq,
+    const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi,
+    const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis,
+    const double *plu, double *plude, const double *pludeli, const double *psnde,
+    const double *pmfu, const double *pmfd, const double *pa, const double *pclv,
+    double *pcovptot, double *prainfrac_toprfz, double *pfsqlf, double *pfsqif,
+    double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur,
+    double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
+    int32_t precision, int32_t chunk_blocks);
+
+/* sizeof(cloudsc_params) as compiled into the library (binding check). */
+size_t cloudsc_b200_params_size(void);
+
+/*
+ * Kernel launch shape used by cloudsc_b200_batched (the autotuner's knobs).
+ * threads_per_cta: columns per CTA (32..256, must divide into NPROMA tiles);
+ * ctas_per_sm: persistent CTAs resident per SM (0 = one wave over all tiles).
+ * Returns CLOUDSC_E_SHAPE for values outside the documented limits.
+ */
+int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm);
+
+/* Last CUDA error string recorded by this library on the calling thread. */
+const char *cloudsc_b200_last_error(void);
+
+/* Library version string. */
+const char *cloudsc_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLOUDSC_B200_H */

@@ -1,0 +1,160 @@
+"""Python binding of libcloudsc_b200.so (the C ABI in include/cloudsc_b200.h).
+
+This mirrors the reference's operator interface for the path: one call per
+NPROMA block with CLOUDSC's argument list (``cloudsc_block``), or one call for
+all blocks (``cloudsc_batched`` on device arrays, ``cloudsc_batched_host`` on
+host arrays).  Errors follow the C ABI: a negative return raises
+``CloudscError``; a positive return is the number of negative-condensate
+warning events the reference would have written to NULOUT
+(cloudsc.F90:3794,3802).
+
+There is no CPU fallback: if the library is missing or no GPU is present the
+calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .fields import BATCHED_FIELDS
+from .params import CloudscParams
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcloudsc_b200.so")
+
+FP64 = 0
+MIXED = 1
+
+
+class CloudscError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"CLOUDSC error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise CloudscError(-4, f"{LIB_PATH} not built; run python -m openifs_b200.build")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER(CloudscParams)
+        vp = ctypes.c_void_p
+        i32 = ctypes.c_int32
+        L.cloudsc_b200_params_default.argtypes = [ctypes.c_double, i32, P]
+        L.cloudsc_b200_params_default.restype = ctypes.c_int
+        L.cloudsc_b200_ncldtop.argtypes = [i32, vp, ctypes.c_double]
+        L.cloudsc_b200_ncldtop.restype = i32
+        L.cloudsc_b200_setup.argtypes = [P]
+        L.cloudsc_b200_setup.restype = ctypes.c_int
+        L.cloudsc_b200_set_launch.argtypes = [i32, i32, i32]
+        L.cloudsc_b200_set_launch.restype = ctypes.c_int
+        L.cloudsc_b200_last_error.restype = ctypes.c_char_p
+        L.cloudsc_b200_version.restype = ctypes.c_char_p
+        L.cloudsc_b200_params_size.restype = ctypes.c_size_t
+        nf = len(BATCHED_FIELDS)
+        L.cloudsc_b200_batched.argtypes = [P, i32, i32, i32, i32, ctypes.c_double] + [vp] * nf + [vp, i32, vp]
+        L.cloudsc_b200_batched.restype = ctypes.c_int
+        L.cloudsc_b200_batched_host.argtypes = [P, i32, i32, i32, i32, ctypes.c_double] + [vp] * nf + [i32, i32]
+        L.cloudsc_b200_batched_host.restype = ctypes.c_int
+        L.cloudsc_b200_block.argtypes = ([P, i32, i32, i32, i32, i32, ctypes.c_double] +
+                                         [vp] * len(BLOCK_ARRAYS_1) + [i32] +
+                                         [vp] * len(BLOCK_ARRAYS_2) + [i32])
+        L.cloudsc_b200_block.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc < 0:
+        raise CloudscError(rc, lib().cloudsc_b200_last_error().decode())
+    return rc
+
+
+def default_params(tsphy=3600.0, ncldtop=None):
+    """Reference defaults (SUCLDP et al.) for time step ``tsphy``."""
+    if ncldtop is None:
+        from .inputs import ncldtop_l137
+        ncldtop = ncldtop_l137()
+    p = CloudscParams()
+    _check(lib().cloudsc_b200_params_default(float(tsphy), int(ncldtop), ctypes.byref(p)))
+    return p
+
+
+def setup(params):
+    """Upload ``params`` to the GPU(s); required before any CLOUDSC call."""
+    return _check(lib().cloudsc_b200_setup(ctypes.byref(params)))
+
+
+def set_launch(precision, threads_per_cta, ctas_per_sm):
+    return _check(lib().cloudsc_b200_set_launch(int(precision), int(threads_per_cta), int(ctas_per_sm)))
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        if not x.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return x.ctypes.data
+    # torch tensor (device or pinned host)
+    if not x.is_contiguous():
+        raise ValueError("tensors must be contiguous")
+    return x.data_ptr()
+
+
+def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64,
+                    stream=None, counter=None):
+    """One persistent launch over all blocks; ``arrays`` are CUDA tensors in
+    the fields.BATCHED_FIELDS layout.  Asynchronous on ``stream``."""
+    args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
+    s = None
+    if stream is not None:
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+    return _check(lib().cloudsc_b200_batched(
+        ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
+        *args, _ptr(counter), int(precision), s))
+
+
+def cloudsc_batched_host(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64,
+                         chunk_blocks=0):
+    """All blocks from host arrays (numpy, or pinned torch CPU tensors), with
+    transfers pipelined against compute.  Synchronous."""
+    args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
+    return _check(lib().cloudsc_b200_batched_host(
+        ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
+        *args, int(precision), int(chunk_blocks)))
+
+
+# Argument list of SUBROUTINE CLOUDSC (cloudsc.F90:14-44) after the seven
+# derived types: (name, is_array); None entries are the unused optional arrays.
+BLOCK_ARRAYS_1 = ["pt", "pq", "tendency_cml_t", "tendency_cml_q", "tendency_cml_a",
+                  "tendency_cml_cld", "tendency_loc_t", "tendency_loc_q", "tendency_loc_a",
+                  "tendency_loc_cld", "pvfa", "pvfl", "pvfi", "pdyna", "pdynl", "pdyni", "pdynr",
+                  "pdyns", "phrsw", "phrlw", "pvervel", "pap", "paph", "pgeom", "plsm", "pgaw",
+                  "ldcum", "kctop", "ktype", "kpbltype", "peis", "plu", "plude", "pludeli",
+                  "psnde", "pmfu", "pmfd", "pgp2dspp"]
+BLOCK_ARRAYS_2 = ["pa", "pclv", "plcrit_aer", "picrit_aer", "pre_ice", "pccn", "pnice",
+                  "pcovptot", "pfsd", "prainfrac_toprfz", "pfsqlf", "pfsqif", "pfcqnng",
+                  "pfcqlng", "pfsqrf", "pfsqsf", "pfcqrng", "pfcqsng", "pfsqltur", "pfsqitur",
+                  "pfplsl", "pfplsn", "pfhpsl", "pfhpsn", "pextra"]
+
+
+def cloudsc_block(params, kidia, kfdia, klon, klev, ptsphy, arrays, lddiag=False, ldslphy=False,
+                  kfldx=0):
+    """The per-block drop-in: CLOUDSC's argument list with host arrays.
+
+    ``arrays`` maps the reference argument names (lower case, without the
+    leading 'p' of PTENDENCY_* spelled as in fields.py) to numpy arrays in
+    the (KLON, ...) Fortran layout of one block, i.e. C shape (..., KLON).
+    Arrays the default configuration does not read may be omitted.
+    """
+    a1 = [_ptr(arrays.get(n)) for n in BLOCK_ARRAYS_1]
+    a2 = [_ptr(arrays.get(n)) for n in BLOCK_ARRAYS_2]
+    return _check(lib().cloudsc_b200_block(
+        ctypes.byref(params), int(kidia), int(kfdia), int(klon), int(klev), int(bool(lddiag)),
+        float(ptsphy), *a1, int(bool(ldslphy)), *a2, int(kfldx)))

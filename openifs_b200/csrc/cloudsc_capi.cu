@@ -1,0 +1,704 @@
+// C ABI of the B200 CLOUDSC implementation (declared in include/cloudsc_b200.h).
+//
+// Host-side responsibilities: the reference's constant set-up for standalone
+// use (cloudsc_b200_params_default), parameter validation and upload to
+// constant memory, argument checking with CLOUDSC's error conventions, and the
+// three launch paths:
+//   cloudsc_b200_batched       device pointers, one persistent launch;
+//   cloudsc_b200_batched_host  host pointers, block chunks pipelined through
+//                              H2D / compute / D2H on three streams;
+//   cloudsc_b200_block         the per-NPROMA-block drop-in with host pointers.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "cloudsc_common.cuh"
+
+namespace cloudsc {
+cudaError_t upload_params(const cloudsc_params &p, const Derived &d);
+cudaError_t launch(int precision, const Fields &f, const Shape &sh, int threads, int grid,
+                   cudaStream_t stream);
+}  // namespace cloudsc
+
+using namespace cloudsc;
+
+namespace {
+
+thread_local std::string t_last_error;
+
+std::mutex g_mu;
+cloudsc_params g_params;
+bool g_have_params = false;
+unsigned long long g_gen = 0;
+constexpr int kMaxDev = 64;
+unsigned long long g_dev_gen[kMaxDev] = {0};
+int g_threads[2] = {128, 64};
+int g_ctas_per_sm[2] = {0, 0};
+
+int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
+  t_last_error = what;
+  if (e != cudaSuccess) {
+    t_last_error += ": ";
+    t_last_error += cudaGetErrorString(e);
+  }
+  return code;
+}
+
+bool params_supported(const cloudsc_params &p) {
+  if (p.laericeauto || p.laericesed || p.laerliqautolsp || p.laerliqcoll) return false;
+  if (p.lcloud_inhomog || p.lrad_cloud_inhomog || p.lspp) return false;
+  if (p.lcldbudc || p.lcldbudl || p.lcldbudi || p.lcldbudt || p.lcldbud_vertint) return false;
+  return true;
+}
+
+Derived make_derived(const cloudsc_params &p) {
+  Derived d;
+  d.zconst_pow_land = std::pow(p.rcl_kk_cloud_num_land, p.rcl_kkbaun);
+  d.zconst_pow_sea = std::pow(p.rcl_kk_cloud_num_sea, p.rcl_kkbaun);
+  d.flt_0p4 = (double)0.4f;
+  d.flt_0p8 = (double)0.8f;
+  return d;
+}
+
+// Make sure the current device holds the latest uploaded parameters.
+int ensure_params(int *dev_out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaGetDevice", e);
+  if (dev < 0 || dev >= kMaxDev) return fail(CLOUDSC_E_CUDA, "device index out of range");
+  if (dev_out) *dev_out = dev;
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_have_params) return fail(CLOUDSC_E_PARAMS, "cloudsc_b200_setup has not been called");
+  if (g_dev_gen[dev] != g_gen) {
+    e = upload_params(g_params, make_derived(g_params));
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "parameter upload", e);
+    g_dev_gen[dev] = g_gen;
+  }
+  return CLOUDSC_OK;
+}
+
+int check_params_match(const cloudsc_params *p) {
+  if (!p) return fail(CLOUDSC_E_NULL, "params is NULL");
+  if (p->magic != CLOUDSC_PARAMS_MAGIC) return fail(CLOUDSC_E_PARAMS, "bad params magic");
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_have_params) return fail(CLOUDSC_E_PARAMS, "cloudsc_b200_setup has not been called");
+  if (std::memcmp(p, &g_params, sizeof(cloudsc_params)) != 0)
+    return fail(CLOUDSC_E_PARAMS, "params differ from the ones passed to cloudsc_b200_setup");
+  return CLOUDSC_OK;
+}
+
+int grid_for(int precision, int tiles, int threads) {
+  int ctas = g_ctas_per_sm[precision];
+  if (ctas <= 0) return tiles;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int g = sms * ctas;
+  (void)threads;
+  return g < tiles ? g : tiles;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cloudsc_b200_last_error(void) { return t_last_error.c_str(); }
+
+const char *cloudsc_b200_version(void) { return "cloudsc_b200 1.0 (sm_100a)"; }
+
+size_t cloudsc_b200_params_size(void) { return sizeof(cloudsc_params); }
+
+// Restatement of the reference defaults (SUCLDP, SUPHEC, YOMCST, SUCUMF,
+// SUECRAD, SU0PHY); see the header for the citations.  Gamma-function values
+// use FCGENERALIZED_GAMMA's binary32 Lanczos coefficients
+// (fcgeneralized_gamma.F90:69-126), as the reference does.
+static double lanczos_gamma_f32coef(double px) {
+  const float coef[6] = {76.18009172947146f, -86.50532032941677f, 24.01409824083091f,
+                         -1.231739572450155f, 0.1208650973866179E-2f, -0.5395239384953E-5f};
+  const double stp = (double)2.5066282746310005f;
+  const double sercst = (double)1.000000000190015f;
+  const double pi = 2.0 * std::asin(1.0);
+  double w = px >= 0.0 ? 1.0 : 0.0;
+  double x = (1.0 - px) * (1.0 - w) + px * w;
+  double tt = x + 5.5;
+  double lead = (x + 0.5) * std::log(tt) - tt;
+  double ser = sercst;
+  for (int j = 0; j < 6; ++j) ser = ser + (double)coef[j] / ((double)(j + 1) + x);
+  double g = std::exp(lead + std::log(stp * ser / x));
+  return g * w + (pi / std::sin(pi * px) / g) * (1.0 - w);
+}
+
+int cloudsc_b200_params_default(double tsphy, int32_t ncldtop, cloudsc_params *p) {
+  if (!p) return fail(CLOUDSC_E_NULL, "params is NULL");
+  if (!(tsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "tsphy must be positive");
+  std::memset(p, 0, sizeof(*p));
+  p->magic = CLOUDSC_PARAMS_MAGIC;
+  p->version = 1;
+  const double plrg = 1.0, pldare = 1.0, plradi = 1.0;  // sudyncore.F90:86-90
+  const double pi = 2.0 * std::asin(1.0);
+  // YOMCST
+  const double rgas = 6.0221367E+23 * 1.380658E-23;  // RNAVO*RKBOL
+  p->rpi = pi;
+  p->ra = 6371229. * plradi;
+  p->rg = 9.80665;
+  p->rd = 1000. * rgas / 28.9644;
+  p->rv = 1000. * rgas / 18.0153;
+  p->rcpd = 3.5 * p->rd;
+  p->retv = p->rv / p->rd - 1.0;
+  p->rtt = 273.16;
+  p->rlvtt = 2.5008E+6;
+  p->rlstt = 2.8345E+6;
+  p->rlmlt = p->rlstt - p->rlvtt;
+  // YOETHF
+  p->r2es = 611.21 * p->rd / p->rv;
+  p->r3les = 17.502;
+  p->r3ies = 22.587;
+  p->r4les = 32.19;
+  p->r4ies = -0.7;
+  p->r5les = p->r3les * (p->rtt - p->r4les);
+  p->r5ies = p->r3ies * (p->rtt - p->r4ies);
+  p->r5alvcp = p->r5les * p->rlvtt / p->rcpd;
+  p->r5alscp = p->r5ies * p->rlstt / p->rcpd;
+  p->ralvdcp = p->rlvtt / p->rcpd;
+  p->ralsdcp = p->rlstt / p->rcpd;
+  p->ralfdcp = p->rlmlt / p->rcpd;
+  p->rtwat = p->rtt;
+  p->rtice = p->rtt - 23.;
+  p->rticecu = p->rtt - 23.;
+  p->rtwat_rtice_r = 1.0 / (p->rtwat - p->rtice);
+  p->rtwat_rticecu_r = 1.0 / (p->rtwat - p->rticecu);
+  p->rkoop1 = 2.583;
+  p->rkoop2 = 0.48116E-2;
+  // TECLDP scalars
+  const double vplrg = pldare * std::sqrt(plrg);
+  p->ramid = 0.8;
+  p->rprc1 = 100.;
+  p->ramin = 1.E-8;
+  p->rlmin = 1.E-8;
+  p->rcldiff = 6.0E-6 * plrg * pldare;
+  p->rcldiff_convi = 10.0;
+  p->rclcrit_sea = 2.5E-4;
+  p->rclcrit_land = 5.5E-4;
+  p->rkconv = plrg * pldare / 6000.;
+  p->rcl_inhomogaut = 1.5;
+  p->rcl_inhomogacc = 3.0;
+  p->rsnowlin1 = plrg * pldare / 1000.;
+  p->rsnowlin2 = 0.030;
+  p->rlcritsnow = 2.0E-5;
+  p->rvice = 0.13 * vplrg;
+  p->rvrain = 4.0 * vplrg;
+  p->rvsnow = 1.0 * vplrg;
+  p->rxfallspeedrain = 1.0;
+  p->rxfallspeedice = 1.0;
+  p->ricehi1 = 1.0 / 30000.;
+  p->ricehi2 = 1.0 / 233.;
+  p->rnice = 0.027;
+  p->rccn = 125.0;
+  p->rcldtopcf = 0.01;
+  p->rdepliqrefrate = 0.5;
+  p->rdepliqrefdepth = 500.0 / plrg;
+  p->rcl_overlapliqice = 0.65;
+  p->rcl_effrime = 1.0;
+  p->riceinit = 1.E-12;
+  p->rthomo = p->rtt - 38.0;
+  p->rprecrhmax = 0.7;
+  p->rpecons = 5.44E-4 * plrg * pldare / p->rg;
+  p->rvrfactor = 5.09E-3 * vplrg;
+  p->rcovpmin = 0.1;
+  p->rtaumel = 2.0 * 3.6E3 / (plrg * pldare);
+  p->rkooptau = 3.0 * 3.6E3 / (plrg * pldare);
+  p->rdenswat = 1000.0;
+  p->rdensref = 1.0;
+  // rain particle size distribution and process constants
+  const double cr = 386.8 * vplrg, ar = p->rdenswat * pi / 6., br = 3.0, x4r = 0.0;
+  const double fzrbb = 2.E2, schmidt = 0.6, dynvisc = 1.717E-5;
+  p->rcl_dr = 0.67;
+  p->rcl_x1r = 0.22;
+  p->rcl_x2r = 2.20;
+  p->rcl_lam1r = ar * p->rcl_x1r * lanczos_gamma_f32coef(br + 1. + x4r);
+  p->rcl_lam2r = 1.0 / (br + 1. + x4r - p->rcl_x2r);
+  p->rcl_cdenom1 = 5.57E11;
+  p->rcl_cdenom2 = 1.03E8;
+  p->rcl_cdenom3 = 2.04E2;
+  p->rcl_ka273 = 2.4E-2;
+  const double g1r = lanczos_gamma_f32coef((p->rcl_dr + 5.) / 2.);
+  const double g3r = lanczos_gamma_f32coef(br + 1.0 + x4r);
+  const double g4r = lanczos_gamma_f32coef(p->rcl_dr + br + 1.0 + x4r);
+  const double g5r = lanczos_gamma_f32coef(3.0 + p->rcl_dr + x4r);
+  const double g6r = lanczos_gamma_f32coef(4.0 + br + x4r);
+  p->rcl_const1r = 2. * pi * p->rcl_x1r * plrg * pldare;
+  p->rcl_const2r = 0.31 * std::pow(schmidt, 0.3333) * g1r * std::pow(cr / dynvisc, 0.5);
+  p->rcl_const3r = (p->rcl_dr + 5.) / 2. - p->rcl_x2r;
+  p->rcl_const4r = 2. - p->rcl_x2r;
+  p->rcl_const7r = cr * g4r / g3r;
+  p->rcl_const8r = 0.0;
+  p->rcl_const9r = pi * 0.25 * p->rcl_x1r * cr * g5r;
+  p->rcl_const10r = 3.0 + p->rcl_dr - p->rcl_x2r;
+  p->rcl_eff_racw = 0.7;
+  p->rcl_kkaac = 67.;
+  p->rcl_kkbac = 1.15;
+  p->rcl_kkaau = 1350.;
+  p->rcl_kkbauq = 2.47;
+  p->rcl_kkbaun = -1.79;
+  p->rcl_kk_cloud_num_sea = 50.;
+  p->rcl_kk_cloud_num_land = 300.;
+  p->rcl_fzrab = -0.66;
+  p->rcl_const5r = pi / (6.) * fzrbb * ar * p->rcl_x1r * g6r;
+  p->rcl_const6r = -1. * (4. + br + x4r - p->rcl_x2r);
+  // cloud ice (RCL_CI/RCL_DI are the Morrison-Gettelman overrides, sucldp.F90:456-457)
+  const double ai = 0.069, bi = 2.0, ci = 100., di = 1.0, x1i = 2.0E6, x2i = 0.0, x4i = 0.0;
+  const double g1i = lanczos_gamma_f32coef(bi + 1.0 + x4i);
+  const double g2i = lanczos_gamma_f32coef(x4i + 2.0);
+  const double g3i = lanczos_gamma_f32coef((di + 5.0 + 2.0 * x4i) / 2.0);
+  const double g4i = lanczos_gamma_f32coef(di + bi + 1.0 + x4i);
+  p->rcl_const1i = 1.0 / (ai * x1i * g1i);
+  p->rcl_const2i = 1.0 * pi * x1i;
+  p->rcl_const3i = 0.44 * std::pow(0.6, 1.0 / 3.0) * std::pow(ci, 0.5) * g3i / std::pow(1.717E-5, 0.5);
+  p->rcl_const4i = (2.0 + x4i - x2i) / (bi + 1.0 + x4i - x2i);
+  p->rcl_const5i = (5.0 + di + 2.0 * x4i - 2.0 * x2i) / (2.0 * (bi + 1. + x4i - x2i));
+  p->rcl_const6i = g2i;
+  p->rcl_const7i = ci * g4i / g1i;
+  p->rcl_apb1 = 7.14E11;
+  p->rcl_apb2 = 1.16E8;
+  p->rcl_apb3 = 2.416E2;
+  // snow
+  const double as = 0.069, bs = 2.0, cs = 16.8 * vplrg, ds = 0.527, x2s = 0.0, x4s = 0.0;
+  p->rcl_x1s = 2.0E6;
+  const double g1s = lanczos_gamma_f32coef(bs + 1.0 + x4s);
+  const double g2s = lanczos_gamma_f32coef(3.0 + ds + x4s);
+  const double g3s = lanczos_gamma_f32coef((ds + 5.0 + 2.0 * x4s) / 2.0);
+  const double g4s = lanczos_gamma_f32coef(x4s + 2.0);
+  p->rcl_lam1s = as * p->rcl_x1s * lanczos_gamma_f32coef(bs + 1.0 + x4s);
+  p->rcl_lam2s = 1.0 / (bs + 1. + x4s - x2s);
+  p->rcl_const1s = 1.0 / (as * p->rcl_x1s * g1s);
+  p->rcl_const2s = 1.0 * pi * p->rcl_x1s;
+  p->rcl_const3s = 0.44 * std::pow(0.6, 1.0 / 3.0) * std::pow(cs, 0.5) * g3s / std::pow(1.717E-5, 0.5);
+  p->rcl_const4s = (2.0 + x4s - x2s) / (bs + 1.0 + x4s - x2s);
+  p->rcl_const5s = (5.0 + ds + 2.0 * x4s - 2.0 * x2s) / (2.0 * (bs + 1. + x4s - x2s));
+  p->rcl_const6s = g4s;
+  p->rcl_const7s = pi * 0.25 * p->rcl_x1s * cs * g2s;
+  p->rcl_const8s = (3.0 + ds + x4s - x2s) / (bs + 1.0 + x4s - x2s);
+  // switches and the remaining derived types
+  p->ncldtop = ncldtop;
+  p->lcldbud_timeint = 1;
+  p->rssicefactor = std::fmin(tsphy / p->rkooptau, 1.0);
+  p->lmfdsnow = 1;
+  p->rmfadvw = 0.0;
+  p->rmfadvwdd = 0.0;
+  p->rcloud_frac_std = 1.0;
+  return CLOUDSC_OK;
+}
+
+int32_t cloudsc_b200_ncldtop(int32_t klev, const double *stpre, double rcldtopp) {
+  if (!stpre || klev < 2) return -1;
+  int32_t nc = 2;
+  for (int32_t jlev = klev; jlev >= 2; --jlev)
+    if (stpre[jlev - 1] > rcldtopp) nc = jlev;
+  return nc;
+}
+
+int cloudsc_b200_setup(const cloudsc_params *p) {
+  if (!p) return fail(CLOUDSC_E_NULL, "params is NULL");
+  if (p->magic != CLOUDSC_PARAMS_MAGIC || p->version != 1)
+    return fail(CLOUDSC_E_PARAMS, "bad params magic or version");
+  if (!params_supported(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED,
+                "a switch this build does not implement is on (aerosol, inhomogeneity, SPP or budgets)");
+  if (p->ncldtop < 2) return fail(CLOUDSC_E_SHAPE, "ncldtop must be >= 2");
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_params = *p;
+    g_have_params = true;
+    ++g_gen;
+  }
+  return ensure_params(nullptr);
+}
+
+int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm) {
+  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (threads_per_cta < 32 || threads_per_cta > 256 || threads_per_cta % 32)
+    return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32 in [32,256]");
+  if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(CLOUDSC_E_SHAPE, "ctas_per_sm must be in [0,32]");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_threads[precision] = threads_per_cta;
+  g_ctas_per_sm[precision] = ctas_per_sm;
+  return CLOUDSC_OK;
+}
+
+static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaStream_t stream) {
+  int threads, tiles;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    threads = g_threads[precision];
+  }
+  tiles = sh.ngpblks * ((sh.nproma + threads - 1) / threads);
+  int grid = grid_for(precision, tiles, threads);
+  cudaError_t e = launch(precision, f, sh, threads, grid, stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+int cloudsc_b200_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi, const double *pap,
+    const double *paph, const double *plsm, const int32_t *ldcum, const int32_t *ktype,
+    const double *peis, const double *plu, double *plude, const double *pludeli,
+    const double *psnde, const double *pmfu, const double *pmfd, const double *pa,
+    const double *pclv, double *pcovptot, double *prainfrac_toprfz, double *pfsqlf,
+    double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
+    double *pfplsn, double *pfhpsl, double *pfhpsn, uint32_t *ncounters, int32_t precision,
+    void *stream) {
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  const void *req[] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+                       ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
+                       pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+                       pmfd, pa, pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng,
+                       pfsqrf, pfsqsf, pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl,
+                       pfhpsn};
+  for (const void *q : req)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  rc = ensure_params(nullptr);
+  if (rc) return rc;
+  Fields f = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+              ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl, pvfi,
+              pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu, pmfd, pa,
+              pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng, pfsqrf, pfsqsf,
+              pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl, pfhpsn, ncounters};
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
+  return launch_checked(precision, f, sh, (cudaStream_t)stream);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Host-pointer paths.  Device memory comes from a per-thread workspace that is
+// grown on demand and kept until the thread exits, so repeated calls from the
+// same OpenMP thread (EC_PHYS_DRV calls CLOUDSC once per block) allocate once.
+// ---------------------------------------------------------------------------
+namespace {
+
+// Per-block sizes (in elements) of every array the kernel touches, in the
+// order of the Fields struct.
+struct Layout {
+  size_t s1, s2, s2h;
+  size_t n_in2 = 0;
+};
+
+enum Kind { K2, K3_5, K3_4, K3_2, KH, K1 };
+struct Arr {
+  Kind kind;
+  bool in, out;  // copied to / from the device
+};
+// Fields order: pt, pq, cml_t, cml_q, cml_a, cml_cld, loc_t, loc_q, loc_a, loc_cld,
+// pvfl, pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+// pmfd, pa, pclv, pcovptot, prainfrac, 14 fluxes
+const Arr kArrs[42] = {
+    {K2, 1, 0},   {K2, 1, 0},   {K2, 1, 0},   {K2, 1, 0},   {K2, 1, 0},   {K3_5, 1, 0},
+    {K2, 0, 1},   {K2, 0, 1},   {K2, 0, 1},   {K3_5, 0, 1}, {K2, 1, 0},   {K2, 1, 0},
+    {K2, 1, 0},   {KH, 1, 0},   {K1, 1, 0},   {K1, 1, 0},   {K1, 1, 0},   {K1, 1, 0},
+    {K2, 1, 0},   {K2, 1, 1},   {K3_4, 1, 0}, {K3_2, 1, 0}, {K2, 1, 0},   {K2, 1, 0},
+    {K2, 1, 0},   {K3_5, 1, 0}, {K2, 0, 1},   {K1, 0, 1},   {KH, 0, 1},   {KH, 0, 1},
+    {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},
+    {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1},   {KH, 0, 1}};
+
+size_t elems(Kind k, size_t np, size_t klev) {
+  switch (k) {
+    case K2: return np * klev;
+    case K3_5: return np * klev * 5;
+    case K3_4: return np * klev * 4;
+    case K3_2: return np * klev * 2;
+    case KH: return np * (klev + 1);
+    default: return np;
+  }
+}
+// rows of nproma elements per block (for strided column-range copies)
+size_t rows(Kind k, size_t klev) { return elems(k, 1, klev); }
+
+struct Workspace {
+  int dev = -1;
+  char *buf = nullptr;
+  size_t cap = 0;
+  cudaStream_t st[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_in[4], ev_done[4], ev_out[4];
+  bool events = false;
+  uint32_t *counter = nullptr;
+  ~Workspace() {
+    // Thread exit: release without touching a torn-down context.
+    if (buf) cudaFree(buf);
+    if (counter) cudaFree(counter);
+    for (auto &s : st)
+      if (s) cudaStreamDestroy(s);
+    if (events)
+      for (int i = 0; i < 4; ++i) {
+        cudaEventDestroy(ev_in[i]);
+        cudaEventDestroy(ev_done[i]);
+        cudaEventDestroy(ev_out[i]);
+      }
+  }
+  int prepare(int device, size_t bytes) {
+    cudaError_t e;
+    if (dev != device) {
+      // a different device: drop everything owned on the old one
+      if (buf) cudaFree(buf);
+      if (counter) cudaFree(counter);
+      buf = nullptr;
+      counter = nullptr;
+      cap = 0;
+      for (auto &s : st) s = nullptr;
+      events = false;
+      dev = device;
+    }
+    if (!st[0])
+      for (auto &s : st) {
+        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaStreamCreate", e);
+      }
+    if (!events) {
+      for (int i = 0; i < 4; ++i) {
+        cudaEventCreateWithFlags(&ev_in[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev_done[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&ev_out[i], cudaEventDisableTiming);
+      }
+      events = true;
+    }
+    if (!counter) {
+      e = cudaMalloc(&counter, 64);
+      if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaMalloc(counter)", e);
+    }
+    if (bytes > cap) {
+      if (buf) cudaFree(buf);
+      buf = nullptr;
+      e = cudaMalloc(&buf, bytes);
+      if (e != cudaSuccess) {
+        cap = 0;
+        return fail(CLOUDSC_E_CUDA, "cudaMalloc(workspace)", e);
+      }
+      cap = bytes;
+    }
+    return CLOUDSC_OK;
+  }
+};
+
+thread_local Workspace t_ws;
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Carve the device arrays of `nblk` blocks out of `base`; returns bytes used.
+size_t carve(char *base, size_t np, size_t klev, size_t nblk, void *dptr[42]) {
+  size_t off = 0;
+  for (int i = 0; i < 42; ++i) {
+    size_t esz = (kArrs[i].kind == K1 && (i == 15 || i == 16)) ? 4 : 8;
+    size_t n = elems(kArrs[i].kind, np, klev) * nblk * esz;
+    if (dptr) dptr[i] = base ? base + off : nullptr;
+    off += align256(n);
+  }
+  return off;
+}
+
+Fields fields_from(void *d[42], uint32_t *counter) {
+  Fields f;
+  f.pt = (const double *)d[0]; f.pq = (const double *)d[1]; f.cml_t = (const double *)d[2];
+  f.cml_q = (const double *)d[3]; f.cml_a = (const double *)d[4]; f.cml_cld = (const double *)d[5];
+  f.loc_t = (double *)d[6]; f.loc_q = (double *)d[7]; f.loc_a = (double *)d[8]; f.loc_cld = (double *)d[9];
+  f.pvfl = (const double *)d[10]; f.pvfi = (const double *)d[11]; f.pap = (const double *)d[12];
+  f.paph = (const double *)d[13]; f.plsm = (const double *)d[14]; f.ldcum = (const int32_t *)d[15];
+  f.ktype = (const int32_t *)d[16]; f.peis = (const double *)d[17]; f.plu = (const double *)d[18];
+  f.plude = (double *)d[19]; f.pludeli = (const double *)d[20]; f.psnde = (const double *)d[21];
+  f.pmfu = (const double *)d[22]; f.pmfd = (const double *)d[23]; f.pa = (const double *)d[24];
+  f.pclv = (const double *)d[25]; f.pcovptot = (double *)d[26]; f.prainfrac_toprfz = (double *)d[27];
+  f.pfsqlf = (double *)d[28]; f.pfsqif = (double *)d[29]; f.pfcqnng = (double *)d[30];
+  f.pfcqlng = (double *)d[31]; f.pfsqrf = (double *)d[32]; f.pfsqsf = (double *)d[33];
+  f.pfcqrng = (double *)d[34]; f.pfcqsng = (double *)d[35]; f.pfsqltur = (double *)d[36];
+  f.pfsqitur = (double *)d[37]; f.pfplsl = (double *)d[38]; f.pfplsn = (double *)d[39];
+  f.pfhpsl = (double *)d[40]; f.pfhpsn = (double *)d[41];
+  f.ncounters = counter;
+  return f;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cloudsc_b200_block(
+    const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
+    int32_t lddiag, double ptsphy, const double *pt, const double *pq,
+    const double *ptendency_cml_t, const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_cld, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_cld, const double *pvfa, const double *pvfl,
+    const double *pvfi, const double *pdyna, const double *pdynl, const double *pdyni,
+    const double *pdynr, const double *pdyns, const double *phrsw, const double *phrlw,
+    const double *pvervel, const double *pap, const double *paph, const double *pgeom,
+    const double *plsm, const double *pgaw, const int32_t *ldcum, const int32_t *kctop,
+    const int32_t *ktype, const int32_t *kpbltype, double *peis, const double *plu, double *plude,
+    const double *pludeli, const double *psnde, const double *pmfu, const double *pmfd,
+    const double *pgp2dspp, int32_t ldslphy, const double *pa, const double *pclv,
+    const double *plcrit_aer, const double *picrit_aer, const double *pre_ice, const double *pccn,
+    const double *pnice, double *pcovptot, double *pfsd, double *prainfrac_toprfz, double *pfsqlf,
+    double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
+    double *pfplsn, double *pfhpsl, double *pfhpsn, double *pextra, int32_t kfldx) {
+  (void)lddiag; (void)pvfa; (void)pdyna; (void)pdynl; (void)pdyni; (void)pdynr; (void)pdyns;
+  (void)phrsw; (void)phrlw; (void)pvervel; (void)pgeom; (void)pgaw; (void)kctop; (void)kpbltype;
+  (void)pgp2dspp; (void)ldslphy; (void)plcrit_aer; (void)picrit_aer; (void)pre_ice; (void)pccn;
+  (void)pnice; (void)pfsd; (void)pextra; (void)kfldx;
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
+    return fail(CLOUDSC_E_SHAPE, "inconsistent KIDIA/KFDIA/KLON/KLEV");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  const void *host[42] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+                          ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
+                          pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+                          pmfd, pa, pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng,
+                          pfsqrf, pfsqsf, pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl,
+                          pfhpsn};
+  for (const void *q : host)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  int dev = 0;
+  rc = ensure_params(&dev);
+  if (rc) return rc;
+  const size_t np = klon, kl = klev;
+  size_t bytes = carve(nullptr, np, kl, 1, nullptr);
+  rc = t_ws.prepare(dev, bytes);
+  if (rc) return rc;
+  void *d[42];
+  carve(t_ws.buf, np, kl, 1, d);
+  cudaStream_t s = t_ws.st[0];
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+    if (!kArrs[i].in) continue;
+    size_t esz = (i == 15 || i == 16) ? 4 : 8;
+    e = cudaMemcpyAsync(d[i], host[i], elems(kArrs[i].kind, np, kl) * esz, cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  Fields f = fields_from(d, t_ws.counter);
+  Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
+  rc = launch_checked(0, f, sh, s);
+  if (rc) return rc;
+  // copy back only columns KIDIA..KFDIA of every output row
+  const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
+  for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+    if (!kArrs[i].out) continue;
+    size_t nrow = rows(kArrs[i].kind, kl);
+    e = cudaMemcpy2DAsync((double *)host[i] + c0, np * 8, (double *)d[i] + c0, np * 8, ncol * 8, nrow,
+                          cudaMemcpyDeviceToHost, s);
+  }
+  uint32_t nwarn = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
+  return (int)nwarn;
+}
+
+int cloudsc_b200_batched_host(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi, const double *pap,
+    const double *paph, const double *plsm, const int32_t *ldcum, const int32_t *ktype,
+    const double *peis, const double *plu, double *plude, const double *pludeli,
+    const double *psnde, const double *pmfu, const double *pmfd, const double *pa,
+    const double *pclv, double *pcovptot, double *prainfrac_toprfz, double *pfsqlf,
+    double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
+    double *pfplsn, double *pfhpsl, double *pfhpsn, int32_t precision, int32_t chunk_blocks) {
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  const void *host[42] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+                          ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
+                          pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+                          pmfd, pa, pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng,
+                          pfsqrf, pfsqsf, pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl,
+                          pfhpsn};
+  for (const void *q : host)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  int dev = 0;
+  rc = ensure_params(&dev);
+  if (rc) return rc;
+  const size_t np = nproma, kl = klev;
+  int cb = chunk_blocks > 0 ? chunk_blocks : 64;
+  if (cb > ngpblks) cb = ngpblks;
+  const int nslot = 3;
+  const size_t slot_bytes = carve(nullptr, np, kl, cb, nullptr);
+  rc = t_ws.prepare(dev, slot_bytes * nslot);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), t_ws.st[1]);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaMemsetAsync", e);
+  const int nchunk = (ngpblks + cb - 1) / cb;
+  for (int c = 0; c < nchunk && e == cudaSuccess; ++c) {
+    const int slot = c % nslot;
+    const int b0 = c * cb, nb = (b0 + cb <= ngpblks) ? cb : ngpblks - b0;
+    void *d[42];
+    carve(t_ws.buf + slot * slot_bytes, np, kl, cb, d);
+    // the slot is free once its previous D2H has finished
+    if (c >= nslot) e = cudaStreamWaitEvent(t_ws.st[0], t_ws.ev_out[slot], 0);
+    for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+      if (!kArrs[i].in) continue;
+      size_t esz = (i == 15 || i == 16) ? 4 : 8;
+      size_t per = elems(kArrs[i].kind, np, kl) * esz;
+      e = cudaMemcpyAsync(d[i], (const char *)host[i] + (size_t)b0 * per, per * nb, cudaMemcpyHostToDevice,
+                          t_ws.st[0]);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_in[slot], t_ws.st[0]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[1], t_ws.ev_in[slot], 0);
+    if (e != cudaSuccess) break;
+    Fields f = fields_from(d, t_ws.counter);
+    int ngptot_c = ngptot - b0 * nproma;
+    if (ngptot_c > nb * nproma) ngptot_c = nb * nproma;
+    Shape sh = {nproma, klev, nb, ngptot_c, 0, ptsphy};
+    rc = launch_checked(precision, f, sh, t_ws.st[1]);
+    if (rc) return rc;
+    e = cudaEventRecord(t_ws.ev_done[slot], t_ws.st[1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[slot], 0);
+    // Whole blocks are copied back in one piece; a partial last block (columns
+    // beyond NGPTOT) returns only its computed columns, leaving the padding
+    // of the caller's array untouched as the reference does.
+    const int icend_last = ngptot_c - (nb - 1) * nproma;
+    const int nfull = (icend_last == nproma) ? nb : nb - 1;
+    for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+      if (!kArrs[i].out) continue;
+      size_t per = elems(kArrs[i].kind, np, kl) * 8;
+      char *hb = (char *)host[i] + (size_t)b0 * per;
+      if (nfull > 0)
+        e = cudaMemcpyAsync(hb, d[i], per * nfull, cudaMemcpyDeviceToHost, t_ws.st[2]);
+      if (e == cudaSuccess && nfull < nb)
+        e = cudaMemcpy2DAsync(hb + per * nfull, np * 8, (char *)d[i] + per * nfull, np * 8,
+                              (size_t)icend_last * 8, rows(kArrs[i].kind, kl), cudaMemcpyDeviceToHost,
+                              t_ws.st[2]);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_out[slot], t_ws.st[2]);
+  }
+  uint32_t nwarn = 0;
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[(nchunk - 1) % nslot], 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, t_ws.st[2]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t_ws.st[2]);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "pipelined host path", e);
+  return (int)nwarn;
+}
+
+}  // extern "C"

@@ -1,0 +1,45 @@
+// Shared device-side definitions for the CLOUDSC kernels (FP64 and FP32-mixed).
+//
+// Species indices follow yoecldp.F90:102-107 shifted to 0-based:
+//   L=0 (NCLDQL) cloud liquid, I=1 (NCLDQI) cloud ice, R=2 (NCLDQR) rain,
+//   S=3 (NCLDQS) snow, V=4 (NCLDQV) vapour.
+#pragma once
+#include <cstdint>
+#include "../../include/cloudsc_b200.h"
+
+namespace cloudsc {
+
+constexpr int L = 0, I = 1, R = 2, S = 3, V = 4;
+
+// Loop-invariant values hoisted out of the level loop and computed once on the
+// host with the same libm expression the reference evaluates per point.
+struct Derived {
+  double zconst_pow_land;  // RCL_KK_CLOUD_NUM_LAND**RCL_KKBAUN (cloudsc.F90:2179-2181)
+  double zconst_pow_sea;   // RCL_KK_CLOUD_NUM_SEA**RCL_KKBAUN
+  double flt_0p4;          // REAL(0.4,4) widened: the default-REAL exponent at :2320,:2980
+  double flt_0p8;          // REAL(0.8,4) widened: the threshold at :2889
+};
+
+// Pointers of the batched (NPROMA, <dims>, NGPBLKS) arrays; block ib of an
+// array with per-block size S starts at ib*S.
+struct Fields {
+  const double *pt, *pq, *cml_t, *cml_q, *cml_a, *cml_cld;
+  double *loc_t, *loc_q, *loc_a, *loc_cld;
+  const double *pvfl, *pvfi, *pap, *paph, *plsm;
+  const int32_t *ldcum, *ktype;
+  const double *peis, *plu;
+  double *plude;
+  const double *pludeli, *psnde, *pmfu, *pmfd, *pa, *pclv;
+  double *pcovptot, *prainfrac_toprfz;
+  double *pfsqlf, *pfsqif, *pfcqnng, *pfcqlng, *pfsqrf, *pfsqsf, *pfcqrng, *pfcqsng;
+  double *pfsqltur, *pfsqitur, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
+  uint32_t *ncounters;
+};
+
+struct Shape {
+  int nproma, klev, ngpblks, ngptot;
+  int kidia0;  // first column of every block computed (0-based KIDIA-1)
+  double ptsphy;
+};
+
+}  // namespace cloudsc

@@ -1,0 +1,101 @@
+"""The arrays of the batched CLOUDSC call, in C-ABI argument order.
+
+Every array is stored as the Fortran (NPROMA, <dims>, NGPBLKS) block layout of
+EC_PHYS_DRV (ifs-source/arpifs/phys_ec/ec_phys_drv.F90:145-185); in numpy /
+torch C order that is shape (NGPBLKS, <dims reversed>, NPROMA):
+
+    "2d"  (KLEV, NPROMA)          a (KLON,KLEV) field
+    "3dN" (N, KLEV, NPROMA)       a (KLON,KLEV,N) field
+    "hl"  (KLEV+1, NPROMA)        a half-level (KLON,KLEV+1) field
+    "1d"  (NPROMA,)               a (KLON) field
+"""
+import numpy as np
+
+# (name, kind, dtype, role) with role in {"in", "out", "inout"}; the order is
+# the argument order of cloudsc_b200_batched / cloudsc_b200_batched_host.
+BATCHED_FIELDS = [
+    ("pt", "2d", np.float64, "in"),
+    ("pq", "2d", np.float64, "in"),
+    ("tendency_cml_t", "2d", np.float64, "in"),
+    ("tendency_cml_q", "2d", np.float64, "in"),
+    ("tendency_cml_a", "2d", np.float64, "in"),
+    ("tendency_cml_cld", "3d5", np.float64, "in"),
+    ("tendency_loc_t", "2d", np.float64, "out"),
+    ("tendency_loc_q", "2d", np.float64, "out"),
+    ("tendency_loc_a", "2d", np.float64, "out"),
+    ("tendency_loc_cld", "3d5", np.float64, "out"),
+    ("pvfl", "2d", np.float64, "in"),
+    ("pvfi", "2d", np.float64, "in"),
+    ("pap", "2d", np.float64, "in"),
+    ("paph", "hl", np.float64, "in"),
+    ("plsm", "1d", np.float64, "in"),
+    ("ldcum", "1d", np.int32, "in"),
+    ("ktype", "1d", np.int32, "in"),
+    ("peis", "1d", np.float64, "in"),
+    ("plu", "2d", np.float64, "in"),
+    ("plude", "2d", np.float64, "inout"),
+    ("pludeli", "3d4", np.float64, "in"),
+    ("psnde", "3d2", np.float64, "in"),
+    ("pmfu", "2d", np.float64, "in"),
+    ("pmfd", "2d", np.float64, "in"),
+    ("pa", "2d", np.float64, "in"),
+    ("pclv", "3d5", np.float64, "in"),
+    ("pcovptot", "2d", np.float64, "out"),
+    ("prainfrac_toprfz", "1d", np.float64, "out"),
+    ("pfsqlf", "hl", np.float64, "out"),
+    ("pfsqif", "hl", np.float64, "out"),
+    ("pfcqnng", "hl", np.float64, "out"),
+    ("pfcqlng", "hl", np.float64, "out"),
+    ("pfsqrf", "hl", np.float64, "out"),
+    ("pfsqsf", "hl", np.float64, "out"),
+    ("pfcqrng", "hl", np.float64, "out"),
+    ("pfcqsng", "hl", np.float64, "out"),
+    ("pfsqltur", "hl", np.float64, "out"),
+    ("pfsqitur", "hl", np.float64, "out"),
+    ("pfplsl", "hl", np.float64, "out"),
+    ("pfplsn", "hl", np.float64, "out"),
+    ("pfhpsl", "hl", np.float64, "out"),
+    ("pfhpsn", "hl", np.float64, "out"),
+]
+FIELD_INDEX = {f[0]: i for i, f in enumerate(BATCHED_FIELDS)}
+INPUT_NAMES = [f[0] for f in BATCHED_FIELDS if f[3] in ("in", "inout")]
+OUTPUT_NAMES = [f[0] for f in BATCHED_FIELDS if f[3] in ("out", "inout")]
+KIND = {f[0]: f[1] for f in BATCHED_FIELDS}
+DTYPE = {f[0]: f[2] for f in BATCHED_FIELDS}
+
+
+def block_shape(kind, nproma, klev):
+    if kind == "2d":
+        return (klev, nproma)
+    if kind == "hl":
+        return (klev + 1, nproma)
+    if kind == "1d":
+        return (nproma,)
+    if kind.startswith("3d"):
+        return (int(kind[2:]), klev, nproma)
+    raise ValueError(kind)
+
+
+def batched_shape(name, ngpblks, nproma, klev):
+    return (ngpblks,) + block_shape(KIND[name], nproma, klev)
+
+
+def alloc(ngpblks, nproma, klev, names=None, alloc_fn=None):
+    """Zero-filled arrays for `names` (default: all) in the batched layout."""
+    names = names or [f[0] for f in BATCHED_FIELDS]
+    out = {}
+    for n in names:
+        shp = batched_shape(n, ngpblks, nproma, klev)
+        out[n] = alloc_fn(shp, DTYPE[n]) if alloc_fn else np.zeros(shp, DTYPE[n])
+    return out
+
+
+# Algorithmic HBM traffic of one FP64 column (bytes): every array element the
+# default configuration reads or writes, once.
+def bytes_per_column(klev=137, fp=8):
+    reads_lv = 26  # PT PQ CML_T CML_Q CML_A CML_CLD*4 PA PCLV*4 PAP PAPH PLU PLUDE
+    #                PLUDELI*2 PSNDE*2 PMFU PMFD PVFL PVFI
+    read = (reads_lv * klev + 1) * fp + 2 * fp + 2 * 4  # + extra PAPH half level, PLSM PEIS, KTYPE LDCUM
+    writes_lv = 9  # LOC_T LOC_Q LOC_A LOC_CLD*4 PCOVPTOT PLUDE
+    write = (writes_lv * klev + 14 * (klev + 1) + 1) * fp
+    return read, write

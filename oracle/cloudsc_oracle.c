@@ -1,0 +1,1193 @@
+/*
+ * ORACLE -- TEST INFRASTRUCTURE ONLY.  Never linked into the product library;
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
+ *
+ * Line-by-line CPU restatement of the reference's double-precision CLOUDSC:
+ *   ifs-source/arpifs/phys_ec/cloudsc.F90            (SUBROUTINE CLOUDSC)
+ *   ifs-source/arpifs/phys_ec/cloud_supersatcheck.F90:111-226
+ *   ifs-source/arpifs/function/fcttre.func.h:37-184   (saturation functions)
+ *   ifs-source/arpifs/function/fccld.func.h:26-27     (FOKOOP)
+ * in the reference's default configuration (options hard-wired at
+ * cloudsc.F90:727-793; LSPP, aerosol, inhomogeneity and budget switches off).
+ * Loop order (JK outer, JL inner), local arrays and the order of every
+ * floating-point operation follow the Fortran source; it is compiled with
+ * -O2 -ffp-contract=off (no FMA contraction, like the reference's -no-fma
+ * builds, compile_flags.cmake:535) and uses glibc exp/log/pow.
+ * Precision quirks reproduced: default-REAL (binary32) literals at
+ * cloudsc.F90:2320,2889,2980; the MIN(..)/ZCORQSMIX parenthesisation at :2733;
+ * the PFSQRF/PFSQSF/PFCQRNG/PFCQSNG recurrences at :4251-4256.
+ *
+ * Parity unpinned: no CLOUDSC golden vector exists in the reference and the
+ * Fortran cannot be compiled in this image; this restatement is the checker.
+ * Outputs the reference leaves undefined are written as zeros here:
+ * PCOVPTOT(:,1:NCLDTOP-1).  PTENDENCY_LOC_CLD(:,:,NCLV) and PFSD are not touched.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "oracle.h"
+
+#define NCLV 5
+#define NCLDQL 1
+#define NCLDQI 2
+#define NCLDQR 3
+#define NCLDQS 4
+#define NCLDQV 5
+
+/* 1-based Fortran-order accessors */
+#define A1(a, jl) (a)[(jl)-1]
+#define A2(a, jl, jk) (a)[((size_t)(jk)-1) * klon + ((jl)-1)]
+#define A3(a, jl, jk, jm, n2) (a)[(((size_t)(jm)-1) * (n2) + ((jk)-1)) * klon + ((jl)-1)]
+#define L2(a, jl, jm) (a)[((size_t)(jm)-1) * klon + ((jl)-1)]
+#define L3(a, jl, jm, jn) (a)[((((size_t)(jn)-1) * NCLV + ((jm)-1)) * klon) + ((jl)-1)]
+
+static inline double fmin_(double a, double b) { return a < b ? a : b; }
+static inline double fmax_(double a, double b) { return a > b ? a : b; }
+
+/* ---------------- fcttre.func.h / fccld.func.h ---------------- */
+static inline double foedelta(const cloudsc_params *p, double t) {
+  return fmax_(0.0, copysign(1.0, t - p->rtt));
+}
+static inline double foealfa(const cloudsc_params *p, double t) {
+  double x = (fmax_(p->rtice, fmin_(p->rtwat, t)) - p->rtice) * p->rtwat_rtice_r;
+  return fmin_(1.0, x * x);
+}
+static inline double foeewm(const cloudsc_params *p, double t) {
+  return p->r2es * (foealfa(p, t) * exp(p->r3les * (t - p->rtt) / (t - p->r4les)) +
+                    (1.0 - foealfa(p, t)) * exp(p->r3ies * (t - p->rtt) / (t - p->r4ies)));
+}
+static inline double foedem(const cloudsc_params *p, double t) {
+  double xl = t - p->r4les, xi = t - p->r4ies;
+  return foealfa(p, t) * p->r5alvcp * (1.0 / (xl * xl)) +
+         (1.0 - foealfa(p, t)) * p->r5alscp * (1.0 / (xi * xi));
+}
+static inline double foeldcpm(const cloudsc_params *p, double t) {
+  return foealfa(p, t) * p->ralvdcp + (1.0 - foealfa(p, t)) * p->ralsdcp;
+}
+static inline double foeeliq(const cloudsc_params *p, double t) {
+  return p->r2es * exp(p->r3les * (t - p->rtt) / (t - p->r4les));
+}
+static inline double foeeice(const cloudsc_params *p, double t) {
+  return p->r2es * exp(p->r3ies * (t - p->rtt) / (t - p->r4ies));
+}
+static inline double foeew(const cloudsc_params *p, double t) {
+  double d = foedelta(p, t);
+  return p->r2es * exp((p->r3les * d + p->r3ies * (1.0 - d)) * (t - p->rtt) /
+                       (t - (p->r4les * d + p->r4ies * (1.0 - d))));
+}
+static inline double foeeliq2ice(const cloudsc_params *p, double t) {
+  return exp((t - p->rtt) * (p->r3les / (t - p->r4les) - p->r3ies / (t - p->r4ies)));
+}
+static inline double fokoop(const cloudsc_params *p, double t) {
+  return fmin_(p->rkoop1 - p->rkoop2 * t, foeeliq2ice(p, t));
+}
+
+/* ---------------- cloud_supersatcheck.F90:111-226 (KFTLIQICE=1) ---------------- */
+static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, const double *pt,
+                          const double *pq, const double *pa, const double *pp,
+                          double *pt_adj, double *pq_adj, double *pa_adj, double *pl_adj,
+                          double *pi_adj) {
+  const double zepsec = 1.E-14;
+  for (int jl = kidia; jl <= kfdia; jl++) {
+    double za_upd = 0.0, zda = 0.0;
+    double zt = pt[jl - 1], zq = pq[jl - 1], za = pa[jl - 1];
+    double zp_r = 1.0 / pp[jl - 1];
+    zt = fmax_(zt, 160.0);
+    za = fmax_(fmin_(za, 1.0), 0.0);
+    /* ZRHC/ZSIGK (:128-133) are computed by the reference but never used */
+    double zfoeeliq = fmin_(foeeliq(p, zt) * zp_r, 0.5);
+    double zqsliq = zfoeeliq / (1.0 - p->retv * zfoeeliq);
+    (void)zqsliq;
+    double zfoeeice = fmin_(foeew(p, zt) * zp_r, 0.5);
+    double zfokoop = fmin_(zfoeeice * (p->rkoop1 - p->rkoop2 * zt), zfoeeliq);
+    double zqsliqk = zfokoop / (1.0 - p->retv * zfokoop);
+    double zfoealfa = foealfa(p, zt);
+    double zfoeemix = fmin_(foeewm(p, zt) * zp_r, 0.5);
+    double zcor = 1.0 / (1.0 - p->retv * zfoeemix);
+    double zqsmix = zfoeemix * zcor;
+    double zcorqsmix = 1.0 + zqsmix * zcor * foedem(p, zt);
+    zqsliqk = 0.5 * (zqsliqk + zqsmix);
+    double zqslim = za * zqsmix + (1.0 - za) * zqsliqk;
+    double zcond = fmax_(zq - zqslim, 0.0);
+    if (zcond > zepsec) {
+      double zfaci = zfoealfa + (1.0 - zfoealfa) * p->rssicefactor;
+      zda = (1.0 - za) * zfaci;
+      za_upd = za + zda;
+      zqslim = za_upd * zqsmix + (1.0 - za_upd) * zqsliqk;
+      zcond = (zq - zqslim) / zcorqsmix;
+    }
+    pt_adj[jl - 1] = foeldcpm(p, zt) * zcond;
+    pq_adj[jl - 1] = -zcond;
+    pa_adj[jl - 1] = zda;
+    pl_adj[jl - 1] = zcond * zfoealfa;
+    pi_adj[jl - 1] = zcond * (1.0 - zfoealfa);
+  }
+}
+
+static int params_supported(const cloudsc_params *p) {
+  if (p->laericeauto || p->laericesed || p->laerliqautolsp || p->laerliqcoll) return 0;
+  if (p->lcloud_inhomog || p->lrad_cloud_inhomog || p->lspp) return 0;
+  if (p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint) return 0;
+  return 1;
+}
+
+int oracle_cloudsc(
+    const cloudsc_params *p, int kidia, int kfdia, int klon, int klev, int lddiag,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_cld, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_cld, const double *pvfa,
+    const double *pvfl, const double *pvfi, const double *pdyna, const double *pdynl,
+    const double *pdyni, const double *pdynr, const double *pdyns, const double *phrsw,
+    const double *phrlw, const double *pvervel, const double *pap, const double *paph,
+    const double *pgeom, const double *plsm, const double *pgaw, const int32_t *ldcum,
+    const int32_t *kctop, const int32_t *ktype, const int32_t *kpbltype, double *peis,
+    const double *plu, double *plude, const double *pludeli, const double *psnde,
+    const double *pmfu, const double *pmfd, const double *pgp2dspp, int ldslphy,
+    const double *pa, const double *pclv, const double *plcrit_aer,
+    const double *picrit_aer, const double *pre_ice, const double *pccn,
+    const double *pnice, double *pcovptot, double *pfsd, double *prainfrac_toprfz,
+    double *pfsqlf, double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf,
+    double *pfsqsf, double *pfcqrng, double *pfcqsng, double *pfsqltur,
+    double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
+    double *pextra, int kfldx) {
+  (void)lddiag; (void)pvfa; (void)pdyna; (void)pdynl; (void)pdyni; (void)pdynr;
+  (void)pdyns; (void)phrsw; (void)phrlw; (void)pvervel; (void)pgeom; (void)pgaw;
+  (void)kctop; (void)kpbltype; (void)pgp2dspp; (void)ldslphy; (void)plcrit_aer;
+  (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice; (void)pfsd; (void)pextra;
+  (void)kfldx;
+
+  if (!p || p->magic != CLOUDSC_PARAMS_MAGIC) return CLOUDSC_E_PARAMS;
+  if (!params_supported(p)) return CLOUDSC_E_UNSUPPORTED;
+  if (kidia < 1 || kfdia > klon || kidia > kfdia || klev < 2) return CLOUDSC_E_SHAPE;
+  const int ncldtop = p->ncldtop;
+  if (ncldtop < 2 || ncldtop > klev) return CLOUDSC_E_SHAPE;
+  int nwarn = 0;
+
+  /* constants (cloudsc.F90:693-848) */
+  const double zepsilon = 100.0 * 0x1p-52; /* 100*EPSILON(1._JPRB) */
+  const int iphase[NCLV + 1] = {0, 1, 2, 1, 2, 0};
+  const int imelt[NCLV + 1] = {0, NCLDQI, NCLDQR, NCLDQS, NCLDQR, -99};
+  double zvqx[NCLV + 1];
+  int llfall[NCLV + 1];
+  zvqx[NCLDQV] = 0.0;
+  zvqx[NCLDQL] = 0.0;
+  zvqx[NCLDQI] = p->rvice;
+  zvqx[NCLDQR] = p->rvrain;
+  zvqx[NCLDQS] = p->rvsnow;
+  for (int jm = 1; jm <= NCLV; jm++) llfall[jm] = zvqx[jm] > 0.0;
+
+  const double zqtmst = 1.0 / ptsphy;
+  const double zrdcp = p->rd / p->rcpd;
+  const double zepsec = 1.E-14;
+  const double zrg_r = 1.0 / p->rg;
+  const double zrldcp = 1.0 / (p->ralsdcp - p->ralvdcp);
+  const double ztw1 = 1329.31, ztw2 = 0.0074615, ztw3 = 0.85E5, ztw4 = 40.637, ztw5 = 275.0;
+  const double flt_0p4 = (double)0.4f, flt_0p8 = (double)0.8f;
+
+  /* ---- local arrays ---- */
+  size_t n1 = (size_t)klon, n2 = (size_t)klon * klev, n2h = (size_t)klon * (klev + 1);
+  /* 67 (KLON) arrays, 13 (KLON,KLEV) arrays, 4 (KLON,KLEV,NCLV), 1 (KLON,KLEV+1,NCLV),
+     13 (KLON,NCLV) and 3 (KLON,NCLV,NCLV); sized with margin */
+  double *buf = (double *)calloc(
+      n1 * 80 + n2 * 16 + n2 * NCLV * 4 + n2h * NCLV + n1 * NCLV * 16 + n1 * NCLV * NCLV * 3,
+      sizeof(double));
+  if (!buf) return CLOUDSC_E_TOO_LARGE;
+  double *w = buf;
+#define TAKE(n) (w += (n), w - (n))
+  double *zadvw = TAKE(n1), *zadvwd = TAKE(n1), *zpaphd = TAKE(n1);
+  double *zliqcld = TAKE(n1), *zicecld = TAKE(n1), *zlicld = TAKE(n1), *zrainaut = TAKE(n1);
+  double *zrainacc = TAKE(n1), *zsnowaut = TAKE(n1), *zsnowrime = TAKE(n1), *zldefr = TAKE(n1);
+  double *zacust = TAKE(n1), *zqpretot = TAKE(n1), *zlfinalsum = TAKE(n1);
+  double *zsolab = TAKE(n1), *zsolac = TAKE(n1), *zicetot = TAKE(n1), *zdp = TAKE(n1);
+  double *zgdp = TAKE(n1), *zrho = TAKE(n1), *zdtgdp = TAKE(n1), *zrdtgdp = TAKE(n1);
+  double *zdtgdpf = TAKE(n1), *zdqsliqdt = TAKE(n1), *zdqsicedt = TAKE(n1), *zdqsmixdt = TAKE(n1);
+  double *zcorqsliq = TAKE(n1), *zcorqsice = TAKE(n1), *zcorqsmix = TAKE(n1);
+  double *zevaplimliq = TAKE(n1), *zevaplimice = TAKE(n1), *zevaplimmix = TAKE(n1);
+  double *zmf = TAKE(n1), *zdqs = TAKE(n1), *zldifdt = TAKE(n1), *zanewm1 = TAKE(n1);
+  double *zda = TAKE(n1), *zcovpclr = TAKE(n1), *zcovpmax = TAKE(n1), *zcovptot = TAKE(n1);
+  double *zcldtopdist = TAKE(n1), *zraincld = TAKE(n1), *zraincldm1 = TAKE(n1);
+  double *zsnowcld = TAKE(n1), *zsnowcldm1 = TAKE(n1), *zicenuclei = TAKE(n1);
+  double *zmeltmax = TAKE(n1), *zfrzmax = TAKE(n1), *zlamr = TAKE(n1), *zlams = TAKE(n1);
+  double *zlami = TAKE(n1), *zn0r = TAKE(n1), *zn0s = TAKE(n1), *zn0i = TAKE(n1);
+  double *zpsacr = TAKE(n1), *zpiacr = TAKE(n1), *zpsdep = TAKE(n1), *zsinksum = TAKE(n1);
+  double *zq_upd = TAKE(n1), *zt_upd = TAKE(n1), *za_upd = TAKE(n1);
+  double *zt_adj = TAKE(n1), *zq_adj = TAKE(n1), *za_adj = TAKE(n1), *zl_adj = TAKE(n1);
+  double *zi_adj = TAKE(n1);
+  int *llrainliq = (int *)TAKE(n1); /* n1 doubles >= n1 ints */
+
+  double *ztp1 = TAKE(n2), *zli = TAKE(n2), *za = TAKE(n2), *zaorig = TAKE(n2);
+  double *zliqfrac = TAKE(n2), *zicefrac = TAKE(n2), *zfoealfa = TAKE(n2);
+  double *zfoeewm = TAKE(n2), *zfoeew = TAKE(n2), *zfoeeliqt = TAKE(n2);
+  double *zqsmix = TAKE(n2), *zqsliq = TAKE(n2), *zqsice = TAKE(n2);
+  double *zqx = TAKE(n2 * NCLV), *zqx0 = TAKE(n2 * NCLV), *zlneg = TAKE(n2 * NCLV);
+  double *zqxn2d = TAKE(n2 * NCLV);
+  double *zpfplsx = TAKE(n2h * NCLV);
+  double *zqxn = TAKE(n1 * NCLV), *zqxfg = TAKE(n1 * NCLV), *zqxnm1 = TAKE(n1 * NCLV);
+  double *zfluxq = TAKE(n1 * NCLV), *zfallsink = TAKE(n1 * NCLV), *zfallsrce = TAKE(n1 * NCLV);
+  double *zfallspeed = TAKE(n1 * NCLV), *zconvsrce = TAKE(n1 * NCLV), *zconvsink = TAKE(n1 * NCLV);
+  double *zlcust = TAKE(n1 * NCLV), *zratio = TAKE(n1 * NCLV);
+  int *iorder = (int *)TAKE(n1 * NCLV);
+  int *llindex3 = (int *)TAKE(n1 * NCLV);
+  double *zsolqa = TAKE(n1 * NCLV * NCLV), *zsolqb = TAKE(n1 * NCLV * NCLV);
+  double *zqlhs = TAKE(n1 * NCLV * NCLV);
+#undef TAKE
+
+  int jl, jk, jm, jn, jo, ik;
+
+  /* cloudsc.F90:696-703 */
+  for (jl = kidia; jl <= kfdia; jl++) {
+    A1(zadvw, jl) = 1.0;
+    A1(zadvwd, jl) = 1.0;
+    if (A1(ktype, jl) == 1 && p->rmfadvw > 0) {
+      A1(zadvw, jl) = 1.0 - p->rmfadvw;
+      A1(zadvwd, jl) = 1.0 - p->rmfadvw * p->rmfadvwdd;
+    }
+  }
+
+  /* 1. initial values (:963-1011) */
+  for (jk = 1; jk <= klev; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(ptendency_loc_t, jl, jk) = 0.0;
+      A2(ptendency_loc_q, jl, jk) = 0.0;
+      A2(ptendency_loc_a, jl, jk) = 0.0;
+    }
+  for (jm = 1; jm <= NCLV - 1; jm++)
+    for (jk = 1; jk <= klev; jk++)
+      for (jl = kidia; jl <= kfdia; jl++) A3(ptendency_loc_cld, jl, jk, jm, klev) = 0.0;
+
+  for (jk = 1; jk <= klev; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(ztp1, jl, jk) = A2(pt, jl, jk) + ptsphy * A2(ptendency_cml_t, jl, jk);
+      A3(zqx, jl, jk, NCLDQV, klev) = A2(pq, jl, jk) + ptsphy * A2(ptendency_cml_q, jl, jk);
+      A3(zqx0, jl, jk, NCLDQV, klev) = A2(pq, jl, jk) + ptsphy * A2(ptendency_cml_q, jl, jk);
+      A2(za, jl, jk) = A2(pa, jl, jk) + ptsphy * A2(ptendency_cml_a, jl, jk);
+      A2(zaorig, jl, jk) = A2(pa, jl, jk) + ptsphy * A2(ptendency_cml_a, jl, jk);
+    }
+  for (jm = 1; jm <= NCLV - 1; jm++)
+    for (jk = 1; jk <= klev; jk++)
+      for (jl = kidia; jl <= kfdia; jl++) {
+        A3(zqx, jl, jk, jm, klev) =
+            A3(pclv, jl, jk, jm, klev) + ptsphy * A3(ptendency_cml_cld, jl, jk, jm, klev);
+        A3(zqx0, jl, jk, jm, klev) =
+            A3(pclv, jl, jk, jm, klev) + ptsphy * A3(ptendency_cml_cld, jl, jk, jm, klev);
+      }
+  /* ZPFPLSX, ZQXN2D, ZLNEG are zero from calloc (:1007-1009) */
+  for (jl = kidia; jl <= kfdia; jl++) {
+    A1(prainfrac_toprfz, jl) = 0.0;
+    A1(llrainliq, jl) = 1;
+  }
+  /* tropopause search (:1016-1027) is dead code: ZTRPAUS is never used */
+
+  /* saturation values (:1087-1115) */
+  for (jk = 1; jk <= klev; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double t = A2(ztp1, jl, jk), pap_ = A2(pap, jl, jk);
+      A2(zfoealfa, jl, jk) = foealfa(p, t);
+      A2(zfoeewm, jl, jk) = fmin_(foeewm(p, t) / pap_, 0.5);
+      A2(zqsmix, jl, jk) = A2(zfoeewm, jl, jk);
+      A2(zqsmix, jl, jk) = A2(zqsmix, jl, jk) / (1.0 - p->retv * A2(zqsmix, jl, jk));
+      double zalfa = foedelta(p, t);
+      A2(zfoeew, jl, jk) = fmin_((zalfa * foeeliq(p, t) + (1.0 - zalfa) * foeeice(p, t)) / pap_, 0.5);
+      A2(zfoeew, jl, jk) = fmin_(0.5, A2(zfoeew, jl, jk));
+      A2(zqsice, jl, jk) = A2(zfoeew, jl, jk) / (1.0 - p->retv * A2(zfoeew, jl, jk));
+      A2(zfoeeliqt, jl, jk) = fmin_(foeeliq(p, t) / pap_, 0.5);
+      A2(zqsliq, jl, jk) = A2(zfoeeliqt, jl, jk);
+      A2(zqsliq, jl, jk) = A2(zqsliq, jl, jk) / (1.0 - p->retv * A2(zqsliq, jl, jk));
+    }
+
+  /* 2. tidy up (:1127-1199) */
+  for (jk = 1; jk <= klev; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A3(zqx, jl, jk, NCLDQL, klev) + A3(zqx, jl, jk, NCLDQI, klev) < p->rlmin ||
+          A2(za, jl, jk) < p->ramin) {
+        double zqadj;
+        A3(zlneg, jl, jk, NCLDQL, klev) = A3(zlneg, jl, jk, NCLDQL, klev) + A3(zqx, jl, jk, NCLDQL, klev);
+        zqadj = A3(zqx, jl, jk, NCLDQL, klev) * zqtmst;
+        A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + zqadj;
+        A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) - p->ralvdcp * zqadj;
+        A3(zqx, jl, jk, NCLDQV, klev) = A3(zqx, jl, jk, NCLDQV, klev) + A3(zqx, jl, jk, NCLDQL, klev);
+        A3(zqx, jl, jk, NCLDQL, klev) = 0.0;
+        A3(zlneg, jl, jk, NCLDQI, klev) = A3(zlneg, jl, jk, NCLDQI, klev) + A3(zqx, jl, jk, NCLDQI, klev);
+        zqadj = A3(zqx, jl, jk, NCLDQI, klev) * zqtmst;
+        A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + zqadj;
+        A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) - p->ralsdcp * zqadj;
+        A3(zqx, jl, jk, NCLDQV, klev) = A3(zqx, jl, jk, NCLDQV, klev) + A3(zqx, jl, jk, NCLDQI, klev);
+        A3(zqx, jl, jk, NCLDQI, klev) = 0.0;
+        A2(za, jl, jk) = 0.0;
+      }
+    }
+  for (jm = 1; jm <= NCLV - 1; jm++)
+    for (jk = 1; jk <= klev; jk++)
+      for (jl = kidia; jl <= kfdia; jl++) {
+        if (A3(zqx, jl, jk, jm, klev) < p->rlmin) {
+          A3(zlneg, jl, jk, jm, klev) = A3(zlneg, jl, jk, jm, klev) + A3(zqx, jl, jk, jm, klev);
+          double zqadj = A3(zqx, jl, jk, jm, klev) * zqtmst;
+          A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + zqadj;
+          if (iphase[jm] == 1) A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) - p->ralvdcp * zqadj;
+          if (iphase[jm] == 2) A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) - p->ralsdcp * zqadj;
+          A3(zqx, jl, jk, NCLDQV, klev) = A3(zqx, jl, jk, NCLDQV, klev) + A3(zqx, jl, jk, jm, klev);
+          A3(zqx, jl, jk, jm, klev) = 0.0;
+        }
+      }
+  for (jk = 1; jk <= klev; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(za, jl, jk) = fmax_(0.0, fmin_(1.0, A2(za, jl, jk)));
+      A2(zli, jl, jk) = A3(zqx, jl, jk, NCLDQL, klev) + A3(zqx, jl, jk, NCLDQI, klev);
+      if (A2(zli, jl, jk) > p->rlmin) {
+        A2(zliqfrac, jl, jk) = A3(zqx, jl, jk, NCLDQL, klev) / A2(zli, jl, jk);
+        A2(zicefrac, jl, jk) = 1.0 - A2(zliqfrac, jl, jk);
+      } else {
+        A2(zliqfrac, jl, jk) = 0.0;
+        A2(zicefrac, jl, jk) = 0.0;
+      }
+    }
+
+  /* reset single-level variables (:1205-1211) -- zero from calloc */
+
+  /* ================= level loop (:1219-4128) ================= */
+  for (jk = ncldtop; jk <= klev; jk++) {
+    for (jm = 1; jm <= NCLV; jm++)
+      for (jl = kidia; jl <= kfdia; jl++) L2(zqxfg, jl, jm) = A3(zqx, jl, jk, jm, klev);
+
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A1(zlicld, jl) = 0.0;
+      A1(zrainaut, jl) = 0.0;
+      A1(zrainacc, jl) = 0.0;
+      A1(zsnowaut, jl) = 0.0;
+      A1(zsnowrime, jl) = 0.0;
+      A1(zldefr, jl) = 0.0;
+      A1(zacust, jl) = 0.0;
+      A1(zqpretot, jl) = 0.0;
+      A1(zlfinalsum, jl) = 0.0;
+      A1(zsolab, jl) = 0.0;
+      A1(zsolac, jl) = 0.0;
+      A1(zicetot, jl) = 0.0;
+    }
+    memset(zsolqb, 0, sizeof(double) * n1 * NCLV * NCLV);
+    memset(zsolqa, 0, sizeof(double) * n1 * NCLV * NCLV);
+    memset(zfallspeed, 0, sizeof(double) * n1 * NCLV);
+    memset(zfallsrce, 0, sizeof(double) * n1 * NCLV);
+    memset(zfallsink, 0, sizeof(double) * n1 * NCLV);
+    memset(zconvsrce, 0, sizeof(double) * n1 * NCLV);
+    memset(zconvsink, 0, sizeof(double) * n1 * NCLV);
+
+    /* derived variables (:1275-1326) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double t = A2(ztp1, jl, jk);
+      A1(zdp, jl) = A2(paph, jl, jk + 1) - A2(paph, jl, jk);
+      A1(zgdp, jl) = p->rg / A1(zdp, jl);
+      A1(zrho, jl) = A2(pap, jl, jk) / (p->rd * t);
+      A1(zdtgdp, jl) = ptsphy * A1(zgdp, jl);
+      A1(zrdtgdp, jl) = A1(zdp, jl) * (1.0 / (ptsphy * p->rg));
+      if (jk > 1) A1(zdtgdpf, jl) = ptsphy * p->rg / (A2(pap, jl, jk) - A2(pap, jl, jk - 1));
+      double xl = t - p->r4les, xi = t - p->r4ies;
+      double zfacw = p->r5les / (xl * xl);
+      double zcor = 1.0 / (1.0 - p->retv * A2(zfoeeliqt, jl, jk));
+      A1(zdqsliqdt, jl) = zfacw * zcor * A2(zqsliq, jl, jk);
+      A1(zcorqsliq, jl) = 1.0 + p->ralvdcp * A1(zdqsliqdt, jl);
+      double zfaci = p->r5ies / (xi * xi);
+      zcor = 1.0 / (1.0 - p->retv * A2(zfoeew, jl, jk));
+      A1(zdqsicedt, jl) = zfaci * zcor * A2(zqsice, jl, jk);
+      A1(zcorqsice, jl) = 1.0 + p->ralsdcp * A1(zdqsicedt, jl);
+      double zalfaw = A2(zfoealfa, jl, jk);
+      double zfac = zalfaw * zfacw + (1.0 - zalfaw) * zfaci;
+      zcor = 1.0 / (1.0 - p->retv * A2(zfoeewm, jl, jk));
+      A1(zdqsmixdt, jl) = zfac * zcor * A2(zqsmix, jl, jk);
+      A1(zcorqsmix, jl) = 1.0 + foeldcpm(p, t) * A1(zdqsmixdt, jl);
+      double qv = A3(zqx, jl, jk, NCLDQV, klev);
+      A1(zevaplimmix, jl) = fmax_((A2(zqsmix, jl, jk) - qv) / A1(zcorqsmix, jl), 0.0);
+      A1(zevaplimliq, jl) = fmax_((A2(zqsliq, jl, jk) - qv) / A1(zcorqsliq, jl), 0.0);
+      A1(zevaplimice, jl) = fmax_((A2(zqsice, jl, jk) - qv) / A1(zcorqsice, jl), 0.0);
+      double ztmpa = 1.0 / fmax_(A2(za, jl, jk), 0.01);
+      A1(zliqcld, jl) = A3(zqx, jl, jk, NCLDQL, klev) * ztmpa;
+      A1(zicecld, jl) = A3(zqx, jl, jk, NCLDQI, klev) * ztmpa;
+      A1(zlicld, jl) = A1(zliqcld, jl) + A1(zicecld, jl);
+    }
+
+    /* evaporate very small amounts (:1332-1344) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A3(zqx, jl, jk, NCLDQL, klev) < p->rlmin) {
+        L3(zsolqa, jl, NCLDQV, NCLDQL) = A3(zqx, jl, jk, NCLDQL, klev);
+        L3(zsolqa, jl, NCLDQL, NCLDQV) = -A3(zqx, jl, jk, NCLDQL, klev);
+      }
+      if (A3(zqx, jl, jk, NCLDQI, klev) < p->rlmin) {
+        L3(zsolqa, jl, NCLDQV, NCLDQI) = A3(zqx, jl, jk, NCLDQI, klev);
+        L3(zsolqa, jl, NCLDQI, NCLDQV) = -A3(zqx, jl, jk, NCLDQI, klev);
+      }
+    }
+
+    /* 3.2 detrainment (:1362-1398) */
+    if (jk < klev && jk >= ncldtop) {
+      for (jl = kidia; jl <= kfdia; jl++) {
+        A2(plude, jl, jk) = A2(plude, jl, jk) * A1(zdtgdp, jl);
+        if (A1(ldcum, jl) && A2(plude, jl, jk) > zepsec && A2(plu, jl, jk + 1) > zepsec) {
+          A1(zsolac, jl) = A1(zsolac, jl) + A2(plude, jl, jk) / A2(plu, jl, jk + 1);
+          L2(zconvsrce, jl, NCLDQL) = A3(pludeli, jl, jk, 1, klev) * A1(zdtgdp, jl);
+          L2(zconvsrce, jl, NCLDQI) = A3(pludeli, jl, jk, 2, klev) * A1(zdtgdp, jl);
+          L3(zsolqa, jl, NCLDQL, NCLDQL) = L3(zsolqa, jl, NCLDQL, NCLDQL) + L2(zconvsrce, jl, NCLDQL);
+          L3(zsolqa, jl, NCLDQI, NCLDQI) = L3(zsolqa, jl, NCLDQI, NCLDQI) + L2(zconvsrce, jl, NCLDQI);
+        } else {
+          A2(plude, jl, jk) = 0.0;
+        }
+        if (p->lmfdsnow) {
+          L2(zconvsrce, jl, NCLDQR) = A3(psnde, jl, jk, 1, klev) * A1(zdtgdp, jl);
+          L2(zconvsrce, jl, NCLDQS) = A3(psnde, jl, jk, 2, klev) * A1(zdtgdp, jl);
+          L3(zsolqa, jl, NCLDQR, NCLDQR) = L3(zsolqa, jl, NCLDQR, NCLDQR) + L2(zconvsrce, jl, NCLDQR);
+          L3(zsolqa, jl, NCLDQS, NCLDQS) = L3(zsolqa, jl, NCLDQS, NCLDQS) + L2(zconvsrce, jl, NCLDQS);
+        }
+      }
+    }
+
+    /* 3.3 subsidence source and evaporation (:1419-1492) */
+    if (jk > ncldtop) {
+      for (jl = kidia; jl <= kfdia; jl++) {
+        A1(zmf, jl) = fmax_(0.0, (A2(pmfu, jl, jk) * A1(zadvw, jl) + A2(pmfd, jl, jk) * A1(zadvwd, jl)) *
+                                     A1(zdtgdp, jl));
+        A1(zacust, jl) = A1(zmf, jl) * A1(zanewm1, jl);
+      }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        L2(zlcust, jl, NCLDQL) = A1(zmf, jl) * L2(zqxnm1, jl, NCLDQL);
+        L2(zlcust, jl, NCLDQI) = A1(zmf, jl) * L2(zqxnm1, jl, NCLDQI);
+        L2(zconvsrce, jl, NCLDQL) = L2(zconvsrce, jl, NCLDQL) + L2(zlcust, jl, NCLDQL);
+        L2(zconvsrce, jl, NCLDQI) = L2(zconvsrce, jl, NCLDQI) + L2(zlcust, jl, NCLDQI);
+      }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        double zdtdp = zrdcp * 0.5 * (A2(ztp1, jl, jk - 1) + A2(ztp1, jl, jk)) / A2(paph, jl, jk);
+        double zwtot = fmin_(p->rg * (A2(pmfu, jl, jk) * A1(zadvw, jl) + A2(pmfd, jl, jk) * A1(zadvwd, jl)),
+                             (A2(pap, jl, jk) - A2(pap, jl, jk - 1)) / ptsphy);
+        double zdtforc = zdtdp * ptsphy * zwtot;
+        A1(zdqs, jl) = A1(zanewm1, jl) * zdtforc * A1(zdqsmixdt, jl);
+      }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        double zlfinal = fmax_(0.0, L2(zlcust, jl, NCLDQL) - A1(zdqs, jl));
+        double zevap = fmin_((L2(zlcust, jl, NCLDQL) - zlfinal), A1(zevaplimmix, jl));
+        zlfinal = L2(zlcust, jl, NCLDQL) - zevap;
+        A1(zlfinalsum, jl) = A1(zlfinalsum, jl) + zlfinal;
+        L3(zsolqa, jl, NCLDQL, NCLDQL) = L3(zsolqa, jl, NCLDQL, NCLDQL) + L2(zlcust, jl, NCLDQL);
+        L3(zsolqa, jl, NCLDQV, NCLDQL) = L3(zsolqa, jl, NCLDQV, NCLDQL) + zevap;
+        L3(zsolqa, jl, NCLDQL, NCLDQV) = L3(zsolqa, jl, NCLDQL, NCLDQV) - zevap;
+      }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        double zlfinal = fmax_(0.0, L2(zlcust, jl, NCLDQI) - A1(zdqs, jl));
+        double zevap = fmin_((L2(zlcust, jl, NCLDQI) - zlfinal), A1(zevaplimmix, jl));
+        zlfinal = L2(zlcust, jl, NCLDQI) - zevap;
+        A1(zlfinalsum, jl) = A1(zlfinalsum, jl) + zlfinal;
+        L3(zsolqa, jl, NCLDQI, NCLDQI) = L3(zsolqa, jl, NCLDQI, NCLDQI) + L2(zlcust, jl, NCLDQI);
+        L3(zsolqa, jl, NCLDQV, NCLDQI) = L3(zsolqa, jl, NCLDQV, NCLDQI) + zevap;
+        L3(zsolqa, jl, NCLDQI, NCLDQV) = L3(zsolqa, jl, NCLDQI, NCLDQV) - zevap;
+      }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        A1(zsolac, jl) = A1(zsolac, jl) + A1(zacust, jl);
+        if (A1(zlfinalsum, jl) < zepsec) A1(zsolac, jl) = A1(zsolac, jl) - A1(zacust, jl);
+      }
+    }
+
+    /* subsidence sink (:1499-1514) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (jk < klev) {
+        double zmfdn = fmax_(0.0, (A2(pmfu, jl, jk + 1) * A1(zadvw, jl) + A2(pmfd, jl, jk + 1) * A1(zadvwd, jl)) *
+                                      A1(zdtgdp, jl));
+        A1(zsolab, jl) = A1(zsolab, jl) + zmfdn;
+        L3(zsolqb, jl, NCLDQL, NCLDQL) = L3(zsolqb, jl, NCLDQL, NCLDQL) + zmfdn;
+        L3(zsolqb, jl, NCLDQI, NCLDQI) = L3(zsolqb, jl, NCLDQI, NCLDQI) + zmfdn;
+        L2(zconvsink, jl, NCLDQL) = zmfdn;
+        L2(zconvsink, jl, NCLDQI) = zmfdn;
+      }
+    }
+
+    /* 3.4 erosion, ITURBEROSION=3 (:1689-1754) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A1(zldifdt, jl) = p->rcldiff * ptsphy;
+      if (A1(ktype, jl) >= 2 && A2(plude, jl, jk) > zepsec && A1(peis, jl) < 10.0) {
+        A1(zldifdt, jl) = 20.0 * p->rcldiff_convi * A1(zldifdt, jl);
+      } else if (A1(ktype, jl) == 1 && A2(plude, jl, jk) > zepsec) {
+        A1(zldifdt, jl) = 2.0 * p->rcldiff_convi * A1(zldifdt, jl);
+      }
+    }
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A2(zli, jl, jk) > zepsec) {
+        double zaa = A2(za, jl, jk);
+        double zqe = (A3(zqx, jl, jk, NCLDQV, klev) - zaa * A2(zqsmix, jl, jk)) / fmax_(zepsec, 1.0 - zaa);
+        double ze = fmax_(A2(zqsmix, jl, jk) - zqe, 0.0);
+        double zleros = 0.333 * zaa * (1. - zaa) * A1(zldifdt, jl) * ze;
+        zleros = fmin_(zleros, A1(zevaplimmix, jl));
+        zleros = fmin_(zleros, A2(zli, jl, jk));
+        double zaeros = 0.5 * zleros / A1(zlicld, jl);
+        A1(zsolac, jl) = A1(zsolac, jl) - zaeros;
+        L3(zsolqa, jl, NCLDQV, NCLDQL) = L3(zsolqa, jl, NCLDQV, NCLDQL) + A2(zliqfrac, jl, jk) * zleros;
+        L3(zsolqa, jl, NCLDQL, NCLDQV) = L3(zsolqa, jl, NCLDQL, NCLDQV) - A2(zliqfrac, jl, jk) * zleros;
+        L3(zsolqa, jl, NCLDQV, NCLDQI) = L3(zsolqa, jl, NCLDQV, NCLDQI) + A2(zicefrac, jl, jk) * zleros;
+        L3(zsolqa, jl, NCLDQI, NCLDQV) = L3(zsolqa, jl, NCLDQI, NCLDQV) - A2(zicefrac, jl, jk) * zleros;
+      }
+    }
+
+    /* 4.1 fall speeds (:1783-1844), IVARFALL_ICE=0, IVARFALL_RAIN=1 */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      L2(zfallspeed, jl, NCLDQL) = zvqx[NCLDQL];
+      L2(zfallspeed, jl, NCLDQI) = zvqx[NCLDQI];
+      L2(zfallspeed, jl, NCLDQS) = zvqx[NCLDQS];
+      double zfallcorr = pow(p->rdensref / A1(zrho, jl), 0.4);
+      double ztemp = 0.5 * (A3(zqx, jl, jk, NCLDQR, klev) + L2(zqxnm1, jl, NCLDQR));
+      double zrlambda = pow(A1(zrho, jl) * ztemp / p->rcl_lam1r, p->rcl_lam2r);
+      L2(zfallspeed, jl, NCLDQR) =
+          p->rxfallspeedrain * zfallcorr * p->rcl_const7r * pow(zrlambda, p->rcl_dr);
+    }
+    /* sedimentation source/sink (:1852-1877) */
+    for (jm = 1; jm <= NCLV; jm++) {
+      if (!llfall[jm]) continue;
+      for (jl = kidia; jl <= kfdia; jl++) {
+        if (jk > ncldtop) {
+          L2(zfallsrce, jl, jm) = A3(zpfplsx, jl, jk, jm, klev + 1) * A1(zdtgdp, jl);
+          L3(zsolqa, jl, jm, jm) = L3(zsolqa, jl, jm, jm) + L2(zfallsrce, jl, jm);
+          L2(zqxfg, jl, jm) = L2(zqxfg, jl, jm) + L2(zfallsrce, jl, jm);
+          A1(zqpretot, jl) = A1(zqpretot, jl) + L2(zqxfg, jl, jm);
+        }
+        L2(zfallsink, jl, jm) = A1(zdtgdp, jl) * A1(zrho, jl) * L2(zfallspeed, jl, jm);
+      }
+    }
+
+    /* 4.2 precipitation fraction (:1898-1919) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A1(zqpretot, jl) > zepsec) {
+        A1(zcovptot, jl) = 1.0 - ((1.0 - A1(zcovptot, jl)) *
+                                  (1.0 - fmax_(A2(za, jl, jk), A2(za, jl, jk - 1))) /
+                                  (1.0 - fmin_(A2(za, jl, jk - 1), 1.0 - 1.E-06)));
+        A1(zcovptot, jl) = fmax_(A1(zcovptot, jl), p->rcovpmin);
+        A1(zcovpclr, jl) = fmax_(0.0, A1(zcovptot, jl) - A2(za, jl, jk));
+        A1(zraincld, jl) = 0.5 * (A3(zqx, jl, jk, NCLDQR, klev) + A3(zqx, jl, jk - 1, NCLDQR, klev)) / A1(zcovptot, jl);
+        A1(zraincldm1, jl) = 0.5 * (A3(zqx, jl, jk, NCLDQR, klev) + L2(zqxnm1, jl, NCLDQR)) / A1(zcovptot, jl);
+        A1(zsnowcld, jl) = 0.5 * (A3(zqx, jl, jk, NCLDQS, klev) + A3(zqx, jl, jk - 1, NCLDQS, klev)) / A1(zcovptot, jl);
+        A1(zsnowcldm1, jl) = 0.5 * (A3(zqx, jl, jk, NCLDQS, klev) + L2(zqxnm1, jl, NCLDQS)) / A1(zcovptot, jl);
+        A1(zcovpmax, jl) = fmax_(A1(zcovptot, jl), A1(zcovpmax, jl));
+      } else {
+        A1(zraincld, jl) = 0.0;
+        A1(zraincldm1, jl) = 0.0;
+        A1(zsnowcld, jl) = 0.0;
+        A1(zsnowcldm1, jl) = 0.0;
+        A1(zcovptot, jl) = 0.0;
+        A1(zcovpclr, jl) = 0.0;
+        A1(zcovpmax, jl) = 0.0;
+      }
+    }
+
+    /* 4.3 warm rain, IWARMRAIN=3, IRAINACC=1 (:1930-2259) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A1(zliqcld, jl) > zepsec) {
+        double zconst, zlcrit;
+        if (A1(plsm, jl) > 0.5) {
+          zconst = p->rcl_kk_cloud_num_land;
+          zlcrit = p->rclcrit_land;
+        } else {
+          zconst = p->rcl_kk_cloud_num_sea;
+          zlcrit = p->rclcrit_sea;
+        }
+        (void)zlcrit;
+        double zeaut = p->rcl_inhomogaut, zeacc = p->rcl_inhomogacc;
+        A1(zrainaut, jl) = zeaut * ptsphy * p->rcl_kkaau * pow(A1(zliqcld, jl), p->rcl_kkbauq - 1.0) *
+                           pow(zconst, p->rcl_kkbaun);
+        L3(zsolqb, jl, NCLDQR, NCLDQL) = L3(zsolqb, jl, NCLDQR, NCLDQL) + A1(zrainaut, jl);
+        if (A1(zraincld, jl) > zepsec) {
+          A1(zrainacc, jl) = zeacc * ptsphy * p->rcl_kkaac * pow(A1(zliqcld, jl), p->rcl_kkbac - 1.0) *
+                             pow(A1(zraincld, jl), p->rcl_kkbac);
+        }
+        L3(zsolqb, jl, NCLDQR, NCLDQL) = L3(zsolqb, jl, NCLDQR, NCLDQL) + A1(zrainacc, jl);
+      }
+    }
+
+    /* 4.4 rain evaporation (:2271-2378) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double zaa = A2(za, jl, jk);
+      double zzrh = p->rprecrhmax + (1.0 - p->rprecrhmax) * A1(zcovpmax, jl) / fmax_(zepsec, 1.0 - zaa);
+      zzrh = fmin_(fmax_(zzrh, p->rprecrhmax), 1.0);
+      double zxramid = p->ramid;
+      double zrhc = zxramid;
+      double zsigk = A2(pap, jl, jk) / A2(paph, jl, klev + 1);
+      if (zsigk > 0.8) {
+        double s = (zsigk - 0.8) / 0.2;
+        zrhc = zxramid + (1.0 - zxramid) * (s * s);
+      }
+      zzrh = fmin_(zrhc, zzrh);
+      zzrh = fmin_(0.9, zzrh);
+      double zqsl = A2(zqsliq, jl, jk);
+      double zqe = fmax_(0.0, fmin_(A3(zqx, jl, jk, NCLDQV, klev), zqsl));
+      int llo1 = A1(zcovpclr, jl) > zepsec && A1(zraincldm1, jl) > zepsec && zqe < zzrh * zqsl;
+      if (llo1) {
+        double t = A2(ztp1, jl, jk), rho = A1(zrho, jl);
+        double zpreclr = A1(zraincldm1, jl);
+        double zfallcorr = pow(p->rdensref / rho, flt_0p4);
+        double zesatliq = p->rv / p->rd * foeeliq(p, t);
+        double zlambda = pow(p->rcl_lam1r / (rho * zpreclr), p->rcl_lam2r);
+        double zevap_denom = p->rcl_cdenom1 * zesatliq - p->rcl_cdenom2 * t * zesatliq +
+                             p->rcl_cdenom3 * pow(t, 3.0) * A2(pap, jl, jk);
+        double zcorr2 = pow(t / 273., 1.5) * 393. / (t + 120.);
+        double zsubsat = fmax_(zzrh * zqsl - zqe, 0.0);
+        double zbeta = (0.15 / zqsl) * (t * t) * zesatliq * p->rcl_const1r * (zcorr2 / zevap_denom) *
+                       (0.78 / (pow(zlambda, p->rcl_const4r)) +
+                        p->rcl_const2r * pow(rho * zfallcorr, 0.5) /
+                            (pow(zcorr2, 0.5) * pow(zlambda, p->rcl_const3r)));
+        double zdenom = 1.0 + zbeta * ptsphy * A1(zcorqsliq, jl);
+        double zdpevap = A1(zcovpclr, jl) * zbeta * ptsphy * zsubsat / zdenom;
+        double zevap = fmin_(zdpevap, L2(zqxfg, jl, NCLDQR));
+        L3(zsolqa, jl, NCLDQV, NCLDQR) = L3(zsolqa, jl, NCLDQV, NCLDQR) + zevap;
+        L3(zsolqa, jl, NCLDQR, NCLDQV) = L3(zsolqa, jl, NCLDQR, NCLDQV) - zevap;
+        L2(zqxfg, jl, NCLDQR) = L2(zqxfg, jl, NCLDQR) - zevap;
+      }
+    }
+
+    /* 4.5 ice deposition, IDEPICE=1 (:2404-2499) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double zaa = A2(za, jl, jk), rho = A1(zrho, jl), t = A2(ztp1, jl, jk);
+      if (A2(za, jl, jk - 1) < p->rcldtopcf && zaa >= p->rcldtopcf) {
+        A1(zcldtopdist, jl) = 0.0;
+      } else {
+        A1(zcldtopdist, jl) = A1(zcldtopdist, jl) + A1(zdp, jl) / (rho * p->rg);
+      }
+      double zoverlap_liqice = p->rcl_overlapliqice;
+      double zsupersatice = (A2(zqsliq, jl, jk) - A2(zqsice, jl, jk)) / A2(zqsice, jl, jk);
+      if (t < (p->rtt - 5.) && L2(zqxfg, jl, NCLDQL) > p->rlmin) {
+        double zvpice = foeeice(p, t) * p->rv / p->rd;
+        double zvpliq = zvpice * fokoop(p, t);
+        (void)zvpliq;
+        A1(zicenuclei, jl) = 1000.0 * exp(12.96 * zsupersatice - 0.639);
+        double zadd = p->rlstt * (p->rlstt / (p->rv * t) - 1.0) / (2.4E-2 * t);
+        double zbdd = p->rv * t * A2(pap, jl, jk) / (2.21 * zvpice);
+        double zcvds = 7.8 * pow(A1(zicenuclei, jl) / rho, 0.666) * zsupersatice / (8.87 * (zadd + zbdd));
+        double zice0 = fmax_(A1(zicecld, jl), A1(zicenuclei, jl) * p->riceinit / rho);
+        double zinew = pow(0.666 * zcvds * ptsphy + pow(zice0, 0.666), 1.5);
+        double zdepos = fmax_(zoverlap_liqice * zaa * (zinew - zice0), 0.0);
+        zdepos = fmin_(zdepos, L2(zqxfg, jl, NCLDQL));
+        double zinfactor = fmin_(A1(zicenuclei, jl) / 15000., 1.0);
+        zdepos = zdepos * fmin_(zinfactor + (1.0 - zinfactor) *
+                                                (p->rdepliqrefrate + A1(zcldtopdist, jl) / p->rdepliqrefdepth),
+                                1.0);
+        L3(zsolqa, jl, NCLDQI, NCLDQL) = L3(zsolqa, jl, NCLDQI, NCLDQL) + zdepos;
+        L3(zsolqa, jl, NCLDQL, NCLDQI) = L3(zsolqa, jl, NCLDQL, NCLDQI) - zdepos;
+        L2(zqxfg, jl, NCLDQI) = L2(zqxfg, jl, NCLDQI) + zdepos;
+        L2(zqxfg, jl, NCLDQL) = L2(zqxfg, jl, NCLDQL) - zdepos;
+      }
+    }
+
+    /* 4.6 ISUBLICE=0: no ice sublimation (:2613-2689) */
+
+    /* 4.7 snow deposition, IDEPSNOW=1 (:2698-2745) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A1(zpsdep, jl) = 0.0;
+      double t = A2(ztp1, jl, jk), rho = A1(zrho, jl);
+      double zqsm = A2(zqsmix, jl, jk), qv = A3(zqx, jl, jk, NCLDQV, klev);
+      double zsupersatice = fmax_((qv - zqsm) / zqsm, 0.0);
+      if (t < p->rtt && A1(zsnowcld, jl) > zepsec && zsupersatice > 0.0) {
+        double zvpice = foeeice(p, t) * p->rv / p->rd;
+        double ztcg = 1.0, zfacx1s = 1.0;
+        double zaplusb = p->rcl_apb1 * zvpice - p->rcl_apb2 * zvpice * t + A2(pap, jl, jk) * p->rcl_apb3 * (t * t * t);
+        double zcorrfac = pow(1.0 / rho, 0.5);
+        double zcorrfac2 = (pow(t / 273.0, 1.5)) * (393.0 / (t + 120.0));
+        double zpr02 = rho * A1(zsnowcld, jl) * p->rcl_const1s / (ztcg * zfacx1s);
+        double zterm1 = zsupersatice * (t * t) * zvpice * zcorrfac2 * ztcg * p->rcl_const2s * zfacx1s / (rho * zaplusb);
+        double zterm2 = 0.65 * p->rcl_const6s * pow(zpr02, p->rcl_const4s) +
+                        p->rcl_const3s * pow(zcorrfac, 0.5) * pow(rho, 0.5) * pow(zpr02, p->rcl_const5s) /
+                            pow(zcorrfac2, 0.5);
+        A1(zpsdep, jl) = fmax_(A1(zcovptot, jl) * zterm1 * zterm2 * ptsphy, 0.0);
+        A1(zpsdep, jl) = fmin_(A1(zpsdep, jl), qv - zqsm) / A1(zcorqsmix, jl);
+        L3(zsolqa, jl, NCLDQS, NCLDQV) = L3(zsolqa, jl, NCLDQS, NCLDQV) + A1(zpsdep, jl);
+        L3(zsolqa, jl, NCLDQV, NCLDQS) = L3(zsolqa, jl, NCLDQV, NCLDQS) - A1(zpsdep, jl);
+      }
+    }
+
+    /* revise in-cloud condensate (:2750-2754) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double ztmpa = 1.0 / fmax_(A2(za, jl, jk), 0.01);
+      A1(zliqcld, jl) = L2(zqxfg, jl, NCLDQL) * ztmpa;
+      A1(zicecld, jl) = L2(zqxfg, jl, NCLDQI) * ztmpa;
+    }
+
+    /* 4.8 ice -> snow autoconversion (:2769-2800) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double t = A2(ztp1, jl, jk);
+      if (t <= p->rtt) {
+        if (A1(zicecld, jl) > zepsec) {
+          double zzco = ptsphy * p->rsnowlin1 * exp(p->rsnowlin2 * (t - p->rtt));
+          double zlcrit = p->rlcritsnow;
+          double r = A1(zicecld, jl) / zlcrit;
+          double ztemp = -1. * (r * r);
+          if (ztemp < 50.0) {
+            A1(zsnowaut, jl) = zzco * (1.0 - exp(ztemp));
+          } else {
+            A1(zsnowaut, jl) = zzco;
+          }
+          L3(zsolqb, jl, NCLDQS, NCLDQI) = L3(zsolqb, jl, NCLDQS, NCLDQI) + A1(zsnowaut, jl);
+        }
+      }
+    }
+
+    /* 4.12 melting (:2815-2862) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double t = A2(ztp1, jl, jk);
+      A1(zicetot, jl) = L2(zqxfg, jl, NCLDQI) + L2(zqxfg, jl, NCLDQS);
+      A1(zmeltmax, jl) = 0.0;
+      if (A1(zicetot, jl) > zepsec && t > p->rtt) {
+        double zsubsat = fmax_(A2(zqsice, jl, jk) - A3(zqx, jl, jk, NCLDQV, klev), 0.0);
+        double ztdmtw0 = t - p->rtt - zsubsat * (ztw1 + ztw2 * (A2(pap, jl, jk) - ztw3) - ztw4 * (t - ztw5));
+        double zcons1 = fabs(ptsphy * (1.0 + 0.5 * ztdmtw0) / p->rtaumel);
+        A1(zmeltmax, jl) = fmax_(ztdmtw0 * zcons1 * zrldcp, 0.0);
+      }
+    }
+    for (jm = 1; jm <= NCLV; jm++) {
+      if (iphase[jm] != 2) continue;
+      jn = imelt[jm];
+      for (jl = kidia; jl <= kfdia; jl++) {
+        if (A1(zmeltmax, jl) > zepsec && A1(zicetot, jl) > zepsec) {
+          double zalfa = L2(zqxfg, jl, jm) / A1(zicetot, jl);
+          double zmelt = fmin_(L2(zqxfg, jl, jm), zalfa * A1(zmeltmax, jl));
+          L2(zqxfg, jl, jm) = L2(zqxfg, jl, jm) - zmelt;
+          L2(zqxfg, jl, jn) = L2(zqxfg, jl, jn) + zmelt;
+          L3(zsolqa, jl, jn, jm) = L3(zsolqa, jl, jn, jm) + zmelt;
+          L3(zsolqa, jl, jm, jn) = L3(zsolqa, jl, jm, jn) - zmelt;
+        }
+      }
+    }
+
+    /* 4.13 rain freezing (:2877-2933) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double t = A2(ztp1, jl, jk), qr = A3(zqx, jl, jk, NCLDQR, klev);
+      if (qr > zepsec) {
+        if (t <= p->rtt && A2(ztp1, jl, jk - 1) > p->rtt) {
+          A1(zqpretot, jl) = fmax_(A3(zqx, jl, jk, NCLDQS, klev) + qr, zepsec);
+          A1(prainfrac_toprfz, jl) = qr / A1(zqpretot, jl);
+          A1(llrainliq, jl) = A1(prainfrac_toprfz, jl) > flt_0p8;
+        }
+        if (t < p->rtt) {
+          if (A1(llrainliq, jl)) {
+            double zlambda = pow(p->rcl_lam1r / (A1(zrho, jl) * qr), p->rcl_lam2r);
+            double ztemp = fmin_(p->rcl_fzrab * (t - p->rtt), 50.);
+            double zfrz = ptsphy * (p->rcl_const5r / A1(zrho, jl)) * (exp(ztemp) - 1.) * pow(zlambda, p->rcl_const6r);
+            A1(zfrzmax, jl) = fmax_(zfrz, 0.0);
+          } else {
+            double zcons1 = fabs(ptsphy * (1.0 + 0.5 * (p->rtt - t)) / p->rtaumel);
+            A1(zfrzmax, jl) = fmax_((p->rtt - t) * zcons1 * zrldcp, 0.0);
+          }
+          if (A1(zfrzmax, jl) > zepsec) {
+            double zfrz = fmin_(qr, A1(zfrzmax, jl));
+            L3(zsolqa, jl, NCLDQS, NCLDQR) = L3(zsolqa, jl, NCLDQS, NCLDQR) + zfrz;
+            L3(zsolqa, jl, NCLDQR, NCLDQS) = L3(zsolqa, jl, NCLDQR, NCLDQS) - zfrz;
+          }
+        }
+      }
+    }
+
+    /* 4.14 homogeneous freezing of cloud liquid (:2948-2960) */
+    for (jl = kidia; jl <= kfdia; jl++)
+      A1(zfrzmax, jl) = fmax_((p->rthomo - A2(ztp1, jl, jk)) * zrldcp, 0.0);
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A1(zfrzmax, jl) > zepsec && L2(zqxfg, jl, NCLDQL) > zepsec) {
+        double zfrz = fmin_(L2(zqxfg, jl, NCLDQL), A1(zfrzmax, jl));
+        L3(zsolqa, jl, NCLDQI, NCLDQL) = L3(zsolqa, jl, NCLDQI, NCLDQL) + zfrz;
+        L3(zsolqa, jl, NCLDQL, NCLDQI) = L3(zsolqa, jl, NCLDQL, NCLDQI) - zfrz;
+      }
+    }
+
+    /* 4.9 riming (:2973-3017) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      if (A2(ztp1, jl, jk) <= p->rtt && A1(zliqcld, jl) > zepsec) {
+        double rho = A1(zrho, jl);
+        double zfallcorr = pow(p->rdensref / rho, flt_0p4);
+        if (A1(zsnowcld, jl) > zepsec && A1(zcovptot, jl) > 0.01) {
+          A1(zsnowrime, jl) = p->rcl_effrime * A1(zcovptot, jl) * ptsphy * p->rcl_const7s * zfallcorr *
+                              pow(rho * A1(zsnowcld, jl) * p->rcl_const1s, p->rcl_const8s);
+          A1(zsnowrime, jl) = fmin_(A1(zsnowrime, jl), 1.0);
+          L3(zsolqb, jl, NCLDQS, NCLDQL) = L3(zsolqb, jl, NCLDQS, NCLDQL) + A1(zsnowrime, jl);
+        }
+      }
+    }
+
+    /* PSD slopes (:3026-3069) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double rho = A1(zrho, jl);
+      if (A1(zraincld, jl) > zepsec) {
+        A1(zlamr, jl) = pow(p->rcl_lam1r / (rho * A1(zraincld, jl)), p->rcl_lam2r);
+        A1(zn0r, jl) = p->rcl_x1r * pow(A1(zlamr, jl), p->rcl_x2r);
+      } else {
+        A1(zlamr, jl) = 0.0;
+        A1(zn0r, jl) = 0.0;
+      }
+      if (A1(zsnowcld, jl) > zepsec) {
+        A1(zlams, jl) = pow(p->rcl_lam1s / (rho * A1(zsnowcld, jl)), p->rcl_lam2s);
+        A1(zn0s, jl) = p->rcl_x1s;
+      } else {
+        A1(zlams, jl) = 0.0;
+        A1(zn0s, jl) = 0.0;
+      }
+      if (A1(zicecld, jl) > zepsec) {
+        A1(zlami, jl) = pow(p->rcl_lam1s / (rho * A1(zicecld, jl)), p->rcl_lam2s);
+        A1(zn0i, jl) = p->rcl_x1s;
+      } else {
+        A1(zlami, jl) = 0.0;
+        A1(zn0i, jl) = 0.0;
+      }
+    }
+
+    /* PSACR: snow accretes rain (:3084-3115) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A1(zpsacr, jl) = 0.0;
+      if (A2(ztp1, jl, jk) <= p->rtt && A1(prainfrac_toprfz, jl) < zepsec && A1(zraincld, jl) > zepsec &&
+          A1(zsnowcld, jl) > zepsec) {
+        double fr = L2(zfallspeed, jl, NCLDQR), fs = L2(zfallspeed, jl, NCLDQS);
+        double zfalldiff = fmax_(fabs(fr - fs), (fr + fs) / 8.);
+        double lr = A1(zlamr, jl), ls = A1(zlams, jl);
+        double zfac = p->rpi * p->rpi * p->rdenswat * 1.0 * A1(zrho, jl) * A1(zn0r, jl) * A1(zn0s, jl) /
+                      (ls * (lr * lr * lr));
+        double zrat = lr / ls;
+        A1(zpsacr, jl) = A1(zcovptot, jl) * ptsphy * zfac * zfalldiff * ((0.5 * zrat + 2.) * zrat + 5.) /
+                         (lr * lr * lr);
+        L3(zsolqa, jl, NCLDQS, NCLDQR) = L3(zsolqa, jl, NCLDQS, NCLDQR) + A1(zpsacr, jl);
+        L3(zsolqa, jl, NCLDQR, NCLDQS) = L3(zsolqa, jl, NCLDQR, NCLDQS) - A1(zpsacr, jl);
+      }
+    }
+    /* PRACS off (IP_RAIN_ACCRETES_SNOW=0) */
+    /* PIACR: ice accretes rain (:3171-3198) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A1(zpiacr, jl) = 0.0;
+      if (A2(ztp1, jl, jk) <= p->rtt && A1(prainfrac_toprfz, jl) < zepsec && A1(zraincld, jl) > zepsec &&
+          A1(zicecld, jl) > zepsec) {
+        double fr = L2(zfallspeed, jl, NCLDQR), fi = L2(zfallspeed, jl, NCLDQI);
+        double zfalldiff = fmax_(fabs(fr - fi), (fr + fi) / 8.);
+        double lr = A1(zlamr, jl), li = A1(zlami, jl);
+        double zfac = p->rpi * p->rpi * p->rdenswat * 0.1 * A1(zrho, jl) * A1(zn0r, jl) * A1(zn0i, jl) /
+                      (li * (lr * lr * lr));
+        double zrat = lr / li;
+        A1(zpiacr, jl) = A1(zcovptot, jl) * ptsphy * zfac * zfalldiff * ((0.5 * zrat + 2.) * zrat + 5.) /
+                         (lr * lr * lr);
+        L3(zsolqa, jl, NCLDQI, NCLDQR) = L3(zsolqa, jl, NCLDQI, NCLDQR) + A1(zpiacr, jl);
+        L3(zsolqa, jl, NCLDQR, NCLDQI) = L3(zsolqa, jl, NCLDQR, NCLDQI) - A1(zpiacr, jl);
+      }
+    }
+    /* PRACI off (IP_RAIN_ACCRETES_ICE=0) */
+
+    /* 4.15 snow sublimation, ISUBLSNOW=1 (:3254-3318) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double zaa = A2(za, jl, jk), zqsi = A2(zqsice, jl, jk);
+      double zzrh = p->rprecrhmax + (1.0 - p->rprecrhmax) * A1(zcovpmax, jl) / fmax_(zepsec, 1.0 - zaa);
+      zzrh = fmin_(fmax_(zzrh, p->rprecrhmax), 1.0);
+      double zqe = (A3(zqx, jl, jk, NCLDQV, klev) - zaa * zqsi) / fmax_(zepsec, 1.0 - zaa);
+      zqe = fmax_(0.0, fmin_(zqe, zqsi));
+      int llo1 = A1(zcovpclr, jl) > zepsec && L2(zqxfg, jl, NCLDQS) > zepsec && zqe < zzrh * zqsi;
+      if (llo1) {
+        double a = A1(zcovptot, jl) * A1(zdtgdp, jl);
+        double zpreclr = L2(zqxfg, jl, NCLDQS) * A1(zcovpclr, jl) / copysign(fmax_(fabs(a), zepsilon), a);
+        double zbeta1 = sqrt(A2(pap, jl, jk) / A2(paph, jl, klev + 1)) / p->rvrfactor * zpreclr /
+                        fmax_(A1(zcovpclr, jl), zepsec);
+        double zbeta = p->rg * p->rpecons * pow(zbeta1, 0.5777);
+        double zdenom = 1.0 + zbeta * ptsphy * A1(zcorqsice, jl);
+        double zdpr = A1(zcovpclr, jl) * zbeta * (zqsi - zqe) / zdenom * A1(zdp, jl) * zrg_r;
+        double zdpevap = zdpr * A1(zdtgdp, jl);
+        double zevap = fmin_(zdpevap, L2(zqxfg, jl, NCLDQS));
+        L3(zsolqa, jl, NCLDQV, NCLDQS) = L3(zsolqa, jl, NCLDQV, NCLDQS) + zevap;
+        L3(zsolqa, jl, NCLDQS, NCLDQV) = L3(zsolqa, jl, NCLDQS, NCLDQV) - zevap;
+        A1(zcovptot, jl) = fmax_(p->rcovpmin, A1(zcovptot, jl) - fmax_(0.0, (A1(zcovptot, jl) - zaa) * zevap /
+                                                                                L2(zqxfg, jl, NCLDQS)));
+        L2(zqxfg, jl, NCLDQS) = L2(zqxfg, jl, NCLDQS) - zevap;
+      }
+    }
+
+    /* evaporate small precipitation amounts (:3402-3412) */
+    for (jm = 1; jm <= NCLV; jm++) {
+      if (!llfall[jm]) continue;
+      for (jl = kidia; jl <= kfdia; jl++) {
+        if (L2(zqxfg, jl, jm) < p->rlmin) {
+          L3(zsolqa, jl, NCLDQV, jm) = L3(zsolqa, jl, NCLDQV, jm) + L2(zqxfg, jl, jm);
+          L3(zsolqa, jl, jm, NCLDQV) = L3(zsolqa, jl, jm, NCLDQV) - L2(zqxfg, jl, jm);
+        }
+      }
+    }
+
+    /* 5.1 cloud cover (:3429-3438) */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double zanew = (A2(za, jl, jk) + A1(zsolac, jl)) / (1.0 + A1(zsolab, jl));
+      zanew = fmin_(zanew, 1.0);
+      if (zanew < p->ramin) zanew = 0.0;
+      A1(zda, jl) = zanew - A2(zaorig, jl, jk);
+      A1(zanewm1, jl) = zanew;
+    }
+
+    /* 5.2.1 sink truncation (:3455-3536) */
+    for (jm = 1; jm <= NCLV; jm++) {
+      for (jl = kidia; jl <= kfdia; jl++) A1(zsinksum, jl) = 0.0;
+      for (jn = 1; jn <= NCLV; jn++)
+        for (jl = kidia; jl <= kfdia; jl++) A1(zsinksum, jl) = A1(zsinksum, jl) - L3(zsolqa, jl, jm, jn);
+      for (jl = kidia; jl <= kfdia; jl++) {
+        double zmax = fmax_(A3(zqx, jl, jk, jm, klev), zepsec);
+        double zrat = fmax_(A1(zsinksum, jl), zmax);
+        L2(zratio, jl, jm) = zmax / zrat;
+      }
+    }
+    for (jl = kidia; jl <= kfdia; jl++) {
+      int iordv[NCLV + 1];
+      iordv[1] = 1;
+      for (jm = 2; jm <= NCLV; jm++) {
+        for (jn = jm - 1; jn >= 1; jn--) {
+          if (L2(zratio, jl, iordv[jn]) <= L2(zratio, jl, jm)) break;
+          iordv[jn + 1] = iordv[jn];
+        }
+        iordv[jn + 1] = jm;
+      }
+      for (jm = 1; jm <= NCLV; jm++) L2(iorder, jl, jm) = iordv[jm];
+    }
+    for (jm = 1; jm <= NCLV; jm++) {
+      for (jl = kidia; jl <= kfdia; jl++) A1(zsinksum, jl) = 0.0;
+      for (jn = 1; jn <= NCLV; jn++)
+        for (jl = kidia; jl <= kfdia; jl++) {
+          jo = L2(iorder, jl, jm);
+          L2(llindex3, jl, jn) = L3(zsolqa, jl, jo, jn) < 0.0;
+          A1(zsinksum, jl) = A1(zsinksum, jl) - L3(zsolqa, jl, jo, jn);
+        }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        jo = L2(iorder, jl, jm);
+        double zmm = fmax_(A3(zqx, jl, jk, jo, klev), zepsec);
+        double zrr = fmax_(A1(zsinksum, jl), zmm);
+        L2(zratio, jl, 1) = zmm / zrr;
+      }
+      for (jl = kidia; jl <= kfdia; jl++) {
+        jo = L2(iorder, jl, jm);
+        double zzratio = L2(zratio, jl, 1);
+        for (jn = 1; jn <= NCLV; jn++) {
+          if (L2(llindex3, jl, jn)) {
+            L3(zsolqa, jl, jo, jn) = L3(zsolqa, jl, jo, jn) * zzratio;
+            L3(zsolqa, jl, jn, jo) = L3(zsolqa, jl, jn, jo) * zzratio;
+          }
+        }
+      }
+    }
+
+    /* 5.2.2 LHS / RHS (:3546-3587) */
+    for (jm = 1; jm <= NCLV; jm++)
+      for (jn = 1; jn <= NCLV; jn++) {
+        if (jn == jm) {
+          for (jl = kidia; jl <= kfdia; jl++) L3(zqlhs, jl, jn, jm) = 1.0 + L2(zfallsink, jl, jm);
+          for (jl = kidia; jl <= kfdia; jl++)
+            for (jo = 1; jo <= NCLV; jo++) L3(zqlhs, jl, jn, jm) = L3(zqlhs, jl, jn, jm) + L3(zsolqb, jl, jo, jn);
+        } else {
+          for (jl = kidia; jl <= kfdia; jl++) L3(zqlhs, jl, jn, jm) = -L3(zsolqb, jl, jn, jm);
+        }
+      }
+    for (jm = 1; jm <= NCLV; jm++)
+      for (jl = kidia; jl <= kfdia; jl++) {
+        double zexplicit = 0.0;
+        for (jn = 1; jn <= NCLV; jn++) zexplicit = zexplicit + L3(zsolqa, jl, jm, jn);
+        L2(zqxn, jl, jm) = A3(zqx, jl, jk, jm, klev) + zexplicit;
+      }
+
+    /* non-pivoting LU and substitution (:3600-3628) */
+    for (jn = 1; jn <= NCLV - 1; jn++)
+      for (jm = jn + 1; jm <= NCLV; jm++) {
+        for (jl = kidia; jl <= kfdia; jl++) L3(zqlhs, jl, jm, jn) = L3(zqlhs, jl, jm, jn) / L3(zqlhs, jl, jn, jn);
+        for (ik = jn + 1; ik <= NCLV; ik++)
+          for (jl = kidia; jl <= kfdia; jl++)
+            L3(zqlhs, jl, jm, ik) = L3(zqlhs, jl, jm, ik) - L3(zqlhs, jl, jm, jn) * L3(zqlhs, jl, jn, ik);
+      }
+    for (jn = 2; jn <= NCLV; jn++)
+      for (jm = 1; jm <= jn - 1; jm++)
+        for (jl = kidia; jl <= kfdia; jl++)
+          L2(zqxn, jl, jn) = L2(zqxn, jl, jn) - L3(zqlhs, jl, jn, jm) * L2(zqxn, jl, jm);
+    for (jl = kidia; jl <= kfdia; jl++) L2(zqxn, jl, NCLV) = L2(zqxn, jl, NCLV) / L3(zqlhs, jl, NCLV, NCLV);
+    for (jn = NCLV - 1; jn >= 1; jn--) {
+      for (jm = jn + 1; jm <= NCLV; jm++)
+        for (jl = kidia; jl <= kfdia; jl++)
+          L2(zqxn, jl, jn) = L2(zqxn, jl, jn) - L3(zqlhs, jl, jn, jm) * L2(zqxn, jl, jm);
+      for (jl = kidia; jl <= kfdia; jl++) L2(zqxn, jl, jn) = L2(zqxn, jl, jn) / L3(zqlhs, jl, jn, jn);
+    }
+
+    /* clip small values (:3633-3640) */
+    for (jn = 1; jn <= NCLV - 1; jn++)
+      for (jl = kidia; jl <= kfdia; jl++)
+        if (L2(zqxn, jl, jn) < zepsec) {
+          L2(zqxn, jl, NCLDQV) = L2(zqxn, jl, NCLDQV) + L2(zqxn, jl, jn);
+          L2(zqxn, jl, jn) = 0.0;
+        }
+    for (jm = 1; jm <= NCLV; jm++)
+      for (jl = kidia; jl <= kfdia; jl++) {
+        L2(zqxnm1, jl, jm) = L2(zqxn, jl, jm);
+        A3(zqxn2d, jl, jk, jm, klev) = L2(zqxn, jl, jm);
+      }
+
+    /* 5.3 fluxes to next level (:3658-3672) */
+    for (jm = 1; jm <= NCLV; jm++)
+      for (jl = kidia; jl <= kfdia; jl++)
+        A3(zpfplsx, jl, jk + 1, jm, klev + 1) = L2(zfallsink, jl, jm) * L2(zqxn, jl, jm) * A1(zrdtgdp, jl);
+    for (jl = kidia; jl <= kfdia; jl++)
+      A1(zqpretot, jl) = A3(zpfplsx, jl, jk + 1, NCLDQS, klev + 1) + A3(zpfplsx, jl, jk + 1, NCLDQR, klev + 1);
+    for (jl = kidia; jl <= kfdia; jl++)
+      if (A1(zqpretot, jl) < zepsec) A1(zcovptot, jl) = 0.0;
+
+    /* 6.1 T and condensate tendencies (:3713-3745) */
+    for (jm = 1; jm <= NCLV - 1; jm++) {
+      for (jl = kidia; jl <= kfdia; jl++)
+        L2(zfluxq, jl, jm) = L2(zconvsrce, jl, jm) + L2(zfallsrce, jl, jm) -
+                             (L2(zfallsink, jl, jm) + L2(zconvsink, jl, jm)) * L2(zqxn, jl, jm);
+      if (iphase[jm] == 1)
+        for (jl = kidia; jl <= kfdia; jl++)
+          A2(ptendency_loc_t, jl, jk) =
+              A2(ptendency_loc_t, jl, jk) +
+              p->ralvdcp * (L2(zqxn, jl, jm) - A3(zqx, jl, jk, jm, klev) - L2(zfluxq, jl, jm)) * zqtmst;
+      if (iphase[jm] == 2)
+        for (jl = kidia; jl <= kfdia; jl++)
+          A2(ptendency_loc_t, jl, jk) =
+              A2(ptendency_loc_t, jl, jk) +
+              p->ralsdcp * (L2(zqxn, jl, jm) - A3(zqx, jl, jk, jm, klev) - L2(zfluxq, jl, jm)) * zqtmst;
+      for (jl = kidia; jl <= kfdia; jl++)
+        A3(ptendency_loc_cld, jl, jk, jm, klev) =
+            A3(ptendency_loc_cld, jl, jk, jm, klev) + (L2(zqxn, jl, jm) - A3(zqx0, jl, jk, jm, klev)) * zqtmst;
+    }
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(ptendency_loc_q, jl, jk) =
+          A2(ptendency_loc_q, jl, jk) + (L2(zqxn, jl, NCLDQV) - A3(zqx, jl, jk, NCLDQV, klev)) * zqtmst;
+      A2(ptendency_loc_a, jl, jk) = A2(ptendency_loc_a, jl, jk) + A1(zda, jl) * zqtmst;
+      A1(zq_upd, jl) = A2(pq, jl, jk) + ptsphy * (A2(ptendency_loc_q, jl, jk) + A2(ptendency_cml_q, jl, jk));
+      A1(zt_upd, jl) = A2(pt, jl, jk) + ptsphy * (A2(ptendency_loc_t, jl, jk) + A2(ptendency_cml_t, jl, jk));
+      A1(za_upd, jl) = A2(pa, jl, jk) + ptsphy * (A2(ptendency_loc_a, jl, jk) + A2(ptendency_cml_a, jl, jk));
+    }
+
+    /* 6.4 supersaturation check (:3772-3809) */
+    {
+      double zpp[klon];
+      for (jl = kidia; jl <= kfdia; jl++) zpp[jl - 1] = A2(pap, jl, jk);
+      supersatcheck(p, kidia, kfdia, zt_upd, zq_upd, za_upd, zpp, zt_adj, zq_adj, za_adj, zl_adj, zi_adj);
+    }
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + A1(zq_adj, jl) * zqtmst;
+      A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) + A1(zt_adj, jl) * zqtmst;
+      A2(ptendency_loc_a, jl, jk) = A2(ptendency_loc_a, jl, jk) + A1(za_adj, jl) * zqtmst;
+      A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) = A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) + A1(zl_adj, jl) * zqtmst;
+      A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) = A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) + A1(zi_adj, jl) * zqtmst;
+      A1(zl_adj, jl) = A3(zqx0, jl, jk, NCLDQL, klev) + A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) * ptsphy;
+      if (A1(zl_adj, jl) < -p->rlmin) nwarn++;
+      if (A1(zl_adj, jl) < 0.0) {
+        A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) = A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) - A1(zl_adj, jl) * zqtmst;
+        A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + A1(zl_adj, jl) * zqtmst;
+        A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) - p->ralvdcp * A1(zl_adj, jl) * zqtmst;
+      }
+      A1(zi_adj, jl) = A3(zqx0, jl, jk, NCLDQI, klev) + A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) * ptsphy;
+      if (A1(zi_adj, jl) < -p->rlmin) nwarn++;
+      if (A1(zi_adj, jl) < 0.0) {
+        A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) = A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) - A1(zi_adj, jl) * zqtmst;
+        A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + A1(zi_adj, jl) * zqtmst;
+        A2(ptendency_loc_t, jl, jk) = A2(ptendency_loc_t, jl, jk) - p->ralsdcp * A1(zi_adj, jl) * zqtmst;
+      }
+    }
+    for (jl = kidia; jl <= kfdia; jl++) A2(pcovptot, jl, jk) = A1(zcovptot, jl);
+    /* ZANEWP (:3819-3823) and the budget section 7 (:3832-4126) feed only the
+       FSD/PEXTRA diagnostics, which are off in this configuration */
+  }
+  /* PCOVPTOT above the cloud top: left undefined by the reference, zero here */
+  for (jk = 1; jk < ncldtop; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) A2(pcovptot, jl, jk) = 0.0;
+
+  /* 8. fluxes (:4218-4303) */
+  for (jk = 1; jk <= klev + 1; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(pfplsl, jl, jk) = A3(zpfplsx, jl, jk, NCLDQR, klev + 1) + A3(zpfplsx, jl, jk, NCLDQL, klev + 1);
+      A2(pfplsn, jl, jk) = A3(zpfplsx, jl, jk, NCLDQS, klev + 1) + A3(zpfplsx, jl, jk, NCLDQI, klev + 1);
+    }
+  for (jl = kidia; jl <= kfdia; jl++) {
+    A2(pfsqlf, jl, 1) = 0.0;
+    A2(pfsqif, jl, 1) = 0.0;
+    A2(pfsqrf, jl, 1) = 0.0;
+    A2(pfsqsf, jl, 1) = 0.0;
+    A2(pfcqlng, jl, 1) = 0.0;
+    A2(pfcqnng, jl, 1) = 0.0;
+    A2(pfcqrng, jl, 1) = 0.0;
+    A2(pfcqsng, jl, 1) = 0.0;
+    A2(pfsqltur, jl, 1) = 0.0;
+    A2(pfsqitur, jl, 1) = 0.0;
+  }
+  for (jk = 1; jk <= klev; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      double zgdph_r = -zrg_r * (A2(paph, jl, jk + 1) - A2(paph, jl, jk)) * zqtmst;
+      A2(pfsqlf, jl, jk + 1) = A2(pfsqlf, jl, jk);
+      A2(pfsqif, jl, jk + 1) = A2(pfsqif, jl, jk);
+      A2(pfsqrf, jl, jk + 1) = A2(pfsqlf, jl, jk);
+      A2(pfsqsf, jl, jk + 1) = A2(pfsqif, jl, jk);
+      A2(pfcqlng, jl, jk + 1) = A2(pfcqlng, jl, jk);
+      A2(pfcqnng, jl, jk + 1) = A2(pfcqnng, jl, jk);
+      A2(pfcqrng, jl, jk + 1) = A2(pfcqlng, jl, jk);
+      A2(pfcqsng, jl, jk + 1) = A2(pfcqnng, jl, jk);
+      A2(pfsqltur, jl, jk + 1) = A2(pfsqltur, jl, jk);
+      A2(pfsqitur, jl, jk + 1) = A2(pfsqitur, jl, jk);
+      A2(pfsqlf, jl, jk + 1) =
+          A2(pfsqlf, jl, jk + 1) +
+          (A3(zqxn2d, jl, jk, NCLDQL, klev) - A3(zqx0, jl, jk, NCLDQL, klev) + A2(pvfl, jl, jk) * ptsphy) * zgdph_r +
+          A3(pludeli, jl, jk, 1, klev);
+      A2(pfcqlng, jl, jk + 1) = A2(pfcqlng, jl, jk + 1) + A3(zlneg, jl, jk, NCLDQL, klev) * zgdph_r;
+      A2(pfsqltur, jl, jk + 1) = A2(pfsqltur, jl, jk + 1) + A2(pvfl, jl, jk) * ptsphy * zgdph_r;
+      A2(pfsqrf, jl, jk + 1) =
+          A2(pfsqrf, jl, jk + 1) + (A3(zqxn2d, jl, jk, NCLDQR, klev) - A3(zqx0, jl, jk, NCLDQR, klev)) * zgdph_r;
+      A2(pfcqrng, jl, jk + 1) = A2(pfcqrng, jl, jk + 1) + A3(zlneg, jl, jk, NCLDQR, klev) * zgdph_r;
+      A2(pfsqif, jl, jk + 1) =
+          A2(pfsqif, jl, jk + 1) +
+          (A3(zqxn2d, jl, jk, NCLDQI, klev) - A3(zqx0, jl, jk, NCLDQI, klev) + A2(pvfi, jl, jk) * ptsphy) * zgdph_r +
+          A3(pludeli, jl, jk, 2, klev);
+      A2(pfcqnng, jl, jk + 1) = A2(pfcqnng, jl, jk + 1) + A3(zlneg, jl, jk, NCLDQI, klev) * zgdph_r;
+      A2(pfsqitur, jl, jk + 1) = A2(pfsqitur, jl, jk + 1) + A2(pvfi, jl, jk) * ptsphy * zgdph_r;
+      A2(pfsqsf, jl, jk + 1) =
+          A2(pfsqsf, jl, jk + 1) + (A3(zqxn2d, jl, jk, NCLDQS, klev) - A3(zqx0, jl, jk, NCLDQS, klev)) * zgdph_r;
+      A2(pfcqsng, jl, jk + 1) = A2(pfcqsng, jl, jk + 1) + A3(zlneg, jl, jk, NCLDQS, klev) * zgdph_r;
+    }
+  for (jk = 1; jk <= klev + 1; jk++)
+    for (jl = kidia; jl <= kfdia; jl++) {
+      A2(pfhpsl, jl, jk) = -p->rlvtt * A2(pfplsl, jl, jk);
+      A2(pfhpsn, jl, jk) = -p->rlstt * A2(pfplsn, jl, jk);
+    }
+
+  free(buf);
+  return nwarn;
+}
+
+int oracle_cloudsc_batched(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_cld, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_cld, const double *pvfl,
+    const double *pvfi, const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis, const double *plu,
+    double *plude, const double *pludeli, const double *psnde, const double *pmfu,
+    const double *pmfd, const double *pa, const double *pclv, double *pcovptot,
+    double *prainfrac_toprfz, double *pfsqlf, double *pfsqif, double *pfcqnng,
+    double *pfcqlng, double *pfsqrf, double *pfsqsf, double *pfcqrng, double *pfcqsng,
+    double *pfsqltur, double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
+    double *pfhpsn, int nthreads) {
+  if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
+      ngptot <= nproma * (ngpblks - 1))
+    return CLOUDSC_E_SHAPE;
+  const size_t s2 = (size_t)nproma * klev, s2h = (size_t)nproma * (klev + 1), s1 = nproma;
+  int total = 0, err = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) reduction(min : err)
+  for (int ib = 0; ib < ngpblks; ib++) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    double *peis_blk = (double *)(peis + ib * s1); /* read only by CLOUDSC */
+    int r = oracle_cloudsc(
+        p, 1, icend, nproma, klev, 0, ptsphy, pt + ib * s2, pq + ib * s2, ptendency_cml_t + ib * s2,
+        ptendency_cml_q + ib * s2, ptendency_cml_a + ib * s2, ptendency_cml_cld + ib * s2 * NCLV,
+        ptendency_loc_t + ib * s2, ptendency_loc_q + ib * s2, ptendency_loc_a + ib * s2,
+        ptendency_loc_cld + ib * s2 * NCLV, NULL, pvfl + ib * s2, pvfi + ib * s2, NULL, NULL, NULL,
+        NULL, NULL, NULL, NULL, NULL, pap + ib * s2, paph + ib * s2h, NULL, plsm + ib * s1, NULL,
+        ldcum + ib * s1, NULL, ktype + ib * s1, NULL, peis_blk, plu + ib * s2, plude + ib * s2,
+        pludeli + ib * s2 * 4, psnde + ib * s2 * 2, pmfu + ib * s2, pmfd + ib * s2, NULL, 0,
+        pa + ib * s2, pclv + ib * s2 * NCLV, NULL, NULL, NULL, NULL, NULL, pcovptot + ib * s2, NULL,
+        prainfrac_toprfz + ib * s1, pfsqlf + ib * s2h, pfsqif + ib * s2h, pfcqnng + ib * s2h,
+        pfcqlng + ib * s2h, pfsqrf + ib * s2h, pfsqsf + ib * s2h, pfcqrng + ib * s2h,
+        pfcqsng + ib * s2h, pfsqltur + ib * s2h, pfsqitur + ib * s2h, pfplsl + ib * s2h,
+        pfplsn + ib * s2h, pfhpsl + ib * s2h, pfhpsn + ib * s2h, NULL, 0);
+    if (r < 0) err = r < err ? r : err;
+    else total += r;
+  }
+  return err < 0 ? err : total;
+}

@@ -1,0 +1,76 @@
+"""ORACLE -- TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of liboracle_cloudsc.so, the CPU restatement of the reference's
+double-precision CLOUDSC (cloudsc_oracle.c).  Only tests/, the smoke test and
+bench.py's CPU-baseline leg use it, as the checker; the product never calls it.
+Parity unpinned: the reference has no CLOUDSC golden vectors and cannot be
+compiled here (no Fortran compiler).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liboracle_cloudsc.so")
+_lib = None
+
+
+def build():
+    r = subprocess.run(["make", "-s", "-C", _HERE], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        from openifs_b200.params import CloudscParams
+        from openifs_b200.fields import BATCHED_FIELDS
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER(CloudscParams)
+        vp = ctypes.c_void_p
+        i32 = ctypes.c_int
+        L.oracle_params_default.argtypes = [ctypes.c_double, i32, P]
+        L.oracle_params_default.restype = i32
+        L.oracle_fcgeneralized_gamma.argtypes = [ctypes.c_double]
+        L.oracle_fcgeneralized_gamma.restype = ctypes.c_double
+        L.oracle_cloudsc_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
+                                             [vp] * len(BATCHED_FIELDS) + [i32])
+        L.oracle_cloudsc_batched.restype = i32
+        _lib = L
+    return _lib
+
+
+def params_default(tsphy, ncldtop):
+    from openifs_b200.params import CloudscParams
+    p = CloudscParams()
+    rc = lib().oracle_params_default(float(tsphy), int(ncldtop), ctypes.byref(p))
+    if rc != 0:
+        raise RuntimeError(f"oracle_params_default returned {rc}")
+    return p
+
+
+def gamma(x):
+    return lib().oracle_fcgeneralized_gamma(float(x))
+
+
+def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthreads=0):
+    """Run the oracle over all blocks of ``arrays`` (numpy, fields layout), in
+    place.  Returns the number of negative-condensate warning events."""
+    from openifs_b200.fields import BATCHED_FIELDS
+    ptrs = []
+    for n, *_ in BATCHED_FIELDS:
+        a = arrays[n]
+        if not (isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"]):
+            raise ValueError(f"{n}: need a C-contiguous numpy array")
+        ptrs.append(a.ctypes.data)
+    rc = lib().oracle_cloudsc_batched(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
+                                      int(ngptot), float(ptsphy), *ptrs, int(nthreads))
+    if rc < 0:
+        raise RuntimeError(f"oracle_cloudsc_batched returned {rc}")
+    return rc
