@@ -1,0 +1,358 @@
+"""CLOUDSC on B200: columns/s of the FP64 and FP32-mixed kernels.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Workload (the configuration the headline metric is quoted on): 262,144
+columns = 2,048 NPROMA blocks of 128, L137, PTSPHY 3600 s, seeded synthetic
+state (openifs_b200/inputs.py, seed 2).  One step is one batched CLOUDSC call
+over every column; inputs stay resident in HBM (15 GB, far above the 126 MB
+L2, so no flush is needed between steps).  PLUDE is INOUT (cloudsc.F90:1367),
+so it is restored from a pristine copy before every step, outside the timed
+kernel.  ``value`` is FP64 columns/s; the FP32-mixed form is reported beside
+it with its error against the FP64 kernel.  ``e2e`` is the same FP64 metric
+through cloudsc_b200_batched_host with page-locked host buffers (copies in
+the timed region).  Under torchrun each rank runs its own 262,144 columns
+(weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NPROMA, NGPBLKS, KLEV, PTSPHY, SEED = 128, 2048, 137, 3600.0, 2
+NCOL = NPROMA * NGPBLKS
+WORKLOAD = ("CLOUDSC, 262,144 columns (2,048 NPROMA blocks of 128) x L137, PTSPHY 3600 s, "
+            "seeded synthetic state")
+METRIC = "CLOUDSC columns/s on 1 B200: FP64 vs FP32-mixed vs surrogate, at fixed error"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason sampling during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(p_oracle, nblocks=64, threads=0):
+    """The oracle (the reference algorithm restated in C, system libm) on a
+    bounded sample of the workload: ``nblocks`` NPROMA blocks of 128, OpenMP
+    over blocks (ec_phys_drv.F90:438).  Returns columns/s."""
+    from openifs_b200 import inputs
+    from oracle import oracle
+    arrs = inputs.generate(nblocks, NPROMA, p_oracle, seed=SEED)
+    work = {k: v.copy() for k, v in arrs.items()}
+    oracle.cloudsc_batched(p_oracle, work, NPROMA, KLEV, nblocks, nblocks * NPROMA, PTSPHY,
+                           threads, libm="glibc")  # warm
+    best = None
+    reps = 0
+    t_end = time.perf_counter() + 10.0
+    while reps < 2 or time.perf_counter() < t_end:
+        work = {k: v.copy() for k, v in arrs.items()}
+        t = time.perf_counter()
+        oracle.cloudsc_batched(p_oracle, work, NPROMA, KLEV, nblocks, nblocks * NPROMA, PTSPHY,
+                               threads, libm="glibc")
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+        reps += 1
+    return nblocks * NPROMA / best, reps
+
+
+def run_reference(a):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from openifs_b200 import cloudsc, inputs
+    from oracle import oracle
+    nc = inputs.ncldtop_l137()
+    p = oracle.params_default(PTSPHY, nc)
+    ncores = os.cpu_count() or 1
+    nblocks = 64
+    arrs = inputs.generate(nblocks, NPROMA, p, seed=SEED)
+    times = []
+    for i in range(a.warmup + a.steps):
+        work = {k: v.copy() for k, v in arrs.items()}
+        t = time.perf_counter()
+        oracle.cloudsc_batched(p, work, NPROMA, KLEV, nblocks, nblocks * NPROMA, PTSPHY, 0,
+                               libm="glibc")
+        if i >= a.warmup:
+            times.append(time.perf_counter() - t)
+    ms = 1e3 * statistics.mean(times)
+    val = nblocks * NPROMA / (ms * 1e-3)
+    sample = f"{nblocks} NPROMA blocks of 128 ({nblocks * NPROMA} columns) of the workload per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "columns/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, openifs_b200/inputs.py)",
+        "config": {"workload": WORKLOAD, "columns": NCOL, "nproma": NPROMA, "klev": KLEV,
+                   "sample_columns_per_step": nblocks * NPROMA},
+        "cpu_baseline": {"value": val, "unit": "columns/s", "cores": ncores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": val, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("the reference Fortran cannot be compiled in this image (no Fortran compiler); "
+                 "the reference arm is its C restatement (oracle/cloudsc_oracle.c, system libm), "
+                 f"OpenMP over NPROMA blocks on {ncores} host threads"),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a):
+    import torch
+    from openifs_b200 import cloudsc, fields, inputs
+
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    p = cloudsc.default_params(PTSPHY, inputs.ncldtop_l137())
+    cloudsc.setup(p)
+    host = inputs.generate(NGPBLKS, NPROMA, p, seed=SEED + 1000 * rank)
+    d = {k: torch.from_numpy(v).to(dev) for k, v in host.items()}
+    plude0 = d["plude"].clone()
+    stream = torch.cuda.current_stream(dev)
+
+    def step(prec):
+        d["plude"].copy_(plude0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=prec,
+                                stream=stream)
+        e1.record(stream)
+        return e0, e1
+
+    def timed(prec, k, w):
+        for _ in range(w):
+            step(prec)
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [step(prec) for _ in range(k)]
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            torch.distributed.barrier()
+        ms = [a_.elapsed_time(b_) for a_, b_ in ev]
+        return ms
+
+    results = {}
+    clocks = None
+    for prec, name in ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed")):
+        if name == "fp64":
+            with ClockSampler(local) as cs:
+                ms = timed(prec, a.steps, a.warmup)
+            clocks = cs.summary()
+        else:
+            ms = timed(prec, a.steps, a.warmup)
+        mean_ms = statistics.mean(ms)
+        if world > 1:
+            t = torch.tensor([mean_ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            mean_ms = float(t.item())
+        results[name] = {"ms": mean_ms, "min_ms": min(ms)}
+
+    # fixed-error check of the mixed form against the FP64 kernel (same inputs)
+    outs = fields.OUTPUT_NAMES
+    d["plude"].copy_(plude0)
+    cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.FP64)
+    ref = {n: d[n].clone() for n in outs}
+    d["plude"].copy_(plude0)
+    cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.MIXED)
+    torch.cuda.synchronize(dev)
+    err = {}
+    for n in ["tendency_loc_t", "tendency_loc_q", "tendency_loc_a", "tendency_loc_cld",
+              "pfplsl", "pfplsn"]:
+        r, g = ref[n], d[n]
+        if n == "tendency_loc_cld":
+            r, g = r[:, :4], g[:, :4]
+        if n in ("pfplsl", "pfplsn"):  # surface fluxes
+            r, g = r[:, -1], g[:, -1]
+        diff = (g - r).abs()
+        err[n] = {"max_abs_over_max": float(diff.max() / r.abs().max().clamp_min(1e-300)),
+                  "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
+    del ref
+
+    # end to end through the host-pointer API (page-locked buffers, copies timed)
+    e2e = None
+    if not a.no_e2e:
+        pin = {k: torch.from_numpy(v).pin_memory() for k, v in host.items()}
+        plude_h = pin["plude"].clone()
+        h2d = sum(pin[n].numel() * pin[n].element_size() for n in fields.INPUT_NAMES)
+        d2h = sum(pin[n].numel() * pin[n].element_size() for n in fields.OUTPUT_NAMES)
+        tt = []
+        for i in range(max(1, a.warmup) + a.steps):
+            pin["plude"].copy_(plude_h)
+            t = time.perf_counter()
+            cloudsc.cloudsc_batched_host(p, pin, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY)
+            dt = time.perf_counter() - t
+            if i >= max(1, a.warmup):
+                tt.append(dt)
+        e2e_s = statistics.mean(tt)
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * NCOL / e2e_s, "unit": "columns/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
+               "api": "cloudsc_b200_batched_host, page-locked host arrays"}
+        del pin
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return 0
+
+    rb, wb = fields.bytes_per_column()
+    algo_bytes = NCOL * (rb + wb)
+    peaks = _peaks()
+    ms64 = results["fp64"]["ms"]
+    achieved = algo_bytes / (ms64 * 1e-3) / 1e9
+    peak, peak_src = (peaks["hbm_gbs"], "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)") if peaks \
+        else (6650.0, "fallback")
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "cloudsc_fp64_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": algo_bytes, "kernel": "cloudsc_kernel<double>"}
+
+    from oracle import oracle
+    po = oracle.params_default(PTSPHY, p.ncldtop)
+    cpu_val, reps = cpu_baseline(po)
+    ncores = os.cpu_count() or 1
+
+    value = world * NCOL / (ms64 * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms64,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, openifs_b200/inputs.py; no public dataset involved)",
+        "config": {"workload": WORKLOAD, "columns_per_gpu": NCOL, "nproma": NPROMA,
+                   "ngpblks": NGPBLKS, "klev": KLEV, "ptsphy": PTSPHY,
+                   "l2": "inputs 15 GB resident in HBM, > 126 MB L2; no flush needed",
+                   "launch": "one persistent launch per step"},
+        "forms": {
+            "fp64": {"columns_per_s": value, "ms": ms64, "min_ms": results["fp64"]["min_ms"]},
+            "mixed": {"columns_per_s": world * NCOL / (results["mixed"]["ms"] * 1e-3),
+                      "ms": results["mixed"]["ms"], "speedup_vs_fp64": ms64 / results["mixed"]["ms"],
+                      "error_vs_fp64": err},
+            "surrogate": None,
+        },
+        "roofline": roofline,
+        "cpu_baseline": {"value": cpu_val, "unit": "columns/s", "cores": ncores, "kind": "port",
+                         "sample": f"64 NPROMA blocks of 128 (8,192 columns) of the workload, "
+                                   f"best of {reps} warm runs, OpenMP over blocks"},
+        "e2e": e2e,
+        "clocks": clocks,
+        "gpu_launches": a.steps,
+    }
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,964 @@
+// Per-column CLOUDSC body (device code), shared by the GPU kernels
+// (cloudsc_kernels.cu) and by the host build of the same code that the tests
+// compare against the oracle (tests/hostemu).  The including file provides:
+//   CSC_DEV           function qualifiers (__device__ __forceinline__ on the GPU)
+//   KP<Real>()        the KParams<Real> block, c_kd the KParamsD block
+//   ld(p), atomic_add(p, v), xexp/xpow/xsqrt/xabs/xsign overloads
+// See cloudsc_column.cuh for the numerical contract.
+#pragma once
+#include "cloudsc_column.cuh"
+
+namespace cloudsc {
+
+// ---------------------------------------------------------------------------
+// Sink truncation of one species row (cloudsc.F90:3500-3535 for one JM):
+// the sink sum over the row's structurally non-zero entries in column order,
+// the scaling factor, then every negative entry (JO,n) and its mirror (n,JO)
+// rescaled; a negative diagonal entry is scaled twice, as the reference's JN
+// loop does.
+// ---------------------------------------------------------------------------
+#define ROWSCALE_BEGIN(QJO)                         \
+  {                                                 \
+    double zmm = mx(QJO, zepsec);                   \
+    double zrr = mx(ss, zmm);                       \
+    double zr = zmm / zrr;
+#define ROWSCALE_END }
+#define SCL(F, A, B) \
+  if (F) {           \
+    A = A * zr;      \
+    B = B * zr;      \
+  }
+
+struct QA {
+  // explicit sources/sinks ZSOLQA(a,b): "+" is a source of a and sink of b
+  double LL, LI, LV, IL, II, IR, IV, RI, RR, RS, RV, SR, SS, SV, VL, VI, VR, VS;
+};
+
+CSC_DEV void scale_row(int jo, QA &q, const double qx[5]) {
+  const double zepsec = 1.E-14;
+  double ss;
+  switch (jo) {
+    case L: {
+      bool fLL = q.LL < 0.0, fLI = q.LI < 0.0, fLV = q.LV < 0.0;
+      ss = 0.0 - q.LL;
+      ss = ss - q.LI;
+      ss = ss - q.LV;
+      ROWSCALE_BEGIN(qx[L])
+      SCL(fLL, q.LL, q.LL)
+      SCL(fLI, q.LI, q.IL)
+      SCL(fLV, q.LV, q.VL)
+      ROWSCALE_END
+    } break;
+    case I: {
+      bool fIL = q.IL < 0.0, fII = q.II < 0.0, fIR = q.IR < 0.0, fIV = q.IV < 0.0;
+      ss = 0.0 - q.IL;
+      ss = ss - q.II;
+      ss = ss - q.IR;
+      ss = ss - q.IV;
+      ROWSCALE_BEGIN(qx[I])
+      SCL(fIL, q.IL, q.LI)
+      SCL(fII, q.II, q.II)
+      SCL(fIR, q.IR, q.RI)
+      SCL(fIV, q.IV, q.VI)
+      ROWSCALE_END
+    } break;
+    case R: {
+      bool fRI = q.RI < 0.0, fRR = q.RR < 0.0, fRS = q.RS < 0.0, fRV = q.RV < 0.0;
+      ss = 0.0 - q.RI;
+      ss = ss - q.RR;
+      ss = ss - q.RS;
+      ss = ss - q.RV;
+      ROWSCALE_BEGIN(qx[R])
+      SCL(fRI, q.RI, q.IR)
+      SCL(fRR, q.RR, q.RR)
+      SCL(fRS, q.RS, q.SR)
+      SCL(fRV, q.RV, q.VR)
+      ROWSCALE_END
+    } break;
+    case S: {
+      bool fSR = q.SR < 0.0, fSS = q.SS < 0.0, fSV = q.SV < 0.0;
+      ss = 0.0 - q.SR;
+      ss = ss - q.SS;
+      ss = ss - q.SV;
+      ROWSCALE_BEGIN(qx[S])
+      SCL(fSR, q.SR, q.RS)
+      SCL(fSS, q.SS, q.SS)
+      SCL(fSV, q.SV, q.VS)
+      ROWSCALE_END
+    } break;
+    default: {
+      bool fVL = q.VL < 0.0, fVI = q.VI < 0.0, fVR = q.VR < 0.0, fVS = q.VS < 0.0;
+      ss = 0.0 - q.VL;
+      ss = ss - q.VI;
+      ss = ss - q.VR;
+      ss = ss - q.VS;
+      ROWSCALE_BEGIN(qx[V])
+      SCL(fVL, q.VL, q.LV)
+      SCL(fVI, q.VI, q.IV)
+      SCL(fVR, q.VR, q.RV)
+      SCL(fVS, q.VS, q.SV)
+      ROWSCALE_END
+    } break;
+  }
+}
+
+// ZRATIO for every species from the current ZSOLQA (cloudsc.F90:3455-3474).
+CSC_DEV void sink_ratios(const QA &q, const double qx[5], double r[5]) {
+  const double zepsec = 1.E-14;
+  double s;
+  s = 0.0 - q.LL; s = s - q.LI; s = s - q.LV;
+  { double zmax = mx(qx[L], zepsec); r[L] = zmax / mx(s, zmax); }
+  s = 0.0 - q.IL; s = s - q.II; s = s - q.IR; s = s - q.IV;
+  { double zmax = mx(qx[I], zepsec); r[I] = zmax / mx(s, zmax); }
+  s = 0.0 - q.RI; s = s - q.RR; s = s - q.RS; s = s - q.RV;
+  { double zmax = mx(qx[R], zepsec); r[R] = zmax / mx(s, zmax); }
+  s = 0.0 - q.SR; s = s - q.SS; s = s - q.SV;
+  { double zmax = mx(qx[S], zepsec); r[S] = zmax / mx(s, zmax); }
+  s = 0.0 - q.VL; s = s - q.VI; s = s - q.VR; s = s - q.VS;
+  { double zmax = mx(qx[V], zepsec); r[V] = zmax / mx(s, zmax); }
+}
+
+// ---------------------------------------------------------------------------
+// CLOUD_SUPERSATCHECK (cloud_supersatcheck.F90:111-226, KFTLIQICE=1), double.
+// ---------------------------------------------------------------------------
+CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp,
+                                              double &t_adj, double &q_adj, double &a_adj,
+                                              double &l_adj, double &i_adj) {
+  const KParamsD &k = c_kd;
+  const double zepsec = 1.E-14;
+  double zda = 0.0;
+  double zt = mx(pt, 160.0);
+  double za = mx(mn(pa, 1.0), 0.0);
+  double zp_r = 1.0 / pp;
+  double el = xexp(k.r3les * (zt - k.rtt) / (zt - k.r4les));
+  double x = (mx(k.rtice, mn(k.rtwat, zt)) - k.rtice) * k.rtwat_rtice_r;
+  double alfa = mn(1.0, x * x);
+  bool delta = copysign(1.0, zt - k.rtt) > 0.0;  // FOEDELTA = 1
+  double ei = 0.0;
+  if (!delta || alfa < 1.0) ei = xexp(k.r3ies * (zt - k.rtt) / (zt - k.r4ies));
+  double zfoeeliq = mn((k.r2es * el) * zp_r, 0.5);
+  double foeew = delta ? k.r2es * el : k.r2es * ei;
+  double zfoeeice = mn(foeew * zp_r, 0.5);
+  double zfokoop = mn(zfoeeice * (k.rkoop1 - k.rkoop2 * zt), zfoeeliq);
+  double zqsliqk = zfokoop / (1.0 - k.retv * zfokoop);
+  double wsum = (alfa < 1.0) ? alfa * el + (1.0 - alfa) * ei : el;
+  double zfoeemix = mn((k.r2es * wsum) * zp_r, 0.5);
+  double zcor = 1.0 / (1.0 - k.retv * zfoeemix);
+  double zqsmix = zfoeemix * zcor;
+  double xl = zt - k.r4les, xi = zt - k.r4ies;
+  double foedem = alfa * k.r5alvcp * (1.0 / (xl * xl)) + (1.0 - alfa) * k.r5alscp * (1.0 / (xi * xi));
+  double zcorqsmix = 1.0 + zqsmix * zcor * foedem;
+  zqsliqk = 0.5 * (zqsliqk + zqsmix);
+  double zqslim = za * zqsmix + (1.0 - za) * zqsliqk;
+  double zcond = mx(pq - zqslim, 0.0);
+  if (zcond > zepsec) {
+    double zfaci = alfa + (1.0 - alfa) * k.rssicefactor;
+    zda = (1.0 - za) * zfaci;
+    double za_upd = za + zda;
+    zqslim = za_upd * zqsmix + (1.0 - za_upd) * zqsliqk;
+    zcond = (pq - zqslim) / zcorqsmix;
+  }
+  double foeldcpm = alfa * k.ralvdcp + (1.0 - alfa) * k.ralsdcp;
+  t_adj = foeldcpm * zcond;
+  q_adj = -zcond;
+  a_adj = zda;
+  l_adj = zcond * alfa;
+  i_adj = zcond * (1.0 - alfa);
+}
+
+// ---------------------------------------------------------------------------
+// The column body.
+// ---------------------------------------------------------------------------
+template <typename Real, bool F32M>
+CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
+  const KParams<Real> &P = KP<Real>();
+  const KParamsD &PD = c_kd;
+  typedef double D;
+#define C(x) Real(x)
+  const int np = sh.nproma, klev = sh.klev;
+  const size_t s2 = (size_t)np * klev, s2h = (size_t)np * (klev + 1);
+  const size_t o2 = (size_t)ib * s2 + jl, o2h = (size_t)ib * s2h + jl, o1 = (size_t)ib * np + jl;
+  const D dt = sh.ptsphy;
+  const D zqtmst = 1.0 / dt;
+  const Real rdt = Real(dt), rqtmst = Real(zqtmst);
+  const Real zepsec = C(1.E-14);
+  const D zepsecd = 1.E-14;
+  const Real zepsilon = C(100.0 * 0x1p-52);  // 100*EPSILON(1._JPRB), cloudsc.F90:693
+  const int ncldtop0 = P.ncldtop - 1;  // 0-based first level of the loop
+  const Real zrdtgdp_f = C(1.0) / (rdt * P.rg);
+
+  // per-column inputs
+  const Real plsm = Real(ld(F.plsm + o1));
+  const bool ldcum = ld(F.ldcum + o1) != 0;
+  const int ktype = ld(F.ktype + o1);
+  const Real peis = Real(ld(F.peis + o1));
+  const D paph_surf = ld(F.paph + o2h + (size_t)klev * np);
+  Real zadvw = C(1.0), zadvwd = C(1.0);
+  if (ktype == 1 && P.rmfadvw > C(0.0)) {
+    zadvw = C(1.0) - P.rmfadvw;
+    zadvwd = C(1.0) - P.rmfadvw * P.rmfadvwdd;
+  }
+  const Real zconstpow = plsm > C(0.5) ? P.zconst_pow_land : P.zconst_pow_sea;
+
+  // state carried between levels
+  D paph_k = ld(F.paph + o2h);
+  Real pmfu_k = Real(ld(F.pmfu + o2)), pmfd_k = Real(ld(F.pmfd + o2));
+  Real za_prev = C(0.0), qr_prev = C(0.0), qs_prev = C(0.0), t_prev = C(0.0), pap_prev = C(0.0);
+  Real qxnm1_l = C(0.0), qxnm1_i = C(0.0), qxnm1_r = C(0.0), qxnm1_s = C(0.0);
+  Real zanewm1 = C(0.0), zcovptot = C(0.0), zcovpmax = C(0.0), zcldtopdist = C(0.0);
+  bool llrainliq = true;
+  Real prainfrac = C(0.0);
+  Real pfplsx_i = C(0.0), pfplsx_r = C(0.0), pfplsx_s = C(0.0);  // ZPFPLSX(JK)
+  D fsqlf = 0.0, fsqif = 0.0, fcqlng = 0.0, fcqnng = 0.0, fsqltur = 0.0, fsqitur = 0.0;
+  unsigned nwarn = 0;
+
+  // flux index 1 (:4231-4241)
+  F.pfsqlf[o2h] = 0.0; F.pfsqif[o2h] = 0.0; F.pfsqrf[o2h] = 0.0; F.pfsqsf[o2h] = 0.0;
+  F.pfcqlng[o2h] = 0.0; F.pfcqnng[o2h] = 0.0; F.pfcqrng[o2h] = 0.0; F.pfcqsng[o2h] = 0.0;
+  F.pfsqltur[o2h] = 0.0; F.pfsqitur[o2h] = 0.0;
+
+  // (KLON,KLEV,N) arrays: the block stride is N*KLON*KLEV, species m at +m*KLON*KLEV
+  const size_t o5 = (size_t)ib * 5 * s2 + jl, o4 = (size_t)ib * 4 * s2 + jl, o2s = (size_t)ib * 2 * s2 + jl;
+  for (int k = 0; k < klev; ++k) {
+    const size_t ok = o2 + (size_t)k * np;
+    const size_t ok5 = o5 + (size_t)k * np, ok4 = o4 + (size_t)k * np, ok2s = o2s + (size_t)k * np;
+    // ---------------- loads for level k ----------------
+    const D pt_k = ld(F.pt + ok), pq_k = ld(F.pq + ok), pa_k = ld(F.pa + ok);
+    const D cml_t = ld(F.cml_t + ok), cml_q = ld(F.cml_q + ok), cml_a = ld(F.cml_a + ok);
+    const D cl_l = ld(F.cml_cld + ok5), cl_i = ld(F.cml_cld + ok5 + s2),
+            cl_r = ld(F.cml_cld + ok5 + 2 * s2), cl_s = ld(F.cml_cld + ok5 + 3 * s2);
+    const D pc_l = ld(F.pclv + ok5), pc_i = ld(F.pclv + ok5 + s2), pc_r = ld(F.pclv + ok5 + 2 * s2),
+            pc_s = ld(F.pclv + ok5 + 3 * s2);
+    const D pap_kd = ld(F.pap + ok);
+    const D paph_k1 = ld(F.paph + o2h + (size_t)(k + 1) * np);
+    const D pvfl = ld(F.pvfl + ok), pvfi = ld(F.pvfi + ok);
+    const D pludeli1 = ld(F.pludeli + ok4), pludeli2 = ld(F.pludeli + ok4 + s2);
+    const bool last = (k == klev - 1);
+    Real pmfu_k1 = C(0.0), pmfd_k1 = C(0.0), plu_k1 = C(0.0);
+    if (!last) {
+      pmfu_k1 = Real(ld(F.pmfu + ok + np));
+      pmfd_k1 = Real(ld(F.pmfd + ok + np));
+      plu_k1 = Real(ld(F.plu + ok + np));
+    }
+    D plude_k = F.plude[ok];
+    const Real pap_k = Real(pap_kd);
+
+    // ---------------- first guess (:982-1002) ----------------
+    const Real t = Real(pt_k + dt * cml_t);
+    Real qv = Real(pq_k + dt * cml_q);
+    Real a = Real(pa_k + dt * cml_a);
+    const D aorig = pa_k + dt * cml_a;
+    const D q0_l = pc_l + dt * cl_l, q0_i = pc_i + dt * cl_i, q0_r = pc_r + dt * cl_r,
+            q0_s = pc_s + dt * cl_s;
+    Real ql = Real(q0_l), qi = Real(q0_i), qr = Real(q0_r), qs = Real(q0_s);
+
+    // ---------------- saturation (:1087-1115) ----------------
+    // (only the loop levels JK >= NCLDTOP read these)
+    Real alfa = C(0.0), zfoeewm = C(0.0), zqsmix = C(0.0), zfoeew = C(0.0), zqsice = C(0.0);
+    Real zfoeeliqt = C(0.0), zqsliq = C(0.0), el_e = C(0.0), ei_e = C(0.0);
+    if (k >= ncldtop0) {
+      Real x = (mx(P.rtice, mn(P.rtwat, t)) - P.rtice) * P.rtwat_rtice_r;
+      alfa = mn(C(1.0), x * x);
+      el_e = mexp<F32M>(P.r3les * (t - P.rtt) / (t - P.r4les));
+      bool delta = xsign(C(1.0), t - P.rtt) > C(0.0);
+      ei_e = C(0.0);
+      if (!delta || alfa < C(1.0)) ei_e = mexp<F32M>(P.r3ies * (t - P.rtt) / (t - P.r4ies));
+      Real wsum = (alfa < C(1.0)) ? alfa * el_e + (C(1.0) - alfa) * ei_e : el_e;
+      zfoeewm = mn((P.r2es * wsum) / pap_k, C(0.5));
+      zqsmix = zfoeewm;
+      zqsmix = zqsmix / (C(1.0) - P.retv * zqsmix);
+      Real eew = delta ? P.r2es * el_e : P.r2es * ei_e;
+      zfoeew = mn(eew / pap_k, C(0.5));
+      zfoeew = mn(C(0.5), zfoeew);
+      zqsice = zfoeew / (C(1.0) - P.retv * zfoeew);
+      zfoeeliqt = mn((P.r2es * el_e) / pap_k, C(0.5));
+      zqsliq = zfoeeliqt;
+      zqsliq = zqsliq / (C(1.0) - P.retv * zqsliq);
+    }
+
+    // ---------------- tidy up (:1127-1199) ----------------
+    D loc_t = 0.0, loc_q = 0.0;
+    D lneg_l = 0.0, lneg_i = 0.0, lneg_r = 0.0, lneg_s = 0.0;
+    if (ql + qi < P.rlmin || a < P.ramin) {
+      D qadj;
+      lneg_l = lneg_l + D(ql);
+      qadj = D(ql) * zqtmst;
+      loc_q = loc_q + qadj;
+      loc_t = loc_t - PD.ralvdcp * qadj;
+      qv = qv + ql;
+      ql = C(0.0);
+      lneg_i = lneg_i + D(qi);
+      qadj = D(qi) * zqtmst;
+      loc_q = loc_q + qadj;
+      loc_t = loc_t - PD.ralsdcp * qadj;
+      qv = qv + qi;
+      qi = C(0.0);
+      a = C(0.0);
+    }
+#define TIDY(QQ, LNEG, RAL)               \
+  if (QQ < P.rlmin) {                     \
+    LNEG = LNEG + D(QQ);                  \
+    D qadj = D(QQ) * zqtmst;              \
+    loc_q = loc_q + qadj;                 \
+    loc_t = loc_t - PD.RAL * qadj;        \
+    qv = qv + QQ;                         \
+    QQ = C(0.0);                          \
+  }
+    TIDY(ql, lneg_l, ralvdcp)
+    TIDY(qi, lneg_i, ralsdcp)
+    TIDY(qr, lneg_r, ralvdcp)
+    TIDY(qs, lneg_s, ralsdcp)
+#undef TIDY
+    a = mx(C(0.0), mn(C(1.0), a));
+    const Real zli = ql + qi;
+    Real liqfrac = C(0.0), icefrac = C(0.0);
+    if (zli > P.rlmin) {
+      liqfrac = ql / zli;
+      icefrac = C(1.0) - liqfrac;
+    }
+
+    D loc_a = 0.0, loc_cl = 0.0, loc_ci = 0.0, loc_cr = 0.0, loc_cs = 0.0;
+    D qxn2d_l = 0.0, qxn2d_i = 0.0, qxn2d_r = 0.0, qxn2d_s = 0.0;
+    Real pfplsx_i_n = C(0.0), pfplsx_r_n = C(0.0), pfplsx_s_n = C(0.0);
+    Real covp_out = C(0.0);
+
+    if (k >= ncldtop0) {
+      // ================= level physics (:1228-3823) =================
+      Real qxfg_l = ql, qxfg_i = qi, qxfg_r = qr, qxfg_s = qs;
+      Real solac = C(0.0), solab = C(0.0);
+      QA q;
+      q.LL = q.LI = q.LV = q.IL = q.II = q.IR = q.IV = q.RI = q.RR = q.RS = q.RV = q.SR = q.SS = q.SV =
+          q.VL = q.VI = q.VR = q.VS = 0.0;
+      Real qb_ll = C(0.0), qb_ii = C(0.0), qb_rl = C(0.0), qb_si = C(0.0), qb_sl = C(0.0);
+      Real convsrce_l = C(0.0), convsrce_i = C(0.0), convsrce_r = C(0.0), convsrce_s = C(0.0);
+      Real convsink_l = C(0.0), convsink_i = C(0.0);
+      Real fallsrce_i = C(0.0), fallsrce_r = C(0.0), fallsrce_s = C(0.0);
+      Real qpretot = C(0.0);
+      // The ZSOLQA accumulators are double in both instantiations; in the
+      // FP32-mixed kernel each process rate (Real) is widened when added.
+#define QADD(E, X) q.E = q.E + double(X)
+#define QSUB(E, X) q.E = q.E - double(X)
+
+      // derived variables (:1281-1324)
+      const Real zdp = Real(paph_k1 - paph_k);
+      const Real zgdp = P.rg / zdp;
+      const Real zrho = pap_k / (P.rd * t);
+      const Real zdtgdp = rdt * zgdp;
+      const Real zrdtgdp = zdp * zrdtgdp_f;
+      Real zcorqsliq, zcorqsice, zcorqsmix, zdqsmixdt, zevaplimmix;
+      {
+        Real xl = t - P.r4les, xi = t - P.r4ies;
+        Real zfacw = P.r5les / (xl * xl);
+        Real zcor = C(1.0) / (C(1.0) - P.retv * zfoeeliqt);
+        Real zdqsliqdt = zfacw * zcor * zqsliq;
+        zcorqsliq = C(1.0) + P.ralvdcp * zdqsliqdt;
+        Real zfaci = P.r5ies / (xi * xi);
+        zcor = C(1.0) / (C(1.0) - P.retv * zfoeew);
+        Real zdqsicedt = zfaci * zcor * zqsice;
+        zcorqsice = C(1.0) + P.ralsdcp * zdqsicedt;
+        Real zfac = alfa * zfacw + (C(1.0) - alfa) * zfaci;
+        zcor = C(1.0) / (C(1.0) - P.retv * zfoeewm);
+        zdqsmixdt = zfac * zcor * zqsmix;
+        Real foeldcpm = alfa * P.ralvdcp + (C(1.0) - alfa) * P.ralsdcp;
+        zcorqsmix = C(1.0) + foeldcpm * zdqsmixdt;
+        zevaplimmix = mx((zqsmix - qv) / zcorqsmix, C(0.0));
+      }
+      const Real ztmpa = C(1.0) / mx(a, C(0.01));
+      Real zliqcld = ql * ztmpa;
+      Real zicecld = qi * ztmpa;
+      const Real zlicld = zliqcld + zicecld;
+
+      // evaporate very small amounts (:1334-1342)
+      if (ql < P.rlmin) {
+        q.VL = double(ql);
+        q.LV = -double(ql);
+      }
+      if (qi < P.rlmin) {
+        q.VI = double(qi);
+        q.IV = -double(qi);
+      }
+
+      // 3.2 detrainment (:1362-1398)
+      if (!last) {
+        plude_k = plude_k * D(zdtgdp);
+        if (ldcum && Real(plude_k) > zepsec && plu_k1 > zepsec) {
+          solac = solac + Real(plude_k) / plu_k1;
+          convsrce_l = Real(pludeli1) * zdtgdp;
+          convsrce_i = Real(pludeli2) * zdtgdp;
+          QADD(LL, convsrce_l);
+          QADD(II, convsrce_i);
+        } else {
+          plude_k = 0.0;
+        }
+        if (P.lmfdsnow) {
+          convsrce_r = Real(ld(F.psnde + ok2s)) * zdtgdp;
+          convsrce_s = Real(ld(F.psnde + ok2s + s2)) * zdtgdp;
+          QADD(RR, convsrce_r);
+          QADD(SS, convsrce_s);
+        }
+        F.plude[ok] = plude_k;
+      }
+
+      // 3.3 subsidence source and evaporation (:1419-1492)
+      if (k > ncldtop0) {
+        Real zmf = mx(C(0.0), (pmfu_k * zadvw + pmfd_k * zadvwd) * zdtgdp);
+        Real zacust = zmf * zanewm1;
+        Real lcust_l = zmf * qxnm1_l;
+        Real lcust_i = zmf * qxnm1_i;
+        convsrce_l = convsrce_l + lcust_l;
+        convsrce_i = convsrce_i + lcust_i;
+        Real zdtdp = P.zrdcp * C(0.5) * (t_prev + t) / Real(paph_k);
+        Real zwtot = mn(P.rg * (pmfu_k * zadvw + pmfd_k * zadvwd), (pap_k - pap_prev) / rdt);
+        Real zdtforc = zdtdp * rdt * zwtot;
+        Real zdqs = zanewm1 * zdtforc * zdqsmixdt;
+        Real lfinalsum = C(0.0);
+        {
+          Real zlfinal = mx(C(0.0), lcust_l - zdqs);
+          Real zevap = mn((lcust_l - zlfinal), zevaplimmix);
+          zlfinal = lcust_l - zevap;
+          lfinalsum = lfinalsum + zlfinal;
+          QADD(LL, lcust_l);
+          QADD(VL, zevap);
+          QSUB(LV, zevap);
+        }
+        {
+          Real zlfinal = mx(C(0.0), lcust_i - zdqs);
+          Real zevap = mn((lcust_i - zlfinal), zevaplimmix);
+          zlfinal = lcust_i - zevap;
+          lfinalsum = lfinalsum + zlfinal;
+          QADD(II, lcust_i);
+          QADD(VI, zevap);
+          QSUB(IV, zevap);
+        }
+        solac = solac + zacust;
+        if (lfinalsum < zepsec) solac = solac - zacust;
+      }
+
+      // subsidence sink (:1499-1514)
+      if (!last) {
+        Real zmfdn = mx(C(0.0), (pmfu_k1 * zadvw + pmfd_k1 * zadvwd) * zdtgdp);
+        solab = solab + zmfdn;
+        qb_ll = qb_ll + zmfdn;
+        qb_ii = qb_ii + zmfdn;
+        convsink_l = zmfdn;
+        convsink_i = zmfdn;
+      }
+
+      // 3.4 erosion, ITURBEROSION=3 (:1689-1754)
+      {
+        Real zldifdt = P.rcldiff * rdt;
+        Real pl = Real(plude_k);
+        if (ktype >= 2 && pl > zepsec && peis < C(10.0)) {
+          zldifdt = C(20.0) * P.rcldiff_convi * zldifdt;
+        } else if (ktype == 1 && pl > zepsec) {
+          zldifdt = C(2.0) * P.rcldiff_convi * zldifdt;
+        }
+        if (zli > zepsec) {
+          Real zqe = (qv - a * zqsmix) / mx(zepsec, C(1.0) - a);
+          Real ze = mx(zqsmix - zqe, C(0.0));
+          Real zleros = C(0.333) * a * (C(1.) - a) * zldifdt * ze;
+          zleros = mn(zleros, zevaplimmix);
+          zleros = mn(zleros, zli);
+          Real zaeros = C(0.5) * zleros / zlicld;
+          solac = solac - zaeros;
+          QADD(VL, liqfrac * zleros);
+          QSUB(LV, liqfrac * zleros);
+          QADD(VI, icefrac * zleros);
+          QSUB(IV, icefrac * zleros);
+        }
+      }
+
+      // 4.1 fall speeds (:1783-1844), sedimentation (:1852-1877)
+      const Real fs_i = P.rvice, fs_s = P.rvsnow;
+      Real fs_r = C(0.0);
+      {
+        Real ztemp = C(0.5) * (qr + qxnm1_r);
+        if (ztemp != C(0.0)) {
+          Real zfallcorr = mpow<F32M>(P.rdensref / zrho, C(0.4));
+          Real zrlambda = mpow<F32M>(zrho * ztemp / P.rcl_lam1r, P.rcl_lam2r);
+          fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpow<F32M>(zrlambda, P.rcl_dr);
+        }
+      }
+      if (k > ncldtop0) {
+        fallsrce_i = pfplsx_i * zdtgdp;
+        QADD(II, fallsrce_i);
+        qxfg_i = qxfg_i + fallsrce_i;
+        qpretot = qpretot + qxfg_i;
+        fallsrce_r = pfplsx_r * zdtgdp;
+        QADD(RR, fallsrce_r);
+        qxfg_r = qxfg_r + fallsrce_r;
+        qpretot = qpretot + qxfg_r;
+        fallsrce_s = pfplsx_s * zdtgdp;
+        QADD(SS, fallsrce_s);
+        qxfg_s = qxfg_s + fallsrce_s;
+        qpretot = qpretot + qxfg_s;
+      }
+      const Real fallsink_i = zdtgdp * zrho * fs_i;
+      const Real fallsink_r = zdtgdp * zrho * fs_r;
+      const Real fallsink_s = zdtgdp * zrho * fs_s;
+
+      // 4.2 precipitation fraction (:1898-1919)
+      Real zcovpclr, zraincld, zraincldm1, zsnowcld;
+      if (qpretot > zepsec) {
+        zcovptot = C(1.0) - ((C(1.0) - zcovptot) * (C(1.0) - mx(a, za_prev)) /
+                             (C(1.0) - mn(za_prev, C(1.0) - C(1.E-06))));
+        zcovptot = mx(zcovptot, P.rcovpmin);
+        zcovpclr = mx(C(0.0), zcovptot - a);
+        zraincld = C(0.5) * (qr + qr_prev) / zcovptot;
+        zraincldm1 = C(0.5) * (qr + qxnm1_r) / zcovptot;
+        zsnowcld = C(0.5) * (qs + qs_prev) / zcovptot;
+        zcovpmax = mx(zcovptot, zcovpmax);
+      } else {
+        zraincld = C(0.0);
+        zraincldm1 = C(0.0);
+        zsnowcld = C(0.0);
+        zcovptot = C(0.0);
+        zcovpclr = C(0.0);
+        zcovpmax = C(0.0);
+      }
+
+      // 4.3 warm rain, IWARMRAIN=3, IRAINACC=1 (:1930-2259)
+      if (zliqcld > zepsec) {
+        Real zrainaut = P.rcl_inhomogaut * rdt * P.rcl_kkaau * mpow<F32M>(zliqcld, P.kkbauq_m1) * zconstpow;
+        qb_rl = qb_rl + zrainaut;
+        Real zrainacc = C(0.0);
+        if (zraincld > zepsec) {
+          zrainacc = P.rcl_inhomogacc * rdt * P.rcl_kkaac * mpow<F32M>(zliqcld, P.kkbac_m1) *
+                     mpow<F32M>(zraincld, P.rcl_kkbac);
+        }
+        qb_rl = qb_rl + zrainacc;
+      }
+
+      // 4.4 rain evaporation (:2271-2378)
+      {
+        Real zzrh = P.rprecrhmax + (C(1.0) - P.rprecrhmax) * zcovpmax / mx(zepsec, C(1.0) - a);
+        zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
+        Real zrhc = P.ramid;
+        Real zsigk = pap_k / Real(paph_surf);
+        if (zsigk > C(0.8)) {
+          Real s = (zsigk - C(0.8)) / C(0.2);
+          zrhc = P.ramid + (C(1.0) - P.ramid) * (s * s);
+        }
+        zzrh = mn(zrhc, zzrh);
+        zzrh = mn(C(0.9), zzrh);
+        Real zqe = mx(C(0.0), mn(qv, zqsliq));
+        if (zcovpclr > zepsec && zraincldm1 > zepsec && zqe < zzrh * zqsliq) {
+          Real zpreclr = zraincldm1;
+          Real zfallcorr = mpow<F32M>(P.rdensref / zrho, P.flt_0p4);
+          Real zesatliq = P.rv / P.rd * (P.r2es * el_e);
+          Real zlambda = mpow<F32M>(P.rcl_lam1r / (zrho * zpreclr), P.rcl_lam2r);
+          Real zevap_denom = P.rcl_cdenom1 * zesatliq - P.rcl_cdenom2 * t * zesatliq +
+                             P.rcl_cdenom3 * mpow<F32M>(t, C(3.0)) * pap_k;
+          Real zcorr2 = mpow<F32M>(t / C(273.), C(1.5)) * C(393.) / (t + C(120.));
+          Real zsubsat = mx(zzrh * zqsliq - zqe, C(0.0));
+          Real zbeta = (C(0.15) / zqsliq) * (t * t) * zesatliq * P.rcl_const1r * (zcorr2 / zevap_denom) *
+                       (C(0.78) / (mpow<F32M>(zlambda, P.rcl_const4r)) +
+                        P.rcl_const2r * mpow<F32M>(zrho * zfallcorr, C(0.5)) /
+                            (mpow<F32M>(zcorr2, C(0.5)) * mpow<F32M>(zlambda, P.rcl_const3r)));
+          Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
+          Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
+          Real zevap = mn(zdpevap, qxfg_r);
+          QADD(VR, zevap);
+          QSUB(RV, zevap);
+          qxfg_r = qxfg_r - zevap;
+        }
+      }
+
+      // 4.5 ice deposition, IDEPICE=1 (:2404-2499)
+      {
+        if (za_prev < P.rcldtopcf && a >= P.rcldtopcf) {
+          zcldtopdist = C(0.0);
+        } else {
+          zcldtopdist = zcldtopdist + zdp / (zrho * P.rg);
+        }
+        if (t < (P.rtt - C(5.)) && qxfg_l > P.rlmin) {
+          Real zsupersatice = (zqsliq - zqsice) / zqsice;
+          Real zvpice = (P.r2es * ei_e) * P.rv / P.rd;
+          Real zicenuclei = C(1000.0) * mexp<F32M>(C(12.96) * zsupersatice - C(0.639));
+          Real zadd = P.rlstt * (P.rlstt / (P.rv * t) - C(1.0)) / (C(2.4E-2) * t);
+          Real zbdd = P.rv * t * pap_k / (C(2.21) * zvpice);
+          Real zcvds = C(7.8) * mpow<F32M>(zicenuclei / zrho, C(0.666)) * zsupersatice / (C(8.87) * (zadd + zbdd));
+          Real zice0 = mx(zicecld, zicenuclei * P.riceinit / zrho);
+          Real zinew = mpow<F32M>(C(0.666) * zcvds * rdt + mpow<F32M>(zice0, C(0.666)), C(1.5));
+          Real zdepos = mx(P.rcl_overlapliqice * a * (zinew - zice0), C(0.0));
+          zdepos = mn(zdepos, qxfg_l);
+          Real zinfactor = mn(zicenuclei / C(15000.), C(1.0));
+          zdepos = zdepos * mn(zinfactor + (C(1.0) - zinfactor) *
+                                               (P.rdepliqrefrate + zcldtopdist / P.rdepliqrefdepth),
+                               C(1.0));
+          QADD(IL, zdepos);
+          QSUB(LI, zdepos);
+          qxfg_i = qxfg_i + zdepos;
+          qxfg_l = qxfg_l - zdepos;
+        }
+      }
+
+      // 4.7 snow deposition, IDEPSNOW=1 (:2698-2745)
+      {
+        Real zsupersatice = mx((qv - zqsmix) / zqsmix, C(0.0));
+        if (t < P.rtt && zsnowcld > zepsec && zsupersatice > C(0.0)) {
+          Real zvpice = (P.r2es * ei_e) * P.rv / P.rd;
+          Real zaplusb = P.rcl_apb1 * zvpice - P.rcl_apb2 * zvpice * t + pap_k * P.rcl_apb3 * (t * t * t);
+          Real zcorrfac = mpow<F32M>(C(1.0) / zrho, C(0.5));
+          Real zcorrfac2 = (mpow<F32M>(t / C(273.0), C(1.5))) * (C(393.0) / (t + C(120.0)));
+          Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
+          Real zterm1 = zsupersatice * (t * t) * zvpice * zcorrfac2 * P.rcl_const2s / (zrho * zaplusb);
+          Real zterm2 = C(0.65) * P.rcl_const6s * mpow<F32M>(zpr02, P.rcl_const4s) +
+                        P.rcl_const3s * mpow<F32M>(zcorrfac, C(0.5)) * mpow<F32M>(zrho, C(0.5)) *
+                            mpow<F32M>(zpr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
+          Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
+          zpsdep = mn(zpsdep, qv - zqsmix) / zcorqsmix;
+          QADD(SV, zpsdep);
+          QSUB(VS, zpsdep);
+        }
+      }
+
+      // revise in-cloud condensate (:2750-2754)
+      zliqcld = qxfg_l * ztmpa;
+      zicecld = qxfg_i * ztmpa;
+
+      // 4.8 ice -> snow autoconversion (:2769-2800)
+      if (t <= P.rtt && zicecld > zepsec) {
+        Real zzco = rdt * P.rsnowlin1 * mexp<F32M>(P.rsnowlin2 * (t - P.rtt));
+        Real r = zicecld / P.rlcritsnow;
+        Real ztemp = C(-1.) * (r * r);
+        Real zsnowaut = (ztemp < C(50.0)) ? zzco * (C(1.0) - mexp<F32M>(ztemp)) : zzco;
+        qb_si = qb_si + zsnowaut;
+      }
+
+      // 4.12 melting (:2815-2862)
+      {
+        Real zicetot = qxfg_i + qxfg_s;
+        Real zmeltmax = C(0.0);
+        if (zicetot > zepsec && t > P.rtt) {
+          Real zsubsat = mx(zqsice - qv, C(0.0));
+          Real ztdmtw0 = t - P.rtt -
+                         zsubsat * (C(1329.31) + C(0.0074615) * (pap_k - C(0.85E5)) - C(40.637) * (t - C(275.0)));
+          Real zcons1 = xabs(rdt * (C(1.0) + C(0.5) * ztdmtw0) / P.rtaumel);
+          zmeltmax = mx(ztdmtw0 * zcons1 * P.zrldcp, C(0.0));
+        }
+        if (zmeltmax > zepsec && zicetot > zepsec) {
+          Real zalfa = qxfg_i / zicetot;
+          Real zmelt = mn(qxfg_i, zalfa * zmeltmax);
+          qxfg_i = qxfg_i - zmelt;
+          qxfg_r = qxfg_r + zmelt;
+          QADD(RI, zmelt);
+          QSUB(IR, zmelt);
+          zalfa = qxfg_s / zicetot;
+          zmelt = mn(qxfg_s, zalfa * zmeltmax);
+          qxfg_s = qxfg_s - zmelt;
+          qxfg_r = qxfg_r + zmelt;
+          QADD(RS, zmelt);
+          QSUB(SR, zmelt);
+        }
+      }
+
+      // 4.13 rain freezing (:2877-2933)
+      if (qr > zepsec) {
+        if (t <= P.rtt && t_prev > P.rtt) {
+          Real zqpre = mx(qs + qr, zepsec);
+          prainfrac = qr / zqpre;
+          llrainliq = prainfrac > P.flt_0p8;
+        }
+        if (t < P.rtt) {
+          Real zfrzmax;
+          if (llrainliq) {
+            Real zlambda = mpow<F32M>(P.rcl_lam1r / (zrho * qr), P.rcl_lam2r);
+            Real ztemp = mn(P.rcl_fzrab * (t - P.rtt), C(50.));
+            Real zfrz = rdt * (P.rcl_const5r / zrho) * (mexp<F32M>(ztemp) - C(1.)) * mpow<F32M>(zlambda, P.rcl_const6r);
+            zfrzmax = mx(zfrz, C(0.0));
+          } else {
+            Real zcons1 = xabs(rdt * (C(1.0) + C(0.5) * (P.rtt - t)) / P.rtaumel);
+            zfrzmax = mx((P.rtt - t) * zcons1 * P.zrldcp, C(0.0));
+          }
+          if (zfrzmax > zepsec) {
+            Real zfrz = mn(qr, zfrzmax);
+            QADD(SR, zfrz);
+            QSUB(RS, zfrz);
+          }
+        }
+      }
+
+      // 4.14 homogeneous freezing of cloud liquid (:2948-2960)
+      {
+        Real zfrzmax = mx((P.rthomo - t) * P.zrldcp, C(0.0));
+        if (zfrzmax > zepsec && qxfg_l > zepsec) {
+          Real zfrz = mn(qxfg_l, zfrzmax);
+          QADD(IL, zfrz);
+          QSUB(LI, zfrz);
+        }
+      }
+
+      // 4.9 riming (:2973-3017)
+      if (t <= P.rtt && zliqcld > zepsec && zsnowcld > zepsec && zcovptot > C(0.01)) {
+        Real zfallcorr = mpow<F32M>(P.rdensref / zrho, P.flt_0p4);
+        Real zsnowrime = P.rcl_effrime * zcovptot * rdt * P.rcl_const7s * zfallcorr *
+                         mpow<F32M>(zrho * zsnowcld * P.rcl_const1s, P.rcl_const8s);
+        zsnowrime = mn(zsnowrime, C(1.0));
+        qb_sl = qb_sl + zsnowrime;
+      }
+
+      // PSD slopes (:3026-3069), PSACR (:3084-3115), PIACR (:3171-3198)
+      if (t <= P.rtt && prainfrac < zepsec && zraincld > zepsec) {
+        Real zlamr = mpow<F32M>(P.rcl_lam1r / (zrho * zraincld), P.rcl_lam2r);
+        Real zn0r = P.rcl_x1r * mpow<F32M>(zlamr, P.rcl_x2r);
+        Real zlamr3 = zlamr * zlamr * zlamr;
+        if (zsnowcld > zepsec) {
+          Real zlams = mpow<F32M>(P.rcl_lam1s / (zrho * zsnowcld), P.rcl_lam2s);
+          Real zn0s = P.rcl_x1s;
+          Real zfalldiff = mx(xabs(fs_r - fs_s), (fs_r + fs_s) / C(8.));
+          Real zfac = P.rpi * P.rpi * P.rdenswat * zrho * zn0r * zn0s / (zlams * zlamr3);
+          Real zrat = zlamr / zlams;
+          Real zpsacr =
+              zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
+          QADD(SR, zpsacr);
+          QSUB(RS, zpsacr);
+        }
+        if (zicecld > zepsec) {
+          Real zlami = mpow<F32M>(P.rcl_lam1s / (zrho * zicecld), P.rcl_lam2s);
+          Real zn0i = P.rcl_x1s;
+          Real zfalldiff = mx(xabs(fs_r - fs_i), (fs_r + fs_i) / C(8.));
+          Real zfac = P.rpi * P.rpi * P.rdenswat * C(0.1) * zrho * zn0r * zn0i / (zlami * zlamr3);
+          Real zrat = zlamr / zlami;
+          Real zpiacr =
+              zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
+          QADD(IR, zpiacr);
+          QSUB(RI, zpiacr);
+        }
+      }
+
+      // 4.15 snow sublimation, ISUBLSNOW=1 (:3254-3318)
+      {
+        Real zzrh = P.rprecrhmax + (C(1.0) - P.rprecrhmax) * zcovpmax / mx(zepsec, C(1.0) - a);
+        zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
+        Real zqe = (qv - a * zqsice) / mx(zepsec, C(1.0) - a);
+        zqe = mx(C(0.0), mn(zqe, zqsice));
+        if (zcovpclr > zepsec && qxfg_s > zepsec && zqe < zzrh * zqsice) {
+          Real aa = zcovptot * zdtgdp;
+          Real zpreclr = qxfg_s * zcovpclr / xsign(mx(xabs(aa), zepsilon), aa);
+          Real zbeta1 = xsqrt(pap_k / Real(paph_surf)) / P.rvrfactor * zpreclr / mx(zcovpclr, zepsec);
+          Real zbeta = P.rg * P.rpecons * mpow<F32M>(zbeta1, C(0.5777));
+          Real zdenom = C(1.0) + zbeta * rdt * zcorqsice;
+          Real zdpr = zcovpclr * zbeta * (zqsice - zqe) / zdenom * zdp * P.zrg_r;
+          Real zdpevap = zdpr * zdtgdp;
+          Real zevap = mn(zdpevap, qxfg_s);
+          QADD(VS, zevap);
+          QSUB(SV, zevap);
+          zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), (zcovptot - a) * zevap / qxfg_s));
+          qxfg_s = qxfg_s - zevap;
+        }
+      }
+
+      // evaporate small precipitation amounts (:3402-3412)
+      if (qxfg_i < P.rlmin) { QADD(VI, qxfg_i); QSUB(IV, qxfg_i); }
+      if (qxfg_r < P.rlmin) { QADD(VR, qxfg_r); QSUB(RV, qxfg_r); }
+      if (qxfg_s < P.rlmin) { QADD(VS, qxfg_s); QSUB(SV, qxfg_s); }
+#undef QADD
+#undef QSUB
+
+      // 5.1 cloud cover (:3429-3438)
+      D zda;
+      {
+        Real zanew = (a + solac) / (C(1.0) + solab);
+        zanew = mn(zanew, C(1.0));
+        if (zanew < P.ramin) zanew = C(0.0);
+        zda = D(zanew) - aorig;
+        zanewm1 = zanew;
+      }
+
+      // 5.2.1 sink truncation (:3455-3536), double
+      const double qx[5] = {double(ql), double(qi), double(qr), double(qs), double(qv)};
+      {
+        double ratio[5];
+        sink_ratios(q, qx, ratio);
+        double sr[5];
+        int ord[5];
+        sr[0] = ratio[0];
+        ord[0] = 0;
+#pragma unroll
+        for (int jm = 1; jm < 5; ++jm) {
+          const double rj = ratio[jm];
+          bool done = false;
+#pragma unroll
+          for (int jn = jm - 1; jn >= 0; --jn) {
+            if (!done) {
+              if (sr[jn] <= rj) {
+                sr[jn + 1] = rj;
+                ord[jn + 1] = jm;
+                done = true;
+              } else {
+                sr[jn + 1] = sr[jn];
+                ord[jn + 1] = ord[jn];
+              }
+            }
+          }
+          if (!done) {
+            sr[0] = rj;
+            ord[0] = jm;
+          }
+        }
+#pragma unroll
+        for (int jm = 0; jm < 5; ++jm) scale_row(ord[jm], q, qx);
+      }
+
+      // 5.2.2 solve (:3546-3628), double, lower-triangular form
+      double x_l, x_i, x_r, x_s, x_v;
+      {
+        x_l = qx[L] + (((0.0 + q.LL) + q.LI) + q.LV);
+        x_i = qx[I] + ((((0.0 + q.IL) + q.II) + q.IR) + q.IV);
+        x_r = qx[R] + ((((0.0 + q.RI) + q.RR) + q.RS) + q.RV);
+        x_s = qx[S] + (((0.0 + q.SR) + q.SS) + q.SV);
+        x_v = qx[V] + ((((0.0 + q.VL) + q.VI) + q.VR) + q.VS);
+        const double d_l = ((1.0 + 0.0) + double(qb_ll) + double(qb_rl)) + double(qb_sl);
+        const double d_i = ((1.0 + double(fallsink_i)) + double(qb_ii)) + double(qb_si);
+        const double d_r = 1.0 + double(fallsink_r);
+        const double d_s = 1.0 + double(fallsink_s);
+        const double m_rl = (-double(qb_rl)) / d_l;
+        const double m_sl = (-double(qb_sl)) / d_l;
+        const double m_si = (-double(qb_si)) / d_i;
+        x_r = x_r - m_rl * x_l;
+        x_s = x_s - m_sl * x_l;
+        x_s = x_s - m_si * x_i;
+        x_s = x_s / d_s;
+        x_r = x_r / d_r;
+        x_i = x_i / d_i;
+        x_l = x_l / d_l;
+        // clip (:3633-3640)
+        if (x_l < zepsecd) { x_v = x_v + x_l; x_l = 0.0; }
+        if (x_i < zepsecd) { x_v = x_v + x_i; x_i = 0.0; }
+        if (x_r < zepsecd) { x_v = x_v + x_r; x_r = 0.0; }
+        if (x_s < zepsecd) { x_v = x_v + x_s; x_s = 0.0; }
+      }
+      qxnm1_l = Real(x_l);
+      qxnm1_i = Real(x_i);
+      qxnm1_r = Real(x_r);
+      qxnm1_s = Real(x_s);
+      qxn2d_l = x_l; qxn2d_i = x_i; qxn2d_r = x_r; qxn2d_s = x_s;
+
+      // 5.3 fluxes to next level (:3658-3672)
+      pfplsx_i_n = Real(double(fallsink_i) * x_i * double(zrdtgdp));
+      pfplsx_r_n = Real(double(fallsink_r) * x_r * double(zrdtgdp));
+      pfplsx_s_n = Real(double(fallsink_s) * x_s * double(zrdtgdp));
+      if (pfplsx_s_n + pfplsx_r_n < zepsec) zcovptot = C(0.0);
+
+      // 6.1-6.3 tendencies (:3713-3769), double
+      {
+        D fq;
+        fq = D(convsrce_l) + 0.0 - (0.0 + D(convsink_l)) * x_l;
+        loc_t = loc_t + PD.ralvdcp * (x_l - D(ql) - fq) * zqtmst;
+        loc_cl = 0.0 + (x_l - q0_l) * zqtmst;
+        fq = D(convsrce_i) + D(fallsrce_i) - (D(fallsink_i) + D(convsink_i)) * x_i;
+        loc_t = loc_t + PD.ralsdcp * (x_i - D(qi) - fq) * zqtmst;
+        loc_ci = 0.0 + (x_i - q0_i) * zqtmst;
+        fq = D(convsrce_r) + D(fallsrce_r) - (D(fallsink_r) + 0.0) * x_r;
+        loc_t = loc_t + PD.ralvdcp * (x_r - D(qr) - fq) * zqtmst;
+        loc_cr = 0.0 + (x_r - q0_r) * zqtmst;
+        fq = D(convsrce_s) + D(fallsrce_s) - (D(fallsink_s) + 0.0) * x_s;
+        loc_t = loc_t + PD.ralsdcp * (x_s - D(qs) - fq) * zqtmst;
+        loc_cs = 0.0 + (x_s - q0_s) * zqtmst;
+        loc_q = loc_q + (x_v - D(qv)) * zqtmst;
+        loc_a = 0.0 + zda * zqtmst;
+      }
+      // 6.4 supersaturation check (:3765-3809), double
+      {
+        D q_upd = pq_k + dt * (loc_q + cml_q);
+        D t_upd = pt_k + dt * (loc_t + cml_t);
+        D a_upd = pa_k + dt * (loc_a + cml_a);
+        D t_adj, q_adj, a_adj, l_adj, i_adj;
+        supersatcheck(t_upd, q_upd, a_upd, pap_kd, t_adj, q_adj, a_adj, l_adj, i_adj);
+        loc_q = loc_q + q_adj * zqtmst;
+        loc_t = loc_t + t_adj * zqtmst;
+        loc_a = loc_a + a_adj * zqtmst;
+        loc_cl = loc_cl + l_adj * zqtmst;
+        loc_ci = loc_ci + i_adj * zqtmst;
+        D zl_adj = q0_l + loc_cl * dt;
+        if (zl_adj < -PD.rlmin) nwarn++;
+        if (zl_adj < 0.0) {
+          loc_cl = loc_cl - zl_adj * zqtmst;
+          loc_q = loc_q + zl_adj * zqtmst;
+          loc_t = loc_t - PD.ralvdcp * zl_adj * zqtmst;
+        }
+        D zi_adj = q0_i + loc_ci * dt;
+        if (zi_adj < -PD.rlmin) nwarn++;
+        if (zi_adj < 0.0) {
+          loc_ci = loc_ci - zi_adj * zqtmst;
+          loc_q = loc_q + zi_adj * zqtmst;
+          loc_t = loc_t - PD.ralsdcp * zi_adj * zqtmst;
+        }
+      }
+      covp_out = zcovptot;
+    }  // k >= ncldtop0
+
+    // ---------------- outputs of level k ----------------
+    F.loc_t[ok] = loc_t;
+    F.loc_q[ok] = loc_q;
+    F.loc_a[ok] = loc_a;
+    F.loc_cld[ok5] = loc_cl;
+    F.loc_cld[ok5 + s2] = loc_ci;
+    F.loc_cld[ok5 + 2 * s2] = loc_cr;
+    F.loc_cld[ok5 + 3 * s2] = loc_cs;
+    F.pcovptot[ok] = D(covp_out);
+
+    // precipitation fluxes at half level k (:4218-4224, 4297-4303)
+    {
+      const size_t oh = o2h + (size_t)k * np;
+      const D fl = D(pfplsx_r) + 0.0, fn = D(pfplsx_s) + D(pfplsx_i);
+      F.pfplsl[oh] = fl;
+      F.pfplsn[oh] = fn;
+      F.pfhpsl[oh] = -PD.rlvtt * fl;
+      F.pfhpsn[oh] = -PD.rlstt * fn;
+    }
+    // DDH flux recurrences to half level k+1 (:4244-4292)
+    {
+      const size_t oh1 = o2h + (size_t)(k + 1) * np;
+      const D zgdph_r = -PD.zrg_r * (paph_k1 - paph_k) * zqtmst;
+      const D sqrf = fsqlf + (qxn2d_r - q0_r) * zgdph_r;
+      const D cqrng = fcqlng + lneg_r * zgdph_r;
+      const D sqsf = fsqif + (qxn2d_s - q0_s) * zgdph_r;
+      const D cqsng = fcqnng + lneg_s * zgdph_r;
+      fsqlf = fsqlf + (qxn2d_l - q0_l + pvfl * dt) * zgdph_r + pludeli1;
+      fcqlng = fcqlng + lneg_l * zgdph_r;
+      fsqltur = fsqltur + pvfl * dt * zgdph_r;
+      fsqif = fsqif + (qxn2d_i - q0_i + pvfi * dt) * zgdph_r + pludeli2;
+      fcqnng = fcqnng + lneg_i * zgdph_r;
+      fsqitur = fsqitur + pvfi * dt * zgdph_r;
+      F.pfsqlf[oh1] = fsqlf;
+      F.pfsqif[oh1] = fsqif;
+      F.pfsqrf[oh1] = sqrf;
+      F.pfsqsf[oh1] = sqsf;
+      F.pfcqlng[oh1] = fcqlng;
+      F.pfcqnng[oh1] = fcqnng;
+      F.pfcqrng[oh1] = cqrng;
+      F.pfcqsng[oh1] = cqsng;
+      F.pfsqltur[oh1] = fsqltur;
+      F.pfsqitur[oh1] = fsqitur;
+    }
+
+    // carry to level k+1
+    za_prev = a;
+    qr_prev = qr;
+    qs_prev = qs;
+    t_prev = t;
+    pap_prev = pap_k;
+    paph_k = paph_k1;
+    pmfu_k = pmfu_k1;
+    pmfd_k = pmfd_k1;
+    pfplsx_i = pfplsx_i_n;
+    pfplsx_r = pfplsx_r_n;
+    pfplsx_s = pfplsx_s_n;
+  }
+  // precipitation fluxes at the surface half level KLEV+1
+  {
+    const size_t oh = o2h + (size_t)klev * np;
+    const D fl = D(pfplsx_r) + 0.0, fn = D(pfplsx_s) + D(pfplsx_i);
+    F.pfplsl[oh] = fl;
+    F.pfplsn[oh] = fn;
+    F.pfhpsl[oh] = -PD.rlvtt * fl;
+    F.pfhpsn[oh] = -PD.rlstt * fn;
+  }
+  F.prainfrac_toprfz[o1] = D(prainfrac);
+  if (nwarn && F.ncounters) atomic_add(F.ncounters, nwarn);
+#undef C
+}
+
+}  // namespace cloudsc

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 #include "cloudsc_common.cuh"
+#include "plibm.h"
 
 namespace cloudsc {
 cudaError_t upload_params(const cloudsc_params &p, const Derived &d);
@@ -57,8 +58,10 @@ bool params_supported(const cloudsc_params &p) {
 
 Derived make_derived(const cloudsc_params &p) {
   Derived d;
-  d.zconst_pow_land = std::pow(p.rcl_kk_cloud_num_land, p.rcl_kkbaun);
-  d.zconst_pow_sea = std::pow(p.rcl_kk_cloud_num_sea, p.rcl_kkbaun);
+  // ZCONST**RCL_KKBAUN (cloudsc.F90:2179-2181) takes one of two values; it is
+  // evaluated once here with the kernels' own pow.
+  d.zconst_pow_land = plibm_pow(p.rcl_kk_cloud_num_land, p.rcl_kkbaun);
+  d.zconst_pow_sea = plibm_pow(p.rcl_kk_cloud_num_sea, p.rcl_kkbaun);
   d.flt_0p4 = (double)0.4f;
   d.flt_0p8 = (double)0.8f;
   return d;

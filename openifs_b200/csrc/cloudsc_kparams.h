@@ -1,0 +1,50 @@
+// Host-side conversion of cloudsc_params into the kernels' constant blocks.
+#pragma once
+#include "cloudsc_column.cuh"
+
+namespace cloudsc {
+
+template <typename Real>
+inline void fill_kparams(const cloudsc_params &p, const Derived &d, KParams<Real> &k) {
+#define F_(n) k.n = Real(p.n)
+  F_(rg); F_(rd); F_(rv); F_(retv); F_(rtt); F_(rlvtt); F_(rlstt); F_(rpi);
+  F_(r2es); F_(r3les); F_(r3ies); F_(r4les); F_(r4ies); F_(r5les); F_(r5ies); F_(r5alvcp); F_(r5alscp);
+  F_(ralvdcp); F_(ralsdcp); F_(rtwat); F_(rtice); F_(rtwat_rtice_r); F_(rkoop1); F_(rkoop2);
+  F_(ramid); F_(ramin); F_(rlmin); F_(rcldiff); F_(rcldiff_convi); F_(rcovpmin); F_(rprecrhmax); F_(rpecons);
+  F_(rvrfactor); F_(rtaumel); F_(rssicefactor); F_(rsnowlin1); F_(rsnowlin2); F_(rlcritsnow); F_(rthomo);
+  F_(rvice); F_(rvsnow); F_(rxfallspeedrain); F_(rcldtopcf); F_(rdepliqrefrate); F_(rdepliqrefdepth);
+  F_(riceinit); F_(rdensref); F_(rdenswat); F_(rcl_overlapliqice); F_(rcl_effrime);
+  F_(rcl_inhomogaut); F_(rcl_inhomogacc); F_(rcl_kkaac); F_(rcl_kkbac); F_(rcl_kkaau); F_(rcl_kkbauq);
+  F_(rcl_dr); F_(rcl_x1r); F_(rcl_x2r); F_(rcl_lam1r); F_(rcl_lam2r);
+  F_(rcl_const1r); F_(rcl_const2r); F_(rcl_const3r); F_(rcl_const4r); F_(rcl_const5r); F_(rcl_const6r);
+  F_(rcl_const7r); F_(rcl_cdenom1); F_(rcl_cdenom2); F_(rcl_cdenom3); F_(rcl_fzrab);
+  F_(rcl_x1s); F_(rcl_lam1s); F_(rcl_lam2s);
+  F_(rcl_const1s); F_(rcl_const2s); F_(rcl_const3s); F_(rcl_const4s); F_(rcl_const5s); F_(rcl_const6s);
+  F_(rcl_const7s); F_(rcl_const8s);
+  F_(rcl_apb1); F_(rcl_apb2); F_(rcl_apb3);
+  F_(rmfadvw); F_(rmfadvwdd);
+#undef F_
+  k.zrdcp = Real(p.rd / p.rcpd);
+  k.zrg_r = Real(1.0 / p.rg);
+  k.zrldcp = Real(1.0 / (p.ralsdcp - p.ralvdcp));
+  k.zconst_pow_land = Real(d.zconst_pow_land);
+  k.zconst_pow_sea = Real(d.zconst_pow_sea);
+  k.flt_0p4 = Real(d.flt_0p4);
+  k.flt_0p8 = Real(d.flt_0p8);
+  k.kkbauq_m1 = Real(p.rcl_kkbauq - 1.0);
+  k.kkbac_m1 = Real(p.rcl_kkbac - 1.0);
+  k.ncldtop = p.ncldtop;
+  k.lmfdsnow = p.lmfdsnow;
+}
+
+
+inline void fill_kparams_d(const cloudsc_params &p, KParamsD &dd) {
+  dd.rg = p.rg; dd.retv = p.retv; dd.rtt = p.rtt; dd.rtice = p.rtice; dd.rtwat = p.rtwat;
+  dd.rtwat_rtice_r = p.rtwat_rtice_r; dd.r2es = p.r2es; dd.r3les = p.r3les; dd.r3ies = p.r3ies;
+  dd.r4les = p.r4les; dd.r4ies = p.r4ies; dd.r5alvcp = p.r5alvcp; dd.r5alscp = p.r5alscp;
+  dd.ralvdcp = p.ralvdcp; dd.ralsdcp = p.ralsdcp; dd.rkoop1 = p.rkoop1; dd.rkoop2 = p.rkoop2;
+  dd.rssicefactor = p.rssicefactor; dd.rlmin = p.rlmin; dd.rlvtt = p.rlvtt; dd.rlstt = p.rlstt;
+  dd.zrg_r = 1.0 / p.rg;
+}
+
+}  // namespace cloudsc

@@ -30,6 +30,19 @@
 #endif
 #include "oracle.h"
 
+/*
+ * libm: the reference's results depend on the last bit of EXP and ** (see
+ * plibm.h).  The default build uses the system libm (glibc), i.e. the
+ * reference as a gfortran build on Linux would run it; built with
+ * -DORACLE_PLIBM it uses the portable exp/pow of plibm.h, the libm the B200
+ * kernels use, so that the comparison isolates the kernels' logic.
+ */
+#ifdef ORACLE_PLIBM
+#include "../openifs_b200/csrc/plibm.h"
+#define exp(x) plibm_exp(x)
+#define pow(x, y) plibm_pow(x, y)
+#endif
+
 #define NCLV 5
 #define NCLDQL 1
 #define NCLDQI 2

@@ -13,25 +13,28 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "liboracle_cloudsc.so")
-_lib = None
+LIB_PATHS = {"glibc": os.path.join(_HERE, "liboracle_cloudsc.so"),
+             "plibm": os.path.join(_HERE, "liboracle_cloudsc_plibm.so")}
+_libs = {}
 
 
 def build():
     r = subprocess.run(["make", "-s", "-C", _HERE], capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
-    return LIB_PATH
+    return LIB_PATHS
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
+def lib(libm="glibc"):
+    """The oracle linked against the system libm ("glibc", the reference as a
+    gfortran/Linux build runs it) or against plibm.h ("plibm", the libm of
+    the B200 kernels)."""
+    if libm not in _libs:
+        if not os.path.exists(LIB_PATHS[libm]):
             build()
         from openifs_b200.params import CloudscParams
         from openifs_b200.fields import BATCHED_FIELDS
-        L = ctypes.CDLL(LIB_PATH)
+        L = ctypes.CDLL(LIB_PATHS[libm])
         P = ctypes.POINTER(CloudscParams)
         vp = ctypes.c_void_p
         i32 = ctypes.c_int
@@ -42,8 +45,8 @@ def lib():
         L.oracle_cloudsc_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
                                              [vp] * len(BATCHED_FIELDS) + [i32])
         L.oracle_cloudsc_batched.restype = i32
-        _lib = L
-    return _lib
+        _libs[libm] = L
+    return _libs[libm]
 
 
 def params_default(tsphy, ncldtop):
@@ -59,7 +62,7 @@ def gamma(x):
     return lib().oracle_fcgeneralized_gamma(float(x))
 
 
-def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthreads=0):
+def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthreads=0, libm="glibc"):
     """Run the oracle over all blocks of ``arrays`` (numpy, fields layout), in
     place.  Returns the number of negative-condensate warning events."""
     from openifs_b200.fields import BATCHED_FIELDS
@@ -69,7 +72,7 @@ def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthre
         if not (isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"]):
             raise ValueError(f"{n}: need a C-contiguous numpy array")
         ptrs.append(a.ctypes.data)
-    rc = lib().oracle_cloudsc_batched(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
+    rc = lib(libm).oracle_cloudsc_batched(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
                                       int(ngptot), float(ptsphy), *ptrs, int(nthreads))
     if rc < 0:
         raise RuntimeError(f"oracle_cloudsc_batched returned {rc}")

@@ -1,0 +1,85 @@
+// TEST INFRASTRUCTURE ONLY -- not part of the product library.
+//
+// The GPU kernels' per-column code (openifs_b200/csrc/cloudsc_body.cuh),
+// compiled unchanged for the host with no FMA contraction.  Double precision
+// uses plibm.h's exp/pow, exactly as on the GPU; compiled with
+// -DHOSTEMU_GLIBC the double-precision exp/pow are glibc's instead.  The tests
+// compare it with the oracle built against the same libm: a bit-for-bit match
+// proves that the kernel's logic (its fused single pass, sparse 5x5 matrices,
+// operation order) restates the reference exactly.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#define CSC_DEV inline
+#include "../../openifs_b200/csrc/cloudsc_column.cuh"
+#include "../../openifs_b200/csrc/cloudsc_kparams.h"
+
+namespace cloudsc {
+static KParams<double> c_kpd;
+static KParams<float> c_kpf;
+static KParamsD c_kd;
+template <typename Real>
+inline const KParams<Real> &KP();
+template <>
+inline const KParams<double> &KP<double>() { return c_kpd; }
+template <>
+inline const KParams<float> &KP<float>() { return c_kpf; }
+template <typename T>
+inline T ld(const T *p) { return *p; }
+inline void atomic_add(uint32_t *p, uint32_t v) { *p += v; }
+inline double xabs(double x) { return std::fabs(x); }
+inline float xabs(float x) { return std::fabs(x); }
+inline double xsign(double a, double b) { return std::copysign(a, b); }
+inline float xsign(float a, float b) { return std::copysign(a, b); }
+}  // namespace cloudsc
+
+#include "../../openifs_b200/csrc/cloudsc_body.cuh"
+
+using namespace cloudsc;
+
+extern "C" int hostemu_batched(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+                               double ptsphy, void **a, int precision) {
+  Derived d;
+#ifdef CLOUDSC_HOST_LIBM_GLIBC
+  d.zconst_pow_land = std::pow(p->rcl_kk_cloud_num_land, p->rcl_kkbaun);
+  d.zconst_pow_sea = std::pow(p->rcl_kk_cloud_num_sea, p->rcl_kkbaun);
+#else
+  d.zconst_pow_land = plibm_pow(p->rcl_kk_cloud_num_land, p->rcl_kkbaun);
+  d.zconst_pow_sea = plibm_pow(p->rcl_kk_cloud_num_sea, p->rcl_kkbaun);
+#endif
+  d.flt_0p4 = (double)0.4f;
+  d.flt_0p8 = (double)0.8f;
+  fill_kparams(*p, d, c_kpd);
+  fill_kparams(*p, d, c_kpf);
+  fill_kparams_d(*p, c_kd);
+  uint32_t nwarn = 0;
+  Fields f;
+  f.pt = (const double *)a[0]; f.pq = (const double *)a[1]; f.cml_t = (const double *)a[2];
+  f.cml_q = (const double *)a[3]; f.cml_a = (const double *)a[4]; f.cml_cld = (const double *)a[5];
+  f.loc_t = (double *)a[6]; f.loc_q = (double *)a[7]; f.loc_a = (double *)a[8]; f.loc_cld = (double *)a[9];
+  f.pvfl = (const double *)a[10]; f.pvfi = (const double *)a[11]; f.pap = (const double *)a[12];
+  f.paph = (const double *)a[13]; f.plsm = (const double *)a[14]; f.ldcum = (const int32_t *)a[15];
+  f.ktype = (const int32_t *)a[16]; f.peis = (const double *)a[17]; f.plu = (const double *)a[18];
+  f.plude = (double *)a[19]; f.pludeli = (const double *)a[20]; f.psnde = (const double *)a[21];
+  f.pmfu = (const double *)a[22]; f.pmfd = (const double *)a[23]; f.pa = (const double *)a[24];
+  f.pclv = (const double *)a[25]; f.pcovptot = (double *)a[26]; f.prainfrac_toprfz = (double *)a[27];
+  f.pfsqlf = (double *)a[28]; f.pfsqif = (double *)a[29]; f.pfcqnng = (double *)a[30];
+  f.pfcqlng = (double *)a[31]; f.pfsqrf = (double *)a[32]; f.pfsqsf = (double *)a[33];
+  f.pfcqrng = (double *)a[34]; f.pfcqsng = (double *)a[35]; f.pfsqltur = (double *)a[36];
+  f.pfsqitur = (double *)a[37]; f.pfplsl = (double *)a[38]; f.pfplsn = (double *)a[39];
+  f.pfhpsl = (double *)a[40]; f.pfhpsn = (double *)a[41];
+  f.ncounters = &nwarn;
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
+  for (int ib = 0; ib < ngpblks; ++ib) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    for (int jl = 0; jl < icend; ++jl) {
+      if (precision == 0)
+        cloudsc_column<double, false>(f, sh, ib, jl);
+      else
+        cloudsc_column<double, true>(f, sh, ib, jl);
+    }
+  }
+  return (int)nwarn;
+}

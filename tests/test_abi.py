@@ -1,0 +1,87 @@
+"""The C-ABI library loads without a GPU, exports every function declared in
+include/cloudsc_b200.h, agrees with the Python struct mirror, and reports
+argument errors with CLOUDSC's error codes (checked before any device work)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from openifs_b200 import cloudsc, fields, inputs
+from openifs_b200.params import CloudscParams
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "cloudsc_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(cloudsc_b200_\w+)\s*\(", txt)))
+
+
+def test_exports_every_declared_symbol(built):
+    lib = cloudsc.lib()
+    names = _declared()
+    assert len(names) >= 9
+    for n in names:
+        assert hasattr(lib, n), n
+
+
+def test_struct_size_matches(built):
+    assert ctypes.sizeof(CloudscParams) == cloudsc.lib().cloudsc_b200_params_size()
+
+
+def test_version(built):
+    assert b"sm_100a" in cloudsc.lib().cloudsc_b200_version()
+
+
+def test_error_codes_without_device_work(built):
+    p = cloudsc.default_params()
+    try:
+        cloudsc.setup(p)  # on a CPU-only host this fails at the upload (-4) but keeps p
+    except cloudsc.CloudscError as e:
+        assert e.code == -4
+    arrs = {n: None for n, *_ in fields.BATCHED_FIELDS}
+    # a NULL array
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc.cloudsc_batched(p, {**arrs, **{n: np.zeros(1) for n in fields.INPUT_NAMES}},
+                                32, 137, 2, 64, 3600.0)
+    assert e.value.code == -1
+    full = {n: np.zeros(1) for n, *_ in fields.BATCHED_FIELDS}
+    # NGPTOT inconsistent with NPROMA*NGPBLKS
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc.cloudsc_batched(p, full, 32, 137, 2, 65, 3600.0)
+    assert e.value.code == -2
+    # KLEV smaller than NCLDTOP
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc.cloudsc_batched(p, full, 32, 10, 2, 64, 3600.0)
+    assert e.value.code == -2
+    # parameters that differ from the uploaded ones
+    q = p.copy()
+    q.ramid = 0.9
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc.cloudsc_batched(q, full, 32, 137, 2, 64, 3600.0)
+    assert e.value.code == -5
+    # bad launch shape
+    with pytest.raises(cloudsc.CloudscError):
+        cloudsc.set_launch(0, 48, 0)
+
+
+def test_block_entry_argument_checks(built):
+    p = cloudsc.default_params()
+    try:
+        cloudsc.setup(p)
+    except cloudsc.CloudscError:
+        pass
+    with pytest.raises(cloudsc.CloudscError) as e:  # KFDIA > KLON
+        cloudsc.cloudsc_block(p, 1, 40, 32, 137, 3600.0, {})
+    assert e.value.code == -2
+    with pytest.raises(cloudsc.CloudscError) as e:  # missing required arrays
+        cloudsc.cloudsc_block(p, 1, 32, 32, 137, 3600.0, {})
+    assert e.value.code == -1
+
+
+def test_bytes_per_column():
+    rb, wb = fields.bytes_per_column()
+    assert (rb, wb) == (28528, 25328)

@@ -1,0 +1,64 @@
+"""The GPU kernels' column code, compiled for the host (tests/hostemu), against
+the oracle: bit-for-bit with either libm, on the metric's configuration 1 and
+on the edge cases.  This proves the kernel's restatement of the reference's
+logic (single fused pass over the levels, sparse 5x5 matrices, operation
+order) without a GPU; the GPU tests then show the device build matches the
+host build."""
+import numpy as np
+import pytest
+
+from openifs_b200 import inputs
+from tests import util
+
+
+@pytest.fixture(scope="module")
+def pp(built):
+    return util.params()
+
+
+@pytest.mark.parametrize("libm", ["plibm", "glibc"])
+def test_config1_bit_exact(pp, libm):
+    p, po = pp
+    arrs = inputs.generate(100, 32, p, seed=1)
+    ref, nw = util.run_oracle(po, arrs, 32, 100, 3200, libm=libm)
+    emu, nwe = util.run_hostemu(p, arrs, 32, 100, 3200, libm=libm)
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), n
+    assert nw == nwe
+
+
+@pytest.mark.parametrize("case", util.EDGE_CASES)
+def test_edge_cases_bit_exact(pp, case):
+    p, po = pp
+    arrs = util.apply_case(inputs.generate(4, 37, p, seed=5), case)
+    ngptot = 4 * 37 - 6
+    ref, _ = util.run_oracle(po, arrs, 37, 4, ngptot)
+    emu, _ = util.run_hostemu(p, arrs, 37, 4, ngptot)
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), (case, n)
+
+
+def test_libm_sensitivity_of_the_reference(pp):
+    """The reference algorithm with two correct libms (glibc and plibm, within
+    1 ulp of each other) -- the spread any GPU build is measured against."""
+    p, po = pp
+    arrs = inputs.generate(100, 32, p, seed=1)
+    a, _ = util.run_oracle(po, arrs, 32, 100, 3200, libm="plibm")
+    b, _ = util.run_oracle(po, arrs, 32, 100, 3200, libm="glibc")
+    rep, _ = util.compare(a, b)
+    assert max(rep.values()) < 1e-8
+    assert max(rep.values()) > 1e-14  # the libms do differ
+
+
+def test_mixed_form_on_host(pp):
+    """The FP32-mixed column code (host build, glibc float libm) against the
+    FP64 oracle: species, T and surface-flux tendencies within 1e-5
+    (max |err| / max |ref| per field)."""
+    p, po = pp
+    arrs = inputs.generate(100, 32, p, seed=1)
+    ref, _ = util.run_oracle(po, arrs, 32, 100, 3200)
+    emu, _ = util.run_hostemu(p, arrs, 32, 100, 3200, precision=1)
+    st = util.mixed_error_stats(emu, ref)
+    for k in util.MIXED_BOUNDED:
+        assert st[k]["normwise_max"] <= util.MIXED_TOL, (k, st[k])
+    assert np.isfinite(st["tendency_loc_a"]["normwise_max"])
