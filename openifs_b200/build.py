@@ -20,8 +20,11 @@ LIB = os.path.join(HERE, "libcloudsc_b200.so")
 STAMP = os.path.join(HERE, ".libcloudsc_b200.stamp")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# --fmad=false (device) and -ffp-contract=off (host): no multiply-add
+# contraction anywhere, so the kernels, the host-side constant set-up and
+# plibm.h evaluate exactly the operations written.
 NVCC_FLAGS = ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC",
-              "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
+              "-Xcompiler", "-O2", "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr"]
 
 
 def _nvcc():

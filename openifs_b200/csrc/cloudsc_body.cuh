@@ -343,6 +343,8 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
       const Real zdp = Real(paph_k1 - paph_k);
       const Real zgdp = P.rg / zdp;
       const Real zrho = pap_k / (P.rd * t);
+      // (RDENSREF/ZRHO)**0.4 appears in three processes: one shared logarithm
+      const PowBase b_dens = mbase<F32M>(P.rdensref / zrho);
       const Real zdtgdp = rdt * zgdp;
       const Real zrdtgdp = zdp * zrdtgdp_f;
       Real zcorqsliq, zcorqsice, zcorqsmix, zdqsmixdt, zevaplimmix;
@@ -474,7 +476,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
       {
         Real ztemp = C(0.5) * (qr + qxnm1_r);
         if (ztemp != C(0.0)) {
-          Real zfallcorr = mpow<F32M>(P.rdensref / zrho, C(0.4));
+          Real zfallcorr = mpowb<F32M>(b_dens, C(0.4));
           Real zrlambda = mpow<F32M>(zrho * ztemp / P.rcl_lam1r, P.rcl_lam2r);
           fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpow<F32M>(zrlambda, P.rcl_dr);
         }
@@ -519,11 +521,12 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
 
       // 4.3 warm rain, IWARMRAIN=3, IRAINACC=1 (:1930-2259)
       if (zliqcld > zepsec) {
-        Real zrainaut = P.rcl_inhomogaut * rdt * P.rcl_kkaau * mpow<F32M>(zliqcld, P.kkbauq_m1) * zconstpow;
+        const PowBase b_liq = mbase<F32M>(zliqcld);
+        Real zrainaut = P.rcl_inhomogaut * rdt * P.rcl_kkaau * mpowb<F32M>(b_liq, P.kkbauq_m1) * zconstpow;
         qb_rl = qb_rl + zrainaut;
         Real zrainacc = C(0.0);
         if (zraincld > zepsec) {
-          zrainacc = P.rcl_inhomogacc * rdt * P.rcl_kkaac * mpow<F32M>(zliqcld, P.kkbac_m1) *
+          zrainacc = P.rcl_inhomogacc * rdt * P.rcl_kkaac * mpowb<F32M>(b_liq, P.kkbac_m1) *
                      mpow<F32M>(zraincld, P.rcl_kkbac);
         }
         qb_rl = qb_rl + zrainacc;
@@ -544,17 +547,18 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
         Real zqe = mx(C(0.0), mn(qv, zqsliq));
         if (zcovpclr > zepsec && zraincldm1 > zepsec && zqe < zzrh * zqsliq) {
           Real zpreclr = zraincldm1;
-          Real zfallcorr = mpow<F32M>(P.rdensref / zrho, P.flt_0p4);
+          Real zfallcorr = mpowb<F32M>(b_dens, P.flt_0p4);
           Real zesatliq = P.rv / P.rd * (P.r2es * el_e);
           Real zlambda = mpow<F32M>(P.rcl_lam1r / (zrho * zpreclr), P.rcl_lam2r);
+          const PowBase b_lam = mbase<F32M>(zlambda);
           Real zevap_denom = P.rcl_cdenom1 * zesatliq - P.rcl_cdenom2 * t * zesatliq +
                              P.rcl_cdenom3 * mpow<F32M>(t, C(3.0)) * pap_k;
           Real zcorr2 = mpow<F32M>(t / C(273.), C(1.5)) * C(393.) / (t + C(120.));
           Real zsubsat = mx(zzrh * zqsliq - zqe, C(0.0));
           Real zbeta = (C(0.15) / zqsliq) * (t * t) * zesatliq * P.rcl_const1r * (zcorr2 / zevap_denom) *
-                       (C(0.78) / (mpow<F32M>(zlambda, P.rcl_const4r)) +
+                       (C(0.78) / (mpowb<F32M>(b_lam, P.rcl_const4r)) +
                         P.rcl_const2r * mpow<F32M>(zrho * zfallcorr, C(0.5)) /
-                            (mpow<F32M>(zcorr2, C(0.5)) * mpow<F32M>(zlambda, P.rcl_const3r)));
+                            (mpow<F32M>(zcorr2, C(0.5)) * mpowb<F32M>(b_lam, P.rcl_const3r)));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
           Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
           Real zevap = mn(zdpevap, qxfg_r);
@@ -602,10 +606,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           Real zcorrfac = mpow<F32M>(C(1.0) / zrho, C(0.5));
           Real zcorrfac2 = (mpow<F32M>(t / C(273.0), C(1.5))) * (C(393.0) / (t + C(120.0)));
           Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
+          const PowBase b_pr02 = mbase<F32M>(zpr02);
           Real zterm1 = zsupersatice * (t * t) * zvpice * zcorrfac2 * P.rcl_const2s / (zrho * zaplusb);
-          Real zterm2 = C(0.65) * P.rcl_const6s * mpow<F32M>(zpr02, P.rcl_const4s) +
+          Real zterm2 = C(0.65) * P.rcl_const6s * mpowb<F32M>(b_pr02, P.rcl_const4s) +
                         P.rcl_const3s * mpow<F32M>(zcorrfac, C(0.5)) * mpow<F32M>(zrho, C(0.5)) *
-                            mpow<F32M>(zpr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
+                            mpowb<F32M>(b_pr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
           Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
           zpsdep = mn(zpsdep, qv - zqsmix) / zcorqsmix;
           QADD(SV, zpsdep);
@@ -691,7 +696,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
 
       // 4.9 riming (:2973-3017)
       if (t <= P.rtt && zliqcld > zepsec && zsnowcld > zepsec && zcovptot > C(0.01)) {
-        Real zfallcorr = mpow<F32M>(P.rdensref / zrho, P.flt_0p4);
+        Real zfallcorr = mpowb<F32M>(b_dens, P.flt_0p4);
         Real zsnowrime = P.rcl_effrime * zcovptot * rdt * P.rcl_const7s * zfallcorr *
                          mpow<F32M>(zrho * zsnowcld * P.rcl_const1s, P.rcl_const8s);
         zsnowrime = mn(zsnowrime, C(1.0));

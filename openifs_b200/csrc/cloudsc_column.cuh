@@ -81,6 +81,33 @@ CSC_DEV double mpow(double x, double y) {
   if (F32) return (double)powf((float)x, (float)y);
   return xpow(x, y);
 }
+
+// A pow base whose logarithm several calls share (FP64: plibm's double-double
+// ln, computed once; FP32-mixed: nothing is precomputed).  mpowb(b, y) equals
+// mpow(b.x, y) exactly.
+struct PowBase {
+  double x, lhi, llo;
+};
+template <bool F32>
+CSC_DEV PowBase mbase(double x) {
+  PowBase b;
+  b.x = x;
+  b.lhi = 0.0;
+  b.llo = 0.0;
+#if !(defined(CLOUDSC_HOST_LIBM_GLIBC) && !defined(__CUDA_ARCH__))
+  if (!F32) plibm_log_base(x, &b.lhi, &b.llo);
+#endif
+  return b;
+}
+template <bool F32>
+CSC_DEV double mpowb(const PowBase &b, double y) {
+  if (F32) return (double)powf((float)b.x, (float)y);
+#if defined(CLOUDSC_HOST_LIBM_GLIBC) && !defined(__CUDA_ARCH__)
+  return pow(b.x, y);
+#else
+  return plibm_pow_with_log(b.x, y, b.lhi, b.llo);
+#endif
+}
 CSC_DEV float xpow(float x, float y) { return powf(x, y); }
 CSC_DEV double xsqrt(double x) { return sqrt(x); }
 CSC_DEV float xsqrt(float x) { return sqrtf(x); }

@@ -74,13 +74,22 @@ cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
   return e;
 }
 
+// Register budget: __launch_bounds__(CLOUDSC_MAXT, CLOUDSC_MINB).
+#ifndef CLOUDSC_MAXT
+#define CLOUDSC_MAXT 256
+#endif
+#ifndef CLOUDSC_MINB
+#define CLOUDSC_MINB 1
+#endif
+
 // Launch the kernel: precision 0 = FP64, 1 = FP32-mixed.
 cudaError_t launch(int precision, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream) {
+  if (threads > CLOUDSC_MAXT) return cudaErrorInvalidConfiguration;
   if (precision == 0) {
-    cloudsc_kernel<false, 256, 1><<<grid, threads, 0, stream>>>(f, sh);
+    cloudsc_kernel<false, CLOUDSC_MAXT, CLOUDSC_MINB><<<grid, threads, 0, stream>>>(f, sh);
   } else {
-    cloudsc_kernel<true, 256, 1><<<grid, threads, 0, stream>>>(f, sh);
+    cloudsc_kernel<true, CLOUDSC_MAXT, CLOUDSC_MINB><<<grid, threads, 0, stream>>>(f, sh);
   }
   return cudaGetLastError();
 }

@@ -7,26 +7,31 @@
  * 1-EXP(x) with |x| tiny).  Two correct libms that differ by one or two ulp
  * (glibc vs CUDA, or glibc vs Intel's libimf) therefore give CLOUDSC results
  * that differ by up to ~1e-10 element-wise.  These functions use only IEEE
- * correctly-rounded +, -, *, /, and fused multiply-add, in a fixed order, so
- * they return bit-identical results on the host (C/C++, -ffp-contract=off)
+ * correctly-rounded +, -, *, /, sqrt and fused multiply-add, in a fixed order,
+ * so they return bit-identical results on the host (C/C++, -ffp-contract=off)
  * and on the GPU (CUDA, --fmad=false): the B200 kernels and a CPU build of
  * the reference's algorithm linked against this file agree bit for bit.
  *
- * Methods (textbook, written for this project):
- *   exp(x): Cody-Waite reduction x = k*ln2 + r, |r| <= ln2/2, with a fused
- *           multiply-add and a two-part ln2; exp(r) = 1 + (r + r^2 P(r)) with
- *           P the Taylor series 1/2! .. 1/13! (truncation < 5e-18); scaling
- *           by 2^k through the exponent field.
- *   log(x) (double-double, for pow): x = m 2^e with m in [sqrt(1/2), sqrt(2)),
- *           s = (m-1)/(m+1) carried as s_hi + s_lo, log m = 2 atanh(s) =
- *           2s + s^3 T(s^2) with T the atanh series 2/3, 2/5, .. 2/23
- *           (|s| <= 0.1716, truncation < 1e-19), plus e*ln2 in two parts.
- *   pow(x,y) = exp(y * log(x)) with y*log(x) formed as a double-double and
- *           its low part added to the reduced argument.
+ * Methods (textbook, written for this project; tables in plibm_tables.h,
+ * generated exactly by make_plibm_tables.py):
+ *   exp(x): x = (128 m + j) ln2/128 + r, |r| <= ln2/256, with a two-part
+ *           ln2/128 and fused multiply-adds; exp(x) = 2^m (T_j + T_j p(r))
+ *           where T_j = 2^(j/128) is stored as hi + lo and p(r) = expm1(r) is
+ *           its Taylor polynomial to degree 5 (truncation < 6e-19).
+ *   log(x) (double-double, for pow): x = 2^e m, m in [1,2); with the top 7
+ *           mantissa bits j, m*INVC_j = 1 + r, |r| <= 2^-8, formed exactly
+ *           with a fused multiply-add; ln x = e ln2 + (-ln INVC_j) + ln(1+r),
+ *           ln(1+r) by its series to r^7/7 (absolute truncation < 2^-64),
+ *           summed as a double-double.
+ *   pow(x,y) = exp(y ln x) with y ln x a double-double whose low part enters
+ *           the reduced exp argument; exponents 0.5, 1.5, 2 and 3 are
+ *           evaluated as sqrt(x), x*sqrt(x), x*x, x*x*x.
+ * The code paths are branch-free (special inputs are fixed up with selects),
+ * so a compiler can interleave independent calls.
  * Accuracy (tests/test_plibm.py, against glibc): exp within 1 ulp, pow within
  * 2 ulp over the argument ranges CLOUDSC uses.
- * Domain: pow is evaluated for x >= 0 (every CLOUDSC base is >= 0); x < 0
- * returns NaN, x = 0 returns 0 for y > 0, +inf for y < 0, 1 for y = 0.
+ * Domain: CLOUDSC raises only non-negative bases; pow returns NaN for x < 0,
+ * 0 / +inf / 1 for x = 0 and y > 0 / y < 0 / y = 0, and 1 for y = 0.
  */
 #ifndef CLOUDSC_PLIBM_H
 #define CLOUDSC_PLIBM_H
@@ -34,12 +39,43 @@
 #include <stdint.h>
 #include <string.h>
 #include <math.h>
+#include "plibm_tables.h"
 
 #if defined(__CUDACC__)
 #define PLIBM_FN static __host__ __device__ __forceinline__
+#if defined(PLIBM_DEVICE_NOINLINE)
+#define PLIBM_FN_HEAVY static __host__ __device__ __noinline__
+#else
+#define PLIBM_FN_HEAVY PLIBM_FN
+#endif
 #else
 #define PLIBM_FN static inline
+#define PLIBM_FN_HEAVY static inline
 #endif
+
+/* The tables: one copy for host code, one in device global memory (read
+ * through the read-only data cache). */
+static const double plibm_exp_tbl[256] = PLIBM_EXP_TBL_INIT;
+static const double plibm_log_tbl[384] = PLIBM_LOG_TBL_INIT;
+#if defined(__CUDACC__)
+static __device__ const double plibm_exp_tbl_d[256] = PLIBM_EXP_TBL_INIT;
+static __device__ const double plibm_log_tbl_d[384] = PLIBM_LOG_TBL_INIT;
+#endif
+
+PLIBM_FN double plibm_exp_t(int i) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(&plibm_exp_tbl_d[i]);
+#else
+  return plibm_exp_tbl[i];
+#endif
+}
+PLIBM_FN double plibm_log_t(int i) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(&plibm_log_tbl_d[i]);
+#else
+  return plibm_log_tbl[i];
+#endif
+}
 
 PLIBM_FN uint64_t plibm_bits(double x) {
 #if defined(__CUDA_ARCH__)
@@ -66,118 +102,127 @@ PLIBM_FN double plibm_fma(double a, double b, double c) {
   return fma(a, b, c);
 #endif
 }
+PLIBM_FN double plibm_sqrt(double x) {
+#if defined(__CUDA_ARCH__)
+  return __dsqrt_rn(x);
+#else
+  return sqrt(x);
+#endif
+}
 
-#define PLIBM_INV_LN2 0x1.71547652b82fep+0
-#define PLIBM_LN2_HI 0x1.62e42fefa39efp-1
-#define PLIBM_LN2_LO 0x1.abc9e3b39803fp-56
-#define PLIBM_LN2_HI42 0x1.62e42fefa3800p-1 /* 42 significant bits: e*HI42 exact */
+#define PLIBM_INV_LN2_128 0x1.71547652b82fep+7 /* 128/ln2 */
+#define PLIBM_LN2_128_HI 0x1.62e42fefa39efp-8  /* ln2/128 in two parts */
+#define PLIBM_LN2_128_LO 0x1.abc9e3b39803fp-63
+#define PLIBM_LN2_HI42 0x1.62e42fefa3800p-1 /* ln2, 42 significant bits: e*HI42 is exact */
 #define PLIBM_LN2_LO42 0x1.ef35793c76730p-45
 #define PLIBM_SHIFT 0x1.8p52
+#define PLIBM_INF (plibm_from_bits(0x7ff0000000000000ULL))
+#define PLIBM_NAN (plibm_from_bits(0x7ff8000000000000ULL))
 
 /* 2^k for -1022 <= k <= 1023 */
-PLIBM_FN double plibm_pow2i(int k) { return plibm_from_bits((uint64_t)(k + 1023) << 52); }
+PLIBM_FN double plibm_pow2i(int k) { return plibm_from_bits((uint64_t)(int64_t)(k + 1023) << 52); }
 
-/* exp(hi + lo) for |lo| <= ~1e-16 |hi|; the kernel of both exp and pow. */
-PLIBM_FN double plibm_exp_dd(double hi, double lo) {
-  if (hi != hi) return hi + hi;
-  if (hi > 709.8) return HUGE_VAL;
-  if (hi < -745.2) return 0.0;
-  double kd = plibm_fma(hi, PLIBM_INV_LN2, PLIBM_SHIFT);
-  int k = (int)((int64_t)(plibm_bits(kd) & 0xfffffffffffffULL) - (int64_t)(1LL << 51));
+/* exp(hi + lo) for |lo| <= ~1e-15 |hi|; the kernel of both exp and pow. */
+PLIBM_FN_HEAVY double plibm_exp_dd(double hi, double lo) {
+  /* clamp so the main path stays finite; results overflow / underflow naturally */
+  double hc = hi > 709.9 ? 709.9 : hi;
+  hc = hc < -746.0 ? -746.0 : hc;
+  double kd = plibm_fma(hc, PLIBM_INV_LN2_128, PLIBM_SHIFT);
+  int64_t ki = (int64_t)(plibm_bits(kd) & 0xfffffffffffffULL) - (int64_t)(1LL << 51);
   kd = kd - PLIBM_SHIFT;
-  double r = plibm_fma(-kd, PLIBM_LN2_HI, hi);
-  r = plibm_fma(-kd, PLIBM_LN2_LO, r);
+  double r = plibm_fma(-kd, PLIBM_LN2_128_HI, hc);
+  r = plibm_fma(-kd, PLIBM_LN2_128_LO, r);
   r = r + lo;
-  double p = 0x1.6124613a86d09p-33;          /* 1/13! */
-  p = plibm_fma(p, r, 0x1.1eed8eff8d898p-29); /* 1/12! */
-  p = plibm_fma(p, r, 0x1.ae64567f544e4p-26); /* 1/11! */
-  p = plibm_fma(p, r, 0x1.27e4fb7789f5cp-22); /* 1/10! */
-  p = plibm_fma(p, r, 0x1.71de3a556c734p-19); /* 1/9!  */
-  p = plibm_fma(p, r, 0x1.a01a01a01a01ap-16); /* 1/8!  */
-  p = plibm_fma(p, r, 0x1.a01a01a01a01ap-13); /* 1/7!  */
-  p = plibm_fma(p, r, 0x1.6c16c16c16c17p-10); /* 1/6!  */
-  p = plibm_fma(p, r, 0x1.1111111111111p-7);  /* 1/5!  */
-  p = plibm_fma(p, r, 0x1.5555555555555p-5);  /* 1/4!  */
-  p = plibm_fma(p, r, 0x1.5555555555555p-3);  /* 1/3!  */
-  p = plibm_fma(p, r, 0x1.0000000000000p-1);  /* 1/2!  */
-  double q = r * r;
-  double e = 1.0 + plibm_fma(q, p, r);
-  if (k >= -1021 && k <= 1023) return e * plibm_pow2i(k);
-  /* near the overflow / underflow thresholds: scale in two exact steps */
-  if (k > 1023) return (e * plibm_pow2i(k - 512)) * plibm_pow2i(512);
-  return (e * plibm_pow2i(k + 512)) * plibm_pow2i(-512);
+  int j = (int)(ki & 127);
+  int m = (int)(ki >> 7);
+  double thi = plibm_exp_t(2 * j), tlo = plibm_exp_t(2 * j + 1);
+  double p = plibm_fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5); /* 1/120, 1/24 */
+  p = plibm_fma(p, r, 0x1.5555555555555p-3);                          /* 1/6 */
+  p = plibm_fma(p, r, 0x1.0000000000000p-1);                          /* 1/2 */
+  p = plibm_fma(p, r * r, r);                                         /* expm1(r) */
+  double s = plibm_fma(thi, p, tlo);
+  double e = thi + s;
+  int m1 = m >> 1, m2 = m - (m >> 1);
+  double res = (e * plibm_pow2i(m1)) * plibm_pow2i(m2);
+  return hi != hi ? hi : res;
 }
 
 PLIBM_FN double plibm_exp(double x) { return plibm_exp_dd(x, 0.0); }
 
-/* log(x) as hi + lo for finite x > 0. */
-PLIBM_FN void plibm_log_dd(double x, double *hi, double *lo) {
+/* ln(x) as hi + lo for finite x > 0. */
+PLIBM_FN_HEAVY void plibm_log_dd(double x, double *hi, double *lo) {
   uint64_t u = plibm_bits(x);
-  int e = 0;
-  if ((u >> 52) == 0) { /* subnormal */
-    x = x * 0x1p54;
-    u = plibm_bits(x);
-    e = -54;
-  }
-  e += (int)(u >> 52) - 1023;
-  double m = plibm_from_bits((u & 0xfffffffffffffULL) | 0x3ff0000000000000ULL); /* [1,2) */
-  if (m > 0x1.6a09e667f3bcdp+0) { /* > sqrt(2): use m/2 */
-    m = m * 0.5;
-    e += 1;
-  }
-  double f = m - 1.0; /* exact */
-  /* d = m + 1 as d_hi + d_lo (two-sum) */
-  double d_hi = m + 1.0;
-  double bb = d_hi - m;
-  double d_lo = (m - (d_hi - bb)) + (1.0 - bb);
-  double rcp = 1.0 / d_hi;
-  double s_hi = f * rcp;
-  double rem = plibm_fma(-s_hi, d_hi, f);
-  rem = plibm_fma(-s_hi, d_lo, rem);
-  double s_lo = rem * rcp;
-  double z = s_hi * s_hi;
-  double t = 0x1.642c8590b2164p-4;   /* 2/23 */
-  t = plibm_fma(t, z, 0x1.8618618618618p-4); /* 2/21 */
-  t = plibm_fma(t, z, 0x1.af286bca1af28p-4); /* 2/19 */
-  t = plibm_fma(t, z, 0x1.e1e1e1e1e1e1ep-4); /* 2/17 */
-  t = plibm_fma(t, z, 0x1.1111111111111p-3); /* 2/15 */
-  t = plibm_fma(t, z, 0x1.3b13b13b13b14p-3); /* 2/13 */
-  t = plibm_fma(t, z, 0x1.745d1745d1746p-3); /* 2/11 */
-  t = plibm_fma(t, z, 0x1.c71c71c71c71cp-3); /* 2/9  */
-  t = plibm_fma(t, z, 0x1.2492492492492p-2); /* 2/7  */
-  t = plibm_fma(t, z, 0x1.999999999999ap-2); /* 2/5  */
-  t = plibm_fma(t, z, 0x1.5555555555555p-1); /* 2/3  */
-  double tail = (z * s_hi) * t;
+  int sub = (u >> 52) == 0;
+  double xs = sub ? x * 0x1p54 : x;
+  u = plibm_bits(xs);
+  int e = (int)(u >> 52) - 1023 - (sub ? 54 : 0);
+  uint64_t mant = u & 0xfffffffffffffULL;
+  int j = (int)(mant >> 45);
+  double m = plibm_from_bits(mant | 0x3ff0000000000000ULL);
+  double invc = plibm_log_t(3 * j), lchi = plibm_log_t(3 * j + 1), lclo = plibm_log_t(3 * j + 2);
+  double p = m * invc;
+  double perr = plibm_fma(m, invc, -p); /* m*invc = p + perr exactly */
+  double r1 = p - 1.0;                  /* exact */
+  double q = plibm_fma(r1, 0x1.2492492492492p-3, -0x1.5555555555555p-3); /* 1/7, -1/6 */
+  q = plibm_fma(q, r1, 0x1.999999999999ap-3);                           /* 1/5 */
+  q = plibm_fma(q, r1, -0x1.0000000000000p-2);                          /* -1/4 */
+  q = plibm_fma(q, r1, 0x1.5555555555555p-2);                           /* 1/3 */
+  q = plibm_fma(q, r1, -0x1.0000000000000p-1);                          /* -1/2 */
+  double poly = q * (r1 * r1);
+  double corr = plibm_fma(-perr, r1, perr);
   double ed = (double)e;
-  double a_hi = ed * PLIBM_LN2_HI42; /* exact */
-  double b_hi = 2.0 * s_hi;          /* exact */
-  double sum = a_hi + b_hi;          /* two-sum */
-  double bv = sum - a_hi;
-  double err = (a_hi - (sum - bv)) + (b_hi - bv);
-  double low = err + (ed * PLIBM_LN2_LO42 + (2.0 * s_lo + tail));
-  double h = sum + low; /* fast two-sum renormalisation */
-  *lo = low - (h - sum);
+  double a = ed * PLIBM_LN2_HI42; /* exact */
+  double s1 = a + lchi;           /* two-sum */
+  double b1 = s1 - a;
+  double err1 = (a - (s1 - b1)) + (lchi - b1);
+  double s2 = s1 + r1; /* two-sum */
+  double b2 = s2 - s1;
+  double err2 = (s1 - (s2 - b2)) + (r1 - b2);
+  double low = ((err1 + err2) + (lclo + ed * PLIBM_LN2_LO42)) + (corr + poly);
+  double h = s2 + low;
+  *lo = low - (h - s2);
   *hi = h;
 }
 
-PLIBM_FN double plibm_pow(double x, double y) {
-  if (x != x || y != y) return x + y;
-  if (y == 0.0) return 1.0;
-  if (x < 0.0) return (x - x) / (x - x); /* NaN: CLOUDSC never raises a negative base */
-  if (x == 0.0) return y > 0.0 ? 0.0 : HUGE_VAL;
-  if (x == HUGE_VAL) return y > 0.0 ? HUGE_VAL : 0.0;
-  double lhi, llo;
-  plibm_log_dd(x, &lhi, &llo);
-  double t_hi = y * lhi;
-  double t_lo = plibm_fma(y, lhi, -t_hi) + y * llo;
-  return plibm_exp_dd(t_hi, t_lo);
-}
-
-/* pow with a precomputed double-double log of the base (shared-base calls). */
+/* x^y given ln(x) = lhi + llo for finite x > 0 (shared-base calls). */
 PLIBM_FN double plibm_pow_log(double lhi, double llo, double y) {
   double t_hi = y * lhi;
   double t_lo = plibm_fma(y, lhi, -t_hi) + y * llo;
   return plibm_exp_dd(t_hi, t_lo);
+}
+
+/* ln of a base for pow: the log of x for finite x > 0, else of 1 (pow's
+ * special values are fixed up from x itself). */
+PLIBM_FN void plibm_log_base(double x, double *lhi, double *llo) {
+  int ok = (x > 0.0) && (x < PLIBM_INF);
+  plibm_log_dd(ok ? x : 1.0, lhi, llo);
+}
+
+/* x^y given plibm_log_base(x) = lhi + llo; pow(x, y) is exactly this, so
+ * calls that share a base can share its logarithm. */
+PLIBM_FN double plibm_pow_with_log(double x, double y, double lhi, double llo) {
+  /* exponents with exact-operation forms (uniform branches for constant y) */
+  if (y == 0.5) return plibm_sqrt(x);
+  if (y == 1.5) return x * plibm_sqrt(x);
+  if (y == 2.0) return x * x;
+  if (y == 3.0) return (x * x) * x;
+  int ok = (x > 0.0) && (x < PLIBM_INF);
+  double res = plibm_pow_log(lhi, llo, y);
+  double spec_zero = y > 0.0 ? 0.0 : (y < 0.0 ? PLIBM_INF : 1.0);
+  double spec_inf = y > 0.0 ? PLIBM_INF : (y < 0.0 ? 0.0 : 1.0);
+  double spec = x == 0.0 ? spec_zero : (x == PLIBM_INF ? spec_inf : PLIBM_NAN);
+  res = ok ? res : spec;
+  res = y == 0.0 ? 1.0 : res;
+  return y != y ? y : res;
+}
+
+/* True when pow(x, y) does not need ln x (an exact-operation exponent). */
+PLIBM_FN int plibm_pow_is_direct(double y) { return y == 0.5 || y == 1.5 || y == 2.0 || y == 3.0; }
+
+PLIBM_FN double plibm_pow(double x, double y) {
+  double lhi = 0.0, llo = 0.0;
+  if (!plibm_pow_is_direct(y)) plibm_log_base(x, &lhi, &llo);
+  return plibm_pow_with_log(x, y, lhi, llo);
 }
 
 #endif /* CLOUDSC_PLIBM_H */
