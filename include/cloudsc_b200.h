@@ -225,7 +225,8 @@ size_t cloudsc_b200_params_size(void);
 
 /*
  * Kernel launch shape used by cloudsc_b200_batched (the autotuner's knobs).
- * threads_per_cta: columns per CTA (32..256, must divide into NPROMA tiles);
+ * threads_per_cta: columns per CTA, a multiple of 32 up to the kernel's compiled
+ * limit (128 for FP64, 256 for FP32-mixed);
  * ctas_per_sm: persistent CTAs resident per SM (0 = one wave over all tiles).
  * Returns CLOUDSC_E_SHAPE for values outside the documented limits.
  */

@@ -17,12 +17,16 @@ namespace cloudsc {
 // rescaled; a negative diagonal entry is scaled twice, as the reference's JN
 // loop does.
 // ---------------------------------------------------------------------------
-#define ROWSCALE_BEGIN(QJO)                         \
-  {                                                 \
-    double zmm = mx(QJO, zepsec);                   \
-    double zrr = mx(ss, zmm);                       \
-    double zr = zmm / zrr;
-#define ROWSCALE_END }
+// ZRR = MAX(ZSINKSUM, ZMM) and ZRATIO = ZMM/ZRR is exactly 1.0 unless the sink
+// sum exceeds ZMM; scaling by 1.0 changes nothing, so only that case scales.
+#define ROWSCALE_BEGIN(QJO)       \
+  {                               \
+    double zmm = mx(QJO, zepsec); \
+    if (ss > zmm) {               \
+      double zr = zmm / ss;
+#define ROWSCALE_END \
+  }                  \
+  }
 #define SCL(F, A, B) \
   if (F) {           \
     A = A * zr;      \
@@ -773,9 +777,14 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
 
       // 5.2.1 sink truncation (:3455-3536), double
       const double qx[5] = {double(ql), double(qi), double(qr), double(qs), double(qv)};
-      {
-        double ratio[5];
-        sink_ratios(q, qx, ratio);
+      // When no species' sinks exceed its content every ratio is exactly 1.0
+      // (ZMAX/ZMAX), every rescaling in the reference's loop multiplies by 1.0
+      // and the processing order is immaterial: the whole step is then an
+      // exact no-op and is skipped.
+      double ratio[5];
+      sink_ratios(q, qx, ratio);
+      if (ratio[0] != 1.0 || ratio[1] != 1.0 || ratio[2] != 1.0 || ratio[3] != 1.0 ||
+          ratio[4] != 1.0) {
         double sr[5];
         int ord[5];
         sr[0] = ratio[0];

@@ -23,6 +23,7 @@ namespace cloudsc {
 cudaError_t upload_params(const cloudsc_params &p, const Derived &d);
 cudaError_t launch(int precision, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream);
+int max_threads(int precision);
 }  // namespace cloudsc
 
 using namespace cloudsc;
@@ -37,7 +38,7 @@ bool g_have_params = false;
 unsigned long long g_gen = 0;
 constexpr int kMaxDev = 64;
 unsigned long long g_dev_gen[kMaxDev] = {0};
-int g_threads[2] = {128, 64};
+int g_threads[2] = {128, 128};
 int g_ctas_per_sm[2] = {0, 0};
 
 int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -323,8 +324,9 @@ int cloudsc_b200_setup(const cloudsc_params *p) {
 
 int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm) {
   if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
-  if (threads_per_cta < 32 || threads_per_cta > 256 || threads_per_cta % 32)
-    return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32 in [32,256]");
+  if (threads_per_cta < 32 || threads_per_cta > max_threads(precision) || threads_per_cta % 32)
+    return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32, at least 32 and at most "
+                                 "the kernel's compiled limit (128 FP64, 256 FP32-mixed)");
   if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(CLOUDSC_E_SHAPE, "ctas_per_sm must be in [0,32]");
   std::lock_guard<std::mutex> lk(g_mu);
   g_threads[precision] = threads_per_cta;

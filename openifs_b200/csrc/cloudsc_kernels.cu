@@ -74,22 +74,38 @@ cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
   return e;
 }
 
-// Register budget: __launch_bounds__(CLOUDSC_MAXT, CLOUDSC_MINB).
+// Register budget: __launch_bounds__(CLOUDSC_MAXT, CLOUDSC_MINB).  128 threads
+// x 3 CTAs per SM caps the kernels at 168 registers (a few hundred bytes of
+// spills): 12 warps per SM hide more FP64 latency than 8 warps at 255
+// registers (measured 23.2 ms vs 28.6 ms for the FP64 kernel at 262,144
+// columns).
+// The FP32-mixed kernel is fastest with the full 255 registers (measured
+// 22.6 ms vs 27.7 ms at 168).
 #ifndef CLOUDSC_MAXT
-#define CLOUDSC_MAXT 256
+#define CLOUDSC_MAXT 128
 #endif
 #ifndef CLOUDSC_MINB
-#define CLOUDSC_MINB 1
+#define CLOUDSC_MINB 3
 #endif
+#ifndef CLOUDSC_MIX_MAXT
+#define CLOUDSC_MIX_MAXT 256
+#endif
+#ifndef CLOUDSC_MIX_MINB
+#define CLOUDSC_MIX_MINB 1
+#endif
+
+// Largest CTA the kernel of `precision` was compiled for.
+int max_threads(int precision) { return precision == 0 ? CLOUDSC_MAXT : CLOUDSC_MIX_MAXT; }
 
 // Launch the kernel: precision 0 = FP64, 1 = FP32-mixed.
 cudaError_t launch(int precision, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream) {
-  if (threads > CLOUDSC_MAXT) return cudaErrorInvalidConfiguration;
   if (precision == 0) {
+    if (threads > CLOUDSC_MAXT) return cudaErrorInvalidConfiguration;
     cloudsc_kernel<false, CLOUDSC_MAXT, CLOUDSC_MINB><<<grid, threads, 0, stream>>>(f, sh);
   } else {
-    cloudsc_kernel<true, CLOUDSC_MAXT, CLOUDSC_MINB><<<grid, threads, 0, stream>>>(f, sh);
+    if (threads > CLOUDSC_MIX_MAXT) return cudaErrorInvalidConfiguration;
+    cloudsc_kernel<true, CLOUDSC_MIX_MAXT, CLOUDSC_MIX_MINB><<<grid, threads, 0, stream>>>(f, sh);
   }
   return cudaGetLastError();
 }

@@ -78,7 +78,7 @@ def test_edge_columns(cuda, case):
     _check(p, po, arrs, 64, 4, 256)
 
 
-@pytest.mark.parametrize("threads", [32, 64, 128, 256])
+@pytest.mark.parametrize("threads", [32, 64, 128])
 def test_launch_shapes(cuda, threads):
     """Every supported CTA shape and a persistent grid give identical results."""
     p, po = util.params()
