@@ -17,7 +17,9 @@
  *   - KIDIA/KFDIA are 1-based; only columns KIDIA..KFDIA are written;
  *   - LOGICAL arguments are 4-byte integers (non-zero = .TRUE.);
  *   - REAL(KIND=JPRB) is double (the double-precision OpenIFS build);
- *     the *_sp entry points take the single-precision build's REAL(4).
+ *   - outputs the reference leaves undefined: PTENDENCY_LOC_CLD(:,:,NCLV) is
+ *     never written (cloudsc.F90:971 loops to NCLV-1), PCOVPTOT(:,1:NCLDTOP-1)
+ *     is written as 0.
  *
  * Return codes: 0 = success; > 0 = number of negative-condensate warning events
  * (the reference WRITEs a warning to NULOUT for each, cloudsc.F90:3794,3802);
@@ -225,8 +227,8 @@ size_t cloudsc_b200_params_size(void);
 
 /*
  * Kernel launch shape used by cloudsc_b200_batched (the autotuner's knobs).
- * threads_per_cta: columns per CTA, a multiple of 32 up to the kernel's compiled
- * limit (128 for FP64, 256 for FP32-mixed);
+ * threads_per_cta: columns per CTA, a multiple of 32 up to the kernels'
+ * compiled limit of 384 (default 384);
  * ctas_per_sm: persistent CTAs resident per SM (0 = one wave over all tiles).
  * Returns CLOUDSC_E_SHAPE for values outside the documented limits.
  */

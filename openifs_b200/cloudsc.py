@@ -158,3 +158,4 @@ def cloudsc_block(params, kidia, kfdia, klon, klev, ptsphy, arrays, lddiag=False
     return _check(lib().cloudsc_b200_block(
         ctypes.byref(params), int(kidia), int(kfdia), int(klon), int(klev), int(bool(lddiag)),
         float(ptsphy), *a1, int(bool(ldslphy)), *a2, int(kfldx)))
+

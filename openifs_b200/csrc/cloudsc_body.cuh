@@ -4,122 +4,98 @@
 //   CSC_DEV           function qualifiers (__device__ __forceinline__ on the GPU)
 //   KP<Real>()        the KParams<Real> block, c_kd the KParamsD block
 //   ld(p), atomic_add(p, v), xexp/xpow/xsqrt/xabs/xsign overloads
+//   CSC_LEVEL_SYNC()  optional: a barrier of all columns of a CTA at the end
+//                     of every level (nothing on the host)
 // See cloudsc_column.cuh for the numerical contract.
 #pragma once
 #include "cloudsc_column.cuh"
 
+#ifndef CSC_LEVEL_SYNC
+#define CSC_LEVEL_SYNC()
+#endif
+
 namespace cloudsc {
 
-// ---------------------------------------------------------------------------
-// Sink truncation of one species row (cloudsc.F90:3500-3535 for one JM):
-// the sink sum over the row's structurally non-zero entries in column order,
-// the scaling factor, then every negative entry (JO,n) and its mirror (n,JO)
-// rescaled; a negative diagonal entry is scaled twice, as the reference's JN
-// loop does.
-// ---------------------------------------------------------------------------
-// ZRR = MAX(ZSINKSUM, ZMM) and ZRATIO = ZMM/ZRR is exactly 1.0 unless the sink
-// sum exceeds ZMM; scaling by 1.0 changes nothing, so only that case scales.
-#define ROWSCALE_BEGIN(QJO)       \
-  {                               \
-    double zmm = mx(QJO, zepsec); \
-    if (ss > zmm) {               \
-      double zr = zmm / ss;
-#define ROWSCALE_END \
-  }                  \
-  }
-#define SCL(F, A, B) \
-  if (F) {           \
-    A = A * zr;      \
-    B = B * zr;      \
-  }
-
+// ZSOLQA(a,b) of the reference ("+" is a source of a and a sink of b).  Every
+// off-diagonal rate is added to (a,b) and subtracted from (b,a), so
+// ZSOLQA(b,a) == -ZSOLQA(a,b) exactly at all times: negation is exact,
+// round-to-nearest is symmetric, and the sink rescaling multiplies both by the
+// same factor.  Only one entry of each pair is stored:
+//   diagonal LL, II, RR, SS;  pairs LI (IL = -LI), LV (VL = -LV), IR (RI = -IR),
+//   IV (VI = -IV), RS (SR = -RS), RV (VR = -RV), SV (VS = -SV).
+// Every sum below is the reference's sum with a + (-b) written as a - b and
+// 0 - (-b) as 0 + b, which are the same IEEE operations.
 struct QA {
-  // explicit sources/sinks ZSOLQA(a,b): "+" is a source of a and sink of b
-  double LL, LI, LV, IL, II, IR, IV, RI, RR, RS, RV, SR, SS, SV, VL, VI, VR, VS;
+  double LL, II, RR, SS, LI, LV, IR, IV, RS, RV, SV;
 };
 
+// Sink sum of each row JM: -(sum over JN of ZSOLQA(JM,JN)) accumulated as
+// ZSINKSUM = ZSINKSUM - ZSOLQA(JM,JN) in JN order (cloudsc.F90:3459-3466).
+CSC_DEV double sink_sum(int jo, const QA &q) {
+  double s;
+  switch (jo) {
+    case L: s = 0.0 - q.LL; s = s - q.LI; s = s - q.LV; break;
+    case I: s = 0.0 + q.LI; s = s - q.II; s = s - q.IR; s = s - q.IV; break;
+    case R: s = 0.0 + q.IR; s = s - q.RR; s = s - q.RS; s = s - q.RV; break;
+    case S: s = 0.0 + q.RS; s = s - q.SS; s = s - q.SV; break;
+    default: s = 0.0 + q.LV; s = s + q.IV; s = s + q.RV; s = s + q.SV; break;
+  }
+  return s;
+}
+
+// Sink truncation of one species row (cloudsc.F90:3500-3535 for one JM): the
+// scaling factor ZRATIO = ZMM/MAX(ZSINKSUM,ZMM), then every negative entry
+// (JO,n) rescaled together with its mirror (n,JO); a negative diagonal entry
+// is scaled twice, as the reference's JN loop does.  ZRATIO is exactly 1.0
+// unless the sink sum exceeds ZMM, and scaling by 1.0 changes nothing, so only
+// that case scales.
+#define SCL2(F, A) \
+  if (F) {         \
+    A = A * zr;    \
+    A = A * zr;    \
+  }
+#define SCL1(F, A) \
+  if (F) A = A * zr;
 CSC_DEV void scale_row(int jo, QA &q, const double qx[5]) {
   const double zepsec = 1.E-14;
-  double ss;
+  const double ss = sink_sum(jo, q);
+  const double zmm = mx(qx[jo], zepsec);
+  if (!(ss > zmm)) return;
+  const double zr = zmm / ss;
   switch (jo) {
     case L: {
       bool fLL = q.LL < 0.0, fLI = q.LI < 0.0, fLV = q.LV < 0.0;
-      ss = 0.0 - q.LL;
-      ss = ss - q.LI;
-      ss = ss - q.LV;
-      ROWSCALE_BEGIN(qx[L])
-      SCL(fLL, q.LL, q.LL)
-      SCL(fLI, q.LI, q.IL)
-      SCL(fLV, q.LV, q.VL)
-      ROWSCALE_END
+      SCL2(fLL, q.LL) SCL1(fLI, q.LI) SCL1(fLV, q.LV)
     } break;
-    case I: {
-      bool fIL = q.IL < 0.0, fII = q.II < 0.0, fIR = q.IR < 0.0, fIV = q.IV < 0.0;
-      ss = 0.0 - q.IL;
-      ss = ss - q.II;
-      ss = ss - q.IR;
-      ss = ss - q.IV;
-      ROWSCALE_BEGIN(qx[I])
-      SCL(fIL, q.IL, q.LI)
-      SCL(fII, q.II, q.II)
-      SCL(fIR, q.IR, q.RI)
-      SCL(fIV, q.IV, q.VI)
-      ROWSCALE_END
+    case I: {  // (I,L) = -LI < 0  <=>  LI > 0
+      bool fIL = q.LI > 0.0, fII = q.II < 0.0, fIR = q.IR < 0.0, fIV = q.IV < 0.0;
+      SCL1(fIL, q.LI) SCL2(fII, q.II) SCL1(fIR, q.IR) SCL1(fIV, q.IV)
     } break;
     case R: {
-      bool fRI = q.RI < 0.0, fRR = q.RR < 0.0, fRS = q.RS < 0.0, fRV = q.RV < 0.0;
-      ss = 0.0 - q.RI;
-      ss = ss - q.RR;
-      ss = ss - q.RS;
-      ss = ss - q.RV;
-      ROWSCALE_BEGIN(qx[R])
-      SCL(fRI, q.RI, q.IR)
-      SCL(fRR, q.RR, q.RR)
-      SCL(fRS, q.RS, q.SR)
-      SCL(fRV, q.RV, q.VR)
-      ROWSCALE_END
+      bool fRI = q.IR > 0.0, fRR = q.RR < 0.0, fRS = q.RS < 0.0, fRV = q.RV < 0.0;
+      SCL1(fRI, q.IR) SCL2(fRR, q.RR) SCL1(fRS, q.RS) SCL1(fRV, q.RV)
     } break;
     case S: {
-      bool fSR = q.SR < 0.0, fSS = q.SS < 0.0, fSV = q.SV < 0.0;
-      ss = 0.0 - q.SR;
-      ss = ss - q.SS;
-      ss = ss - q.SV;
-      ROWSCALE_BEGIN(qx[S])
-      SCL(fSR, q.SR, q.RS)
-      SCL(fSS, q.SS, q.SS)
-      SCL(fSV, q.SV, q.VS)
-      ROWSCALE_END
+      bool fSR = q.RS > 0.0, fSS = q.SS < 0.0, fSV = q.SV < 0.0;
+      SCL1(fSR, q.RS) SCL2(fSS, q.SS) SCL1(fSV, q.SV)
     } break;
     default: {
-      bool fVL = q.VL < 0.0, fVI = q.VI < 0.0, fVR = q.VR < 0.0, fVS = q.VS < 0.0;
-      ss = 0.0 - q.VL;
-      ss = ss - q.VI;
-      ss = ss - q.VR;
-      ss = ss - q.VS;
-      ROWSCALE_BEGIN(qx[V])
-      SCL(fVL, q.VL, q.LV)
-      SCL(fVI, q.VI, q.IV)
-      SCL(fVR, q.VR, q.RV)
-      SCL(fVS, q.VS, q.SV)
-      ROWSCALE_END
+      bool fVL = q.LV > 0.0, fVI = q.IV > 0.0, fVR = q.RV > 0.0, fVS = q.SV > 0.0;
+      SCL1(fVL, q.LV) SCL1(fVI, q.IV) SCL1(fVR, q.RV) SCL1(fVS, q.SV)
     } break;
   }
 }
+#undef SCL1
+#undef SCL2
 
 // ZRATIO for every species from the current ZSOLQA (cloudsc.F90:3455-3474).
 CSC_DEV void sink_ratios(const QA &q, const double qx[5], double r[5]) {
   const double zepsec = 1.E-14;
-  double s;
-  s = 0.0 - q.LL; s = s - q.LI; s = s - q.LV;
-  { double zmax = mx(qx[L], zepsec); r[L] = zmax / mx(s, zmax); }
-  s = 0.0 - q.IL; s = s - q.II; s = s - q.IR; s = s - q.IV;
-  { double zmax = mx(qx[I], zepsec); r[I] = zmax / mx(s, zmax); }
-  s = 0.0 - q.RI; s = s - q.RR; s = s - q.RS; s = s - q.RV;
-  { double zmax = mx(qx[R], zepsec); r[R] = zmax / mx(s, zmax); }
-  s = 0.0 - q.SR; s = s - q.SS; s = s - q.SV;
-  { double zmax = mx(qx[S], zepsec); r[S] = zmax / mx(s, zmax); }
-  s = 0.0 - q.VL; s = s - q.VI; s = s - q.VR; s = s - q.VS;
-  { double zmax = mx(qx[V], zepsec); r[V] = zmax / mx(s, zmax); }
+#pragma unroll
+  for (int jm = 0; jm < 5; ++jm) {
+    double zmax = mx(qx[jm], zepsec);
+    r[jm] = zmax / mx(sink_sum(jm, q), zmax);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -173,8 +149,10 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp,
 // ---------------------------------------------------------------------------
 // The column body.
 // ---------------------------------------------------------------------------
+// `active` false: the thread only keeps a CTA's per-level barrier company
+// (it computes column (ib, jl), which must be valid, and stores nothing).
 template <typename Real, bool F32M>
-CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
+CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bool active = true) {
   const KParams<Real> &P = KP<Real>();
   const KParamsD &PD = c_kd;
   typedef double D;
@@ -217,9 +195,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
   unsigned nwarn = 0;
 
   // flux index 1 (:4231-4241)
-  F.pfsqlf[o2h] = 0.0; F.pfsqif[o2h] = 0.0; F.pfsqrf[o2h] = 0.0; F.pfsqsf[o2h] = 0.0;
-  F.pfcqlng[o2h] = 0.0; F.pfcqnng[o2h] = 0.0; F.pfcqrng[o2h] = 0.0; F.pfcqsng[o2h] = 0.0;
-  F.pfsqltur[o2h] = 0.0; F.pfsqitur[o2h] = 0.0;
+  if (active) {
+    F.pfsqlf[o2h] = 0.0; F.pfsqif[o2h] = 0.0; F.pfsqrf[o2h] = 0.0; F.pfsqsf[o2h] = 0.0;
+    F.pfcqlng[o2h] = 0.0; F.pfcqnng[o2h] = 0.0; F.pfcqrng[o2h] = 0.0; F.pfcqsng[o2h] = 0.0;
+    F.pfsqltur[o2h] = 0.0; F.pfsqitur[o2h] = 0.0;
+  }
 
   // (KLON,KLEV,N) arrays: the block stride is N*KLON*KLEV, species m at +m*KLON*KLEV
   const size_t o5 = (size_t)ib * 5 * s2 + jl, o4 = (size_t)ib * 4 * s2 + jl, o2s = (size_t)ib * 2 * s2 + jl;
@@ -331,8 +311,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
       Real qxfg_l = ql, qxfg_i = qi, qxfg_r = qr, qxfg_s = qs;
       Real solac = C(0.0), solab = C(0.0);
       QA q;
-      q.LL = q.LI = q.LV = q.IL = q.II = q.IR = q.IV = q.RI = q.RR = q.RS = q.RV = q.SR = q.SS = q.SV =
-          q.VL = q.VI = q.VR = q.VS = 0.0;
+      q.LL = q.II = q.RR = q.SS = q.LI = q.LV = q.IR = q.IV = q.RS = q.RV = q.SV = 0.0;
       Real qb_ll = C(0.0), qb_ii = C(0.0), qb_rl = C(0.0), qb_si = C(0.0), qb_sl = C(0.0);
       Real convsrce_l = C(0.0), convsrce_i = C(0.0), convsrce_r = C(0.0), convsrce_s = C(0.0);
       Real convsink_l = C(0.0), convsink_i = C(0.0);
@@ -340,6 +319,8 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
       Real qpretot = C(0.0);
       // The ZSOLQA accumulators are double in both instantiations; in the
       // FP32-mixed kernel each process rate (Real) is widened when added.
+      // QADD/QSUB act on the stored entry of a pair (see struct QA); the
+      // comment beside each names the reference's pair of updates.
 #define QADD(E, X) q.E = q.E + double(X)
 #define QSUB(E, X) q.E = q.E - double(X)
 
@@ -376,12 +357,10 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
 
       // evaporate very small amounts (:1334-1342)
       if (ql < P.rlmin) {
-        q.VL = double(ql);
-        q.LV = -double(ql);
+        q.LV = -double(ql);  // ZSOLQA(V,L) = ql, ZSOLQA(L,V) = -ql
       }
       if (qi < P.rlmin) {
-        q.VI = double(qi);
-        q.IV = -double(qi);
+        q.IV = -double(qi);  // ZSOLQA(V,I) = qi, ZSOLQA(I,V) = -qi
       }
 
       // 3.2 detrainment (:1362-1398)
@@ -402,7 +381,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           QADD(RR, convsrce_r);
           QADD(SS, convsrce_s);
         }
-        F.plude[ok] = plude_k;
+        if (active) F.plude[ok] = plude_k;
       }
 
       // 3.3 subsidence source and evaporation (:1419-1492)
@@ -424,8 +403,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           zlfinal = lcust_l - zevap;
           lfinalsum = lfinalsum + zlfinal;
           QADD(LL, lcust_l);
-          QADD(VL, zevap);
-          QSUB(LV, zevap);
+          QSUB(LV, zevap);  // (V,L) += zevap, (L,V) -= zevap
         }
         {
           Real zlfinal = mx(C(0.0), lcust_i - zdqs);
@@ -433,8 +411,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           zlfinal = lcust_i - zevap;
           lfinalsum = lfinalsum + zlfinal;
           QADD(II, lcust_i);
-          QADD(VI, zevap);
-          QSUB(IV, zevap);
+          QSUB(IV, zevap);  // (V,I) += zevap, (I,V) -= zevap
         }
         solac = solac + zacust;
         if (lfinalsum < zepsec) solac = solac - zacust;
@@ -467,10 +444,8 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           zleros = mn(zleros, zli);
           Real zaeros = C(0.5) * zleros / zlicld;
           solac = solac - zaeros;
-          QADD(VL, liqfrac * zleros);
-          QSUB(LV, liqfrac * zleros);
-          QADD(VI, icefrac * zleros);
-          QSUB(IV, icefrac * zleros);
+          QSUB(LV, liqfrac * zleros);  // (V,L) +=, (L,V) -=
+          QSUB(IV, icefrac * zleros);  // (V,I) +=, (I,V) -=
         }
       }
 
@@ -566,8 +541,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
           Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
           Real zevap = mn(zdpevap, qxfg_r);
-          QADD(VR, zevap);
-          QSUB(RV, zevap);
+          QSUB(RV, zevap);  // (V,R) += zevap, (R,V) -= zevap
           qxfg_r = qxfg_r - zevap;
         }
       }
@@ -594,8 +568,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           zdepos = zdepos * mn(zinfactor + (C(1.0) - zinfactor) *
                                                (P.rdepliqrefrate + zcldtopdist / P.rdepliqrefdepth),
                                C(1.0));
-          QADD(IL, zdepos);
-          QSUB(LI, zdepos);
+          QSUB(LI, zdepos);  // (I,L) += zdepos, (L,I) -= zdepos
           qxfg_i = qxfg_i + zdepos;
           qxfg_l = qxfg_l - zdepos;
         }
@@ -617,8 +590,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
                             mpowb<F32M>(b_pr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
           Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
           zpsdep = mn(zpsdep, qv - zqsmix) / zcorqsmix;
-          QADD(SV, zpsdep);
-          QSUB(VS, zpsdep);
+          QADD(SV, zpsdep);  // (S,V) += zpsdep, (V,S) -= zpsdep
         }
       }
 
@@ -651,14 +623,12 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           Real zmelt = mn(qxfg_i, zalfa * zmeltmax);
           qxfg_i = qxfg_i - zmelt;
           qxfg_r = qxfg_r + zmelt;
-          QADD(RI, zmelt);
-          QSUB(IR, zmelt);
+          QSUB(IR, zmelt);  // (R,I) += zmelt, (I,R) -= zmelt
           zalfa = qxfg_s / zicetot;
           zmelt = mn(qxfg_s, zalfa * zmeltmax);
           qxfg_s = qxfg_s - zmelt;
           qxfg_r = qxfg_r + zmelt;
-          QADD(RS, zmelt);
-          QSUB(SR, zmelt);
+          QADD(RS, zmelt);  // (R,S) += zmelt, (S,R) -= zmelt
         }
       }
 
@@ -682,8 +652,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           }
           if (zfrzmax > zepsec) {
             Real zfrz = mn(qr, zfrzmax);
-            QADD(SR, zfrz);
-            QSUB(RS, zfrz);
+            QSUB(RS, zfrz);  // (S,R) += zfrz, (R,S) -= zfrz
           }
         }
       }
@@ -693,8 +662,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
         Real zfrzmax = mx((P.rthomo - t) * P.zrldcp, C(0.0));
         if (zfrzmax > zepsec && qxfg_l > zepsec) {
           Real zfrz = mn(qxfg_l, zfrzmax);
-          QADD(IL, zfrz);
-          QSUB(LI, zfrz);
+          QSUB(LI, zfrz);  // (I,L) += zfrz, (L,I) -= zfrz
         }
       }
 
@@ -720,8 +688,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           Real zrat = zlamr / zlams;
           Real zpsacr =
               zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
-          QADD(SR, zpsacr);
-          QSUB(RS, zpsacr);
+          QSUB(RS, zpsacr);  // (S,R) += zpsacr, (R,S) -= zpsacr
         }
         if (zicecld > zepsec) {
           Real zlami = mpow<F32M>(P.rcl_lam1s / (zrho * zicecld), P.rcl_lam2s);
@@ -731,8 +698,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           Real zrat = zlamr / zlami;
           Real zpiacr =
               zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
-          QADD(IR, zpiacr);
-          QSUB(RI, zpiacr);
+          QADD(IR, zpiacr);  // (I,R) += zpiacr, (R,I) -= zpiacr
         }
       }
 
@@ -751,17 +717,16 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
           Real zdpr = zcovpclr * zbeta * (zqsice - zqe) / zdenom * zdp * P.zrg_r;
           Real zdpevap = zdpr * zdtgdp;
           Real zevap = mn(zdpevap, qxfg_s);
-          QADD(VS, zevap);
-          QSUB(SV, zevap);
+          QSUB(SV, zevap);  // (V,S) += zevap, (S,V) -= zevap
           zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), (zcovptot - a) * zevap / qxfg_s));
           qxfg_s = qxfg_s - zevap;
         }
       }
 
       // evaporate small precipitation amounts (:3402-3412)
-      if (qxfg_i < P.rlmin) { QADD(VI, qxfg_i); QSUB(IV, qxfg_i); }
-      if (qxfg_r < P.rlmin) { QADD(VR, qxfg_r); QSUB(RV, qxfg_r); }
-      if (qxfg_s < P.rlmin) { QADD(VS, qxfg_s); QSUB(SV, qxfg_s); }
+      if (qxfg_i < P.rlmin) QSUB(IV, qxfg_i);  // (V,I) +=, (I,V) -=
+      if (qxfg_r < P.rlmin) QSUB(RV, qxfg_r);  // (V,R) +=, (R,V) -=
+      if (qxfg_s < P.rlmin) QSUB(SV, qxfg_s);  // (V,S) +=, (S,V) -=
 #undef QADD
 #undef QSUB
 
@@ -775,16 +740,12 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
         zanewm1 = zanew;
       }
 
-      // 5.2.1 sink truncation (:3455-3536), double
+      // 5.2.1 sink truncation (:3455-3536), double: ratios, insertion sort
+      // (IORDV, stable for ties), rows rescaled in sorted order
       const double qx[5] = {double(ql), double(qi), double(qr), double(qs), double(qv)};
-      // When no species' sinks exceed its content every ratio is exactly 1.0
-      // (ZMAX/ZMAX), every rescaling in the reference's loop multiplies by 1.0
-      // and the processing order is immaterial: the whole step is then an
-      // exact no-op and is skipped.
-      double ratio[5];
-      sink_ratios(q, qx, ratio);
-      if (ratio[0] != 1.0 || ratio[1] != 1.0 || ratio[2] != 1.0 || ratio[3] != 1.0 ||
-          ratio[4] != 1.0) {
+      {
+        double ratio[5];
+        sink_ratios(q, qx, ratio);
         double sr[5];
         int ord[5];
         sr[0] = ratio[0];
@@ -811,18 +772,22 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
             ord[0] = jm;
           }
         }
+        // the order packed 3 bits per position: one copy of the row code
+        unsigned code = 0;
 #pragma unroll
-        for (int jm = 0; jm < 5; ++jm) scale_row(ord[jm], q, qx);
+        for (int jm = 0; jm < 5; ++jm) code |= (unsigned)ord[jm] << (3 * jm);
+#pragma unroll 1
+        for (int jm = 0; jm < 5; ++jm) scale_row((int)((code >> (3 * jm)) & 7u), q, qx);
       }
 
       // 5.2.2 solve (:3546-3628), double, lower-triangular form
       double x_l, x_i, x_r, x_s, x_v;
       {
         x_l = qx[L] + (((0.0 + q.LL) + q.LI) + q.LV);
-        x_i = qx[I] + ((((0.0 + q.IL) + q.II) + q.IR) + q.IV);
-        x_r = qx[R] + ((((0.0 + q.RI) + q.RR) + q.RS) + q.RV);
-        x_s = qx[S] + (((0.0 + q.SR) + q.SS) + q.SV);
-        x_v = qx[V] + ((((0.0 + q.VL) + q.VI) + q.VR) + q.VS);
+        x_i = qx[I] + ((((0.0 - q.LI) + q.II) + q.IR) + q.IV);
+        x_r = qx[R] + ((((0.0 - q.IR) + q.RR) + q.RS) + q.RV);
+        x_s = qx[S] + (((0.0 - q.RS) + q.SS) + q.SV);
+        x_v = qx[V] + ((((0.0 - q.LV) - q.IV) - q.RV) - q.SV);
         const double d_l = ((1.0 + 0.0) + double(qb_ll) + double(qb_rl)) + double(qb_sl);
         const double d_i = ((1.0 + double(fallsink_i)) + double(qb_ii)) + double(qb_si);
         const double d_r = 1.0 + double(fallsink_r);
@@ -904,23 +869,27 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
     }  // k >= ncldtop0
 
     // ---------------- outputs of level k ----------------
-    F.loc_t[ok] = loc_t;
-    F.loc_q[ok] = loc_q;
-    F.loc_a[ok] = loc_a;
-    F.loc_cld[ok5] = loc_cl;
-    F.loc_cld[ok5 + s2] = loc_ci;
-    F.loc_cld[ok5 + 2 * s2] = loc_cr;
-    F.loc_cld[ok5 + 3 * s2] = loc_cs;
-    F.pcovptot[ok] = D(covp_out);
+    if (active) {
+      F.loc_t[ok] = loc_t;
+      F.loc_q[ok] = loc_q;
+      F.loc_a[ok] = loc_a;
+      F.loc_cld[ok5] = loc_cl;
+      F.loc_cld[ok5 + s2] = loc_ci;
+      F.loc_cld[ok5 + 2 * s2] = loc_cr;
+      F.loc_cld[ok5 + 3 * s2] = loc_cs;
+      F.pcovptot[ok] = D(covp_out);
+    }
 
     // precipitation fluxes at half level k (:4218-4224, 4297-4303)
     {
       const size_t oh = o2h + (size_t)k * np;
       const D fl = D(pfplsx_r) + 0.0, fn = D(pfplsx_s) + D(pfplsx_i);
-      F.pfplsl[oh] = fl;
-      F.pfplsn[oh] = fn;
-      F.pfhpsl[oh] = -PD.rlvtt * fl;
-      F.pfhpsn[oh] = -PD.rlstt * fn;
+      if (active) {
+        F.pfplsl[oh] = fl;
+        F.pfplsn[oh] = fn;
+        F.pfhpsl[oh] = -PD.rlvtt * fl;
+        F.pfhpsn[oh] = -PD.rlstt * fn;
+      }
     }
     // DDH flux recurrences to half level k+1 (:4244-4292)
     {
@@ -936,16 +905,18 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
       fsqif = fsqif + (qxn2d_i - q0_i + pvfi * dt) * zgdph_r + pludeli2;
       fcqnng = fcqnng + lneg_i * zgdph_r;
       fsqitur = fsqitur + pvfi * dt * zgdph_r;
-      F.pfsqlf[oh1] = fsqlf;
-      F.pfsqif[oh1] = fsqif;
-      F.pfsqrf[oh1] = sqrf;
-      F.pfsqsf[oh1] = sqsf;
-      F.pfcqlng[oh1] = fcqlng;
-      F.pfcqnng[oh1] = fcqnng;
-      F.pfcqrng[oh1] = cqrng;
-      F.pfcqsng[oh1] = cqsng;
-      F.pfsqltur[oh1] = fsqltur;
-      F.pfsqitur[oh1] = fsqitur;
+      if (active) {
+        F.pfsqlf[oh1] = fsqlf;
+        F.pfsqif[oh1] = fsqif;
+        F.pfsqrf[oh1] = sqrf;
+        F.pfsqsf[oh1] = sqsf;
+        F.pfcqlng[oh1] = fcqlng;
+        F.pfcqnng[oh1] = fcqnng;
+        F.pfcqrng[oh1] = cqrng;
+        F.pfcqsng[oh1] = cqsng;
+        F.pfsqltur[oh1] = fsqltur;
+        F.pfsqitur[oh1] = fsqitur;
+      }
     }
 
     // carry to level k+1
@@ -960,18 +931,21 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl) {
     pfplsx_i = pfplsx_i_n;
     pfplsx_r = pfplsx_r_n;
     pfplsx_s = pfplsx_s_n;
+    CSC_LEVEL_SYNC();
   }
   // precipitation fluxes at the surface half level KLEV+1
   {
     const size_t oh = o2h + (size_t)klev * np;
     const D fl = D(pfplsx_r) + 0.0, fn = D(pfplsx_s) + D(pfplsx_i);
-    F.pfplsl[oh] = fl;
-    F.pfplsn[oh] = fn;
-    F.pfhpsl[oh] = -PD.rlvtt * fl;
-    F.pfhpsn[oh] = -PD.rlstt * fn;
+    if (active) {
+      F.pfplsl[oh] = fl;
+      F.pfplsn[oh] = fn;
+      F.pfhpsl[oh] = -PD.rlvtt * fl;
+      F.pfhpsn[oh] = -PD.rlstt * fn;
+    }
   }
-  F.prainfrac_toprfz[o1] = D(prainfrac);
-  if (nwarn && F.ncounters) atomic_add(F.ncounters, nwarn);
+  if (active) F.prainfrac_toprfz[o1] = D(prainfrac);
+  if (active && nwarn && F.ncounters) atomic_add(F.ncounters, nwarn);
 #undef C
 }
 

@@ -38,7 +38,7 @@ bool g_have_params = false;
 unsigned long long g_gen = 0;
 constexpr int kMaxDev = 64;
 unsigned long long g_dev_gen[kMaxDev] = {0};
-int g_threads[2] = {128, 128};
+int g_threads[2] = {384, 384};
 int g_ctas_per_sm[2] = {0, 0};
 
 int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -326,7 +326,7 @@ int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t 
   if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
   if (threads_per_cta < 32 || threads_per_cta > max_threads(precision) || threads_per_cta % 32)
     return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32, at least 32 and at most "
-                                 "the kernel's compiled limit (128 FP64, 256 FP32-mixed)");
+                                 "the kernel's compiled limit (384)");
   if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(CLOUDSC_E_SHAPE, "ctas_per_sm must be in [0,32]");
   std::lock_guard<std::mutex> lk(g_mu);
   g_threads[precision] = threads_per_cta;
@@ -340,7 +340,7 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
     std::lock_guard<std::mutex> lk(g_mu);
     threads = g_threads[precision];
   }
-  tiles = sh.ngpblks * ((sh.nproma + threads - 1) / threads);
+  tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   int grid = grid_for(precision, tiles, threads);
   cudaError_t e = launch(precision, f, sh, threads, grid, stream);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
@@ -433,6 +433,12 @@ size_t elems(Kind k, size_t np, size_t klev) {
 }
 // rows of nproma elements per block (for strided column-range copies)
 size_t rows(Kind k, size_t klev) { return elems(k, 1, klev); }
+// Rows of array i that a call returns to the caller.  PTENDENCY_LOC_CLD's
+// last species (NCLV) is never written by the reference (cloudsc.F90:971
+// loops to NCLV-1) nor by the kernels, so only its first NCLV-1 species rows
+// are copied back and the caller's NCLV slice is left as it was.
+constexpr int kLocCld = 9;
+size_t out_rows(int i, size_t klev) { return i == kLocCld ? 4 * klev : rows(kArrs[i].kind, klev); }
 
 struct Workspace {
   int dev = -1;
@@ -601,7 +607,7 @@ int cloudsc_b200_block(
   const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
   for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
     if (!kArrs[i].out) continue;
-    size_t nrow = rows(kArrs[i].kind, kl);
+    size_t nrow = out_rows(i, kl);
     e = cudaMemcpy2DAsync((double *)host[i] + c0, np * 8, (double *)d[i] + c0, np * 8, ncol * 8, nrow,
                           cudaMemcpyDeviceToHost, s);
   }
@@ -688,12 +694,14 @@ int cloudsc_b200_batched_host(
       if (!kArrs[i].out) continue;
       size_t per = elems(kArrs[i].kind, np, kl) * 8;
       char *hb = (char *)host[i] + (size_t)b0 * per;
-      if (nfull > 0)
+      if (nfull > 0 && i == kLocCld)
+        e = cudaMemcpy2DAsync(hb, per, d[i], per, out_rows(i, kl) * np * 8, nfull, cudaMemcpyDeviceToHost,
+                              t_ws.st[2]);
+      else if (nfull > 0)
         e = cudaMemcpyAsync(hb, d[i], per * nfull, cudaMemcpyDeviceToHost, t_ws.st[2]);
       if (e == cudaSuccess && nfull < nb)
         e = cudaMemcpy2DAsync(hb + per * nfull, np * 8, (char *)d[i] + per * nfull, np * 8,
-                              (size_t)icend_last * 8, rows(kArrs[i].kind, kl), cudaMemcpyDeviceToHost,
-                              t_ws.st[2]);
+                              (size_t)icend_last * 8, out_rows(i, kl), cudaMemcpyDeviceToHost, t_ws.st[2]);
     }
     if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_out[slot], t_ws.st[2]);
   }
@@ -707,3 +715,4 @@ int cloudsc_b200_batched_host(
 }
 
 }  // extern "C"
+

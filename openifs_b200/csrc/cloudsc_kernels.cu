@@ -9,6 +9,10 @@
 #include <cstdint>
 
 #define CSC_DEV __device__ __forceinline__
+// Every column of a CTA meets the others at the end of each level, so all
+// warps of the CTA run the same stretch of the (very long) level code at the
+// same time and share the instruction cache.
+#define CSC_LEVEL_SYNC() __syncthreads()
 #include "cloudsc_column.cuh"
 
 #include "cloudsc_kparams.h"
@@ -40,16 +44,27 @@ __device__ __forceinline__ float xsign(float a, float b) { return copysignf(a, b
 
 namespace cloudsc {
 
+// Columns are numbered g = ib * NPROMA + jl over all blocks and dealt to CTAs
+// in tiles of blockDim.x consecutive columns (a warp reads 32 neighbouring
+// columns: coalesced).  The tile loop is uniform over the CTA and every thread
+// runs the level loop, so the per-level barrier is reached by all; a thread
+// whose column is outside KIDIA..ICEND computes a valid stand-in column and
+// stores nothing.
 template <bool F32M, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh) {
-  const int tpb = blockDim.x;
-  const int tiles_per_blk = (sh.nproma + tpb - 1) / tpb;
-  const int ntiles = sh.ngpblks * tiles_per_blk;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int ib = tile / tiles_per_blk;
-    const int jl = (tile - ib * tiles_per_blk) * tpb + threadIdx.x;
-    const int icend = min(sh.nproma, sh.ngptot - ib * sh.nproma);
-    if (jl >= sh.kidia0 && jl < icend) cloudsc_column<double, F32M>(F, sh, ib, jl);
+  const long long ncols = (long long)sh.ngpblks * sh.nproma;
+  const long long ntiles = (ncols + blockDim.x - 1) / blockDim.x;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long g = tile * blockDim.x + threadIdx.x;
+    int ib = (int)(g / sh.nproma);
+    int jl = (int)(g - (long long)ib * sh.nproma);
+    bool active = ib < sh.ngpblks;
+    if (active) active = jl >= sh.kidia0 && jl < min(sh.nproma, sh.ngptot - ib * sh.nproma);
+    if (!active) {
+      ib = 0;
+      jl = sh.kidia0;
+    }
+    cloudsc_column<double, F32M>(F, sh, ib, jl, active);
   }
 }
 
@@ -74,21 +89,19 @@ cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
   return e;
 }
 
-// Register budget: __launch_bounds__(CLOUDSC_MAXT, CLOUDSC_MINB).  128 threads
-// x 3 CTAs per SM caps the kernels at 168 registers (a few hundred bytes of
-// spills): 12 warps per SM hide more FP64 latency than 8 warps at 255
-// registers (measured 23.2 ms vs 28.6 ms for the FP64 kernel at 262,144
-// columns).
-// The FP32-mixed kernel is fastest with the full 255 registers (measured
-// 22.6 ms vs 27.7 ms at 168).
+// Register budget and CTA size: __launch_bounds__(MAXT, MINB).  One CTA of
+// 384 threads per SM caps the kernels at 168 registers (some hundred bytes of
+// spills) and keeps 12 warps in per-level lock-step; measured at 262,144
+// columns, FP64: 19.6 ms, against 21.7 ms for three 128-thread CTAs per SM
+// with the same barrier and 23.9 ms without it.
 #ifndef CLOUDSC_MAXT
-#define CLOUDSC_MAXT 128
+#define CLOUDSC_MAXT 384
 #endif
 #ifndef CLOUDSC_MINB
-#define CLOUDSC_MINB 3
+#define CLOUDSC_MINB 1
 #endif
 #ifndef CLOUDSC_MIX_MAXT
-#define CLOUDSC_MIX_MAXT 256
+#define CLOUDSC_MIX_MAXT 384
 #endif
 #ifndef CLOUDSC_MIX_MINB
 #define CLOUDSC_MIX_MINB 1

@@ -78,16 +78,17 @@ def test_edge_columns(cuda, case):
     _check(p, po, arrs, 64, 4, 256)
 
 
-@pytest.mark.parametrize("threads", [32, 64, 128])
+@pytest.mark.parametrize("threads", [32, 96, 128, 384])
 def test_launch_shapes(cuda, threads):
-    """Every supported CTA shape and a persistent grid give identical results."""
+    """CTA shapes that split, match and span NPROMA blocks (tiles cross block
+    boundaries), with a persistent grid, give identical results."""
     p, po = util.params()
     arrs = inputs.generate(6, 128, p, seed=31)
     try:
         cloudsc.set_launch(cloudsc.FP64, threads, 1)
         _check(p, po, arrs, 128, 6, 6 * 128 - 3)
     finally:
-        cloudsc.set_launch(cloudsc.FP64, 128, 0)
+        cloudsc.set_launch(cloudsc.FP64, 384, 0)
 
 
 def test_config2_sampled_blocks(cuda):
@@ -135,6 +136,8 @@ def test_host_pointer_paths(cuda):
     assert max(rep.values()) <= TOL, rep
     last = ngptot - (nblk - 1) * nproma
     assert np.all(host["tendency_loc_t"][-1, :, last:] == 7.0)
+    # PTENDENCY_LOC_CLD(:,:,NCLV) is never written
+    assert np.all(host["tendency_loc_cld"][:, 4] == 7.0)
 
     # per-block drop-in on block 2, columns 5..40 only (copies: PLUDE is INOUT)
     ib, kidia, kfdia = 2, 5, 40
@@ -152,6 +155,7 @@ def test_host_pointer_paths(cuda):
         assert np.array_equal(g[..., cols], o[..., cols]), n
         if n != "plude":
             assert np.all(g[..., :kidia - 1] == 7.0) and np.all(g[..., kfdia:] == 7.0), n
+    assert np.all(blk["tendency_loc_cld"][4] == 7.0)
 
 
 def test_mixed_precision_error(cuda):
