@@ -222,6 +222,43 @@ int cloudsc_b200_batched_host(
     double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
     int32_t precision, int32_t chunk_blocks);
 
+/*
+ * Per-block call that allocates no device memory.  No reference counterpart:
+ * the reference has no device memory at all; this entry exists for callers
+ * that must not allocate after start-up (memory-capped or pre-planned
+ * processes).  Same computation and results as cloudsc_b200_block (FP64),
+ * host pointers, the arrays the default configuration reads and writes, in
+ * cloudsc_b200_batched's order, plus `stream` (a cudaStream_t, NULL = the
+ * default stream) on which the copies and the kernel run; the call returns
+ * after the stream has finished them.
+ *
+ * Device memory: one fixed array inside the library of
+ * cloudsc_b200_block_noalloc_capacity() bytes (16 MiB), shared by every call
+ * in the process: 256 bytes + the block's arrays must fit, i.e. KLON <= 288
+ * at KLEV = 137; larger blocks return CLOUDSC_E_TOO_LARGE (use
+ * cloudsc_b200_block).  Calls are serialised by a lock inside the library;
+ * after a call the array keeps that call's inputs and outputs until the next
+ * call.  The first call on each device looks the array's address up and must
+ * not be made while a stream is being captured.
+ */
+int cloudsc_b200_block_noalloc(
+    const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_cld, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_cld, const double *pvfl,
+    const double *pvfi, const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis,
+    const double *plu, double *plude, const double *pludeli, const double *psnde,
+    const double *pmfu, const double *pmfd, const double *pa, const double *pclv,
+    double *pcovptot, double *prainfrac_toprfz, double *pfsqlf, double *pfsqif,
+    double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur,
+    double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn, void *stream);
+
+/* Bytes of the fixed device array cloudsc_b200_block_noalloc works in. */
+size_t cloudsc_b200_block_noalloc_capacity(void);
+
 /* sizeof(cloudsc_params) as compiled into the library (binding check). */
 size_t cloudsc_b200_params_size(void);
 

@@ -159,3 +159,31 @@ def cloudsc_block(params, kidia, kfdia, klon, klev, ptsphy, arrays, lddiag=False
         ctypes.byref(params), int(kidia), int(kfdia), int(klon), int(klev), int(bool(lddiag)),
         float(ptsphy), *a1, int(bool(ldslphy)), *a2, int(kfldx)))
 
+
+def cloudsc_block_noalloc(params, kidia, kfdia, klon, klev, ptsphy, arrays, stream=None):
+    """cloudsc_b200_block_noalloc: the per-block call that allocates no device
+    memory (it works in one fixed 16 MiB array inside the library; KLON <= 288
+    at KLEV 137).  ``arrays`` as for cloudsc_block (one block, host numpy
+    arrays); the arrays the default configuration reads and writes are
+    required.  Synchronous on ``stream`` (None = the default stream)."""
+    L = lib()
+    f = L.cloudsc_b200_block_noalloc
+    if f.argtypes is None:
+        vp = ctypes.c_void_p
+        f.argtypes = ([ctypes.POINTER(CloudscParams), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                       ctypes.c_int32, ctypes.c_double] + [vp] * len(BATCHED_FIELDS) + [vp])
+        f.restype = ctypes.c_int
+        L.cloudsc_b200_block_noalloc_capacity.restype = ctypes.c_size_t
+    args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
+    s = None
+    if stream is not None:
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+    return _check(f(ctypes.byref(params), int(kidia), int(kfdia), int(klon), int(klev), float(ptsphy),
+                    *args, s))
+
+
+def block_noalloc_capacity():
+    """Bytes of the fixed device array cloudsc_block_noalloc works in."""
+    L = lib()
+    L.cloudsc_b200_block_noalloc_capacity.restype = ctypes.c_size_t
+    return int(L.cloudsc_b200_block_noalloc_capacity())

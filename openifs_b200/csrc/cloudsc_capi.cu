@@ -716,3 +716,104 @@ int cloudsc_b200_batched_host(
 
 }  // extern "C"
 
+// ---------------------------------------------------------------------------
+// cloudsc_b200_block_noalloc: the per-block drop-in without any device
+// allocation.  Its device memory is one file-scope array, g_noalloc_scratch,
+// of kNoAllocBytes, shared by every call in the process; its address is
+// looked up once per device with cudaGetSymbolAddress.  Calls are serialised
+// by g_noalloc_mu (the array holds one block at a time).  After a call
+// returns, the array still holds that call's inputs and outputs until the
+// next call overwrites them.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocBytes = size_t(16) << 20;  // 16 MiB
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDev] = {nullptr};
+
+}  // namespace
+
+extern "C" {
+
+size_t cloudsc_b200_block_noalloc_capacity(void) { return kNoAllocBytes; }
+
+int cloudsc_b200_block_noalloc(
+    const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi, const double *pap,
+    const double *paph, const double *plsm, const int32_t *ldcum, const int32_t *ktype,
+    const double *peis, const double *plu, double *plude, const double *pludeli,
+    const double *psnde, const double *pmfu, const double *pmfd, const double *pa,
+    const double *pclv, double *pcovptot, double *prainfrac_toprfz, double *pfsqlf,
+    double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
+    double *pfplsn, double *pfhpsl, double *pfhpsn, void *stream) {
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
+    return fail(CLOUDSC_E_SHAPE, "inconsistent KIDIA/KFDIA/KLON/KLEV");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  const void *host[42] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+                          ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
+                          pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+                          pmfd, pa, pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng,
+                          pfsqrf, pfsqsf, pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl,
+                          pfhpsn};
+  for (const void *q : host)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  const size_t np = klon, kl = klev;
+  // the first 256 bytes hold the warning counter, the arrays follow
+  const size_t need = 256 + carve(nullptr, np, kl, 1, nullptr);
+  if (need > kNoAllocBytes) {
+    t_last_error = "cloudsc_b200_block_noalloc: this block needs " + std::to_string(need) +
+                   " bytes of device scratch, the fixed array holds " + std::to_string(kNoAllocBytes) +
+                   " (reduce KLON or use cloudsc_b200_block)";
+    return CLOUDSC_E_TOO_LARGE;
+  }
+  int dev = 0;
+  rc = ensure_params(&dev);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *a = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+    if (e != cudaSuccess || !a) return fail(CLOUDSC_E_CUDA, "cudaGetSymbolAddress(scratch)", e);
+    g_noalloc_ptr[dev] = a;
+  }
+  char *base = (char *)g_noalloc_ptr[dev];
+  uint32_t *counter = (uint32_t *)base;
+  void *d[42];
+  carve(base + 256, np, kl, 1, d);
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+    if (!kArrs[i].in) continue;
+    size_t esz = (i == 15 || i == 16) ? 4 : 8;
+    e = cudaMemcpyAsync(d[i], host[i], elems(kArrs[i].kind, np, kl) * esz, cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  Fields f = fields_from(d, counter);
+  Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
+  rc = launch_checked(0, f, sh, s);
+  if (rc) return rc;
+  const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
+  for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+    if (!kArrs[i].out) continue;
+    size_t nrow = out_rows(i, kl);
+    e = cudaMemcpy2DAsync((double *)host[i] + c0, np * 8, (double *)d[i] + c0, np * 8, ncol * 8, nrow,
+                          cudaMemcpyDeviceToHost, s);
+  }
+  uint32_t nwarn = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
+  return (int)nwarn;
+}
+
+}  // extern "C"
