@@ -57,7 +57,7 @@ template <typename T>
 CSC_DEV T mx(T a, T b) { return a > b ? a : b; }
 
 // Double precision uses the portable exp/pow of plibm.h (bit-identical on the
-// host and the GPU); single precision uses the CUDA/C library.
+// host and the GPU).
 #if defined(CLOUDSC_HOST_LIBM_GLIBC) && !defined(__CUDA_ARCH__)
 // host test builds only: the system libm, to measure libm sensitivity
 CSC_DEV double xexp(double x) { return exp(x); }
@@ -66,19 +66,41 @@ CSC_DEV double xpow(double x, double y) { return pow(x, y); }
 CSC_DEV double xexp(double x) { return plibm_exp(x); }
 CSC_DEV double xpow(double x, double y) { return plibm_pow(x, y); }
 #endif
-CSC_DEV float xexp(float x) { return expf(x); }
+// FP32 transcendentals of the FP32-mixed kernel: on the GPU the special-
+// function-unit forms (__expf, __powf: one ex2 / lg2 each, relative error of a
+// few 1e-7 times the size of the exponent's argument), on the host the C
+// library; exponents 0.5, 1.5, 2 and 3 are evaluated exactly as roots and
+// products, as plibm does in double.
+CSC_DEV float xexp(float x) {
+#if defined(__CUDA_ARCH__)
+  return __expf(x);
+#else
+  return expf(x);
+#endif
+}
+CSC_DEV float xpow(float x, float y) {
+  if (y == 0.5f) return sqrtf(x);
+  if (y == 1.5f) return x * sqrtf(x);
+  if (y == 2.0f) return x * x;
+  if (y == 3.0f) return x * x * x;
+#if defined(__CUDA_ARCH__)
+  return __powf(x, y);
+#else
+  return powf(x, y);
+#endif
+}
 
 // Transcendentals of the microphysics: FP64 (plibm) in the FP64 kernel,
-// FP32 (the CUDA/C library's expf/powf on the rounded argument) in the
-// FP32-mixed kernel.  Everything else in both kernels is FP64.
+// FP32 (xexp/xpow above, on the argument rounded to float) in the FP32-mixed
+// kernel.  Everything else in both kernels is FP64.
 template <bool F32>
 CSC_DEV double mexp(double x) {
-  if (F32) return (double)expf((float)x);
+  if (F32) return (double)xexp((float)x);
   return xexp(x);
 }
 template <bool F32>
 CSC_DEV double mpow(double x, double y) {
-  if (F32) return (double)powf((float)x, (float)y);
+  if (F32) return (double)xpow((float)x, (float)y);
   return xpow(x, y);
 }
 
@@ -101,14 +123,13 @@ CSC_DEV PowBase mbase(double x) {
 }
 template <bool F32>
 CSC_DEV double mpowb(const PowBase &b, double y) {
-  if (F32) return (double)powf((float)b.x, (float)y);
+  if (F32) return (double)xpow((float)b.x, (float)y);
 #if defined(CLOUDSC_HOST_LIBM_GLIBC) && !defined(__CUDA_ARCH__)
   return pow(b.x, y);
 #else
   return plibm_pow_with_log(b.x, y, b.lhi, b.llo);
 #endif
 }
-CSC_DEV float xpow(float x, float y) { return powf(x, y); }
 CSC_DEV double xsqrt(double x) { return sqrt(x); }
 CSC_DEV float xsqrt(float x) { return sqrtf(x); }
 
