@@ -224,9 +224,11 @@ int cloudsc_b200_batched_host(
 
 /*
  * Per-block call that allocates no device memory.  No reference counterpart:
- * the reference has no device memory at all; this entry exists for callers
- * that must not allocate after start-up (memory-capped or pre-planned
- * processes).  Same computation and results as cloudsc_b200_block (FP64),
+ * the reference has no device memory at all.  This entry is for callers that
+ * cannot call cudaMalloc: a model run whose GPU memory is fully reserved up
+ * front by its own pool or arena, where a later allocation fails or would
+ * fragment it, and drivers that must not allocate between time steps.  Same
+ * computation and results as cloudsc_b200_block (FP64),
  * host pointers, the arrays the default configuration reads and writes, in
  * cloudsc_b200_batched's order, plus `stream` (a cudaStream_t, NULL = the
  * default stream) on which the copies and the kernel run; the call returns
@@ -236,10 +238,13 @@ int cloudsc_b200_batched_host(
  * cloudsc_b200_block_noalloc_capacity() bytes (16 MiB), shared by every call
  * in the process: 256 bytes + the block's arrays must fit, i.e. KLON <= 288
  * at KLEV = 137; larger blocks return CLOUDSC_E_TOO_LARGE (use
- * cloudsc_b200_block).  Calls are serialised by a lock inside the library;
- * after a call the array keeps that call's inputs and outputs until the next
- * call.  The first call on each device looks the array's address up and must
- * not be made while a stream is being captured.
+ * cloudsc_b200_block).  Two calls whose GPU work overlapped would race on
+ * the shared array; to prevent that, calls are serialised by a lock inside
+ * the library and each returns only after its stream has finished.  After a
+ * call the array keeps that call's inputs and outputs until the next call
+ * (the warning counter is cleared at the start of each call).  The first call
+ * on each device looks the array's address up and should come before any
+ * stream capture.
  */
 int cloudsc_b200_block_noalloc(
     const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,

@@ -728,7 +728,7 @@ int cloudsc_b200_batched_host(
 namespace {
 
 constexpr size_t kNoAllocBytes = size_t(16) << 20;  // 16 MiB
-__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[kMaxDev] = {nullptr};
