@@ -43,7 +43,8 @@ def _sources():
 
 def _digest(paths):
     h = hashlib.sha256()
-    for p in paths + [os.path.join(ROOT, "include", "cloudsc_b200.h")]:
+    inc = os.path.join(ROOT, "include")
+    for p in paths + sorted(os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")):
         with open(p, "rb") as f:
             h.update(p.encode())
             h.update(f.read())
