@@ -50,6 +50,107 @@ typedef struct cs_gemm_desc {
  * (tcgen05, one persistent CTA per SM). */
 int cs_conv_gemm(const cs_gemm_desc *g, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Column data in CLOUDSC's batched storage (NPROMA, dims, NGPBLKS), device
+ * pointers, double precision (LDCUM int32).  Column c = ib * NPROMA + jl.
+ * The surrogate reads the inputs and writes LOC_T, LOC_Q, LOC_A, LOC_CLD(1:4),
+ * PLUDE, PFPLSL/PFPLSN and PFHPSL/PFHPSN; it predicts no DDH flux.
+ */
+typedef struct cs_columns {
+  const double *pt, *pq, *pap, *paph, *pclv, *pa, *pmfu, *pmfd;
+  const double *cml_t, *cml_q, *cml_a, *cml_cld, *plu, *pludeli, *psnde;
+  const int32_t *ldcum;
+  double *plude; /* INOUT: read as the input detrainment, written as CLOUDSC does */
+  double *loc_t, *loc_q, *loc_a, *loc_cld, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
+  int32_t nproma, klev, ngpblks, lp; /* lp: padded rows per column (>= klev + 4) */
+} cs_columns;
+
+#define CS_NIN 14   /* input channels per level  */
+#define CS_NOUT 9   /* output channels per level */
+
+/* Input feature transform: f = use_log ? log(x + eps) : x; (f - mean) * inv_std */
+typedef struct cs_norm {
+  float mean[16], inv_std[16], eps[16];
+  int32_t use_log[16];
+} cs_norm;
+
+/* Network input: x0[c*lp + 2 + l][tap*16 + ch] = feature ch of level l+tap-2
+ * (zero outside the column); bf16 [ncol*lp][128]. */
+int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream);
+/* Raw (untransformed) input features, f32 [ncol*lp][16], for statistics. */
+int cs_raw_features(const cs_columns *c, float *feat, void *stream);
+/* Training targets from CLOUDSC's outputs, divided by scale[ch]: f32
+ * [ncol*lp][16] (LOC_T, LOC_Q, LOC_A, LOC_CLD l,i,r,s, PFPLSL, PFPLSN at the
+ * half level below the level). */
+int cs_prep_targets(const cs_columns *c, const float *scale16, float *t, void *stream);
+
+/* Training batch from stored features: for j < nb, batch column j is data
+ * column cols[j] (device int32): x0 (bf16 [nb*lp][128]) as cs_prep_inputs
+ * builds it from feat (f32 [*][16], cs_raw_features layout), and tb (f32
+ * [nb*lp][16]) copied from tgt (cs_prep_targets layout). */
+int cs_prep_batch(const float *feat, const float *tgt, const int32_t *cols, int32_t nb, int32_t lp,
+                  int32_t klev, const cs_norm *nrm, void *x0, float *tb, void *stream);
+
+/* MSE loss over valid rows and the first CS_NOUT channels of each of the
+ * nheads (1 or 2) output heads; y f32 and dy bf16 are [rows][64 * nheads]
+ * (head h in columns 64h..64h+CS_NOUT-1):
+ * dy = 2 w (y - t) / count, loss_sum += sum w (y - t)^2 / count. */
+int cs_loss(const float *y, const float *t, int32_t rows, int32_t lp, int32_t klev, const float *w16,
+            int32_t nheads, void *dy, double *loss_sum, void *stream);
+
+/* dw[t][n][k] += sum_r dz[r][n] * x[r + t - taps/2][k] (f32, CUDA cores);
+ * db[n] += sum_r dz[r][n] when db is not NULL. */
+int cs_wgrad(const void *dz, const void *x, int32_t rows, int32_t n, int32_t k, int32_t taps, float *dw,
+             float *db, void *stream);
+
+typedef struct cs_adam {
+  float lr, beta1, beta2, eps, weight_decay, bc1, bc2; /* bc = 1 - beta^step */
+} cs_adam;
+/* AdamW step on f32 master weights p [taps][n][k] (or a bias: taps = 1,
+ * k = 1); zeroes g; writes bf16 copies w (same layout) and wt
+ * ([taps][k][n], taps reversed: the backward-data operand) when not NULL. */
+int cs_adamw(float *p, float *g, float *m, float *v, int32_t taps, int32_t n, int32_t k, const cs_adam *hp,
+             void *w, void *wt, void *stream);
+
+/* Guard of the surrogate's output.  The small parameter structs (cs_norm,
+ * cs_adam, cs_guard) and the w16 / scale16 arrays of the calls above and
+ * below are read from HOST memory at the call; everything else is device
+ * memory. */
+typedef struct cs_guard {
+  float out_scale[16];   /* de-normalisation of the network outputs            */
+  double rg, ralvdcp, ralsdcp, rlvtt, rlstt, ptsphy;
+  int32_t ncldtop;       /* first level of CLOUDSC's level loop (1-based)      */
+  double neg_tol;        /* condensate after the step below -neg_tol: flag      */
+  double closure_tol;    /* raw water/enthalpy non-closure above this: flag     */
+  double spread_tol;     /* RMS head disagreement (normalised) above this: flag */
+  int32_t capacity;      /* length of the flagged-column list                   */
+} cs_guard;
+
+/* Turn the network output y ([rows][64 * nheads] f32) into CLOUDSC
+ * outputs: mean of the heads, de-normalised; surface precipitation
+ * diagnosed from the column water budget and the temperature tendency
+ * shifted by a column constant so that water and enthalpy close exactly;
+ * PLUDE and the enthalpy fluxes as CLOUDSC defines them.  Columns failing the
+ * guard are appended to flagged[0..capacity) (count in *nflagged, which must
+ * start at 0); diag (float4 per column, or NULL) = {raw water non-closure,
+ * raw enthalpy non-closure, head spread, flagged}. */
+int cs_post(const cs_columns *c, const float *y, int32_t nheads, const cs_guard *g, int32_t *nflagged,
+            int32_t *flagged, float *diag, void *stream);
+
+/* One array of column data for cs_move_columns: per-column rows and element
+ * size, base pointers in two batched layouts. */
+typedef struct cs_colarray {
+  const void *src;
+  void *dst;
+  int32_t rows, esize;
+} cs_colarray;
+/* gather (dir 0): dst column j <- src column idx[min(j, n-1)] for j < cap,
+ *                 n = min(*count, cap) (all from column 0 when n = 0);
+ * scatter (dir 1): dst column idx[j] <- src column j for j < n.
+ * arrays: device array of narr descriptors. */
+int cs_move_columns(const cs_colarray *arrays, int32_t narr, int32_t nproma_src, int32_t nproma_dst,
+                    const int32_t *idx, const int32_t *count, int32_t cap, int32_t dir, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,568 @@
+// Data, training and guard kernels of the learned CLOUDSC surrogate (sm_100a).
+// The network's GEMMs are in surrogate_gemm.cu; see include/cloudsc_surrogate.h
+// for the interfaces.
+//
+// Column budgets used by the guard (both hold to rounding for CLOUDSC itself;
+// the oracle tests check them):
+//   water     sum_k dp/g (LOC_Q + LOC_L + LOC_I + LOC_R + LOC_S)
+//               = S_l + S_i + S_r + S_s - P_rain - P_snow
+//   enthalpy  sum_k dp/g (LOC_T - RALVDCP (LOC_L + LOC_R) - RALSDCP (LOC_I + LOC_S))
+//               = RALVDCP (P_rain - S_l - S_r) + RALSDCP (P_snow - S_i - S_s)
+// with S the column sums of the convective detrainment sources CLOUDSC applies
+// (PLUDELI where PLUDE is detrained, PSNDE on the loop levels, cloudsc.F90:
+// 1362-1398) and P the surface precipitation fluxes (PFPLSL, PFPLSN at KLEV+1).
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <string.h>
+#include "cloudsc_surrogate.h"
+
+namespace sk {
+
+constexpr double ZEPSEC = 1.0e-14;
+
+// 16 floats passed by value (host arrays of the C ABI)
+struct F16 {
+  float v[16];
+};
+
+struct Cols {
+  cs_columns c;
+  __device__ __forceinline__ size_t o2(int col, int k) const {  // (NPROMA,KLEV) element
+    const int ib = col / c.nproma, jl = col - ib * c.nproma;
+    return ((size_t)ib * c.klev + k) * c.nproma + jl;
+  }
+  __device__ __forceinline__ size_t oh(int col, int k) const {  // (NPROMA,KLEV+1)
+    const int ib = col / c.nproma, jl = col - ib * c.nproma;
+    return ((size_t)ib * (c.klev + 1) + k) * c.nproma + jl;
+  }
+  __device__ __forceinline__ size_t o3(int col, int m, int n, int k) const {  // (NPROMA,KLEV,n)
+    const int ib = col / c.nproma, jl = col - ib * c.nproma;
+    return (((size_t)ib * n + m) * c.klev + k) * c.nproma + jl;
+  }
+  __device__ __forceinline__ size_t o1(int col) const { return (size_t)col; }
+};
+
+// The 14 raw input features of (column, level): T, q, p, the four
+// condensates, PLUDE (detrained condensate), cloud fraction, the convective
+// mass flux PMFU + PMFD, and the forcing tendencies of T, q, a and l + i.
+__device__ __forceinline__ void raw_features(const Cols &C, int col, int k, float f[CS_NIN]) {
+  const cs_columns &c = C.c;
+  const size_t o = C.o2(col, k);
+  f[0] = (float)c.pt[o];
+  f[1] = (float)c.pq[o];
+  f[2] = (float)c.pap[o];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) f[3 + m] = (float)c.pclv[C.o3(col, m, 5, k)];
+  f[7] = (float)c.plude[o];
+  f[8] = (float)c.pa[o];
+  f[9] = (float)(c.pmfu[o] + c.pmfd[o]);
+  f[10] = (float)c.cml_t[o];
+  f[11] = (float)c.cml_q[o];
+  f[12] = (float)c.cml_a[o];
+  f[13] = (float)(c.cml_cld[C.o3(col, 0, 5, k)] + c.cml_cld[C.o3(col, 1, 5, k)]);
+}
+
+// Threads are numbered level-major (row r of every column, then the next
+// row) so that a warp reads one level of 32 neighbouring columns.
+__global__ void raw_features_kernel(Cols C, float *feat) {
+  const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp;
+  const long long n = (long long)ncol * lp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
+    const int k = r - 2;
+    float f[CS_NIN];
+    if (k >= 0 && k < C.c.klev) {
+      raw_features(C, col, k, f);
+    } else {
+#pragma unroll
+      for (int i = 0; i < CS_NIN; ++i) f[i] = 0.0f;
+    }
+    float4 *d = (float4 *)(feat + ((size_t)col * lp + r) * 16);
+    d[0] = make_float4(f[0], f[1], f[2], f[3]);
+    d[1] = make_float4(f[4], f[5], f[6], f[7]);
+    d[2] = make_float4(f[8], f[9], f[10], f[11]);
+    d[3] = make_float4(f[12], f[13], 0.0f, 0.0f);
+  }
+}
+
+__global__ void prep_inputs_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *x0) {
+  const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
+  const long long n = (long long)ncol * lp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
+    const int k = r - 2;
+    __align__(16) __nv_bfloat16 row[128];
+#pragma unroll
+    for (int i = 0; i < 128; ++i) row[i] = __float2bfloat16(0.0f);
+    if (k >= 0 && k < klev) {
+#pragma unroll 1
+      for (int tap = 0; tap < 5; ++tap) {
+        const int ks = k + tap - 2;
+        if (ks < 0 || ks >= klev) continue;
+        float f[CS_NIN];
+        raw_features(C, col, ks, f);
+#pragma unroll
+        for (int ch = 0; ch < CS_NIN; ++ch) {
+          float x = f[ch];
+          if (nrm.use_log[ch]) x = __logf(fmaxf(x, 0.0f) + nrm.eps[ch]);
+          row[tap * 16 + ch] = __float2bfloat16((x - nrm.mean[ch]) * nrm.inv_std[ch]);
+        }
+      }
+    }
+    uint4 *d = (uint4 *)(x0 + ((size_t)col * lp + r) * 128);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) d[i] = ((uint4 *)row)[i];
+  }
+}
+
+__global__ void prep_targets_kernel(Cols C, F16 scale, float *tgt) {
+  const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
+  const long long n = (long long)ncol * lp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
+    const int k = r - 2;
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+    if (k >= 0 && k < klev) {
+      const cs_columns &c = C.c;
+      const size_t o = C.o2(col, k);
+      v[0] = (float)c.loc_t[o];
+      v[1] = (float)c.loc_q[o];
+      v[2] = (float)c.loc_a[o];
+#pragma unroll
+      for (int m = 0; m < 4; ++m) v[3 + m] = (float)c.loc_cld[C.o3(col, m, 5, k)];
+      v[7] = (float)c.pfplsl[C.oh(col, k + 1)];
+      v[8] = (float)c.pfplsn[C.oh(col, k + 1)];
+#pragma unroll
+      for (int i = 0; i < CS_NOUT; ++i) v[i] = v[i] / scale.v[i];
+    }
+    float4 *d = (float4 *)(tgt + ((size_t)col * lp + r) * 16);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+  }
+}
+
+// Training batch: thread per (batch row r, batch column j), level-major.
+__global__ void prep_batch_kernel(const float *__restrict__ feat, const float *__restrict__ tgt,
+                                  const int *__restrict__ cols, int nb, int lp, int klev, cs_norm nrm,
+                                  __nv_bfloat16 *x0, float *tb) {
+  const long long n = (long long)nb * lp;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(t / nb), j = (int)(t - (long long)r * nb);
+    const size_t src = (size_t)cols[j] * lp;
+    const int k = r - 2;
+    __align__(16) __nv_bfloat16 row[128];
+#pragma unroll
+    for (int i = 0; i < 128; ++i) row[i] = __float2bfloat16(0.0f);
+    if (k >= 0 && k < klev) {
+#pragma unroll
+      for (int tap = 0; tap < 5; ++tap) {
+        const int ks = k + tap - 2;
+        if (ks < 0 || ks >= klev) continue;
+        const float4 *f4 = (const float4 *)(feat + (src + 2 + ks) * 16);
+        float f[16];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float4 v = f4[q];
+          f[4 * q] = v.x;
+          f[4 * q + 1] = v.y;
+          f[4 * q + 2] = v.z;
+          f[4 * q + 3] = v.w;
+        }
+#pragma unroll
+        for (int ch = 0; ch < CS_NIN; ++ch) {
+          float x = f[ch];
+          if (nrm.use_log[ch]) x = __logf(fmaxf(x, 0.0f) + nrm.eps[ch]);
+          row[tap * 16 + ch] = __float2bfloat16((x - nrm.mean[ch]) * nrm.inv_std[ch]);
+        }
+      }
+    }
+    uint4 *d = (uint4 *)(x0 + ((size_t)j * lp + r) * 128);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) d[i] = ((uint4 *)row)[i];
+    const float4 *ts = (const float4 *)(tgt + (src + r) * 16);
+    float4 *td = (float4 *)(tb + ((size_t)j * lp + r) * 16);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) td[i] = ts[i];
+  }
+}
+
+// ---------------------------------------------------------------- loss
+__global__ void loss_kernel(const float *__restrict__ y, const float *__restrict__ tg, int rows, int lp, int klev,
+                            F16 w, int nheads, float inv_count, __nv_bfloat16 *dy, double *loss_sum) {
+  const int ys = 64 * nheads;
+  double acc = 0.0;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const int pos = r % lp;
+    const bool valid = pos >= 2 && pos < 2 + klev;
+    for (int h = 0; h < nheads; ++h) {
+      __align__(16) __nv_bfloat16 g[64];
+#pragma unroll
+      for (int i = 0; i < 64; ++i) g[i] = __float2bfloat16(0.0f);
+      if (valid) {
+#pragma unroll
+        for (int i = 0; i < CS_NOUT; ++i) {
+          const float d = y[(size_t)r * ys + 64 * h + i] - tg[(size_t)r * 16 + i];
+          acc += (double)(w.v[i] * d * d * inv_count);
+          g[i] = __float2bfloat16(2.0f * w.v[i] * d * inv_count);
+        }
+      }
+      uint4 *dd = (uint4 *)(dy + (size_t)r * ys + 64 * h);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) dd[i] = ((uint4 *)g)[i];
+    }
+  }
+  // block reduction of the loss
+  __shared__ double red[256];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) atomicAdd(loss_sum, red[0]);
+}
+
+// ---------------------------------------------------------------- gradients
+// One CTA: tap t, a 64 x 64 tile of (n, k), a chunk of rows; 256 threads with
+// 4 x 4 outputs each, rows staged 32 at a time in shared memory.
+constexpr int WG_CHUNK = 2048;
+__global__ void __launch_bounds__(256) wgrad_kernel(const __nv_bfloat16 *__restrict__ dz,
+                                                    const __nv_bfloat16 *__restrict__ x, int rows, int n, int k,
+                                                    int taps, float *dw) {
+  __shared__ float sd[32][64 + 4];
+  __shared__ float sx[32][64 + 4];
+  const int t = blockIdx.z;
+  const int ktiles = k / 64;
+  const int n0 = (blockIdx.y / ktiles) * 64, k0 = (blockIdx.y % ktiles) * 64;
+  const int r0 = blockIdx.x * WG_CHUNK, r1 = min(rows, r0 + WG_CHUNK);
+  const int shift = t - taps / 2;
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  float acc[4][4] = {};
+  for (int rr = r0; rr < r1; rr += 32) {
+    for (int e = tid; e < 32 * 64; e += 256) {
+      const int i = e >> 6, j = e & 63;
+      const int r = rr + i;
+      sd[i][j] = r < r1 ? __bfloat162float(dz[(size_t)r * n + n0 + j]) : 0.0f;
+      const int rx = r + shift;
+      sx[i][j] = (r < r1 && rx >= 0 && rx < rows) ? __bfloat162float(x[(size_t)rx * k + k0 + j]) : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int i = 0; i < 32; ++i) {
+      float a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = sd[i][ty * 4 + q];
+        b[q] = sx[i][tx * 4 + q];
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      atomicAdd(&dw[((size_t)t * n + n0 + ty * 4 + p) * k + k0 + tx * 4 + q], acc[p][q]);
+}
+
+__global__ void bgrad_kernel(const __nv_bfloat16 *__restrict__ dz, int rows, int n, float *db) {
+  const int r0 = blockIdx.x * WG_CHUNK, r1 = min(rows, r0 + WG_CHUNK);
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    float s = 0.0f;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(dz[(size_t)r * n + j]);
+    atomicAdd(&db[j], s);
+  }
+}
+
+// ---------------------------------------------------------------- AdamW
+__global__ void adamw_kernel(float *p, float *g, float *m, float *v, int taps, int n, int k, cs_adam hp,
+                             __nv_bfloat16 *w, __nv_bfloat16 *wt) {
+  const long long cnt = (long long)taps * n * k;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = hp.beta1 * m[i] + (1.0f - hp.beta1) * gi;
+    const float vi = hp.beta2 * v[i] + (1.0f - hp.beta2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    g[i] = 0.0f;
+    float pi = p[i];
+    pi -= hp.lr * ((mi / hp.bc1) / (sqrtf(vi / hp.bc2) + hp.eps) + hp.weight_decay * pi);
+    p[i] = pi;
+    if (w) w[i] = __float2bfloat16(pi);
+    if (wt) {
+      const int t = (int)(i / ((long long)n * k));
+      const int rem = (int)(i - (long long)t * n * k);
+      const int nn = rem / k, kk = rem - nn * k;
+      wt[((size_t)(taps - 1 - t) * k + kk) * n + nn] = __float2bfloat16(pi);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- guard
+// One thread per column.  Pass 1 over the levels: de-normalise, write the
+// outputs, accumulate the budgets and the guard quantities; then the surface
+// precipitation from the water budget and a column-constant LOC_T shift that
+// closes the enthalpy budget; pass 2 applies the shift and writes the
+// enthalpy fluxes.
+__global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_guard gd, int *nflagged,
+                            int *flagged, float4 *diag) {
+  const int ys = 64 * nheads;
+  const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
+  const int k0 = gd.ncldtop - 1;  // first level of CLOUDSC's level loop
+  const double dt = gd.ptsphy, rg = gd.rg;
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += gridDim.x * blockDim.x) {
+    const cs_columns &c = C.c;
+    double w_lhs = 0.0, w_abs = 0.0, e_lhs = 0.0, e_abs = 0.0;
+    double s_l = 0.0, s_i = 0.0, s_r = 0.0, s_s = 0.0, mass = 0.0, spread2 = 0.0;
+    int spread_n = 0;
+    bool negative = false;
+    const bool ldcum = c.ldcum[C.o1(col)] != 0;
+    double pr_pred = 0.0, ps_pred = 0.0;
+    for (int k = 0; k < klev; ++k) {
+      const size_t r = (size_t)col * lp + 2 + k;
+      float yv[CS_NOUT];
+#pragma unroll
+      for (int i = 0; i < CS_NOUT; ++i) {
+        float a = y[r * ys + i];
+        if (nheads == 2) {
+          const float b = y[r * ys + 64 + i];
+          if (i < 7) {
+            spread2 += (double)(a - b) * (double)(a - b);
+            ++spread_n;
+          }
+          a = 0.5f * (a + b);
+        }
+        yv[i] = a * gd.out_scale[i];
+      }
+      const size_t o = C.o2(col, k);
+      const double dp = c.paph[C.oh(col, k + 1)] - c.paph[C.oh(col, k)];
+      const double dpg = dp / rg;
+      const double lt = yv[0], lq = yv[1], la = yv[2], ll = yv[3], li = yv[4], lr = yv[5], ls = yv[6];
+      c.loc_t[o] = lt;
+      c.loc_q[o] = lq;
+      c.loc_a[o] = la;
+      c.loc_cld[C.o3(col, 0, 5, k)] = ll;
+      c.loc_cld[C.o3(col, 1, 5, k)] = li;
+      c.loc_cld[C.o3(col, 2, 5, k)] = lr;
+      c.loc_cld[C.o3(col, 3, 5, k)] = ls;
+      if (k + 1 < klev) {
+        c.pfplsl[C.oh(col, k + 1)] = fmax((double)yv[7], 0.0);
+        c.pfplsn[C.oh(col, k + 1)] = fmax((double)yv[8], 0.0);
+      } else {
+        pr_pred = fmax((double)yv[7], 0.0);
+        ps_pred = fmax((double)yv[8], 0.0);
+      }
+      // convective detrainment exactly as CLOUDSC applies it (cloudsc.F90:1362-1398)
+      if (k >= k0 && k + 1 < klev) {
+        const double zdtgdp = dt * (rg / dp);  // ZDTGDP = PTSPHY * ZGDP, ZGDP = RG / ZDP
+        const double pl = c.plude[o] * zdtgdp;
+        const double plu1 = c.plu[C.o2(col, k + 1)];
+        double plude_out = 0.0;
+        if (ldcum && pl > ZEPSEC && plu1 > ZEPSEC) {
+          plude_out = pl;
+          s_l += c.pludeli[C.o3(col, 0, 4, k)];
+          s_i += c.pludeli[C.o3(col, 1, 4, k)];
+        }
+        s_r += c.psnde[C.o3(col, 0, 2, k)];
+        s_s += c.psnde[C.o3(col, 1, 2, k)];
+        c.plude[o] = plude_out;
+      }
+      w_lhs += dpg * (lq + ll + li + lr + ls);
+      w_abs += fabs(dpg * lq) + fabs(dpg * (ll + li + lr + ls));
+      e_lhs += dpg * (lt - gd.ralvdcp * (ll + lr) - gd.ralsdcp * (li + ls));
+      e_abs += fabs(dpg * lt);
+      mass += dpg;
+      // the condensates after the step must not go negative
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const double q = c.pclv[C.o3(col, m, 5, k)] + dt * (c.cml_cld[C.o3(col, m, 5, k)] + (double)yv[3 + m]);
+        if (q < -gd.neg_tol) negative = true;
+      }
+    }
+    // surface precipitation from the water budget, split as the heads predict
+    const double ptot = (s_l + s_i + s_r + s_s) - w_lhs;
+    const double praw = pr_pred + ps_pred;
+    const double w_raw = fabs(praw - ptot) / (w_abs + fabs(ptot) + fabs(praw) + 1e-30);
+    const double frac = praw > 0.0 ? pr_pred / praw : 0.5;
+    const double pr = frac * ptot, ps = ptot - pr;
+    c.pfplsl[C.oh(col, klev)] = pr;
+    c.pfplsn[C.oh(col, klev)] = ps;
+    c.pfplsl[C.oh(col, 0)] = 0.0;
+    c.pfplsn[C.oh(col, 0)] = 0.0;
+    // enthalpy: a column-constant LOC_T shift closes the budget
+    const double e_rhs = gd.ralvdcp * (pr - s_l - s_r) + gd.ralsdcp * (ps - s_i - s_s);
+    const double e_res = e_lhs - e_rhs;
+    const double e_raw = fabs(e_res) / (e_abs + fabs(e_rhs) + 1e-30);
+    const double shift = e_res / mass;
+    for (int k = 0; k < klev; ++k) {
+      const size_t o = C.o2(col, k);
+      c.loc_t[o] = c.loc_t[o] - shift;
+    }
+    for (int k = 0; k <= klev; ++k) {
+      const size_t oo = C.oh(col, k);
+      c.pfhpsl[oo] = -gd.rlvtt * c.pfplsl[oo];
+      c.pfhpsn[oo] = -gd.rlstt * c.pfplsn[oo];
+    }
+    const double spread = spread_n ? sqrt(spread2 / spread_n) : 0.0;
+    const bool flag = negative || ptot < 0.0 || w_raw > gd.closure_tol || e_raw > gd.closure_tol ||
+                      (nheads == 2 && spread > gd.spread_tol);
+    if (diag) diag[col] = make_float4((float)w_raw, (float)e_raw, (float)spread, flag ? 1.0f : 0.0f);
+    if (flag) {
+      const int slot = atomicAdd(nflagged, 1);
+      if (slot < gd.capacity) flagged[slot] = col;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- column moves
+__global__ void move_columns_kernel(const cs_colarray *__restrict__ arrays, int narr, int nps, int npd,
+                                    const int *__restrict__ idx, const int *__restrict__ count, int cap,
+                                    int dir) {
+  const int n = min(*count, cap);
+  const int ncols = dir == 0 ? cap : n;
+  // blockIdx.y: array; threads over (row, slot j) with j fastest
+  const int a = blockIdx.y;
+  if (a >= narr) return;
+  const cs_colarray A = arrays[a];
+  const long long total = (long long)A.rows * ncols;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    const int row = (int)(t / ncols), j = (int)(t - (long long)row * ncols);
+    int cs, cd;
+    if (dir == 0) {
+      cs = n > 0 ? idx[min(j, n - 1)] : 0;
+      cd = j;
+    } else {
+      cs = j;
+      cd = idx[j];
+    }
+    const int ibs = cs / nps, jls = cs - ibs * nps, ibd = cd / npd, jld = cd - ibd * npd;
+    const size_t os = ((size_t)ibs * A.rows + row) * nps + jls;
+    const size_t od = ((size_t)ibd * A.rows + row) * npd + jld;
+    if (A.esize == 8)
+      ((double *)A.dst)[od] = ((const double *)A.src)[os];
+    else
+      ((int32_t *)A.dst)[od] = ((const int32_t *)A.src)[os];
+  }
+}
+
+int grid_1d(long long n, int threads) {
+  long long g = (n + threads - 1) / threads;
+  const long long cap = 148LL * 32;
+  return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+bool cols_ok(const cs_columns *c) {
+  return c && c->nproma > 0 && c->klev > 0 && c->ngpblks > 0 && c->lp >= c->klev + 4;
+}
+
+}  // namespace sk
+
+extern "C" {
+
+int cs_raw_features(const cs_columns *c, float *feat, void *stream) {
+  using namespace sk;
+  if (!cols_ok(c) || !feat) return CS_E_ARG;
+  Cols C{*c};
+  const long long n = (long long)c->nproma * c->ngpblks * c->lp;
+  raw_features_kernel<<<grid_1d(n, 256), 256, 0, (cudaStream_t)stream>>>(C, feat);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream) {
+  using namespace sk;
+  if (!cols_ok(c) || !nrm || !x0) return CS_E_ARG;
+  Cols C{*c};
+  const long long n = (long long)c->nproma * c->ngpblks * c->lp;
+  prep_inputs_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)x0);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_prep_targets(const cs_columns *c, const float *scale16, float *t, void *stream) {
+  using namespace sk;
+  if (!cols_ok(c) || !scale16 || !t) return CS_E_ARG;
+  Cols C{*c};
+  const long long n = (long long)c->nproma * c->ngpblks * c->lp;
+  F16 sc;
+  memcpy(sc.v, scale16, sizeof(sc.v));
+  prep_targets_kernel<<<grid_1d(n, 256), 256, 0, (cudaStream_t)stream>>>(C, sc, t);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_prep_batch(const float *feat, const float *tgt, const int32_t *cols, int32_t nb, int32_t lp, int32_t klev,
+                  const cs_norm *nrm, void *x0, float *tb, void *stream) {
+  using namespace sk;
+  if (!feat || !tgt || !cols || nb <= 0 || lp < klev + 4 || !nrm || !x0 || !tb) return CS_E_ARG;
+  const long long n = (long long)nb * lp;
+  prep_batch_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(feat, tgt, cols, nb, lp, klev, *nrm,
+                                                                       (__nv_bfloat16 *)x0, tb);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_loss(const float *y, const float *t, int32_t rows, int32_t lp, int32_t klev, const float *w16,
+            int32_t nheads, void *dy, double *loss_sum, void *stream) {
+  using namespace sk;
+  if (!y || !t || !w16 || !dy || !loss_sum || rows <= 0 || lp < klev + 4 || nheads < 1 || nheads > 2)
+    return CS_E_ARG;
+  const long long nvalid = (long long)(rows / lp) * klev * CS_NOUT;
+  const float inv = 1.0f / (float)(nvalid > 0 ? nvalid : 1);
+  F16 w;
+  memcpy(w.v, w16, sizeof(w.v));
+  loss_kernel<<<grid_1d(rows, 256), 256, 0, (cudaStream_t)stream>>>(y, t, rows, lp, klev, w, nheads, inv,
+                                                                     (__nv_bfloat16 *)dy, loss_sum);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_wgrad(const void *dz, const void *x, int32_t rows, int32_t n, int32_t k, int32_t taps, float *dw,
+             float *db, void *stream) {
+  using namespace sk;
+  if (!dz || !x || !dw || rows <= 0 || n % 64 || k % 64 || (taps != 1 && taps != 5)) return CS_E_ARG;
+  dim3 grid((rows + WG_CHUNK - 1) / WG_CHUNK, (n / 64) * (k / 64), taps);
+  wgrad_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)dz, (const __nv_bfloat16 *)x, rows,
+                                                        n, k, taps, dw);
+  if (db) bgrad_kernel<<<(rows + WG_CHUNK - 1) / WG_CHUNK, 128, 0, (cudaStream_t)stream>>>(
+      (const __nv_bfloat16 *)dz, rows, n, db);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_adamw(float *p, float *g, float *m, float *v, int32_t taps, int32_t n, int32_t k, const cs_adam *hp, void *w,
+             void *wt, void *stream) {
+  using namespace sk;
+  if (!p || !g || !m || !v || !hp || taps <= 0 || n <= 0 || k <= 0) return CS_E_ARG;
+  const long long cnt = (long long)taps * n * k;
+  adamw_kernel<<<grid_1d(cnt, 256), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, taps, n, k, *hp,
+                                                                     (__nv_bfloat16 *)w, (__nv_bfloat16 *)wt);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_post(const cs_columns *c, const float *y, int32_t nheads, const cs_guard *g, int32_t *nflagged,
+            int32_t *flagged, float *diag, void *stream) {
+  using namespace sk;
+  if (!cols_ok(c) || !y || !g || !nflagged || (g->capacity > 0 && !flagged) || nheads < 1 || nheads > 2)
+    return CS_E_ARG;
+  Cols C{*c};
+  const int ncol = c->nproma * c->ngpblks;
+  post_kernel<<<grid_1d(ncol, 128), 128, 0, (cudaStream_t)stream>>>(C, y, nheads, *g, nflagged, flagged,
+                                                                      (float4 *)diag);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+int cs_move_columns(const cs_colarray *arrays, int32_t narr, int32_t nproma_src, int32_t nproma_dst,
+                    const int32_t *idx, const int32_t *count, int32_t cap, int32_t dir, void *stream) {
+  using namespace sk;
+  if (!arrays || narr <= 0 || narr > 65535 || nproma_src <= 0 || nproma_dst <= 0 || !idx || !count || cap <= 0 ||
+      (dir != 0 && dir != 1))
+    return CS_E_ARG;
+  dim3 grid(grid_1d((long long)cap * 140, 256) / 4 + 1, narr);
+  move_columns_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(arrays, narr, nproma_src, nproma_dst, idx, count, cap,
+                                                              dir);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,433 @@
+"""Learned CLOUDSC surrogate: a per-column network trained on columns that the
+FP64 GPU kernel computes, run with a conservation/range guard that sends
+flagged columns back to the FP64 kernel.
+
+Network (bf16 weights and activations, f32 accumulation, all GEMMs on the
+tcgen05 tensor cores through cs_conv_gemm; everything else in this package's
+own CUDA kernels, include/cloudsc_surrogate.h):
+
+    x0  [rows,128]  14 normalised input fields at levels l-2..l+2 (one
+                    5-level window of 16 slots per level)
+    h1 = SiLU(x0 W1 + b1)                         the first convolution
+    h2 = h1 + SiLU(conv5(h1; W2) + b2)            second convolution (k = 5)
+    h3 = h2 + SiLU(conv5(h2; W3) + b3)            third convolution (k = 5)
+    h4 = SiLU(h3 W4 + b4)                          MLP head, layer 1
+    y  = h4 W5 + b5   [rows,128]                   MLP head, layer 2: two
+                    output heads of 9 channels (columns 0..8 and 64..72)
+
+One row per (column, level): a column holds LP = 144 rows, level l at row
+2 + l, zero rows around it, so the 5-tap convolutions over levels never mix
+columns.  Outputs per level: LOC_T, LOC_Q, LOC_A, LOC_CLD(l,i,r,s) and the
+rain and snow fluxes at the half level below.  Training: MSE on outputs
+divided by their RMS, AdamW on f32 master weights.
+
+Guard (cs_post): the two heads are averaged; the surface precipitation comes
+from the column water budget and LOC_T is shifted by a column constant so
+that the water and enthalpy budgets close exactly; a column is flagged (and
+recomputed by the FP64 kernel) when a condensate would go negative, the
+network's own surface fluxes or enthalpy miss the budgets by more than a
+tolerance, the diagnosed precipitation is negative, or the heads disagree.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+from . import cloudsc, fields, tcgemm
+
+LP = 144
+KLEV = 137
+NIN, NOUT = 14, 9
+HERE = os.path.dirname(os.path.abspath(__file__))
+WEIGHTS = os.path.join(HERE, "data", "surrogate_w128.npz")
+
+# input channels: (name, log transform epsilon or None)
+IN_CHANNELS = [("t", None), ("q", 1e-8), ("p", 1.0), ("ql", 1e-9), ("qi", 1e-9), ("qr", 1e-9),
+               ("qs", 1e-9), ("plude", 1e-10), ("a", None), ("mflux", None), ("cml_t", None),
+               ("cml_q", None), ("cml_a", None), ("cml_li", None)]
+OUT_CHANNELS = ["loc_t", "loc_q", "loc_a", "loc_l", "loc_i", "loc_r", "loc_s", "pfplsl", "pfplsn"]
+
+
+# ----------------------------------------------------------------- C structs
+class Columns(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in
+                ["pt", "pq", "pap", "paph", "pclv", "pa", "pmfu", "pmfd", "cml_t", "cml_q", "cml_a",
+                 "cml_cld", "plu", "pludeli", "psnde", "ldcum", "plude", "loc_t", "loc_q", "loc_a",
+                 "loc_cld", "pfplsl", "pfplsn", "pfhpsl", "pfhpsn"]] + \
+               [("nproma", ctypes.c_int32), ("klev", ctypes.c_int32), ("ngpblks", ctypes.c_int32),
+                ("lp", ctypes.c_int32)]
+
+
+class Norm(ctypes.Structure):
+    _fields_ = [("mean", ctypes.c_float * 16), ("inv_std", ctypes.c_float * 16),
+                ("eps", ctypes.c_float * 16), ("use_log", ctypes.c_int32 * 16)]
+
+
+class Adam(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_float) for n in ["lr", "beta1", "beta2", "eps", "weight_decay", "bc1", "bc2"]]
+
+
+class Guard(ctypes.Structure):
+    _fields_ = [("out_scale", ctypes.c_float * 16), ("rg", ctypes.c_double), ("ralvdcp", ctypes.c_double),
+                ("ralsdcp", ctypes.c_double), ("rlvtt", ctypes.c_double), ("rlstt", ctypes.c_double),
+                ("ptsphy", ctypes.c_double), ("ncldtop", ctypes.c_int32), ("neg_tol", ctypes.c_double),
+                ("closure_tol", ctypes.c_double), ("spread_tol", ctypes.c_double),
+                ("capacity", ctypes.c_int32)]
+
+
+class ColArray(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_void_p), ("dst", ctypes.c_void_p), ("rows", ctypes.c_int32),
+                ("esize", ctypes.c_int32)]
+
+
+_L = None
+
+
+def _lib():
+    global _L
+    if _L is None:
+        L = cloudsc.lib()
+        vp, i32 = ctypes.c_void_p, ctypes.c_int32
+        L.cs_raw_features.argtypes = [ctypes.POINTER(Columns), vp, vp]
+        L.cs_prep_inputs.argtypes = [ctypes.POINTER(Columns), ctypes.POINTER(Norm), vp, vp]
+        L.cs_prep_targets.argtypes = [ctypes.POINTER(Columns), vp, vp, vp]
+        L.cs_prep_batch.argtypes = [vp, vp, vp, i32, i32, i32, ctypes.POINTER(Norm), vp, vp, vp]
+        L.cs_loss.argtypes = [vp, vp, i32, i32, i32, vp, i32, vp, vp, vp]
+        L.cs_wgrad.argtypes = [vp, vp, i32, i32, i32, i32, vp, vp, vp]
+        L.cs_adamw.argtypes = [vp, vp, vp, vp, i32, i32, i32, ctypes.POINTER(Adam), vp, vp, vp]
+        L.cs_post.argtypes = [ctypes.POINTER(Columns), vp, i32, ctypes.POINTER(Guard), vp, vp, vp, vp]
+        L.cs_move_columns.argtypes = [vp, i32, i32, i32, vp, vp, i32, i32, vp]
+        for f in ["cs_raw_features", "cs_prep_inputs", "cs_prep_targets", "cs_prep_batch", "cs_loss",
+                  "cs_wgrad", "cs_adamw", "cs_post", "cs_move_columns"]:
+            getattr(L, f).restype = ctypes.c_int
+        _L = L
+    return _L
+
+
+def _ok(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed ({rc})")
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+def _stream():
+    import torch
+    return torch.cuda.current_stream().cuda_stream
+
+
+def columns(dev, nproma, ngpblks, klev=KLEV, lp=LP):
+    """Columns struct over CLOUDSC batched device tensors (fields.BATCHED_FIELDS names)."""
+    c = Columns()
+    m = {"pt": "pt", "pq": "pq", "pap": "pap", "paph": "paph", "pclv": "pclv", "pa": "pa", "pmfu": "pmfu",
+         "pmfd": "pmfd", "cml_t": "tendency_cml_t", "cml_q": "tendency_cml_q", "cml_a": "tendency_cml_a",
+         "cml_cld": "tendency_cml_cld", "plu": "plu", "pludeli": "pludeli", "psnde": "psnde",
+         "ldcum": "ldcum", "plude": "plude", "loc_t": "tendency_loc_t", "loc_q": "tendency_loc_q",
+         "loc_a": "tendency_loc_a", "loc_cld": "tendency_loc_cld", "pfplsl": "pfplsl", "pfplsn": "pfplsn",
+         "pfhpsl": "pfhpsl", "pfhpsn": "pfhpsn"}
+    for k, v in m.items():
+        setattr(c, k, dev[v].data_ptr())
+    c.nproma, c.klev, c.ngpblks, c.lp = nproma, klev, ngpblks, lp
+    return c
+
+
+# ----------------------------------------------------------------- network
+class Net:
+    """Parameters (f32 masters, AdamW moments, bf16 forward and transposed
+    copies) and the forward/backward passes on the GPU."""
+
+    def __init__(self, width=128, seed=0, device="cuda"):
+        import torch
+        assert width in (64, 128)
+        self.width, self.dev = width, device
+        W = width
+        self.shapes = {1: (1, W, 128), 2: (5, W, W), 3: (5, W, W), 4: (1, W, W), 5: (1, 128, W)}
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        self.p, self.b = {}, {}
+        for i, (t, n, k) in self.shapes.items():
+            fan_in = t * k
+            gain = {1: 1.0, 2: 0.5, 3: 0.5, 4: 1.0, 5: 0.3}[i]
+            w = torch.randn(t, n, k, generator=g) * (gain * math.sqrt(2.0 / fan_in))
+            self.p[i] = w.to(device)
+            self.b[i] = torch.zeros(n, device=device)
+        self.m = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.v = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.g = {k: torch.zeros_like(v) for k, v in self.p.items()}
+        self.mb = {k: torch.zeros_like(v) for k, v in self.b.items()}
+        self.vb = {k: torch.zeros_like(v) for k, v in self.b.items()}
+        self.gb = {k: torch.zeros_like(v) for k, v in self.b.items()}
+        self.wbf, self.wtbf = {}, {}
+        self.step_count = 0
+        self.norm = Norm()
+        self.out_scale = np.ones(16, np.float32)
+        self.sync_bf16()
+
+    def sync_bf16(self):
+        """bf16 copies of the master weights (forward [t][n][k]; backward
+        [t][k][n] with the taps reversed)."""
+        for i, w in self.p.items():
+            self.wbf[i] = w.bfloat16().contiguous()
+            self.wtbf[i] = w.flip(0).transpose(1, 2).contiguous().bfloat16()
+
+    # -- buffers
+    def buffers(self, rows, train=True):
+        import torch
+        W, d = self.width, self.dev
+        bf = lambda c: torch.empty(rows, c, device=d, dtype=torch.bfloat16)
+        B = {"x0": bf(128), "y": torch.empty(rows, 128, device=d)}
+        if train:
+            for n in ["h1", "h2", "h3", "h4", "z1", "z2", "z3", "z4", "dz1", "dz2", "dz3", "dz4", "g2", "g3"]:
+                B[n] = bf(W)
+            B["dy"] = bf(128)
+            B["tb"] = torch.empty(rows, 16, device=d)
+            B["loss"] = torch.zeros(1, device=d, dtype=torch.float64)
+        else:
+            B["ha"], B["hb"] = bf(W), bf(W)
+        return B
+
+    def forward(self, B, rows, train=True, stream=None):
+        W = self.width
+        G, E = tcgemm.conv_gemm, tcgemm
+        if train:
+            G(B["x0"][:rows], self.wbf[1], E.EPI_SILU, W, 1, LP, KLEV, self.b[1], B["h1"], B["z1"], stream=stream)
+            G(B["h1"][:rows], self.wbf[2], E.EPI_SILU, W, 5, LP, KLEV, self.b[2], B["h2"], B["z2"], B["h1"],
+              stream=stream)
+            G(B["h2"][:rows], self.wbf[3], E.EPI_SILU, W, 5, LP, KLEV, self.b[3], B["h3"], B["z3"], B["h2"],
+              stream=stream)
+            G(B["h3"][:rows], self.wbf[4], E.EPI_SILU, W, 1, LP, KLEV, self.b[4], B["h4"], B["z4"], stream=stream)
+            G(B["h4"][:rows], self.wbf[5], E.EPI_LINEAR_F32, 128, 1, LP, KLEV, self.b[5], outf=B["y"],
+              stream=stream)
+        else:
+            ha, hb = B["ha"], B["hb"]
+            G(B["x0"][:rows], self.wbf[1], E.EPI_SILU, W, 1, LP, KLEV, self.b[1], ha, stream=stream)
+            G(ha[:rows], self.wbf[2], E.EPI_SILU, W, 5, LP, KLEV, self.b[2], hb, resid=ha, stream=stream)
+            G(hb[:rows], self.wbf[3], E.EPI_SILU, W, 5, LP, KLEV, self.b[3], ha, resid=hb, stream=stream)
+            G(ha[:rows], self.wbf[4], E.EPI_SILU, W, 1, LP, KLEV, self.b[4], hb, stream=stream)
+            G(hb[:rows], self.wbf[5], E.EPI_LINEAR_F32, 128, 1, LP, KLEV, self.b[5], outf=B["y"], stream=stream)
+        return B["y"]
+
+    def backward(self, B, rows):
+        """Gradients of the loss whose output gradient is B['dy'], accumulated
+        into self.g / self.gb."""
+        W, L, s = self.width, _lib(), _stream()
+        G, E = tcgemm.conv_gemm, tcgemm
+        G(B["dy"][:rows], self.wtbf[5], E.EPI_BWD, W, 1, LP, KLEV, out=B["dz4"], zprev=B["z4"])
+        G(B["dz4"][:rows], self.wtbf[4], E.EPI_BWD, W, 1, LP, KLEV, out=B["dz3"], zprev=B["z3"], gout=B["g3"])
+        G(B["dz3"][:rows], self.wtbf[3], E.EPI_BWD, W, 5, LP, KLEV, out=B["dz2"], zprev=B["z2"], resid=B["g3"],
+          gout=B["g2"])
+        G(B["dz2"][:rows], self.wtbf[2], E.EPI_BWD, W, 5, LP, KLEV, out=B["dz1"], zprev=B["z1"], resid=B["g2"])
+        for i, dz, x, n, k, t in [(5, "dy", "h4", 128, W, 1), (4, "dz4", "h3", W, W, 1), (3, "dz3", "h2", W, W, 5),
+                                  (2, "dz2", "h1", W, W, 5), (1, "dz1", "x0", W, 128, 1)]:
+            _ok(L.cs_wgrad(_p(B[dz]), _p(B[x]), rows, n, k, t, _p(self.g[i]), _p(self.gb[i]), s), "cs_wgrad")
+
+    def adamw(self, lr, wd=1e-4, beta1=0.9, beta2=0.999, eps=1e-8):
+        L, s = _lib(), _stream()
+        self.step_count += 1
+        t = self.step_count
+        hp = Adam(lr, beta1, beta2, eps, wd, 1 - beta1 ** t, 1 - beta2 ** t)
+        hpb = Adam(lr, beta1, beta2, eps, 0.0, 1 - beta1 ** t, 1 - beta2 ** t)
+        for i, (tp, n, k) in self.shapes.items():
+            _ok(L.cs_adamw(_p(self.p[i]), _p(self.g[i]), _p(self.m[i]), _p(self.v[i]), tp, n, k,
+                           ctypes.byref(hp), _p(self.wbf[i]), _p(self.wtbf[i]), s), "cs_adamw")
+            _ok(L.cs_adamw(_p(self.b[i]), _p(self.gb[i]), _p(self.mb[i]), _p(self.vb[i]), 1, n, 1,
+                           ctypes.byref(hpb), None, None, s), "cs_adamw")
+
+    # -- persistence
+    def state(self):
+        d = {f"w{i}": self.p[i].cpu().numpy() for i in self.p}
+        d.update({f"b{i}": self.b[i].cpu().numpy() for i in self.b})
+        d["norm_mean"] = np.array(self.norm.mean[:], np.float32)
+        d["norm_inv_std"] = np.array(self.norm.inv_std[:], np.float32)
+        d["norm_eps"] = np.array(self.norm.eps[:], np.float32)
+        d["norm_use_log"] = np.array(self.norm.use_log[:], np.int32)
+        d["out_scale"] = self.out_scale.astype(np.float32)
+        d["width"] = np.array(self.width)
+        return d
+
+    def save(self, path):
+        np.savez_compressed(path, **self.state())
+
+    @classmethod
+    def load(cls, path, device="cuda"):
+        import torch
+        z = np.load(path)
+        net = cls(int(z["width"]), device=device)
+        for i in net.p:
+            net.p[i] = torch.from_numpy(z[f"w{i}"]).to(device)
+            net.b[i] = torch.from_numpy(z[f"b{i}"]).to(device)
+        net.norm.mean[:] = z["norm_mean"].tolist()
+        net.norm.inv_std[:] = z["norm_inv_std"].tolist()
+        net.norm.eps[:] = z["norm_eps"].tolist()
+        net.norm.use_log[:] = z["norm_use_log"].tolist()
+        net.out_scale = z["out_scale"].astype(np.float32)
+        net.sync_bf16()
+        return net
+
+
+# ----------------------------------------------------------------- data
+class Dataset:
+    """Raw features and CLOUDSC FP64 targets of many columns, on the GPU
+    (f32 [ncol*LP][16] each)."""
+
+    def __init__(self, params, nchunks, nblk=2048, nproma=128, seed0=1000, ptsphy=3600.0, log=print):
+        import torch
+        from . import inputs
+        ncol_chunk = nblk * nproma
+        self.ncol = ncol_chunk * nchunks
+        self.feat = torch.empty(self.ncol * LP, 16, device="cuda")
+        self.tgt = torch.empty(self.ncol * LP, 16, device="cuda")
+        L, ones = _lib(), np.ones(16, np.float32)
+        cloudsc.setup(params)
+        for ch in range(nchunks):
+            host = inputs.generate(nblk, nproma, params, seed=seed0 + ch)
+            dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+            del host
+            c = columns(dev, nproma, nblk)
+            sl = slice(ch * ncol_chunk * LP, (ch + 1) * ncol_chunk * LP)
+            _ok(L.cs_raw_features(ctypes.byref(c), _p(self.feat[sl]), _stream()), "cs_raw_features")
+            cloudsc.cloudsc_batched(params, dev, nproma, KLEV, nblk, ncol_chunk, ptsphy)
+            _ok(L.cs_prep_targets(ctypes.byref(c), ones.ctypes.data, _p(self.tgt[sl]), _stream()),
+                "cs_prep_targets")
+            torch.cuda.synchronize()
+            del dev
+            if log:
+                log(f"dataset chunk {ch + 1}/{nchunks}")
+        rows = torch.arange(self.ncol * LP, device="cuda") % LP
+        self.valid = (rows >= 2) & (rows < 2 + KLEV)
+
+    def normalisation(self, sample=4_000_000):
+        """Input transform statistics and output RMS scales (over valid rows)."""
+        import torch
+        idx = torch.nonzero(self.valid).squeeze(1)
+        if idx.numel() > sample:
+            idx = idx[torch.randperm(idx.numel(), device="cuda")[:sample]]
+        f = self.feat[idx].double()
+        norm = Norm()
+        for ch, (_, eps) in enumerate(IN_CHANNELS):
+            x = f[:, ch]
+            if eps is not None:
+                x = torch.log(torch.clamp(x, min=0.0) + eps)
+                norm.use_log[ch], norm.eps[ch] = 1, eps
+            mu, sd = float(x.mean()), float(x.std())
+            norm.mean[ch], norm.inv_std[ch] = mu, 1.0 / max(sd, 1e-30)
+        t = self.tgt[idx].double()
+        scale = np.ones(16, np.float32)
+        for ch in range(NOUT):
+            scale[ch] = max(float(t[:, ch].pow(2).mean().sqrt()), 1e-30)
+        return norm, scale
+
+    def apply_scale(self, scale):
+        import torch
+        self.tgt[:, :NOUT] /= torch.from_numpy(scale[:NOUT]).cuda()
+
+
+def train(net, data, steps, nb=512, lr=2e-3, lr_min=5e-5, warmup=200, seed=0, log=print, log_every=500):
+    """AdamW on random batches of nb columns; cosine learning-rate decay."""
+    import torch
+    L = _lib()
+    rows = nb * LP
+    B = net.buffers(rows, train=True)
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    w = np.ones(16, np.float32)
+    hist = []
+    for it in range(steps):
+        cols = torch.randint(0, data.ncol, (nb,), device="cuda", generator=gen, dtype=torch.int32)
+        s = _stream()
+        _ok(L.cs_prep_batch(_p(data.feat), _p(data.tgt), _p(cols), nb, LP, KLEV, ctypes.byref(net.norm),
+                            _p(B["x0"]), _p(B["tb"]), s), "cs_prep_batch")
+        net.forward(B, rows)
+        _ok(L.cs_loss(_p(B["y"]), _p(B["tb"]), rows, LP, KLEV, w.ctypes.data, 2, _p(B["dy"]), _p(B["loss"]), s),
+            "cs_loss")
+        net.backward(B, rows)
+        if it < warmup:
+            cur = lr * (it + 1) / warmup
+        else:
+            f = (it - warmup) / max(1, steps - warmup)
+            cur = lr_min + 0.5 * (lr - lr_min) * (1 + math.cos(math.pi * f))
+        net.adamw(cur)
+        if (it + 1) % log_every == 0 or it == steps - 1:
+            l = float(B["loss"].item()) / log_every / 2.0  # mean over steps and heads
+            B["loss"].zero_()
+            hist.append((it + 1, l))
+            if log:
+                log(f"step {it + 1}: loss {l:.4e} lr {cur:.2e}")
+    return hist
+
+
+# ----------------------------------------------------------------- inference
+class Runner:
+    """Guarded surrogate inference over one batch of CLOUDSC batched device
+    arrays, with the FP64 fallback on at most `capacity` flagged columns."""
+
+    def __init__(self, net, params, nproma, ngpblks, capacity, ptsphy=3600.0, neg_tol=1e-7,
+                 closure_tol=0.5, spread_tol=0.25):
+        import torch
+        self.net, self.params, self.nproma, self.ngpblks = net, params, nproma, ngpblks
+        self.ncol = nproma * ngpblks
+        self.rows = self.ncol * LP
+        self.B = net.buffers(self.rows, train=False)
+        self.cap = int(math.ceil(capacity / nproma)) * nproma
+        self.nflag = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.flagged = torch.zeros(self.cap, dtype=torch.int32, device="cuda")
+        self.diag = torch.zeros(self.ncol, 4, device="cuda")
+        tdt = lambda dt: torch.float64 if np.dtype(dt) == np.float64 else torch.int32
+        self.compact = fields.alloc(self.cap // nproma, nproma, KLEV,
+                                    alloc_fn=lambda shape, dt: torch.zeros(shape, dtype=tdt(dt), device="cuda"))
+        g = Guard()
+        g.out_scale[:] = net.out_scale.tolist()
+        g.rg, g.ralvdcp, g.ralsdcp = params.rg, params.ralvdcp, params.ralsdcp
+        g.rlvtt, g.rlstt, g.ptsphy, g.ncldtop = params.rlvtt, params.rlstt, ptsphy, params.ncldtop
+        g.neg_tol, g.closure_tol, g.spread_tol, g.capacity = neg_tol, closure_tol, spread_tol, self.cap
+        self.guard = g
+        self.ptsphy = ptsphy
+        self.plude_in = None
+
+    def _colarrays(self, dev, direction):
+        import torch
+        arrs = []
+        for name, kind, dtype, role in fields.BATCHED_FIELDS:
+            if direction == 0 and role not in ("in", "inout"):
+                continue
+            if direction == 1 and role not in ("out", "inout"):
+                continue
+            rows = fields.block_shape(kind, 1, KLEV)
+            rows = int(np.prod(rows))
+            src = self.plude_in if (direction == 0 and name == "plude") else dev[name]
+            if direction == 0:
+                arrs.append(ColArray(src.data_ptr(), self.compact[name].data_ptr(), rows, src.element_size()))
+            else:
+                arrs.append(ColArray(self.compact[name].data_ptr(), dev[name].data_ptr(), rows,
+                                     dev[name].element_size()))
+        raw = (ColArray * len(arrs))(*arrs)
+        t = torch.frombuffer(bytearray(bytes(raw)), dtype=torch.uint8).cuda()
+        return t, len(arrs)
+
+    def prepare(self, dev):
+        """Per input batch set-up (outside any timed or captured region)."""
+        import torch
+        self.plude_in = torch.empty_like(dev["plude"])
+        self.cols = columns(dev, self.nproma, self.ngpblks)
+        self.gather = self._colarrays(dev, 0)
+        self.scatter = self._colarrays(dev, 1)
+
+    def run(self, dev):
+        """Surrogate + guard + FP64 fallback, all on the current stream."""
+        L, s = _lib(), _stream()
+        self.plude_in.copy_(dev["plude"])
+        _ok(L.cs_prep_inputs(ctypes.byref(self.cols), ctypes.byref(self.net.norm), _p(self.B["x0"]), s),
+            "cs_prep_inputs")
+        self.net.forward(self.B, self.rows, train=False)
+        self.nflag.zero_()
+        _ok(L.cs_post(ctypes.byref(self.cols), _p(self.B["y"]), 2, ctypes.byref(self.guard), _p(self.nflag),
+                      _p(self.flagged), _p(self.diag), s), "cs_post")
+        ga, na = self.gather
+        _ok(L.cs_move_columns(_p(ga), na, self.nproma, self.nproma, _p(self.flagged), _p(self.nflag), self.cap,
+                              0, s), "cs_move_columns")
+        cloudsc.cloudsc_batched(self.params, self.compact, self.nproma, KLEV, self.cap // self.nproma, self.cap,
+                                self.ptsphy, stream=s)
+        sa, nsa = self.scatter
+        _ok(L.cs_move_columns(_p(sa), nsa, self.nproma, self.nproma, _p(self.flagged), _p(self.nflag), self.cap,
+                              1, s), "cs_move_columns")

@@ -1,0 +1,133 @@
+"""The surrogate's GPU kernels: gradients of the whole network (tcgen05
+forward and backward-data GEMMs, CUDA-core weight gradients, loss kernel)
+against the float64 CPU reference (tests/surrogate_ref.py, itself checked
+against finite differences) on identical bf16-rounded weights and inputs;
+a short training run that must lower the loss; and the guarded inference
+path: exact water/enthalpy closure of every surrogate column and FP64
+results on every flagged column."""
+import numpy as np
+import pytest
+
+from openifs_b200 import cloudsc, fields, inputs, surrogate as S
+from tests import surrogate_ref as R
+from tests import util
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf(x):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(x)).float().bfloat16().double().numpy()
+
+
+@pytest.mark.parametrize("width", [64, 128])
+def test_gradients_match_cpu_reference(cuda, width):
+    import torch
+    rng = np.random.default_rng(11)
+    P = R.random_params(width, rng)
+    for k in list(P):
+        if k.startswith("w"):
+            P[k] = _bf(P[k])
+    x0, tgt = R.random_batch(2, rng)
+    x0 = _bf(x0)
+    loss_ref, G = R.loss_and_grad(P, x0, tgt)
+
+    net = S.Net(width)
+    for i in range(1, 6):
+        net.p[i] = torch.from_numpy(P[f"w{i}"]).float().cuda()
+        net.b[i] = torch.from_numpy(P[f"b{i}"]).float().cuda()
+        net.g[i].zero_()
+        net.gb[i] = torch.zeros_like(net.b[i])
+    net.sync_bf16()
+    rows = x0.shape[0]
+    B = net.buffers(rows)
+    B["x0"].copy_(torch.from_numpy(x0).bfloat16())
+    B["tb"].copy_(torch.from_numpy(tgt).float())
+    net.forward(B, rows)
+    w = np.ones(16, np.float32)
+    L = S._lib()
+    S._ok(L.cs_loss(B["y"].data_ptr(), B["tb"].data_ptr(), rows, S.LP, S.KLEV, w.ctypes.data, 2,
+                    B["dy"].data_ptr(), B["loss"].data_ptr(), S._stream()), "cs_loss")
+    net.backward(B, rows)
+    torch.cuda.synchronize()
+    loss = float(B["loss"].item())
+    assert abs(loss - loss_ref) < 2e-2 * loss_ref, (loss, loss_ref)
+    for i in range(1, 6):
+        g = net.g[i].double().cpu().numpy()
+        r = G[f"w{i}"]
+        rel = np.linalg.norm(g - r) / np.linalg.norm(r)
+        assert rel < 5e-2, (i, rel)
+        gb = net.gb[i].double().cpu().numpy()
+        relb = np.linalg.norm(gb - G[f"b{i}"]) / np.linalg.norm(G[f"b{i}"])
+        assert relb < 5e-2, (i, relb)
+
+
+@pytest.fixture(scope="module")
+def small_data(cuda):
+    p, _ = util.params()
+    data = S.Dataset(p, nchunks=1, nblk=48, nproma=128, seed0=77, log=None)
+    norm, scale = data.normalisation()
+    data.apply_scale(scale)
+    return p, data, norm, scale
+
+
+def test_training_lowers_loss(small_data):
+    p, data, norm, scale = small_data
+    net = S.Net(128, seed=1)
+    net.norm, net.out_scale = norm, scale
+    hist = S.train(net, data, steps=400, nb=64, lr=2e-3, warmup=50, log=None, log_every=100)
+    first, last = hist[0][1], hist[-1][1]
+    # targets are normalised to unit RMS: predicting zero tendencies scores 1.0
+    assert last < 0.5 * first and last < 0.5, hist
+
+
+def test_guarded_inference_closes_budgets(small_data):
+    import torch
+    p, data, norm, scale = small_data
+    net = S.Net(128, seed=1)
+    net.norm, net.out_scale = norm, scale
+    S.train(net, data, steps=300, nb=64, lr=2e-3, warmup=50, log=None, log_every=100)
+    nproma, nblk = 128, 8
+    host = inputs.generate(nblk, nproma, p, seed=91)
+    cloudsc.setup(p)
+    ref = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    cloudsc.cloudsc_batched(p, ref, nproma, S.KLEV, nblk, nproma * nblk, util.PTSPHY)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    run = S.Runner(net, p, nproma, nblk, capacity=256)
+    run.prepare(dev)
+    run.run(dev)
+    torch.cuda.synchronize()
+    nflag = int(run.nflag.item())
+    flagged = set(run.flagged[:min(nflag, run.cap)].cpu().tolist())
+    out = {k: v.cpu().numpy() for k, v in dev.items()}
+    r = {k: v.cpu().numpy() for k, v in ref.items()}
+    ncol = nproma * nblk
+    cols = np.arange(ncol)
+    ib, jl = cols // nproma, cols % nproma
+    # flagged columns carry the FP64 results bit for bit
+    for n in ["tendency_loc_t", "tendency_loc_q", "pfplsl", "pfsqlf"]:
+        for c in list(flagged)[:64]:
+            assert np.array_equal(out[n][c // nproma, ..., c % nproma], r[n][c // nproma, ..., c % nproma]), n
+    # every column closes water and enthalpy (budgets of cs_post) to rounding
+    dp = np.diff(host["paph"], axis=1)
+    g = p.rg
+    L = out["tendency_loc_cld"]
+    lev = np.arange(S.KLEV)
+    loop = ((lev >= p.ncldtop - 1) & (lev < S.KLEV - 1))[None, :, None]
+    active = loop & (out["plude"] != 0.0)
+    sl = (host["pludeli"][:, 0] * active).sum(1)
+    si = (host["pludeli"][:, 1] * active).sum(1)
+    sr = (host["psnde"][:, 0] * loop).sum(1)
+    ss = (host["psnde"][:, 1] * loop).sum(1)
+    w_l = (dp / g * (out["tendency_loc_q"] + L[:, :4].sum(1))).sum(1)
+    w_r = sl + si + sr + ss - out["pfplsl"][:, -1] - out["pfplsn"][:, -1]
+    w_s = (np.abs(dp / g * out["tendency_loc_q"])).sum(1) + np.abs(w_r) + 1e-30
+    e_l = (dp / g * (out["tendency_loc_t"] - p.ralvdcp * (L[:, 0] + L[:, 2]) - p.ralsdcp * (L[:, 1] + L[:, 3]))).sum(1)
+    e_r = p.ralvdcp * (out["pfplsl"][:, -1] - sl - sr) + p.ralsdcp * (out["pfplsn"][:, -1] - si - ss)
+    e_s = (np.abs(dp / g * out["tendency_loc_t"])).sum(1) + np.abs(e_r) + 1e-30
+    wr = np.abs(w_l - w_r) / w_s
+    er = np.abs(e_l - e_r) / e_s
+    assert wr.max() < 1e-10, wr.max()
+    assert er.max() < 1e-10, er.max()
+    # PLUDE as CLOUDSC writes it, on every column
+    assert np.array_equal(out["plude"], r["plude"])
