@@ -9,7 +9,10 @@ over every column; inputs stay resident in HBM (15 GB, far above the 126 MB
 L2, so no flush is needed between steps).  PLUDE is INOUT (cloudsc.F90:1367),
 so it is restored from a pristine copy before every step, outside the timed
 kernel.  ``value`` is FP64 columns/s; the FP32-mixed form is reported beside
-it with its error against the FP64 kernel.  ``e2e`` is the same FP64 metric
+it with its error against the FP64 kernel, and the guarded learned surrogate
+(openifs_b200/surrogate.py) over 1,048,576 columns (4 batches of 262,144 in
+one CUDA graph) with its flagged fraction, errors, budget closure and the
+tensor-core throughput of its GEMMs.  ``e2e`` is the same FP64 metric
 through cloudsc_b200_batched_host with page-locked host buffers (copies in
 the timed region).  Under torchrun each rank runs its own 262,144 columns
 (weak scaling, no collective on the data path).
@@ -30,6 +33,7 @@ sys.path.insert(0, ROOT)
 
 NPROMA, NGPBLKS, KLEV, PTSPHY, SEED = 128, 2048, 137, 3600.0, 2
 NCOL = NPROMA * NGPBLKS
+SUR_BATCHES = 4  # surrogate: 1,048,576 columns as 4 batches of 262,144
 WORKLOAD = ("CLOUDSC, 262,144 columns (2,048 NPROMA blocks of 128) x L137, PTSPHY 3600 s, "
             "seeded synthetic state")
 METRIC = "CLOUDSC columns/s on 1 B200: FP64 vs FP32-mixed vs surrogate, at fixed error"
@@ -42,6 +46,7 @@ def _args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
     return ap.parse_args()
 
 
@@ -180,6 +185,130 @@ def run_reference(a):
     return 0
 
 
+def surrogate_form(a, p, d, plude0, ref, dev, world, rank, ms64):
+    """Guarded surrogate (config: 1,048,576 columns as 4 batches of 262,144,
+    one CUDA graph per pass): columns/s, speed-up over the FP64 kernel,
+    flagged fraction, errors and budget closure of batch 0 against the FP64
+    kernel, tensor-core throughput of the network's GEMMs."""
+    import torch
+    from openifs_b200 import inputs, surrogate as S
+    if not os.path.exists(S.WEIGHTS):
+        return {"unavailable": "no trained weights (python -m openifs_b200.train_surrogate)"}
+    net = S.Net.load(S.WEIGHTS)
+    cap_frac = 0.0625
+    runner = S.Runner(net, p, NPROMA, NGPBLKS, capacity=int(cap_frac * NCOL))
+    d["plude"].copy_(plude0)
+    batches = [d]
+    for i in range(1, SUR_BATCHES):
+        host = inputs.generate(NGPBLKS, NPROMA, p, seed=SEED + 10 * i + 1000 * rank)
+        batches.append({k: torch.from_numpy(v).to(dev) for k, v in host.items()})
+        del host
+    states = [runner.prepare(b) for b in batches]
+    stream = torch.cuda.current_stream(dev)
+    for st in states:  # eager warm-up: one-time attribute and parameter set-up
+        runner.run(st)
+    torch.cuda.synchronize(dev)
+    # the network alone (input preparation + 5 GEMMs), eager, batch 0
+    fw = []
+    for i in range(a.warmup + a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        runner.forward_only(states[0])
+        e1.record(stream)
+        if i >= a.warmup:
+            fw.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    fw_ms = statistics.mean(x.elapsed_time(y) for x, y in fw)
+    gemm = []
+    B = runner.B
+    for i in range(a.warmup + a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        net.forward(B, runner.rows, train=False)
+        e1.record(stream)
+        if i >= a.warmup:
+            gemm.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    gemm_ms = statistics.mean(x.elapsed_time(y) for x, y in gemm)
+    # the guarded pipeline over all batches, captured once, replayed
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for st in states:
+            runner.run(st)
+    for _ in range(a.warmup):
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    ev = []
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        graph.replay()
+        e1.record(stream)
+        ev.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ncols = SUR_BATCHES * NCOL
+    flagged = [int(st.nflag.item()) for st in states]
+    # accuracy and closure of batch 0 against the FP64 kernel
+    err = {}
+    for n in ["tendency_loc_t", "tendency_loc_q", "tendency_loc_a", "tendency_loc_cld", "pfplsl", "pfplsn"]:
+        r, g = ref[n], d[n]
+        if n == "tendency_loc_cld":
+            r, g = r[:, :4], g[:, :4]
+        if n in ("pfplsl", "pfplsn"):
+            r, g = r[:, -1], g[:, -1]
+        err[n] = {"rms_over_rms": float((g - r).pow(2).mean().sqrt() / r.pow(2).mean().sqrt())}
+    closure = _closure(p, d, states[0].plude_in)
+    del graph
+    flops = runner.flops_per_batch()
+    peaks = _peaks() or {}
+    tpk = peaks.get("bf16_tflops", 1590.0)
+    return {
+        "columns_per_s": world * ncols / (ms * 1e-3), "ms_per_pass": ms, "columns_per_pass": ncols,
+        "batches": SUR_BATCHES, "cuda_graph": True,
+        "ms_per_262144_columns": ms / SUR_BATCHES, "speedup_vs_fp64": ms64 / (ms / SUR_BATCHES),
+        "flagged_per_batch": flagged, "flagged_fraction": sum(flagged) / ncols,
+        "fallback_capacity_per_batch": runner.cap,
+        "error_vs_fp64_batch0": err, "closure_batch0": closure,
+        "network": {"width": net.width, "gemm_flop_per_column": flops / NCOL,
+                    "prep_plus_network_ms": fw_ms, "gemm_ms": gemm_ms,
+                    "gemm_tflops": flops / (gemm_ms * 1e-3) / 1e12,
+                    "gemm_frac_of_bf16_peak": flops / (gemm_ms * 1e-3) / 1e12 / tpk,
+                    "bf16_peak_tflops": tpk},
+        "guard": {"neg_tol": runner.guard.neg_tol, "closure_tol": runner.guard.closure_tol,
+                  "spread_tol": runner.guard.spread_tol},
+    }
+
+
+def _closure(p, d, plude_in):
+    """Max relative column non-closure of the water and enthalpy budgets."""
+    import torch
+    g = p.rg
+    dp = d["paph"][:, 1:] - d["paph"][:, :-1]
+    L = d["tendency_loc_cld"]
+    lev = torch.arange(KLEV, device=dp.device)
+    loop = ((lev >= p.ncldtop - 1) & (lev < KLEV - 1))[None, :, None]
+    active = loop & (d["plude"] != 0.0)
+    sl = (d["pludeli"][:, 0] * active).sum(1)
+    si = (d["pludeli"][:, 1] * active).sum(1)
+    sr = (d["psnde"][:, 0] * loop).sum(1)
+    ss = (d["psnde"][:, 1] * loop).sum(1)
+    w_l = (dp / g * (d["tendency_loc_q"] + L[:, :4].sum(1))).sum(1)
+    w_r = sl + si + sr + ss - d["pfplsl"][:, -1] - d["pfplsn"][:, -1]
+    w_s = (dp / g * d["tendency_loc_q"]).abs().sum(1) + w_r.abs() + 1e-30
+    e_l = (dp / g * (d["tendency_loc_t"] - p.ralvdcp * (L[:, 0] + L[:, 2]) - p.ralsdcp * (L[:, 1] + L[:, 3]))).sum(1)
+    e_r = p.ralvdcp * (d["pfplsl"][:, -1] - sl - sr) + p.ralsdcp * (d["pfplsn"][:, -1] - si - ss)
+    e_s = (dp / g * d["tendency_loc_t"]).abs().sum(1) + e_r.abs() + 1e-30
+    return {"water_max_rel": float(((w_l - w_r).abs() / w_s).max()),
+            "enthalpy_max_rel": float(((e_l - e_r).abs() / e_s).max())}
+
+
 def run_ours(a):
     import torch
     from openifs_b200 import cloudsc, fields, inputs
@@ -259,6 +388,13 @@ def run_ours(a):
         diff = (g - r).abs()
         err[n] = {"max_abs_over_max": float(diff.max() / r.abs().max().clamp_min(1e-300)),
                   "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
+
+    sur = None
+    if not a.no_surrogate:
+        d["plude"].copy_(plude0)
+        cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.FP64)
+        ref = {n: d[n].clone() for n in outs}
+        sur = surrogate_form(a, p, d, plude0, ref, dev, world, rank, results["fp64"]["ms"])
     del ref
 
     # end to end through the host-pointer API (page-locked buffers, copies timed)
@@ -330,7 +466,7 @@ def run_ours(a):
             "mixed": {"columns_per_s": world * NCOL / (results["mixed"]["ms"] * 1e-3),
                       "ms": results["mixed"]["ms"], "speedup_vs_fp64": ms64 / results["mixed"]["ms"],
                       "error_vs_fp64": err},
-            "surrogate": None,
+            "surrogate": sur,
         },
         "roofline": roofline,
         "cpu_baseline": {"value": cpu_val, "unit": "columns/s", "cores": ncores, "kind": "port",

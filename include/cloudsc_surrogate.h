@@ -61,6 +61,8 @@ typedef struct cs_columns {
   const double *cml_t, *cml_q, *cml_a, *cml_cld, *plu, *pludeli, *psnde;
   const int32_t *ldcum;
   double *plude; /* INOUT: read as the input detrainment, written as CLOUDSC does */
+  const double *plude_in; /* if not NULL, the input detrainment is read here instead, so
+                           * that repeated calls on one batch see the same input */
   double *loc_t, *loc_q, *loc_a, *loc_cld, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
   int32_t nproma, klev, ngpblks, lp; /* lp: padded rows per column (>= klev + 4) */
 } cs_columns;

@@ -54,7 +54,7 @@ __device__ __forceinline__ void raw_features(const Cols &C, int col, int k, floa
   f[2] = (float)c.pap[o];
 #pragma unroll
   for (int m = 0; m < 4; ++m) f[3 + m] = (float)c.pclv[C.o3(col, m, 5, k)];
-  f[7] = (float)c.plude[o];
+  f[7] = (float)(c.plude_in ? c.plude_in : c.plude)[o];
   f[8] = (float)c.pa[o];
   f[9] = (float)(c.pmfu[o] + c.pmfd[o]);
   f[10] = (float)c.cml_t[o];
@@ -362,7 +362,7 @@ __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_
       // convective detrainment exactly as CLOUDSC applies it (cloudsc.F90:1362-1398)
       if (k >= k0 && k + 1 < klev) {
         const double zdtgdp = dt * (rg / dp);  // ZDTGDP = PTSPHY * ZGDP, ZGDP = RG / ZDP
-        const double pl = c.plude[o] * zdtgdp;
+        const double pl = (c.plude_in ? c.plude_in : c.plude)[o] * zdtgdp;
         const double plu1 = c.plu[C.o2(col, k + 1)];
         double plude_out = 0.0;
         if (ldcum && pl > ZEPSEC && plu1 > ZEPSEC) {

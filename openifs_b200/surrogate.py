@@ -53,8 +53,8 @@ OUT_CHANNELS = ["loc_t", "loc_q", "loc_a", "loc_l", "loc_i", "loc_r", "loc_s", "
 class Columns(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in
                 ["pt", "pq", "pap", "paph", "pclv", "pa", "pmfu", "pmfd", "cml_t", "cml_q", "cml_a",
-                 "cml_cld", "plu", "pludeli", "psnde", "ldcum", "plude", "loc_t", "loc_q", "loc_a",
-                 "loc_cld", "pfplsl", "pfplsn", "pfhpsl", "pfhpsn"]] + \
+                 "cml_cld", "plu", "pludeli", "psnde", "ldcum", "plude", "plude_in", "loc_t", "loc_q",
+                 "loc_a", "loc_cld", "pfplsl", "pfplsn", "pfhpsl", "pfhpsn"]] + \
                [("nproma", ctypes.c_int32), ("klev", ctypes.c_int32), ("ngpblks", ctypes.c_int32),
                 ("lp", ctypes.c_int32)]
 
@@ -119,9 +119,11 @@ def _stream():
     return torch.cuda.current_stream().cuda_stream
 
 
-def columns(dev, nproma, ngpblks, klev=KLEV, lp=LP):
-    """Columns struct over CLOUDSC batched device tensors (fields.BATCHED_FIELDS names)."""
+def columns(dev, nproma, ngpblks, klev=KLEV, lp=LP, plude_in=None):
+    """Columns struct over CLOUDSC batched device tensors (fields.BATCHED_FIELDS
+    names); plude_in: a separate tensor holding the input PLUDE, or None."""
     c = Columns()
+    c.plude_in = None if plude_in is None else plude_in.data_ptr()
     m = {"pt": "pt", "pq": "pq", "pap": "pap", "paph": "paph", "pclv": "pclv", "pa": "pa", "pmfu": "pmfu",
          "pmfd": "pmfd", "cml_t": "tendency_cml_t", "cml_q": "tendency_cml_q", "cml_a": "tendency_cml_a",
          "cml_cld": "tendency_cml_cld", "plu": "plu", "pludeli": "pludeli", "psnde": "psnde",
@@ -163,6 +165,7 @@ class Net:
         self.step_count = 0
         self.norm = Norm()
         self.out_scale = np.ones(16, np.float32)
+        self.guard_tols = (1e-7, 0.5, 0.25)  # negative condensate, raw closure, head spread
         self.sync_bf16()
 
     def sync_bf16(self):
@@ -263,6 +266,8 @@ class Net:
         net.norm.eps[:] = z["norm_eps"].tolist()
         net.norm.use_log[:] = z["norm_use_log"].tolist()
         net.out_scale = z["out_scale"].astype(np.float32)
+        if "guard" in z:
+            net.guard_tols = tuple(float(x) for x in z["guard"])
         net.sync_bf16()
         return net
 
@@ -358,34 +363,53 @@ def train(net, data, steps, nb=512, lr=2e-3, lr_min=5e-5, warmup=200, seed=0, lo
 
 
 # ----------------------------------------------------------------- inference
-class Runner:
-    """Guarded surrogate inference over one batch of CLOUDSC batched device
-    arrays, with the FP64 fallback on at most `capacity` flagged columns."""
+class Batch:
+    """Per-batch state of the guarded inference: the input PLUDE kept aside
+    (so repeated runs see the same input), the column structs and the
+    gather/scatter tables of the FP64 fallback, the flagged-column count."""
 
-    def __init__(self, net, params, nproma, ngpblks, capacity, ptsphy=3600.0, neg_tol=1e-7,
-                 closure_tol=0.5, spread_tol=0.25):
+    def __init__(self, runner, dev):
+        import torch
+        self.dev = dev
+        self.plude_in = dev["plude"].clone()
+        self.cols = columns(dev, runner.nproma, runner.ngpblks, plude_in=self.plude_in)
+        self.gather = runner._colarrays(dev, self.plude_in, 0)
+        self.scatter = runner._colarrays(dev, self.plude_in, 1)
+        self.nflag = torch.zeros(1, dtype=torch.int32, device="cuda")
+        self.flagged = torch.zeros(runner.cap, dtype=torch.int32, device="cuda")
+
+
+class Runner:
+    """Guarded surrogate inference over batches of CLOUDSC batched device
+    arrays (NPROMA x NGPBLKS columns each), with the FP64 fallback on at most
+    `capacity` flagged columns per batch.  Buffers are shared by the batches,
+    which run one after the other on the current stream."""
+
+    def __init__(self, net, params, nproma, ngpblks, capacity, ptsphy=3600.0, neg_tol=None,
+                 closure_tol=None, spread_tol=None):
         import torch
         self.net, self.params, self.nproma, self.ngpblks = net, params, nproma, ngpblks
         self.ncol = nproma * ngpblks
         self.rows = self.ncol * LP
         self.B = net.buffers(self.rows, train=False)
         self.cap = int(math.ceil(capacity / nproma)) * nproma
-        self.nflag = torch.zeros(1, dtype=torch.int32, device="cuda")
-        self.flagged = torch.zeros(self.cap, dtype=torch.int32, device="cuda")
         self.diag = torch.zeros(self.ncol, 4, device="cuda")
         tdt = lambda dt: torch.float64 if np.dtype(dt) == np.float64 else torch.int32
         self.compact = fields.alloc(self.cap // nproma, nproma, KLEV,
                                     alloc_fn=lambda shape, dt: torch.zeros(shape, dtype=tdt(dt), device="cuda"))
+        t_neg, t_clo, t_spr = net.guard_tols
         g = Guard()
         g.out_scale[:] = net.out_scale.tolist()
         g.rg, g.ralvdcp, g.ralsdcp = params.rg, params.ralvdcp, params.ralsdcp
         g.rlvtt, g.rlstt, g.ptsphy, g.ncldtop = params.rlvtt, params.rlstt, ptsphy, params.ncldtop
-        g.neg_tol, g.closure_tol, g.spread_tol, g.capacity = neg_tol, closure_tol, spread_tol, self.cap
+        g.neg_tol = t_neg if neg_tol is None else neg_tol
+        g.closure_tol = t_clo if closure_tol is None else closure_tol
+        g.spread_tol = t_spr if spread_tol is None else spread_tol
+        g.capacity = self.cap
         self.guard = g
         self.ptsphy = ptsphy
-        self.plude_in = None
 
-    def _colarrays(self, dev, direction):
+    def _colarrays(self, dev, plude_in, direction):
         import torch
         arrs = []
         for name, kind, dtype, role in fields.BATCHED_FIELDS:
@@ -393,10 +417,9 @@ class Runner:
                 continue
             if direction == 1 and role not in ("out", "inout"):
                 continue
-            rows = fields.block_shape(kind, 1, KLEV)
-            rows = int(np.prod(rows))
-            src = self.plude_in if (direction == 0 and name == "plude") else dev[name]
+            rows = int(np.prod(fields.block_shape(kind, 1, KLEV)))
             if direction == 0:
+                src = plude_in if name == "plude" else dev[name]
                 arrs.append(ColArray(src.data_ptr(), self.compact[name].data_ptr(), rows, src.element_size()))
             else:
                 arrs.append(ColArray(self.compact[name].data_ptr(), dev[name].data_ptr(), rows,
@@ -406,28 +429,34 @@ class Runner:
         return t, len(arrs)
 
     def prepare(self, dev):
-        """Per input batch set-up (outside any timed or captured region)."""
-        import torch
-        self.plude_in = torch.empty_like(dev["plude"])
-        self.cols = columns(dev, self.nproma, self.ngpblks)
-        self.gather = self._colarrays(dev, 0)
-        self.scatter = self._colarrays(dev, 1)
+        """Per-batch set-up (outside any timed or captured region)."""
+        return Batch(self, dev)
 
-    def run(self, dev):
-        """Surrogate + guard + FP64 fallback, all on the current stream."""
+    def forward_only(self, b):
+        """Input preparation and the network (no guard): for timing."""
         L, s = _lib(), _stream()
-        self.plude_in.copy_(dev["plude"])
-        _ok(L.cs_prep_inputs(ctypes.byref(self.cols), ctypes.byref(self.net.norm), _p(self.B["x0"]), s),
+        _ok(L.cs_prep_inputs(ctypes.byref(b.cols), ctypes.byref(self.net.norm), _p(self.B["x0"]), s),
             "cs_prep_inputs")
         self.net.forward(self.B, self.rows, train=False)
-        self.nflag.zero_()
-        _ok(L.cs_post(ctypes.byref(self.cols), _p(self.B["y"]), 2, ctypes.byref(self.guard), _p(self.nflag),
-                      _p(self.flagged), _p(self.diag), s), "cs_post")
-        ga, na = self.gather
-        _ok(L.cs_move_columns(_p(ga), na, self.nproma, self.nproma, _p(self.flagged), _p(self.nflag), self.cap,
+
+    def run(self, b):
+        """Surrogate + guard + FP64 fallback for batch `b`, on the current stream."""
+        L, s = _lib(), _stream()
+        self.forward_only(b)
+        b.nflag.zero_()
+        _ok(L.cs_post(ctypes.byref(b.cols), _p(self.B["y"]), 2, ctypes.byref(self.guard), _p(b.nflag),
+                      _p(b.flagged), _p(self.diag), s), "cs_post")
+        ga, na = b.gather
+        _ok(L.cs_move_columns(_p(ga), na, self.nproma, self.nproma, _p(b.flagged), _p(b.nflag), self.cap,
                               0, s), "cs_move_columns")
         cloudsc.cloudsc_batched(self.params, self.compact, self.nproma, KLEV, self.cap // self.nproma, self.cap,
                                 self.ptsphy, stream=s)
-        sa, nsa = self.scatter
-        _ok(L.cs_move_columns(_p(sa), nsa, self.nproma, self.nproma, _p(self.flagged), _p(self.nflag), self.cap,
+        sa, nsa = b.scatter
+        _ok(L.cs_move_columns(_p(sa), nsa, self.nproma, self.nproma, _p(b.flagged), _p(b.nflag), self.cap,
                               1, s), "cs_move_columns")
+
+    def flops_per_batch(self):
+        """Multiply-add FLOPs of the network's GEMMs for one batch (padded rows included)."""
+        W = self.net.width
+        per_row = 128 * W + 5 * W * W * 2 + W * W + W * 128
+        return 2.0 * self.rows * per_row

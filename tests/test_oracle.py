@@ -79,3 +79,30 @@ def test_clear_sky_has_no_precipitation(built):
     arrs["ldcum"][:] = 0
     ref, _ = util.run_oracle(po, arrs, 32, 4, 128)
     assert np.all(ref["pfplsl"] == 0.0) and np.all(ref["pfplsn"] == 0.0)
+
+
+def test_column_enthalpy_budget_closes(run):
+    """Liquid-water enthalpy: sum over levels of dp/g (LOC_T - RALVDCP (LOC_L +
+    LOC_R) - RALSDCP (LOC_I + LOC_S)) equals RALVDCP (P_rain - S_l - S_r) +
+    RALSDCP (P_snow - S_i - S_s) (surface precipitation P, detrainment
+    sources S): every phase change heats exactly by its latent heat and
+    every transport of condensate is heat-free.  This is the second budget
+    the surrogate's guard enforces (openifs_b200/csrc/surrogate_kernels.cu)."""
+    p, arrs, ref = run
+    g = p.rg
+    nc = int(p.ncldtop)
+    dp = np.diff(arrs["paph"], axis=1)
+    L = ref["tendency_loc_cld"]
+    lev = np.arange(util.KLEV)
+    loop = ((lev >= nc - 1) & (lev < util.KLEV - 1))[None, :, None]
+    active = loop & (ref["plude"] != 0.0)
+    sl = (arrs["pludeli"][:, 0] * active).sum(1)
+    si = (arrs["pludeli"][:, 1] * active).sum(1)
+    sr = (arrs["psnde"][:, 0] * loop).sum(1)
+    ss = (arrs["psnde"][:, 1] * loop).sum(1)
+    lhs = (dp / g * (ref["tendency_loc_t"] - p.ralvdcp * (L[:, 0] + L[:, 2])
+                     - p.ralsdcp * (L[:, 1] + L[:, 3]))).sum(axis=1)
+    rhs = p.ralvdcp * (ref["pfplsl"][:, -1] - sl - sr) + p.ralsdcp * (ref["pfplsn"][:, -1] - si - ss)
+    scale = (np.abs(dp / g * ref["tendency_loc_t"])).sum(axis=1) + np.abs(rhs)
+    rel = np.abs(lhs - rhs) / scale
+    assert np.median(rel) < 1e-14 and rel.max() < 1e-11, (np.median(rel), rel.max())
