@@ -63,23 +63,31 @@ typedef struct cs_columns {
   double *plude; /* INOUT: read as the input detrainment, written as CLOUDSC does */
   const double *plude_in; /* if not NULL, the input detrainment is read here instead, so
                            * that repeated calls on one batch see the same input */
+  const double *plsm;
+  const float *colsum; /* [ncol][klev][2] from cs_column_sums: condensate and
+                        * precipitation mass above each level (kg m-2) */
   double *loc_t, *loc_q, *loc_a, *loc_cld, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
   int32_t nproma, klev, ngpblks, lp; /* lp: padded rows per column (>= klev + 4) */
 } cs_columns;
 
-#define CS_NIN 14   /* input channels per level  */
+#define CS_NIN 24   /* input channels per level (also the slot stride of one tap) */
 #define CS_NOUT 9   /* output channels per level */
 
 /* Input feature transform: f = use_log ? log(x + eps) : x; (f - mean) * inv_std */
 typedef struct cs_norm {
-  float mean[16], inv_std[16], eps[16];
-  int32_t use_log[16];
+  float mean[32], inv_std[32], eps[32];
+  int32_t use_log[32];
 } cs_norm;
 
-/* Network input: x0[c*lp + 2 + l][tap*16 + ch] = feature ch of level l+tap-2
- * (zero outside the column); bf16 [ncol*lp][128]. */
+/* Column-integrated inputs the 5-level convolutions cannot reach: for every
+ * level, sum over the levels above of dp/g (l + i + r + s) and of dp/g (r + s)
+ * of the input condensates (PCLV); writes colsum (f32 [ncol][klev][2]). */
+int cs_column_sums(const cs_columns *c, float *colsum, void *stream);
+
+/* Network input: x0[c*lp + 2 + l][tap*CS_NIN + ch] = feature ch of level
+ * l+tap-2 (zero outside the column); bf16 [ncol*lp][128]. */
 int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream);
-/* Raw (untransformed) input features, f32 [ncol*lp][16], for statistics. */
+/* Raw (untransformed) input features, f32 [ncol*lp][CS_NIN]. */
 int cs_raw_features(const cs_columns *c, float *feat, void *stream);
 /* Training targets from CLOUDSC's outputs, divided by scale[ch]: f32
  * [ncol*lp][16] (LOC_T, LOC_Q, LOC_A, LOC_CLD l,i,r,s, PFPLSL, PFPLSN at the
@@ -88,7 +96,7 @@ int cs_prep_targets(const cs_columns *c, const float *scale16, float *t, void *s
 
 /* Training batch from stored features: for j < nb, batch column j is data
  * column cols[j] (device int32): x0 (bf16 [nb*lp][128]) as cs_prep_inputs
- * builds it from feat (f32 [*][16], cs_raw_features layout), and tb (f32
+ * builds it from feat (f32 [*][CS_NIN], cs_raw_features layout), and tb (f32
  * [nb*lp][16]) copied from tgt (cs_prep_targets layout). */
 int cs_prep_batch(const float *feat, const float *tgt, const int32_t *cols, int32_t nb, int32_t lp,
                   int32_t klev, const cs_norm *nrm, void *x0, float *tb, void *stream);
@@ -122,20 +130,23 @@ typedef struct cs_guard {
   float out_scale[16];   /* de-normalisation of the network outputs            */
   double rg, ralvdcp, ralsdcp, rlvtt, rlstt, ptsphy;
   int32_t ncldtop;       /* first level of CLOUDSC's level loop (1-based)      */
-  double neg_tol;        /* condensate after the step below -neg_tol: flag      */
+  double neg_tol;        /* refilled condensate / column condensate above this: flag */
   double closure_tol;    /* raw water/enthalpy non-closure above this: flag     */
   double spread_tol;     /* RMS head disagreement (normalised) above this: flag */
   int32_t capacity;      /* length of the flagged-column list                   */
 } cs_guard;
 
 /* Turn the network output y ([rows][64 * nheads] f32) into CLOUDSC
- * outputs: mean of the heads, de-normalised; surface precipitation
- * diagnosed from the column water budget and the temperature tendency
- * shifted by a column constant so that water and enthalpy close exactly;
- * PLUDE and the enthalpy fluxes as CLOUDSC defines them.  Columns failing the
- * guard are appended to flagged[0..capacity) (count in *nflagged, which must
- * start at 0); diag (float4 per column, or NULL) = {raw water non-closure,
- * raw enthalpy non-closure, head spread, flagged}. */
+ * outputs: mean of the heads, de-normalised; condensates that the step would
+ * drive negative are refilled from vapour with their latent heat (as
+ * CLOUDSC's own clean-up does, cloudsc.F90:3779-3809); LOC_Q is then shifted
+ * by a column constant so that the water budget closes with the predicted
+ * surface precipitation, and LOC_T by one so that the enthalpy budget closes;
+ * PLUDE and the enthalpy fluxes as CLOUDSC defines them.  Columns failing
+ * the guard are appended to flagged[0..capacity) (count in *nflagged, which
+ * must start at 0); diag (float4 per column, or NULL) = {raw water
+ * non-closure, raw enthalpy non-closure, head spread, refilled condensate
+ * relative to the column's condensate}. */
 int cs_post(const cs_columns *c, const float *y, int32_t nheads, const cs_guard *g, int32_t *nflagged,
             int32_t *flagged, float *diag, void *stream);
 

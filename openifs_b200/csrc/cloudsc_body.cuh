@@ -228,13 +228,16 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
     const Real pap_k = Real(pap_kd);
 
     // ---------------- first guess (:982-1002) ----------------
-    const Real t = Real(pt_k + dt * cml_t);
-    Real qv = Real(pq_k + dt * cml_q);
-    Real a = Real(pa_k + dt * cml_a);
-    const D aorig = pa_k + dt * cml_a;
+    // The state is kept in double in both kernels (tendencies are small
+    // differences of it); `Real` copies feed the process rates.
+    const D tD = pt_k + dt * cml_t;
+    D qvD = pq_k + dt * cml_q;
+    D aD = pa_k + dt * cml_a;
+    const D aorig = aD;
     const D q0_l = pc_l + dt * cl_l, q0_i = pc_i + dt * cl_i, q0_r = pc_r + dt * cl_r,
             q0_s = pc_s + dt * cl_s;
-    Real ql = Real(q0_l), qi = Real(q0_i), qr = Real(q0_r), qs = Real(q0_s);
+    D qlD = q0_l, qiD = q0_i, qrD = q0_r, qsD = q0_s;
+    const Real t = Real(tD);
 
     // ---------------- saturation (:1087-1115) ----------------
     // (only the loop levels JK >= NCLDTOP read these)
@@ -260,40 +263,42 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       zqsliq = zqsliq / (C(1.0) - P.retv * zqsliq);
     }
 
-    // ---------------- tidy up (:1127-1199) ----------------
+    // ---------------- tidy up (:1127-1199), double ----------------
     D loc_t = 0.0, loc_q = 0.0;
     D lneg_l = 0.0, lneg_i = 0.0, lneg_r = 0.0, lneg_s = 0.0;
-    if (ql + qi < P.rlmin || a < P.ramin) {
+    if (qlD + qiD < D(P.rlmin) || aD < D(P.ramin)) {
       D qadj;
-      lneg_l = lneg_l + D(ql);
-      qadj = D(ql) * zqtmst;
+      lneg_l = lneg_l + qlD;
+      qadj = qlD * zqtmst;
       loc_q = loc_q + qadj;
       loc_t = loc_t - PD.ralvdcp * qadj;
-      qv = qv + ql;
-      ql = C(0.0);
-      lneg_i = lneg_i + D(qi);
-      qadj = D(qi) * zqtmst;
+      qvD = qvD + qlD;
+      qlD = 0.0;
+      lneg_i = lneg_i + qiD;
+      qadj = qiD * zqtmst;
       loc_q = loc_q + qadj;
       loc_t = loc_t - PD.ralsdcp * qadj;
-      qv = qv + qi;
-      qi = C(0.0);
-      a = C(0.0);
+      qvD = qvD + qiD;
+      qiD = 0.0;
+      aD = 0.0;
     }
 #define TIDY(QQ, LNEG, RAL)               \
-  if (QQ < P.rlmin) {                     \
-    LNEG = LNEG + D(QQ);                  \
-    D qadj = D(QQ) * zqtmst;              \
+  if (QQ < D(P.rlmin)) {                  \
+    LNEG = LNEG + QQ;                     \
+    D qadj = QQ * zqtmst;                 \
     loc_q = loc_q + qadj;                 \
     loc_t = loc_t - PD.RAL * qadj;        \
-    qv = qv + QQ;                         \
-    QQ = C(0.0);                          \
+    qvD = qvD + QQ;                       \
+    QQ = 0.0;                             \
   }
-    TIDY(ql, lneg_l, ralvdcp)
-    TIDY(qi, lneg_i, ralsdcp)
-    TIDY(qr, lneg_r, ralvdcp)
-    TIDY(qs, lneg_s, ralsdcp)
+    TIDY(qlD, lneg_l, ralvdcp)
+    TIDY(qiD, lneg_i, ralsdcp)
+    TIDY(qrD, lneg_r, ralvdcp)
+    TIDY(qsD, lneg_s, ralsdcp)
 #undef TIDY
-    a = mx(C(0.0), mn(C(1.0), a));
+    aD = mx(0.0, mn(1.0, aD));
+    const Real qv = Real(qvD), a = Real(aD);
+    const Real ql = Real(qlD), qi = Real(qiD), qr = Real(qrD), qs = Real(qsD);
     const Real zli = ql + qi;
     Real liqfrac = C(0.0), icefrac = C(0.0);
     if (zli > P.rlmin) {
@@ -308,7 +313,10 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
 
     if (k >= ncldtop0) {
       // ================= level physics (:1228-3823) =================
-      Real qxfg_l = ql, qxfg_i = qi, qxfg_r = qr, qxfg_s = qs;
+      // running first-guess amounts (ZQXFG) in double: the limiters below take
+      // min(rate, ZQXFG) and the clean-up removes ZQXFG exactly, so the solve's
+      // residues stay at double rounding in the FP32-mixed kernel too
+      D qxfg_l = qlD, qxfg_i = qiD, qxfg_r = qrD, qxfg_s = qsD;
       Real solac = C(0.0), solab = C(0.0);
       QA q;
       q.LL = q.II = q.RR = q.SS = q.LI = q.LV = q.IR = q.IV = q.RS = q.RV = q.SV = 0.0;
@@ -316,7 +324,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       Real convsrce_l = C(0.0), convsrce_i = C(0.0), convsrce_r = C(0.0), convsrce_s = C(0.0);
       Real convsink_l = C(0.0), convsink_i = C(0.0);
       Real fallsrce_i = C(0.0), fallsrce_r = C(0.0), fallsrce_s = C(0.0);
-      Real qpretot = C(0.0);
+      D qpretot = 0.0;
       // The ZSOLQA accumulators are double in both instantiations; in the
       // FP32-mixed kernel each process rate (Real) is widened when added.
       // QADD/QSUB act on the stored entry of a pair (see struct QA); the
@@ -356,11 +364,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       const Real zlicld = zliqcld + zicecld;
 
       // evaporate very small amounts (:1334-1342)
-      if (ql < P.rlmin) {
-        q.LV = -double(ql);  // ZSOLQA(V,L) = ql, ZSOLQA(L,V) = -ql
+      if (qlD < D(P.rlmin)) {
+        q.LV = -qlD;  // ZSOLQA(V,L) = ql, ZSOLQA(L,V) = -ql
       }
-      if (qi < P.rlmin) {
-        q.IV = -double(qi);  // ZSOLQA(V,I) = qi, ZSOLQA(I,V) = -qi
+      if (qiD < D(P.rlmin)) {
+        q.IV = -qiD;  // ZSOLQA(V,I) = qi, ZSOLQA(I,V) = -qi
       }
 
       // 3.2 detrainment (:1362-1398)
@@ -540,7 +548,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
                             (mpow<F32M>(zcorr2, C(0.5)) * mpowb<F32M>(b_lam, P.rcl_const3r)));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
           Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
-          Real zevap = mn(zdpevap, qxfg_r);
+          D zevap = mn(D(zdpevap), qxfg_r);
           QSUB(RV, zevap);  // (V,R) += zevap, (R,V) -= zevap
           qxfg_r = qxfg_r - zevap;
         }
@@ -562,12 +570,12 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zcvds = C(7.8) * mpow<F32M>(zicenuclei / zrho, C(0.666)) * zsupersatice / (C(8.87) * (zadd + zbdd));
           Real zice0 = mx(zicecld, zicenuclei * P.riceinit / zrho);
           Real zinew = mpow<F32M>(C(0.666) * zcvds * rdt + mpow<F32M>(zice0, C(0.666)), C(1.5));
-          Real zdepos = mx(P.rcl_overlapliqice * a * (zinew - zice0), C(0.0));
+          D zdepos = D(mx(P.rcl_overlapliqice * a * (zinew - zice0), C(0.0)));
           zdepos = mn(zdepos, qxfg_l);
           Real zinfactor = mn(zicenuclei / C(15000.), C(1.0));
-          zdepos = zdepos * mn(zinfactor + (C(1.0) - zinfactor) *
+          zdepos = zdepos * D(mn(zinfactor + (C(1.0) - zinfactor) *
                                                (P.rdepliqrefrate + zcldtopdist / P.rdepliqrefdepth),
-                               C(1.0));
+                               C(1.0)));
           QSUB(LI, zdepos);  // (I,L) += zdepos, (L,I) -= zdepos
           qxfg_i = qxfg_i + zdepos;
           qxfg_l = qxfg_l - zdepos;
@@ -595,8 +603,8 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       }
 
       // revise in-cloud condensate (:2750-2754)
-      zliqcld = qxfg_l * ztmpa;
-      zicecld = qxfg_i * ztmpa;
+      zliqcld = Real(qxfg_l) * ztmpa;
+      zicecld = Real(qxfg_i) * ztmpa;
 
       // 4.8 ice -> snow autoconversion (:2769-2800)
       if (t <= P.rtt && zicecld > zepsec) {
@@ -609,7 +617,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
 
       // 4.12 melting (:2815-2862)
       {
-        Real zicetot = qxfg_i + qxfg_s;
+        D zicetot = qxfg_i + qxfg_s;
         Real zmeltmax = C(0.0);
         if (zicetot > zepsec && t > P.rtt) {
           Real zsubsat = mx(zqsice - qv, C(0.0));
@@ -619,13 +627,13 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           zmeltmax = mx(ztdmtw0 * zcons1 * P.zrldcp, C(0.0));
         }
         if (zmeltmax > zepsec && zicetot > zepsec) {
-          Real zalfa = qxfg_i / zicetot;
-          Real zmelt = mn(qxfg_i, zalfa * zmeltmax);
+          D zalfa = qxfg_i / zicetot;
+          D zmelt = mn(qxfg_i, zalfa * D(zmeltmax));
           qxfg_i = qxfg_i - zmelt;
           qxfg_r = qxfg_r + zmelt;
           QSUB(IR, zmelt);  // (R,I) += zmelt, (I,R) -= zmelt
           zalfa = qxfg_s / zicetot;
-          zmelt = mn(qxfg_s, zalfa * zmeltmax);
+          zmelt = mn(qxfg_s, zalfa * D(zmeltmax));
           qxfg_s = qxfg_s - zmelt;
           qxfg_r = qxfg_r + zmelt;
           QADD(RS, zmelt);  // (R,S) += zmelt, (S,R) -= zmelt
@@ -651,7 +659,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
             zfrzmax = mx((P.rtt - t) * zcons1 * P.zrldcp, C(0.0));
           }
           if (zfrzmax > zepsec) {
-            Real zfrz = mn(qr, zfrzmax);
+            D zfrz = mn(qrD, D(zfrzmax));
             QSUB(RS, zfrz);  // (S,R) += zfrz, (R,S) -= zfrz
           }
         }
@@ -661,7 +669,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       {
         Real zfrzmax = mx((P.rthomo - t) * P.zrldcp, C(0.0));
         if (zfrzmax > zepsec && qxfg_l > zepsec) {
-          Real zfrz = mn(qxfg_l, zfrzmax);
+          D zfrz = mn(qxfg_l, D(zfrzmax));
           QSUB(LI, zfrz);  // (I,L) += zfrz, (L,I) -= zfrz
         }
       }
@@ -710,15 +718,15 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         zqe = mx(C(0.0), mn(zqe, zqsice));
         if (zcovpclr > zepsec && qxfg_s > zepsec && zqe < zzrh * zqsice) {
           Real aa = zcovptot * zdtgdp;
-          Real zpreclr = qxfg_s * zcovpclr / xsign(mx(xabs(aa), zepsilon), aa);
+          Real zpreclr = Real(qxfg_s) * zcovpclr / xsign(mx(xabs(aa), zepsilon), aa);
           Real zbeta1 = xsqrt(pap_k / Real(paph_surf)) / P.rvrfactor * zpreclr / mx(zcovpclr, zepsec);
           Real zbeta = P.rg * P.rpecons * mpow<F32M>(zbeta1, C(0.5777));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsice;
           Real zdpr = zcovpclr * zbeta * (zqsice - zqe) / zdenom * zdp * P.zrg_r;
           Real zdpevap = zdpr * zdtgdp;
-          Real zevap = mn(zdpevap, qxfg_s);
+          D zevap = mn(D(zdpevap), qxfg_s);
           QSUB(SV, zevap);  // (V,S) += zevap, (S,V) -= zevap
-          zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), (zcovptot - a) * zevap / qxfg_s));
+          zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), Real(D(zcovptot - a) * zevap / qxfg_s)));
           qxfg_s = qxfg_s - zevap;
         }
       }
@@ -742,7 +750,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
 
       // 5.2.1 sink truncation (:3455-3536), double: ratios, insertion sort
       // (IORDV, stable for ties), rows rescaled in sorted order
-      const double qx[5] = {double(ql), double(qi), double(qr), double(qs), double(qv)};
+      const double qx[5] = {qlD, qiD, qrD, qsD, qvD};
       {
         double ratio[5];
         sink_ratios(q, qx, ratio);
@@ -824,18 +832,18 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       {
         D fq;
         fq = D(convsrce_l) + 0.0 - (0.0 + D(convsink_l)) * x_l;
-        loc_t = loc_t + PD.ralvdcp * (x_l - D(ql) - fq) * zqtmst;
+        loc_t = loc_t + PD.ralvdcp * (x_l - qlD - fq) * zqtmst;
         loc_cl = 0.0 + (x_l - q0_l) * zqtmst;
         fq = D(convsrce_i) + D(fallsrce_i) - (D(fallsink_i) + D(convsink_i)) * x_i;
-        loc_t = loc_t + PD.ralsdcp * (x_i - D(qi) - fq) * zqtmst;
+        loc_t = loc_t + PD.ralsdcp * (x_i - qiD - fq) * zqtmst;
         loc_ci = 0.0 + (x_i - q0_i) * zqtmst;
         fq = D(convsrce_r) + D(fallsrce_r) - (D(fallsink_r) + 0.0) * x_r;
-        loc_t = loc_t + PD.ralvdcp * (x_r - D(qr) - fq) * zqtmst;
+        loc_t = loc_t + PD.ralvdcp * (x_r - qrD - fq) * zqtmst;
         loc_cr = 0.0 + (x_r - q0_r) * zqtmst;
         fq = D(convsrce_s) + D(fallsrce_s) - (D(fallsink_s) + 0.0) * x_s;
-        loc_t = loc_t + PD.ralsdcp * (x_s - D(qs) - fq) * zqtmst;
+        loc_t = loc_t + PD.ralsdcp * (x_s - qsD - fq) * zqtmst;
         loc_cs = 0.0 + (x_s - q0_s) * zqtmst;
-        loc_q = loc_q + (x_v - D(qv)) * zqtmst;
+        loc_q = loc_q + (x_v - qvD) * zqtmst;
         loc_a = 0.0 + zda * zqtmst;
       }
       // 6.4 supersaturation check (:3765-3809), double

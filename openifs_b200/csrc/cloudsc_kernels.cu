@@ -64,6 +64,11 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
       ib = 0;
       jl = sh.kidia0;
     }
+    // FP32-mixed: FP32 transcendentals, everything else in double.  (Process
+    // rates in float as well were measured at 2.06x the FP64 kernel but with
+    // 0.3-4 % tendency errors: float rounding of the rates leaves residues
+    // above CLOUDSC's 1e-14 kg/kg thresholds, which switch precipitation
+    // processes on and off down the column.)
     cloudsc_column<double, F32M>(F, sh, ib, jl, active);
   }
 }

@@ -43,9 +43,14 @@ struct Cols {
   __device__ __forceinline__ size_t o1(int col) const { return (size_t)col; }
 };
 
-// The 14 raw input features of (column, level): T, q, p, the four
-// condensates, PLUDE (detrained condensate), cloud fraction, the convective
-// mass flux PMFU + PMFD, and the forcing tendencies of T, q, a and l + i.
+// The CS_NIN raw input features of (column, level): the 14 fields T, q, p,
+// the four condensates, PLUDE (detrained condensate), cloud fraction, the
+// convective mass flux PMFU + PMFD and the forcing tendencies of T, q, a and
+// l + i; then the other fields CLOUDSC reads: PMFU and PMFD apart, the
+// updraught condensate PLU, the detrained liquid + ice PLUDELI and rain +
+// snow PSNDE, the layer thickness dp, LDCUM, PLSM, and the condensate and
+// precipitation mass above the level (cs_column_sums).  PVFL and PVFI are
+// left out: in CLOUDSC they enter only the DDH flux diagnostics.
 __device__ __forceinline__ void raw_features(const Cols &C, int col, int k, float f[CS_NIN]) {
   const cs_columns &c = C.c;
   const size_t o = C.o2(col, k);
@@ -61,6 +66,26 @@ __device__ __forceinline__ void raw_features(const Cols &C, int col, int k, floa
   f[11] = (float)c.cml_q[o];
   f[12] = (float)c.cml_a[o];
   f[13] = (float)(c.cml_cld[C.o3(col, 0, 5, k)] + c.cml_cld[C.o3(col, 1, 5, k)]);
+  f[14] = (float)c.pmfu[o];
+  f[15] = (float)c.pmfd[o];
+  f[16] = (float)c.plu[o];
+  f[17] = (float)(c.pludeli[C.o3(col, 0, 4, k)] + c.pludeli[C.o3(col, 1, 4, k)]);
+  f[18] = (float)(c.psnde[C.o3(col, 0, 2, k)] + c.psnde[C.o3(col, 1, 2, k)]);
+  f[19] = (float)(c.paph[C.oh(col, k + 1)] - c.paph[C.oh(col, k)]);
+  f[20] = c.ldcum[C.o1(col)] ? 1.0f : 0.0f;
+  f[21] = (float)c.plsm[C.o1(col)];
+  const float *cs = c.colsum + ((size_t)col * c.klev + k) * 2;
+  f[22] = cs[0];
+  f[23] = cs[1];
+}
+
+__device__ __forceinline__ void norm_features(const cs_norm &nrm, const float f[CS_NIN], __nv_bfloat16 *dst) {
+#pragma unroll
+  for (int ch = 0; ch < CS_NIN; ++ch) {
+    float x = f[ch];
+    if (nrm.use_log[ch]) x = __logf(fmaxf(x, 0.0f) + nrm.eps[ch]);
+    dst[ch] = __float2bfloat16((x - nrm.mean[ch]) * nrm.inv_std[ch]);
+  }
 }
 
 // Threads are numbered level-major (row r of every column, then the next
@@ -71,18 +96,16 @@ __global__ void raw_features_kernel(Cols C, float *feat) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
     const int k = r - 2;
-    float f[CS_NIN];
+    __align__(16) float f[CS_NIN];
     if (k >= 0 && k < C.c.klev) {
       raw_features(C, col, k, f);
     } else {
 #pragma unroll
       for (int i = 0; i < CS_NIN; ++i) f[i] = 0.0f;
     }
-    float4 *d = (float4 *)(feat + ((size_t)col * lp + r) * 16);
-    d[0] = make_float4(f[0], f[1], f[2], f[3]);
-    d[1] = make_float4(f[4], f[5], f[6], f[7]);
-    d[2] = make_float4(f[8], f[9], f[10], f[11]);
-    d[3] = make_float4(f[12], f[13], 0.0f, 0.0f);
+    float4 *d = (float4 *)(feat + ((size_t)col * lp + r) * CS_NIN);
+#pragma unroll
+    for (int i = 0; i < CS_NIN / 4; ++i) d[i] = ((float4 *)f)[i];
   }
 }
 
@@ -96,23 +119,36 @@ __global__ void prep_inputs_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *x0) {
 #pragma unroll
     for (int i = 0; i < 128; ++i) row[i] = __float2bfloat16(0.0f);
     if (k >= 0 && k < klev) {
-#pragma unroll 1
+#pragma unroll
       for (int tap = 0; tap < 5; ++tap) {
         const int ks = k + tap - 2;
         if (ks < 0 || ks >= klev) continue;
         float f[CS_NIN];
         raw_features(C, col, ks, f);
-#pragma unroll
-        for (int ch = 0; ch < CS_NIN; ++ch) {
-          float x = f[ch];
-          if (nrm.use_log[ch]) x = __logf(fmaxf(x, 0.0f) + nrm.eps[ch]);
-          row[tap * 16 + ch] = __float2bfloat16((x - nrm.mean[ch]) * nrm.inv_std[ch]);
-        }
+        norm_features(nrm, f, row + tap * CS_NIN);
       }
     }
     uint4 *d = (uint4 *)(x0 + ((size_t)col * lp + r) * 128);
 #pragma unroll
     for (int i = 0; i < 16; ++i) d[i] = ((uint4 *)row)[i];
+  }
+}
+
+__global__ void column_sums_kernel(Cols C, float *colsum) {
+  const int ncol = C.c.nproma * C.c.ngpblks, klev = C.c.klev;
+  for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += gridDim.x * blockDim.x) {
+    const cs_columns &c = C.c;
+    double all = 0.0, prc = 0.0;
+    for (int k = 0; k < klev; ++k) {
+      float *d = colsum + ((size_t)col * klev + k) * 2;
+      d[0] = (float)all;
+      d[1] = (float)prc;
+      const double dpg = (c.paph[C.oh(col, k + 1)] - c.paph[C.oh(col, k)]) / 9.80665;
+      const double ql = c.pclv[C.o3(col, 0, 5, k)], qi = c.pclv[C.o3(col, 1, 5, k)];
+      const double qr = c.pclv[C.o3(col, 2, 5, k)], qs = c.pclv[C.o3(col, 3, 5, k)];
+      all += dpg * (fmax(ql, 0.0) + fmax(qi, 0.0) + fmax(qr, 0.0) + fmax(qs, 0.0));
+      prc += dpg * (fmax(qr, 0.0) + fmax(qs, 0.0));
+    }
   }
 }
 
@@ -161,22 +197,11 @@ __global__ void prep_batch_kernel(const float *__restrict__ feat, const float *_
       for (int tap = 0; tap < 5; ++tap) {
         const int ks = k + tap - 2;
         if (ks < 0 || ks >= klev) continue;
-        const float4 *f4 = (const float4 *)(feat + (src + 2 + ks) * 16);
-        float f[16];
+        const float4 *f4 = (const float4 *)(feat + (src + 2 + ks) * CS_NIN);
+        __align__(16) float f[CS_NIN];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const float4 v = f4[q];
-          f[4 * q] = v.x;
-          f[4 * q + 1] = v.y;
-          f[4 * q + 2] = v.z;
-          f[4 * q + 3] = v.w;
-        }
-#pragma unroll
-        for (int ch = 0; ch < CS_NIN; ++ch) {
-          float x = f[ch];
-          if (nrm.use_log[ch]) x = __logf(fmaxf(x, 0.0f) + nrm.eps[ch]);
-          row[tap * 16 + ch] = __float2bfloat16((x - nrm.mean[ch]) * nrm.inv_std[ch]);
-        }
+        for (int q = 0; q < CS_NIN / 4; ++q) ((float4 *)f)[q] = f4[q];
+        norm_features(nrm, f, row + tap * CS_NIN);
       }
     }
     uint4 *d = (uint4 *)(x0 + ((size_t)j * lp + r) * 128);
@@ -306,25 +331,27 @@ __global__ void adamw_kernel(float *p, float *g, float *m, float *v, int taps, i
 }
 
 // ---------------------------------------------------------------- guard
-// One thread per column.  Pass 1 over the levels: de-normalise, write the
-// outputs, accumulate the budgets and the guard quantities; then the surface
-// precipitation from the water budget and a column-constant LOC_T shift that
-// closes the enthalpy budget; pass 2 applies the shift and writes the
-// enthalpy fluxes.
+// One thread per column.  Pass 1 over the levels: de-normalise, refill
+// condensates the step would drive negative (from vapour, with the latent
+// heat), write the outputs, accumulate the budgets and the guard quantities.
+// Pass 2: the column-constant LOC_Q and LOC_T shifts that close the water and
+// enthalpy budgets with the predicted surface precipitation, and the enthalpy
+// fluxes.
 __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_guard gd, int *nflagged,
                             int *flagged, float4 *diag) {
   const int ys = 64 * nheads;
   const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
   const int k0 = gd.ncldtop - 1;  // first level of CLOUDSC's level loop
   const double dt = gd.ptsphy, rg = gd.rg;
+  const double ral[4] = {gd.ralvdcp, gd.ralsdcp, gd.ralvdcp, gd.ralsdcp};  // l, i, r, s
   for (int col = blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += gridDim.x * blockDim.x) {
     const cs_columns &c = C.c;
     double w_lhs = 0.0, w_abs = 0.0, e_lhs = 0.0, e_abs = 0.0;
     double s_l = 0.0, s_i = 0.0, s_r = 0.0, s_s = 0.0, mass = 0.0, spread2 = 0.0;
+    double refill = 0.0, cond = 0.0;
     int spread_n = 0;
-    bool negative = false;
     const bool ldcum = c.ldcum[C.o1(col)] != 0;
-    double pr_pred = 0.0, ps_pred = 0.0;
+    double pr = 0.0, ps = 0.0;
     for (int k = 0; k < klev; ++k) {
       const size_t r = (size_t)col * lp + 2 + k;
       float yv[CS_NOUT];
@@ -344,20 +371,33 @@ __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_
       const size_t o = C.o2(col, k);
       const double dp = c.paph[C.oh(col, k + 1)] - c.paph[C.oh(col, k)];
       const double dpg = dp / rg;
-      const double lt = yv[0], lq = yv[1], la = yv[2], ll = yv[3], li = yv[4], lr = yv[5], ls = yv[6];
-      c.loc_t[o] = lt;
-      c.loc_q[o] = lq;
+      double lt = yv[0], lq = yv[1];
+      const double la = yv[2];
+      double lc[4] = {yv[3], yv[4], yv[5], yv[6]};
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const double q0 = c.pclv[C.o3(col, m, 5, k)] + dt * c.cml_cld[C.o3(col, m, 5, k)];
+        cond += dpg * fmax(q0, 0.0);
+        const double qn = q0 + dt * lc[m];
+        if (qn < 0.0) {  // refill from vapour (cloudsc.F90:3779-3809 does the same for l, i)
+          const double d = -qn / dt;
+          lc[m] += d;
+          lq -= d;
+          lt += ral[m] * d;
+          refill += dpg * d * dt;
+        }
+      }
       c.loc_a[o] = la;
-      c.loc_cld[C.o3(col, 0, 5, k)] = ll;
-      c.loc_cld[C.o3(col, 1, 5, k)] = li;
-      c.loc_cld[C.o3(col, 2, 5, k)] = lr;
-      c.loc_cld[C.o3(col, 3, 5, k)] = ls;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) c.loc_cld[C.o3(col, m, 5, k)] = lc[m];
+      c.loc_q[o] = lq;
+      c.loc_t[o] = lt;
       if (k + 1 < klev) {
         c.pfplsl[C.oh(col, k + 1)] = fmax((double)yv[7], 0.0);
         c.pfplsn[C.oh(col, k + 1)] = fmax((double)yv[8], 0.0);
       } else {
-        pr_pred = fmax((double)yv[7], 0.0);
-        ps_pred = fmax((double)yv[8], 0.0);
+        pr = fmax((double)yv[7], 0.0);
+        ps = fmax((double)yv[8], 0.0);
       }
       // convective detrainment exactly as CLOUDSC applies it (cloudsc.F90:1362-1398)
       if (k >= k0 && k + 1 < klev) {
@@ -374,46 +414,41 @@ __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_
         s_s += c.psnde[C.o3(col, 1, 2, k)];
         c.plude[o] = plude_out;
       }
-      w_lhs += dpg * (lq + ll + li + lr + ls);
-      w_abs += fabs(dpg * lq) + fabs(dpg * (ll + li + lr + ls));
-      e_lhs += dpg * (lt - gd.ralvdcp * (ll + lr) - gd.ralsdcp * (li + ls));
+      w_lhs += dpg * (lq + lc[0] + lc[1] + lc[2] + lc[3]);
+      w_abs += fabs(dpg * lq) + fabs(dpg * (lc[0] + lc[1] + lc[2] + lc[3]));
+      e_lhs += dpg * (lt - gd.ralvdcp * (lc[0] + lc[2]) - gd.ralsdcp * (lc[1] + lc[3]));
       e_abs += fabs(dpg * lt);
       mass += dpg;
-      // the condensates after the step must not go negative
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const double q = c.pclv[C.o3(col, m, 5, k)] + dt * (c.cml_cld[C.o3(col, m, 5, k)] + (double)yv[3 + m]);
-        if (q < -gd.neg_tol) negative = true;
-      }
     }
-    // surface precipitation from the water budget, split as the heads predict
-    const double ptot = (s_l + s_i + s_r + s_s) - w_lhs;
-    const double praw = pr_pred + ps_pred;
-    const double w_raw = fabs(praw - ptot) / (w_abs + fabs(ptot) + fabs(praw) + 1e-30);
-    const double frac = praw > 0.0 ? pr_pred / praw : 0.5;
-    const double pr = frac * ptot, ps = ptot - pr;
+    // water: shift LOC_Q so that sum dp/g (q + condensates) = S - P
+    const double w_rhs = (s_l + s_i + s_r + s_s) - (pr + ps);
+    const double w_res = w_lhs - w_rhs;
+    const double w_raw = fabs(w_res) / (w_abs + fabs(w_rhs) + 1e-30);
+    const double qshift = w_res / mass;
+    // enthalpy: shift LOC_T (the LOC_Q shift does not enter this budget)
+    const double e_rhs = gd.ralvdcp * (pr - s_l - s_r) + gd.ralsdcp * (ps - s_i - s_s);
+    const double e_res = e_lhs - e_rhs;
+    const double e_raw = fabs(e_res) / (e_abs + fabs(e_rhs) + 1e-30);
+    const double tshift = e_res / mass;
+    for (int k = 0; k < klev; ++k) {
+      const size_t o = C.o2(col, k);
+      c.loc_q[o] = c.loc_q[o] - qshift;
+      c.loc_t[o] = c.loc_t[o] - tshift;
+    }
     c.pfplsl[C.oh(col, klev)] = pr;
     c.pfplsn[C.oh(col, klev)] = ps;
     c.pfplsl[C.oh(col, 0)] = 0.0;
     c.pfplsn[C.oh(col, 0)] = 0.0;
-    // enthalpy: a column-constant LOC_T shift closes the budget
-    const double e_rhs = gd.ralvdcp * (pr - s_l - s_r) + gd.ralsdcp * (ps - s_i - s_s);
-    const double e_res = e_lhs - e_rhs;
-    const double e_raw = fabs(e_res) / (e_abs + fabs(e_rhs) + 1e-30);
-    const double shift = e_res / mass;
-    for (int k = 0; k < klev; ++k) {
-      const size_t o = C.o2(col, k);
-      c.loc_t[o] = c.loc_t[o] - shift;
-    }
     for (int k = 0; k <= klev; ++k) {
       const size_t oo = C.oh(col, k);
       c.pfhpsl[oo] = -gd.rlvtt * c.pfplsl[oo];
       c.pfhpsn[oo] = -gd.rlstt * c.pfplsn[oo];
     }
     const double spread = spread_n ? sqrt(spread2 / spread_n) : 0.0;
-    const bool flag = negative || ptot < 0.0 || w_raw > gd.closure_tol || e_raw > gd.closure_tol ||
+    const double refill_rel = refill / (cond + 1e-12);
+    const bool flag = refill_rel > gd.neg_tol || w_raw > gd.closure_tol || e_raw > gd.closure_tol ||
                       (nheads == 2 && spread > gd.spread_tol);
-    if (diag) diag[col] = make_float4((float)w_raw, (float)e_raw, (float)spread, flag ? 1.0f : 0.0f);
+    if (diag) diag[col] = make_float4((float)w_raw, (float)e_raw, (float)spread, (float)refill_rel);
     if (flag) {
       const int slot = atomicAdd(nflagged, 1);
       if (slot < gd.capacity) flagged[slot] = col;
@@ -468,16 +503,24 @@ extern "C" {
 
 int cs_raw_features(const cs_columns *c, float *feat, void *stream) {
   using namespace sk;
-  if (!cols_ok(c) || !feat) return CS_E_ARG;
+  if (!cols_ok(c) || !feat || !c->colsum) return CS_E_ARG;
   Cols C{*c};
   const long long n = (long long)c->nproma * c->ngpblks * c->lp;
   raw_features_kernel<<<grid_1d(n, 256), 256, 0, (cudaStream_t)stream>>>(C, feat);
   return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
 }
 
+int cs_column_sums(const cs_columns *c, float *colsum, void *stream) {
+  using namespace sk;
+  if (!cols_ok(c) || !colsum) return CS_E_ARG;
+  Cols C{*c};
+  column_sums_kernel<<<grid_1d((long long)c->nproma * c->ngpblks, 128), 128, 0, (cudaStream_t)stream>>>(C, colsum);
+  return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
 int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream) {
   using namespace sk;
-  if (!cols_ok(c) || !nrm || !x0) return CS_E_ARG;
+  if (!cols_ok(c) || !nrm || !x0 || !c->colsum) return CS_E_ARG;
   Cols C{*c};
   const long long n = (long long)c->nproma * c->ngpblks * c->lp;
   prep_inputs_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)x0);

@@ -38,14 +38,18 @@ from . import cloudsc, fields, tcgemm
 
 LP = 144
 KLEV = 137
-NIN, NOUT = 14, 9
+NIN, NOUT = 24, 9
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "data", "surrogate_w128.npz")
 
-# input channels: (name, log transform epsilon or None)
+# input channels: (name, log transform epsilon or None).  The first 14 are the
+# fields of the workload description; the rest are the other fields CLOUDSC
+# reads (with the 14 alone the held-out tendency error was ~37 % RMS).
 IN_CHANNELS = [("t", None), ("q", 1e-8), ("p", 1.0), ("ql", 1e-9), ("qi", 1e-9), ("qr", 1e-9),
                ("qs", 1e-9), ("plude", 1e-10), ("a", None), ("mflux", None), ("cml_t", None),
-               ("cml_q", None), ("cml_a", None), ("cml_li", None)]
+               ("cml_q", None), ("cml_a", None), ("cml_li", None),
+               ("pmfu", None), ("pmfd", None), ("plu", 1e-7), ("pludeli", 1e-10), ("psnde", 1e-10),
+               ("dp", None), ("ldcum", None), ("plsm", None), ("cond_above", 1e-4), ("prec_above", 1e-4)]
 OUT_CHANNELS = ["loc_t", "loc_q", "loc_a", "loc_l", "loc_i", "loc_r", "loc_s", "pfplsl", "pfplsn"]
 
 
@@ -53,15 +57,15 @@ OUT_CHANNELS = ["loc_t", "loc_q", "loc_a", "loc_l", "loc_i", "loc_r", "loc_s", "
 class Columns(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in
                 ["pt", "pq", "pap", "paph", "pclv", "pa", "pmfu", "pmfd", "cml_t", "cml_q", "cml_a",
-                 "cml_cld", "plu", "pludeli", "psnde", "ldcum", "plude", "plude_in", "loc_t", "loc_q",
-                 "loc_a", "loc_cld", "pfplsl", "pfplsn", "pfhpsl", "pfhpsn"]] + \
+                 "cml_cld", "plu", "pludeli", "psnde", "ldcum", "plude", "plude_in", "plsm", "colsum",
+                 "loc_t", "loc_q", "loc_a", "loc_cld", "pfplsl", "pfplsn", "pfhpsl", "pfhpsn"]] + \
                [("nproma", ctypes.c_int32), ("klev", ctypes.c_int32), ("ngpblks", ctypes.c_int32),
                 ("lp", ctypes.c_int32)]
 
 
 class Norm(ctypes.Structure):
-    _fields_ = [("mean", ctypes.c_float * 16), ("inv_std", ctypes.c_float * 16),
-                ("eps", ctypes.c_float * 16), ("use_log", ctypes.c_int32 * 16)]
+    _fields_ = [("mean", ctypes.c_float * 32), ("inv_std", ctypes.c_float * 32),
+                ("eps", ctypes.c_float * 32), ("use_log", ctypes.c_int32 * 32)]
 
 
 class Adam(ctypes.Structure):
@@ -90,6 +94,7 @@ def _lib():
         L = cloudsc.lib()
         vp, i32 = ctypes.c_void_p, ctypes.c_int32
         L.cs_raw_features.argtypes = [ctypes.POINTER(Columns), vp, vp]
+        L.cs_column_sums.argtypes = [ctypes.POINTER(Columns), vp, vp]
         L.cs_prep_inputs.argtypes = [ctypes.POINTER(Columns), ctypes.POINTER(Norm), vp, vp]
         L.cs_prep_targets.argtypes = [ctypes.POINTER(Columns), vp, vp, vp]
         L.cs_prep_batch.argtypes = [vp, vp, vp, i32, i32, i32, ctypes.POINTER(Norm), vp, vp, vp]
@@ -98,7 +103,7 @@ def _lib():
         L.cs_adamw.argtypes = [vp, vp, vp, vp, i32, i32, i32, ctypes.POINTER(Adam), vp, vp, vp]
         L.cs_post.argtypes = [ctypes.POINTER(Columns), vp, i32, ctypes.POINTER(Guard), vp, vp, vp, vp]
         L.cs_move_columns.argtypes = [vp, i32, i32, i32, vp, vp, i32, i32, vp]
-        for f in ["cs_raw_features", "cs_prep_inputs", "cs_prep_targets", "cs_prep_batch", "cs_loss",
+        for f in ["cs_raw_features", "cs_column_sums", "cs_prep_inputs", "cs_prep_targets", "cs_prep_batch", "cs_loss",
                   "cs_wgrad", "cs_adamw", "cs_post", "cs_move_columns"]:
             getattr(L, f).restype = ctypes.c_int
         _L = L
@@ -119,17 +124,19 @@ def _stream():
     return torch.cuda.current_stream().cuda_stream
 
 
-def columns(dev, nproma, ngpblks, klev=KLEV, lp=LP, plude_in=None):
+def columns(dev, nproma, ngpblks, colsum, klev=KLEV, lp=LP, plude_in=None):
     """Columns struct over CLOUDSC batched device tensors (fields.BATCHED_FIELDS
-    names); plude_in: a separate tensor holding the input PLUDE, or None."""
+    names); colsum: f32 [ncol, klev, 2] work tensor for cs_column_sums;
+    plude_in: a separate tensor holding the input PLUDE, or None."""
     c = Columns()
     c.plude_in = None if plude_in is None else plude_in.data_ptr()
+    c.colsum = colsum.data_ptr()
     m = {"pt": "pt", "pq": "pq", "pap": "pap", "paph": "paph", "pclv": "pclv", "pa": "pa", "pmfu": "pmfu",
          "pmfd": "pmfd", "cml_t": "tendency_cml_t", "cml_q": "tendency_cml_q", "cml_a": "tendency_cml_a",
          "cml_cld": "tendency_cml_cld", "plu": "plu", "pludeli": "pludeli", "psnde": "psnde",
          "ldcum": "ldcum", "plude": "plude", "loc_t": "tendency_loc_t", "loc_q": "tendency_loc_q",
          "loc_a": "tendency_loc_a", "loc_cld": "tendency_loc_cld", "pfplsl": "pfplsl", "pfplsn": "pfplsn",
-         "pfhpsl": "pfhpsl", "pfhpsn": "pfhpsn"}
+         "pfhpsl": "pfhpsl", "pfhpsn": "pfhpsn", "plsm": "plsm"}
     for k, v in m.items():
         setattr(c, k, dev[v].data_ptr())
     c.nproma, c.klev, c.ngpblks, c.lp = nproma, klev, ngpblks, lp
@@ -165,7 +172,7 @@ class Net:
         self.step_count = 0
         self.norm = Norm()
         self.out_scale = np.ones(16, np.float32)
-        self.guard_tols = (1e-7, 0.5, 0.25)  # negative condensate, raw closure, head spread
+        self.guard_tols = (0.05, 0.5, 0.25)  # refilled condensate, raw closure, head spread
         self.sync_bf16()
 
     def sync_bf16(self):
@@ -282,7 +289,7 @@ class Dataset:
         from . import inputs
         ncol_chunk = nblk * nproma
         self.ncol = ncol_chunk * nchunks
-        self.feat = torch.empty(self.ncol * LP, 16, device="cuda")
+        self.feat = torch.empty(self.ncol * LP, NIN, device="cuda")
         self.tgt = torch.empty(self.ncol * LP, 16, device="cuda")
         L, ones = _lib(), np.ones(16, np.float32)
         cloudsc.setup(params)
@@ -290,8 +297,10 @@ class Dataset:
             host = inputs.generate(nblk, nproma, params, seed=seed0 + ch)
             dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
             del host
-            c = columns(dev, nproma, nblk)
+            colsum = torch.empty(ncol_chunk, KLEV, 2, device="cuda")
+            c = columns(dev, nproma, nblk, colsum)
             sl = slice(ch * ncol_chunk * LP, (ch + 1) * ncol_chunk * LP)
+            _ok(L.cs_column_sums(ctypes.byref(c), _p(colsum), _stream()), "cs_column_sums")
             _ok(L.cs_raw_features(ctypes.byref(c), _p(self.feat[sl]), _stream()), "cs_raw_features")
             cloudsc.cloudsc_batched(params, dev, nproma, KLEV, nblk, ncol_chunk, ptsphy)
             _ok(L.cs_prep_targets(ctypes.byref(c), ones.ctypes.data, _p(self.tgt[sl]), _stream()),
@@ -317,7 +326,7 @@ class Dataset:
                 x = torch.log(torch.clamp(x, min=0.0) + eps)
                 norm.use_log[ch], norm.eps[ch] = 1, eps
             mu, sd = float(x.mean()), float(x.std())
-            norm.mean[ch], norm.inv_std[ch] = mu, 1.0 / max(sd, 1e-30)
+            norm.mean[ch], norm.inv_std[ch] = mu, (1.0 / sd if sd > 0 else 0.0)
         t = self.tgt[idx].double()
         scale = np.ones(16, np.float32)
         for ch in range(NOUT):
@@ -372,7 +381,8 @@ class Batch:
         import torch
         self.dev = dev
         self.plude_in = dev["plude"].clone()
-        self.cols = columns(dev, runner.nproma, runner.ngpblks, plude_in=self.plude_in)
+        self.colsum = torch.empty(runner.ncol, KLEV, 2, device="cuda")
+        self.cols = columns(dev, runner.nproma, runner.ngpblks, self.colsum, plude_in=self.plude_in)
         self.gather = runner._colarrays(dev, self.plude_in, 0)
         self.scatter = runner._colarrays(dev, self.plude_in, 1)
         self.nflag = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -435,6 +445,7 @@ class Runner:
     def forward_only(self, b):
         """Input preparation and the network (no guard): for timing."""
         L, s = _lib(), _stream()
+        _ok(L.cs_column_sums(ctypes.byref(b.cols), _p(b.colsum), s), "cs_column_sums")
         _ok(L.cs_prep_inputs(ctypes.byref(b.cols), ctypes.byref(self.net.norm), _p(self.B["x0"]), s),
             "cs_prep_inputs")
         self.net.forward(self.B, self.rows, train=False)

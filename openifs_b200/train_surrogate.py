@@ -7,9 +7,8 @@ calibrate its guard.
 Each chunk is 262,144 seeded synthetic columns (2,048 NPROMA blocks of 128,
 openifs_b200/inputs.py) that cloudsc_b200_batched (FP64) turns into targets.
 A held-out chunk (another seed) gives the reported errors and the guard
-thresholds: the head-spread and raw-closure tolerances are set at the
-`--flag-quantile` quantile of the held-out columns, the negative-condensate
-tolerance is fixed.  The weights, input/output normalisation, thresholds and
+thresholds: the head-spread, raw-closure and refilled-condensate tolerances are each set
+at the `--flag-quantile` quantile of the held-out columns.  The weights, input/output normalisation, thresholds and
 the held-out statistics go into one .npz (and a .json beside it).
 """
 import argparse
@@ -26,7 +25,7 @@ def _log(msg):
     print(msg, flush=True)
 
 
-def evaluate(net, params, seed, nblk=2048, nproma=128, flag_quantile=0.98, neg_tol=1e-7):
+def evaluate(net, params, seed, nblk=2048, nproma=128, flag_quantile=0.99):
     """Held-out errors of the raw network and of the guarded surrogate."""
     import torch
     from . import cloudsc, inputs, surrogate as S
@@ -37,6 +36,7 @@ def evaluate(net, params, seed, nblk=2048, nproma=128, flag_quantile=0.98, neg_t
     dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
     del host
     ncol = nproma * nblk
+    plude0 = dev["plude"].clone()
     # calibration pass: nothing flagged, diagnostics only
     run = S.Runner(net, params, nproma, nblk, capacity=nproma, neg_tol=1e30, closure_tol=1e30, spread_tol=1e30)
     b = run.prepare(dev)
@@ -45,10 +45,12 @@ def evaluate(net, params, seed, nblk=2048, nproma=128, flag_quantile=0.98, neg_t
     diag = run.diag.cpu().numpy()
     spread_tol = float(np.quantile(diag[:, 2], flag_quantile))
     closure_tol = float(np.quantile(np.maximum(diag[:, 0], diag[:, 1]), flag_quantile))
+    neg_tol = float(np.quantile(diag[:, 3], flag_quantile))
     raw_err = _errors(dev, ref)
     # guarded pass
     del run, b
     torch.cuda.empty_cache()
+    dev["plude"].copy_(plude0)  # the first pass wrote PLUDE's output
     cap = int(math.ceil(0.0625 * ncol))
     run = S.Runner(net, params, nproma, nblk, capacity=cap, neg_tol=neg_tol, closure_tol=closure_tol,
                    spread_tol=spread_tol)
@@ -86,7 +88,7 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--width", type=int, default=128)
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--flag-quantile", type=float, default=0.98)
+    ap.add_argument("--flag-quantile", type=float, default=0.99)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     import torch
