@@ -67,10 +67,13 @@ typedef struct cs_columns {
   const float *colsum; /* [ncol][klev][2] from cs_column_sums: condensate and
                         * precipitation mass above each level (kg m-2) */
   double *loc_t, *loc_q, *loc_a, *loc_cld, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
+  /* saturation constants (cloudsc_params names) for the humidity features */
+  double r2es, r3les, r3ies, r4les, r4ies, rtt, rtice, rtwat, retv, ptsphy;
   int32_t nproma, klev, ngpblks, lp; /* lp: padded rows per column (>= klev + 4) */
 } cs_columns;
 
-#define CS_NIN 24   /* input channels per level (also the slot stride of one tap) */
+#define CS_NIN 25   /* input channels per level (also the slot stride of one tap) */
+#define CS_FSTRIDE 28 /* floats per row of the raw-feature buffer (16-byte rows) */
 #define CS_NOUT 9   /* output channels per level */
 
 /* Input feature transform: f = use_log ? log(x + eps) : x; (f - mean) * inv_std */
@@ -87,7 +90,7 @@ int cs_column_sums(const cs_columns *c, float *colsum, void *stream);
 /* Network input: x0[c*lp + 2 + l][tap*CS_NIN + ch] = feature ch of level
  * l+tap-2 (zero outside the column); bf16 [ncol*lp][128]. */
 int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream);
-/* Raw (untransformed) input features, f32 [ncol*lp][CS_NIN]. */
+/* Raw (untransformed) input features, f32 [ncol*lp][CS_FSTRIDE]. */
 int cs_raw_features(const cs_columns *c, float *feat, void *stream);
 /* Training targets from CLOUDSC's outputs, divided by scale[ch]: f32
  * [ncol*lp][16] (LOC_T, LOC_Q, LOC_A, LOC_CLD l,i,r,s, PFPLSL, PFPLSN at the
@@ -96,7 +99,7 @@ int cs_prep_targets(const cs_columns *c, const float *scale16, float *t, void *s
 
 /* Training batch from stored features: for j < nb, batch column j is data
  * column cols[j] (device int32): x0 (bf16 [nb*lp][128]) as cs_prep_inputs
- * builds it from feat (f32 [*][CS_NIN], cs_raw_features layout), and tb (f32
+ * builds it from feat (f32 [*][CS_FSTRIDE], cs_raw_features layout), and tb (f32
  * [nb*lp][16]) copied from tgt (cs_prep_targets layout). */
 int cs_prep_batch(const float *feat, const float *tgt, const int32_t *cols, int32_t nb, int32_t lp,
                   int32_t klev, const cs_norm *nrm, void *x0, float *tb, void *stream);

@@ -48,9 +48,12 @@ struct Cols {
 // convective mass flux PMFU + PMFD and the forcing tendencies of T, q, a and
 // l + i; then the other fields CLOUDSC reads: PMFU and PMFD apart, the
 // updraught condensate PLU, the detrained liquid + ice PLUDELI and rain +
-// snow PSNDE, the layer thickness dp, LDCUM, PLSM, and the condensate and
-// precipitation mass above the level (cs_column_sums).  PVFL and PVFI are
-// left out: in CLOUDSC they enter only the DDH flux diagnostics.
+// snow PSNDE, the layer thickness dp, the first-guess relative humidity over
+// the mixed phase and over ice (the scheme's own saturation formulas,
+// fcttre.func.h FOEEWM / FOEEICE, at T + dt CML_T and q + dt CML_Q), PLSM, and
+// the condensate and precipitation mass above the level (cs_column_sums).
+// PVFL and PVFI are left out: in CLOUDSC they enter only the DDH flux
+// diagnostics; LDCUM is implied by PLUDE and the mass fluxes.
 __device__ __forceinline__ void raw_features(const Cols &C, int col, int k, float f[CS_NIN]) {
   const cs_columns &c = C.c;
   const size_t o = C.o2(col, k);
@@ -72,7 +75,18 @@ __device__ __forceinline__ void raw_features(const Cols &C, int col, int k, floa
   f[17] = (float)(c.pludeli[C.o3(col, 0, 4, k)] + c.pludeli[C.o3(col, 1, 4, k)]);
   f[18] = (float)(c.psnde[C.o3(col, 0, 2, k)] + c.psnde[C.o3(col, 1, 2, k)]);
   f[19] = (float)(c.paph[C.oh(col, k + 1)] - c.paph[C.oh(col, k)]);
-  f[20] = c.ldcum[C.o1(col)] ? 1.0f : 0.0f;
+  {
+    const double t = c.pt[o] + c.ptsphy * c.cml_t[o], q = c.pq[o] + c.ptsphy * c.cml_q[o], p = c.pap[o];
+    const double x = (fmax(c.rtice, fmin(c.rtwat, t)) - c.rtice) / (c.rtwat - c.rtice);
+    const double alfa = fmin(1.0, x * x);
+    const double el = exp(c.r3les * (t - c.rtt) / (t - c.r4les));
+    const double ei = exp(c.r3ies * (t - c.rtt) / (t - c.r4ies));
+    const double emix = fmin(c.r2es * (alfa * el + (1.0 - alfa) * ei) / p, 0.5);
+    const double eice = fmin(c.r2es * ei / p, 0.5);
+    const double qsmix = emix / (1.0 - c.retv * emix), qsice = eice / (1.0 - c.retv * eice);
+    f[20] = (float)(q / qsmix);
+    f[24] = (float)(q / qsice);
+  }
   f[21] = (float)c.plsm[C.o1(col)];
   const float *cs = c.colsum + ((size_t)col * c.klev + k) * 2;
   f[22] = cs[0];
@@ -96,16 +110,13 @@ __global__ void raw_features_kernel(Cols C, float *feat) {
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
     const int k = r - 2;
-    __align__(16) float f[CS_NIN];
-    if (k >= 0 && k < C.c.klev) {
-      raw_features(C, col, k, f);
-    } else {
+    __align__(16) float f[CS_FSTRIDE];
 #pragma unroll
-      for (int i = 0; i < CS_NIN; ++i) f[i] = 0.0f;
-    }
-    float4 *d = (float4 *)(feat + ((size_t)col * lp + r) * CS_NIN);
+    for (int i = 0; i < CS_FSTRIDE; ++i) f[i] = 0.0f;
+    if (k >= 0 && k < C.c.klev) raw_features(C, col, k, f);
+    float4 *d = (float4 *)(feat + ((size_t)col * lp + r) * CS_FSTRIDE);
 #pragma unroll
-    for (int i = 0; i < CS_NIN / 4; ++i) d[i] = ((float4 *)f)[i];
+    for (int i = 0; i < CS_FSTRIDE / 4; ++i) d[i] = ((float4 *)f)[i];
   }
 }
 
@@ -197,10 +208,10 @@ __global__ void prep_batch_kernel(const float *__restrict__ feat, const float *_
       for (int tap = 0; tap < 5; ++tap) {
         const int ks = k + tap - 2;
         if (ks < 0 || ks >= klev) continue;
-        const float4 *f4 = (const float4 *)(feat + (src + 2 + ks) * CS_NIN);
-        __align__(16) float f[CS_NIN];
+        const float4 *f4 = (const float4 *)(feat + (src + 2 + ks) * CS_FSTRIDE);
+        __align__(16) float f[CS_FSTRIDE];
 #pragma unroll
-        for (int q = 0; q < CS_NIN / 4; ++q) ((float4 *)f)[q] = f4[q];
+        for (int q = 0; q < CS_FSTRIDE / 4; ++q) ((float4 *)f)[q] = f4[q];
         norm_features(nrm, f, row + tap * CS_NIN);
       }
     }

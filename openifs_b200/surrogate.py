@@ -38,7 +38,8 @@ from . import cloudsc, fields, tcgemm
 
 LP = 144
 KLEV = 137
-NIN, NOUT = 24, 9
+NIN, NOUT = 25, 9
+FSTRIDE = 28  # floats per row of the raw-feature buffer
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "data", "surrogate_w128.npz")
 
@@ -49,7 +50,8 @@ IN_CHANNELS = [("t", None), ("q", 1e-8), ("p", 1.0), ("ql", 1e-9), ("qi", 1e-9),
                ("qs", 1e-9), ("plude", 1e-10), ("a", None), ("mflux", None), ("cml_t", None),
                ("cml_q", None), ("cml_a", None), ("cml_li", None),
                ("pmfu", None), ("pmfd", None), ("plu", 1e-7), ("pludeli", 1e-10), ("psnde", 1e-10),
-               ("dp", None), ("ldcum", None), ("plsm", None), ("cond_above", 1e-4), ("prec_above", 1e-4)]
+               ("dp", None), ("rh_mix", None), ("plsm", None), ("cond_above", 1e-4), ("prec_above", 1e-4),
+               ("rh_ice", None)]
 OUT_CHANNELS = ["loc_t", "loc_q", "loc_a", "loc_l", "loc_i", "loc_r", "loc_s", "pfplsl", "pfplsn"]
 
 
@@ -59,6 +61,8 @@ class Columns(ctypes.Structure):
                 ["pt", "pq", "pap", "paph", "pclv", "pa", "pmfu", "pmfd", "cml_t", "cml_q", "cml_a",
                  "cml_cld", "plu", "pludeli", "psnde", "ldcum", "plude", "plude_in", "plsm", "colsum",
                  "loc_t", "loc_q", "loc_a", "loc_cld", "pfplsl", "pfplsn", "pfhpsl", "pfhpsn"]] + \
+               [(n, ctypes.c_double) for n in ["r2es", "r3les", "r3ies", "r4les", "r4ies", "rtt", "rtice",
+                                                "rtwat", "retv", "ptsphy"]] + \
                [("nproma", ctypes.c_int32), ("klev", ctypes.c_int32), ("ngpblks", ctypes.c_int32),
                 ("lp", ctypes.c_int32)]
 
@@ -124,13 +128,16 @@ def _stream():
     return torch.cuda.current_stream().cuda_stream
 
 
-def columns(dev, nproma, ngpblks, colsum, klev=KLEV, lp=LP, plude_in=None):
+def columns(dev, nproma, ngpblks, colsum, params, ptsphy=3600.0, klev=KLEV, lp=LP, plude_in=None):
     """Columns struct over CLOUDSC batched device tensors (fields.BATCHED_FIELDS
     names); colsum: f32 [ncol, klev, 2] work tensor for cs_column_sums;
     plude_in: a separate tensor holding the input PLUDE, or None."""
     c = Columns()
     c.plude_in = None if plude_in is None else plude_in.data_ptr()
     c.colsum = colsum.data_ptr()
+    for n in ["r2es", "r3les", "r3ies", "r4les", "r4ies", "rtt", "rtice", "rtwat", "retv"]:
+        setattr(c, n, getattr(params, n))
+    c.ptsphy = ptsphy
     m = {"pt": "pt", "pq": "pq", "pap": "pap", "paph": "paph", "pclv": "pclv", "pa": "pa", "pmfu": "pmfu",
          "pmfd": "pmfd", "cml_t": "tendency_cml_t", "cml_q": "tendency_cml_q", "cml_a": "tendency_cml_a",
          "cml_cld": "tendency_cml_cld", "plu": "plu", "pludeli": "pludeli", "psnde": "psnde",
@@ -289,7 +296,7 @@ class Dataset:
         from . import inputs
         ncol_chunk = nblk * nproma
         self.ncol = ncol_chunk * nchunks
-        self.feat = torch.empty(self.ncol * LP, NIN, device="cuda")
+        self.feat = torch.empty(self.ncol * LP, FSTRIDE, device="cuda")
         self.tgt = torch.empty(self.ncol * LP, 16, device="cuda")
         L, ones = _lib(), np.ones(16, np.float32)
         cloudsc.setup(params)
@@ -298,7 +305,7 @@ class Dataset:
             dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
             del host
             colsum = torch.empty(ncol_chunk, KLEV, 2, device="cuda")
-            c = columns(dev, nproma, nblk, colsum)
+            c = columns(dev, nproma, nblk, colsum, params, ptsphy)
             sl = slice(ch * ncol_chunk * LP, (ch + 1) * ncol_chunk * LP)
             _ok(L.cs_column_sums(ctypes.byref(c), _p(colsum), _stream()), "cs_column_sums")
             _ok(L.cs_raw_features(ctypes.byref(c), _p(self.feat[sl]), _stream()), "cs_raw_features")
@@ -382,7 +389,8 @@ class Batch:
         self.dev = dev
         self.plude_in = dev["plude"].clone()
         self.colsum = torch.empty(runner.ncol, KLEV, 2, device="cuda")
-        self.cols = columns(dev, runner.nproma, runner.ngpblks, self.colsum, plude_in=self.plude_in)
+        self.cols = columns(dev, runner.nproma, runner.ngpblks, self.colsum, runner.params, runner.ptsphy,
+                            plude_in=self.plude_in)
         self.gather = runner._colarrays(dev, self.plude_in, 0)
         self.scatter = runner._colarrays(dev, self.plude_in, 1)
         self.nflag = torch.zeros(1, dtype=torch.int32, device="cuda")

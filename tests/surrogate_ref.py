@@ -131,6 +131,6 @@ def random_batch(ncol, rng):
     rows = ncol * LP
     v = valid_rows(rows)
     x0 = rng.standard_normal((rows, 128)) * v
-    x0[:, 120:] = 0.0
+    x0[:, 125:] = 0.0
     tgt = rng.standard_normal((rows, 16)) * v
     return x0, tgt
