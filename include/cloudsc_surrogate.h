@@ -50,6 +50,12 @@ typedef struct cs_gemm_desc {
  * (tcgen05, one persistent CTA per SM). */
 int cs_conv_gemm(const cs_gemm_desc *g, void *stream);
 
+/* Which kernel cs_conv_gemm runs: 0 (default) the warp-specialised one
+ * (weights resident in shared memory, one halo tile per K block for the 5
+ * taps, double-buffered TMEM accumulator), 1 the simple single-thread
+ * pipeline (kept as a cross-check). */
+int cs_set_gemm_impl(int32_t impl);
+
 /* ------------------------------------------------------------------------
  * Column data in CLOUDSC's batched storage (NPROMA, dims, NGPBLKS), device
  * pointers, double precision (LDCUM int32).  Column c = ib * NPROMA + jl.
@@ -88,8 +94,9 @@ typedef struct cs_norm {
 int cs_column_sums(const cs_columns *c, float *colsum, void *stream);
 
 /* Network input: x0[c*lp + 2 + l][tap*CS_NIN + ch] = feature ch of level
- * l+tap-2 (zero outside the column); bf16 [ncol*lp][128]. */
-int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream);
+ * l+tap-2 (zero outside the column); bf16 [ncol*lp][128].  fbuf: work
+ * buffer, bf16 [ncol*lp][32] (the normalised features of every level). */
+int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *fbuf, void *x0, void *stream);
 /* Raw (untransformed) input features, f32 [ncol*lp][CS_FSTRIDE]. */
 int cs_raw_features(const cs_columns *c, float *feat, void *stream);
 /* Training targets from CLOUDSC's outputs, divided by scale[ch]: f32

@@ -47,9 +47,9 @@ struct Args {
   unsigned *err;              // or null
 };
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float silu(float z) { return __fdividef(z, 1.0f + __expf(-z)); }
 __device__ __forceinline__ float dsilu(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = __fdividef(1.0f, 1.0f + __expf(-z));
   return s * (1.0f + z * (1.0f - s));
 }
 __device__ __forceinline__ void flag(unsigned *err, unsigned bit) {
@@ -229,6 +229,260 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) tcg::tmem_dealloc(tmem, TMEM_COLS);
 }
 
+// ------------------------------------------------------------------ epilogue
+// 32 accumulator columns c0..c0+31 of output row `row` (fused epilogue).
+// 32 bf16 of row-major storage as 4 x 16-byte loads.
+__device__ __forceinline__ void load_bf16x32(const __nv_bfloat16 *p, float (&f)[32]) {
+  __align__(16) __nv_bfloat16 t[32];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) ((uint4 *)t)[q] = __ldg((const uint4 *)p + q);
+#pragma unroll
+  for (int i = 0; i < 32; ++i) f[i] = __bfloat162float(t[i]);
+}
+
+template <int BN, int EPI>
+__device__ __forceinline__ void epilogue32(const Args &a, const float (&v)[32], int row, bool valid, int c0,
+                                           const float *bias) {
+  const size_t o = (size_t)row * BN + c0;
+  if (EPI == CS_EPI_SILU) {
+    float r[32];
+    if (a.resid) load_bf16x32(a.resid + o, r);
+    __align__(16) __nv_bfloat16 h[32], z[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      float zz = v[i] + bias[c0 + i];
+      float hh = silu(zz);
+      if (a.resid) hh += r[i];
+      if (!valid) {
+        zz = 0.0f;
+        hh = 0.0f;
+      }
+      z[i] = __float2bfloat16(zz);
+      h[i] = __float2bfloat16(hh);
+    }
+    uint4 *dh = (uint4 *)(a.out + o);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dh[i] = ((uint4 *)h)[i];
+    if (a.out_pre) {
+      uint4 *dz = (uint4 *)(a.out_pre + o);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dz[i] = ((uint4 *)z)[i];
+    }
+  } else if (EPI == CS_EPI_LINEAR_F32) {
+    float4 *d = (float4 *)(a.outf + o);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float4 w;
+      w.x = valid ? v[4 * i + 0] + bias[c0 + 4 * i + 0] : 0.0f;
+      w.y = valid ? v[4 * i + 1] + bias[c0 + 4 * i + 1] : 0.0f;
+      w.z = valid ? v[4 * i + 2] + bias[c0 + 4 * i + 2] : 0.0f;
+      w.w = valid ? v[4 * i + 3] + bias[c0 + 4 * i + 3] : 0.0f;
+      d[i] = w;
+    }
+  } else {  // CS_EPI_BWD
+    float r[32], zp[32];
+    if (a.resid) load_bf16x32(a.resid + o, r);
+    load_bf16x32(a.zprev + o, zp);
+    __align__(16) __nv_bfloat16 g[32], dz[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      float gg = v[i];
+      if (a.resid) gg += r[i];
+      float d = gg * dsilu(zp[i]);
+      if (!valid) {
+        gg = 0.0f;
+        d = 0.0f;
+      }
+      g[i] = __float2bfloat16(gg);
+      dz[i] = __float2bfloat16(d);
+    }
+    uint4 *dd = (uint4 *)(a.out + o);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) dd[i] = ((uint4 *)dz)[i];
+    if (a.gout) {
+      uint4 *dg = (uint4 *)(a.gout + o);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) dg[i] = ((uint4 *)g)[i];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ warp-specialised kernel
+// 576 threads: warp 0 loads (TMA), warp 1 issues the MMAs, warps 2-17 drain
+// TMEM: warp w reads TMEM lanes 32*(w%4).. (its 32 rows) and one 32-column
+// slice, so four warps per scheduler share the epilogue's latency.  The weights of all taps stay in
+// shared memory for the whole launch.  For a 5-tap convolution each 64-wide
+// K block of A is one TMA box of BM+4 rows (the tile plus a 2-row halo on each
+// side); tap t reads rows t..t+BM-1 of it through a descriptor whose base
+// address is moved by t rows.  The accumulator is double-buffered in
+// TMEM (2 x BN columns) so the epilogue of one tile overlaps the MMAs of the
+// next.
+constexpr int EPI_WARPS = 16;
+constexpr int WS_THREADS = 64 + 32 * EPI_WARPS;
+constexpr int WS_SMEM = 227 * 1024;
+
+template <int BN, int EPI, int TAPS>
+__global__ void __launch_bounds__(WS_THREADS, 1)
+    conv_gemm_ws_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Args a,
+                        int nst) {
+  constexpr int HALO = TAPS == 5 ? 2 : 0;
+  constexpr int BOXR = BM + 2 * HALO;                    // rows per A box
+  constexpr int A_TILE = ((BOXR + 7) / 8) * 8 * 128;     // bytes, multiple of 1024
+  constexpr int W_TILE = BN * 128;                        // one (tap, kb) tile of W
+  constexpr uint32_t IDESC = tcg::idesc_bf16_f32(BM, BN);
+  constexpr int TMEM_COLS = 2 * BN;                       // two accumulators
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int kb_n = a.kb_per_tap;
+  uint8_t *wbase = smem;
+  uint8_t *abase = smem + TAPS * kb_n * W_TILE;
+  float *sbias = (float *)(abase + nst * A_TILE);  // BN floats
+  uint64_t *bars = (uint64_t *)(abase + nst * A_TILE + 512);
+  uint64_t *wfull = bars, *full = bars + 1, *empty = full + nst, *tfull = empty + nst, *tempty = tfull + 2;
+  uint64_t *drain = tempty + 2;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+  volatile uint32_t *issued = (volatile uint32_t *)(tmem_slot + 2);   // A stages issued (producer)
+  volatile uint32_t *consumed = (volatile uint32_t *)(tmem_slot + 3); // A stages consumed (MMA)
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = (a.rows + BM - 1) / BM;
+  if (tid == 0) {
+    tcg::mbar_init(wfull, 1);
+    for (int s = 0; s < nst; ++s) {
+      tcg::mbar_init(&full[s], 1);
+      tcg::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tcg::mbar_init(&tfull[b], 1);
+      tcg::mbar_init(&tempty[b], EPI_WARPS);  // one arrival per epilogue warp
+    }
+    tcg::mbar_init(drain, 1);
+    *abort_flag = 0;
+    *issued = 0;
+    *consumed = 0;
+    tcg::mbar_fence_init();
+    tcg::tma_prefetch_desc(&tmA);
+    tcg::tma_prefetch_desc(&tmB);
+  }
+  if (warp == 1) {
+    tcg::tmem_alloc(tmem_slot, TMEM_COLS);
+    tcg::tmem_relinquish();
+  }
+  for (int c = tid; c < BN; c += blockDim.x) sbias[c] = a.bias ? a.bias[c] : 0.0f;
+  tcg::tc_fence_before();
+  __syncthreads();
+  tcg::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- producer
+    tcg::mbar_arrive_expect_tx(wfull, (uint32_t)(TAPS * kb_n * W_TILE));
+    for (int t = 0; t < TAPS; ++t)
+      for (int kb = 0; kb < kb_n; ++kb)
+        tcg::tma_load_2d(wbase + (t * kb_n + kb) * W_TILE, &tmB, wfull, kb * BK, t * BN);
+    uint32_t it = 0;
+    for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x) {
+      for (int kb = 0; kb < kb_n; ++kb) {
+        const int s = it % nst;
+        if (it >= (uint32_t)nst && !tcg::mbar_wait(&empty[s], ((it / nst) - 1) & 1)) {
+          flag(a.err, 1u);
+          *abort_flag = 1;
+          break;
+        }
+        tcg::mbar_arrive_expect_tx(&full[s], BOXR * 128);
+        tcg::tma_load_2d(abase + s * A_TILE, &tmA, &full[s], kb * BK, tile * BM - HALO);
+        ++it;
+        *issued = it;
+      }
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    bool ok = tcg::mbar_wait(wfull, 0);
+    uint32_t it = 0, i = 0;
+    for (int tile = blockIdx.x; ok && tile < ntiles && !*abort_flag; tile += gridDim.x, ++i) {
+      const int buf = i & 1;
+      if (i >= 2) ok = tcg::mbar_wait(&tempty[buf], ((i >> 1) - 1) & 1);
+      if (!ok) break;
+      tcg::tc_fence_after();
+      const uint32_t acc = tmem + (uint32_t)(buf * BN);
+      for (int kb = 0; kb < kb_n && ok; ++kb) {
+        const int s = it % nst;
+        ok = tcg::mbar_wait(&full[s], (it / nst) & 1);
+        if (!ok) break;
+        tcg::tc_fence_after();
+        const uint32_t sa = tcg::smem_u32(abase + s * A_TILE);
+#pragma unroll
+        for (int t = 0; t < TAPS; ++t) {
+          const uint64_t db = tcg::sdesc_k_sw128(tcg::smem_u32(wbase + (t * kb_n + kb) * W_TILE));
+          const uint64_t da = tcg::sdesc_k_sw128_rows(sa, (uint32_t)t);
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk)
+            tcg::mma_bf16(acc, da + 2 * kk, db + 2 * kk, IDESC, (kb > 0 || t > 0 || kk > 0) ? 1u : 0u);
+        }
+        tcg::mma_commit(&empty[s]);
+        ++it;
+        *consumed = it;
+      }
+      if (ok) tcg::mma_commit(&tfull[buf]);
+    }
+    if (!ok) {
+      flag(a.err, 1u);
+      *abort_flag = 1;
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue
+    const int quarter = warp & 3;
+    const int slice = (warp - 2) >> 2;   // 32-column slice of this warp
+    const bool has_cols = slice * 32 < BN;
+    uint32_t i = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+      const int buf = i & 1;
+      // one lane waits; the whole warp follows its verdict (tcgen05.ld is
+      // warp-collective)
+      int ok = 1;
+      if (lane == 0) ok = tcg::mbar_wait(&tfull[buf], (i >> 1) & 1) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        if (lane == 0) {
+          flag(a.err, 2u);
+          *abort_flag = 1;
+        }
+        break;
+      }
+      __syncwarp();
+      tcg::tc_fence_after();
+      if (has_cols) {
+        const int c0 = slice * 32;
+        const int row = tile * BM + quarter * 32 + lane;
+        const int pos = a.lp > 0 ? row % a.lp : 2;
+        const bool in_range = row < a.rows;
+        const bool valid = in_range && (a.lp <= 0 || (pos >= 2 && pos < 2 + a.klev));
+        float v[32];
+        tcg::tmem_ld32(tmem + (uint32_t)(buf * BN) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0, v);
+        if (in_range) epilogue32<BN, EPI>(a, v, row, valid, c0, sbias);
+      }
+      tcg::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tcg::mbar_arrive(&tempty[buf]);
+      if (__shfl_sync(0xffffffffu, lane == 0 ? *abort_flag : 0, 0)) break;
+    }
+  }
+  __syncthreads();
+  // On an abort, let every copy and MMA this CTA issued land before shared
+  // memory and TMEM are released (bounded waits).
+  if (tid == 0 && *abort_flag) {
+    for (uint32_t q = *consumed; q < *issued; ++q) (void)tcg::mbar_wait(&full[q % nst], (q / nst) & 1);
+  }
+  if (tid == 32 && *abort_flag) {
+    tcg::mma_commit(drain);
+    (void)tcg::mbar_wait(drain, 0);
+  }
+  tcg::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tcg::tmem_dealloc(tmem, TMEM_COLS);
+}
+
 // ------------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -272,7 +526,42 @@ cudaError_t launch_t(const CUtensorMap &ma, const CUtensorMap &mb, const Args &a
   return cudaGetLastError();
 }
 
+template <int BN, int EPI, int TAPS>
+cudaError_t launch_ws_t(const CUtensorMap &ma, const CUtensorMap &mb, const Args &a, int grid, int nst,
+                        cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(conv_gemm_ws_kernel<BN, EPI, TAPS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  conv_gemm_ws_kernel<BN, EPI, TAPS><<<grid, WS_THREADS, WS_SMEM, st>>>(ma, mb, a, nst);
+  return cudaGetLastError();
+}
+
+template <int BN>
+cudaError_t launch_ws_n(const CUtensorMap &ma, const CUtensorMap &mb, const Args &a, int grid, int nst,
+                        cudaStream_t st) {
+  if (a.taps == 5) {
+    if (a.epi == CS_EPI_SILU) return launch_ws_t<BN, CS_EPI_SILU, 5>(ma, mb, a, grid, nst, st);
+    if (a.epi == CS_EPI_BWD) return launch_ws_t<BN, CS_EPI_BWD, 5>(ma, mb, a, grid, nst, st);
+    return launch_ws_t<BN, CS_EPI_LINEAR_F32, 5>(ma, mb, a, grid, nst, st);
+  }
+  if (a.epi == CS_EPI_SILU) return launch_ws_t<BN, CS_EPI_SILU, 1>(ma, mb, a, grid, nst, st);
+  if (a.epi == CS_EPI_BWD) return launch_ws_t<BN, CS_EPI_BWD, 1>(ma, mb, a, grid, nst, st);
+  return launch_ws_t<BN, CS_EPI_LINEAR_F32, 1>(ma, mb, a, grid, nst, st);
+}
+
+int g_impl = 0;  // 0: warp-specialised kernel, 1: the single-thread pipeline
+
 }  // namespace sg
+
+extern "C" int cs_set_gemm_impl(int32_t impl) {
+  if (impl != 0 && impl != 1) return CS_E_ARG;
+  sg::g_impl = impl;
+  return CS_OK;
+}
 
 extern "C" int cs_conv_gemm(const cs_gemm_desc *g, void *stream) {
   using namespace sg;
@@ -287,8 +576,17 @@ extern "C" int cs_conv_gemm(const cs_gemm_desc *g, void *stream) {
        (uintptr_t)g->outf) &
       15)
     return CS_E_ARG;
+  // warp-specialised kernel: all weights resident in shared memory plus at
+  // least two A stages of BM + halo rows
+  const int halo = g->taps == 5 ? 2 : 0;
+  const int a_tile = ((BM + 2 * halo + 7) / 8) * 8 * 128;
+  const int w_bytes = g->taps * (g->k / 64) * g->n * 128;
+  int nst = (WS_SMEM - 1024 - 1024 - w_bytes) / a_tile;
+  if (nst > 8) nst = 8;
+  const bool ws = g_impl == 0 && nst >= 2;
   CUtensorMap ma, mb;
-  if (!make_map(&ma, g->a, (uint64_t)g->rows, (uint64_t)g->k, BM)) return CS_E_CUDA;
+  if (!make_map(&ma, g->a, (uint64_t)g->rows, (uint64_t)g->k, ws ? (uint32_t)(BM + 2 * halo) : (uint32_t)BM))
+    return CS_E_CUDA;
   if (!make_map(&mb, g->w, (uint64_t)g->taps * g->n, (uint64_t)g->k, (uint32_t)g->n)) return CS_E_CUDA;
   Args a;
   memset(&a, 0, sizeof(a));
@@ -314,6 +612,10 @@ extern "C" int cs_conv_gemm(const cs_gemm_desc *g, void *stream) {
   const int grid = ntiles < sms ? ntiles : sms;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e;
+  if (ws) {
+    e = g->n == 128 ? launch_ws_n<128>(ma, mb, a, grid, nst, st) : launch_ws_n<64>(ma, mb, a, grid, nst, st);
+    return e == cudaSuccess ? CS_OK : CS_E_CUDA;
+  }
   if (g->n == 128) {
     if (g->epi == CS_EPI_SILU) e = launch_t<128, CS_EPI_SILU>(ma, mb, a, grid, st);
     else if (g->epi == CS_EPI_BWD) e = launch_t<128, CS_EPI_BWD>(ma, mb, a, grid, st);

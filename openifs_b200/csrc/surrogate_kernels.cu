@@ -120,12 +120,34 @@ __global__ void raw_features_kernel(Cols C, float *feat) {
   }
 }
 
-__global__ void prep_inputs_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *x0) {
+// Input preparation in two passes: (1) the normalised features of every
+// (column, level) once, bf16 [ncol*lp][32] (threads level-major: a warp reads
+// one level of 32 neighbouring columns); (2) the 5-level im2col window of every
+// row (threads row-major: a warp writes 32 consecutive 256-byte rows).
+__global__ void features_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *fb) {
   const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
   const long long n = (long long)ncol * lp;
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
     const int k = r - 2;
+    __align__(16) __nv_bfloat16 row[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) row[i] = __float2bfloat16(0.0f);
+    if (k >= 0 && k < klev) {
+      float f[CS_NIN];
+      raw_features(C, col, k, f);
+      norm_features(nrm, f, row);
+    }
+    uint4 *d = (uint4 *)(fb + ((size_t)col * lp + r) * 32);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) d[i] = ((uint4 *)row)[i];
+  }
+}
+
+__global__ void im2col_kernel(const __nv_bfloat16 *__restrict__ fb, long long rows, int lp, int klev,
+                              __nv_bfloat16 *x0) {
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows; r += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(r % lp) - 2;
     __align__(16) __nv_bfloat16 row[128];
 #pragma unroll
     for (int i = 0; i < 128; ++i) row[i] = __float2bfloat16(0.0f);
@@ -134,12 +156,15 @@ __global__ void prep_inputs_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *x0) {
       for (int tap = 0; tap < 5; ++tap) {
         const int ks = k + tap - 2;
         if (ks < 0 || ks >= klev) continue;
-        float f[CS_NIN];
-        raw_features(C, col, ks, f);
-        norm_features(nrm, f, row + tap * CS_NIN);
+        __align__(16) __nv_bfloat16 f[32];
+        const uint4 *s4 = (const uint4 *)(fb + (r + tap - 2) * 32);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) ((uint4 *)f)[q] = __ldg(s4 + q);
+#pragma unroll
+        for (int ch = 0; ch < CS_NIN; ++ch) row[tap * CS_NIN + ch] = f[ch];
       }
     }
-    uint4 *d = (uint4 *)(x0 + ((size_t)col * lp + r) * 128);
+    uint4 *d = (uint4 *)(x0 + r * 128);
 #pragma unroll
     for (int i = 0; i < 16; ++i) d[i] = ((uint4 *)row)[i];
   }
@@ -529,12 +554,14 @@ int cs_column_sums(const cs_columns *c, float *colsum, void *stream) {
   return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
 }
 
-int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *x0, void *stream) {
+int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *fbuf, void *x0, void *stream) {
   using namespace sk;
-  if (!cols_ok(c) || !nrm || !x0 || !c->colsum) return CS_E_ARG;
+  if (!cols_ok(c) || !nrm || !x0 || !fbuf || !c->colsum) return CS_E_ARG;
   Cols C{*c};
   const long long n = (long long)c->nproma * c->ngpblks * c->lp;
-  prep_inputs_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)x0);
+  features_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)fbuf);
+  im2col_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)fbuf, n, c->lp, c->klev,
+                                                                    (__nv_bfloat16 *)x0);
   return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
 }
 

@@ -106,6 +106,19 @@ __device__ __forceinline__ uint64_t sdesc_k_sw128(uint32_t saddr) {
          | ((uint64_t)1 << 46)               // descriptor version
          | ((uint64_t)2 << 61);              // swizzle: 128 B
 }
+// The same for the tile that starts `rows` 128-byte rows past a 1024-byte
+// aligned base: the tensor core applies the 128-byte swizzle to the absolute
+// shared-memory address bits (as TMA does when it writes the tile), so a
+// start address moved by whole rows reads the shifted rows correctly with a
+// base offset of 0 (measured on the B200; a base offset equal to the row
+// phase reads wrong data).  Used to read a 5-tap convolution's shifted
+// operands out of one halo tile.
+__device__ __forceinline__ uint64_t sdesc_k_sw128_rows(uint32_t base, uint32_t rows) {
+  return sdesc_k_sw128(base + rows * 128u);
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 // D[tmem] (+)= A[smem] * B[smem]^T, issued by one thread.
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                          uint32_t accumulate) {

@@ -99,7 +99,7 @@ def _lib():
         vp, i32 = ctypes.c_void_p, ctypes.c_int32
         L.cs_raw_features.argtypes = [ctypes.POINTER(Columns), vp, vp]
         L.cs_column_sums.argtypes = [ctypes.POINTER(Columns), vp, vp]
-        L.cs_prep_inputs.argtypes = [ctypes.POINTER(Columns), ctypes.POINTER(Norm), vp, vp]
+        L.cs_prep_inputs.argtypes = [ctypes.POINTER(Columns), ctypes.POINTER(Norm), vp, vp, vp]
         L.cs_prep_targets.argtypes = [ctypes.POINTER(Columns), vp, vp, vp]
         L.cs_prep_batch.argtypes = [vp, vp, vp, i32, i32, i32, ctypes.POINTER(Norm), vp, vp, vp]
         L.cs_loss.argtypes = [vp, vp, i32, i32, i32, vp, i32, vp, vp, vp]
@@ -410,6 +410,7 @@ class Runner:
         self.ncol = nproma * ngpblks
         self.rows = self.ncol * LP
         self.B = net.buffers(self.rows, train=False)
+        self.fbuf = torch.empty(self.rows, 32, device="cuda", dtype=torch.bfloat16)
         self.cap = int(math.ceil(capacity / nproma)) * nproma
         self.diag = torch.zeros(self.ncol, 4, device="cuda")
         tdt = lambda dt: torch.float64 if np.dtype(dt) == np.float64 else torch.int32
@@ -454,8 +455,8 @@ class Runner:
         """Input preparation and the network (no guard): for timing."""
         L, s = _lib(), _stream()
         _ok(L.cs_column_sums(ctypes.byref(b.cols), _p(b.colsum), s), "cs_column_sums")
-        _ok(L.cs_prep_inputs(ctypes.byref(b.cols), ctypes.byref(self.net.norm), _p(self.B["x0"]), s),
-            "cs_prep_inputs")
+        _ok(L.cs_prep_inputs(ctypes.byref(b.cols), ctypes.byref(self.net.norm), _p(self.fbuf), _p(self.B["x0"]),
+                             s), "cs_prep_inputs")
         self.net.forward(self.B, self.rows, train=False)
 
     def run(self, b):

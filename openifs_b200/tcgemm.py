@@ -30,6 +30,15 @@ def _lib_fn():
     return _fn
 
 
+def set_impl(impl):
+    """0: warp-specialised kernel (default); 1: the single-thread pipeline."""
+    L = cloudsc.lib()
+    L.cs_set_gemm_impl.argtypes = [ctypes.c_int32]
+    L.cs_set_gemm_impl.restype = ctypes.c_int
+    if L.cs_set_gemm_impl(int(impl)) != 0:
+        raise ValueError(impl)
+
+
 def _p(t):
     return None if t is None else t.data_ptr()
 

@@ -11,6 +11,13 @@ pytestmark = pytest.mark.gpu
 LP, KLEV = 144, 137
 
 
+@pytest.fixture(params=[0, 1], ids=["warp_specialised", "single_thread"], autouse=True)
+def impl(request, cuda):
+    tcgemm.set_impl(request.param)
+    yield request.param
+    tcgemm.set_impl(0)
+
+
 def _torch():
     import torch
     return torch
