@@ -189,73 +189,68 @@ def surrogate_form(a, p, d, plude0, ref, dev, world, rank, ms64):
     """Guarded surrogate (config: 1,048,576 columns as 4 batches of 262,144,
     one CUDA graph per pass): columns/s, speed-up over the FP64 kernel,
     flagged fraction, errors and budget closure of batch 0 against the FP64
-    kernel, tensor-core throughput of the network's GEMMs."""
+    kernel, tensor-core throughput of the network's GEMMs.  The width-128
+    network is the configured one; a width-64 network, if its weights exist,
+    is timed on the same batches as an ablation."""
     import torch
     from openifs_b200 import inputs, surrogate as S
     if not os.path.exists(S.WEIGHTS):
         return {"unavailable": "no trained weights (python -m openifs_b200.train_surrogate)"}
-    net = S.Net.load(S.WEIGHTS)
-    cap_frac = 0.0625
-    runner = S.Runner(net, p, NPROMA, NGPBLKS, capacity=int(cap_frac * NCOL))
     d["plude"].copy_(plude0)
     batches = [d]
     for i in range(1, SUR_BATCHES):
         host = inputs.generate(NGPBLKS, NPROMA, p, seed=SEED + 10 * i + 1000 * rank)
         batches.append({k: torch.from_numpy(v).to(dev) for k, v in host.items()})
         del host
+    pristine = [b["plude"].clone() for b in batches]  # PLUDE is INOUT
+    res = _surrogate_run(a, S.WEIGHTS, p, batches, d, ref, dev, world, ms64)
+    w64 = S.WEIGHTS.replace("w128", "w64")
+    if os.path.exists(w64):
+        for b, p0 in zip(batches, pristine):
+            b["plude"].copy_(p0)
+        res["ablation_width64"] = _surrogate_run(a, w64, p, batches, d, ref, dev, world, ms64)
+    return res
+
+
+def _surrogate_run(a, path, p, batches, d, ref, dev, world, ms64):
+    import torch
+    from openifs_b200 import surrogate as S
+    net = S.Net.load(path)
+    cap_frac = 0.0625
+    runner = S.Runner(net, p, NPROMA, NGPBLKS, capacity=int(cap_frac * NCOL))
     states = [runner.prepare(b) for b in batches]
     stream = torch.cuda.current_stream(dev)
     for st in states:  # eager warm-up: one-time attribute and parameter set-up
         runner.run(st)
     torch.cuda.synchronize(dev)
-    # the network alone (input preparation + 5 GEMMs), eager, batch 0
-    fw = []
-    for i in range(a.warmup + a.steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        runner.forward_only(states[0])
-        e1.record(stream)
-        if i >= a.warmup:
-            fw.append((e0, e1))
-    torch.cuda.synchronize(dev)
-    fw_ms = statistics.mean(x.elapsed_time(y) for x, y in fw)
-    gemm = []
-    B = runner.B
-    for i in range(a.warmup + a.steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        net.forward(B, runner.rows, train=False)
-        e1.record(stream)
-        if i >= a.warmup:
-            gemm.append((e0, e1))
-    torch.cuda.synchronize(dev)
-    gemm_ms = statistics.mean(x.elapsed_time(y) for x, y in gemm)
-    # the guarded pipeline over all batches, captured once, replayed
+
+    def timed(fn):
+        ev = []
+        for i in range(a.warmup + a.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            if i >= a.warmup:
+                ev.append((e0, e1))
+        torch.cuda.synchronize(dev)
+        return statistics.mean(x.elapsed_time(y) for x, y in ev)
+
+    fw_ms = timed(lambda: runner.forward_only(states[0]))           # input preparation + network
+    gemm_ms = timed(lambda: net.forward(runner.B, runner.rows, train=False))  # the five GEMMs
     graph = torch.cuda.CUDAGraph()
     with torch.cuda.graph(graph):
         for st in states:
             runner.run(st)
-    for _ in range(a.warmup):
-        graph.replay()
-    torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    ev = []
-    for _ in range(a.steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        graph.replay()
-        e1.record(stream)
-        ev.append((e0, e1))
-    torch.cuda.synchronize(dev)
-    ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    ms = timed(graph.replay)
     if world > 1:
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     ncols = SUR_BATCHES * NCOL
     flagged = [int(st.nflag.item()) for st in states]
-    # accuracy and closure of batch 0 against the FP64 kernel
     err = {}
     for n in ["tendency_loc_t", "tendency_loc_q", "tendency_loc_a", "tendency_loc_cld", "pfplsl", "pfplsn"]:
         r, g = ref[n], d[n]
@@ -269,7 +264,7 @@ def surrogate_form(a, p, d, plude0, ref, dev, world, rank, ms64):
     flops = runner.flops_per_batch()
     peaks = _peaks() or {}
     tpk = peaks.get("bf16_tflops", 1590.0)
-    return {
+    out = {
         "columns_per_s": world * ncols / (ms * 1e-3), "ms_per_pass": ms, "columns_per_pass": ncols,
         "batches": SUR_BATCHES, "cuda_graph": True,
         "ms_per_262144_columns": ms / SUR_BATCHES, "speedup_vs_fp64": ms64 / (ms / SUR_BATCHES),
@@ -283,7 +278,11 @@ def surrogate_form(a, p, d, plude0, ref, dev, world, rank, ms64):
                     "bf16_peak_tflops": tpk},
         "guard": {"neg_tol": runner.guard.neg_tol, "closure_tol": runner.guard.closure_tol,
                   "spread_tol": runner.guard.spread_tol},
+        "weights": os.path.relpath(path, ROOT),
     }
+    del states, runner, net
+    torch.cuda.empty_cache()
+    return out
 
 
 def _closure(p, d, plude_in):

@@ -112,8 +112,8 @@ int cs_prep_batch(const float *feat, const float *tgt, const int32_t *cols, int3
                   int32_t klev, const cs_norm *nrm, void *x0, float *tb, void *stream);
 
 /* MSE loss over valid rows and the first CS_NOUT channels of each of the
- * nheads (1 or 2) output heads; y f32 and dy bf16 are [rows][64 * nheads]
- * (head h in columns 64h..64h+CS_NOUT-1):
+ * nheads (1 or 2) output heads; y f32 and dy bf16 are [rows][64] (head h in
+ * columns 32h..32h+CS_NOUT-1):
  * dy = 2 w (y - t) / count, loss_sum += sum w (y - t)^2 / count. */
 int cs_loss(const float *y, const float *t, int32_t rows, int32_t lp, int32_t klev, const float *w16,
             int32_t nheads, void *dy, double *loss_sum, void *stream);
@@ -146,7 +146,7 @@ typedef struct cs_guard {
   int32_t capacity;      /* length of the flagged-column list                   */
 } cs_guard;
 
-/* Turn the network output y ([rows][64 * nheads] f32) into CLOUDSC
+/* Turn the network output y ([rows][64] f32, head h at column 32h) into CLOUDSC
  * outputs: mean of the heads, de-normalised; condensates that the step would
  * drive negative are refilled from vapour with their latent heat (as
  * CLOUDSC's own clean-up does, cloudsc.F90:3779-3809); LOC_Q is then shifted

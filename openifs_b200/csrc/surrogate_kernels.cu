@@ -253,27 +253,26 @@ __global__ void prep_batch_kernel(const float *__restrict__ feat, const float *_
 // ---------------------------------------------------------------- loss
 __global__ void loss_kernel(const float *__restrict__ y, const float *__restrict__ tg, int rows, int lp, int klev,
                             F16 w, int nheads, float inv_count, __nv_bfloat16 *dy, double *loss_sum) {
-  const int ys = 64 * nheads;
   double acc = 0.0;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
     const int pos = r % lp;
     const bool valid = pos >= 2 && pos < 2 + klev;
-    for (int h = 0; h < nheads; ++h) {
-      __align__(16) __nv_bfloat16 g[64];
+    __align__(16) __nv_bfloat16 g[64];
 #pragma unroll
-      for (int i = 0; i < 64; ++i) g[i] = __float2bfloat16(0.0f);
-      if (valid) {
+    for (int i = 0; i < 64; ++i) g[i] = __float2bfloat16(0.0f);
+    if (valid) {
+      for (int h = 0; h < nheads; ++h) {
 #pragma unroll
         for (int i = 0; i < CS_NOUT; ++i) {
-          const float d = y[(size_t)r * ys + 64 * h + i] - tg[(size_t)r * 16 + i];
+          const float d = y[(size_t)r * 64 + 32 * h + i] - tg[(size_t)r * 16 + i];
           acc += (double)(w.v[i] * d * d * inv_count);
-          g[i] = __float2bfloat16(2.0f * w.v[i] * d * inv_count);
+          g[32 * h + i] = __float2bfloat16(2.0f * w.v[i] * d * inv_count);
         }
       }
-      uint4 *dd = (uint4 *)(dy + (size_t)r * ys + 64 * h);
-#pragma unroll
-      for (int i = 0; i < 8; ++i) dd[i] = ((uint4 *)g)[i];
     }
+    uint4 *dd = (uint4 *)(dy + (size_t)r * 64);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dd[i] = ((uint4 *)g)[i];
   }
   // block reduction of the loss
   __shared__ double red[256];
@@ -375,7 +374,7 @@ __global__ void adamw_kernel(float *p, float *g, float *m, float *v, int taps, i
 // fluxes.
 __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_guard gd, int *nflagged,
                             int *flagged, float4 *diag) {
-  const int ys = 64 * nheads;
+  const int ys = 64;
   const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
   const int k0 = gd.ncldtop - 1;  // first level of CLOUDSC's level loop
   const double dt = gd.ptsphy, rg = gd.rg;
@@ -395,7 +394,7 @@ __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_
       for (int i = 0; i < CS_NOUT; ++i) {
         float a = y[r * ys + i];
         if (nheads == 2) {
-          const float b = y[r * ys + 64 + i];
+          const float b = y[r * ys + 32 + i];
           if (i < 7) {
             spread2 += (double)(a - b) * (double)(a - b);
             ++spread_n;

@@ -12,8 +12,8 @@ own CUDA kernels, include/cloudsc_surrogate.h):
     h2 = h1 + SiLU(conv5(h1; W2) + b2)            second convolution (k = 5)
     h3 = h2 + SiLU(conv5(h2; W3) + b3)            third convolution (k = 5)
     h4 = SiLU(h3 W4 + b4)                          MLP head, layer 1
-    y  = h4 W5 + b5   [rows,128]                   MLP head, layer 2: two
-                    output heads of 9 channels (columns 0..8 and 64..72)
+    y  = h4 W5 + b5   [rows,64]                    MLP head, layer 2: two
+                    output heads of 9 channels (columns 0..8 and 32..40)
 
 One row per (column, level): a column holds LP = 144 rows, level l at row
 2 + l, zero rows around it, so the 5-tap convolutions over levels never mix
@@ -160,7 +160,7 @@ class Net:
         assert width in (64, 128)
         self.width, self.dev = width, device
         W = width
-        self.shapes = {1: (1, W, 128), 2: (5, W, W), 3: (5, W, W), 4: (1, W, W), 5: (1, 128, W)}
+        self.shapes = {1: (1, W, 128), 2: (5, W, W), 3: (5, W, W), 4: (1, W, W), 5: (1, 64, W)}
         g = torch.Generator(device="cpu").manual_seed(seed)
         self.p, self.b = {}, {}
         for i, (t, n, k) in self.shapes.items():
@@ -194,11 +194,11 @@ class Net:
         import torch
         W, d = self.width, self.dev
         bf = lambda c: torch.empty(rows, c, device=d, dtype=torch.bfloat16)
-        B = {"x0": bf(128), "y": torch.empty(rows, 128, device=d)}
+        B = {"x0": bf(128), "y": torch.empty(rows, 64, device=d)}
         if train:
             for n in ["h1", "h2", "h3", "h4", "z1", "z2", "z3", "z4", "dz1", "dz2", "dz3", "dz4", "g2", "g3"]:
                 B[n] = bf(W)
-            B["dy"] = bf(128)
+            B["dy"] = bf(64)
             B["tb"] = torch.empty(rows, 16, device=d)
             B["loss"] = torch.zeros(1, device=d, dtype=torch.float64)
         else:
@@ -215,7 +215,7 @@ class Net:
             G(B["h2"][:rows], self.wbf[3], E.EPI_SILU, W, 5, LP, KLEV, self.b[3], B["h3"], B["z3"], B["h2"],
               stream=stream)
             G(B["h3"][:rows], self.wbf[4], E.EPI_SILU, W, 1, LP, KLEV, self.b[4], B["h4"], B["z4"], stream=stream)
-            G(B["h4"][:rows], self.wbf[5], E.EPI_LINEAR_F32, 128, 1, LP, KLEV, self.b[5], outf=B["y"],
+            G(B["h4"][:rows], self.wbf[5], E.EPI_LINEAR_F32, 64, 1, LP, KLEV, self.b[5], outf=B["y"],
               stream=stream)
         else:
             ha, hb = B["ha"], B["hb"]
@@ -223,7 +223,7 @@ class Net:
             G(ha[:rows], self.wbf[2], E.EPI_SILU, W, 5, LP, KLEV, self.b[2], hb, resid=ha, stream=stream)
             G(hb[:rows], self.wbf[3], E.EPI_SILU, W, 5, LP, KLEV, self.b[3], ha, resid=hb, stream=stream)
             G(ha[:rows], self.wbf[4], E.EPI_SILU, W, 1, LP, KLEV, self.b[4], hb, stream=stream)
-            G(hb[:rows], self.wbf[5], E.EPI_LINEAR_F32, 128, 1, LP, KLEV, self.b[5], outf=B["y"], stream=stream)
+            G(hb[:rows], self.wbf[5], E.EPI_LINEAR_F32, 64, 1, LP, KLEV, self.b[5], outf=B["y"], stream=stream)
         return B["y"]
 
     def backward(self, B, rows):
@@ -236,7 +236,7 @@ class Net:
         G(B["dz3"][:rows], self.wtbf[3], E.EPI_BWD, W, 5, LP, KLEV, out=B["dz2"], zprev=B["z2"], resid=B["g3"],
           gout=B["g2"])
         G(B["dz2"][:rows], self.wtbf[2], E.EPI_BWD, W, 5, LP, KLEV, out=B["dz1"], zprev=B["z1"], resid=B["g2"])
-        for i, dz, x, n, k, t in [(5, "dy", "h4", 128, W, 1), (4, "dz4", "h3", W, W, 1), (3, "dz3", "h2", W, W, 5),
+        for i, dz, x, n, k, t in [(5, "dy", "h4", 64, W, 1), (4, "dz4", "h3", W, W, 1), (3, "dz3", "h2", W, W, 5),
                                   (2, "dz2", "h1", W, W, 5), (1, "dz1", "x0", W, 128, 1)]:
             _ok(L.cs_wgrad(_p(B[dz]), _p(B[x]), rows, n, k, t, _p(self.g[i]), _p(self.gb[i]), s), "cs_wgrad")
 
@@ -478,5 +478,5 @@ class Runner:
     def flops_per_batch(self):
         """Multiply-add FLOPs of the network's GEMMs for one batch (padded rows included)."""
         W = self.net.width
-        per_row = 128 * W + 5 * W * W * 2 + W * W + W * 128
+        per_row = 128 * W + 5 * W * W * 2 + W * W + W * 64
         return 2.0 * self.rows * per_row

@@ -1,8 +1,7 @@
 """Train the CLOUDSC surrogate on columns computed by the FP64 GPU kernel and
 calibrate its guard.
 
-    python -m openifs_b200.train_surrogate --chunks 8 --steps 20000 \
-        --out openifs_b200/data/surrogate_w128.npz
+    python -m openifs_b200.train_surrogate --chunks 8 --steps 40000 --widths 128,64
 
 Each chunk is 262,144 seeded synthetic columns (2,048 NPROMA blocks of 128,
 openifs_b200/inputs.py) that cloudsc_b200_batched (FP64) turns into targets.
@@ -83,13 +82,13 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--chunks", type=int, default=8)
     ap.add_argument("--nblk", type=int, default=2048)
-    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--steps", type=int, default=40000)
     ap.add_argument("--nb", type=int, default=512)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--width", type=int, default=128)
+    ap.add_argument("--widths", default="128", help="comma-separated, each 64 or 128")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--flag-quantile", type=float, default=0.99)
-    ap.add_argument("--out", default=None)
+    ap.add_argument("--outdir", default=None)
     a = ap.parse_args(argv)
     import torch
     from . import cloudsc, surrogate as S
@@ -101,27 +100,33 @@ def main(argv=None):
     norm, scale = data.normalisation()
     data.apply_scale(scale)
     _log(f"dataset: {data.ncol} columns in {time.time() - t0:.1f} s")
-    net = S.Net(a.width, seed=a.seed)
-    net.norm, net.out_scale = norm, scale
-    torch.cuda.synchronize()
-    t1 = time.time()
-    hist = S.train(net, data, a.steps, nb=a.nb, lr=a.lr, log=_log, log_every=1000)
-    torch.cuda.synchronize()
-    train_s = time.time() - t1
-    _log(f"training: {a.steps} steps of {a.nb} columns in {train_s:.1f} s")
+    nets = {}
+    for width in [int(w) for w in a.widths.split(",")]:
+        net = S.Net(width, seed=a.seed)
+        net.norm, net.out_scale = norm, scale
+        torch.cuda.synchronize()
+        t1 = time.time()
+        hist = S.train(net, data, a.steps, nb=a.nb, lr=a.lr, log=_log, log_every=1000)
+        torch.cuda.synchronize()
+        train_s = time.time() - t1
+        _log(f"width {width}: {a.steps} steps of {a.nb} columns in {train_s:.1f} s")
+        nets[width] = (net, hist, train_s)
     del data
     torch.cuda.empty_cache()
-    ev = evaluate(net, params, seed=5000, flag_quantile=a.flag_quantile)
-    ev.update({"train_columns": int(a.chunks * a.nblk * 128), "steps": a.steps, "batch_columns": a.nb,
-               "train_seconds": train_s, "loss_history": hist, "width": a.width})
-    _log(json.dumps(ev, indent=1))
-    out = a.out or os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", f"surrogate_w{a.width}.npz")
-    st = net.state()
-    st["guard"] = np.array([ev["neg_tol"], ev["closure_tol"], ev["spread_tol"]])
-    np.savez_compressed(out, **st)
-    with open(os.path.splitext(out)[0] + ".json", "w") as f:
-        json.dump(ev, f, indent=1)
-    _log(f"saved {out}")
+    outdir = a.outdir or os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+    for width, (net, hist, train_s) in nets.items():
+        ev = evaluate(net, params, seed=5000, flag_quantile=a.flag_quantile)
+        ev.update({"train_columns": int(a.chunks * a.nblk * 128), "steps": a.steps, "batch_columns": a.nb,
+                   "train_seconds": train_s, "loss_history": hist, "width": width})
+        _log(json.dumps({k: v for k, v in ev.items() if k != "loss_history"}, indent=1))
+        out = os.path.join(outdir, f"surrogate_w{width}.npz")
+        st = net.state()
+        st["guard"] = np.array([ev["neg_tol"], ev["closure_tol"], ev["spread_tol"]])
+        np.savez_compressed(out, **st)
+        with open(os.path.splitext(out)[0] + ".json", "w") as f:
+            json.dump(ev, f, indent=1)
+        _log(f"saved {out}")
+        torch.cuda.empty_cache()
 
 
 if __name__ == "__main__":

@@ -84,7 +84,7 @@ def forward(P, x0):
 
 def loss_and_grad(P, x0, tgt, nout=9):
     """MSE over valid rows and the first nout channels of both heads (columns
-    0.. and 64..), normalised by (columns * KLEV * nout) as cs_loss does."""
+    0.. and 32..), normalised by (columns * KLEV * nout) as cs_loss does."""
     rows = x0.shape[0]
     v = valid_rows(rows)
     c = forward(P, x0)
@@ -92,7 +92,7 @@ def loss_and_grad(P, x0, tgt, nout=9):
     count = (rows // LP) * KLEV * nout
     dy = np.zeros_like(y)
     loss = 0.0
-    for h in (0, 64):
+    for h in (0, 32):
         d = (y[:, h:h + nout] - tgt[:, :nout]) * v
         loss += (d * d).sum() / count
         dy[:, h:h + nout] = 2.0 * d / count
@@ -119,7 +119,7 @@ def loss_and_grad(P, x0, tgt, nout=9):
 
 def random_params(width, rng):
     W = width
-    shapes = {1: (1, W, 128), 2: (5, W, W), 3: (5, W, W), 4: (1, W, W), 5: (1, 128, W)}
+    shapes = {1: (1, W, 128), 2: (5, W, W), 3: (5, W, W), 4: (1, W, W), 5: (1, 64, W)}
     P = {}
     for i, s in shapes.items():
         P[f"w{i}"] = rng.standard_normal(s) * np.sqrt(2.0 / (s[0] * s[2])) * (0.5 if i in (2, 3) else 1.0)
