@@ -270,7 +270,7 @@ size_t cloudsc_b200_params_size(void);
 /*
  * Kernel launch shape used by cloudsc_b200_batched (the autotuner's knobs).
  * threads_per_cta: columns per CTA, a multiple of 32 up to the kernels'
- * compiled limit of 384 (default 384);
+ * compiled limit of 448 (default 448);
  * ctas_per_sm: persistent CTAs resident per SM (0 = one wave over all tiles).
  * Returns CLOUDSC_E_SHAPE for values outside the documented limits.
  */

@@ -38,7 +38,7 @@ bool g_have_params = false;
 unsigned long long g_gen = 0;
 constexpr int kMaxDev = 64;
 unsigned long long g_dev_gen[kMaxDev] = {0};
-int g_threads[2] = {384, 384};
+int g_threads[2] = {448, 448};
 int g_ctas_per_sm[2] = {0, 0};
 
 int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -326,7 +326,7 @@ int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t 
   if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
   if (threads_per_cta < 32 || threads_per_cta > max_threads(precision) || threads_per_cta % 32)
     return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32, at least 32 and at most "
-                                 "the kernel's compiled limit (384)");
+                                 "the kernel's compiled limit (448)");
   if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(CLOUDSC_E_SHAPE, "ctas_per_sm must be in [0,32]");
   std::lock_guard<std::mutex> lk(g_mu);
   g_threads[precision] = threads_per_cta;

@@ -95,18 +95,19 @@ cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
 }
 
 // Register budget and CTA size: __launch_bounds__(MAXT, MINB).  One CTA of
-// 384 threads per SM caps the kernels at 168 registers (some hundred bytes of
-// spills) and keeps 12 warps in per-level lock-step; measured at 262,144
-// columns, FP64: 19.6 ms, against 21.7 ms for three 128-thread CTAs per SM
-// with the same barrier and 23.9 ms without it.
+// 448 threads per SM: 14 warps in per-level lock-step at 128 registers (some
+// hundred bytes of spills), and 262,144 columns are 586 tiles = 3.96 waves
+// over 148 SMs.  Measured at 262,144 columns, FP64: 15.98 ms; 384 threads
+// (168 registers) 17.77 ms; 480 threads 16.17 ms; three 128-thread CTAs per
+// SM with the same barrier 21.7 ms; no barrier 23.9 ms.
 #ifndef CLOUDSC_MAXT
-#define CLOUDSC_MAXT 384
+#define CLOUDSC_MAXT 448
 #endif
 #ifndef CLOUDSC_MINB
 #define CLOUDSC_MINB 1
 #endif
 #ifndef CLOUDSC_MIX_MAXT
-#define CLOUDSC_MIX_MAXT 384
+#define CLOUDSC_MIX_MAXT 448
 #endif
 #ifndef CLOUDSC_MIX_MINB
 #define CLOUDSC_MIX_MINB 1

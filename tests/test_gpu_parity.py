@@ -78,7 +78,7 @@ def test_edge_columns(cuda, case):
     _check(p, po, arrs, 64, 4, 256)
 
 
-@pytest.mark.parametrize("threads", [32, 96, 128, 384])
+@pytest.mark.parametrize("threads", [32, 96, 128, 448])
 def test_launch_shapes(cuda, threads):
     """CTA shapes that split, match and span NPROMA blocks (tiles cross block
     boundaries), with a persistent grid, give identical results."""
@@ -88,7 +88,7 @@ def test_launch_shapes(cuda, threads):
         cloudsc.set_launch(cloudsc.FP64, threads, 1)
         _check(p, po, arrs, 128, 6, 6 * 128 - 3)
     finally:
-        cloudsc.set_launch(cloudsc.FP64, 384, 0)
+        cloudsc.set_launch(cloudsc.FP64, 448, 0)
 
 
 def test_config2_sampled_blocks(cuda):
