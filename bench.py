@@ -64,19 +64,28 @@ class ClockSampler:
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, interval_ms=20):
         self.index = index
+        self.interval_ms = interval_ms
         self.proc = None
         self.lines = []
+        self.start, self.end = 0, None
 
     def __enter__(self):
+        """Start sampling and return once the first sample has arrived (at
+        most 10 s), so that the samples kept, the ones after it, all fall in
+        the timed region that follows."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.005)
+            self.start = len(self.lines)
         except Exception:
             self.proc = None
         return self
@@ -86,6 +95,7 @@ class ClockSampler:
             self.lines.append(ln.strip())
 
     def __exit__(self, *a):
+        self.end = len(self.lines)
         if self.proc:
             self.proc.terminate()
             try:
@@ -96,7 +106,7 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.start:self.end]:
             parts = [x.strip() for x in ln.split(",")]
             if len(parts) < 7:
                 continue
@@ -352,6 +362,18 @@ def run_ours(a):
         ms = [a_.elapsed_time(b_) for a_, b_ in ev]
         return ms
 
+    # launch schedule per precision: the autotuner's recorded choice for this
+    # device and shape, or tuned now (untimed; rank 0 records it)
+    from openifs_b200 import autotune
+    schedule = {}
+    for prec, name in ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed")):
+        entry, src = autotune.apply_cached(prec, NPROMA, KLEV, NGPBLKS), "cache"
+        if entry is None:
+            entry = autotune.tune(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, prec, stream=stream,
+                                  cache=autotune.DEFAULT_CACHE if rank == 0 else None)["best"]
+            src = "tuned in this run"
+        schedule[name] = dict(entry, source=src)
+
     results = {}
     clocks = None
     for prec, name in ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed")):
@@ -401,8 +423,7 @@ def run_ours(a):
     if not a.no_e2e:
         pin = {k: torch.from_numpy(v).pin_memory() for k, v in host.items()}
         plude_h = pin["plude"].clone()
-        h2d = sum(pin[n].numel() * pin[n].element_size() for n in fields.INPUT_NAMES)
-        d2h = sum(pin[n].numel() * pin[n].element_size() for n in fields.OUTPUT_NAMES)
+        h2d, d2h = fields.host_copy_bytes(NPROMA, KLEV, NGPBLKS, NCOL)
         tt = []
         for i in range(max(1, a.warmup) + a.steps):
             pin["plude"].copy_(plude_h)
@@ -459,7 +480,8 @@ def run_ours(a):
         "config": {"workload": WORKLOAD, "columns_per_gpu": NCOL, "nproma": NPROMA,
                    "ngpblks": NGPBLKS, "klev": KLEV, "ptsphy": PTSPHY,
                    "l2": "inputs 15 GB resident in HBM, > 126 MB L2; no flush needed",
-                   "launch": "one persistent launch per step"},
+                   "launch": "one launch per step over all blocks",
+                   "schedule": schedule},
         "forms": {
             "fp64": {"columns_per_s": value, "ms": ms64, "min_ms": results["fp64"]["min_ms"]},
             "mixed": {"columns_per_s": world * NCOL / (results["mixed"]["ms"] * 1e-3),

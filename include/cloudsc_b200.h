@@ -268,12 +268,32 @@ size_t cloudsc_b200_block_noalloc_capacity(void);
 size_t cloudsc_b200_params_size(void);
 
 /*
- * Kernel launch shape used by cloudsc_b200_batched (the autotuner's knobs).
- * threads_per_cta: columns per CTA, a multiple of 32 up to the kernels'
- * compiled limit of 448 (default 448);
- * ctas_per_sm: persistent CTAs resident per SM (0 = one wave over all tiles).
- * Returns CLOUDSC_E_SHAPE for values outside the documented limits.
+ * Launch schedule of the kernels (the autotuner's knobs; no reference
+ * counterpart: the reference runs CLOUDSC on CPU threads, one NPROMA block
+ * per call, ec_phys_drv.F90:438).  Every entry point that launches a kernel
+ * uses the schedule set for its precision (0 FP64, 1 FP32-mixed).
+ *
+ * The kernels are compiled in several variants, each a
+ * __launch_bounds__(max_threads, min_ctas) pair that fixes the register
+ * budget per thread.  cloudsc_b200_num_variants() gives their number;
+ * cloudsc_b200_variant_info() the bounds of variant v and, when a device is
+ * present, its registers and local (spill) bytes per thread (-1 without one).
+ *
+ * cloudsc_b200_set_schedule(): variant, columns per CTA (a multiple of 32 up
+ * to the variant's max_threads) and ctas_per_sm, the persistent CTAs resident
+ * per SM (0 = one CTA per tile of columns, a grid over all tiles).  Default:
+ * the (512, 1) variant, 448 columns per CTA, ctas_per_sm 0.
+ * cloudsc_b200_set_launch(): the same with the variant chosen as the one-CTA-
+ * per-SM variant with the most registers that holds threads_per_cta.
+ * Return CLOUDSC_E_SHAPE for values outside these limits.
  */
+int cloudsc_b200_num_variants(void);
+int cloudsc_b200_variant_info(int32_t precision, int32_t variant, int32_t *max_threads,
+                              int32_t *min_ctas, int32_t *regs, int32_t *local_bytes);
+int cloudsc_b200_set_schedule(int32_t precision, int32_t variant, int32_t threads_per_cta,
+                              int32_t ctas_per_sm);
+int cloudsc_b200_get_schedule(int32_t precision, int32_t *variant, int32_t *threads_per_cta,
+                              int32_t *ctas_per_sm);
 int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm);
 
 /* Last CUDA error string recorded by this library on the calling thread. */

@@ -53,6 +53,14 @@ def lib():
         L.cloudsc_b200_setup.restype = ctypes.c_int
         L.cloudsc_b200_set_launch.argtypes = [i32, i32, i32]
         L.cloudsc_b200_set_launch.restype = ctypes.c_int
+        pi32 = ctypes.POINTER(i32)
+        L.cloudsc_b200_num_variants.restype = ctypes.c_int
+        L.cloudsc_b200_variant_info.argtypes = [i32, i32, pi32, pi32, pi32, pi32]
+        L.cloudsc_b200_variant_info.restype = ctypes.c_int
+        L.cloudsc_b200_set_schedule.argtypes = [i32, i32, i32, i32]
+        L.cloudsc_b200_set_schedule.restype = ctypes.c_int
+        L.cloudsc_b200_get_schedule.argtypes = [i32, pi32, pi32, pi32]
+        L.cloudsc_b200_get_schedule.restype = ctypes.c_int
         L.cloudsc_b200_last_error.restype = ctypes.c_char_p
         L.cloudsc_b200_version.restype = ctypes.c_char_p
         L.cloudsc_b200_params_size.restype = ctypes.c_size_t
@@ -92,6 +100,31 @@ def setup(params):
 
 def set_launch(precision, threads_per_cta, ctas_per_sm):
     return _check(lib().cloudsc_b200_set_launch(int(precision), int(threads_per_cta), int(ctas_per_sm)))
+
+
+def num_variants():
+    """Number of compiled (max threads, min CTAs per SM) kernel variants."""
+    return int(lib().cloudsc_b200_num_variants())
+
+
+def variant_info(precision, variant):
+    """{"max_threads", "min_ctas", "regs", "local_bytes"} of a compiled
+    variant (regs and local_bytes are -1 without a GPU)."""
+    v = [ctypes.c_int32() for _ in range(4)]
+    _check(lib().cloudsc_b200_variant_info(int(precision), int(variant), *[ctypes.byref(x) for x in v]))
+    return dict(zip(("max_threads", "min_ctas", "regs", "local_bytes"), (x.value for x in v)))
+
+
+def set_schedule(precision, variant, threads_per_cta, ctas_per_sm):
+    return _check(lib().cloudsc_b200_set_schedule(int(precision), int(variant), int(threads_per_cta),
+                                                  int(ctas_per_sm)))
+
+
+def get_schedule(precision):
+    """(variant, threads_per_cta, ctas_per_sm) used for `precision`."""
+    v = [ctypes.c_int32() for _ in range(3)]
+    _check(lib().cloudsc_b200_get_schedule(int(precision), *[ctypes.byref(x) for x in v]))
+    return tuple(x.value for x in v)
 
 
 def _ptr(x):

@@ -21,9 +21,12 @@
 
 namespace cloudsc {
 cudaError_t upload_params(const cloudsc_params &p, const Derived &d);
-cudaError_t launch(int precision, const Fields &f, const Shape &sh, int threads, int grid,
+int num_variants();
+int default_variant();
+void variant_bounds(int v, int *maxt, int *minb);
+cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes);
+cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream);
-int max_threads(int precision);
 }  // namespace cloudsc
 
 using namespace cloudsc;
@@ -38,8 +41,12 @@ bool g_have_params = false;
 unsigned long long g_gen = 0;
 constexpr int kMaxDev = 64;
 unsigned long long g_dev_gen[kMaxDev] = {0};
-int g_threads[2] = {448, 448};
-int g_ctas_per_sm[2] = {0, 0};
+// Launch schedule per precision (0 FP64, 1 FP32-mixed): compiled variant,
+// columns per CTA, persistent CTAs per SM (0: one CTA per column tile).
+struct Schedule {
+  int variant, threads, ctas_per_sm;
+};
+Schedule g_sched[2] = {{default_variant(), 448, 0}, {default_variant(), 448, 0}};
 
 int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
   t_last_error = what;
@@ -95,14 +102,12 @@ int check_params_match(const cloudsc_params *p) {
   return CLOUDSC_OK;
 }
 
-int grid_for(int precision, int tiles, int threads) {
-  int ctas = g_ctas_per_sm[precision];
+int grid_for(int ctas, int tiles) {
   if (ctas <= 0) return tiles;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int g = sms * ctas;
-  (void)threads;
   return g < tiles ? g : tiles;
 }
 
@@ -322,27 +327,83 @@ int cloudsc_b200_setup(const cloudsc_params *p) {
   return ensure_params(nullptr);
 }
 
-int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm) {
+int cloudsc_b200_num_variants(void) { return num_variants(); }
+
+int cloudsc_b200_variant_info(int32_t precision, int32_t variant, int32_t *max_threads, int32_t *min_ctas,
+                              int32_t *regs, int32_t *local_bytes) {
   if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
-  if (threads_per_cta < 32 || threads_per_cta > max_threads(precision) || threads_per_cta % 32)
-    return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32, at least 32 and at most "
-                                 "the kernel's compiled limit (448)");
-  if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(CLOUDSC_E_SHAPE, "ctas_per_sm must be in [0,32]");
-  std::lock_guard<std::mutex> lk(g_mu);
-  g_threads[precision] = threads_per_cta;
-  g_ctas_per_sm[precision] = ctas_per_sm;
+  if (variant < 0 || variant >= num_variants()) return fail(CLOUDSC_E_SHAPE, "no such variant");
+  int mt = 0, mb = 0, r = -1, l = -1;
+  variant_bounds(variant, &mt, &mb);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) == cudaSuccess && ndev > 0) {
+    cudaError_t e = variant_attributes(precision, variant, &r, &l);
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaFuncGetAttributes", e);
+  } else {
+    cudaGetLastError();  // no device: registers and local bytes stay -1
+  }
+  if (max_threads) *max_threads = mt;
+  if (min_ctas) *min_ctas = mb;
+  if (regs) *regs = r;
+  if (local_bytes) *local_bytes = l;
   return CLOUDSC_OK;
 }
 
+int cloudsc_b200_set_schedule(int32_t precision, int32_t variant, int32_t threads_per_cta,
+                              int32_t ctas_per_sm) {
+  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (variant < 0 || variant >= num_variants()) return fail(CLOUDSC_E_SHAPE, "no such variant");
+  int mt = 0, mb = 0;
+  variant_bounds(variant, &mt, &mb);
+  if (threads_per_cta < 32 || threads_per_cta > mt || threads_per_cta % 32)
+    return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32, at least 32 and at most "
+                                 "the variant's compiled limit");
+  if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(CLOUDSC_E_SHAPE, "ctas_per_sm must be in [0,32]");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_sched[precision] = {variant, threads_per_cta, ctas_per_sm};
+  return CLOUDSC_OK;
+}
+
+int cloudsc_b200_get_schedule(int32_t precision, int32_t *variant, int32_t *threads_per_cta,
+                              int32_t *ctas_per_sm) {
+  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  std::lock_guard<std::mutex> lk(g_mu);
+  const Schedule sc = g_sched[precision];
+  if (variant) *variant = sc.variant;
+  if (threads_per_cta) *threads_per_cta = sc.threads;
+  if (ctas_per_sm) *ctas_per_sm = sc.ctas_per_sm;
+  return CLOUDSC_OK;
+}
+
+// The variant with the most registers per thread that still holds a CTA of
+// threads_per_cta: the smallest compiled limit >= threads_per_cta among the
+// one-CTA-per-SM variants.
+int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm) {
+  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  int best = -1, best_mt = 1 << 30;
+  for (int v = 0; v < num_variants(); ++v) {
+    int mt = 0, mb = 0;
+    variant_bounds(v, &mt, &mb);
+    if (mb == 1 && mt >= threads_per_cta && mt < best_mt) {
+      best = v;
+      best_mt = mt;
+    }
+  }
+  if (best < 0 || threads_per_cta < 32 || threads_per_cta % 32)
+    return fail(CLOUDSC_E_SHAPE, "threads_per_cta must be a multiple of 32, at least 32 and at most "
+                                 "the largest compiled limit");
+  return cloudsc_b200_set_schedule(precision, best, threads_per_cta, ctas_per_sm);
+}
+
 static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaStream_t stream) {
-  int threads, tiles;
+  Schedule sc;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    threads = g_threads[precision];
+    sc = g_sched[precision];
   }
-  tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
-  int grid = grid_for(precision, tiles, threads);
-  cudaError_t e = launch(precision, f, sh, threads, grid, stream);
+  const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + sc.threads - 1) / sc.threads);
+  const int grid = grid_for(sc.ctas_per_sm, tiles);
+  cudaError_t e = launch(precision, sc.variant, f, sh, sc.threads, grid, stream);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
   return CLOUDSC_OK;
 }
@@ -439,6 +500,30 @@ size_t rows(Kind k, size_t klev) { return elems(k, 1, klev); }
 // are copied back and the caller's NCLV slice is left as it was.
 constexpr int kLocCld = 9;
 size_t out_rows(int i, size_t klev) { return i == kLocCld ? 4 * klev : rows(kArrs[i].kind, klev); }
+// Rows of input array i that the kernels read, from the start of each block's
+// slab.  The species arrays are read only in part at the default
+// configuration: PTENDENCY_CML_CLD and PCLV for species 1..NCLV-1
+// (cloudsc.F90:995-999, vapour comes from PQ), PLUDELI for its first two
+// components (liquid and ice detrainment, :1372-1373, :4265, :4280).  Only these rows cross
+// PCIe; the device rows after them are never read.
+constexpr int kCmlCld = 5, kPludeli = 20, kPclv = 25;
+size_t in_rows(int i, size_t klev) {
+  if (i == kCmlCld || i == kPclv) return 4 * klev;
+  if (i == kPludeli) return 2 * klev;
+  return rows(kArrs[i].kind, klev);
+}
+size_t elem_size(int i) { return (i == 15 || i == 16) ? 4 : 8; }
+// Host-to-device copy of blocks b0 .. b0+nb-1 of input array i (the rows the
+// kernels read) into a device slab of nb blocks.
+cudaError_t copy_in(void *dst, const void *host, int i, size_t np, size_t kl, size_t b0, size_t nb,
+                    cudaStream_t s) {
+  const size_t esz = elem_size(i);
+  const size_t per = elems(kArrs[i].kind, np, kl) * esz;  // one block's slab
+  const size_t used = in_rows(i, kl) * np * esz;
+  const char *src = (const char *)host + b0 * per;
+  if (used == per) return cudaMemcpyAsync(dst, src, per * nb, cudaMemcpyHostToDevice, s);
+  return cudaMemcpy2DAsync(dst, per, src, per, used, nb, cudaMemcpyHostToDevice, s);
+}
 
 struct Workspace {
   int dev = -1;
@@ -592,11 +677,8 @@ int cloudsc_b200_block(
   carve(t_ws.buf, np, kl, 1, d);
   cudaStream_t s = t_ws.st[0];
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
-    if (!kArrs[i].in) continue;
-    size_t esz = (i == 15 || i == 16) ? 4 : 8;
-    e = cudaMemcpyAsync(d[i], host[i], elems(kArrs[i].kind, np, kl) * esz, cudaMemcpyHostToDevice, s);
-  }
+  for (int i = 0; i < 42 && e == cudaSuccess; ++i)
+    if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, 0, 1, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
   Fields f = fields_from(d, t_ws.counter);
@@ -667,13 +749,8 @@ int cloudsc_b200_batched_host(
     carve(t_ws.buf + slot * slot_bytes, np, kl, cb, d);
     // the slot is free once its previous D2H has finished
     if (c >= nslot) e = cudaStreamWaitEvent(t_ws.st[0], t_ws.ev_out[slot], 0);
-    for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
-      if (!kArrs[i].in) continue;
-      size_t esz = (i == 15 || i == 16) ? 4 : 8;
-      size_t per = elems(kArrs[i].kind, np, kl) * esz;
-      e = cudaMemcpyAsync(d[i], (const char *)host[i] + (size_t)b0 * per, per * nb, cudaMemcpyHostToDevice,
-                          t_ws.st[0]);
-    }
+    for (int i = 0; i < 42 && e == cudaSuccess; ++i)
+      if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, b0, nb, t_ws.st[0]);
     if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_in[slot], t_ws.st[0]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[1], t_ws.ev_in[slot], 0);
     if (e != cudaSuccess) break;
@@ -791,11 +868,8 @@ int cloudsc_b200_block_noalloc(
   carve(base + 256, np, kl, 1, d);
   cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e = cudaSuccess;
-  for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
-    if (!kArrs[i].in) continue;
-    size_t esz = (i == 15 || i == 16) ? 4 : 8;
-    e = cudaMemcpyAsync(d[i], host[i], elems(kArrs[i].kind, np, kl) * esz, cudaMemcpyHostToDevice, s);
-  }
+  for (int i = 0; i < 42 && e == cudaSuccess; ++i)
+    if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, 0, 1, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
   Fields f = fields_from(d, counter);

@@ -94,39 +94,62 @@ cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
   return e;
 }
 
-// Register budget and CTA size: __launch_bounds__(MAXT, MINB).  One CTA of
-// 448 threads per SM: 14 warps in per-level lock-step at 128 registers (some
-// hundred bytes of spills), and 262,144 columns are 586 tiles = 3.96 waves
-// over 148 SMs.  Measured at 262,144 columns, FP64: 15.98 ms; 384 threads
-// (168 registers) 17.77 ms; 480 threads 16.17 ms; three 128-thread CTAs per
-// SM with the same barrier 21.7 ms; no barrier 23.9 ms.
-#ifndef CLOUDSC_MAXT
-#define CLOUDSC_MAXT 448
-#endif
-#ifndef CLOUDSC_MINB
-#define CLOUDSC_MINB 1
-#endif
-#ifndef CLOUDSC_MIX_MAXT
-#define CLOUDSC_MIX_MAXT 448
-#endif
-#ifndef CLOUDSC_MIX_MINB
-#define CLOUDSC_MIX_MINB 1
-#endif
+// Compiled launch variants: the __launch_bounds__(MAXT, MINB) pairs the
+// kernels are built with.  MAXT x MINB threads share an SM's 65,536
+// registers, so each pair fixes the register budget per thread (and with it
+// the spills) and the CTA size it is meant for; the autotuner picks a
+// variant, a CTA size up to its MAXT and the persistence at run time.
+// Measured at 262,144 columns, FP64: (448,1) 15.98 ms with 128 registers;
+// (384,1) 17.77 ms with 168; three 128-thread CTAs per SM 21.7 ms.
+struct Variant {
+  int maxt, minb;
+};
+constexpr Variant kVariants[] = {{640, 1}, {512, 1}, {384, 1}, {256, 1}, {256, 2}, {128, 3}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+constexpr int kDefaultVariant = 1;  // (512, 1), run with 448 columns per CTA
 
-// Largest CTA the kernel of `precision` was compiled for.
-int max_threads(int precision) { return precision == 0 ? CLOUDSC_MAXT : CLOUDSC_MIX_MAXT; }
+int num_variants() { return kNumVariants; }
+int default_variant() { return kDefaultVariant; }
+void variant_bounds(int v, int *maxt, int *minb) {
+  *maxt = kVariants[v].maxt;
+  *minb = kVariants[v].minb;
+}
 
-// Launch the kernel: precision 0 = FP64, 1 = FP32-mixed.
-cudaError_t launch(int precision, const Fields &f, const Shape &sh, int threads, int grid,
-                   cudaStream_t stream) {
-  if (precision == 0) {
-    if (threads > CLOUDSC_MAXT) return cudaErrorInvalidConfiguration;
-    cloudsc_kernel<false, CLOUDSC_MAXT, CLOUDSC_MINB><<<grid, threads, 0, stream>>>(f, sh);
-  } else {
-    if (threads > CLOUDSC_MIX_MAXT) return cudaErrorInvalidConfiguration;
-    cloudsc_kernel<true, CLOUDSC_MIX_MAXT, CLOUDSC_MIX_MINB><<<grid, threads, 0, stream>>>(f, sh);
+template <bool F32M>
+static const void *kernel_ptr(int v) {
+  switch (v) {
+    case 0: return (const void *)cloudsc_kernel<F32M, kVariants[0].maxt, kVariants[0].minb>;
+    case 1: return (const void *)cloudsc_kernel<F32M, kVariants[1].maxt, kVariants[1].minb>;
+    case 2: return (const void *)cloudsc_kernel<F32M, kVariants[2].maxt, kVariants[2].minb>;
+    case 3: return (const void *)cloudsc_kernel<F32M, kVariants[3].maxt, kVariants[3].minb>;
+    case 4: return (const void *)cloudsc_kernel<F32M, kVariants[4].maxt, kVariants[4].minb>;
+    case 5: return (const void *)cloudsc_kernel<F32M, kVariants[5].maxt, kVariants[5].minb>;
+    default: return nullptr;
   }
-  return cudaGetLastError();
+}
+static_assert(kNumVariants == 6, "kernel_ptr lists every variant");
+
+// Registers and local (spill) bytes per thread of variant v (needs a device).
+cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes) {
+  const void *k = precision == 0 ? kernel_ptr<false>(v) : kernel_ptr<true>(v);
+  if (!k) return cudaErrorInvalidValue;
+  cudaFuncAttributes a;
+  cudaError_t e = cudaFuncGetAttributes(&a, k);
+  if (e != cudaSuccess) return e;
+  *regs = a.numRegs;
+  *local_bytes = (int)a.localSizeBytes;
+  return cudaSuccess;
+}
+
+// Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed.
+cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
+                   cudaStream_t stream) {
+  if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
+  const void *k = precision == 0 ? kernel_ptr<false>(v) : kernel_ptr<true>(v);
+  Fields fa = f;
+  Shape sa = sh;
+  void *args[] = {&fa, &sa};
+  return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, 0, stream);
 }
 
 }  // namespace cloudsc

@@ -99,3 +99,15 @@ def bytes_per_column(klev=137, fp=8):
     writes_lv = 9  # LOC_T LOC_Q LOC_A LOC_CLD*4 PCOVPTOT PLUDE
     write = (writes_lv * klev + 14 * (klev + 1) + 1) * fp
     return read, write
+
+
+def host_copy_bytes(nproma, klev, ngpblks, ngptot=None):
+    """Bytes cloudsc_b200_batched_host copies (host to device, device to host).
+
+    Inputs cross PCIe as whole blocks, and only the rows the default
+    configuration reads (bytes_per_column's read list: four of the five
+    PTENDENCY_CML_CLD and PCLV species, two of the four PLUDELI components);
+    outputs come back for the NGPTOT computed columns only."""
+    ngptot = nproma * ngpblks if ngptot is None else ngptot
+    read, write = bytes_per_column(klev)
+    return read * nproma * ngpblks, write * ngptot

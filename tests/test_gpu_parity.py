@@ -117,10 +117,20 @@ def test_config2_sampled_blocks(cuda):
     assert not bad, bad
 
 
+def _poison_unread(a, ax):
+    sl = (slice(None),) * ax
+    a["tendency_cml_cld"][sl + (4,)] = np.nan
+    a["pclv"][sl + (4,)] = np.nan
+    a["pludeli"][sl + (slice(2, 4),)] = np.nan
+
+
 def test_host_pointer_paths(cuda):
     """cloudsc_b200_batched_host (pipelined chunks, partial last chunk and
     block) and the per-block drop-in cloudsc_b200_block give the same results
-    as the oracle; the block entry leaves columns outside KIDIA..KFDIA alone."""
+    as the oracle; the block entry leaves columns outside KIDIA..KFDIA alone.
+    The input rows the scheme never reads (the vapour species of
+    PTENDENCY_CML_CLD and PCLV, PLUDELI's third and fourth components) are
+    NaN on the host: they are not copied to the device."""
     p, po = util.params()
     nproma, nblk, ngptot = 64, 7, 7 * 64 - 9
     arrs = inputs.generate(nblk, nproma, p, seed=41)
@@ -130,6 +140,7 @@ def test_host_pointer_paths(cuda):
     for n in util.fields.OUTPUT_NAMES:
         if n != "plude":
             host[n][:] = 7.0  # sentinel: untouched padding must survive
+    _poison_unread(host, 1)
     cloudsc.cloudsc_batched_host(p, host, nproma, util.KLEV, nblk, ngptot, util.PTSPHY,
                                  chunk_blocks=3)
     rep, _ = util.compare(host, ref, ngptot=ngptot, nproma=nproma)
@@ -146,6 +157,7 @@ def test_host_pointer_paths(cuda):
     for n in util.fields.OUTPUT_NAMES:
         if n != "plude":
             blk[n][:] = 7.0
+    _poison_unread(blk, 0)
     cloudsc.cloudsc_block(p, kidia, kfdia, nproma, util.KLEV, util.PTSPHY, blk)
     # oracle over the whole block; columns are independent, so compare the range
     ref1, _ = util.run_oracle(po, one, nproma, 1, nproma, libm="plibm")
