@@ -365,8 +365,9 @@ def run_ours(a):
     # launch schedule per precision: the autotuner's recorded choice for this
     # device and shape, or tuned now (untimed; rank 0 records it)
     from openifs_b200 import autotune
+    forms = ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed"), (cloudsc.PHYS32, "phys32"))
     schedule = {}
-    for prec, name in ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed")):
+    for prec, name in forms:
         entry, src = autotune.apply_cached(prec, NPROMA, KLEV, NGPBLKS), "cache"
         if entry is None:
             entry = autotune.tune(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, prec, stream=stream,
@@ -376,7 +377,7 @@ def run_ours(a):
 
     results = {}
     clocks = None
-    for prec, name in ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed")):
+    for prec, name in forms:
         if name == "fp64":
             with ClockSampler(local) as cs:
                 ms = timed(prec, a.steps, a.warmup)
@@ -390,25 +391,33 @@ def run_ours(a):
             mean_ms = float(t.item())
         results[name] = {"ms": mean_ms, "min_ms": min(ms)}
 
-    # fixed-error check of the mixed form against the FP64 kernel (same inputs)
+    # fixed-error check of the reduced-precision forms against the FP64 kernel
+    # (same inputs): every tendency, the four condensate species separately,
+    # and the surface rain and snow fluxes
     outs = fields.OUTPUT_NAMES
     d["plude"].copy_(plude0)
     cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.FP64)
     ref = {n: d[n].clone() for n in outs}
-    d["plude"].copy_(plude0)
-    cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.MIXED)
-    torch.cuda.synchronize(dev)
-    err = {}
-    for n in ["tendency_loc_t", "tendency_loc_q", "tendency_loc_a", "tendency_loc_cld",
-              "pfplsl", "pfplsn"]:
-        r, g = ref[n], d[n]
-        if n == "tendency_loc_cld":
-            r, g = r[:, :4], g[:, :4]
-        if n in ("pfplsl", "pfplsn"):  # surface fluxes
-            r, g = r[:, -1], g[:, -1]
-        diff = (g - r).abs()
-        err[n] = {"max_abs_over_max": float(diff.max() / r.abs().max().clamp_min(1e-300)),
-                  "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
+    errs = {}
+    for prec, name in forms[1:]:
+        d["plude"].copy_(plude0)
+        cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=prec)
+        torch.cuda.synchronize(dev)
+        err = {}
+        cases = [("tendency_loc_t", None), ("tendency_loc_q", None), ("tendency_loc_a", None)]
+        cases += [("tendency_loc_cld", m) for m in range(4)] + [("pfplsl", -1), ("pfplsn", -1)]
+        for n, sl in cases:
+            r, g = ref[n], d[n]
+            label = n
+            if n == "tendency_loc_cld":
+                r, g = r[:, sl], g[:, sl]
+                label = f"{n}_{'lirs'[sl]}"
+            elif sl is not None:  # surface fluxes
+                r, g = r[:, sl], g[:, sl]
+            diff = (g - r).abs()
+            err[label] = {"max_abs_over_max": float(diff.max() / r.abs().max().clamp_min(1e-300)),
+                          "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
+        errs[name] = err
 
     sur = None
     if not a.no_surrogate:
@@ -486,7 +495,13 @@ def run_ours(a):
             "fp64": {"columns_per_s": value, "ms": ms64, "min_ms": results["fp64"]["min_ms"]},
             "mixed": {"columns_per_s": world * NCOL / (results["mixed"]["ms"] * 1e-3),
                       "ms": results["mixed"]["ms"], "speedup_vs_fp64": ms64 / results["mixed"]["ms"],
-                      "error_vs_fp64": err},
+                      "arithmetic": "FP32 exponentials and powers; everything else FP64",
+                      "error_vs_fp64": errs["mixed"]},
+            "phys32": {"columns_per_s": world * NCOL / (results["phys32"]["ms"] * 1e-3),
+                       "ms": results["phys32"]["ms"], "speedup_vs_fp64": ms64 / results["phys32"]["ms"],
+                       "arithmetic": "FP32 process rates and transcendentals; state, sink limiters, 5x5 "
+                                     "solve, saturation adjustment and budgets FP64",
+                       "error_vs_fp64": errs["phys32"]},
             "surrogate": sur,
         },
         "roofline": roofline,

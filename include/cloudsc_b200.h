@@ -174,8 +174,11 @@ int cloudsc_b200_block(
  * NPROMA/NGPBLKS/NGPTOT.  The optional `ncounters` device buffer (may be NULL)
  * receives the number of negative-condensate warning events (uint32, added to).
  * `precision` selects the arithmetic: 0 = FP64 (the reference's double
- * build), 1 = FP32-mixed (FP32 microphysics, FP64 5x5 solve, saturation
- * adjustment and budget sums).
+ * build); 1 = FP32-mixed (the exponentials and powers of the microphysics and
+ * of the level's saturation values in FP32, everything else in FP64);
+ * 2 = FP32 physics (the process rates in FP32 as well; the state, the sink
+ * limiters, the 5x5 solve, the saturation adjustment and the tendency and
+ * flux budgets in FP64).
  */
 int cloudsc_b200_batched(
     const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks,
@@ -271,7 +274,8 @@ size_t cloudsc_b200_params_size(void);
  * Launch schedule of the kernels (the autotuner's knobs; no reference
  * counterpart: the reference runs CLOUDSC on CPU threads, one NPROMA block
  * per call, ec_phys_drv.F90:438).  Every entry point that launches a kernel
- * uses the schedule set for its precision (0 FP64, 1 FP32-mixed).
+ * uses the schedule set for its precision (0 FP64, 1 FP32-mixed, 2 FP32
+ * physics).
  *
  * The kernels are compiled in several variants, each a
  * __launch_bounds__(max_threads, min_ctas) pair that fixes the register

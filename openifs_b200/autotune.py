@@ -1,6 +1,6 @@
 """Autotuner of the CLOUDSC kernels' launch schedule.
 
-A schedule, per precision (FP64 or FP32-mixed), is
+A schedule, per precision (FP64, FP32-mixed or FP32 physics), is
 
     variant      one of the compiled __launch_bounds__(max_threads, min_ctas)
                  pairs of the kernels, which fixes the registers per thread
@@ -25,7 +25,7 @@ import statistics
 from . import cloudsc
 
 DEFAULT_CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "schedules.json")
-PREC_NAME = {cloudsc.FP64: "fp64", cloudsc.MIXED: "mixed"}
+PREC_NAME = {cloudsc.FP64: "fp64", cloudsc.MIXED: "mixed", cloudsc.PHYS32: "phys32"}
 
 
 def candidates(precision):
@@ -170,7 +170,7 @@ def ensure(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision, cac
 
 def main(argv=None):
     """python -m openifs_b200.autotune [--nproma 128 --ngpblks 2048]: tune
-    both precisions on seeded synthetic inputs of that shape and record the
+    every precision on seeded synthetic inputs of that shape and record the
     schedules in the cache."""
     import argparse
     import torch
@@ -189,7 +189,7 @@ def main(argv=None):
     host = inputs.generate(a.ngpblks, a.nproma, p, klev=klev, seed=a.seed)
     d = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
     ncol = a.nproma * a.ngpblks
-    for prec in (cloudsc.FP64, cloudsc.MIXED):
+    for prec in (cloudsc.FP64, cloudsc.MIXED, cloudsc.PHYS32):
         r = tune(p, d, a.nproma, klev, a.ngpblks, ncol, a.ptsphy, prec, reps=a.reps, cache=a.cache,
                  log=print)
         print(PREC_NAME[prec], "best", json.dumps(r["best"]))

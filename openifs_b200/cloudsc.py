@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(_HERE, "libcloudsc_b200.so")
 
 FP64 = 0
 MIXED = 1
+PHYS32 = 2  # FP32 process rates; state, solve, saturation adjustment and budgets in FP64
 
 
 class CloudscError(RuntimeError):

@@ -41,12 +41,12 @@ bool g_have_params = false;
 unsigned long long g_gen = 0;
 constexpr int kMaxDev = 64;
 unsigned long long g_dev_gen[kMaxDev] = {0};
-// Launch schedule per precision (0 FP64, 1 FP32-mixed): compiled variant,
+// Launch schedule per precision (0 FP64, 1 FP32-mixed, 2 FP32 physics): compiled variant,
 // columns per CTA, persistent CTAs per SM (0: one CTA per column tile).
 struct Schedule {
   int variant, threads, ctas_per_sm;
 };
-Schedule g_sched[2] = {{default_variant(), 448, 0}, {default_variant(), 448, 0}};
+Schedule g_sched[3] = {{default_variant(), 448, 0}, {default_variant(), 448, 0}, {default_variant(), 448, 0}};
 
 int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
   t_last_error = what;
@@ -331,7 +331,7 @@ int cloudsc_b200_num_variants(void) { return num_variants(); }
 
 int cloudsc_b200_variant_info(int32_t precision, int32_t variant, int32_t *max_threads, int32_t *min_ctas,
                               int32_t *regs, int32_t *local_bytes) {
-  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   if (variant < 0 || variant >= num_variants()) return fail(CLOUDSC_E_SHAPE, "no such variant");
   int mt = 0, mb = 0, r = -1, l = -1;
   variant_bounds(variant, &mt, &mb);
@@ -351,7 +351,7 @@ int cloudsc_b200_variant_info(int32_t precision, int32_t variant, int32_t *max_t
 
 int cloudsc_b200_set_schedule(int32_t precision, int32_t variant, int32_t threads_per_cta,
                               int32_t ctas_per_sm) {
-  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   if (variant < 0 || variant >= num_variants()) return fail(CLOUDSC_E_SHAPE, "no such variant");
   int mt = 0, mb = 0;
   variant_bounds(variant, &mt, &mb);
@@ -366,7 +366,7 @@ int cloudsc_b200_set_schedule(int32_t precision, int32_t variant, int32_t thread
 
 int cloudsc_b200_get_schedule(int32_t precision, int32_t *variant, int32_t *threads_per_cta,
                               int32_t *ctas_per_sm) {
-  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   std::lock_guard<std::mutex> lk(g_mu);
   const Schedule sc = g_sched[precision];
   if (variant) *variant = sc.variant;
@@ -379,7 +379,7 @@ int cloudsc_b200_get_schedule(int32_t precision, int32_t *variant, int32_t *thre
 // threads_per_cta: the smallest compiled limit >= threads_per_cta among the
 // one-CTA-per-SM variants.
 int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm) {
-  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   int best = -1, best_mt = 1 << 30;
   for (int v = 0; v < num_variants(); ++v) {
     int mt = 0, mb = 0;
@@ -424,7 +424,7 @@ int cloudsc_b200_batched(
     void *stream) {
   int rc = check_params_match(p);
   if (rc) return rc;
-  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
     return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
@@ -715,7 +715,7 @@ int cloudsc_b200_batched_host(
     double *pfplsn, double *pfhpsl, double *pfhpsn, int32_t precision, int32_t chunk_blocks) {
   int rc = check_params_match(p);
   if (rc) return rc;
-  if (precision < 0 || precision > 1) return fail(CLOUDSC_E_SHAPE, "precision must be 0 or 1");
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
     return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");

@@ -9,6 +9,11 @@
 #include <cstdint>
 
 #define CSC_DEV __device__ __forceinline__
+// plibm's exp/log tables are read from a shared-memory copy per CTA (filled
+// at kernel start): the table lookups sit on the dependent path of every
+// exp and pow, and shared-memory latency is below the L1 hit latency of a
+// global load.  Measured at 262,144 columns, FP64: 15.75 ms vs 16.05 ms.
+#define PLIBM_SMEM_TABLES 1
 // Every column of a CTA meets the others at the end of each level, so all
 // warps of the CTA run the same stretch of the (very long) level code at the
 // same time and share the instruction cache.
@@ -50,8 +55,23 @@ namespace cloudsc {
 // runs the level loop, so the per-level barrier is reached by all; a thread
 // whose column is outside KIDIA..ICEND computes a valid stand-in column and
 // stores nothing.
-template <bool F32M, int MAXT, int MINB>
+// FORM selects the arithmetic of the column body:
+//   0  FP64, the reference's double build;
+//   1  FP32-mixed: FP32 transcendentals, everything else in double;
+//   2  FP32 physics: the process rates in FP32 as well (Real = float); the
+//      state, the sink limiters, the 5x5 solve, CLOUD_SUPERSATCHECK and the
+//      tendency and flux budgets stay in double.  Float rounding of the rates
+//      leaves residues above CLOUDSC's 1e-14 kg/kg thresholds that switch
+//      precipitation processes on and off down the column, so this form is
+//      faster but further from FP64 (measured tendency errors of 0.3-4 %).
+template <int FORM, int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh) {
+  // Let ptxas place part of the register spills in shared memory instead of
+  // local memory (a PTX pragma; the spill slots it moves no longer go
+  // through L1/L2).  With the shared-memory tables, FP64: 15.29 ms vs
+  // 15.75 ms; FP32-mixed: 11.28 ms vs 11.72 ms.
+  asm volatile(".pragma \"enable_smem_spilling\";");
+  plibm_load_tables();
   const long long ncols = (long long)sh.ngpblks * sh.nproma;
   const long long ntiles = (ncols + blockDim.x - 1) / blockDim.x;
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -64,12 +84,10 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
       ib = 0;
       jl = sh.kidia0;
     }
-    // FP32-mixed: FP32 transcendentals, everything else in double.  (Process
-    // rates in float as well were measured at 2.06x the FP64 kernel but with
-    // 0.3-4 % tendency errors: float rounding of the rates leaves residues
-    // above CLOUDSC's 1e-14 kg/kg thresholds, which switch precipitation
-    // processes on and off down the column.)
-    cloudsc_column<double, F32M>(F, sh, ib, jl, active);
+    if (FORM == 2)
+      cloudsc_column<float, true>(F, sh, ib, jl, active);
+    else
+      cloudsc_column<double, FORM == 1>(F, sh, ib, jl, active);
   }
 }
 
@@ -115,23 +133,31 @@ void variant_bounds(int v, int *maxt, int *minb) {
   *minb = kVariants[v].minb;
 }
 
-template <bool F32M>
-static const void *kernel_ptr(int v) {
+template <int FORM>
+static const void *kernel_ptr_form(int v) {
   switch (v) {
-    case 0: return (const void *)cloudsc_kernel<F32M, kVariants[0].maxt, kVariants[0].minb>;
-    case 1: return (const void *)cloudsc_kernel<F32M, kVariants[1].maxt, kVariants[1].minb>;
-    case 2: return (const void *)cloudsc_kernel<F32M, kVariants[2].maxt, kVariants[2].minb>;
-    case 3: return (const void *)cloudsc_kernel<F32M, kVariants[3].maxt, kVariants[3].minb>;
-    case 4: return (const void *)cloudsc_kernel<F32M, kVariants[4].maxt, kVariants[4].minb>;
-    case 5: return (const void *)cloudsc_kernel<F32M, kVariants[5].maxt, kVariants[5].minb>;
+    case 0: return (const void *)cloudsc_kernel<FORM, kVariants[0].maxt, kVariants[0].minb>;
+    case 1: return (const void *)cloudsc_kernel<FORM, kVariants[1].maxt, kVariants[1].minb>;
+    case 2: return (const void *)cloudsc_kernel<FORM, kVariants[2].maxt, kVariants[2].minb>;
+    case 3: return (const void *)cloudsc_kernel<FORM, kVariants[3].maxt, kVariants[3].minb>;
+    case 4: return (const void *)cloudsc_kernel<FORM, kVariants[4].maxt, kVariants[4].minb>;
+    case 5: return (const void *)cloudsc_kernel<FORM, kVariants[5].maxt, kVariants[5].minb>;
     default: return nullptr;
   }
 }
-static_assert(kNumVariants == 6, "kernel_ptr lists every variant");
+static_assert(kNumVariants == 6, "kernel_ptr_form lists every variant");
+static const void *kernel_ptr(int precision, int v) {
+  switch (precision) {
+    case 0: return kernel_ptr_form<0>(v);
+    case 1: return kernel_ptr_form<1>(v);
+    case 2: return kernel_ptr_form<2>(v);
+    default: return nullptr;
+  }
+}
 
 // Registers and local (spill) bytes per thread of variant v (needs a device).
 cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes) {
-  const void *k = precision == 0 ? kernel_ptr<false>(v) : kernel_ptr<true>(v);
+  const void *k = kernel_ptr(precision, v);
   if (!k) return cudaErrorInvalidValue;
   cudaFuncAttributes a;
   cudaError_t e = cudaFuncGetAttributes(&a, k);
@@ -141,11 +167,13 @@ cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes
   return cudaSuccess;
 }
 
-// Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed.
+// Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed,
+// 2 = FP32 physics.
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream) {
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  const void *k = precision == 0 ? kernel_ptr<false>(v) : kernel_ptr<true>(v);
+  const void *k = kernel_ptr(precision, v);
+  if (!k) return cudaErrorInvalidValue;
   Fields fa = f;
   Shape sa = sh;
   void *args[] = {&fa, &sa};

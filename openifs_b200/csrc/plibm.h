@@ -62,15 +62,32 @@ static __device__ const double plibm_exp_tbl_d[256] = PLIBM_EXP_TBL_INIT;
 static __device__ const double plibm_log_tbl_d[384] = PLIBM_LOG_TBL_INIT;
 #endif
 
+/* With PLIBM_SMEM_TABLES, device code reads per-CTA shared-memory copies of
+ * the tables, which every kernel that calls plibm fills first with
+ * plibm_load_tables() (all threads of the CTA, then a CTA barrier). */
+#if defined(__CUDACC__) && defined(PLIBM_SMEM_TABLES)
+static __shared__ double plibm_exp_tbl_s[256];
+static __shared__ double plibm_log_tbl_s[384];
+static __device__ __forceinline__ void plibm_load_tables() {
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) plibm_exp_tbl_s[i] = plibm_exp_tbl_d[i];
+  for (int i = threadIdx.x; i < 384; i += blockDim.x) plibm_log_tbl_s[i] = plibm_log_tbl_d[i];
+  __syncthreads();
+}
+#endif
+
 PLIBM_FN double plibm_exp_t(int i) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && defined(PLIBM_SMEM_TABLES)
+  return plibm_exp_tbl_s[i];
+#elif defined(__CUDA_ARCH__)
   return __ldg(&plibm_exp_tbl_d[i]);
 #else
   return plibm_exp_tbl[i];
 #endif
 }
 PLIBM_FN double plibm_log_t(int i) {
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && defined(PLIBM_SMEM_TABLES)
+  return plibm_log_tbl_s[i];
+#elif defined(__CUDA_ARCH__)
   return __ldg(&plibm_log_tbl_d[i]);
 #else
   return plibm_log_tbl[i];

@@ -182,3 +182,20 @@ def test_mixed_precision_error(cuda):
         print(k, v)
     for k, v in stats.items():
         assert np.isfinite(v["normwise_max"]), k
+
+
+def test_phys32_form(cuda):
+    """FP32-physics kernel (FP32 process rates; state, solve, saturation
+    adjustment and budgets in FP64) vs the FP64 oracle: finite everywhere,
+    RMS errors of the T and q tendencies and of the surface fluxes bounded
+    (threshold flips make it far less accurate than the FP32-mixed form)."""
+    p, po = util.params()
+    arrs = inputs.generate(100, 32, p, seed=1)
+    ref, _ = util.run_oracle(po, arrs, 32, 100, 3200, libm="plibm")
+    gpu, _ = util.run_gpu(p, arrs, 32, 100, 3200, precision=cloudsc.PHYS32)
+    stats = util.mixed_error_stats(gpu, ref)
+    for k, v in stats.items():
+        print(k, v)
+        assert np.isfinite(v["normwise_max"]), k
+    for k in ("tendency_loc_t", "tendency_loc_q"):
+        assert stats[k]["rms_ratio"] < 0.1, (k, stats[k])
