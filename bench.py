@@ -8,8 +8,11 @@ state (openifs_b200/inputs.py, seed 2).  One step is one batched CLOUDSC call
 over every column; inputs stay resident in HBM (15 GB, far above the 126 MB
 L2, so no flush is needed between steps).  PLUDE is INOUT (cloudsc.F90:1367),
 so it is restored from a pristine copy before every step, outside the timed
-kernel.  ``value`` is FP64 columns/s; the FP32-mixed form is reported beside
-it with its error against the FP64 kernel, and the guarded learned surrogate
+kernel.  ``value`` is FP64 columns/s; the FP32-mixed and FP32-physics forms
+are reported beside it with their errors against the FP64 kernel, the launch
+schedule of each form comes from the autotuner's record (or is tuned in the
+run), CLOUD_SATADJ (the saturation adjustment before CLOUDSC) is timed on the
+same columns with its HBM roofline, and the guarded learned surrogate
 (openifs_b200/surrogate.py) over 1,048,576 columns (4 batches of 262,144 in
 one CUDA graph) with its flagged fraction, errors, budget closure and the
 tensor-core throughput of its GEMMs.  ``e2e`` is the same FP64 metric
@@ -193,6 +196,69 @@ def run_reference(a):
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def satadj_form(a, p, host, dev, world, rank, stream):
+    """CLOUD_SATADJ (the saturation adjustment that runs before CLOUDSC) on
+    the same 262,144 columns: device time of the batched kernel, its HBM
+    roofline, the per-point water/enthalpy closure, and the oracle on a
+    64-block sample of the same inputs for the CPU rate."""
+    import torch
+    from openifs_b200 import cloudsc, fields, inputs
+    from oracle import oracle
+    sh = inputs.satadj_from(host, NPROMA, seed=SEED + 1000 * rank)
+    d = {k: torch.from_numpy(v).to(dev) for k, v in sh.items()}
+
+    def step():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloudsc.satadj_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, stream=stream)
+        e1.record(stream)
+        return e0, e1
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    ev = [step() for _ in range(a.steps)]
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    q, l, i, tt = (d[f"tendency_loc_{c}"] for c in "qlit")
+    water = float((q + l + i).abs().max() / q.abs().max())
+    enth = float((tt - p.ralvdcp * l - p.ralsdcp * i).abs().max() / tt.abs().max())
+    rb, wb = fields.satadj_bytes_per_column(KLEV, p.ncldtop)
+    algo = NCOL * (rb + wb)
+    peaks = _peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    del d
+    torch.cuda.empty_cache()
+    # CPU: the oracle (glibc) on 64 blocks of the same input, all host threads
+    po = oracle.params_default(PTSPHY, p.ncldtop)
+    nb = 64
+    sub = {k: np.ascontiguousarray(v[:nb]) for k, v in sh.items()}
+    best = None
+    for _ in range(3):
+        w = {k: v.copy() for k, v in sub.items()}
+        t0 = time.perf_counter()
+        oracle.satadj_batched(po, w, NPROMA, KLEV, nb, nb * NPROMA, PTSPHY, 0, libm="glibc")
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    return {"columns_per_s": world * NCOL / (ms * 1e-3), "ms": ms,
+            "parity": "bit-identical to the oracle (GPU tests)",
+            "closure_max_rel": {"water": water, "enthalpy": enth},
+            "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / (ms * 1e-3) / 1e9 / peak, "algorithmic_bytes_per_launch": algo,
+                         "kernel": "satadj_kernel"},
+            "cpu_oracle": {"columns_per_s": nb * NPROMA / best, "cores": os.cpu_count() or 1,
+                           "sample": f"{nb} NPROMA blocks of 128, best of 3, OpenMP over blocks"}}
 
 
 def surrogate_form(a, p, d, plude0, ref, dev, world, rank, ms64):
@@ -419,6 +485,8 @@ def run_ours(a):
                           "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
         errs[name] = err
 
+    sat = satadj_form(a, p, host, dev, world, rank, stream)
+
     sur = None
     if not a.no_surrogate:
         d["plude"].copy_(plude0)
@@ -504,6 +572,7 @@ def run_ours(a):
                        "error_vs_fp64": errs["phys32"]},
             "surrogate": sur,
         },
+        "satadj": sat,
         "roofline": roofline,
         "cpu_baseline": {"value": cpu_val, "unit": "columns/s", "cores": ncores, "kind": "port",
                          "sample": f"64 NPROMA blocks of 128 (8,192 columns) of the workload, "

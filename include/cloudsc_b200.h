@@ -264,6 +264,54 @@ int cloudsc_b200_block_noalloc(
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur,
     double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn, void *stream);
 
+/*
+ * CLOUD_SATADJ, the saturation adjustment CALLPAR runs before CLOUDSC
+ * (callpar.F90:1253-1279), FP64, bit-identical to a C restatement of the
+ * reference built with the kernels' libm.
+ *
+ * Per-block drop-in with HOST pointers: the argument list of
+ * ifs-source/arpifs/phys_ec/cloud_satadj.F90:13-26 in the same order (derived
+ * types -> cloudsc_params).  Replaces CALL CLOUD_SATADJ at
+ * callpar.F90:1253-1279.  PL/PI and their tendencies are the liquid and ice
+ * (KLON,KLEV) slices of the cloud arrays.  Not read at the default
+ * configuration, may be NULL: ktype, pmfu, pmfd, pgp2dspp, pextra (the
+ * budget switches and SPP are rejected with CLOUDSC_E_UNSUPPORTED).  Only
+ * components 3 and 4 of PLUDELI are read.  Columns KIDIA..KFDIA of the five
+ * tendencies are written, zero above NCLDTOP.  Returns the number of
+ * negative-condensate warnings (cloud_satadj.F90:828,836) or a CLOUDSC_E_*.
+ */
+int cloudsc_b200_satadj_block(
+    const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
+    const int32_t *ktype, int32_t lddiag, double ptsphy, const double *pap, const double *paph,
+    const double *pt, const double *pq, const double *pa, const double *pl, const double *pi,
+    const double *ptendency_cml_t, const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_l, const double *ptendency_cml_i, const double *phrsw,
+    const double *phrlw, const double *ptendency_vdf_t, const double *ptendency_vdf_q,
+    const double *pmfu, const double *pmfd, const double *pludeli, const double *pvervel,
+    const double *pgp2dspp, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_l, double *ptendency_loc_i,
+    double *pextra, int32_t kfldx);
+
+/*
+ * Batched CLOUD_SATADJ with DEVICE pointers over NGPBLKS blocks stored
+ * (NPROMA, ..., NGPBLKS) like cloudsc_b200_batched; one kernel launch, one
+ * GPU thread per (column, level) point.  Argument order: that of
+ * cloud_satadj.F90:13-26 without the arguments the default configuration does
+ * not read, NPROMA/NGPBLKS/NGPTOT for KIDIA/KFDIA/KLON.  `ncounters` (may be
+ * NULL) receives the warning count (uint32, added to).  Returns without
+ * synchronising.
+ */
+int cloudsc_b200_satadj_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+    double ptsphy, const double *pap, const double *paph, const double *pt, const double *pq,
+    const double *pa, const double *pl, const double *pi, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a, const double *ptendency_cml_l,
+    const double *ptendency_cml_i, const double *phrsw, const double *phrlw,
+    const double *ptendency_vdf_t, const double *ptendency_vdf_q, const double *pludeli,
+    const double *pvervel, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_l, double *ptendency_loc_i,
+    uint32_t *ncounters, void *stream);
+
 /* Bytes of the fixed device array cloudsc_b200_block_noalloc works in. */
 size_t cloudsc_b200_block_noalloc_capacity(void);
 

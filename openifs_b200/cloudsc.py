@@ -62,6 +62,13 @@ def lib():
         L.cloudsc_b200_set_schedule.restype = ctypes.c_int
         L.cloudsc_b200_get_schedule.argtypes = [i32, pi32, pi32, pi32]
         L.cloudsc_b200_get_schedule.restype = ctypes.c_int
+        from .fields import SATADJ_FIELDS
+        ns = len(SATADJ_FIELDS)
+        L.cloudsc_b200_satadj_batched.argtypes = [P, i32, i32, i32, i32, ctypes.c_double] + [vp] * ns + [vp, vp]
+        L.cloudsc_b200_satadj_batched.restype = ctypes.c_int
+        L.cloudsc_b200_satadj_block.argtypes = ([P, i32, i32, i32, i32, vp, i32, ctypes.c_double] + [vp] * 16 +
+                                                [vp, vp, vp, vp, vp] + [vp] * 5 + [vp, i32])
+        L.cloudsc_b200_satadj_block.restype = ctypes.c_int
         L.cloudsc_b200_last_error.restype = ctypes.c_char_p
         L.cloudsc_b200_version.restype = ctypes.c_char_p
         L.cloudsc_b200_params_size.restype = ctypes.c_size_t
@@ -221,3 +228,34 @@ def block_noalloc_capacity():
     L = lib()
     L.cloudsc_b200_block_noalloc_capacity.restype = ctypes.c_size_t
     return int(L.cloudsc_b200_block_noalloc_capacity())
+
+
+def satadj_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, counter=None, stream=None):
+    """CLOUD_SATADJ over every block of ``arrays`` (torch CUDA tensors in the
+    fields.SATADJ_FIELDS layout); outputs written in place, asynchronously on
+    ``stream``."""
+    from .fields import SATADJ_FIELDS
+    ptrs = [_ptr(arrays[n]) for n, *_ in SATADJ_FIELDS]
+    cnt = _ptr(counter) if counter is not None else None
+    st = stream.cuda_stream if stream is not None else None
+    return _check(lib().cloudsc_b200_satadj_batched(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
+                                                    int(ngptot), float(ptsphy), *ptrs, cnt, st))
+
+
+def satadj_block(params, kidia, kfdia, klon, klev, ptsphy, arrays):
+    """Per-block drop-in with host (numpy) arrays of one block, shapes as one
+    block of fields.SATADJ_FIELDS; returns the warning count."""
+    a = arrays
+
+    def h(n):
+        x = a[n]
+        if not (isinstance(x, np.ndarray) and x.flags["C_CONTIGUOUS"] and x.dtype == np.float64):
+            raise ValueError(f"{n}: need a C-contiguous float64 numpy array")
+        return x.ctypes.data
+
+    ins = ["pap", "paph", "pt", "pq", "pa", "pl", "pi", "tendency_cml_t", "tendency_cml_q", "tendency_cml_a",
+           "tendency_cml_l", "tendency_cml_i", "phrsw", "phrlw", "tendency_vdf_t", "tendency_vdf_q"]
+    outs = ["tendency_loc_t", "tendency_loc_q", "tendency_loc_a", "tendency_loc_l", "tendency_loc_i"]
+    return _check(lib().cloudsc_b200_satadj_block(
+        ctypes.byref(params), int(kidia), int(kfdia), int(klon), int(klev), None, 0, float(ptsphy),
+        *[h(n) for n in ins], None, None, h("pludeli"), h("pvervel"), None, *[h(n) for n in outs], None, 0))

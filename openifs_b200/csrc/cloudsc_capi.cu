@@ -7,7 +7,9 @@
 //   cloudsc_b200_batched       device pointers, one persistent launch;
 //   cloudsc_b200_batched_host  host pointers, block chunks pipelined through
 //                              H2D / compute / D2H on three streams;
-//   cloudsc_b200_block         the per-NPROMA-block drop-in with host pointers.
+//   cloudsc_b200_block         the per-NPROMA-block drop-in with host pointers;
+// and the same two forms (device-pointer batched, per-block host) of
+// CLOUD_SATADJ, the saturation adjustment that runs before CLOUDSC.
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdio>
@@ -27,6 +29,7 @@ void variant_bounds(int v, int *maxt, int *minb);
 cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes);
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream);
+cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream);
 }  // namespace cloudsc
 
 using namespace cloudsc;
@@ -885,6 +888,133 @@ int cloudsc_b200_block_noalloc(
   }
   uint32_t nwarn = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
+  return (int)nwarn;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// CLOUD_SATADJ entry points (cloud_satadj.F90:13-26).
+// ---------------------------------------------------------------------------
+namespace {
+
+int satadj_shape_ok(const cloudsc_params *p, double ptsphy) {
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (!params_supported(*p)) return fail(CLOUDSC_E_UNSUPPORTED, "a parameter switch this build lacks is on");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  return CLOUDSC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cloudsc_b200_satadj_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot, double ptsphy,
+    const double *pap, const double *paph, const double *pt, const double *pq, const double *pa,
+    const double *pl, const double *pi, const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_l, const double *ptendency_cml_i,
+    const double *phrsw, const double *phrlw, const double *ptendency_vdf_t,
+    const double *ptendency_vdf_q, const double *pludeli, const double *pvervel,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_l, double *ptendency_loc_i, uint32_t *ncounters, void *stream) {
+  int rc = satadj_shape_ok(p, ptsphy);
+  if (rc) return rc;
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  const void *req[] = {pap, paph, pt, pq, pa, pl, pi, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a,
+                       ptendency_cml_l, ptendency_cml_i, phrsw, phrlw, ptendency_vdf_t, ptendency_vdf_q,
+                       pludeli, pvervel, ptendency_loc_t, ptendency_loc_q, ptendency_loc_a,
+                       ptendency_loc_l, ptendency_loc_i};
+  for (const void *q : req)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  rc = ensure_params(nullptr);
+  if (rc) return rc;
+  SatadjFields f = {pap, paph, pt, pq, pa, pl, pi, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a,
+                    ptendency_cml_l, ptendency_cml_i, phrsw, phrlw, ptendency_vdf_t, ptendency_vdf_q,
+                    pludeli, pvervel, ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_l,
+                    ptendency_loc_i, ncounters};
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
+  cudaError_t e = launch_satadj(f, sh, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+int cloudsc_b200_satadj_block(
+    const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev, const int32_t *ktype,
+    int32_t lddiag, double ptsphy, const double *pap, const double *paph, const double *pt,
+    const double *pq, const double *pa, const double *pl, const double *pi,
+    const double *ptendency_cml_t, const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_l, const double *ptendency_cml_i, const double *phrsw,
+    const double *phrlw, const double *ptendency_vdf_t, const double *ptendency_vdf_q,
+    const double *pmfu, const double *pmfd, const double *pludeli, const double *pvervel,
+    const double *pgp2dspp, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_l, double *ptendency_loc_i, double *pextra,
+    int32_t kfldx) {
+  (void)ktype; (void)lddiag; (void)pmfu; (void)pmfd; (void)pgp2dspp; (void)pextra; (void)kfldx;
+  int rc = satadj_shape_ok(p, ptsphy);
+  if (rc) return rc;
+  if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
+    return fail(CLOUDSC_E_SHAPE, "inconsistent KIDIA/KFDIA/KLON/KLEV");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  // inputs in the order of SatadjFields; PLUDELI is copied for its components
+  // 3 and 4 only (the ones the scheme reads, :407, :411)
+  const double *in[18] = {pap, paph, pt, pq, pa, pl, pi, ptendency_cml_t, ptendency_cml_q,
+                          ptendency_cml_a, ptendency_cml_l, ptendency_cml_i, phrsw, phrlw,
+                          ptendency_vdf_t, ptendency_vdf_q, pludeli, pvervel};
+  double *out[5] = {ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_l, ptendency_loc_i};
+  for (const double *q : in)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  for (double *q : out)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  int dev = 0;
+  rc = ensure_params(&dev);
+  if (rc) return rc;
+  const size_t s2 = (size_t)klon * klev, s2h = (size_t)klon * (klev + 1);
+  auto elems_of = [&](int i) { return i == 1 ? s2h : (i == 16 ? 4 * s2 : s2); };
+  size_t total = 0;
+  for (int i = 0; i < 18; ++i) total += elems_of(i);
+  total += 5 * s2;
+  rc = t_ws.prepare(dev, total * sizeof(double));
+  if (rc) return rc;
+  double *d_in[18], *d_out[5];
+  double *cur = (double *)t_ws.buf;
+  for (int i = 0; i < 18; ++i) {
+    d_in[i] = cur;
+    cur += elems_of(i);
+  }
+  for (int i = 0; i < 5; ++i) {
+    d_out[i] = cur;
+    cur += s2;
+  }
+  cudaStream_t s = t_ws.st[0];
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < 18 && e == cudaSuccess; ++i) {
+    if (i == 16)
+      e = cudaMemcpyAsync(d_in[i] + 2 * s2, in[i] + 2 * s2, 2 * s2 * sizeof(double), cudaMemcpyHostToDevice, s);
+    else
+      e = cudaMemcpyAsync(d_in[i], in[i], elems_of(i) * sizeof(double), cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  SatadjFields f = {d_in[0], d_in[1], d_in[2], d_in[3], d_in[4], d_in[5], d_in[6], d_in[7], d_in[8],
+                    d_in[9], d_in[10], d_in[11], d_in[12], d_in[13], d_in[14], d_in[15], d_in[16], d_in[17],
+                    d_out[0], d_out[1], d_out[2], d_out[3], d_out[4], t_ws.counter};
+  Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
+  e = launch_satadj(f, sh, s);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  // copy back columns KIDIA..KFDIA of every level
+  const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
+  for (int i = 0; i < 5 && e == cudaSuccess; ++i)
+    e = cudaMemcpy2DAsync(out[i] + c0, klon * sizeof(double), d_out[i] + c0, klon * sizeof(double),
+                          ncol * sizeof(double), klev, cudaMemcpyDeviceToHost, s);
+  uint32_t nwarn = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
   return (int)nwarn;

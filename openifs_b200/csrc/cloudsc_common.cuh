@@ -36,6 +36,15 @@ struct Fields {
   uint32_t *ncounters;
 };
 
+// Pointers of the batched CLOUD_SATADJ arrays (same block layout).
+struct SatadjFields {
+  const double *pap, *paph, *pt, *pq, *pa, *pl, *pi;
+  const double *cml_t, *cml_q, *cml_a, *cml_l, *cml_i;
+  const double *phrsw, *phrlw, *vdf_t, *vdf_q, *pludeli, *pvervel;
+  double *loc_t, *loc_q, *loc_a, *loc_l, *loc_i;
+  uint32_t *ncounters;
+};
+
 struct Shape {
   int nproma, klev, ngpblks, ngptot;
   int kidia0;  // first column of every block computed (0-based KIDIA-1)

@@ -46,6 +46,7 @@ __device__ __forceinline__ float xsign(float a, float b) { return copysignf(a, b
 }  // namespace cloudsc
 
 #include "cloudsc_body.cuh"
+#include "satadj_point.cuh"
 
 namespace cloudsc {
 
@@ -89,6 +90,56 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
     else
       cloudsc_column<double, FORM == 1>(F, sh, ib, jl, active);
   }
+}
+
+// CLOUD_SATADJ: one thread per (column, level) point, points numbered
+// (ib * KLEV + jk) * NPROMA + jl -- the element offset of a level field -- so
+// consecutive threads read consecutive columns of one level (coalesced).  A
+// grid-stride loop covers all points of all blocks; levels above NCLDTOP get
+// zero tendencies (cloud_satadj.F90:338-346).
+constexpr int kSatadjThreads = 256;
+__global__ void __launch_bounds__(kSatadjThreads) satadj_kernel(SatadjFields F, Shape sh) {
+  plibm_load_tables();
+  const KParams<double> &k = KP<double>();
+  const double dt = sh.ptsphy;
+  const double zqtmst = 1.0 / dt;
+  const unsigned long long np = sh.nproma, kl = sh.klev;
+  const unsigned long long npts = (unsigned long long)sh.ngpblks * kl * np;
+  const int jktop = k.ncldtop - 1;  // first 0-based level with cloud processes
+  int nwarn = 0;
+  for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
+       idx += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long row = idx / np;
+    const int jl = (int)(idx - row * np);
+    const unsigned long long ib = row / kl;
+    const int jk = (int)(row - ib * kl);
+    const long long icend = (long long)sh.ngptot - (long long)ib * (long long)np;
+    if (jl < sh.kidia0 || jl >= icend) continue;
+    if (jk < jktop) {
+      F.loc_t[idx] = 0.0;
+      F.loc_q[idx] = 0.0;
+      F.loc_a[idx] = 0.0;
+      F.loc_l[idx] = 0.0;
+      F.loc_i[idx] = 0.0;
+      continue;
+    }
+    const size_t oh = (size_t)(ib * (kl + 1) + jk) * np + jl;  // PAPH(jl, jk)
+    const size_t o4 = (size_t)(ib * 4 * kl + jk) * np + jl;     // PLUDELI(jl, jk, 1)
+    const size_t sl = (size_t)kl * np;                          // one PLUDELI component
+    double lt, lq, la, ll, li;
+    satadj_point(k, dt, zqtmst, ld(F.pap + idx), ld(F.paph + oh), ld(F.paph + oh + np),
+                 ld(F.paph + (size_t)(ib * (kl + 1) + kl) * np + jl), ld(F.pt + idx), ld(F.pq + idx),
+                 ld(F.pa + idx), ld(F.pl + idx), ld(F.pi + idx), ld(F.cml_t + idx), ld(F.cml_q + idx),
+                 ld(F.cml_a + idx), ld(F.cml_l + idx), ld(F.cml_i + idx), ld(F.phrsw + idx),
+                 ld(F.phrlw + idx), ld(F.vdf_t + idx), ld(F.vdf_q + idx), ld(F.pludeli + o4 + 2 * sl),
+                 ld(F.pludeli + o4 + 3 * sl), ld(F.pvervel + idx), lt, lq, la, ll, li, nwarn);
+    F.loc_t[idx] = lt;
+    F.loc_q[idx] = lq;
+    F.loc_a[idx] = la;
+    F.loc_l[idx] = ll;
+    F.loc_i[idx] = li;
+  }
+  if (nwarn && F.ncounters) atomic_add(F.ncounters, (uint32_t)nwarn);
 }
 
 }  // namespace cloudsc
@@ -180,5 +231,19 @@ cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int t
   return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, 0, stream);
 }
 
-}  // namespace cloudsc
+// Launch CLOUD_SATADJ over every point of the batched arrays: a grid of
+// 256-thread CTAs, at most 16 per SM, striding over the points.
+cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream) {
+  const unsigned long long npts = (unsigned long long)sh.ngpblks * sh.klev * sh.nproma;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  unsigned long long blocks = (npts + kSatadjThreads - 1) / kSatadjThreads;
+  const unsigned long long cap = (unsigned long long)sms * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  satadj_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
+  return cudaGetLastError();
+}
 
+}  // namespace cloudsc

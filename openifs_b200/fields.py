@@ -111,3 +111,59 @@ def host_copy_bytes(nproma, klev, ngpblks, ngptot=None):
     ngptot = nproma * ngpblks if ngptot is None else ngptot
     read, write = bytes_per_column(klev)
     return read * nproma * ngpblks, write * ngptot
+
+
+# The arrays of the batched CLOUD_SATADJ call (cloudsc_b200_satadj_batched),
+# in its argument order: the argument order of cloud_satadj.F90:13-26 without
+# the arguments the default configuration does not read (KTYPE, LDDIAG, PMFU,
+# PMFD, PGP2DSPP, PEXTRA).  PL/PI and their tendencies are the liquid and ice
+# slices of CALLPAR's STATE_T0%CLD / TENDENCY_CML%CLD (callpar.F90:1253-1279).
+SATADJ_FIELDS = [
+    ("pap", "2d", np.float64, "in"),
+    ("paph", "hl", np.float64, "in"),
+    ("pt", "2d", np.float64, "in"),
+    ("pq", "2d", np.float64, "in"),
+    ("pa", "2d", np.float64, "in"),
+    ("pl", "2d", np.float64, "in"),
+    ("pi", "2d", np.float64, "in"),
+    ("tendency_cml_t", "2d", np.float64, "in"),
+    ("tendency_cml_q", "2d", np.float64, "in"),
+    ("tendency_cml_a", "2d", np.float64, "in"),
+    ("tendency_cml_l", "2d", np.float64, "in"),
+    ("tendency_cml_i", "2d", np.float64, "in"),
+    ("phrsw", "2d", np.float64, "in"),
+    ("phrlw", "2d", np.float64, "in"),
+    ("tendency_vdf_t", "2d", np.float64, "in"),
+    ("tendency_vdf_q", "2d", np.float64, "in"),
+    ("pludeli", "3d4", np.float64, "in"),
+    ("pvervel", "2d", np.float64, "in"),
+    ("tendency_loc_t", "2d", np.float64, "out"),
+    ("tendency_loc_q", "2d", np.float64, "out"),
+    ("tendency_loc_a", "2d", np.float64, "out"),
+    ("tendency_loc_l", "2d", np.float64, "out"),
+    ("tendency_loc_i", "2d", np.float64, "out"),
+]
+SATADJ_INPUTS = [f[0] for f in SATADJ_FIELDS if f[3] == "in"]
+SATADJ_OUTPUTS = [f[0] for f in SATADJ_FIELDS if f[3] == "out"]
+
+
+def satadj_alloc(ngpblks, nproma, klev, alloc_fn=None):
+    """Zero-filled CLOUD_SATADJ arrays in the batched layout."""
+    out = {}
+    for n, kind, dt, _ in SATADJ_FIELDS:
+        shp = (ngpblks,) + block_shape(kind, nproma, klev)
+        out[n] = alloc_fn(shp, dt) if alloc_fn else np.zeros(shp, dt)
+    return out
+
+
+# Algorithmic HBM traffic of one CLOUD_SATADJ column (bytes, default
+# configuration).  Levels NCLDTOP..KLEV read 17 level fields (PT PQ PA PL PI,
+# five CML tendencies, PHRSW PHRLW, the two VDF tendencies, PLUDELI(3:4),
+# PVERVEL) and PAP, plus PAPH on half levels NCLDTOP..KLEV+1; the levels
+# above NCLDTOP read nothing (cloud_satadj.F90:338-345).  All KLEV levels of
+# the 5 tendencies are written.
+def satadj_bytes_per_column(klev=137, ncldtop=15, fp=8):
+    nlev = klev - ncldtop + 1
+    read = (18 * nlev + nlev + 1) * fp
+    write = 5 * klev * fp
+    return read, write

@@ -174,6 +174,56 @@ def _block(rng, nproma, klev, ncldtop, c):
     return out
 
 
+def generate_satadj(ngpblks, nproma, params, klev=KLEV_L137, seed=1, blocks=None):
+    """Inputs (and zeroed outputs) of a batched CLOUD_SATADJ call, in the
+    layout of fields.SATADJ_FIELDS.
+
+    The state (T, q, cloud fraction, liquid, ice), pressures and cumulative
+    tendencies are those of ``generate`` for the same seed; the fields only
+    CLOUD_SATADJ reads come from a second stream per block,
+    ``default_rng([seed, ib, 7])``:
+
+    * PVERVEL (omega) ~ N(0, 0.3 Pa/s);
+    * PHRSW ~ U(0, 2e-5 K/s), PHRLW ~ N(-2e-5, 1e-5 K/s);
+    * PTENDENCY_VDF_T ~ N(0, 1e-4 K/s), PTENDENCY_VDF_Q ~ q N(0, 1e-5 /s);
+    * PLUDELI(3) (detrained vapour) = U(0, 1) PLUDE and PLUDELI(4) (detrained
+      enthalpy, K kg m-2 s-1) = 2500 PLUDE N(0, 1) on the convective levels
+      of ``generate``, zero elsewhere.
+    """
+    base = generate(ngpblks, nproma, params, klev=klev, seed=seed, blocks=blocks)
+    return satadj_from(base, nproma, klev=klev, seed=seed,
+                       blocks=list(range(ngpblks)) if blocks is None else list(blocks))
+
+
+def satadj_from(base, nproma, klev=KLEV_L137, seed=1, blocks=None):
+    """The CLOUD_SATADJ inputs of ``generate_satadj`` built from an existing
+    ``generate`` result ``base`` (same seed; ``blocks`` = the block indices
+    ``base`` holds, default all)."""
+    from .fields import satadj_alloc
+    nb = base["pt"].shape[0]
+    ids = list(range(nb)) if blocks is None else list(blocks)
+    out = satadj_alloc(len(ids), nproma, klev)
+    for n in ("pap", "paph", "pt", "pq", "pa", "tendency_cml_t", "tendency_cml_q", "tendency_cml_a"):
+        out[n][:] = base[n]
+    out["pl"][:] = base["pclv"][:, 0]
+    out["pi"][:] = base["pclv"][:, 1]
+    out["tendency_cml_l"][:] = base["tendency_cml_cld"][:, 0]
+    out["tendency_cml_i"][:] = base["tendency_cml_cld"][:, 1]
+    out["pludeli"][:, :2] = base["pludeli"][:, :2]
+    for j, ib in enumerate(ids):
+        rng = np.random.default_rng([int(seed), int(ib), 7])
+        shp = (klev, nproma)
+        out["pvervel"][j] = rng.normal(0.0, 0.3, shp)
+        out["phrsw"][j] = rng.uniform(0.0, 2e-5, shp)
+        out["phrlw"][j] = rng.normal(-2e-5, 1e-5, shp)
+        out["tendency_vdf_t"][j] = rng.normal(0.0, 1e-4, shp)
+        out["tendency_vdf_q"][j] = base["pq"][j] * rng.normal(0.0, 1e-5, shp)
+        plude = base["plude"][j]
+        out["pludeli"][j, 2] = rng.uniform(0.0, 1.0, shp) * plude
+        out["pludeli"][j, 3] = 2500.0 * plude * rng.normal(0.0, 1.0, shp)
+    return out
+
+
 def constants_from(params):
     keys = ["rtice", "rtwat", "rtwat_rtice_r", "r2es", "r3les", "r3ies", "r4les", "r4ies", "rtt",
             "retv", "rd", "rg"]

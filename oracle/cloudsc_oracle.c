@@ -98,9 +98,9 @@ static inline double fokoop(const cloudsc_params *p, double t) {
   return fmin_(p->rkoop1 - p->rkoop2 * t, foeeliq2ice(p, t));
 }
 
-/* ---------------- cloud_supersatcheck.F90:111-226 (KFTLIQICE=1) ---------------- */
-static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, const double *pt,
-                          const double *pq, const double *pa, const double *pp,
+/* ---------------- cloud_supersatcheck.F90:111-226 ---------------- */
+static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, int kftliqice,
+                          const double *pt, const double *pq, const double *pa, const double *pp,
                           double *pt_adj, double *pq_adj, double *pa_adj, double *pl_adj,
                           double *pi_adj) {
   const double zepsec = 1.E-14;
@@ -135,8 +135,14 @@ static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, const d
     pt_adj[jl - 1] = foeldcpm(p, zt) * zcond;
     pq_adj[jl - 1] = -zcond;
     pa_adj[jl - 1] = zda;
-    pl_adj[jl - 1] = zcond * zfoealfa;
-    pi_adj[jl - 1] = zcond * (1.0 - zfoealfa);
+    if (kftliqice == 1) { /* split by the mixed-phase fraction (:211-214) */
+      pl_adj[jl - 1] = zcond * zfoealfa;
+      pi_adj[jl - 1] = zcond * (1.0 - zfoealfa);
+    } else { /* all liquid down to homogeneous freezing (:215-223) */
+      int liquid = pt[jl - 1] + pt_adj[jl - 1] >= p->rthomo;
+      pl_adj[jl - 1] = liquid ? zcond : 0.0;
+      pi_adj[jl - 1] = liquid ? 0.0 : zcond;
+    }
   }
 }
 
@@ -1066,7 +1072,7 @@ int oracle_cloudsc(
     {
       double zpp[klon];
       for (jl = kidia; jl <= kfdia; jl++) zpp[jl - 1] = A2(pap, jl, jk);
-      supersatcheck(p, kidia, kfdia, zt_upd, zq_upd, za_upd, zpp, zt_adj, zq_adj, za_adj, zl_adj, zi_adj);
+      supersatcheck(p, kidia, kfdia, 1, zt_upd, zq_upd, za_upd, zpp, zt_adj, zq_adj, za_adj, zl_adj, zi_adj);
     }
     for (jl = kidia; jl <= kfdia; jl++) {
       A2(ptendency_loc_q, jl, jk) = A2(ptendency_loc_q, jl, jk) + A1(zq_adj, jl) * zqtmst;
@@ -1199,6 +1205,275 @@ int oracle_cloudsc_batched(
         pfcqlng + ib * s2h, pfsqrf + ib * s2h, pfsqsf + ib * s2h, pfcqrng + ib * s2h,
         pfcqsng + ib * s2h, pfsqltur + ib * s2h, pfsqitur + ib * s2h, pfplsl + ib * s2h,
         pfplsn + ib * s2h, pfhpsl + ib * s2h, pfhpsn + ib * s2h, NULL, 0);
+    if (r < 0) err = r < err ? r : err;
+    else total += r;
+  }
+  return err < 0 ? err : total;
+}
+
+/* =========================================================================
+ * CLOUD_SATADJ (ifs-source/arpifs/phys_ec/cloud_satadj.F90:13-1092), the
+ * saturation adjustment CALLPAR runs before CLOUDSC (callpar.F90:1253-1279),
+ * restated in its default configuration: no SPP perturbations (:313-332), the
+ * budget diagnostics (:845-940) off.  Loop order and the order of every
+ * floating-point operation follow the Fortran.  Quantities the reference
+ * computes but never uses at this configuration (ZQSLIQ, ZCORQSLIQ,
+ * ZEVAPLIMMIX, ZQSLIM, ZQSLIQ_UPD, ZQSICE_UPD, ZQSLIQK_UPD, ZRDTGDP, ZRHO,
+ * ZDZ, ZLICLD) are not formed.
+ * ========================================================================= */
+
+/* QSATMIXADJ (cloud_satadj.F90:948-1017): two Newton steps of the mixed-phase
+ * saturation adjustment; returns the adjusted humidity. */
+static double qsatmixadj(const cloudsc_params *p, double pt, double pq, double pp) {
+  double zt = pt, zq = pq;
+  const double zp_r = 1.0 / pp;
+  for (int ji = 1; ji <= 2; ji++) {
+    double zfoeet = fmin_(foeewm(p, zt) * zp_r, 0.5);
+    double zcor = 1.0 / (1.0 - p->retv * zfoeet);
+    double zqsat = zfoeet * zcor;
+    double zcorqs = 1.0 + zqsat * zcor * foedem(p, zt);
+    double zcond = (zq - zqsat) / zcorqs;
+    zt = zt + foeldcpm(p, zt) * zcond;
+    zq = zq - zcond;
+  }
+  return zq;
+}
+
+int oracle_cloud_satadj(
+    const cloudsc_params *p, int kidia, int kfdia, int klon, int klev, const int32_t *ktype,
+    int lddiag, double ptsphy, const double *pap, const double *paph, const double *pt,
+    const double *pq, const double *pa, const double *pl, const double *pi,
+    const double *ptendency_cml_t, const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_l, const double *ptendency_cml_i, const double *phrsw,
+    const double *phrlw, const double *ptendency_vdf_t, const double *ptendency_vdf_q,
+    const double *pmfu, const double *pmfd, const double *pludeli, const double *pvervel,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_l, double *ptendency_loc_i) {
+  (void)ktype; (void)lddiag; (void)pmfu; (void)pmfd;
+  if (!params_supported(p)) return CLOUDSC_E_UNSUPPORTED;
+  if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia) return CLOUDSC_E_SHAPE;
+  const int ncldtop = p->ncldtop;
+  const double zqtmst = 1.0 / ptsphy; /* :291 */
+  const double zrdcp = p->rd / p->rcpd;
+  const double zepsec = 1.E-14;
+  int nwarn = 0;
+  const size_t nb = (size_t)klon * 19;
+  double *buf = (double *)malloc(nb * sizeof(double));
+  if (!buf) return CLOUDSC_E_CUDA;
+  double *zt = buf, *zq = zt + klon, *za = zq + klon, *zl = za + klon, *zi = zl + klon;
+  double *zdtforce = zi + klon, *zdqforce = zdtforce + klon, *zli = zdqforce + klon;
+  double *zliqfrac = zli + klon, *zicefrac = zliqfrac + klon, *zrhc = zicefrac + klon;
+  double *zqsliqk = zrhc + klon, *zqsmix = zqsliqk + klon, *zqsmix_upd = zqsmix + klon;
+  double *zcorqsmix_upd = zqsmix_upd + klon, *zdqs = zcorqsmix_upd + klon;
+  double *zt_upd = zdqs + klon, *zq_upd = zt_upd + klon, *za_upd = zq_upd + klon;
+  double zt_adj[1], zq_adj[1], za_adj[1], zl_adj[1], zi_adj[1];
+
+  for (int jk = 1; jk <= ncldtop - 1; jk++) /* :338-345 */
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      A2(ptendency_loc_t, jl, jk) = 0.0;
+      A2(ptendency_loc_q, jl, jk) = 0.0;
+      A2(ptendency_loc_a, jl, jk) = 0.0;
+      A2(ptendency_loc_l, jl, jk) = 0.0;
+      A2(ptendency_loc_i, jl, jk) = 0.0;
+    }
+
+  for (int jk = ncldtop; jk <= klev; jk++) {
+    /* updated state (:357-366) */
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      A1(zt, jl) = A2(pt, jl, jk) + ptsphy * A2(ptendency_cml_t, jl, jk);
+      A1(zq, jl) = A2(pq, jl, jk) + ptsphy * A2(ptendency_cml_q, jl, jk);
+      A1(za, jl) = A2(pa, jl, jk) + ptsphy * A2(ptendency_cml_a, jl, jk);
+      A1(zl, jl) = A2(pl, jl, jk) + ptsphy * A2(ptendency_cml_l, jl, jk);
+      A1(zi, jl) = A2(pi, jl, jk) + ptsphy * A2(ptendency_cml_i, jl, jk);
+      A1(za, jl) = fmax_(0.0, fmin_(1.0, A1(za, jl)));
+    }
+    /* T and q forcing of condensation/evaporation (:384-413) */
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      double zdp = A2(paph, jl, jk + 1) - A2(paph, jl, jk);
+      double zgdp = p->rg / zdp;
+      double zdtgdp = ptsphy * zgdp;
+      double zdtdp = zrdcp * A2(pt, jl, jk) / A2(pap, jl, jk);
+      double zdpmxdt = zdp * zqtmst;
+      double zwtot = A2(pvervel, jl, jk);
+      zwtot = fmin_(zdpmxdt, fmax_(-zdpmxdt, zwtot));
+      double zzzdt = A2(phrsw, jl, jk) + A2(phrlw, jl, jk);
+      double zdtdiab = fmin_(zdpmxdt * zdtdp, fmax_(-zdpmxdt * zdtdp, zzzdt)) * ptsphy;
+      A1(zdtforce, jl) = zdtdp * zwtot * ptsphy + zdtdiab + A3(pludeli, jl, jk, 4, klev) * zdtgdp +
+                         A2(ptendency_vdf_t, jl, jk) * ptsphy;
+      A1(zdqforce, jl) = A3(pludeli, jl, jk, 3, klev) * zdtgdp + A2(ptendency_vdf_q, jl, jk) * ptsphy;
+    }
+    /* saturation of the start-of-step and of the updated state (:435-552) */
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      const double t0 = A2(pt, jl, jk), pp = A2(pap, jl, jk);
+      double zp_r = 1.0 / pp;
+      A1(zli, jl) = A1(zl, jl) + A1(zi, jl);
+      if (A1(zli, jl) > p->rlmin) {
+        A1(zliqfrac, jl) = A1(zl, jl) / A1(zli, jl);
+        A1(zicefrac, jl) = 1.0 - A1(zliqfrac, jl);
+      } else {
+        A1(zliqfrac, jl) = 0.0;
+        A1(zicefrac, jl) = 0.0;
+      }
+      A1(zrhc, jl) = p->ramid;
+      double zsigk = pp / A2(paph, jl, klev + 1);
+      if (zsigk > 0.8) {
+        double x = (zsigk - 0.8) / 0.2;
+        A1(zrhc, jl) = p->ramid + (1.0 - p->ramid) * (x * x);
+      }
+      double zfoeeliq = fmin_(foeeliq(p, t0) * zp_r, 0.5);
+      double zfoeeice = fmin_(foeew(p, t0) * zp_r, 0.5);
+      double zfokoop = fmin_(zfoeeice * (p->rkoop1 - p->rkoop2 * t0), zfoeeliq);
+      A1(zqsliqk, jl) = zfokoop / (1.0 - p->retv * zfokoop);
+      double zfoeemix = fmin_(foeewm(p, t0) * zp_r, 0.5);
+      double zcor = 1.0 / (1.0 - p->retv * zfoeemix);
+      A1(zqsmix, jl) = zfoeemix * zcor;
+      A1(zqsliqk, jl) = 0.5 * (A1(zqsliqk, jl) + A1(zqsmix, jl));
+      /* updated state */
+      const double tu = A1(zt, jl);
+      zfoeemix = fmin_(foeewm(p, tu) * zp_r, 0.5);
+      zcor = 1.0 / (1.0 - p->retv * zfoeemix);
+      A1(zqsmix_upd, jl) = zfoeemix * zcor;
+      A1(zcorqsmix_upd, jl) = 1.0 + A1(zqsmix_upd, jl) * zcor * foedem(p, tu);
+    }
+    /* condensation/evaporation from dqsat/dt (:574-593) */
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      double zttmp = A2(pt, jl, jk) + A1(zdtforce, jl);
+      zttmp = fmax_(zttmp, 160.0);
+      double zqtmp = A1(zqsmix, jl) + A1(zdqforce, jl);
+      double zqsatnew = qsatmixadj(p, zttmp, zqtmp, A2(pap, jl, jk));
+      A1(zdqs, jl) = zqsatnew - zqtmp;
+    }
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      const double pa0 = A2(pa, jl, jk), pq0 = A2(pq, jl, jk), t0 = A2(pt, jl, jk);
+      const double dqs = A1(zdqs, jl), qsliqk = A1(zqsliqk, jl);
+      /* clear-air condensation, new cloud (:602-655) */
+      double env_l = 0.0, env_i = 0.0, zacond = 0.0;
+      if (dqs <= -p->rlmin && pa0 < 1.0 - zepsec) {
+        double zqe = (pq0 - pa0 * A1(zqsmix, jl)) / fmax_(zepsec, 1.0 - pa0);
+        zqe = fmax_(0.0, zqe);
+        if (zqe >= A1(zrhc, jl) * qsliqk && zqe < qsliqk) {
+          zacond = -(1.0 - pa0) * dqs / fmax_(2.0 * (qsliqk - zqe), zepsec);
+          zacond = fmin_(zacond, 1.0 - pa0);
+          double zlcond_env = -dqs * 0.5 * zacond;
+          double zzdl = 2.0 * (qsliqk - zqe) / fmax_(zepsec, 1.0 - pa0);
+          if (dqs < -zzdl) {
+            double zlcondlim = (pa0 - 1.0) * dqs - qsliqk + pq0;
+            zlcond_env = fmin_(zlcond_env, zlcondlim);
+          }
+          zlcond_env = fmax_(zlcond_env, 0.0);
+          if (zlcond_env < p->rlmin || (1.0 - pa0) < zepsec) {
+            zlcond_env = 0.0;
+            zacond = 0.0;
+          }
+          if (zlcond_env == 0.0) zacond = 0.0;
+          if (t0 > p->rthomo) env_l = zlcond_env;
+          else env_i = zlcond_env;
+        }
+      }
+      /* condensation in the cloudy part (:662-695) */
+      double cld_l = 0.0, cld_i = 0.0;
+      if (pa0 > zepsec && dqs <= -p->rlmin) {
+        double zlcond_cld = fmax_(-dqs, 0.0);
+        double zcdmax = fmax_((A1(zq, jl) - A1(zqsmix_upd, jl)) / A1(zcorqsmix_upd, jl), 0.0);
+        zlcond_cld = fmin_(zlcond_cld, zcdmax);
+        zlcond_cld = pa0 * zlcond_cld;
+        if (zlcond_cld < p->rlmin) zlcond_cld = 0.0;
+        if (t0 > p->rthomo) cld_l = zlcond_cld;
+        else cld_i = zlcond_cld;
+      }
+      /* evaporation of the cloudy part (:703-723) */
+      double ev_l = 0.0, ev_i = 0.0, zaevap = 0.0;
+      if (dqs > 0.0 && A1(zli, jl) > 0.0) {
+        double zlevap_cld = fmin_(pa0 * dqs, A1(zli, jl));
+        ev_l = A1(zliqfrac, jl) * zlevap_cld;
+        ev_i = A1(zicefrac, jl) * zlevap_cld;
+      }
+      /* state for the supersaturation check (:738-757) */
+      A1(zt_upd, jl) = A1(zt, jl) + p->ralvdcp * (cld_l + env_l - ev_l) + p->ralsdcp * (cld_i + env_i - ev_i);
+      A1(zq_upd, jl) = A1(zq, jl) + (ev_l - cld_l - env_l) + (ev_i - cld_i - env_i);
+      double zanew = A1(za, jl) + zacond - zaevap;
+      zanew = fmin_(zanew, 1.0);
+      if (zanew < p->ramin) zanew = 0.0;
+      A1(za_upd, jl) = zanew;
+      /* supersaturation check (:767-793), IFTLIQICE = 2 */
+      double pp = A2(pap, jl, jk);
+      supersatcheck(p, 1, 1, 2, &A1(zt_upd, jl), &A1(zq_upd, jl), &A1(za_upd, jl), &pp, zt_adj, zq_adj,
+                    za_adj, zl_adj, zi_adj);
+      double supl, supi;
+      if (A1(zt_upd, jl) > p->rthomo) {
+        supl = zl_adj[0] + zi_adj[0];
+        supi = 0.0;
+      } else {
+        supl = 0.0;
+        supi = zl_adj[0] + zi_adj[0];
+      }
+      double zsupsata = za_adj[0];
+      /* tendencies (:801-822) */
+      double tt = p->ralvdcp * (cld_l + env_l + supl - ev_l) * zqtmst +
+                  p->ralsdcp * (cld_i + env_i + supi - ev_i) * zqtmst;
+      double tq = (ev_l - cld_l - env_l - supl + ev_i - cld_i - env_i - supi) * zqtmst;
+      zanew = A1(za, jl) + zacond - zaevap + zsupsata;
+      zanew = fmin_(zanew, 1.0);
+      if (zanew < p->ramin) zanew = 0.0;
+      double ta = (zanew - A1(za, jl)) * zqtmst;
+      double tl = (cld_l + env_l + supl - ev_l) * zqtmst;
+      double ti = (cld_i + env_i + supi - ev_i) * zqtmst;
+      /* negative clean-up (:824-843) */
+      double ladj = A1(zl, jl) + tl * ptsphy;
+      if (ladj < -p->rlmin) nwarn++;
+      if (ladj < 0.0) {
+        tl = tl - ladj;
+        tq = tq + ladj;
+        tt = tt - p->ralvdcp * ladj;
+      }
+      double iadj = A1(zi, jl) + ti * ptsphy;
+      if (iadj < -p->rlmin) nwarn++;
+      if (iadj < 0.0) {
+        ti = ti - iadj;
+        tq = tq + iadj;
+        tt = tt - p->ralsdcp * iadj;
+      }
+      A2(ptendency_loc_t, jl, jk) = tt;
+      A2(ptendency_loc_q, jl, jk) = tq;
+      A2(ptendency_loc_a, jl, jk) = ta;
+      A2(ptendency_loc_l, jl, jk) = tl;
+      A2(ptendency_loc_i, jl, jk) = ti;
+    }
+  }
+  free(buf);
+  return nwarn;
+}
+
+int oracle_cloud_satadj_batched(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot, double ptsphy,
+    const double *pap, const double *paph, const double *pt, const double *pq, const double *pa,
+    const double *pl, const double *pi, const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_l, const double *ptendency_cml_i,
+    const double *phrsw, const double *phrlw, const double *ptendency_vdf_t,
+    const double *ptendency_vdf_q, const double *pludeli, const double *pvervel,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_l, double *ptendency_loc_i, int nthreads) {
+  if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
+      ngptot <= nproma * (ngpblks - 1))
+    return CLOUDSC_E_SHAPE;
+  const size_t s2 = (size_t)nproma * klev, s2h = (size_t)nproma * (klev + 1);
+  int total = 0, err = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) reduction(min : err)
+  for (int ib = 0; ib < ngpblks; ib++) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    const size_t o = ib * s2;
+    int r = oracle_cloud_satadj(
+        p, 1, icend, nproma, klev, NULL, 0, ptsphy, pap + o, paph + ib * s2h, pt + o, pq + o, pa + o,
+        pl + o, pi + o, ptendency_cml_t + o, ptendency_cml_q + o, ptendency_cml_a + o,
+        ptendency_cml_l + o, ptendency_cml_i + o, phrsw + o, phrlw + o, ptendency_vdf_t + o,
+        ptendency_vdf_q + o, NULL, NULL, pludeli + o * 4, pvervel + o, ptendency_loc_t + o,
+        ptendency_loc_q + o, ptendency_loc_a + o, ptendency_loc_l + o, ptendency_loc_i + o);
     if (r < 0) err = r < err ? r : err;
     else total += r;
   }

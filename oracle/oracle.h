@@ -3,8 +3,9 @@
  * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load it.
  *
  * A line-by-line CPU restatement of the reference's double-precision CLOUDSC
- * (ifs-source/arpifs/phys_ec/cloudsc.F90) and its helpers, used as the checker
- * for the B200 kernels.  Parity unpinned: the reference ships no CLOUDSC golden
+ * (ifs-source/arpifs/phys_ec/cloudsc.F90), of CLOUD_SATADJ
+ * (ifs-source/arpifs/phys_ec/cloud_satadj.F90) and of their helpers, used as
+ * the checker for the B200 kernels.  Parity unpinned: the reference ships no CLOUDSC golden
  * vectors and cannot be compiled here (no Fortran compiler in the image).
  */
 #ifndef CLOUDSC_ORACLE_H
@@ -62,6 +63,33 @@ int oracle_cloudsc_batched(
     double *pfcqlng, double *pfsqrf, double *pfsqsf, double *pfcqrng, double *pfcqsng,
     double *pfsqltur, double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
     double *pfhpsn, int nthreads);
+
+/*
+ * CLOUD_SATADJ, one NPROMA block, the argument list of cloud_satadj.F90:13-26
+ * (derived types -> p; PGP2DSPP and the PEXTRA budgets are not used at the
+ * default configuration).  Returns the negative-condensate warning count.
+ */
+int oracle_cloud_satadj(
+    const cloudsc_params *p, int kidia, int kfdia, int klon, int klev, const int32_t *ktype,
+    int lddiag, double ptsphy, const double *pap, const double *paph, const double *pt,
+    const double *pq, const double *pa, const double *pl, const double *pi,
+    const double *ptendency_cml_t, const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_l, const double *ptendency_cml_i, const double *phrsw,
+    const double *phrlw, const double *ptendency_vdf_t, const double *ptendency_vdf_q,
+    const double *pmfu, const double *pmfd, const double *pludeli, const double *pvervel,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_l, double *ptendency_loc_i);
+
+/* CLOUD_SATADJ over NPROMA blocks stored (NPROMA,...,NGPBLKS), OpenMP over blocks. */
+int oracle_cloud_satadj_batched(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot, double ptsphy,
+    const double *pap, const double *paph, const double *pt, const double *pq, const double *pa,
+    const double *pl, const double *pi, const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_l, const double *ptendency_cml_i,
+    const double *phrsw, const double *phrlw, const double *ptendency_vdf_t,
+    const double *ptendency_vdf_q, const double *pludeli, const double *pvervel,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_l, double *ptendency_loc_i, int nthreads);
 
 #ifdef __cplusplus
 }

@@ -1,7 +1,7 @@
 """ORACLE -- TEST INFRASTRUCTURE ONLY.
 
 ctypes wrapper of liboracle_cloudsc.so, the CPU restatement of the reference's
-double-precision CLOUDSC (cloudsc_oracle.c).  Only tests/, the smoke test and
+double-precision CLOUDSC and CLOUD_SATADJ (cloudsc_oracle.c).  Only tests/, the smoke test and
 bench.py's CPU-baseline leg use it, as the checker; the product never calls it.
 Parity unpinned: the reference has no CLOUDSC golden vectors and cannot be
 compiled here (no Fortran compiler).
@@ -45,6 +45,10 @@ def lib(libm="glibc"):
         L.oracle_cloudsc_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
                                              [vp] * len(BATCHED_FIELDS) + [i32])
         L.oracle_cloudsc_batched.restype = i32
+        from openifs_b200.fields import SATADJ_FIELDS
+        L.oracle_cloud_satadj_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
+                                                  [vp] * len(SATADJ_FIELDS) + [i32])
+        L.oracle_cloud_satadj_batched.restype = i32
         _libs[libm] = L
     return _libs[libm]
 
@@ -76,4 +80,21 @@ def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthre
                                       int(ngptot), float(ptsphy), *ptrs, int(nthreads))
     if rc < 0:
         raise RuntimeError(f"oracle_cloudsc_batched returned {rc}")
+    return rc
+
+
+def satadj_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthreads=0, libm="glibc"):
+    """CLOUD_SATADJ over all blocks of ``arrays`` (numpy, fields.SATADJ_FIELDS
+    layout), outputs in place.  Returns the negative-condensate warning count."""
+    from openifs_b200.fields import SATADJ_FIELDS
+    ptrs = []
+    for n, *_ in SATADJ_FIELDS:
+        a = arrays[n]
+        if not (isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"]):
+            raise ValueError(f"{n}: need a C-contiguous numpy array")
+        ptrs.append(a.ctypes.data)
+    rc = lib(libm).oracle_cloud_satadj_batched(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
+                                               int(ngptot), float(ptsphy), *ptrs, int(nthreads))
+    if rc < 0:
+        raise RuntimeError(f"oracle_cloud_satadj_batched returned {rc}")
     return rc

@@ -83,3 +83,41 @@ extern "C" int hostemu_batched(const cloudsc_params *p, int nproma, int klev, in
   }
   return (int)nwarn;
 }
+
+// CLOUD_SATADJ: the kernel's point code (satadj_point.cuh) over every point of
+// the batched arrays, in the order of fields.SATADJ_FIELDS.
+#include "../../openifs_b200/csrc/satadj_point.cuh"
+
+extern "C" int hostemu_satadj_batched(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+                                      double ptsphy, void **a) {
+  Derived d;
+  d.zconst_pow_land = d.zconst_pow_sea = 0.0;
+  d.flt_0p4 = (double)0.4f;
+  d.flt_0p8 = (double)0.8f;
+  fill_kparams(*p, d, c_kpd);
+  const double **in = (const double **)a;
+  double **out = (double **)(a + 18);
+  const KParams<double> &k = c_kpd;
+  const double zqtmst = 1.0 / ptsphy;
+  const size_t np = nproma, kl = klev;
+  int nwarn = 0;
+  for (int ib = 0; ib < ngpblks; ++ib) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    for (int jk = 0; jk < klev; ++jk)
+      for (int jl = 0; jl < icend; ++jl) {
+        const size_t i = (ib * kl + jk) * np + jl;
+        if (jk < k.ncldtop - 1) {
+          for (int m = 0; m < 5; ++m) out[m][i] = 0.0;
+          continue;
+        }
+        const size_t oh = (ib * (kl + 1) + jk) * np + jl, o4 = (ib * 4 * kl + jk) * np + jl;
+        satadj_point(k, ptsphy, zqtmst, in[0][i], in[1][oh], in[1][oh + np], in[1][(ib * (kl + 1) + kl) * np + jl],
+                     in[2][i], in[3][i], in[4][i], in[5][i], in[6][i], in[7][i], in[8][i], in[9][i], in[10][i],
+                     in[11][i], in[12][i], in[13][i], in[14][i], in[15][i], in[16][o4 + 2 * kl * np],
+                     in[16][o4 + 3 * kl * np], in[17][i], out[0][i], out[1][i], out[2][i], out[3][i], out[4][i],
+                     nwarn);
+      }
+  }
+  return nwarn;
+}

@@ -62,3 +62,57 @@ def test_mixed_form_on_host(pp):
     for k in util.MIXED_BOUNDED:
         assert st[k]["normwise_max"] <= util.MIXED_TOL, (k, st[k])
     assert np.isfinite(st["tendency_loc_a"]["normwise_max"])
+
+
+@pytest.mark.parametrize("libm", ["plibm", "glibc"])
+def test_satadj_bit_exact(pp, libm):
+    """CLOUD_SATADJ: the kernel's point code against the oracle, bit for bit,
+    on 64 blocks of 32 columns with a ragged last block."""
+    p, po = pp
+    arrs = inputs.generate_satadj(64, 32, p, seed=11)
+    ngptot = 64 * 32 - 7
+    ref, nw = util.run_oracle_satadj(po, arrs, 32, 64, ngptot, libm=libm)
+    emu, nwe = util.run_hostemu_satadj(p, arrs, 32, 64, ngptot, libm=libm)
+    for n in util.fields.SATADJ_OUTPUTS:
+        assert np.array_equal(emu[n], ref[n]), n
+    assert nw == nwe
+    # the padding columns of the last block are untouched
+    assert np.all(emu["tendency_loc_t"][-1, :, 32 - 7:] == 0.0)
+
+
+SATADJ_CASES = ["clear", "overcast", "cold", "warm", "strong_ascent", "strong_descent", "no_forcing"]
+
+
+def apply_satadj_case(a, case):
+    """Turn a generated CLOUD_SATADJ input into a case its branches single out."""
+    if case == "clear":  # no cloud, no condensate: only clear-air condensation
+        for n in ("pa", "pl", "pi", "tendency_cml_a", "tendency_cml_l", "tendency_cml_i"):
+            a[n][:] = 0.0
+    elif case == "overcast":  # full cloud cover: no clear-air condensation branch
+        a["pa"][:] = 1.0
+        a["tendency_cml_a"][:] = 0.0
+    elif case == "cold":  # below homogeneous freezing: everything goes to ice
+        a["pt"][:] = np.minimum(a["pt"], 225.0)
+    elif case == "warm":
+        a["pt"][:] = np.maximum(a["pt"], 285.0)
+    elif case == "strong_ascent":  # omega beyond the dp/dt clamp: condensation
+        a["pvervel"][:] = -50.0
+    elif case == "strong_descent":  # evaporation
+        a["pvervel"][:] = 50.0
+    elif case == "no_forcing":
+        for n in ("pvervel", "phrsw", "phrlw", "tendency_vdf_t", "tendency_vdf_q"):
+            a[n][:] = 0.0
+        a["pludeli"][:, 2:] = 0.0
+    return a
+
+
+@pytest.mark.parametrize("case", SATADJ_CASES)
+def test_satadj_edge_cases_bit_exact(pp, case):
+    p, po = pp
+    arrs = apply_satadj_case(inputs.generate_satadj(4, 37, p, seed=13), case)
+    ngptot = 4 * 37 - 5
+    ref, nw = util.run_oracle_satadj(po, arrs, 37, 4, ngptot)
+    emu, nwe = util.run_hostemu_satadj(p, arrs, 37, 4, ngptot)
+    for n in util.fields.SATADJ_OUTPUTS:
+        assert np.array_equal(emu[n], ref[n]), (case, n)
+    assert nw == nwe

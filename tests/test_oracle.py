@@ -106,3 +106,26 @@ def test_column_enthalpy_budget_closes(run):
     scale = (np.abs(dp / g * ref["tendency_loc_t"])).sum(axis=1) + np.abs(rhs)
     rel = np.abs(lhs - rhs) / scale
     assert np.median(rel) < 1e-14 and rel.max() < 1e-11, (np.median(rel), rel.max())
+
+
+def test_satadj_conserves_water_and_enthalpy():
+    """CLOUD_SATADJ only moves water between vapour and condensate: at every
+    point dq + dl + di = 0 and dT = (Lv/cp) dl + (Ls/cp) di up to rounding,
+    and levels above NCLDTOP are untouched (cloud_satadj.F90:338-345, 801-843)."""
+    import numpy as np
+    from openifs_b200 import fields, inputs
+    from tests import util
+    p, po = util.params()
+    a = inputs.generate_satadj(16, 32, po, seed=17)
+    out, _ = util.run_oracle_satadj(po, a, 32, 16, 16 * 32, libm="glibc")
+    q, l, i, t = (out[f"tendency_loc_{s}"] for s in "qlit")
+    scale_q = np.abs(q).max()
+    assert scale_q > 0
+    assert np.abs(q + l + i).max() <= 1e-12 * scale_q
+    h = t - po.ralvdcp * l - po.ralsdcp * i
+    assert np.abs(h).max() <= 1e-12 * np.abs(t).max()
+    top = po.ncldtop - 1
+    for n in fields.SATADJ_OUTPUTS:
+        assert np.all(out[n][:, :top] == 0.0), n
+    # condensation, evaporation and cloud-cover changes all occur
+    assert (l > 0).any() and (l < 0).any() and (out["tendency_loc_a"] != 0).any()

@@ -165,3 +165,27 @@ def run_gpu(p, arrs, nproma, ngpblks, ngptot, precision=cloudsc.FP64, device="cu
     torch.cuda.synchronize()
     out = {k: v.cpu().numpy() for k, v in dev.items()}
     return out, int(cnt.item())
+
+
+def run_hostemu_satadj(p, arrs, nproma, ngpblks, ngptot, libm="plibm"):
+    """The SATADJ kernel's point code built for the host (tests/hostemu)."""
+    import ctypes
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hostemu")
+    name = "libcloudsc_hostemu.so" if libm == "plibm" else "libcloudsc_hostemu_glibc.so"
+    path = os.path.join(here, name)
+    import subprocess
+    subprocess.run(["make", "-s", "-C", here], check=True)
+    L = ctypes.CDLL(path)
+    out = {k: v.copy() for k, v in arrs.items()}
+    ptrs = (ctypes.c_void_p * len(fields.SATADJ_FIELDS))(*[out[n].ctypes.data for n, *_ in fields.SATADJ_FIELDS])
+    nw = L.hostemu_satadj_batched(ctypes.byref(p), int(nproma), KLEV, int(ngpblks), int(ngptot),
+                                  ctypes.c_double(PTSPHY), ptrs)
+    return out, nw
+
+
+def run_oracle_satadj(po, arrs, nproma, ngpblks, ngptot, libm="plibm"):
+    from oracle import oracle
+    out = {k: v.copy() for k, v in arrs.items()}
+    nw = oracle.satadj_batched(po, out, nproma, KLEV, ngpblks, ngptot, PTSPHY, libm=libm)
+    return out, nw
