@@ -11,8 +11,9 @@ so it is restored from a pristine copy before every step, outside the timed
 kernel.  ``value`` is FP64 columns/s; the FP32-mixed and FP32-physics forms
 are reported beside it with their errors against the FP64 kernel, the launch
 schedule of each form comes from the autotuner's record (or is tuned in the
-run), CLOUD_SATADJ (the saturation adjustment before CLOUDSC) is timed on the
-same columns with its HBM roofline, and the guarded learned surrogate
+run), CLOUD_SATADJ (the saturation adjustment before CLOUDSC) and SLTEND's
+supersaturation adjustment (after it) are timed on the same columns with
+their HBM rooflines, and the guarded learned surrogate
 (openifs_b200/surrogate.py) over 1,048,576 columns (4 batches of 262,144 in
 one CUDA graph) with its flagged fraction, errors, budget closure and the
 tensor-core throughput of its GEMMs.  ``e2e`` is the same FP64 metric
@@ -261,6 +262,51 @@ def satadj_form(a, p, host, dev, world, rank, stream):
                            "sample": f"{nb} NPROMA blocks of 128, best of 3, OpenMP over blocks"}}
 
 
+def sltend_form(a, p, host, dev, world, rank, stream):
+    """SLTEND's supersaturation adjustment (the CLOUD_SUPERSATCHECK reuse
+    after the cloud scheme) on the same 262,144 columns: device time of the
+    batched kernel (tendencies restored before each step, outside the timed
+    events) and its HBM roofline."""
+    import torch
+    from openifs_b200 import cloudsc, fields, inputs
+    sh = inputs.sltend_from(host, NPROMA, seed=SEED + 1000 * rank)
+    d = {k: torch.from_numpy(v).to(dev) for k, v in sh.items()}
+    keep = {n: d[n].clone() for n in ("ptent", "ptenq", "ptena", "ptencld")}
+
+    def step():
+        for n, v in keep.items():
+            d[n].copy_(v)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloudsc.sltend_supersat_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, stream=stream)
+        e1.record(stream)
+        return e0, e1
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ev = [step() for _ in range(a.steps)]
+    torch.cuda.synchronize(dev)
+    ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    adjusted = float((d["padjl"] != 0).logical_or(d["padji"] != 0).double().mean())
+    rb, wb = fields.sltend_bytes_per_column(KLEV, p.ncldtop)
+    algo = NCOL * (rb + wb)
+    peaks = _peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    del d, keep
+    torch.cuda.empty_cache()
+    return {"columns_per_s": world * NCOL / (ms * 1e-3), "ms": ms,
+            "parity": "bit-identical to the oracle (GPU tests)", "points_adjusted": adjusted,
+            "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / (ms * 1e-3) / 1e9 / peak, "algorithmic_bytes_per_launch": algo,
+                         "kernel": "sltend_supersat_kernel"}}
+
+
 def surrogate_form(a, p, d, plude0, ref, dev, world, rank, ms64):
     """Guarded surrogate (config: 1,048,576 columns as 4 batches of 262,144,
     one CUDA graph per pass): columns/s, speed-up over the FP64 kernel,
@@ -486,6 +532,7 @@ def run_ours(a):
         errs[name] = err
 
     sat = satadj_form(a, p, host, dev, world, rank, stream)
+    slt = sltend_form(a, p, host, dev, world, rank, stream)
 
     sur = None
     if not a.no_surrogate:
@@ -573,6 +620,7 @@ def run_ours(a):
             "surrogate": sur,
         },
         "satadj": sat,
+        "sltend_supersat": slt,
         "roofline": roofline,
         "cpu_baseline": {"value": cpu_val, "unit": "columns/s", "cores": ncores, "kind": "port",
                          "sample": f"64 NPROMA blocks of 128 (8,192 columns) of the workload, "

@@ -312,6 +312,27 @@ int cloudsc_b200_satadj_batched(
     double *ptendency_loc_a, double *ptendency_loc_l, double *ptendency_loc_i,
     uint32_t *ncounters, void *stream);
 
+/*
+ * The supersaturation adjustment of SLTEND (sltend.F90:380-410), the second
+ * caller of CLOUD_SUPERSATCHECK (cloud_supersatcheck.F90:9-231, KFTLIQICE =
+ * 1), batched with DEVICE pointers over (NPROMA, ..., NGPBLKS) blocks, one GPU
+ * thread per point; FP64, bit-identical to the oracle's restatement.  On
+ * levels NCLDTOP..KLEV the state PT + TSPHY*(PCENT+PTENT) (and the same for
+ * q and cloud fraction) is checked and the adjustments are added to PTENT,
+ * PTENQ, PTENA and the liquid and ice species of PTENCLD (KLON,KLEV,NCLV)
+ * (INOUT); padja/padjl/padji (may be NULL) receive the cloud-fraction, liquid
+ * and ice adjustment rates (SLTEND's ZADJA/ZADJL/ZADJI).  prs1 (half-level
+ * pressure) is accepted for the reference's argument list; its surface value
+ * feeds only a quantity CLOUD_SUPERSATCHECK never uses.  Returns without
+ * synchronising.
+ */
+int cloudsc_b200_sltend_supersat_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+    double tsphy, const double *pt, const double *pq, const double *pa, const double *prsf1,
+    const double *prs1, const double *pcent, const double *pcenq, const double *pcena,
+    double *ptent, double *ptenq, double *ptena, double *ptencld, double *padja, double *padjl,
+    double *padji, void *stream);
+
 /* Bytes of the fixed device array cloudsc_b200_block_noalloc works in. */
 size_t cloudsc_b200_block_noalloc_capacity(void);
 

@@ -69,6 +69,10 @@ def lib():
         L.cloudsc_b200_satadj_block.argtypes = ([P, i32, i32, i32, i32, vp, i32, ctypes.c_double] + [vp] * 16 +
                                                 [vp, vp, vp, vp, vp] + [vp] * 5 + [vp, i32])
         L.cloudsc_b200_satadj_block.restype = ctypes.c_int
+        from .fields import SLTEND_FIELDS
+        L.cloudsc_b200_sltend_supersat_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
+                                                           [vp] * len(SLTEND_FIELDS) + [vp])
+        L.cloudsc_b200_sltend_supersat_batched.restype = ctypes.c_int
         L.cloudsc_b200_last_error.restype = ctypes.c_char_p
         L.cloudsc_b200_version.restype = ctypes.c_char_p
         L.cloudsc_b200_params_size.restype = ctypes.c_size_t
@@ -259,3 +263,16 @@ def satadj_block(params, kidia, kfdia, klon, klev, ptsphy, arrays):
     return _check(lib().cloudsc_b200_satadj_block(
         ctypes.byref(params), int(kidia), int(kfdia), int(klon), int(klev), None, 0, float(ptsphy),
         *[h(n) for n in ins], None, None, h("pludeli"), h("pvervel"), None, *[h(n) for n in outs], None, 0))
+
+
+def sltend_supersat_batched(params, arrays, nproma, klev, ngpblks, ngptot, tsphy, stream=None, diagnostics=True):
+    """SLTEND's supersaturation adjustment over every block of ``arrays``
+    (torch CUDA tensors, fields.SLTEND_FIELDS layout); the tendencies are
+    updated in place, the rates written when ``diagnostics``."""
+    from .fields import SLTEND_FIELDS
+    ptrs = []
+    for n, *_ in SLTEND_FIELDS:
+        ptrs.append(_ptr(arrays[n]) if (diagnostics or not n.startswith("padj")) else None)
+    st = stream.cuda_stream if stream is not None else None
+    return _check(lib().cloudsc_b200_sltend_supersat_batched(ctypes.byref(params), int(nproma), int(klev),
+                                                             int(ngpblks), int(ngptot), float(tsphy), *ptrs, st))

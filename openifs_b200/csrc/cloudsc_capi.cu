@@ -30,6 +30,7 @@ cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream);
 cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream);
+cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaStream_t stream);
 }  // namespace cloudsc
 
 using namespace cloudsc;
@@ -1018,6 +1019,38 @@ int cloudsc_b200_satadj_block(
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
   return (int)nwarn;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// SLTEND's supersaturation adjustment (sltend.F90:380-410), the reuse of
+// CLOUD_SUPERSATCHECK after the cloud scheme.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int cloudsc_b200_sltend_supersat_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot, double tsphy,
+    const double *pt, const double *pq, const double *pa, const double *prsf1, const double *prs1,
+    const double *pcent, const double *pcenq, const double *pcena, double *ptent, double *ptenq,
+    double *ptena, double *ptencld, double *padja, double *padjl, double *padji, void *stream) {
+  int rc = satadj_shape_ok(p, tsphy);
+  if (rc) return rc;
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  const void *req[] = {pt, pq, pa, prsf1, prs1, pcent, pcenq, pcena, ptent, ptenq, ptena, ptencld};
+  for (const void *q : req)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  rc = ensure_params(nullptr);
+  if (rc) return rc;
+  SltendFields f = {pt, pq, pa, prsf1, prs1, pcent, pcenq, pcena, ptent, ptenq, ptena, ptencld,
+                    padja, padjl, padji};
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, tsphy};
+  cudaError_t e = launch_sltend_supersat(f, sh, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
 }
 
 }  // extern "C"

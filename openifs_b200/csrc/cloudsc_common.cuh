@@ -45,6 +45,13 @@ struct SatadjFields {
   uint32_t *ncounters;
 };
 
+// Pointers of the batched arrays of SLTEND's supersaturation adjustment
+// (same block layout; ptencld has NCLV species per block).
+struct SltendFields {
+  const double *pt, *pq, *pa, *prsf1, *prs1, *pcent, *pcenq, *pcena;
+  double *ptent, *ptenq, *ptena, *ptencld, *padja, *padjl, *padji;
+};
+
 struct Shape {
   int nproma, klev, ngpblks, ngptot;
   int kidia0;  // first column of every block computed (0-based KIDIA-1)

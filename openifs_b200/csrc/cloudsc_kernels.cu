@@ -145,6 +145,45 @@ __global__ void __launch_bounds__(kSatadjThreads, 4) satadj_kernel(SatadjFields 
   if (nwarn && F.ncounters) atomic_add(F.ncounters, (uint32_t)nwarn);
 }
 
+// SLTEND's supersaturation adjustment (sltend.F90:380-410): one thread per
+// (column, level) point on levels NCLDTOP..KLEV, numbered like satadj_kernel;
+// the tendencies are updated in place and the diagnostics written where
+// their pointers are not NULL.
+__global__ void __launch_bounds__(kSatadjThreads, 4) sltend_supersat_kernel(SltendFields F, Shape sh) {
+  plibm_load_tables();
+  const KParams<double> &k = KP<double>();
+  const double tsphy = sh.ptsphy;
+  const double zrtsphy = 1.0 / tsphy;
+  const unsigned long long np = sh.nproma, kl = sh.klev;
+  const unsigned long long npts = (unsigned long long)sh.ngpblks * kl * np;
+  const int jktop = k.ncldtop - 1;
+  for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
+       idx += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long row = idx / np;
+    const int jl = (int)(idx - row * np);
+    const unsigned long long ib = row / kl;
+    const int jk = (int)(row - ib * kl);
+    const long long icend = (long long)sh.ngptot - (long long)ib * (long long)np;
+    if (jl < sh.kidia0 || jl >= icend || jk < jktop) continue;
+    const size_t oc = (size_t)(ib * 5 * kl + jk) * np + jl;  // PTENCLD(jl, jk, NCLDQL)
+    const size_t sl = (size_t)kl * np;
+    const double tent = F.ptent[idx], tenq = F.ptenq[idx], tena = F.ptena[idx];
+    const double zt = ld(F.pt + idx) + tsphy * (ld(F.pcent + idx) + tent);
+    const double zq = ld(F.pq + idx) + tsphy * (ld(F.pcenq + idx) + tenq);
+    const double za = ld(F.pa + idx) + tsphy * (ld(F.pcena + idx) + tena);
+    double ta, qa, aa, la, ia;
+    supersatcheck_kft1(k, zt, zq, za, ld(F.prsf1 + idx), ta, qa, aa, la, ia);
+    F.ptent[idx] = tent + ta * zrtsphy;
+    F.ptenq[idx] = tenq + qa * zrtsphy;
+    F.ptena[idx] = tena + aa * zrtsphy;
+    F.ptencld[oc] = F.ptencld[oc] + la * zrtsphy;
+    F.ptencld[oc + sl] = F.ptencld[oc + sl] + ia * zrtsphy;
+    if (F.padja) F.padja[idx] = aa * zrtsphy;
+    if (F.padjl) F.padjl[idx] = la * zrtsphy;
+    if (F.padji) F.padji[idx] = ia * zrtsphy;
+  }
+}
+
 }  // namespace cloudsc
 
 // ---------------------------------------------------------------------------
@@ -246,6 +285,19 @@ cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t s
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   satadj_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaStream_t stream) {
+  const unsigned long long npts = (unsigned long long)sh.ngpblks * sh.klev * sh.nproma;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  unsigned long long blocks = (npts + kSatadjThreads - 1) / kSatadjThreads;
+  const unsigned long long cap = (unsigned long long)sms * 64;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  sltend_supersat_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
   return cudaGetLastError();
 }
 

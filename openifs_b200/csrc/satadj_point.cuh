@@ -101,6 +101,42 @@ CSC_DEV void supersat_cond(const KParams<double> &k, double pt, double pq, doubl
   da = zda;
 }
 
+// CLOUD_SUPERSATCHECK with KFTLIQICE = 1 (cloud_supersatcheck.F90:111-223):
+// all five adjustments, liquid and ice split by the mixed-phase fraction.
+CSC_DEV void supersatcheck_kft1(const KParams<double> &k, double pt, double pq, double pa, double pp,
+                                double &t_adj, double &q_adj, double &a_adj, double &l_adj, double &i_adj) {
+  const double zepsec = 1.E-14;
+  double zda = 0.0;
+  const double zt = mx(pt, 160.0);
+  const double za = mx(mn(pa, 1.0), 0.0);
+  const double zp_r = 1.0 / pp;
+  const Sat s = sat_at(k, zt);
+  const double zfoeeliq = mn((k.r2es * s.el) * zp_r, 0.5);
+  const double foeew = s.delta ? k.r2es * s.el : k.r2es * s.ei;
+  const double zfoeeice = mn(foeew * zp_r, 0.5);
+  const double zfokoop = mn(zfoeeice * (k.rkoop1 - k.rkoop2 * zt), zfoeeliq);
+  double zqsliqk = zfokoop / (1.0 - k.retv * zfokoop);
+  const double zfoeemix = mn(sat_foeewm(k, s) * zp_r, 0.5);
+  const double zcor = 1.0 / (1.0 - k.retv * zfoeemix);
+  const double zqsmix = zfoeemix * zcor;
+  const double zcorqsmix = 1.0 + zqsmix * zcor * sat_foedem(k, s, zt);
+  zqsliqk = 0.5 * (zqsliqk + zqsmix);
+  double zqslim = za * zqsmix + (1.0 - za) * zqsliqk;
+  double zcond = mx(pq - zqslim, 0.0);
+  if (zcond > zepsec) {
+    const double zfaci = s.alfa + (1.0 - s.alfa) * k.rssicefactor;
+    zda = (1.0 - za) * zfaci;
+    const double za_upd = za + zda;
+    zqslim = za_upd * zqsmix + (1.0 - za_upd) * zqsliqk;
+    zcond = (pq - zqslim) / zcorqsmix;
+  }
+  t_adj = sat_foeldcpm(k, s) * zcond;
+  q_adj = -zcond;
+  a_adj = zda;
+  l_adj = zcond * s.alfa;
+  i_adj = zcond * (1.0 - s.alfa);
+}
+
 // The five CLOUD_SATADJ tendencies of one point at level jk >= NCLDTOP
 // (arguments are that point's inputs; psurf = PAPH(KLEV+1)).  nwarn is
 // incremented for each negative-condensate warning the reference prints

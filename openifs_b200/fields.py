@@ -167,3 +167,42 @@ def satadj_bytes_per_column(klev=137, ncldtop=15, fp=8):
     read = (18 * nlev + nlev + 1) * fp
     write = 5 * klev * fp
     return read, write
+
+
+# The arrays of the batched SLTEND supersaturation adjustment
+# (cloudsc_b200_sltend_supersat_batched), in its argument order.  "inout"
+# tendencies are updated in place.
+SLTEND_FIELDS = [
+    ("pt", "2d", np.float64, "in"),
+    ("pq", "2d", np.float64, "in"),
+    ("pa", "2d", np.float64, "in"),
+    ("prsf1", "2d", np.float64, "in"),
+    ("prs1", "hl", np.float64, "in"),
+    ("pcent", "2d", np.float64, "in"),
+    ("pcenq", "2d", np.float64, "in"),
+    ("pcena", "2d", np.float64, "in"),
+    ("ptent", "2d", np.float64, "inout"),
+    ("ptenq", "2d", np.float64, "inout"),
+    ("ptena", "2d", np.float64, "inout"),
+    ("ptencld", "3d5", np.float64, "inout"),
+    ("padja", "2d", np.float64, "out"),
+    ("padjl", "2d", np.float64, "out"),
+    ("padji", "2d", np.float64, "out"),
+]
+SLTEND_OUTPUTS = [f[0] for f in SLTEND_FIELDS if f[3] in ("out", "inout")]
+
+
+def sltend_alloc(ngpblks, nproma, klev, alloc_fn=None):
+    out = {}
+    for n, kind, dt, _ in SLTEND_FIELDS:
+        shp = (ngpblks,) + block_shape(kind, nproma, klev)
+        out[n] = alloc_fn(shp, dt) if alloc_fn else np.zeros(shp, dt)
+    return out
+
+
+# Algorithmic HBM traffic of one column of the SLTEND adjustment (bytes):
+# levels NCLDTOP..KLEV read 12 level fields (PT PQ PA PRSF1, three PCEN, three
+# PTEN, PTENCLD liquid and ice) and write 8 (five tendencies, three rates).
+def sltend_bytes_per_column(klev=137, ncldtop=15, fp=8):
+    nlev = klev - ncldtop + 1
+    return 12 * nlev * fp, 8 * nlev * fp

@@ -224,6 +224,44 @@ def satadj_from(base, nproma, klev=KLEV_L137, seed=1, blocks=None):
     return out
 
 
+def generate_sltend(ngpblks, nproma, params, klev=KLEV_L137, seed=1, blocks=None):
+    """Inputs of SLTEND's supersaturation adjustment in the layout of
+    fields.SLTEND_FIELDS: the state, pressures and cumulative tendencies
+    (PCENT/Q/A = the CML tendencies) of ``generate`` for the same seed, and
+    new physics tendencies from ``default_rng([seed, ib, 11])``: PTENT ~ N(0,
+    1e-4 K/s), PTENQ ~ q N(0, 2e-5 /s), PTENA ~ N(0, 1e-5 /s), PTENCLD ~ the
+    species' amount times N(0, 1e-5 /s)."""
+    base = generate(ngpblks, nproma, params, klev=klev, seed=seed, blocks=blocks)
+    return sltend_from(base, nproma, klev=klev, seed=seed,
+                       blocks=list(range(ngpblks)) if blocks is None else list(blocks))
+
+
+def sltend_from(base, nproma, klev=KLEV_L137, seed=1, blocks=None):
+    """The inputs of ``generate_sltend`` built from an existing ``generate``
+    result ``base`` (same seed; ``blocks`` = the block indices it holds)."""
+    from .fields import sltend_alloc
+    nb = base["pt"].shape[0]
+    ids = list(range(nb)) if blocks is None else list(blocks)
+    out = sltend_alloc(len(ids), nproma, klev)
+    out["pt"][:] = base["pt"]
+    out["pq"][:] = base["pq"]
+    out["pa"][:] = base["pa"]
+    out["prsf1"][:] = base["pap"]
+    out["prs1"][:] = base["paph"]
+    out["pcent"][:] = base["tendency_cml_t"]
+    out["pcenq"][:] = base["tendency_cml_q"]
+    out["pcena"][:] = base["tendency_cml_a"]
+    for j, ib in enumerate(ids):
+        rng = np.random.default_rng([int(seed), int(ib), 11])
+        shp = (klev, nproma)
+        out["ptent"][j] = rng.normal(0.0, 1e-4, shp)
+        out["ptenq"][j] = base["pq"][j] * rng.normal(0.0, 2e-5, shp)
+        out["ptena"][j] = rng.normal(0.0, 1e-5, shp)
+        for m in range(4):
+            out["ptencld"][j, m] = base["pclv"][j, m] * rng.normal(0.0, 1e-5, shp)
+    return out
+
+
 def constants_from(params):
     keys = ["rtice", "rtwat", "rtwat_rtice_r", "r2es", "r3les", "r3ies", "r4les", "r4ies", "rtt",
             "retv", "rd", "rg"]

@@ -1479,3 +1479,80 @@ int oracle_cloud_satadj_batched(
   }
   return err < 0 ? err : total;
 }
+
+/* =========================================================================
+ * The supersaturation adjustment of SLTEND (ifs-source/arpifs/phys_ec/
+ * sltend.F90:380-410): the state updated by the cumulative and the new
+ * physics tendencies is checked with CLOUD_SUPERSATCHECK (KFTLIQICE = 1) on
+ * levels NCLDTOP..KLEV and the adjustments are added to the tendencies.
+ * PTENCLD is (KLON,KLEV,NCLV); its liquid and ice species are updated.  The
+ * diagnostics ZADJA/ZADJL/ZADJI (:406-408) go to padja/padjl/padji (may be
+ * NULL).  Levels above NCLDTOP are not touched.  SLTEND passes the section
+ * PRSF1(KIDIA:KFDIA,JK) to the KLON-sized dummy PP of CLOUD_SUPERSATCHECK,
+ * which then reads PP(JL) for JL = KIDIA..KFDIA; with KIDIA = 1 (the whole
+ * block, as EC_PHYS_DRV calls it) that is PRSF1(JL,JK), which is what this
+ * restatement reads for any KIDIA.
+ * ========================================================================= */
+int oracle_sltend_supersat(
+    const cloudsc_params *p, int kidia, int kfdia, int klon, int klev, double tsphy, const double *pt,
+    const double *pq, const double *pa, const double *prsf1, const double *prs1, const double *pcent,
+    const double *pcenq, const double *pcena, double *ptent, double *ptenq, double *ptena, double *ptencld,
+    double *padja, double *padjl, double *padji) {
+  if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia) return CLOUDSC_E_SHAPE;
+  const double zrtsphy = 1.0 / tsphy; /* :271 */
+  double *buf = (double *)malloc((size_t)klon * 9 * sizeof(double));
+  if (!buf) return CLOUDSC_E_CUDA;
+  double *zt = buf, *zq = zt + klon, *za = zq + klon, *ta = za + klon, *qa = ta + klon, *aa = qa + klon;
+  double *la = aa + klon, *ia = la + klon, *pp = ia + klon;
+  for (int jk = p->ncldtop; jk <= klev; jk++) {
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      A1(zt, jl) = A2(pt, jl, jk) + tsphy * (A2(pcent, jl, jk) + A2(ptent, jl, jk));
+      A1(zq, jl) = A2(pq, jl, jk) + tsphy * (A2(pcenq, jl, jk) + A2(ptenq, jl, jk));
+      A1(za, jl) = A2(pa, jl, jk) + tsphy * (A2(pcena, jl, jk) + A2(ptena, jl, jk));
+      A1(pp, jl) = A2(prsf1, jl, jk);
+    }
+    supersatcheck(p, kidia, kfdia, 1, zt, zq, za, pp, ta, qa, aa, la, ia);
+    for (int jl = kidia; jl <= kfdia; jl++) {
+      A2(ptent, jl, jk) = A2(ptent, jl, jk) + A1(ta, jl) * zrtsphy;
+      A2(ptenq, jl, jk) = A2(ptenq, jl, jk) + A1(qa, jl) * zrtsphy;
+      A2(ptena, jl, jk) = A2(ptena, jl, jk) + A1(aa, jl) * zrtsphy;
+      A3(ptencld, jl, jk, NCLDQL, klev) = A3(ptencld, jl, jk, NCLDQL, klev) + A1(la, jl) * zrtsphy;
+      A3(ptencld, jl, jk, NCLDQI, klev) = A3(ptencld, jl, jk, NCLDQI, klev) + A1(ia, jl) * zrtsphy;
+      if (padja) A2(padja, jl, jk) = A1(aa, jl) * zrtsphy;
+      if (padjl) A2(padjl, jl, jk) = A1(la, jl) * zrtsphy;
+      if (padji) A2(padji, jl, jk) = A1(ia, jl) * zrtsphy;
+    }
+  }
+  (void)prs1; /* PSURF feeds only ZRHC, which CLOUD_SUPERSATCHECK never uses */
+  free(buf);
+  return 0;
+}
+
+int oracle_sltend_supersat_batched(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot, double tsphy, const double *pt,
+    const double *pq, const double *pa, const double *prsf1, const double *prs1, const double *pcent,
+    const double *pcenq, const double *pcena, double *ptent, double *ptenq, double *ptena, double *ptencld,
+    double *padja, double *padjl, double *padji, int nthreads) {
+  if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
+      ngptot <= nproma * (ngpblks - 1))
+    return CLOUDSC_E_SHAPE;
+  const size_t s2 = (size_t)nproma * klev, s2h = (size_t)nproma * (klev + 1);
+  int err = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1) reduction(min : err)
+  for (int ib = 0; ib < ngpblks; ib++) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    const size_t o = ib * s2;
+    int r = oracle_sltend_supersat(p, 1, icend, nproma, klev, tsphy, pt + o, pq + o, pa + o, prsf1 + o,
+                                   prs1 + ib * s2h, pcent + o, pcenq + o, pcena + o, ptent + o, ptenq + o,
+                                   ptena + o, ptencld + o * NCLV, padja ? padja + o : NULL,
+                                   padjl ? padjl + o : NULL, padji ? padji + o : NULL);
+    if (r < 0) err = r < err ? r : err;
+  }
+  return err;
+}

@@ -91,6 +91,19 @@ int oracle_cloud_satadj_batched(
     double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
     double *ptendency_loc_l, double *ptendency_loc_i, int nthreads);
 
+/* The supersaturation adjustment of SLTEND (sltend.F90:380-410), one block
+ * and batched over (NPROMA,...,NGPBLKS) blocks. */
+int oracle_sltend_supersat(
+    const cloudsc_params *p, int kidia, int kfdia, int klon, int klev, double tsphy, const double *pt,
+    const double *pq, const double *pa, const double *prsf1, const double *prs1, const double *pcent,
+    const double *pcenq, const double *pcena, double *ptent, double *ptenq, double *ptena, double *ptencld,
+    double *padja, double *padjl, double *padji);
+int oracle_sltend_supersat_batched(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot, double tsphy, const double *pt,
+    const double *pq, const double *pa, const double *prsf1, const double *prs1, const double *pcent,
+    const double *pcenq, const double *pcena, double *ptent, double *ptenq, double *ptena, double *ptencld,
+    double *padja, double *padjl, double *padji, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,10 @@ def lib(libm="glibc"):
         L.oracle_cloud_satadj_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
                                                   [vp] * len(SATADJ_FIELDS) + [i32])
         L.oracle_cloud_satadj_batched.restype = i32
+        from openifs_b200.fields import SLTEND_FIELDS
+        L.oracle_sltend_supersat_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
+                                                     [vp] * len(SLTEND_FIELDS) + [i32])
+        L.oracle_sltend_supersat_batched.restype = i32
         _libs[libm] = L
     return _libs[libm]
 
@@ -97,4 +101,21 @@ def satadj_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, nthrea
                                                int(ngptot), float(ptsphy), *ptrs, int(nthreads))
     if rc < 0:
         raise RuntimeError(f"oracle_cloud_satadj_batched returned {rc}")
+    return rc
+
+
+def sltend_supersat_batched(params, arrays, nproma, klev, ngpblks, ngptot, tsphy, nthreads=0, libm="glibc"):
+    """SLTEND's supersaturation adjustment over all blocks (numpy,
+    fields.SLTEND_FIELDS layout), in place."""
+    from openifs_b200.fields import SLTEND_FIELDS
+    ptrs = []
+    for n, *_ in SLTEND_FIELDS:
+        a = arrays[n]
+        if not (isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"]):
+            raise ValueError(f"{n}: need a C-contiguous numpy array")
+        ptrs.append(a.ctypes.data)
+    rc = lib(libm).oracle_sltend_supersat_batched(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
+                                                  int(ngptot), float(tsphy), *ptrs, int(nthreads))
+    if rc < 0:
+        raise RuntimeError(f"oracle_sltend_supersat_batched returned {rc}")
     return rc

@@ -121,3 +121,42 @@ extern "C" int hostemu_satadj_batched(const cloudsc_params *p, int nproma, int k
   }
   return nwarn;
 }
+
+// SLTEND's supersaturation adjustment: the kernel's point code over every
+// point, arrays in the order of fields.SLTEND_FIELDS.
+extern "C" int hostemu_sltend_batched(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+                                      double tsphy, void **a) {
+  Derived d;
+  d.zconst_pow_land = d.zconst_pow_sea = 0.0;
+  d.flt_0p4 = (double)0.4f;
+  d.flt_0p8 = (double)0.8f;
+  fill_kparams(*p, d, c_kpd);
+  const KParams<double> &k = c_kpd;
+  const double **in = (const double **)a;
+  double *ptent = (double *)a[8], *ptenq = (double *)a[9], *ptena = (double *)a[10], *ptencld = (double *)a[11];
+  double *padja = (double *)a[12], *padjl = (double *)a[13], *padji = (double *)a[14];
+  const double zrtsphy = 1.0 / tsphy;
+  const size_t np = nproma, kl = klev;
+  for (int ib = 0; ib < ngpblks; ++ib) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    for (int jk = k.ncldtop - 1; jk < klev; ++jk)
+      for (int jl = 0; jl < icend; ++jl) {
+        const size_t i = (ib * kl + jk) * np + jl, oc = (ib * 5 * kl + jk) * np + jl;
+        const double zt = in[0][i] + tsphy * (in[5][i] + ptent[i]);
+        const double zq = in[1][i] + tsphy * (in[6][i] + ptenq[i]);
+        const double za = in[2][i] + tsphy * (in[7][i] + ptena[i]);
+        double ta, qa, aa, la, ia;
+        supersatcheck_kft1(k, zt, zq, za, in[3][i], ta, qa, aa, la, ia);
+        ptent[i] = ptent[i] + ta * zrtsphy;
+        ptenq[i] = ptenq[i] + qa * zrtsphy;
+        ptena[i] = ptena[i] + aa * zrtsphy;
+        ptencld[oc] = ptencld[oc] + la * zrtsphy;
+        ptencld[oc + kl * np] = ptencld[oc + kl * np] + ia * zrtsphy;
+        padja[i] = aa * zrtsphy;
+        padjl[i] = la * zrtsphy;
+        padji[i] = ia * zrtsphy;
+      }
+  }
+  return 0;
+}

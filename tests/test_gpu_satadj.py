@@ -72,3 +72,25 @@ def test_block_entry(cuda):
     for n in fields.SATADJ_OUTPUTS:
         assert np.array_equal(blk[n][:, cols], ref[n][0][:, cols]), n
         assert np.all(blk[n][:, :kidia - 1] == 7.0) and np.all(blk[n][:, kfdia:] == 7.0), n
+
+
+@pytest.mark.parametrize("nproma,nblk,cut", [(32, 40, 0), (128, 6, 17)])
+def test_sltend_supersat_bit_exact(cuda, nproma, nblk, cut):
+    """SLTEND's supersaturation adjustment on the GPU against the oracle;
+    with the diagnostics off the tendencies are the same."""
+    import torch
+    p, po = util.params()
+    arrs = inputs.generate_sltend(nblk, nproma, p, seed=51 + nproma)
+    ngptot = nproma * nblk - cut
+    ref = util.run_oracle_sltend(po, arrs, nproma, nblk, ngptot)
+    cloudsc.setup(p)
+    for diag in (True, False):
+        d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
+        cloudsc.sltend_supersat_batched(p, d, nproma, util.KLEV, nblk, ngptot, util.PTSPHY, diagnostics=diag)
+        torch.cuda.synchronize()
+        for n in fields.SLTEND_OUTPUTS:
+            g = d[n].cpu().numpy()
+            if n.startswith("padj") and not diag:
+                assert np.all(g == 0.0), n
+                continue
+            assert np.array_equal(g, ref[n]), (diag, n)

@@ -116,3 +116,17 @@ def test_satadj_edge_cases_bit_exact(pp, case):
     for n in util.fields.SATADJ_OUTPUTS:
         assert np.array_equal(emu[n], ref[n]), (case, n)
     assert nw == nwe
+
+
+@pytest.mark.parametrize("libm", ["plibm", "glibc"])
+def test_sltend_supersat_bit_exact(pp, libm):
+    """SLTEND's supersaturation adjustment (the CLOUD_SUPERSATCHECK reuse
+    after the cloud scheme): the kernel's point code against the oracle."""
+    p, po = pp
+    arrs = inputs.generate_sltend(32, 32, p, seed=19)
+    ngptot = 32 * 32 - 3
+    ref = util.run_oracle_sltend(po, arrs, 32, 32, ngptot, libm=libm)
+    emu = util.run_hostemu_sltend(p, arrs, 32, 32, ngptot, libm=libm)
+    for n in util.fields.SLTEND_OUTPUTS:
+        assert np.array_equal(emu[n], ref[n]), n
+    assert (ref["padjl"] != 0).any() and (ref["padji"] != 0).any()

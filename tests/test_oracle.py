@@ -129,3 +129,24 @@ def test_satadj_conserves_water_and_enthalpy():
         assert np.all(out[n][:, :top] == 0.0), n
     # condensation, evaporation and cloud-cover changes all occur
     assert (l > 0).any() and (l < 0).any() and (out["tendency_loc_a"] != 0).any()
+
+
+def test_sltend_supersat_conserves():
+    """SLTEND's supersaturation adjustment moves water from vapour to
+    condensate only: dq + dl + di = 0 and dT = (Lv/cp) dl + (Ls/cp) di per
+    point, up to rounding; levels above NCLDTOP are untouched."""
+    import numpy as np
+    from openifs_b200 import inputs
+    from tests import util
+    p, po = util.params()
+    a = inputs.generate_sltend(16, 32, po, seed=23)
+    out = util.run_oracle_sltend(po, a, 32, 16, 16 * 32, libm="glibc")
+    dt, dq = out["ptent"] - a["ptent"], out["ptenq"] - a["ptenq"]
+    dl = out["ptencld"][:, 0] - a["ptencld"][:, 0]
+    di = out["ptencld"][:, 1] - a["ptencld"][:, 1]
+    assert (dq != 0).any()
+    assert np.abs(dq + dl + di).max() <= 1e-9 * np.abs(dq).max()
+    assert np.abs(dt - po.ralvdcp * dl - po.ralsdcp * di).max() <= 1e-9 * np.abs(dt).max()
+    top = po.ncldtop - 1
+    assert np.array_equal(out["ptent"][:, :top], a["ptent"][:, :top])
+    assert np.array_equal(out["ptencld"][:, 2:], a["ptencld"][:, 2:])

@@ -189,3 +189,26 @@ def run_oracle_satadj(po, arrs, nproma, ngpblks, ngptot, libm="plibm"):
     out = {k: v.copy() for k, v in arrs.items()}
     nw = oracle.satadj_batched(po, out, nproma, KLEV, ngpblks, ngptot, PTSPHY, libm=libm)
     return out, nw
+
+
+def run_hostemu_sltend(p, arrs, nproma, ngpblks, ngptot, libm="plibm"):
+    """SLTEND's supersaturation adjustment, the kernel's point code on the host."""
+    import ctypes
+    import os
+    import subprocess
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hostemu")
+    subprocess.run(["make", "-s", "-C", here], check=True)
+    name = "libcloudsc_hostemu.so" if libm == "plibm" else "libcloudsc_hostemu_glibc.so"
+    L = ctypes.CDLL(os.path.join(here, name))
+    out = {k: v.copy() for k, v in arrs.items()}
+    ptrs = (ctypes.c_void_p * len(fields.SLTEND_FIELDS))(*[out[n].ctypes.data for n, *_ in fields.SLTEND_FIELDS])
+    L.hostemu_sltend_batched(ctypes.byref(p), int(nproma), KLEV, int(ngpblks), int(ngptot),
+                             ctypes.c_double(PTSPHY), ptrs)
+    return out
+
+
+def run_oracle_sltend(po, arrs, nproma, ngpblks, ngptot, libm="plibm"):
+    from oracle import oracle
+    out = {k: v.copy() for k, v in arrs.items()}
+    oracle.sltend_supersat_batched(po, out, nproma, KLEV, ngpblks, ngptot, PTSPHY, libm=libm)
+    return out
