@@ -262,6 +262,56 @@ def satadj_form(a, p, host, dev, world, rank, stream):
                            "sample": f"{nb} NPROMA blocks of 128, best of 3, OpenMP over blocks"}}
 
 
+def budget_form(a, p, d, plude0, dev, world, stream, ms64):
+    """The FP64 kernel with every cloud budget section on (LCLDBUDC/L/I/T,
+    the vertical integral, LCLDBUD_TIMEINT; cloudsc.F90:3832-4110) on the same
+    columns: device time and its overhead over the plain FP64 kernel.  The
+    budget-only inputs are seeded device noise and PEXTRA (94 fields) starts
+    at zero; parity of this form is in the tests."""
+    import torch
+    from openifs_b200 import cloudsc, fields
+    flags = {"lcldbudc": 1, "lcldbudl": 1, "lcldbudi": 1, "lcldbudt": 1, "lcldbud_vertint": 1,
+             "lcldbud_timeint": 1, "lbud23": 1}
+    pb = type(p).from_buffer_copy(p)
+    for k, v in flags.items():
+        setattr(pb, k, v)
+    kf = fields.budget_fields_needed(pb)
+    g = torch.Generator(device=dev).manual_seed(SEED)
+    shp = (NGPBLKS, KLEV, NPROMA)
+    diag = {n: torch.randn(shp, device=dev, dtype=torch.float64, generator=g) * 1e-5
+            for n in ("pvfa", "pdyna", "pdynl", "pdyni", "pdyns", "phrsw", "phrlw")}
+    diag["kctop"] = torch.zeros((NGPBLKS, NPROMA), device=dev, dtype=torch.int32)
+    diag["kpbltype"] = torch.zeros((NGPBLKS, NPROMA), device=dev, dtype=torch.int32)
+    diag["pextra"] = torch.zeros((NGPBLKS, kf, KLEV, NPROMA), device=dev, dtype=torch.float64)
+    cloudsc.setup(pb)
+    try:
+        def step():
+            d["plude"].copy_(plude0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cloudsc.cloudsc_batched_diag(pb, d, diag, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, stream=stream)
+            e1.record(stream)
+            return e0, e1
+        for _ in range(a.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        ev = [step() for _ in range(a.steps)]
+        torch.cuda.synchronize(dev)
+        ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    finally:
+        cloudsc.setup(p)
+        d["plude"].copy_(plude0)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    del diag
+    torch.cuda.empty_cache()
+    return {"ms": ms, "columns_per_s": world * NCOL / (ms * 1e-3), "overhead_vs_fp64": ms / ms64 - 1.0,
+            "sections": sorted(flags), "pextra_fields": kf}
+
+
 def sltend_form(a, p, host, dev, world, rank, stream):
     """SLTEND's supersaturation adjustment (the CLOUD_SUPERSATCHECK reuse
     after the cloud scheme) on the same 262,144 columns: device time of the
@@ -531,6 +581,7 @@ def run_ours(a):
                           "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
         errs[name] = err
 
+    bud = budget_form(a, p, d, plude0, dev, world, stream, results["fp64"]["ms"])
     sat = satadj_form(a, p, host, dev, world, rank, stream)
     slt = sltend_form(a, p, host, dev, world, rank, stream)
 
@@ -619,6 +670,7 @@ def run_ours(a):
                        "error_vs_fp64": errs["phys32"]},
             "surrogate": sur,
         },
+        "budget_diagnostics": bud,
         "satadj": sat,
         "sltend_supersat": slt,
         "roofline": roofline,

@@ -92,7 +92,7 @@ typedef struct cloudsc_params {
    * are the reference defaults noted beside each (others -> CLOUDSC_E_UNSUPPORTED) */
   int32_t laericeauto, laericesed, laerliqautolsp, laerliqcoll; /* all 0 (NAERCLD=0) */
   int32_t lcloud_inhomog;                                       /* 0 */
-  int32_t lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint; /* 0 */
+  int32_t lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint; /* any: budgets to PEXTRA, FP64 */
   int32_t lcldbud_timeint;                                      /* any */
   int32_t lcldbudget, lscmec;                                   /* 0 (diagnostic only) */
   /* ---- TECUMF (sucumf.F90:203,228-229) ---- */
@@ -138,7 +138,10 @@ int cloudsc_b200_setup(const cloudsc_params *p);
  * device workspace per calling thread), as EC_PHYS_DRV does under OpenMP
  * (ec_phys_drv.F90:438).  Arrays the default configuration does not read may be NULL:
  * pvfa, pdyna..pdyns, phrsw, phrlw, pvervel, pgeom, pgaw, kctop, kpbltype,
- * pgp2dspp, plcrit_aer, picrit_aer, pre_ice, pccn, pnice, pfsd, pextra.
+ * pgp2dspp, plcrit_aer, picrit_aer, pre_ice, pccn, pnice, pfsd, pextra.  With
+ * a cloud budget switch on (LCLDBUD*), the budget diagnostics are added to
+ * PEXTRA(KIDIA:KFDIA,:,1:KFLDX) and the inputs the sections that are on read
+ * are required (see cloudsc_b200_batched_diag).
  */
 int cloudsc_b200_block(
     const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
@@ -332,6 +335,42 @@ int cloudsc_b200_sltend_supersat_batched(
     const double *prs1, const double *pcent, const double *pcenq, const double *pcena,
     double *ptent, double *ptenq, double *ptena, double *ptencld, double *padja, double *padjl,
     double *padji, void *stream);
+
+/*
+ * cloudsc_b200_batched (FP64) with the cloud budget diagnostics
+ * (cloudsc.F90:3832-4110) that LCLDBUDC, LCLDBUDL, LCLDBUDI, LCLDBUDT and
+ * LCLDBUD_VERTINT switch on, with LCLDBUD_TIMEINT and LBUD23 as in the
+ * reference: the same arrays, then the inputs only the budgets read (PVFA,
+ * PDYNA, PDYNL, PDYNI, PDYNS, PHRSW, PHRLW, KCTOP, KPBLTYPE; those of sections
+ * that are off may be NULL) and PEXTRA (NPROMA, KLEV, KFLDX, NGPBLKS), INOUT:
+ * the diagnostics are added to it.  CLOUDSC_E_SHAPE when KFLDX is below the
+ * fields the sections need (the reference ABORTs, cloudsc.F90:3945-4106) or,
+ * with the vertical integral, KLEV < 84.  With no budget switch on it is
+ * cloudsc_b200_batched at FP64.  Budgets are also written by
+ * cloudsc_b200_block (its PEXTRA/KFLDX arguments); cloudsc_b200_batched,
+ * cloudsc_b200_batched_host and cloudsc_b200_block_noalloc return
+ * CLOUDSC_E_UNSUPPORTED when a budget switch is on.  No reference
+ * counterpart beyond the CLOUDSC call itself: this is its batched form.
+ */
+int cloudsc_b200_batched_diag(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks,
+    int32_t ngptot, double ptsphy, const double *pt, const double *pq,
+    const double *ptendency_cml_t, const double *ptendency_cml_q,
+    const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi,
+    const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis,
+    const double *plu, double *plude, const double *pludeli, const double *psnde,
+    const double *pmfu, const double *pmfd, const double *pa, const double *pclv,
+    double *pcovptot, double *prainfrac_toprfz, double *pfsqlf, double *pfsqif,
+    double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur,
+    double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
+    const double *pvfa, const double *pdyna, const double *pdynl, const double *pdyni,
+    const double *pdyns, const double *phrsw, const double *phrlw, const int32_t *kctop,
+    const int32_t *kpbltype, double *pextra, int32_t kfldx, uint32_t *ncounters,
+    void *stream);
 
 /* Bytes of the fixed device array cloudsc_b200_block_noalloc works in. */
 size_t cloudsc_b200_block_noalloc_capacity(void);

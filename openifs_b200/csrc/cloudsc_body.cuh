@@ -147,11 +147,166 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp,
 }
 
 // ---------------------------------------------------------------------------
+// Cloud budget diagnostics of one level (cloudsc.F90:3832-4110): the level's
+// budget terms added to PEXTRA(JL, *, *) (INOUT, (KLON,KLEV,KFLDX) per block;
+// `base` is the offset of PEXTRA(JL,1,1)).  Field pointer IS starts at 26
+// with LBUD23; each section on moves it on (+1, +12, +22, +20, +13).  The
+// vertical integral accumulates over the levels into the slots IK = 1..83 of
+// one field.  ZPIEVAP, ZPRACS and ZPRACI are zero in this configuration
+// (ISUBLICE = 0, PRACS and PRACI off); the KTYPE/KPBLTYPE == IS+1 tests are
+// as written at :3925,3929.
+// ---------------------------------------------------------------------------
+template <typename Real>
+CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double *cc, const double *bl,
+                           const double *bi, size_t base, int np, int klev, int k, double dt, double zqtmst,
+                           double zdp, double zrho, double pvfa, double pdyna, double pvfl, double pdynl,
+                           double pvfi, double pdyni, double pdyns, double phrsw, double phrlw, double xl,
+                           double xi, double psdep, double psacr, double piacr, double prainfrac, int ktype,
+                           int kpbltype, int kctop, double peis) {
+  double *px = F.pextra + base;
+  const size_t sk = (size_t)np, sf = (size_t)np * klev;
+  // PEXTRA(JL, IK, IS) with 1-based IK and IS
+  auto X = [&](int ik, int is) -> double & { return px[(size_t)(is - 1) * sf + (size_t)(ik - 1) * sk]; };
+  int is = P.lbud23 ? 26 : 0;
+  const double zdt = P.lcldbud_timeint ? dt : 1.0;
+  const int jk = k + 1;
+  if (P.lcldbud_vertint) {
+    const double zdz = zdp / (zrho * double(P.rg));
+    X(4, is + 1) = X(4, is + 1) + cc[2] * zdz * zdt;
+    X(6, is + 1) = X(6, is + 1) + cc[3] * zdz * zdt;
+    X(7, is + 1) = X(7, is + 1) + (cc[4] + cc[6]) * zdz * zdt;
+    X(8, is + 1) = X(8, is + 1) + cc[5] * zdz * zdt;
+    X(9, is + 1) = X(9, is + 1) + cc[7] * zdz * zdt;
+    X(10, is + 1) = X(10, is + 1) + cc[12] * zdz * zdt;
+    X(11, is + 1) = X(11, is + 1) + pvfa * zdz * zdt;
+    X(12, is + 1) = X(12, is + 1) + pdyna * zdz * zdt;
+    X(14 + 5, is + 1) = X(14 + 5, is + 1) + bl[2] * zdz * zdt;
+    X(14 + 7, is + 1) = X(14 + 7, is + 1) + bl[3] * zdz * zdt;
+    X(14 + 8, is + 1) = X(14 + 8, is + 1) + (bl[4] + bl[6]) * zdz * zdt;
+    X(14 + 9, is + 1) = X(14 + 9, is + 1) + bl[5] * zdz * zdt;
+    X(14 + 10, is + 1) = X(14 + 10, is + 1) + bl[7] * zdz * zdt;
+    X(14 + 11, is + 1) = X(14 + 11, is + 1) + bl[11] * zdz * zdt;
+    X(14 + 12, is + 1) = X(14 + 12, is + 1) + bl[14] * zdz * zdt;
+    X(14 + 13, is + 1) = X(14 + 13, is + 1) + bl[15] * zdz * zdt;
+    X(14 + 14, is + 1) = X(14 + 14, is + 1) + bl[12] * zdz * zdt;
+    X(14 + 15, is + 1) = X(14 + 15, is + 1) + bl[13] * zdz * zdt;
+    X(14 + 16, is + 1) = X(14 + 16, is + 1) + bl[17] * zdz * zdt;
+    X(14 + 17, is + 1) = X(14 + 17, is + 1) + (bl[18] + bl[19]) * zdz * zdt;
+    X(14 + 18, is + 1) = X(14 + 18, is + 1) + bl[20] * zdz * zdt;
+    X(14 + 19, is + 1) = X(14 + 19, is + 1) + bl[21] * zdz * zdt;
+    X(14 + 20, is + 1) = X(14 + 20, is + 1) + 0.0 * zdz * zdt * zqtmst;
+    X(14 + 21, is + 1) = X(14 + 21, is + 1) + psacr * zdz * zdt * zqtmst;
+    X(14 + 22, is + 1) = X(14 + 22, is + 1) + 0.0 * zdz * zdt * zqtmst;
+    X(14 + 23, is + 1) = X(14 + 23, is + 1) + piacr * zdz * zdt * zqtmst;
+    X(14 + 24, is + 1) = X(14 + 24, is + 1) + pvfl * zdz * zdt;
+    X(14 + 25, is + 1) = X(14 + 25, is + 1) + pdynl * zdz * zdt;
+    X(39 + 5, is + 1) = X(39 + 5, is + 1) + bi[2] * zdz * zdt;
+    X(39 + 7, is + 1) = X(39 + 7, is + 1) + bi[3] * zdz * zdt;
+    X(39 + 8, is + 1) = X(39 + 8, is + 1) + (bi[4] + bi[6]) * zdz * zdt;
+    X(39 + 9, is + 1) = X(39 + 9, is + 1) + bi[5] * zdz * zdt;
+    X(39 + 10, is + 1) = X(39 + 10, is + 1) + bi[7] * zdz * zdt;
+    X(39 + 11, is + 1) = X(39 + 11, is + 1) + bi[11] * zdz * zdt;
+    X(39 + 12, is + 1) = X(39 + 12, is + 1) + (bi[12] + bi[13]) * zdz * zdt;
+    X(39 + 13, is + 1) = X(39 + 13, is + 1) + bi[14] * zdz * zdt;
+    X(39 + 14, is + 1) = X(39 + 14, is + 1) + bi[16] * zdz * zdt;
+    X(39 + 15, is + 1) = X(39 + 15, is + 1) + bi[17] * zdz * zdt;
+    X(39 + 16, is + 1) = X(39 + 16, is + 1) + psdep * zqtmst * zdz * zdt;
+    X(39 + 17, is + 1) = X(39 + 17, is + 1) + pvfi * zdz * zdt;
+    X(39 + 18, is + 1) = X(39 + 18, is + 1) + pdyni * zdz * zdt;
+    X(39 + 19, is + 1) = X(39 + 19, is + 1) + pdyns * zdz * zdt;
+    X(60, is + 1) = prainfrac;
+    if (ktype == 0) X(70, is + 1) = X(70, is + 1) + 1.0;
+    if (ktype == is + 1) X(71, is + 1) = X(71, is + 1) + 1.0;
+    if (ktype == 2) X(72, is + 1) = X(72, is + 1) + 1.0;
+    if (ktype == 3) X(73, is + 1) = X(73, is + 1) + 1.0;
+    if (kpbltype == 0) X(74, is + 1) = X(74, is + 1) + 1.0;
+    if (kpbltype == is + 1) X(75, is + 1) = X(75, is + 1) + 1.0;
+    if (kpbltype == 2) X(76, is + 1) = X(76, is + 1) + 1.0;
+    if (kpbltype == 3) X(77, is + 1) = X(77, is + 1) + 1.0;
+    X(78, is + 1) = X(78, is + 1) + peis;
+    if (peis > 6.0) X(79, is + 1) = X(79, is + 1) + 1.0;
+    if (peis > 8.0) X(80, is + 1) = X(80, is + 1) + 1.0;
+    if (peis > 10.0) X(81, is + 1) = X(81, is + 1) + 1.0;
+    if (ktype >= 2 && peis < double(P.reisthsc)) X(82, is + 1) = X(82, is + 1) + 1.0;
+    if (ktype > 0) X(83, is + 1) = double(kctop);
+    is = is + 1;
+  }
+  if (P.lcldbudc) {  // :3948-3970
+    X(jk, is + 4) = X(jk, is + 4) + cc[2] * zdt;
+    X(jk, is + 6) = X(jk, is + 6) + cc[3] * zdt;
+    X(jk, is + 7) = X(jk, is + 7) + (cc[4] + cc[6]) * zdt;
+    X(jk, is + 8) = X(jk, is + 8) + cc[5] * zdt;
+    X(jk, is + 9) = X(jk, is + 9) + cc[7] * zdt;
+    X(jk, is + 11) = X(jk, is + 11) + pvfa * zdt;
+    X(jk, is + 12) = X(jk, is + 12) + pdyna * zdt;
+    is = is + 12;
+  }
+  if (P.lcldbudl) {  // :3972-4007
+    X(jk, is + 5) = X(jk, is + 5) + bl[2] * zdt;
+    X(jk, is + 7) = X(jk, is + 7) + bl[3] * zdt;
+    X(jk, is + 8) = X(jk, is + 8) + (bl[4] + bl[6]) * zdt;
+    X(jk, is + 9) = X(jk, is + 9) + bl[5] * zdt;
+    X(jk, is + 10) = X(jk, is + 10) + bl[7] * zdt;
+    X(jk, is + 11) = X(jk, is + 11) + bl[11] * zdt;
+    X(jk, is + 12) = X(jk, is + 12) + bl[12] * zdt;
+    X(jk, is + 13) = X(jk, is + 13) + bl[13] * zdt;
+    X(jk, is + 14) = X(jk, is + 14) + bl[14] * zdt;
+    X(jk, is + 15) = X(jk, is + 15) + bl[15] * zdt;
+    X(jk, is + 16) = X(jk, is + 16) + bl[17] * zdt;
+    X(jk, is + 17) = X(jk, is + 17) + (bl[18] + bl[19]) * zdt;
+    X(jk, is + 18) = X(jk, is + 18) + bl[20] * zdt;
+    X(jk, is + 19) = X(jk, is + 19) + bl[21] * zdt;
+    X(jk, is + 20) = X(jk, is + 20) + pvfl * zdt;
+    X(jk, is + 21) = X(jk, is + 21) + pdynl * zdt;
+    X(jk, is + 22) = X(jk, is + 22) + xl;
+    is = is + 22;
+  }
+  if (P.lcldbudi) {  // :4009-4048
+    X(jk, is + 5) = X(jk, is + 5) + bi[2] * zdt;
+    X(jk, is + 7) = X(jk, is + 7) + bi[3] * zdt;
+    X(jk, is + 8) = X(jk, is + 8) + (bi[4] + bi[6]) * zdt;
+    X(jk, is + 9) = X(jk, is + 9) + bi[5] * zdt;
+    X(jk, is + 10) = X(jk, is + 10) + bi[7] * zdt;
+    X(jk, is + 11) = X(jk, is + 11) + bi[11] * zdt;
+    X(jk, is + 12) = X(jk, is + 12) + (bi[12] + bi[13]) * zdt;
+    X(jk, is + 13) = X(jk, is + 13) + bi[14] * zdt;
+    X(jk, is + 14) = X(jk, is + 14) + (bi[15] + bi[16]) * zdt;
+    X(jk, is + 15) = X(jk, is + 15) + psdep * zqtmst * zdt;
+    X(jk, is + 16) = X(jk, is + 16) + bi[17] * zdt;
+    X(jk, is + 17) = X(jk, is + 17) + pvfi * zdt;
+    X(jk, is + 18) = X(jk, is + 18) + 0.0 * zqtmst * zdt;
+    X(jk, is + 19) = X(jk, is + 19) + pdyni * zdt;
+    X(jk, is + 20) = X(jk, is + 20) + xi;
+    is = is + 20;
+  }
+  if (P.lcldbudt) {  // :4051-4106
+    const double lv = double(P.ralvdcp), ls = double(P.ralsdcp), lf = double(P.ralfdcp);
+    X(jk, is + 1) = X(jk, is + 1) + phrsw;
+    X(jk, is + 2) = X(jk, is + 2) + phrlw;
+    X(jk, is + 3) = X(jk, is + 3) + ((bl[1] + bl[2] + bl[9] + bl[10]) * lv - bi[11] * lv) * zdt;
+    X(jk, is + 4) = X(jk, is + 4) + (bi[1] + bi[2] + bi[9] + bi[10] + bi[11]) * ls * zdt;
+    X(jk, is + 5) = X(jk, is + 5) + bi[11] * lf * zdt;
+    X(jk, is + 6) = X(jk, is + 6) + (bl[7] + bl[8] + bl[5]) * lv * zdt;
+    X(jk, is + 7) = X(jk, is + 7) + (bi[7] + bi[8] + bi[5]) * ls * zdt;
+    X(jk, is + 8) = X(jk, is + 8) + bl[20] * lv * zdt;
+    X(jk, is + 9) = X(jk, is + 9) + bi[17] * ls * zdt;
+    X(jk, is + 10) = X(jk, is + 10) + bi[15] * lf * zdt;
+    X(jk, is + 11) = X(jk, is + 11) + bi[16] * lf * zdt;
+    X(jk, is + 12) = X(jk, is + 12) - (bl[12] + bl[13] + bl[18] + bl[19]) * lf * zdt;
+    X(jk, is + 13) = X(jk, is + 13) + bl[21] * lf * zdt;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The column body.
 // ---------------------------------------------------------------------------
 // `active` false: the thread only keeps a CTA's per-level barrier company
 // (it computes column (ib, jl), which must be valid, and stores nothing).
-template <typename Real, bool F32M>
+// BUD: the form with the cloud budget diagnostics (cloudsc.F90:3832-4110),
+// FP64 only; the budget terms ZBUDCC/ZBUDL/ZBUDI of each level are collected
+// where the reference stores them and written to PEXTRA at the end of the
+// level.  Without BUD none of this code is compiled.
+template <typename Real, bool F32M, bool BUD = false>
 CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bool active = true) {
   const KParams<Real> &P = KP<Real>();
   const KParamsD &PD = c_kd;
@@ -325,6 +480,22 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       Real convsink_l = C(0.0), convsink_i = C(0.0);
       Real fallsrce_i = C(0.0), fallsrce_r = C(0.0), fallsrce_s = C(0.0);
       D qpretot = 0.0;
+      // cloud budget terms of this level, 1-based as ZBUDCC(:,1:12),
+      // ZBUDL(:,1:21), ZBUDI(:,1:17) (zero at the start of each level,
+      // :1271-1273), and the process rates the budget reads
+      struct Bud {
+        double cc[13], l[22], i[18];
+      } bd;
+      Real b_rainaut = C(0.0), b_rainacc = C(0.0), b_snowaut = C(0.0), b_snowrime = C(0.0);
+      Real b_psdep = C(0.0), b_psacr = C(0.0), b_piacr = C(0.0);
+      if constexpr (BUD) {
+#pragma unroll
+        for (int n = 0; n < 13; ++n) bd.cc[n] = 0.0;
+#pragma unroll
+        for (int n = 0; n < 22; ++n) bd.l[n] = 0.0;
+#pragma unroll
+        for (int n = 0; n < 18; ++n) bd.i[n] = 0.0;
+      }
       // The ZSOLQA accumulators are double in both instantiations; in the
       // FP32-mixed kernel each process rate (Real) is widened when added.
       // QADD/QSUB act on the stored entry of a pair (see struct QA); the
@@ -380,6 +551,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           convsrce_i = Real(pludeli2) * zdtgdp;
           QADD(LL, convsrce_l);
           QADD(II, convsrce_i);
+          if constexpr (BUD) {  // :1378-1380
+            bd.l[3] = convsrce_l * zqtmst;
+            bd.i[3] = convsrce_i * zqtmst;
+            bd.cc[3] = zqtmst * plude_k / plu_k1;
+          }
         } else {
           plude_k = 0.0;
         }
@@ -412,6 +588,10 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           lfinalsum = lfinalsum + zlfinal;
           QADD(LL, lcust_l);
           QSUB(LV, zevap);  // (V,L) += zevap, (L,V) -= zevap
+          if constexpr (BUD) {  // :1459-1460
+            bd.l[4] = lcust_l * zqtmst;
+            bd.l[5] = -zevap * zqtmst;
+          }
         }
         {
           Real zlfinal = mx(C(0.0), lcust_i - zdqs);
@@ -420,9 +600,17 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           lfinalsum = lfinalsum + zlfinal;
           QADD(II, lcust_i);
           QSUB(IV, zevap);  // (V,I) += zevap, (I,V) -= zevap
+          if constexpr (BUD) {  // :1475-1476
+            bd.i[4] = lcust_i * zqtmst;
+            bd.i[5] = -zevap * zqtmst;
+          }
         }
         solac = solac + zacust;
-        if (lfinalsum < zepsec) solac = solac - zacust;
+        if constexpr (BUD) bd.cc[4] = zacust * zqtmst;  // :1484
+        if (lfinalsum < zepsec) {
+          solac = solac - zacust;
+          if constexpr (BUD) bd.cc[5] = -zacust * zqtmst;  // :1488
+        }
       }
 
       // subsidence sink (:1499-1514)
@@ -454,6 +642,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           solac = solac - zaeros;
           QSUB(LV, liqfrac * zleros);  // (V,L) +=, (L,V) -=
           QSUB(IV, icefrac * zleros);  // (V,I) +=, (I,V) -=
+          if constexpr (BUD) {  // :1749-1751
+            bd.l[7] = -liqfrac * zleros * zqtmst;
+            bd.i[7] = -icefrac * zleros * zqtmst;
+            bd.cc[7] = -zaeros * zqtmst;
+          }
         }
       }
 
@@ -471,6 +664,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       if (k > ncldtop0) {
         fallsrce_i = pfplsx_i * zdtgdp;
         QADD(II, fallsrce_i);
+        if constexpr (BUD) bd.i[12] = fallsrce_i * zqtmst;  // :1865
         qxfg_i = qxfg_i + fallsrce_i;
         qpretot = qpretot + qxfg_i;
         fallsrce_r = pfplsx_r * zdtgdp;
@@ -517,6 +711,10 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
                      mpow<F32M>(zraincld, P.rcl_kkbac);
         }
         qb_rl = qb_rl + zrainacc;
+        if constexpr (BUD) {
+          b_rainaut = zrainaut;
+          b_rainacc = zrainacc;
+        }
       }
 
       // 4.4 rain evaporation (:2271-2378)
@@ -550,6 +748,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
           D zevap = mn(D(zdpevap), qxfg_r);
           QSUB(RV, zevap);  // (V,R) += zevap, (R,V) -= zevap
+          if constexpr (BUD) bd.l[20] = -zevap * zqtmst;  // :2363
           qxfg_r = qxfg_r - zevap;
         }
       }
@@ -579,6 +778,10 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           QSUB(LI, zdepos);  // (I,L) += zdepos, (L,I) -= zdepos
           qxfg_i = qxfg_i + zdepos;
           qxfg_l = qxfg_l - zdepos;
+          if constexpr (BUD) {  // :2495-2496
+            bd.l[11] = -zdepos * zqtmst;
+            bd.i[11] = zdepos * zqtmst;
+          }
         }
       }
 
@@ -599,6 +802,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
           zpsdep = mn(zpsdep, qv - zqsmix) / zcorqsmix;
           QADD(SV, zpsdep);  // (S,V) += zpsdep, (V,S) -= zpsdep
+          if constexpr (BUD) b_psdep = zpsdep;
         }
       }
 
@@ -613,6 +817,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         Real ztemp = C(-1.) * (r * r);
         Real zsnowaut = (ztemp < C(50.0)) ? zzco * (C(1.0) - mexp<F32M>(ztemp)) : zzco;
         qb_si = qb_si + zsnowaut;
+        if constexpr (BUD) b_snowaut = zsnowaut;
       }
 
       // 4.12 melting (:2815-2862)
@@ -632,11 +837,16 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           qxfg_i = qxfg_i - zmelt;
           qxfg_r = qxfg_r + zmelt;
           QSUB(IR, zmelt);  // (R,I) += zmelt, (I,R) -= zmelt
+          if constexpr (BUD) {  // :2856-2857
+            bd.i[15] = -zmelt * zqtmst;
+            bd.l[17] = zmelt * zqtmst;
+          }
           zalfa = qxfg_s / zicetot;
           zmelt = mn(qxfg_s, zalfa * D(zmeltmax));
           qxfg_s = qxfg_s - zmelt;
           qxfg_r = qxfg_r + zmelt;
           QADD(RS, zmelt);  // (R,S) += zmelt, (S,R) -= zmelt
+          if constexpr (BUD) bd.i[16] = -zmelt * zqtmst;  // :2858
         }
       }
 
@@ -661,6 +871,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           if (zfrzmax > zepsec) {
             D zfrz = mn(qrD, D(zfrzmax));
             QSUB(RS, zfrz);  // (S,R) += zfrz, (R,S) -= zfrz
+            if constexpr (BUD) bd.l[18] = -zfrz * zqtmst;  // :2927
           }
         }
       }
@@ -671,6 +882,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         if (zfrzmax > zepsec && qxfg_l > zepsec) {
           D zfrz = mn(qxfg_l, D(zfrzmax));
           QSUB(LI, zfrz);  // (I,L) += zfrz, (L,I) -= zfrz
+          if constexpr (BUD) bd.l[19] = -zfrz * zqtmst;  // :2958
         }
       }
 
@@ -681,6 +893,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
                          mpow<F32M>(zrho * zsnowcld * P.rcl_const1s, P.rcl_const8s);
         zsnowrime = mn(zsnowrime, C(1.0));
         qb_sl = qb_sl + zsnowrime;
+        if constexpr (BUD) b_snowrime = zsnowrime;
       }
 
       // PSD slopes (:3026-3069), PSACR (:3084-3115), PIACR (:3171-3198)
@@ -697,6 +910,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zpsacr =
               zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
           QSUB(RS, zpsacr);  // (S,R) += zpsacr, (R,S) -= zpsacr
+          if constexpr (BUD) b_psacr = zpsacr;
         }
         if (zicecld > zepsec) {
           Real zlami = mpow<F32M>(P.rcl_lam1s / (zrho * zicecld), P.rcl_lam2s);
@@ -707,6 +921,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zpiacr =
               zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
           QADD(IR, zpiacr);  // (I,R) += zpiacr, (R,I) -= zpiacr
+          if constexpr (BUD) b_piacr = zpiacr;
         }
       }
 
@@ -726,6 +941,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zdpevap = zdpr * zdtgdp;
           D zevap = mn(D(zdpevap), qxfg_s);
           QSUB(SV, zevap);  // (V,S) += zevap, (S,V) -= zevap
+          if constexpr (BUD) bd.i[17] = -zevap * zqtmst;  // :3304
           zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), Real(D(zcovptot - a) * zevap / qxfg_s)));
           qxfg_s = qxfg_s - zevap;
         }
@@ -828,6 +1044,17 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       pfplsx_s_n = Real(double(fallsink_s) * x_s * double(zrdtgdp));
       if (pfplsx_s_n + pfplsx_r_n < zepsec) zcovptot = C(0.0);
 
+      if constexpr (BUD) {  // diagnosed implicit rates (:3675-3699)
+        bd.l[14] = -b_rainaut * x_l * zqtmst;
+        bd.l[15] = -b_rainacc * x_l * zqtmst;
+        bd.cc[6] = -convsink_l * zanewm1 * zqtmst;
+        bd.l[6] = -convsink_l * x_l * zqtmst;
+        bd.i[6] = -convsink_i * x_i * zqtmst;
+        bd.i[13] = -fallsink_i * x_i * zqtmst;
+        bd.l[21] = -b_snowrime * x_l * zqtmst;
+        bd.i[14] = -b_snowaut * x_i * zqtmst;
+      }
+
       // 6.1-6.3 tendencies (:3713-3769), double
       {
         D fq;
@@ -858,6 +1085,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         loc_a = loc_a + a_adj * zqtmst;
         loc_cl = loc_cl + l_adj * zqtmst;
         loc_ci = loc_ci + i_adj * zqtmst;
+        if constexpr (BUD) {  // :3787-3789
+          bd.cc[2] = a_adj * zqtmst;
+          bd.l[2] = l_adj * zqtmst;
+          bd.i[2] = i_adj * zqtmst;
+        }
         D zl_adj = q0_l + loc_cl * dt;
         if (zl_adj < -PD.rlmin) nwarn++;
         if (zl_adj < 0.0) {
@@ -874,6 +1106,17 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         }
       }
       covp_out = zcovptot;
+      if constexpr (BUD) {
+        // inputs a section that is off does not read may be NULL
+        auto opt = [&](const double *q) { return q ? ld(q + ok) : 0.0; };
+        auto opti = [&](const int32_t *q) { return q ? ld(q + o1) : 0; };
+        if (active)
+          write_budgets(F, P, bd.cc, bd.l, bd.i, (size_t)ib * np * klev * F.kfldx + jl, np, klev, k, dt,
+                        zqtmst, double(zdp), double(zrho), opt(F.pvfa), opt(F.pdyna), double(pvfl),
+                        opt(F.pdynl), double(pvfi), opt(F.pdyni), opt(F.pdyns), opt(F.phrsw), opt(F.phrlw),
+                        x_l, x_i, double(b_psdep), double(b_psacr), double(b_piacr), double(prainfrac), ktype,
+                        opti(F.kpbltype), opti(F.kctop), double(peis));
+      }
     }  // k >= ncldtop0
 
     // ---------------- outputs of level k ----------------

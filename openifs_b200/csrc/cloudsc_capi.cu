@@ -64,8 +64,39 @@ int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
 bool params_supported(const cloudsc_params &p) {
   if (p.laericeauto || p.laericesed || p.laerliqautolsp || p.laerliqcoll) return false;
   if (p.lcloud_inhomog || p.lrad_cloud_inhomog || p.lspp) return false;
-  if (p.lcldbudc || p.lcldbudl || p.lcldbudi || p.lcldbudt || p.lcldbud_vertint) return false;
   return true;
+}
+
+// The cloud budget diagnostics (LCLDBUD*, cloudsc.F90:3832-4110) are on: the
+// FP64 kernel form that writes PEXTRA runs.
+bool budgets_on(const cloudsc_params &p) {
+  return p.lcldbudc || p.lcldbudl || p.lcldbudi || p.lcldbudt || p.lcldbud_vertint;
+}
+
+// Arguments of the budget form, checked as the reference does (it ABORTs when
+// KFLDX is too small, cloudsc.F90:3945-4106, or KLEV < 60 with the vertical
+// integral, :3851, which writes level slots up to 83); an input a section
+// that is on reads must not be NULL.
+int budget_args_ok(const cloudsc_params &p, int klev, int kfldx, const void *pextra, const void *pvfa,
+                   const void *pdyna, const void *pdynl, const void *pdyni, const void *pdyns,
+                   const void *phrsw, const void *phrlw, const void *kctop, const void *kpbltype) {
+  const int need = (p.lbud23 ? 26 : 0) + (p.lcldbud_vertint ? 1 : 0) + (p.lcldbudc ? 12 : 0) +
+                   (p.lcldbudl ? 22 : 0) + (p.lcldbudi ? 20 : 0) + (p.lcldbudt ? 13 : 0);
+  if (!pextra || kfldx < need)
+    return fail(CLOUDSC_E_SHAPE, "the budget diagnostics need PEXTRA with enough fields (KFLDX)");
+  if (p.lcldbud_vertint && klev < 84)
+    return fail(CLOUDSC_E_SHAPE, "the vertical-integral budget writes PEXTRA levels up to 83");
+  const bool ok = !((p.lcldbudc || p.lcldbud_vertint) && (!pvfa || !pdyna)) &&
+                  !((p.lcldbudl || p.lcldbud_vertint) && !pdynl) &&
+                  !((p.lcldbudi || p.lcldbud_vertint) && !pdyni) && !(p.lcldbud_vertint && !pdyns) &&
+                  !(p.lcldbudt && (!phrsw || !phrlw)) && !(p.lcldbud_vertint && (!kctop || !kpbltype));
+  if (!ok) return fail(CLOUDSC_E_NULL, "an input the budget diagnostics read is NULL");
+  return CLOUDSC_OK;
+}
+
+bool current_budgets_on() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_have_params && budgets_on(g_params);
 }
 
 Derived make_derived(const cloudsc_params &p) {
@@ -399,15 +430,24 @@ int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t 
   return cloudsc_b200_set_schedule(precision, best, threads_per_cta, ctas_per_sm);
 }
 
+// With the budget diagnostics on, the FP64 form that writes PEXTRA (kernel
+// form 3, launched with the FP64 schedule) runs instead of the plain one.
 static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaStream_t stream) {
   Schedule sc;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     sc = g_sched[precision];
   }
+  int form = precision;
+  if (current_budgets_on()) {
+    if (precision != 0) return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics are FP64 only");
+    if (!f.pextra) return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use "
+                                                      "cloudsc_b200_batched_diag or cloudsc_b200_block");
+    form = 3;
+  }
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + sc.threads - 1) / sc.threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
-  cudaError_t e = launch(precision, sc.variant, f, sh, sc.threads, grid, stream);
+  cudaError_t e = launch(form, sc.variant, f, sh, sc.threads, grid, stream);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
   return CLOUDSC_OK;
 }
@@ -451,6 +491,54 @@ int cloudsc_b200_batched(
               pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl, pfhpsn, ncounters};
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
   return launch_checked(precision, f, sh, (cudaStream_t)stream);
+}
+
+int cloudsc_b200_batched_diag(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a, const double *ptendency_cml_cld,
+    double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_cld, const double *pvfl, const double *pvfi, const double *pap,
+    const double *paph, const double *plsm, const int32_t *ldcum, const int32_t *ktype,
+    const double *peis, const double *plu, double *plude, const double *pludeli,
+    const double *psnde, const double *pmfu, const double *pmfd, const double *pa,
+    const double *pclv, double *pcovptot, double *prainfrac_toprfz, double *pfsqlf,
+    double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
+    double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
+    double *pfplsn, double *pfhpsl, double *pfhpsn, const double *pvfa, const double *pdyna,
+    const double *pdynl, const double *pdyni, const double *pdyns, const double *phrsw,
+    const double *phrlw, const int32_t *kctop, const int32_t *kpbltype, double *pextra,
+    int32_t kfldx, uint32_t *ncounters, void *stream) {
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  const void *req[] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+                       ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
+                       pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+                       pmfd, pa, pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng,
+                       pfsqrf, pfsqsf, pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl,
+                       pfhpsn};
+  for (const void *q : req)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  if (budgets_on(*p)) {
+    rc = budget_args_ok(*p, klev, kfldx, pextra, pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop,
+                        kpbltype);
+    if (rc) return rc;
+  }
+  rc = ensure_params(nullptr);
+  if (rc) return rc;
+  Fields f = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+              ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl, pvfi,
+              pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu, pmfd, pa,
+              pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng, pfsqrf, pfsqsf,
+              pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl, pfhpsn, ncounters,
+              pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop, kpbltype, pextra, kfldx};
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
+  return launch_checked(0, f, sh, (cudaStream_t)stream);
 }
 
 }  // extern "C"
@@ -611,7 +699,7 @@ size_t carve(char *base, size_t np, size_t klev, size_t nblk, void *dptr[42]) {
 }
 
 Fields fields_from(void *d[42], uint32_t *counter) {
-  Fields f;
+  Fields f{};
   f.pt = (const double *)d[0]; f.pq = (const double *)d[1]; f.cml_t = (const double *)d[2];
   f.cml_q = (const double *)d[3]; f.cml_a = (const double *)d[4]; f.cml_cld = (const double *)d[5];
   f.loc_t = (double *)d[6]; f.loc_q = (double *)d[7]; f.loc_a = (double *)d[8]; f.loc_cld = (double *)d[9];
@@ -652,10 +740,8 @@ int cloudsc_b200_block(
     double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
     double *pfplsn, double *pfhpsl, double *pfhpsn, double *pextra, int32_t kfldx) {
-  (void)lddiag; (void)pvfa; (void)pdyna; (void)pdynl; (void)pdyni; (void)pdynr; (void)pdyns;
-  (void)phrsw; (void)phrlw; (void)pvervel; (void)pgeom; (void)pgaw; (void)kctop; (void)kpbltype;
-  (void)pgp2dspp; (void)ldslphy; (void)plcrit_aer; (void)picrit_aer; (void)pre_ice; (void)pccn;
-  (void)pnice; (void)pfsd; (void)pextra; (void)kfldx;
+  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)pgaw; (void)pgp2dspp; (void)ldslphy;
+  (void)plcrit_aer; (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice; (void)pfsd;
   int rc = check_params_match(p);
   if (rc) return rc;
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
@@ -670,12 +756,22 @@ int cloudsc_b200_block(
                           pfhpsn};
   for (const void *q : host)
     if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  const bool bud = budgets_on(*p);
+  if (bud) {
+    rc = budget_args_ok(*p, klev, kfldx, pextra, pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop,
+                        kpbltype);
+    if (rc) return rc;
+  }
   int dev = 0;
   rc = ensure_params(&dev);
   if (rc) return rc;
   const size_t np = klon, kl = klev;
-  size_t bytes = carve(nullptr, np, kl, 1, nullptr);
-  rc = t_ws.prepare(dev, bytes);
+  const size_t bytes = carve(nullptr, np, kl, 1, nullptr);
+  // with the budget diagnostics: 7 level fields, 2 int columns and PEXTRA after the arrays
+  const size_t s2b = np * kl * 8, nx = bud ? (size_t)kfldx : 0;
+  const size_t base = (bytes + 255) / 256 * 256;
+  const size_t extra = bud ? 7 * s2b + 2 * ((np * 4 + 255) / 256 * 256) + nx * s2b : 0;
+  rc = t_ws.prepare(dev, base + extra);
   if (rc) return rc;
   void *d[42];
   carve(t_ws.buf, np, kl, 1, d);
@@ -686,6 +782,27 @@ int cloudsc_b200_block(
   if (e == cudaSuccess) e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), s);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
   Fields f = fields_from(d, t_ws.counter);
+  double *dx = nullptr;
+  if (bud) {
+    char *b = t_ws.buf + base;
+    const double *lv[7] = {pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw};
+    const double **dst[7] = {&f.pvfa, &f.pdyna, &f.pdynl, &f.pdyni, &f.pdyns, &f.phrsw, &f.phrlw};
+    for (int i = 0; i < 7 && e == cudaSuccess; ++i, b += s2b) {
+      *dst[i] = lv[i] ? (const double *)b : nullptr;
+      if (lv[i]) e = cudaMemcpyAsync(b, lv[i], s2b, cudaMemcpyHostToDevice, s);
+    }
+    const int32_t *iv[2] = {kctop, kpbltype};
+    const int32_t **idst[2] = {&f.kctop, &f.kpbltype};
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i, b += (np * 4 + 255) / 256 * 256) {
+      *idst[i] = iv[i] ? (const int32_t *)b : nullptr;
+      if (iv[i]) e = cudaMemcpyAsync(b, iv[i], np * 4, cudaMemcpyHostToDevice, s);
+    }
+    dx = (double *)b;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dx, pextra, nx * s2b, cudaMemcpyHostToDevice, s);
+    f.pextra = dx;
+    f.kfldx = kfldx;
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  }
   Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
   rc = launch_checked(0, f, sh, s);
   if (rc) return rc;
@@ -697,6 +814,8 @@ int cloudsc_b200_block(
     e = cudaMemcpy2DAsync((double *)host[i] + c0, np * 8, (double *)d[i] + c0, np * 8, ncol * 8, nrow,
                           cudaMemcpyDeviceToHost, s);
   }
+  if (bud && e == cudaSuccess)  // PEXTRA(KIDIA:KFDIA, :, :)
+    e = cudaMemcpy2DAsync(pextra + c0, np * 8, dx + c0, np * 8, ncol * 8, kl * nx, cudaMemcpyDeviceToHost, s);
   uint32_t nwarn = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -720,6 +839,8 @@ int cloudsc_b200_batched_host(
   int rc = check_params_match(p);
   if (rc) return rc;
   if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
+  if (budgets_on(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_block");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
     return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
@@ -835,6 +956,8 @@ int cloudsc_b200_block_noalloc(
     double *pfplsn, double *pfhpsl, double *pfhpsn, void *stream) {
   int rc = check_params_match(p);
   if (rc) return rc;
+  if (budgets_on(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_block");
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
     return fail(CLOUDSC_E_SHAPE, "inconsistent KIDIA/KFDIA/KLON/KLEV");
   if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");

@@ -156,6 +156,9 @@ struct KParams {
   // derived, loop-invariant
   Real zrdcp, zrg_r, zrldcp, zconst_pow_land, zconst_pow_sea, flt_0p4, flt_0p8;
   Real kkbauq_m1, kkbac_m1;
+  // cloud budget diagnostics (cloudsc.F90:3832-4110)
+  Real ralfdcp, reisthsc;
+  int lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint, lcldbud_timeint, lbud23;
   int ncldtop, lmfdsnow;
 };
 

@@ -34,6 +34,11 @@ struct Fields {
   double *pfsqlf, *pfsqif, *pfcqnng, *pfcqlng, *pfsqrf, *pfsqsf, *pfcqrng, *pfcqsng;
   double *pfsqltur, *pfsqitur, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
   uint32_t *ncounters;
+  // read only by the cloud budget diagnostics (the kernel form with budgets)
+  const double *pvfa, *pdyna, *pdynl, *pdyni, *pdyns, *phrsw, *phrlw;
+  const int32_t *kctop, *kpbltype;
+  double *pextra;  // PEXTRA (NPROMA, KLEV, KFLDX) per block, INOUT
+  int kfldx;
 };
 
 // Pointers of the batched CLOUD_SATADJ arrays (same block layout).

@@ -59,6 +59,7 @@ namespace cloudsc {
 // FORM selects the arithmetic of the column body:
 //   0  FP64, the reference's double build;
 //   1  FP32-mixed: FP32 transcendentals, everything else in double;
+//   3  FP64 with the cloud budget diagnostics (LCLDBUD*: PEXTRA written);
 //   2  FP32 physics: the process rates in FP32 as well (Real = float); the
 //      state, the sink limiters, the 5x5 solve, CLOUD_SUPERSATCHECK and the
 //      tendency and flux budgets stay in double.  Float rounding of the rates
@@ -85,8 +86,10 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
       ib = 0;
       jl = sh.kidia0;
     }
-    if (FORM == 2)
+    if constexpr (FORM == 2)
       cloudsc_column<float, true>(F, sh, ib, jl, active);
+    else if constexpr (FORM == 3)
+      cloudsc_column<double, false, true>(F, sh, ib, jl, active);
     else
       cloudsc_column<double, FORM == 1>(F, sh, ib, jl, active);
   }
@@ -244,6 +247,7 @@ static const void *kernel_ptr(int precision, int v) {
     case 0: return kernel_ptr_form<0>(v);
     case 1: return kernel_ptr_form<1>(v);
     case 2: return kernel_ptr_form<2>(v);
+    case 3: return kernel_ptr_form<3>(v);
     default: return nullptr;
   }
 }

@@ -33,6 +33,15 @@ inline void fill_kparams(const cloudsc_params &p, const Derived &d, KParams<Real
   k.flt_0p8 = Real(d.flt_0p8);
   k.kkbauq_m1 = Real(p.rcl_kkbauq - 1.0);
   k.kkbac_m1 = Real(p.rcl_kkbac - 1.0);
+  k.ralfdcp = Real(p.ralfdcp);
+  k.reisthsc = Real(p.reisthsc);
+  k.lcldbudc = p.lcldbudc;
+  k.lcldbudl = p.lcldbudl;
+  k.lcldbudi = p.lcldbudi;
+  k.lcldbudt = p.lcldbudt;
+  k.lcldbud_vertint = p.lcldbud_vertint;
+  k.lcldbud_timeint = p.lcldbud_timeint;
+  k.lbud23 = p.lbud23;
   k.ncldtop = p.ncldtop;
   k.lmfdsnow = p.lmfdsnow;
 }

@@ -206,3 +206,27 @@ def sltend_alloc(ngpblks, nproma, klev, alloc_fn=None):
 def sltend_bytes_per_column(klev=137, ncldtop=15, fp=8):
     nlev = klev - ncldtop + 1
     return 12 * nlev * fp, 8 * nlev * fp
+
+
+# The arrays that only the cloud budget diagnostics read (LCLDBUDC/L/I/T,
+# LCLDBUD_VERTINT; cloudsc.F90:3832-4110), in the argument order of
+# cloudsc_b200_batched_diag after the BATCHED_FIELDS arrays.  PEXTRA is
+# (KLON, KLEV, KFLDX) per block: numpy shape (NGPBLKS, KFLDX, KLEV, NPROMA).
+DIAG_FIELDS = [
+    ("pvfa", "2d", np.float64, "in"),
+    ("pdyna", "2d", np.float64, "in"),
+    ("pdynl", "2d", np.float64, "in"),
+    ("pdyni", "2d", np.float64, "in"),
+    ("pdyns", "2d", np.float64, "in"),
+    ("phrsw", "2d", np.float64, "in"),
+    ("phrlw", "2d", np.float64, "in"),
+    ("kctop", "1d", np.int32, "in"),
+    ("kpbltype", "1d", np.int32, "in"),
+    ("pextra", "extra", np.float64, "inout"),
+]
+
+
+def budget_fields_needed(params):
+    """PEXTRA fields the budget sections of ``params`` write (cloudsc.F90:3832-4110)."""
+    return ((26 if params.lbud23 else 0) + (1 if params.lcldbud_vertint else 0) + (12 if params.lcldbudc else 0) +
+            (22 if params.lcldbudl else 0) + (20 if params.lcldbudi else 0) + (13 if params.lcldbudt else 0))

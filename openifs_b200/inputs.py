@@ -262,6 +262,38 @@ def sltend_from(base, nproma, klev=KLEV_L137, seed=1, blocks=None):
     return out
 
 
+def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None):
+    """The inputs only the cloud budget diagnostics read (fields.DIAG_FIELDS)
+    for the blocks of an existing ``generate`` result ``base``, from
+    ``default_rng([seed, ib, 13])``: PVFA ~ N(0, 1e-5 /s); PDYNA ~ N(0, 1e-5
+    /s); PDYNL/I/S ~ the species' amount times N(0, 1e-5 /s); PHRSW ~ U(0,
+    2e-5 K/s), PHRLW ~ N(-2e-5, 1e-5 K/s); KCTOP a level index 1..KLEV on the
+    convective columns, 0 elsewhere; KPBLTYPE in 0..3; PEXTRA ~ N(0, 1) (it is
+    INOUT: the diagnostics add to it)."""
+    nb = base["pt"].shape[0]
+    ids = list(range(nb)) if blocks is None else list(blocks)
+    shp2 = (nb, klev, nproma)
+    out = {n: np.zeros(shp2) for n in ("pvfa", "pdyna", "pdynl", "pdyni", "pdyns", "phrsw", "phrlw")}
+    out["kctop"] = np.zeros((nb, nproma), np.int32)
+    out["kpbltype"] = np.zeros((nb, nproma), np.int32)
+    out["pextra"] = np.zeros((nb, kfldx, klev, nproma))
+    for j, ib in enumerate(ids):
+        rng = np.random.default_rng([int(seed), int(ib), 13])
+        shp = (klev, nproma)
+        out["pvfa"][j] = rng.normal(0.0, 1e-5, shp)
+        out["pdyna"][j] = rng.normal(0.0, 1e-5, shp)
+        out["pdynl"][j] = base["pclv"][j, 0] * rng.normal(0.0, 1e-5, shp)
+        out["pdyni"][j] = base["pclv"][j, 1] * rng.normal(0.0, 1e-5, shp)
+        out["pdyns"][j] = base["pclv"][j, 3] * rng.normal(0.0, 1e-5, shp)
+        out["phrsw"][j] = rng.uniform(0.0, 2e-5, shp)
+        out["phrlw"][j] = rng.normal(-2e-5, 1e-5, shp)
+        conv = base["ktype"][j] > 0
+        out["kctop"][j] = np.where(conv, rng.integers(1, klev + 1, nproma), 0).astype(np.int32)
+        out["kpbltype"][j] = rng.integers(0, 4, nproma).astype(np.int32)
+        out["pextra"][j] = rng.normal(0.0, 1.0, (kfldx, klev, nproma))
+    return out
+
+
 def constants_from(params):
     keys = ["rtice", "rtwat", "rtwat_rtice_r", "r2es", "r3les", "r3ies", "r4les", "r4ies", "rtt",
             "retv", "rd", "rg"]

@@ -52,6 +52,11 @@
 
 /* 1-based Fortran-order accessors */
 #define A1(a, jl) (a)[(jl)-1]
+/* budget terms and PEXTRA(KLON,KLEV,KFLDX), 1-based like the Fortran */
+#define BCC(jl, n) zbudcc[((size_t)(n)-1) * klon + ((jl)-1)]
+#define BL(jl, n) zbudl[((size_t)(n)-1) * klon + ((jl)-1)]
+#define BI(jl, n) zbudi[((size_t)(n)-1) * klon + ((jl)-1)]
+#define PX(jl, ik, is) pextra[(((size_t)(is)-1) * klev + ((ik)-1)) * klon + ((jl)-1)]
 #define A2(a, jl, jk) (a)[((size_t)(jk)-1) * klon + ((jl)-1)]
 #define A3(a, jl, jk, jm, n2) (a)[(((size_t)(jm)-1) * (n2) + ((jk)-1)) * klon + ((jl)-1)]
 #define L2(a, jl, jm) (a)[((size_t)(jm)-1) * klon + ((jl)-1)]
@@ -149,7 +154,6 @@ static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, int kft
 static int params_supported(const cloudsc_params *p) {
   if (p->laericeauto || p->laericesed || p->laerliqautolsp || p->laerliqcoll) return 0;
   if (p->lcloud_inhomog || p->lrad_cloud_inhomog || p->lspp) return 0;
-  if (p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint) return 0;
   return 1;
 }
 
@@ -173,11 +177,9 @@ int oracle_cloudsc(
     double *pfsqsf, double *pfcqrng, double *pfcqsng, double *pfsqltur,
     double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
     double *pextra, int kfldx) {
-  (void)lddiag; (void)pvfa; (void)pdyna; (void)pdynl; (void)pdyni; (void)pdynr;
-  (void)pdyns; (void)phrsw; (void)phrlw; (void)pvervel; (void)pgeom; (void)pgaw;
-  (void)kctop; (void)kpbltype; (void)pgp2dspp; (void)ldslphy; (void)plcrit_aer;
-  (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice; (void)pfsd; (void)pextra;
-  (void)kfldx;
+  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)pgaw; (void)pgp2dspp;
+  (void)ldslphy; (void)plcrit_aer; (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice;
+  (void)pfsd;
 
   if (!p || p->magic != CLOUDSC_PARAMS_MAGIC) return CLOUDSC_E_PARAMS;
   if (!params_supported(p)) return CLOUDSC_E_UNSUPPORTED;
@@ -185,6 +187,23 @@ int oracle_cloudsc(
   const int ncldtop = p->ncldtop;
   if (ncldtop < 2 || ncldtop > klev) return CLOUDSC_E_SHAPE;
   int nwarn = 0;
+
+  /* cloud budget diagnostics (:3832-4110): which sections are on, and the
+     PEXTRA fields they need (the reference ABORTs when KFLDX is too small,
+     :3945,3970,4007,4048,4106, or KLEV < 60 with the vertical integral,
+     :3851; the vertical integral writes level slots up to 83) */
+  const int lbud = p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint;
+  if (lbud) {
+    int need = (p->lbud23 ? 26 : 0) + (p->lcldbud_vertint ? 1 : 0) + (p->lcldbudc ? 12 : 0) +
+               (p->lcldbudl ? 22 : 0) + (p->lcldbudi ? 20 : 0) + (p->lcldbudt ? 13 : 0);
+    if (!pextra || kfldx < need) return CLOUDSC_E_SHAPE;
+    if (p->lcldbud_vertint && (klev < 84 || !ktype || !kpbltype || !kctop)) return CLOUDSC_E_SHAPE;
+    if ((p->lcldbudc || p->lcldbud_vertint) && (!pvfa || !pdyna)) return CLOUDSC_E_NULL;
+    if ((p->lcldbudl || p->lcldbud_vertint) && !pdynl) return CLOUDSC_E_NULL;
+    if ((p->lcldbudi || p->lcldbud_vertint) && !pdyni) return CLOUDSC_E_NULL;
+    if (p->lcldbud_vertint && !pdyns) return CLOUDSC_E_NULL;
+    if (p->lcldbudt && (!phrsw || !phrlw)) return CLOUDSC_E_NULL;
+  }
 
   /* constants (cloudsc.F90:693-848) */
   const double zepsilon = 100.0 * 0x1p-52; /* 100*EPSILON(1._JPRB) */
@@ -212,7 +231,7 @@ int oracle_cloudsc(
   /* 67 (KLON) arrays, 13 (KLON,KLEV) arrays, 4 (KLON,KLEV,NCLV), 1 (KLON,KLEV+1,NCLV),
      13 (KLON,NCLV) and 3 (KLON,NCLV,NCLV); sized with margin */
   double *buf = (double *)calloc(
-      n1 * 80 + n2 * 16 + n2 * NCLV * 4 + n2h * NCLV + n1 * NCLV * 16 + n1 * NCLV * NCLV * 3,
+      n1 * 140 + n2 * 16 + n2 * NCLV * 4 + n2h * NCLV + n1 * NCLV * 16 + n1 * NCLV * NCLV * 3,
       sizeof(double));
   if (!buf) return CLOUDSC_E_TOO_LARGE;
   double *w = buf;
@@ -236,6 +255,8 @@ int oracle_cloudsc(
   double *zq_upd = TAKE(n1), *zt_upd = TAKE(n1), *za_upd = TAKE(n1);
   double *zt_adj = TAKE(n1), *zq_adj = TAKE(n1), *za_adj = TAKE(n1), *zl_adj = TAKE(n1);
   double *zi_adj = TAKE(n1);
+  /* budget terms ZBUDCC(:,1:12), ZBUDL(:,1:21), ZBUDI(:,1:17), reset per level */
+  double *zbudcc = TAKE(n1 * 12), *zbudl = TAKE(n1 * 21), *zbudi = TAKE(n1 * 17);
   int *llrainliq = (int *)TAKE(n1); /* n1 doubles >= n1 ints */
 
   double *ztp1 = TAKE(n2), *zli = TAKE(n2), *za = TAKE(n2), *zaorig = TAKE(n2);
@@ -393,6 +414,9 @@ int oracle_cloudsc(
     memset(zfallsink, 0, sizeof(double) * n1 * NCLV);
     memset(zconvsrce, 0, sizeof(double) * n1 * NCLV);
     memset(zconvsink, 0, sizeof(double) * n1 * NCLV);
+    memset(zbudcc, 0, sizeof(double) * n1 * 12); /* :1271-1273 */
+    memset(zbudl, 0, sizeof(double) * n1 * 21);
+    memset(zbudi, 0, sizeof(double) * n1 * 17);
 
     /* derived variables (:1275-1326) */
     for (jl = kidia; jl <= kfdia; jl++) {
@@ -449,6 +473,9 @@ int oracle_cloudsc(
           L2(zconvsrce, jl, NCLDQI) = A3(pludeli, jl, jk, 2, klev) * A1(zdtgdp, jl);
           L3(zsolqa, jl, NCLDQL, NCLDQL) = L3(zsolqa, jl, NCLDQL, NCLDQL) + L2(zconvsrce, jl, NCLDQL);
           L3(zsolqa, jl, NCLDQI, NCLDQI) = L3(zsolqa, jl, NCLDQI, NCLDQI) + L2(zconvsrce, jl, NCLDQI);
+          BL(jl, 3) = L2(zconvsrce, jl, NCLDQL) * zqtmst; /* :1378-1380 */
+          BI(jl, 3) = L2(zconvsrce, jl, NCLDQI) * zqtmst;
+          BCC(jl, 3) = zqtmst * A2(plude, jl, jk) / A2(plu, jl, jk + 1);
         } else {
           A2(plude, jl, jk) = 0.0;
         }
@@ -489,6 +516,8 @@ int oracle_cloudsc(
         L3(zsolqa, jl, NCLDQL, NCLDQL) = L3(zsolqa, jl, NCLDQL, NCLDQL) + L2(zlcust, jl, NCLDQL);
         L3(zsolqa, jl, NCLDQV, NCLDQL) = L3(zsolqa, jl, NCLDQV, NCLDQL) + zevap;
         L3(zsolqa, jl, NCLDQL, NCLDQV) = L3(zsolqa, jl, NCLDQL, NCLDQV) - zevap;
+        BL(jl, 4) = L2(zlcust, jl, NCLDQL) * zqtmst; /* :1459-1460 */
+        BL(jl, 5) = -zevap * zqtmst;
       }
       for (jl = kidia; jl <= kfdia; jl++) {
         double zlfinal = fmax_(0.0, L2(zlcust, jl, NCLDQI) - A1(zdqs, jl));
@@ -498,10 +527,16 @@ int oracle_cloudsc(
         L3(zsolqa, jl, NCLDQI, NCLDQI) = L3(zsolqa, jl, NCLDQI, NCLDQI) + L2(zlcust, jl, NCLDQI);
         L3(zsolqa, jl, NCLDQV, NCLDQI) = L3(zsolqa, jl, NCLDQV, NCLDQI) + zevap;
         L3(zsolqa, jl, NCLDQI, NCLDQV) = L3(zsolqa, jl, NCLDQI, NCLDQV) - zevap;
+        BI(jl, 4) = L2(zlcust, jl, NCLDQI) * zqtmst; /* :1475-1476 */
+        BI(jl, 5) = -zevap * zqtmst;
       }
       for (jl = kidia; jl <= kfdia; jl++) {
         A1(zsolac, jl) = A1(zsolac, jl) + A1(zacust, jl);
-        if (A1(zlfinalsum, jl) < zepsec) A1(zsolac, jl) = A1(zsolac, jl) - A1(zacust, jl);
+        BCC(jl, 4) = A1(zacust, jl) * zqtmst; /* :1484-1489 */
+        if (A1(zlfinalsum, jl) < zepsec) {
+          A1(zsolac, jl) = A1(zsolac, jl) - A1(zacust, jl);
+          BCC(jl, 5) = -A1(zacust, jl) * zqtmst;
+        }
       }
     }
 
@@ -541,6 +576,9 @@ int oracle_cloudsc(
         L3(zsolqa, jl, NCLDQL, NCLDQV) = L3(zsolqa, jl, NCLDQL, NCLDQV) - A2(zliqfrac, jl, jk) * zleros;
         L3(zsolqa, jl, NCLDQV, NCLDQI) = L3(zsolqa, jl, NCLDQV, NCLDQI) + A2(zicefrac, jl, jk) * zleros;
         L3(zsolqa, jl, NCLDQI, NCLDQV) = L3(zsolqa, jl, NCLDQI, NCLDQV) - A2(zicefrac, jl, jk) * zleros;
+        BL(jl, 7) = -A2(zliqfrac, jl, jk) * zleros * zqtmst; /* :1749-1751 */
+        BI(jl, 7) = -A2(zicefrac, jl, jk) * zleros * zqtmst;
+        BCC(jl, 7) = -zaeros * zqtmst;
       }
     }
 
@@ -564,6 +602,7 @@ int oracle_cloudsc(
           L3(zsolqa, jl, jm, jm) = L3(zsolqa, jl, jm, jm) + L2(zfallsrce, jl, jm);
           L2(zqxfg, jl, jm) = L2(zqxfg, jl, jm) + L2(zfallsrce, jl, jm);
           A1(zqpretot, jl) = A1(zqpretot, jl) + L2(zqxfg, jl, jm);
+          if (jm == NCLDQI) BI(jl, 12) = L2(zfallsrce, jl, jm) * zqtmst; /* :1864-1866 */
         }
         L2(zfallsink, jl, jm) = A1(zdtgdp, jl) * A1(zrho, jl) * L2(zfallspeed, jl, jm);
       }
@@ -653,6 +692,7 @@ int oracle_cloudsc(
         double zevap = fmin_(zdpevap, L2(zqxfg, jl, NCLDQR));
         L3(zsolqa, jl, NCLDQV, NCLDQR) = L3(zsolqa, jl, NCLDQV, NCLDQR) + zevap;
         L3(zsolqa, jl, NCLDQR, NCLDQV) = L3(zsolqa, jl, NCLDQR, NCLDQV) - zevap;
+        BL(jl, 20) = -zevap * zqtmst; /* :2363 */
         L2(zqxfg, jl, NCLDQR) = L2(zqxfg, jl, NCLDQR) - zevap;
       }
     }
@@ -687,6 +727,8 @@ int oracle_cloudsc(
         L3(zsolqa, jl, NCLDQL, NCLDQI) = L3(zsolqa, jl, NCLDQL, NCLDQI) - zdepos;
         L2(zqxfg, jl, NCLDQI) = L2(zqxfg, jl, NCLDQI) + zdepos;
         L2(zqxfg, jl, NCLDQL) = L2(zqxfg, jl, NCLDQL) - zdepos;
+        BL(jl, 11) = -zdepos * zqtmst; /* :2495-2496 */
+        BI(jl, 11) = zdepos * zqtmst;
       }
     }
 
@@ -765,6 +807,9 @@ int oracle_cloudsc(
           L2(zqxfg, jl, jn) = L2(zqxfg, jl, jn) + zmelt;
           L3(zsolqa, jl, jn, jm) = L3(zsolqa, jl, jn, jm) + zmelt;
           L3(zsolqa, jl, jm, jn) = L3(zsolqa, jl, jm, jn) - zmelt;
+          if (jm == NCLDQI) BI(jl, 15) = -zmelt * zqtmst; /* :2856-2858 */
+          if (jm == NCLDQI) BL(jl, 17) = zmelt * zqtmst;
+          if (jm == NCLDQS) BI(jl, 16) = -zmelt * zqtmst;
         }
       }
     }
@@ -792,6 +837,7 @@ int oracle_cloudsc(
             double zfrz = fmin_(qr, A1(zfrzmax, jl));
             L3(zsolqa, jl, NCLDQS, NCLDQR) = L3(zsolqa, jl, NCLDQS, NCLDQR) + zfrz;
             L3(zsolqa, jl, NCLDQR, NCLDQS) = L3(zsolqa, jl, NCLDQR, NCLDQS) - zfrz;
+            BL(jl, 18) = -zfrz * zqtmst; /* :2927 */
           }
         }
       }
@@ -805,6 +851,7 @@ int oracle_cloudsc(
         double zfrz = fmin_(L2(zqxfg, jl, NCLDQL), A1(zfrzmax, jl));
         L3(zsolqa, jl, NCLDQI, NCLDQL) = L3(zsolqa, jl, NCLDQI, NCLDQL) + zfrz;
         L3(zsolqa, jl, NCLDQL, NCLDQI) = L3(zsolqa, jl, NCLDQL, NCLDQI) - zfrz;
+        BL(jl, 19) = -zfrz * zqtmst; /* :2958 */
       }
     }
 
@@ -905,6 +952,7 @@ int oracle_cloudsc(
         double zevap = fmin_(zdpevap, L2(zqxfg, jl, NCLDQS));
         L3(zsolqa, jl, NCLDQV, NCLDQS) = L3(zsolqa, jl, NCLDQV, NCLDQS) + zevap;
         L3(zsolqa, jl, NCLDQS, NCLDQV) = L3(zsolqa, jl, NCLDQS, NCLDQV) - zevap;
+        BI(jl, 17) = -zevap * zqtmst; /* :3304 */
         A1(zcovptot, jl) = fmax_(p->rcovpmin, A1(zcovptot, jl) - fmax_(0.0, (A1(zcovptot, jl) - zaa) * zevap /
                                                                                 L2(zqxfg, jl, NCLDQS)));
         L2(zqxfg, jl, NCLDQS) = L2(zqxfg, jl, NCLDQS) - zevap;
@@ -1040,6 +1088,19 @@ int oracle_cloudsc(
     for (jl = kidia; jl <= kfdia; jl++)
       if (A1(zqpretot, jl) < zepsec) A1(zcovptot, jl) = 0.0;
 
+    /* diagnosed rates of the implicit processes (:3675-3699), IWARMRAIN=3,
+       IP_SNOW_ACCRETES_RAIN=1 */
+    for (jl = kidia; jl <= kfdia; jl++) {
+      BL(jl, 14) = -A1(zrainaut, jl) * L2(zqxn, jl, NCLDQL) * zqtmst;
+      BL(jl, 15) = -A1(zrainacc, jl) * L2(zqxn, jl, NCLDQL) * zqtmst;
+      BCC(jl, 6) = -L2(zconvsink, jl, NCLDQL) * A1(zanewm1, jl) * zqtmst;
+      BL(jl, 6) = -L2(zconvsink, jl, NCLDQL) * L2(zqxn, jl, NCLDQL) * zqtmst;
+      BI(jl, 6) = -L2(zconvsink, jl, NCLDQI) * L2(zqxn, jl, NCLDQI) * zqtmst;
+      BI(jl, 13) = -L2(zfallsink, jl, NCLDQI) * L2(zqxn, jl, NCLDQI) * zqtmst;
+      BL(jl, 21) = -A1(zsnowrime, jl) * L2(zqxn, jl, NCLDQL) * zqtmst;
+      BI(jl, 14) = -A1(zsnowaut, jl) * L2(zqxn, jl, NCLDQI) * zqtmst;
+    }
+
     /* 6.1 T and condensate tendencies (:3713-3745) */
     for (jm = 1; jm <= NCLV - 1; jm++) {
       for (jl = kidia; jl <= kfdia; jl++)
@@ -1080,6 +1141,9 @@ int oracle_cloudsc(
       A2(ptendency_loc_a, jl, jk) = A2(ptendency_loc_a, jl, jk) + A1(za_adj, jl) * zqtmst;
       A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) = A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) + A1(zl_adj, jl) * zqtmst;
       A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) = A3(ptendency_loc_cld, jl, jk, NCLDQI, klev) + A1(zi_adj, jl) * zqtmst;
+      BCC(jl, 2) = A1(za_adj, jl) * zqtmst; /* :3787-3789 */
+      BL(jl, 2) = A1(zl_adj, jl) * zqtmst;
+      BI(jl, 2) = A1(zi_adj, jl) * zqtmst;
       A1(zl_adj, jl) = A3(zqx0, jl, jk, NCLDQL, klev) + A3(ptendency_loc_cld, jl, jk, NCLDQL, klev) * ptsphy;
       if (A1(zl_adj, jl) < -p->rlmin) nwarn++;
       if (A1(zl_adj, jl) < 0.0) {
@@ -1096,8 +1160,158 @@ int oracle_cloudsc(
       }
     }
     for (jl = kidia; jl <= kfdia; jl++) A2(pcovptot, jl, jk) = A1(zcovptot, jl);
-    /* ZANEWP (:3819-3823) and the budget section 7 (:3832-4126) feed only the
-       FSD/PEXTRA diagnostics, which are off in this configuration */
+    /* ZANEWP (:3819-3823) feeds only the FSD diagnostic (off) */
+
+    /* 7. cloud budget diagnostics (:3832-4110).  ZPIEVAP, ZPRACS and ZPRACI
+       are zero in this configuration (ISUBLICE=0, PRACS/PRACI off). */
+    if (lbud) {
+      int is = p->lbud23 ? 26 : 0;
+      const double zdt = p->lcldbud_timeint ? ptsphy : 1.0;
+      if (p->lcldbud_vertint) {
+        for (jl = kidia; jl <= kfdia; jl++) {
+          const double zdz = A1(zdp, jl) / (A1(zrho, jl) * p->rg);
+          int k = 0;
+          PX(jl, k + 4, is + 1) = PX(jl, k + 4, is + 1) + BCC(jl, 2) * zdz * zdt;
+          PX(jl, k + 6, is + 1) = PX(jl, k + 6, is + 1) + BCC(jl, 3) * zdz * zdt;
+          PX(jl, k + 7, is + 1) = PX(jl, k + 7, is + 1) + (BCC(jl, 4) + BCC(jl, 6)) * zdz * zdt;
+          PX(jl, k + 8, is + 1) = PX(jl, k + 8, is + 1) + BCC(jl, 5) * zdz * zdt;
+          PX(jl, k + 9, is + 1) = PX(jl, k + 9, is + 1) + BCC(jl, 7) * zdz * zdt;
+          PX(jl, k + 10, is + 1) = PX(jl, k + 10, is + 1) + BCC(jl, 12) * zdz * zdt;
+          PX(jl, k + 11, is + 1) = PX(jl, k + 11, is + 1) + A2(pvfa, jl, jk) * zdz * zdt;
+          PX(jl, k + 12, is + 1) = PX(jl, k + 12, is + 1) + A2(pdyna, jl, jk) * zdz * zdt;
+          k = 14;
+          PX(jl, k + 5, is + 1) = PX(jl, k + 5, is + 1) + BL(jl, 2) * zdz * zdt;
+          PX(jl, k + 7, is + 1) = PX(jl, k + 7, is + 1) + BL(jl, 3) * zdz * zdt;
+          PX(jl, k + 8, is + 1) = PX(jl, k + 8, is + 1) + (BL(jl, 4) + BL(jl, 6)) * zdz * zdt;
+          PX(jl, k + 9, is + 1) = PX(jl, k + 9, is + 1) + BL(jl, 5) * zdz * zdt;
+          PX(jl, k + 10, is + 1) = PX(jl, k + 10, is + 1) + BL(jl, 7) * zdz * zdt;
+          PX(jl, k + 11, is + 1) = PX(jl, k + 11, is + 1) + BL(jl, 11) * zdz * zdt;
+          PX(jl, k + 12, is + 1) = PX(jl, k + 12, is + 1) + BL(jl, 14) * zdz * zdt;
+          PX(jl, k + 13, is + 1) = PX(jl, k + 13, is + 1) + BL(jl, 15) * zdz * zdt;
+          PX(jl, k + 14, is + 1) = PX(jl, k + 14, is + 1) + BL(jl, 12) * zdz * zdt;
+          PX(jl, k + 15, is + 1) = PX(jl, k + 15, is + 1) + BL(jl, 13) * zdz * zdt;
+          PX(jl, k + 16, is + 1) = PX(jl, k + 16, is + 1) + BL(jl, 17) * zdz * zdt;
+          PX(jl, k + 17, is + 1) = PX(jl, k + 17, is + 1) + (BL(jl, 18) + BL(jl, 19)) * zdz * zdt;
+          PX(jl, k + 18, is + 1) = PX(jl, k + 18, is + 1) + BL(jl, 20) * zdz * zdt;
+          PX(jl, k + 19, is + 1) = PX(jl, k + 19, is + 1) + BL(jl, 21) * zdz * zdt;
+          PX(jl, k + 20, is + 1) = PX(jl, k + 20, is + 1) + 0.0 * zdz * zdt * zqtmst; /* ZPRACS */
+          PX(jl, k + 21, is + 1) = PX(jl, k + 21, is + 1) + A1(zpsacr, jl) * zdz * zdt * zqtmst;
+          PX(jl, k + 22, is + 1) = PX(jl, k + 22, is + 1) + 0.0 * zdz * zdt * zqtmst; /* ZPRACI */
+          PX(jl, k + 23, is + 1) = PX(jl, k + 23, is + 1) + A1(zpiacr, jl) * zdz * zdt * zqtmst;
+          PX(jl, k + 24, is + 1) = PX(jl, k + 24, is + 1) + A2(pvfl, jl, jk) * zdz * zdt;
+          PX(jl, k + 25, is + 1) = PX(jl, k + 25, is + 1) + A2(pdynl, jl, jk) * zdz * zdt;
+          k = 39;
+          PX(jl, k + 5, is + 1) = PX(jl, k + 5, is + 1) + BI(jl, 2) * zdz * zdt;
+          PX(jl, k + 7, is + 1) = PX(jl, k + 7, is + 1) + BI(jl, 3) * zdz * zdt;
+          PX(jl, k + 8, is + 1) = PX(jl, k + 8, is + 1) + (BI(jl, 4) + BI(jl, 6)) * zdz * zdt;
+          PX(jl, k + 9, is + 1) = PX(jl, k + 9, is + 1) + BI(jl, 5) * zdz * zdt;
+          PX(jl, k + 10, is + 1) = PX(jl, k + 10, is + 1) + BI(jl, 7) * zdz * zdt;
+          PX(jl, k + 11, is + 1) = PX(jl, k + 11, is + 1) + BI(jl, 11) * zdz * zdt;
+          PX(jl, k + 12, is + 1) = PX(jl, k + 12, is + 1) + (BI(jl, 12) + BI(jl, 13)) * zdz * zdt;
+          PX(jl, k + 13, is + 1) = PX(jl, k + 13, is + 1) + BI(jl, 14) * zdz * zdt;
+          PX(jl, k + 14, is + 1) = PX(jl, k + 14, is + 1) + BI(jl, 16) * zdz * zdt;
+          PX(jl, k + 15, is + 1) = PX(jl, k + 15, is + 1) + BI(jl, 17) * zdz * zdt;
+          PX(jl, k + 16, is + 1) = PX(jl, k + 16, is + 1) + A1(zpsdep, jl) * zqtmst * zdz * zdt;
+          PX(jl, k + 17, is + 1) = PX(jl, k + 17, is + 1) + A2(pvfi, jl, jk) * zdz * zdt;
+          PX(jl, k + 18, is + 1) = PX(jl, k + 18, is + 1) + A2(pdyni, jl, jk) * zdz * zdt;
+          PX(jl, k + 19, is + 1) = PX(jl, k + 19, is + 1) + A2(pdyns, jl, jk) * zdz * zdt;
+          PX(jl, 60, is + 1) = A1(prainfrac_toprfz, jl);
+          k = 70;
+          /* KTYPE/KPBLTYPE == IS+1 as written at :3925,3929 */
+          if (A1(ktype, jl) == 0) PX(jl, k, is + 1) = PX(jl, k, is + 1) + 1.0;
+          if (A1(ktype, jl) == is + 1) PX(jl, k + 1, is + 1) = PX(jl, k + 1, is + 1) + 1.0;
+          if (A1(ktype, jl) == 2) PX(jl, k + 2, is + 1) = PX(jl, k + 2, is + 1) + 1.0;
+          if (A1(ktype, jl) == 3) PX(jl, k + 3, is + 1) = PX(jl, k + 3, is + 1) + 1.0;
+          if (A1(kpbltype, jl) == 0) PX(jl, k + 4, is + 1) = PX(jl, k + 4, is + 1) + 1.0;
+          if (A1(kpbltype, jl) == is + 1) PX(jl, k + 5, is + 1) = PX(jl, k + 5, is + 1) + 1.0;
+          if (A1(kpbltype, jl) == 2) PX(jl, k + 6, is + 1) = PX(jl, k + 6, is + 1) + 1.0;
+          if (A1(kpbltype, jl) == 3) PX(jl, k + 7, is + 1) = PX(jl, k + 7, is + 1) + 1.0;
+          PX(jl, k + 8, is + 1) = PX(jl, k + 8, is + 1) + A1(peis, jl);
+          if (A1(peis, jl) > 6.0) PX(jl, k + 9, is + 1) = PX(jl, k + 9, is + 1) + 1.0;
+          if (A1(peis, jl) > 8.0) PX(jl, k + 10, is + 1) = PX(jl, k + 10, is + 1) + 1.0;
+          if (A1(peis, jl) > 10.0) PX(jl, k + 11, is + 1) = PX(jl, k + 11, is + 1) + 1.0;
+          if (A1(ktype, jl) >= 2 && A1(peis, jl) < p->reisthsc) PX(jl, k + 12, is + 1) = PX(jl, k + 12, is + 1) + 1.0;
+          if (A1(ktype, jl) > 0) PX(jl, k + 13, is + 1) = (double)A1(kctop, jl);
+        }
+        is = is + 1;
+      }
+      if (p->lcldbudc) { /* :3948-3970 */
+        for (jl = kidia; jl <= kfdia; jl++) {
+          PX(jl, jk, is + 4) = PX(jl, jk, is + 4) + BCC(jl, 2) * zdt;
+          PX(jl, jk, is + 6) = PX(jl, jk, is + 6) + BCC(jl, 3) * zdt;
+          PX(jl, jk, is + 7) = PX(jl, jk, is + 7) + (BCC(jl, 4) + BCC(jl, 6)) * zdt;
+          PX(jl, jk, is + 8) = PX(jl, jk, is + 8) + BCC(jl, 5) * zdt;
+          PX(jl, jk, is + 9) = PX(jl, jk, is + 9) + BCC(jl, 7) * zdt;
+          PX(jl, jk, is + 11) = PX(jl, jk, is + 11) + A2(pvfa, jl, jk) * zdt;
+          PX(jl, jk, is + 12) = PX(jl, jk, is + 12) + A2(pdyna, jl, jk) * zdt;
+        }
+        is = is + 12;
+      }
+      if (p->lcldbudl) { /* :3972-4007 */
+        for (jl = kidia; jl <= kfdia; jl++) {
+          PX(jl, jk, is + 5) = PX(jl, jk, is + 5) + BL(jl, 2) * zdt;
+          PX(jl, jk, is + 7) = PX(jl, jk, is + 7) + BL(jl, 3) * zdt;
+          PX(jl, jk, is + 8) = PX(jl, jk, is + 8) + (BL(jl, 4) + BL(jl, 6)) * zdt;
+          PX(jl, jk, is + 9) = PX(jl, jk, is + 9) + BL(jl, 5) * zdt;
+          PX(jl, jk, is + 10) = PX(jl, jk, is + 10) + BL(jl, 7) * zdt;
+          PX(jl, jk, is + 11) = PX(jl, jk, is + 11) + BL(jl, 11) * zdt;
+          PX(jl, jk, is + 12) = PX(jl, jk, is + 12) + BL(jl, 12) * zdt;
+          PX(jl, jk, is + 13) = PX(jl, jk, is + 13) + BL(jl, 13) * zdt;
+          PX(jl, jk, is + 14) = PX(jl, jk, is + 14) + BL(jl, 14) * zdt;
+          PX(jl, jk, is + 15) = PX(jl, jk, is + 15) + BL(jl, 15) * zdt;
+          PX(jl, jk, is + 16) = PX(jl, jk, is + 16) + BL(jl, 17) * zdt;
+          PX(jl, jk, is + 17) = PX(jl, jk, is + 17) + (BL(jl, 18) + BL(jl, 19)) * zdt;
+          PX(jl, jk, is + 18) = PX(jl, jk, is + 18) + BL(jl, 20) * zdt;
+          PX(jl, jk, is + 19) = PX(jl, jk, is + 19) + BL(jl, 21) * zdt;
+          PX(jl, jk, is + 20) = PX(jl, jk, is + 20) + A2(pvfl, jl, jk) * zdt;
+          PX(jl, jk, is + 21) = PX(jl, jk, is + 21) + A2(pdynl, jl, jk) * zdt;
+          PX(jl, jk, is + 22) = PX(jl, jk, is + 22) + L2(zqxn, jl, NCLDQL);
+        }
+        is = is + 22;
+      }
+      if (p->lcldbudi) { /* :4009-4048 */
+        for (jl = kidia; jl <= kfdia; jl++) {
+          PX(jl, jk, is + 5) = PX(jl, jk, is + 5) + BI(jl, 2) * zdt;
+          PX(jl, jk, is + 7) = PX(jl, jk, is + 7) + BI(jl, 3) * zdt;
+          PX(jl, jk, is + 8) = PX(jl, jk, is + 8) + (BI(jl, 4) + BI(jl, 6)) * zdt;
+          PX(jl, jk, is + 9) = PX(jl, jk, is + 9) + BI(jl, 5) * zdt;
+          PX(jl, jk, is + 10) = PX(jl, jk, is + 10) + BI(jl, 7) * zdt;
+          PX(jl, jk, is + 11) = PX(jl, jk, is + 11) + BI(jl, 11) * zdt;
+          PX(jl, jk, is + 12) = PX(jl, jk, is + 12) + (BI(jl, 12) + BI(jl, 13)) * zdt;
+          PX(jl, jk, is + 13) = PX(jl, jk, is + 13) + BI(jl, 14) * zdt;
+          PX(jl, jk, is + 14) = PX(jl, jk, is + 14) + (BI(jl, 15) + BI(jl, 16)) * zdt;
+          PX(jl, jk, is + 15) = PX(jl, jk, is + 15) + A1(zpsdep, jl) * zqtmst * zdt;
+          PX(jl, jk, is + 16) = PX(jl, jk, is + 16) + BI(jl, 17) * zdt;
+          PX(jl, jk, is + 17) = PX(jl, jk, is + 17) + A2(pvfi, jl, jk) * zdt;
+          PX(jl, jk, is + 18) = PX(jl, jk, is + 18) + 0.0 * zqtmst * zdt; /* ZPIEVAP */
+          PX(jl, jk, is + 19) = PX(jl, jk, is + 19) + A2(pdyni, jl, jk) * zdt;
+          PX(jl, jk, is + 20) = PX(jl, jk, is + 20) + L2(zqxn, jl, NCLDQI);
+        }
+        is = is + 20;
+      }
+      if (p->lcldbudt) { /* :4051-4106 */
+        for (jl = kidia; jl <= kfdia; jl++) {
+          PX(jl, jk, is + 1) = PX(jl, jk, is + 1) + A2(phrsw, jl, jk);
+          PX(jl, jk, is + 2) = PX(jl, jk, is + 2) + A2(phrlw, jl, jk);
+          PX(jl, jk, is + 3) = PX(jl, jk, is + 3) +
+                               ((BL(jl, 1) + BL(jl, 2) + BL(jl, 9) + BL(jl, 10)) * p->ralvdcp -
+                                BI(jl, 11) * p->ralvdcp) * zdt;
+          PX(jl, jk, is + 4) = PX(jl, jk, is + 4) +
+                               (BI(jl, 1) + BI(jl, 2) + BI(jl, 9) + BI(jl, 10) + BI(jl, 11)) * p->ralsdcp * zdt;
+          PX(jl, jk, is + 5) = PX(jl, jk, is + 5) + BI(jl, 11) * p->ralfdcp * zdt;
+          PX(jl, jk, is + 6) = PX(jl, jk, is + 6) + (BL(jl, 7) + BL(jl, 8) + BL(jl, 5)) * p->ralvdcp * zdt;
+          PX(jl, jk, is + 7) = PX(jl, jk, is + 7) + (BI(jl, 7) + BI(jl, 8) + BI(jl, 5)) * p->ralsdcp * zdt;
+          PX(jl, jk, is + 8) = PX(jl, jk, is + 8) + BL(jl, 20) * p->ralvdcp * zdt;
+          PX(jl, jk, is + 9) = PX(jl, jk, is + 9) + BI(jl, 17) * p->ralsdcp * zdt;
+          PX(jl, jk, is + 10) = PX(jl, jk, is + 10) + BI(jl, 15) * p->ralfdcp * zdt;
+          PX(jl, jk, is + 11) = PX(jl, jk, is + 11) + BI(jl, 16) * p->ralfdcp * zdt;
+          PX(jl, jk, is + 12) = PX(jl, jk, is + 12) -
+                                (BL(jl, 12) + BL(jl, 13) + BL(jl, 18) + BL(jl, 19)) * p->ralfdcp * zdt;
+          PX(jl, jk, is + 13) = PX(jl, jk, is + 13) + BL(jl, 21) * p->ralfdcp * zdt;
+        }
+        is = is + 13;
+      }
+    }
   }
   /* PCOVPTOT above the cloud top: left undefined by the reference, zero here */
   for (jk = 1; jk < ncldtop; jk++)
@@ -1555,4 +1769,58 @@ int oracle_sltend_supersat_batched(
     if (r < 0) err = r < err ? r : err;
   }
   return err;
+}
+
+/* The block loop of oracle_cloudsc_batched with the arrays the cloud budget
+ * diagnostics read (PVFA, PDYNA/L/I/S, PHRSW, PHRLW, KCTOP, KPBLTYPE) and
+ * PEXTRA (NPROMA, KLEV, KFLDX, NGPBLKS), INOUT. */
+int oracle_cloudsc_batched_diag(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_cld, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_cld, const double *pvfl,
+    const double *pvfi, const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis, const double *plu,
+    double *plude, const double *pludeli, const double *psnde, const double *pmfu,
+    const double *pmfd, const double *pa, const double *pclv, double *pcovptot,
+    double *prainfrac_toprfz, double *pfsqlf, double *pfsqif, double *pfcqnng,
+    double *pfcqlng, double *pfsqrf, double *pfsqsf, double *pfcqrng, double *pfcqsng,
+    double *pfsqltur, double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
+    double *pfhpsn, const double *pvfa, const double *pdyna, const double *pdynl,
+    const double *pdyni, const double *pdyns, const double *phrsw, const double *phrlw,
+    const int32_t *kctop, const int32_t *kpbltype, double *pextra, int kfldx, int nthreads) {
+  if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
+      ngptot <= nproma * (ngpblks - 1))
+    return CLOUDSC_E_SHAPE;
+  const size_t s2 = (size_t)nproma * klev, s2h = (size_t)nproma * (klev + 1), s1 = nproma;
+  const size_t sx = s2 * (size_t)(kfldx > 0 ? kfldx : 0);
+  int total = 0, err = 0;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+  (void)nthreads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : total) reduction(min : err)
+  for (int ib = 0; ib < ngpblks; ib++) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    const size_t o = ib * s2, o1 = ib * s1;
+    int r = oracle_cloudsc(
+        p, 1, icend, nproma, klev, 0, ptsphy, pt + o, pq + o, ptendency_cml_t + o, ptendency_cml_q + o,
+        ptendency_cml_a + o, ptendency_cml_cld + o * NCLV, ptendency_loc_t + o, ptendency_loc_q + o,
+        ptendency_loc_a + o, ptendency_loc_cld + o * NCLV, pvfa ? pvfa + o : NULL, pvfl + o, pvfi + o,
+        pdyna ? pdyna + o : NULL, pdynl ? pdynl + o : NULL, pdyni ? pdyni + o : NULL, NULL,
+        pdyns ? pdyns + o : NULL, phrsw ? phrsw + o : NULL, phrlw ? phrlw + o : NULL, NULL, pap + o,
+        paph + ib * s2h, NULL, plsm + o1, NULL, ldcum + o1, kctop ? kctop + o1 : NULL, ktype + o1,
+        kpbltype ? kpbltype + o1 : NULL, (double *)(peis + o1), plu + o, plude + o, pludeli + o * 4,
+        psnde + o * 2, pmfu + o, pmfd + o, NULL, 0, pa + o, pclv + o * NCLV, NULL, NULL, NULL, NULL, NULL,
+        pcovptot + o, NULL, prainfrac_toprfz + o1, pfsqlf + ib * s2h, pfsqif + ib * s2h,
+        pfcqnng + ib * s2h, pfcqlng + ib * s2h, pfsqrf + ib * s2h, pfsqsf + ib * s2h, pfcqrng + ib * s2h,
+        pfcqsng + ib * s2h, pfsqltur + ib * s2h, pfsqitur + ib * s2h, pfplsl + ib * s2h,
+        pfplsn + ib * s2h, pfhpsl + ib * s2h, pfhpsn + ib * s2h, pextra ? pextra + ib * sx : NULL, kfldx);
+    if (r < 0) err = r < err ? r : err;
+    else total += r;
+  }
+  return err < 0 ? err : total;
 }

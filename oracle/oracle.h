@@ -91,6 +91,25 @@ int oracle_cloud_satadj_batched(
     double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
     double *ptendency_loc_l, double *ptendency_loc_i, int nthreads);
 
+/* oracle_cloudsc_batched with the cloud budget diagnostics' inputs and
+ * PEXTRA (NPROMA, KLEV, KFLDX, NGPBLKS), INOUT. */
+int oracle_cloudsc_batched_diag(
+    const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+    double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
+    const double *ptendency_cml_q, const double *ptendency_cml_a,
+    const double *ptendency_cml_cld, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_cld, const double *pvfl,
+    const double *pvfi, const double *pap, const double *paph, const double *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const double *peis, const double *plu,
+    double *plude, const double *pludeli, const double *psnde, const double *pmfu,
+    const double *pmfd, const double *pa, const double *pclv, double *pcovptot,
+    double *prainfrac_toprfz, double *pfsqlf, double *pfsqif, double *pfcqnng,
+    double *pfcqlng, double *pfsqrf, double *pfsqsf, double *pfcqrng, double *pfcqsng,
+    double *pfsqltur, double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
+    double *pfhpsn, const double *pvfa, const double *pdyna, const double *pdynl,
+    const double *pdyni, const double *pdyns, const double *phrsw, const double *phrlw,
+    const int32_t *kctop, const int32_t *kpbltype, double *pextra, int kfldx, int nthreads);
+
 /* The supersaturation adjustment of SLTEND (sltend.F90:380-410), one block
  * and batched over (NPROMA,...,NGPBLKS) blocks. */
 int oracle_sltend_supersat(

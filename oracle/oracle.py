@@ -49,6 +49,9 @@ def lib(libm="glibc"):
         L.oracle_cloud_satadj_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
                                                   [vp] * len(SATADJ_FIELDS) + [i32])
         L.oracle_cloud_satadj_batched.restype = i32
+        L.oracle_cloudsc_batched_diag.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
+                                                  [vp] * (len(BATCHED_FIELDS) + 10) + [i32, i32])
+        L.oracle_cloudsc_batched_diag.restype = i32
         from openifs_b200.fields import SLTEND_FIELDS
         L.oracle_sltend_supersat_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
                                                      [vp] * len(SLTEND_FIELDS) + [i32])
@@ -118,4 +121,25 @@ def sltend_supersat_batched(params, arrays, nproma, klev, ngpblks, ngptot, tsphy
                                                   int(ngptot), float(tsphy), *ptrs, int(nthreads))
     if rc < 0:
         raise RuntimeError(f"oracle_sltend_supersat_batched returned {rc}")
+    return rc
+
+
+def cloudsc_batched_diag(params, arrays, diag, nproma, klev, ngpblks, ngptot, ptsphy, nthreads=0, libm="glibc"):
+    """oracle cloudsc_batched with the cloud budget diagnostics: ``diag``
+    holds the fields.DIAG_FIELDS arrays (PEXTRA updated in place)."""
+    from openifs_b200.fields import BATCHED_FIELDS, DIAG_FIELDS
+    ptrs = []
+    for n, *_ in BATCHED_FIELDS:
+        a = arrays[n]
+        if not (isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"]):
+            raise ValueError(f"{n}: need a C-contiguous numpy array")
+        ptrs.append(a.ctypes.data)
+    for n, *_ in DIAG_FIELDS:
+        a = diag.get(n)
+        ptrs.append(None if a is None else a.ctypes.data)
+    kfldx = diag["pextra"].shape[1]
+    rc = lib(libm).oracle_cloudsc_batched_diag(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
+                                               int(ngptot), float(ptsphy), *ptrs, int(kfldx), int(nthreads))
+    if rc < 0:
+        raise RuntimeError(f"oracle_cloudsc_batched_diag returned {rc}")
     return rc

@@ -160,3 +160,50 @@ extern "C" int hostemu_sltend_batched(const cloudsc_params *p, int nproma, int k
   }
   return 0;
 }
+
+// CLOUDSC with the cloud budget diagnostics (the kernel's BUD form): the
+// BATCHED_FIELDS arrays in `a`, then PVFA, PDYNA, PDYNL, PDYNI, PDYNS, PHRSW,
+// PHRLW, KCTOP, KPBLTYPE, PEXTRA (fields.DIAG_FIELDS order) in `b`.
+extern "C" int hostemu_batched_diag(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
+                                    double ptsphy, void **a, void **b, int kfldx) {
+  Derived d;
+#ifdef CLOUDSC_HOST_LIBM_GLIBC
+  d.zconst_pow_land = std::pow(p->rcl_kk_cloud_num_land, p->rcl_kkbaun);
+  d.zconst_pow_sea = std::pow(p->rcl_kk_cloud_num_sea, p->rcl_kkbaun);
+#else
+  d.zconst_pow_land = plibm_pow(p->rcl_kk_cloud_num_land, p->rcl_kkbaun);
+  d.zconst_pow_sea = plibm_pow(p->rcl_kk_cloud_num_sea, p->rcl_kkbaun);
+#endif
+  d.flt_0p4 = (double)0.4f;
+  d.flt_0p8 = (double)0.8f;
+  fill_kparams(*p, d, c_kpd);
+  fill_kparams(*p, d, c_kpf);
+  fill_kparams_d(*p, c_kd);
+  uint32_t nwarn = 0;
+  Fields f{};
+  const double **ad = (const double **)a;
+  f.pt = ad[0]; f.pq = ad[1]; f.cml_t = ad[2]; f.cml_q = ad[3]; f.cml_a = ad[4]; f.cml_cld = ad[5];
+  f.loc_t = (double *)a[6]; f.loc_q = (double *)a[7]; f.loc_a = (double *)a[8]; f.loc_cld = (double *)a[9];
+  f.pvfl = ad[10]; f.pvfi = ad[11]; f.pap = ad[12]; f.paph = ad[13]; f.plsm = ad[14];
+  f.ldcum = (const int32_t *)a[15]; f.ktype = (const int32_t *)a[16]; f.peis = ad[17]; f.plu = ad[18];
+  f.plude = (double *)a[19]; f.pludeli = ad[20]; f.psnde = ad[21]; f.pmfu = ad[22]; f.pmfd = ad[23];
+  f.pa = ad[24]; f.pclv = ad[25]; f.pcovptot = (double *)a[26]; f.prainfrac_toprfz = (double *)a[27];
+  f.pfsqlf = (double *)a[28]; f.pfsqif = (double *)a[29]; f.pfcqnng = (double *)a[30];
+  f.pfcqlng = (double *)a[31]; f.pfsqrf = (double *)a[32]; f.pfsqsf = (double *)a[33];
+  f.pfcqrng = (double *)a[34]; f.pfcqsng = (double *)a[35]; f.pfsqltur = (double *)a[36];
+  f.pfsqitur = (double *)a[37]; f.pfplsl = (double *)a[38]; f.pfplsn = (double *)a[39];
+  f.pfhpsl = (double *)a[40]; f.pfhpsn = (double *)a[41];
+  f.ncounters = &nwarn;
+  const double **bd = (const double **)b;
+  f.pvfa = bd[0]; f.pdyna = bd[1]; f.pdynl = bd[2]; f.pdyni = bd[3]; f.pdyns = bd[4];
+  f.phrsw = bd[5]; f.phrlw = bd[6]; f.kctop = (const int32_t *)b[7]; f.kpbltype = (const int32_t *)b[8];
+  f.pextra = (double *)b[9];
+  f.kfldx = kfldx;
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
+  for (int ib = 0; ib < ngpblks; ++ib) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    for (int jl = 0; jl < icend; ++jl) cloudsc_column<double, false, true>(f, sh, ib, jl);
+  }
+  return (int)nwarn;
+}

@@ -1,0 +1,66 @@
+"""The cloud budget diagnostics (LCLDBUDC/L/I/T, LCLDBUD_VERTINT;
+cloudsc.F90:3832-4110) on the B200 against the oracle: PEXTRA and every
+output bit for bit, through the batched entry and the per-block host entry."""
+import numpy as np
+import pytest
+
+from openifs_b200 import cloudsc, fields, inputs
+from tests import util
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("flags", util.BUDGET_CASES)
+def test_batched_diag_bit_exact(cuda, flags):
+    import torch
+    p0, po0 = util.params()
+    p, po = util.with_flags(p0, flags), util.with_flags(po0, flags)
+    nproma, nblk = 64, 5
+    ngptot = nproma * nblk - 9
+    arrs = inputs.generate(nblk, nproma, p, seed=37)
+    diag = inputs.generate_diag(arrs, nproma, fields.budget_fields_needed(p) + 2, seed=37)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot)
+    try:
+        cloudsc.setup(p)
+        d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
+        g = {k: torch.from_numpy(v).cuda() for k, v in diag.items()}
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        cloudsc.cloudsc_batched_diag(p, d, g, nproma, util.KLEV, nblk, ngptot, util.PTSPHY, counter=cnt)
+        torch.cuda.synchronize()
+        assert np.array_equal(g["pextra"].cpu().numpy(), dref["pextra"])
+        for n in util.COMPARED:
+            assert np.array_equal(util.defined(n, d[n].cpu().numpy()), util.defined(n, ref[n])), n
+        assert int(cnt.item()) == nw
+        # the plain batched entry refuses: it has no PEXTRA
+        with pytest.raises(cloudsc.CloudscError):
+            cloudsc.cloudsc_batched(p, d, nproma, util.KLEV, nblk, ngptot, util.PTSPHY)
+    finally:
+        cloudsc.setup(p0)
+
+
+def test_block_entry_budgets(cuda):
+    """cloudsc_b200_block with all budget sections on: PEXTRA(KIDIA:KFDIA,:,:)
+    as the oracle, the other columns of PEXTRA untouched."""
+    p0, po0 = util.params()
+    flags = util.BUDGET_CASES[-1]
+    p, po = util.with_flags(p0, flags), util.with_flags(po0, flags)
+    nproma = 40
+    arrs = inputs.generate(1, nproma, p, seed=41)
+    kf = fields.budget_fields_needed(p)
+    diag = inputs.generate_diag(arrs, nproma, kf, seed=41)
+    ref, dref, _ = util.run_oracle_diag(po, arrs, diag, nproma, 1, nproma)
+    blk = {k: np.ascontiguousarray(v[0]) for k, v in arrs.items()}
+    blk.update({k: np.ascontiguousarray(v[0]) for k, v in diag.items()})
+    kidia, kfdia = 3, 37
+    try:
+        cloudsc.setup(p)
+        cloudsc.cloudsc_block(p, kidia, kfdia, nproma, util.KLEV, util.PTSPHY, blk, kfldx=kf)
+    finally:
+        cloudsc.setup(p0)
+    cols = slice(kidia - 1, kfdia)
+    assert np.array_equal(blk["pextra"][..., cols], dref["pextra"][0][..., cols])
+    assert np.array_equal(blk["pextra"][..., :kidia - 1], diag["pextra"][0][..., :kidia - 1])
+    assert np.array_equal(blk["pextra"][..., kfdia:], diag["pextra"][0][..., kfdia:])
+    for n in util.COMPARED:
+        g, o = util.defined(n, blk[n][None]), util.defined(n, ref[n])
+        assert np.array_equal(g[..., cols], o[..., cols]), n

@@ -130,3 +130,27 @@ def test_sltend_supersat_bit_exact(pp, libm):
     for n in util.fields.SLTEND_OUTPUTS:
         assert np.array_equal(emu[n], ref[n]), n
     assert (ref["padjl"] != 0).any() and (ref["padji"] != 0).any()
+
+
+@pytest.mark.parametrize("flags", util.BUDGET_CASES)
+def test_budget_diagnostics_bit_exact(pp, flags):
+    """The cloud budget diagnostics (LCLDBUDC/L/I/T, the vertical integral;
+    cloudsc.F90:3832-4110): the kernel's budget form on the host against the
+    oracle, PEXTRA bit for bit; the other outputs are unchanged by the
+    budgets."""
+    p0, po0 = pp
+    p, po = util.with_flags(p0, flags), util.with_flags(po0, flags)
+    nproma, nblk = 32, 6
+    ngptot = nproma * nblk - 3
+    arrs = inputs.generate(nblk, nproma, p, seed=29)
+    kf = util.fields.budget_fields_needed(p) + 1
+    diag = inputs.generate_diag(arrs, nproma, kf, seed=29)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot)
+    emu, demu, nwe = util.run_hostemu_diag(p, arrs, diag, nproma, nblk, ngptot)
+    assert nw == nwe
+    assert np.array_equal(demu["pextra"], dref["pextra"])
+    assert (dref["pextra"] != diag["pextra"]).any()
+    plain, _ = util.run_oracle(po0, arrs, nproma, nblk, ngptot, libm="plibm")
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), n
+        assert np.array_equal(util.defined(n, ref[n]), util.defined(n, plain[n])), n

@@ -212,3 +212,50 @@ def run_oracle_sltend(po, arrs, nproma, ngpblks, ngptot, libm="plibm"):
     out = {k: v.copy() for k, v in arrs.items()}
     oracle.sltend_supersat_batched(po, out, nproma, KLEV, ngpblks, ngptot, PTSPHY, libm=libm)
     return out
+
+
+
+def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm"):
+    """The kernel's column code with the budget diagnostics, on the host."""
+    import ctypes
+    import os
+    import subprocess
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hostemu")
+    subprocess.run(["make", "-s", "-C", here], check=True)
+    name = "libcloudsc_hostemu.so" if libm == "plibm" else "libcloudsc_hostemu_glibc.so"
+    L = ctypes.CDLL(os.path.join(here, name))
+    out = {k: v.copy() for k, v in arrs.items()}
+    dout = {k: v.copy() for k, v in diag.items()}
+    a = (ctypes.c_void_p * len(fields.BATCHED_FIELDS))(*[out[n].ctypes.data for n, *_ in fields.BATCHED_FIELDS])
+    b = (ctypes.c_void_p * len(fields.DIAG_FIELDS))(
+        *[(dout[n].ctypes.data if dout.get(n) is not None else None) for n, *_ in fields.DIAG_FIELDS])
+    nw = L.hostemu_batched_diag(ctypes.byref(p), int(nproma), KLEV, int(ngpblks), int(ngptot),
+                                ctypes.c_double(PTSPHY), a, b, int(dout["pextra"].shape[1]))
+    return out, dout, nw
+
+
+def run_oracle_diag(po, arrs, diag, nproma, ngpblks, ngptot, libm="plibm"):
+    from oracle import oracle
+    out = {k: v.copy() for k, v in arrs.items()}
+    dout = {k: v.copy() for k, v in diag.items()}
+    nw = oracle.cloudsc_batched_diag(po, out, dout, nproma, KLEV, ngpblks, ngptot, PTSPHY, libm=libm)
+    return out, dout, nw
+
+
+BUDGET_CASES = [
+    {"lcldbudc": 1},
+    {"lcldbudl": 1},
+    {"lcldbudi": 1},
+    {"lcldbudt": 1},
+    {"lcldbud_vertint": 1},
+    {"lcldbudc": 1, "lcldbudl": 1, "lcldbudi": 1, "lcldbudt": 1, "lcldbud_vertint": 1, "lcldbud_timeint": 1,
+     "lbud23": 1},
+]
+
+
+def with_flags(p, flags):
+    """A copy of the params struct ``p`` with ``flags`` set."""
+    q = type(p).from_buffer_copy(p)
+    for k, v in flags.items():
+        setattr(q, k, v)
+    return q
