@@ -91,7 +91,7 @@ typedef struct cloudsc_params {
   /* switches that select code paths; the values the B200 kernels implement
    * are the reference defaults noted beside each (others -> CLOUDSC_E_UNSUPPORTED) */
   int32_t laericeauto, laericesed, laerliqautolsp, laerliqcoll; /* all 0 (NAERCLD=0) */
-  int32_t lcloud_inhomog;                                       /* 0 */
+  int32_t lcloud_inhomog;                                       /* any (FP64) */
   int32_t lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint; /* any: budgets to PEXTRA, FP64 */
   int32_t lcldbud_timeint;                                      /* any */
   int32_t lcldbudget, lscmec;                                   /* 0 (diagnostic only) */
@@ -100,12 +100,34 @@ typedef struct cloudsc_params {
   double rmfadvw, rmfadvwdd;                                    /* any (default 0) */
   /* ---- TERAD / TEPHY / TVDF / TSPP_CONFIG ---- */
   double rcloud_frac_std;                                       /* suecrad.F90:745 */
-  int32_t lrad_cloud_inhomog;                                   /* 0 */
+  int32_t lrad_cloud_inhomog;                                   /* any (FP64): PFSD */
   int32_t lbud23;                                               /* any (budgets off) */
   double reisthsc;                                              /* unused when budgets off */
-  int32_t lspp;                                                 /* 0 */
+  int32_t lspp;                                                 /* any */
   int32_t pad_;
+  /* ---- SPP perturbations (YDSPP_CONFIG, cloudsc.F90:850-939), read when
+   * lspp: perturbation n of RAMID, RCLDIFF, RCLCRIT, RLCRITSNOW, RAINEVAP,
+   * SNOWSUBLIM, FALLSPEED, CLOUDINHOM (n = 0..7, CLOUDSC_SPP_* below) is on
+   * when its pointer YDSPP_CONFIG%PPTR%x > 0; spp_mp[n] is its PN%MP (the
+   * 1-based PGP2DSPP field; CLOUDINHOM also uses MP+1), spp_mu[2n+i] and
+   * spp_xmag[2n+i] its PN%MU(i+1) and PN%XMAG(i+1).  A parameter X becomes
+   * X*EXP(MU + XMAG*PGP2DSPP(JL,MP)). ---- */
+  int32_t spp_on[8];
+  int32_t spp_mp[8];
+  double spp_mu[16];
+  double spp_xmag[16];
+  int32_t spp_lramidlimit1;                                     /* YDSPP_CONFIG%LRAMIDLIMIT1 */
+  int32_t spp_nrftotal;                                         /* fields of PGP2DSPP (SM%NRFTOTAL) */
 } cloudsc_params;
+
+#define CLOUDSC_SPP_RAMID 0
+#define CLOUDSC_SPP_RCLDIFF 1
+#define CLOUDSC_SPP_RCLCRIT 2
+#define CLOUDSC_SPP_RLCRITSNOW 3
+#define CLOUDSC_SPP_RAINEVAP 4
+#define CLOUDSC_SPP_SNOWSUBLIM 5
+#define CLOUDSC_SPP_FALLSPEED 6
+#define CLOUDSC_SPP_CLOUDINHOM 7
 
 /*
  * Fill *p with the reference defaults of SUCLDP/SUPHEC/YOMCST/SUCUMF/SUECRAD
@@ -337,19 +359,27 @@ int cloudsc_b200_sltend_supersat_batched(
     double *padji, void *stream);
 
 /*
- * cloudsc_b200_batched (FP64) with the cloud budget diagnostics
- * (cloudsc.F90:3832-4110) that LCLDBUDC, LCLDBUDL, LCLDBUDI, LCLDBUDT and
- * LCLDBUD_VERTINT switch on, with LCLDBUD_TIMEINT and LBUD23 as in the
- * reference: the same arrays, then the inputs only the budgets read (PVFA,
- * PDYNA, PDYNL, PDYNI, PDYNS, PHRSW, PHRLW, KCTOP, KPBLTYPE; those of sections
- * that are off may be NULL) and PEXTRA (NPROMA, KLEV, KFLDX, NGPBLKS), INOUT:
- * the diagnostics are added to it.  CLOUDSC_E_SHAPE when KFLDX is below the
+ * cloudsc_b200_batched (FP64) with the optional configurations: the cloud
+ * budget diagnostics (cloudsc.F90:3832-4110) that LCLDBUDC, LCLDBUDL,
+ * LCLDBUDI, LCLDBUDT and LCLDBUD_VERTINT switch on, with LCLDBUD_TIMEINT and
+ * LBUD23 as in the reference; the SPP perturbations (LSPP and the spp_*
+ * fields of cloudsc_params, cloudsc.F90:850-939); the cloud-inhomogeneity
+ * paths (LCLOUD_INHOMOG: autoconversion/accretion enhancement from the
+ * liquid FSD, :1937-2098; LRAD_CLOUD_INHOMOG: PFSD, :3819-3823, 4112-4125,
+ * 4307-4359).  The same arrays as cloudsc_b200_batched, then the inputs
+ * only these read: PVFA, PDYNA, PDYNL, PDYNI, PDYNS, PHRSW, PHRLW (budgets),
+ * PGAW (NPROMA, NGPBLKS; inhomogeneity), KCTOP, KPBLTYPE (vertical-integral
+ * budget), PGP2DSPP (NPROMA, NRFTOTAL, NGPBLKS; SPP), PFSD (NPROMA, KLEV,
+ * NGPBLKS; written with LRAD_CLOUD_INHOMOG), PEXTRA (NPROMA, KLEV, KFLDX,
+ * NGPBLKS, INOUT: the budgets are added to it); arrays of options that are
+ * off may be NULL.  CLOUDSC_E_SHAPE when KFLDX is below the
  * fields the sections need (the reference ABORTs, cloudsc.F90:3945-4106) or,
- * with the vertical integral, KLEV < 84.  With no budget switch on it is
- * cloudsc_b200_batched at FP64.  Budgets are also written by
- * cloudsc_b200_block (its PEXTRA/KFLDX arguments); cloudsc_b200_batched,
- * cloudsc_b200_batched_host and cloudsc_b200_block_noalloc return
- * CLOUDSC_E_UNSUPPORTED when a budget switch is on.  No reference
+ * with the vertical integral, KLEV < 84, or an SPP field pointer is outside
+ * 1..NRFTOTAL.  With no option on it is cloudsc_b200_batched at FP64.  The
+ * options also work through cloudsc_b200_block (its own arguments);
+ * cloudsc_b200_batched, cloudsc_b200_batched_host and
+ * cloudsc_b200_block_noalloc return
+ * CLOUDSC_E_UNSUPPORTED when one of these options is on.  No reference
  * counterpart beyond the CLOUDSC call itself: this is its batched form.
  */
 int cloudsc_b200_batched_diag(
@@ -368,9 +398,9 @@ int cloudsc_b200_batched_diag(
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur,
     double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
     const double *pvfa, const double *pdyna, const double *pdynl, const double *pdyni,
-    const double *pdyns, const double *phrsw, const double *phrlw, const int32_t *kctop,
-    const int32_t *kpbltype, double *pextra, int32_t kfldx, uint32_t *ncounters,
-    void *stream);
+    const double *pdyns, const double *phrsw, const double *phrlw, const double *pgaw,
+    const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp, double *pfsd,
+    double *pextra, int32_t kfldx, uint32_t *ncounters, void *stream);
 
 /* Bytes of the fixed device array cloudsc_b200_block_noalloc works in. */
 size_t cloudsc_b200_block_noalloc_capacity(void);

@@ -63,7 +63,7 @@ def lib():
         L.cloudsc_b200_get_schedule.argtypes = [i32, pi32, pi32, pi32]
         L.cloudsc_b200_get_schedule.restype = ctypes.c_int
         L.cloudsc_b200_batched_diag.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
-                                                [vp] * (len(BATCHED_FIELDS) + 10) + [i32, vp, vp])
+                                                [vp] * (len(BATCHED_FIELDS) + 13) + [i32, vp, vp])
         L.cloudsc_b200_batched_diag.restype = ctypes.c_int
         from .fields import SATADJ_FIELDS
         ns = len(SATADJ_FIELDS)
@@ -282,14 +282,15 @@ def sltend_supersat_batched(params, arrays, nproma, klev, ngpblks, ngptot, tsphy
 
 
 def cloudsc_batched_diag(params, arrays, diag, nproma, klev, ngpblks, ngptot, ptsphy, counter=None, stream=None):
-    """cloudsc_batched (FP64) with the cloud budget diagnostics the params
-    switch on (LCLDBUDC/L/I/T, LCLDBUD_VERTINT): ``diag`` holds the
-    fields.DIAG_FIELDS device tensors; PEXTRA, (NGPBLKS, KFLDX, KLEV, NPROMA),
-    is added to in place."""
+    """cloudsc_batched (FP64) with the optional configurations the params
+    switch on (budget diagnostics, SPP, cloud inhomogeneity): ``diag`` holds
+    the fields.DIAG_FIELDS device tensors (those of options that are off may
+    be omitted); PEXTRA, (NGPBLKS, KFLDX, KLEV, NPROMA), is added to and PFSD
+    written in place."""
     from .fields import DIAG_FIELDS
     ptrs = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
     dptrs = [_ptr(diag.get(n)) for n, *_ in DIAG_FIELDS]
-    kfldx = int(diag["pextra"].shape[1])
+    kfldx = int(diag["pextra"].shape[1]) if diag.get("pextra") is not None else 0
     cnt = _ptr(counter) if counter is not None else None
     st = stream.cuda_stream if stream is not None else None
     return _check(lib().cloudsc_b200_batched_diag(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),

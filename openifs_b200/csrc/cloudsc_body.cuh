@@ -306,7 +306,11 @@ CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double
 // FP64 only; the budget terms ZBUDCC/ZBUDL/ZBUDI of each level are collected
 // where the reference stores them and written to PEXTRA at the end of the
 // level.  Without BUD none of this code is compiled.
-template <typename Real, bool F32M, bool BUD = false>
+// OPT: the form with the SPP perturbations (LSPP) and the cloud-inhomogeneity
+// paths (LCLOUD_INHOMOG, LRAD_CLOUD_INHOMOG -> PFSD), FP64 only
+// (cloudsc.F90:850-939, 1937-2110, 2282-2348, 2781-2783, 3288-3290,
+// 3819-3823, 4112-4125, 4307-4359).  Without OPT none of this code exists.
+template <typename Real, bool F32M, bool BUD = false, bool OPT = false>
 CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bool active = true) {
   const KParams<Real> &P = KP<Real>();
   const KParamsD &PD = c_kd;
@@ -336,6 +340,29 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
     zadvwd = C(1.0) - P.rmfadvw * P.rmfadvwdd;
   }
   const Real zconstpow = plsm > C(0.5) ? P.zconst_pow_land : P.zconst_pow_sea;
+
+  // SPP: the factors EXP(MU + XMAG*PGP2DSPP(JL,MP)) of this column, one per
+  // perturbation (CLOUDINHOM: two, fields MP and MP+1); grid-box length and
+  // the default FSD for the inhomogeneity paths
+  double sppf[9];
+  double zgridlen = 0.0;
+  const bool spp = OPT && P.lspp;
+  if constexpr (OPT) {
+#pragma unroll
+    for (int n = 0; n < 9; ++n) sppf[n] = 1.0;
+    if (P.lspp) {
+      const double *g = F.pgp2dspp + (size_t)ib * np * F.nrftotal + jl;
+#pragma unroll 1
+      for (int n = 0; n < 8; ++n)
+        if (P.spp_on[n]) sppf[n] = xexp(double(P.spp_mu[2 * n]) + double(P.spp_xmag[2 * n]) * ld(g + (size_t)(P.spp_mp[n] - 1) * np));
+      if (P.spp_on[CLOUDSC_SPP_CLOUDINHOM])
+        sppf[8] = xexp(double(P.spp_mu[2 * CLOUDSC_SPP_CLOUDINHOM + 1]) +
+                       double(P.spp_xmag[2 * CLOUDSC_SPP_CLOUDINHOM + 1]) *
+                           ld(g + (size_t)P.spp_mp[CLOUDSC_SPP_CLOUDINHOM] * np));
+    }
+    if (P.lcloud_inhomog || P.lrad_cloud_inhomog)
+      zgridlen = 2 * double(P.ra) * xsqrt(double(P.rpi) * ld(F.pgaw + o1)) * 0.001;  // :1944
+  }
 
   // state carried between levels
   D paph_k = ld(F.paph + o2h);
@@ -461,6 +488,9 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       icefrac = C(1.0) - liqfrac;
     }
 
+    // FSD bookkeeping of this level (ZLFSD, ZANEWP, ZRATFSD, ZICEF, ZLIQF;
+    // initial values :942-954)
+    double lfsd = double(P.rcloud_frac_std), anewp = 0.0, ratfsd = 0.0, icef = 0.0, liqf = 0.0;
     D loc_a = 0.0, loc_cl = 0.0, loc_ci = 0.0, loc_cr = 0.0, loc_cs = 0.0;
     D qxn2d_l = 0.0, qxn2d_i = 0.0, qxn2d_r = 0.0, qxn2d_s = 0.0;
     Real pfplsx_i_n = C(0.0), pfplsx_r_n = C(0.0), pfplsx_s_n = C(0.0);
@@ -626,6 +656,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       // 3.4 erosion, ITURBEROSION=3 (:1689-1754)
       {
         Real zldifdt = P.rcldiff * rdt;
+        if (spp && P.spp_on[CLOUDSC_SPP_RCLDIFF]) zldifdt = P.rcldiff * rdt * Real(sppf[CLOUDSC_SPP_RCLDIFF]);
         Real pl = Real(plude_k);
         if (ktype >= 2 && pl > zepsec && peis < C(10.0)) {
           zldifdt = C(20.0) * P.rcldiff_convi * zldifdt;
@@ -651,7 +682,9 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       }
 
       // 4.1 fall speeds (:1783-1844), sedimentation (:1852-1877)
-      const Real fs_i = P.rvice, fs_s = P.rvsnow;
+      const Real fs_i = (spp && P.spp_on[CLOUDSC_SPP_FALLSPEED]) ? P.rvice * Real(sppf[CLOUDSC_SPP_FALLSPEED])
+                                                                 : P.rvice;  // :1806-1808
+      const Real fs_s = P.rvsnow;
       Real fs_r = C(0.0);
       {
         Real ztemp = C(0.5) * (qr + qxnm1_r);
@@ -703,11 +736,46 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       // 4.3 warm rain, IWARMRAIN=3, IRAINACC=1 (:1930-2259)
       if (zliqcld > zepsec) {
         const PowBase b_liq = mbase<F32M>(zliqcld);
-        Real zrainaut = P.rcl_inhomogaut * rdt * P.rcl_kkaau * mpowb<F32M>(b_liq, P.kkbauq_m1) * zconstpow;
+        Real zeaut = P.rcl_inhomogaut, zeacc = P.rcl_inhomogacc;
+        if constexpr (OPT) {
+          double zcldraincorr = 0.0;
+          if (P.lcloud_inhomog || P.lrad_cloud_inhomog) {  // :1937-1967
+            const double zqtot = mn((qvD + qlD) * 1000.0, 30.0);
+            zcldraincorr = 1.0 - 0.8 * double(a);
+            const double zphip1 = .2 + .01 * zqtot + .0027 * (zqtot * zqtot) - .00008 * (zqtot * zqtot * zqtot);
+            const double zphip2 = zphip1 - 0.2;
+            const double zphip3 = 0.123 * xexp(-zphip1 * 0.55);
+            const double zanew2 = mx(double(a), 0.1);
+            const double zphic = xpow(zgridlen * zanew2, 1.0 / 3.0) *
+                                 xpow(xpow(zphip3 * zgridlen * zanew2, 1.5) + 3.0 * zphip3, -0.17);
+            double zfracsdc = (zphip1 - zphip2 * zanew2) * zphic;
+            if (double(a) > 0.95) zfracsdc = 0.17 * zphic;
+            lfsd = 1.3 * zfracsdc;
+          }
+          if (P.lcloud_inhomog) {  // :2075-2098
+            const double aa = double(a);
+            const double fc2 = xpow(lfsd, 2.0);
+            const double zea = xpow(1.0 + fc2, (double(P.rcl_kkbauq) - 1.0) * double(P.rcl_kkbauq) / 2.0);
+            const double zphir = xpow(zgridlen * aa, 1.0 / 3.0) * xpow(xpow(0.11 * zgridlen * aa, 1.14) + 1.0, -0.22);
+            double zfracsdr = (1.1 - 0.8 * aa) * zphir;
+            if (aa > 0.95) zfracsdr = 0.3 * zphir;
+            const double fr2 = xpow(zfracsdr, 2.0);
+            const double kb = double(P.rcl_kkbac);
+            const double zec = xpow(1.0 + fc2, (kb - 1.0) * kb / 2.0) * xpow(1.0 + fr2, (kb - 1.0) * kb / 2.0) *
+                               xexp(zcldraincorr * kb * kb * xsqrt(xlog(1.0 + fc2) * xlog(1.0 + fr2)));
+            zeaut = Real(zea);
+            zeacc = Real(zec);
+          }
+          if (spp && P.spp_on[CLOUDSC_SPP_CLOUDINHOM]) {  // :2106-2109
+            zeaut = zeaut * Real(sppf[CLOUDSC_SPP_CLOUDINHOM]);
+            zeacc = zeacc * Real(sppf[8]);
+          }
+        }
+        Real zrainaut = zeaut * rdt * P.rcl_kkaau * mpowb<F32M>(b_liq, P.kkbauq_m1) * zconstpow;
         qb_rl = qb_rl + zrainaut;
         Real zrainacc = C(0.0);
         if (zraincld > zepsec) {
-          zrainacc = P.rcl_inhomogacc * rdt * P.rcl_kkaac * mpowb<F32M>(b_liq, P.kkbac_m1) *
+          zrainacc = zeacc * rdt * P.rcl_kkaac * mpowb<F32M>(b_liq, P.kkbac_m1) *
                      mpow<F32M>(zraincld, P.rcl_kkbac);
         }
         qb_rl = qb_rl + zrainacc;
@@ -721,11 +789,16 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       {
         Real zzrh = P.rprecrhmax + (C(1.0) - P.rprecrhmax) * zcovpmax / mx(zepsec, C(1.0) - a);
         zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
-        Real zrhc = P.ramid;
+        Real zxramid = P.ramid;
+        if (spp && P.spp_on[CLOUDSC_SPP_RAMID]) {  // :2282-2287
+          zxramid = P.ramid * Real(sppf[CLOUDSC_SPP_RAMID]);
+          if (P.spp_lramidlimit1) zxramid = mn(C(1.0), zxramid);
+        }
+        Real zrhc = zxramid;
         Real zsigk = pap_k / Real(paph_surf);
         if (zsigk > C(0.8)) {
           Real s = (zsigk - C(0.8)) / C(0.2);
-          zrhc = P.ramid + (C(1.0) - P.ramid) * (s * s);
+          zrhc = zxramid + (C(1.0) - zxramid) * (s * s);
         }
         zzrh = mn(zrhc, zzrh);
         zzrh = mn(C(0.9), zzrh);
@@ -746,6 +819,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
                             (mpow<F32M>(zcorr2, C(0.5)) * mpowb<F32M>(b_lam, P.rcl_const3r)));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
           Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
+          if (spp && P.spp_on[CLOUDSC_SPP_RAINEVAP]) zdpevap = zdpevap * Real(sppf[CLOUDSC_SPP_RAINEVAP]);
           D zevap = mn(D(zdpevap), qxfg_r);
           QSUB(RV, zevap);  // (V,R) += zevap, (R,V) -= zevap
           if constexpr (BUD) bd.l[20] = -zevap * zqtmst;  // :2363
@@ -813,7 +887,9 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
       // 4.8 ice -> snow autoconversion (:2769-2800)
       if (t <= P.rtt && zicecld > zepsec) {
         Real zzco = rdt * P.rsnowlin1 * mexp<F32M>(P.rsnowlin2 * (t - P.rtt));
-        Real r = zicecld / P.rlcritsnow;
+        Real zlcrit = P.rlcritsnow;
+        if (spp && P.spp_on[CLOUDSC_SPP_RLCRITSNOW]) zlcrit = P.rlcritsnow * Real(sppf[CLOUDSC_SPP_RLCRITSNOW]);
+        Real r = zicecld / zlcrit;
         Real ztemp = C(-1.) * (r * r);
         Real zsnowaut = (ztemp < C(50.0)) ? zzco * (C(1.0) - mexp<F32M>(ztemp)) : zzco;
         qb_si = qb_si + zsnowaut;
@@ -939,6 +1015,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsice;
           Real zdpr = zcovpclr * zbeta * (zqsice - zqe) / zdenom * zdp * P.zrg_r;
           Real zdpevap = zdpr * zdtgdp;
+          if (spp && P.spp_on[CLOUDSC_SPP_SNOWSUBLIM]) zdpevap = zdpevap * Real(sppf[CLOUDSC_SPP_SNOWSUBLIM]);
           D zevap = mn(D(zdpevap), qxfg_s);
           QSUB(SV, zevap);  // (V,S) += zevap, (S,V) -= zevap
           if constexpr (BUD) bd.i[17] = -zevap * zqtmst;  // :3304
@@ -1106,6 +1183,18 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         }
       }
       covp_out = zcovptot;
+      if constexpr (OPT) {
+        if (P.lrad_cloud_inhomog) {
+          const double pda = pa_k + zda;  // :3819-3823
+          if (pda > 0.001) anewp = mx(mx(pda, double(covp_out)), 0.1);
+          if (q0_l + q0_i + plude_k > double(P.rlmin)) {  // :4112-4125
+            ratfsd = plude_k / (plude_k + q0_l + q0_i);
+            ratfsd = mx(0.0, mn(1.0, ratfsd));
+          }
+          icef = x_i;
+          liqf = x_l;
+        }
+      }
       if constexpr (BUD) {
         // inputs a section that is off does not read may be NULL
         auto opt = [&](const double *q) { return q ? ld(q + ok) : 0.0; };
@@ -1118,6 +1207,32 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
                         opti(F.kpbltype), opti(F.kctop), double(peis));
       }
     }  // k >= ncldtop0
+
+    // ice/liquid FSD of level k (:4307-4359), every level; the binary32
+    // literals written as such at :4316,4321-4322 are their float values
+    if constexpr (OPT) {
+      if (P.lrad_cloud_inhomog) {
+        const double zifsdback = 0.446585 * xpow(zgridlen, 1.0 / 3.0) * xpow(xpow(0.308061 * zgridlen, 0.395736) + 1.0, -0.744527);
+        const double zqtot = mx(mn((qvD + qiD) * 1000.0, 30.0), double(0.00001f));
+        const double zrho_f = pap_kd / (double(P.rd) * tD);
+        double zdelz = 1.0 / (double(P.rg) * zrho_f) * (paph_k1 - paph_k) * 0.001;
+        zdelz = mx(mn(zdelz, double(0.5f)), double(0.001f));
+        const double zphi = xpow(zdelz / double(0.24f), double(0.11f)) * xpow(zqtot / double(10.f), double(0.03f));
+        double zifsd = double(P.rcloud_frac_std);
+        if (anewp > 0.95) {
+          zifsd = zifsdback * zphi;
+          zifsd = 1.3 * (zifsd + ratfsd * 1.5);
+        } else if (anewp > 0.001 && anewp <= 0.95) {
+          zifsd = zifsdback * zphi * 1.5;
+          zifsd = 1.3 * (zifsd + ratfsd * 1.5);
+        }
+        double zfsd = double(P.rcloud_frac_std);
+        if (icef > zepsecd) zfsd = zifsd;
+        if (liqf > 0.0 && icef <= zepsecd) zfsd = lfsd;
+        zfsd = mn(mx(0.1, zfsd), 3.575);
+        if (active) F.pfsd[ok] = zfsd;
+      }
+    }
 
     // ---------------- outputs of level k ----------------
     if (active) {

@@ -63,8 +63,32 @@ int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
 
 bool params_supported(const cloudsc_params &p) {
   if (p.laericeauto || p.laericesed || p.laerliqautolsp || p.laerliqcoll) return false;
-  if (p.lcloud_inhomog || p.lrad_cloud_inhomog || p.lspp) return false;
   return true;
+}
+
+// SPP or a cloud-inhomogeneity path is on: the FP64 form with them runs.
+bool opt_on(const cloudsc_params &p) { return p.lspp || p.lcloud_inhomog || p.lrad_cloud_inhomog; }
+
+// Inputs of the SPP / inhomogeneity form: PGP2DSPP (KLON, NRFTOTAL) when a
+// perturbation is on (its MP, and MP+1 for CLOUDINHOM, within NRFTOTAL),
+// PGAW with an inhomogeneity path, PFSD with LRAD_CLOUD_INHOMOG.
+int opt_args_ok(const cloudsc_params &p, const void *pgaw, const void *pgp2dspp, const void *pfsd) {
+  if (p.lspp)
+    for (int n = 0; n < 8; ++n) {
+      if (!p.spp_on[n]) continue;
+      if (!pgp2dspp) return fail(CLOUDSC_E_NULL, "an SPP perturbation is on: PGP2DSPP is required");
+      if (p.spp_mp[n] < 1 || p.spp_mp[n] + (n == CLOUDSC_SPP_CLOUDINHOM ? 1 : 0) > p.spp_nrftotal)
+        return fail(CLOUDSC_E_SHAPE, "an SPP field pointer MP is outside 1..NRFTOTAL");
+    }
+  if ((p.lcloud_inhomog || p.lrad_cloud_inhomog) && !pgaw)
+    return fail(CLOUDSC_E_NULL, "the cloud-inhomogeneity paths need PGAW");
+  if (p.lrad_cloud_inhomog && !pfsd) return fail(CLOUDSC_E_NULL, "LRAD_CLOUD_INHOMOG writes PFSD");
+  return CLOUDSC_OK;
+}
+
+bool current_opt_on() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_have_params && opt_on(g_params);
 }
 
 // The cloud budget diagnostics (LCLDBUD*, cloudsc.F90:3832-4110) are on: the
@@ -439,11 +463,14 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
     sc = g_sched[precision];
   }
   int form = precision;
-  if (current_budgets_on()) {
-    if (precision != 0) return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics are FP64 only");
-    if (!f.pextra) return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use "
-                                                      "cloudsc_b200_batched_diag or cloudsc_b200_block");
-    form = 3;
+  const bool bud = current_budgets_on(), opt = current_opt_on();
+  if (bud || opt) {
+    if (precision != 0)
+      return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics, SPP and the inhomogeneity paths are FP64 only");
+    if (bud && !f.pextra)
+      return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_batched_diag "
+                                         "or cloudsc_b200_block");
+    form = bud && opt ? 5 : (opt ? 4 : 3);
   }
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + sc.threads - 1) / sc.threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
@@ -469,6 +496,9 @@ int cloudsc_b200_batched(
   int rc = check_params_match(p);
   if (rc) return rc;
   if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
+  if (budgets_on(*p) || opt_on(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_batched_diag "
+                                       "or cloudsc_b200_block");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
     return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
@@ -507,8 +537,9 @@ int cloudsc_b200_batched_diag(
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
     double *pfplsn, double *pfhpsl, double *pfhpsn, const double *pvfa, const double *pdyna,
     const double *pdynl, const double *pdyni, const double *pdyns, const double *phrsw,
-    const double *phrlw, const int32_t *kctop, const int32_t *kpbltype, double *pextra,
-    int32_t kfldx, uint32_t *ncounters, void *stream) {
+    const double *phrlw, const double *pgaw, const int32_t *kctop, const int32_t *kpbltype,
+    const double *pgp2dspp, double *pfsd, double *pextra, int32_t kfldx, uint32_t *ncounters,
+    void *stream) {
   int rc = check_params_match(p);
   if (rc) return rc;
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
@@ -529,6 +560,10 @@ int cloudsc_b200_batched_diag(
                         kpbltype);
     if (rc) return rc;
   }
+  if (opt_on(*p)) {
+    rc = opt_args_ok(*p, pgaw, pgp2dspp, pfsd);
+    if (rc) return rc;
+  }
   rc = ensure_params(nullptr);
   if (rc) return rc;
   Fields f = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
@@ -536,7 +571,8 @@ int cloudsc_b200_batched_diag(
               pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu, pmfd, pa,
               pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng, pfsqrf, pfsqsf,
               pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl, pfhpsn, ncounters,
-              pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop, kpbltype, pextra, kfldx};
+              pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop, kpbltype, pextra, kfldx,
+              pgaw, pgp2dspp, pfsd, p->spp_nrftotal};
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
   return launch_checked(0, f, sh, (cudaStream_t)stream);
 }
@@ -740,8 +776,8 @@ int cloudsc_b200_block(
     double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
     double *pfplsn, double *pfhpsl, double *pfhpsn, double *pextra, int32_t kfldx) {
-  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)pgaw; (void)pgp2dspp; (void)ldslphy;
-  (void)plcrit_aer; (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice; (void)pfsd;
+  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)ldslphy; (void)plcrit_aer;
+  (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice;
   int rc = check_params_match(p);
   if (rc) return rc;
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
@@ -756,10 +792,14 @@ int cloudsc_b200_block(
                           pfhpsn};
   for (const void *q : host)
     if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
-  const bool bud = budgets_on(*p);
+  const bool bud = budgets_on(*p), opt = opt_on(*p);
   if (bud) {
     rc = budget_args_ok(*p, klev, kfldx, pextra, pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop,
                         kpbltype);
+    if (rc) return rc;
+  }
+  if (opt) {
+    rc = opt_args_ok(*p, pgaw, pgp2dspp, pfsd);
     if (rc) return rc;
   }
   int dev = 0;
@@ -771,7 +811,11 @@ int cloudsc_b200_block(
   const size_t s2b = np * kl * 8, nx = bud ? (size_t)kfldx : 0;
   const size_t base = (bytes + 255) / 256 * 256;
   const size_t extra = bud ? 7 * s2b + 2 * ((np * 4 + 255) / 256 * 256) + nx * s2b : 0;
-  rc = t_ws.prepare(dev, base + extra);
+  // with SPP / inhomogeneity: PGAW, PGP2DSPP (KLON, NRFTOTAL), PFSD after that
+  const size_t nrf = opt && p->lspp ? (size_t)p->spp_nrftotal : 0;
+  const size_t gawb = (np * 8 + 255) / 256 * 256, sppb = (np * nrf * 8 + 255) / 256 * 256;
+  const size_t extra2 = opt ? gawb + sppb + s2b : 0;
+  rc = t_ws.prepare(dev, base + extra + extra2);
   if (rc) return rc;
   void *d[42];
   carve(t_ws.buf, np, kl, 1, d);
@@ -803,6 +847,20 @@ int cloudsc_b200_block(
     f.kfldx = kfldx;
     if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
   }
+  double *dfsd = nullptr;
+  if (opt) {
+    char *b = t_ws.buf + base + extra;
+    f.pgaw = pgaw ? (const double *)b : nullptr;
+    if (pgaw) e = cudaMemcpyAsync(b, pgaw, np * 8, cudaMemcpyHostToDevice, s);
+    b += gawb;
+    f.pgp2dspp = (pgp2dspp && nrf) ? (const double *)b : nullptr;
+    if (e == cudaSuccess && pgp2dspp && nrf) e = cudaMemcpyAsync(b, pgp2dspp, np * nrf * 8, cudaMemcpyHostToDevice, s);
+    b += sppb;
+    dfsd = pfsd ? (double *)b : nullptr;
+    f.pfsd = dfsd;
+    f.nrftotal = p->spp_nrftotal;
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  }
   Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
   rc = launch_checked(0, f, sh, s);
   if (rc) return rc;
@@ -816,6 +874,8 @@ int cloudsc_b200_block(
   }
   if (bud && e == cudaSuccess)  // PEXTRA(KIDIA:KFDIA, :, :)
     e = cudaMemcpy2DAsync(pextra + c0, np * 8, dx + c0, np * 8, ncol * 8, kl * nx, cudaMemcpyDeviceToHost, s);
+  if (dfsd && e == cudaSuccess)  // PFSD(KIDIA:KFDIA, :)
+    e = cudaMemcpy2DAsync(pfsd + c0, np * 8, dfsd + c0, np * 8, ncol * 8, kl, cudaMemcpyDeviceToHost, s);
   uint32_t nwarn = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -839,8 +899,9 @@ int cloudsc_b200_batched_host(
   int rc = check_params_match(p);
   if (rc) return rc;
   if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
-  if (budgets_on(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_block");
+  if (budgets_on(*p) || opt_on(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_block "
+                                       "or cloudsc_b200_batched_diag");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
     return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
@@ -956,8 +1017,9 @@ int cloudsc_b200_block_noalloc(
     double *pfplsn, double *pfhpsl, double *pfhpsn, void *stream) {
   int rc = check_params_match(p);
   if (rc) return rc;
-  if (budgets_on(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_block");
+  if (budgets_on(*p) || opt_on(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_block "
+                                       "or cloudsc_b200_batched_diag");
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
     return fail(CLOUDSC_E_SHAPE, "inconsistent KIDIA/KFDIA/KLON/KLEV");
   if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");

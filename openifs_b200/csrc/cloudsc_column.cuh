@@ -62,9 +62,11 @@ CSC_DEV T mx(T a, T b) { return a > b ? a : b; }
 // host test builds only: the system libm, to measure libm sensitivity
 CSC_DEV double xexp(double x) { return exp(x); }
 CSC_DEV double xpow(double x, double y) { return pow(x, y); }
+CSC_DEV double xlog(double x) { return log(x); }
 #else
 CSC_DEV double xexp(double x) { return plibm_exp(x); }
 CSC_DEV double xpow(double x, double y) { return plibm_pow(x, y); }
+CSC_DEV double xlog(double x) { return plibm_log(x); }
 #endif
 // FP32 transcendentals of the FP32-mixed kernel: on the GPU the special-
 // function-unit forms (__expf, __powf: one ex2 / lg2 each, relative error of a
@@ -159,6 +161,10 @@ struct KParams {
   // cloud budget diagnostics (cloudsc.F90:3832-4110)
   Real ralfdcp, reisthsc;
   int lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint, lcldbud_timeint, lbud23;
+  // SPP perturbations and the cloud-inhomogeneity/FSD path (:850-939,
+  // 1937-2110, 4307-4359)
+  Real ra, rcloud_frac_std, spp_mu[16], spp_xmag[16];
+  int lspp, lcloud_inhomog, lrad_cloud_inhomog, spp_lramidlimit1, spp_on[8], spp_mp[8];
   int ncldtop, lmfdsnow;
 };
 

@@ -39,6 +39,11 @@ struct Fields {
   const int32_t *kctop, *kpbltype;
   double *pextra;  // PEXTRA (NPROMA, KLEV, KFLDX) per block, INOUT
   int kfldx;
+  // read only by the SPP / cloud-inhomogeneity form
+  const double *pgaw;      // (NPROMA) per block
+  const double *pgp2dspp;  // (NPROMA, NRFTOTAL) per block
+  double *pfsd;            // (NPROMA, KLEV) per block, written with LRAD_CLOUD_INHOMOG
+  int nrftotal;
 };
 
 // Pointers of the batched CLOUD_SATADJ arrays (same block layout).

@@ -60,6 +60,8 @@ namespace cloudsc {
 //   0  FP64, the reference's double build;
 //   1  FP32-mixed: FP32 transcendentals, everything else in double;
 //   3  FP64 with the cloud budget diagnostics (LCLDBUD*: PEXTRA written);
+//   4  FP64 with the SPP perturbations and the cloud-inhomogeneity paths;
+//   5  FP64 with both (3 and 4);
 //   2  FP32 physics: the process rates in FP32 as well (Real = float); the
 //      state, the sink limiters, the 5x5 solve, CLOUD_SUPERSATCHECK and the
 //      tendency and flux budgets stay in double.  Float rounding of the rates
@@ -88,8 +90,8 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
     }
     if constexpr (FORM == 2)
       cloudsc_column<float, true>(F, sh, ib, jl, active);
-    else if constexpr (FORM == 3)
-      cloudsc_column<double, false, true>(F, sh, ib, jl, active);
+    else if constexpr (FORM >= 3)
+      cloudsc_column<double, false, FORM == 3 || FORM == 5, FORM >= 4>(F, sh, ib, jl, active);
     else
       cloudsc_column<double, FORM == 1>(F, sh, ib, jl, active);
   }
@@ -248,6 +250,8 @@ static const void *kernel_ptr(int precision, int v) {
     case 1: return kernel_ptr_form<1>(v);
     case 2: return kernel_ptr_form<2>(v);
     case 3: return kernel_ptr_form<3>(v);
+    case 4: return kernel_ptr_form<4>(v);
+    case 5: return kernel_ptr_form<5>(v);
     default: return nullptr;
   }
 }

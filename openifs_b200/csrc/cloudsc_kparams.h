@@ -42,6 +42,20 @@ inline void fill_kparams(const cloudsc_params &p, const Derived &d, KParams<Real
   k.lcldbud_vertint = p.lcldbud_vertint;
   k.lcldbud_timeint = p.lcldbud_timeint;
   k.lbud23 = p.lbud23;
+  k.ra = Real(p.ra);
+  k.rcloud_frac_std = Real(p.rcloud_frac_std);
+  for (int i = 0; i < 16; ++i) {
+    k.spp_mu[i] = Real(p.spp_mu[i]);
+    k.spp_xmag[i] = Real(p.spp_xmag[i]);
+  }
+  k.lspp = p.lspp;
+  k.lcloud_inhomog = p.lcloud_inhomog;
+  k.lrad_cloud_inhomog = p.lrad_cloud_inhomog;
+  k.spp_lramidlimit1 = p.spp_lramidlimit1;
+  for (int i = 0; i < 8; ++i) {
+    k.spp_on[i] = p.spp_on[i];
+    k.spp_mp[i] = p.spp_mp[i];
+  }
   k.ncldtop = p.ncldtop;
   k.lmfdsnow = p.lmfdsnow;
 }

@@ -23,6 +23,7 @@
  *           with a fused multiply-add; ln x = e ln2 + (-ln INVC_j) + ln(1+r),
  *           ln(1+r) by its series to r^7/7 (absolute truncation < 2^-64),
  *           summed as a double-double.
+ *   log(x) = the high part of that double-double (for the one LOG CLOUDSC calls).
  *   pow(x,y) = exp(y ln x) with y ln x a double-double whose low part enters
  *           the reduced exp argument; exponents 0.5, 1.5, 2 and 3 are
  *           evaluated as sqrt(x), x*sqrt(x), x*x, x*x*x.
@@ -235,6 +236,15 @@ PLIBM_FN double plibm_pow_with_log(double x, double y, double lhi, double llo) {
 
 /* True when pow(x, y) does not need ln x (an exact-operation exponent). */
 PLIBM_FN int plibm_pow_is_direct(double y) { return y == 0.5 || y == 1.5 || y == 2.0 || y == 3.0; }
+
+/* ln(x) for finite x > 0: the rounded sum of plibm_log_dd's double-double
+ * (within 1 ulp).  CLOUDSC's cloud-inhomogeneity path calls it with
+ * arguments >= 1 (cloudsc.F90:2096). */
+PLIBM_FN double plibm_log(double x) {
+  double h, l;
+  plibm_log_dd(x, &h, &l);
+  return h;
+}
 
 PLIBM_FN double plibm_pow(double x, double y) {
   double lhi = 0.0, llo = 0.0;

@@ -208,10 +208,13 @@ def sltend_bytes_per_column(klev=137, ncldtop=15, fp=8):
     return 12 * nlev * fp, 8 * nlev * fp
 
 
-# The arrays that only the cloud budget diagnostics read (LCLDBUDC/L/I/T,
-# LCLDBUD_VERTINT; cloudsc.F90:3832-4110), in the argument order of
-# cloudsc_b200_batched_diag after the BATCHED_FIELDS arrays.  PEXTRA is
-# (KLON, KLEV, KFLDX) per block: numpy shape (NGPBLKS, KFLDX, KLEV, NPROMA).
+# The arrays that only the optional configurations read or write -- the
+# cloud budget diagnostics (LCLDBUDC/L/I/T, LCLDBUD_VERTINT;
+# cloudsc.F90:3832-4110), SPP (LSPP) and the cloud-inhomogeneity paths
+# (LCLOUD_INHOMOG, LRAD_CLOUD_INHOMOG) -- in the argument order of
+# cloudsc_b200_batched_diag after the BATCHED_FIELDS arrays.  PGP2DSPP is
+# (KLON, NRFTOTAL) per block: numpy shape (NGPBLKS, NRFTOTAL, NPROMA); PEXTRA
+# is (KLON, KLEV, KFLDX) per block: numpy shape (NGPBLKS, KFLDX, KLEV, NPROMA).
 DIAG_FIELDS = [
     ("pvfa", "2d", np.float64, "in"),
     ("pdyna", "2d", np.float64, "in"),
@@ -220,8 +223,11 @@ DIAG_FIELDS = [
     ("pdyns", "2d", np.float64, "in"),
     ("phrsw", "2d", np.float64, "in"),
     ("phrlw", "2d", np.float64, "in"),
+    ("pgaw", "1d", np.float64, "in"),
     ("kctop", "1d", np.int32, "in"),
     ("kpbltype", "1d", np.int32, "in"),
+    ("pgp2dspp", "spp", np.float64, "in"),
+    ("pfsd", "2d", np.float64, "out"),
     ("pextra", "extra", np.float64, "inout"),
 ]
 

@@ -262,14 +262,16 @@ def sltend_from(base, nproma, klev=KLEV_L137, seed=1, blocks=None):
     return out
 
 
-def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None):
+def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None, nrftotal=10):
     """The inputs only the cloud budget diagnostics read (fields.DIAG_FIELDS)
     for the blocks of an existing ``generate`` result ``base``, from
     ``default_rng([seed, ib, 13])``: PVFA ~ N(0, 1e-5 /s); PDYNA ~ N(0, 1e-5
     /s); PDYNL/I/S ~ the species' amount times N(0, 1e-5 /s); PHRSW ~ U(0,
     2e-5 K/s), PHRLW ~ N(-2e-5, 1e-5 K/s); KCTOP a level index 1..KLEV on the
     convective columns, 0 elsewhere; KPBLTYPE in 0..3; PEXTRA ~ N(0, 1) (it is
-    INOUT: the diagnostics add to it)."""
+    INOUT: the diagnostics add to it); PGAW ~ U(1e-7, 3e-6) (grid boxes of
+    about 7-40 km); PGP2DSPP ~ N(0, 1) on ``nrftotal`` fields; PFSD zero (an
+    output)."""
     nb = base["pt"].shape[0]
     ids = list(range(nb)) if blocks is None else list(blocks)
     shp2 = (nb, klev, nproma)
@@ -277,6 +279,9 @@ def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None):
     out["kctop"] = np.zeros((nb, nproma), np.int32)
     out["kpbltype"] = np.zeros((nb, nproma), np.int32)
     out["pextra"] = np.zeros((nb, kfldx, klev, nproma))
+    out["pgaw"] = np.zeros((nb, nproma))
+    out["pgp2dspp"] = np.zeros((nb, nrftotal, nproma))
+    out["pfsd"] = np.zeros(shp2)
     for j, ib in enumerate(ids):
         rng = np.random.default_rng([int(seed), int(ib), 13])
         shp = (klev, nproma)
@@ -291,6 +296,8 @@ def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None):
         out["kctop"][j] = np.where(conv, rng.integers(1, klev + 1, nproma), 0).astype(np.int32)
         out["kpbltype"][j] = rng.integers(0, 4, nproma).astype(np.int32)
         out["pextra"][j] = rng.normal(0.0, 1.0, (kfldx, klev, nproma))
+        out["pgaw"][j] = rng.uniform(1e-7, 3e-6, nproma)
+        out["pgp2dspp"][j] = rng.normal(0.0, 1.0, (nrftotal, nproma))
     return out
 
 

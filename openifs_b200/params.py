@@ -29,7 +29,12 @@ def _parse_fields(path=_HDR):
             continue
         typ, rest = stmt.split(None, 1)
         for name in rest.split(","):
-            fields.append((name.strip(), _CTYPES[typ]))
+            name = name.strip()
+            m = re.fullmatch(r"(\w+)\[(\d+)\]", name)
+            if m:  # a one-dimensional array member
+                fields.append((m.group(1), _CTYPES[typ] * int(m.group(2))))
+            else:
+                fields.append((name, _CTYPES[typ]))
     return fields
 
 
@@ -37,7 +42,11 @@ class CloudscParams(ctypes.Structure):
     _fields_ = _parse_fields()
 
     def as_dict(self):
-        return {n: getattr(self, n) for n, _ in self._fields_}
+        out = {}
+        for n, _ in self._fields_:
+            v = getattr(self, n)
+            out[n] = list(v) if isinstance(v, ctypes.Array) else v
+        return out
 
     def copy(self):
         c = CloudscParams()

@@ -41,6 +41,7 @@
 #include "../openifs_b200/csrc/plibm.h"
 #define exp(x) plibm_exp(x)
 #define pow(x, y) plibm_pow(x, y)
+#define log(x) plibm_log(x)
 #endif
 
 #define NCLV 5
@@ -153,9 +154,16 @@ static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, int kft
 
 static int params_supported(const cloudsc_params *p) {
   if (p->laericeauto || p->laericesed || p->laerliqautolsp || p->laerliqcoll) return 0;
-  if (p->lcloud_inhomog || p->lrad_cloud_inhomog || p->lspp) return 0;
   return 1;
 }
+
+/* SPP factor EXP(MU(i+1) + XMAG(i+1)*PGP2DSPP(JL, MP + off)) of perturbation
+ * n (cloudsc.F90:1692,1807,2106-2107,2283,2347,2782,3289). */
+static double spp_fac(const cloudsc_params *p, const double *pgp2dspp, int klon, int jl, int n, int i,
+                      int off) {
+  return exp(p->spp_mu[2 * n + i] + p->spp_xmag[2 * n + i] * pgp2dspp[(size_t)(p->spp_mp[n] + off - 1) * klon + (jl - 1)]);
+}
+#define SPP_ON(n) (p->lspp && p->spp_on[n])
 
 int oracle_cloudsc(
     const cloudsc_params *p, int kidia, int kfdia, int klon, int klev, int lddiag,
@@ -177,9 +185,8 @@ int oracle_cloudsc(
     double *pfsqsf, double *pfcqrng, double *pfcqsng, double *pfsqltur,
     double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
     double *pextra, int kfldx) {
-  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)pgaw; (void)pgp2dspp;
-  (void)ldslphy; (void)plcrit_aer; (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice;
-  (void)pfsd;
+  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)ldslphy; (void)plcrit_aer;
+  (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice;
 
   if (!p || p->magic != CLOUDSC_PARAMS_MAGIC) return CLOUDSC_E_PARAMS;
   if (!params_supported(p)) return CLOUDSC_E_UNSUPPORTED;
@@ -192,6 +199,18 @@ int oracle_cloudsc(
      PEXTRA fields they need (the reference ABORTs when KFLDX is too small,
      :3945,3970,4007,4048,4106, or KLEV < 60 with the vertical integral,
      :3851; the vertical integral writes level slots up to 83) */
+  /* SPP perturbations and the cloud-inhomogeneity/FSD path (:850-939,
+     1937-1971, 2075-2110, 3819-3823, 4112-4124, 4307-4359) */
+  if (p->lspp) {
+    for (int n = 0; n < 8; n++) {
+      if (!p->spp_on[n]) continue;
+      if (!pgp2dspp || p->spp_mp[n] < 1 || p->spp_mp[n] + (n == 7 ? 1 : 0) > p->spp_nrftotal)
+        return CLOUDSC_E_SHAPE;
+    }
+  }
+  const int linhom = p->lcloud_inhomog || p->lrad_cloud_inhomog;
+  if (linhom && !pgaw) return CLOUDSC_E_NULL;
+  if (p->lrad_cloud_inhomog && !pfsd) return CLOUDSC_E_NULL;
   const int lbud = p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint;
   if (lbud) {
     int need = (p->lbud23 ? 26 : 0) + (p->lcldbud_vertint ? 1 : 0) + (p->lcldbudc ? 12 : 0) +
@@ -231,7 +250,7 @@ int oracle_cloudsc(
   /* 67 (KLON) arrays, 13 (KLON,KLEV) arrays, 4 (KLON,KLEV,NCLV), 1 (KLON,KLEV+1,NCLV),
      13 (KLON,NCLV) and 3 (KLON,NCLV,NCLV); sized with margin */
   double *buf = (double *)calloc(
-      n1 * 140 + n2 * 16 + n2 * NCLV * 4 + n2h * NCLV + n1 * NCLV * 16 + n1 * NCLV * NCLV * 3,
+      n1 * 140 + n2 * 22 + n2 * NCLV * 4 + n2h * NCLV + n1 * NCLV * 16 + n1 * NCLV * NCLV * 3,
       sizeof(double));
   if (!buf) return CLOUDSC_E_TOO_LARGE;
   double *w = buf;
@@ -257,6 +276,8 @@ int oracle_cloudsc(
   double *zi_adj = TAKE(n1);
   /* budget terms ZBUDCC(:,1:12), ZBUDL(:,1:21), ZBUDI(:,1:17), reset per level */
   double *zbudcc = TAKE(n1 * 12), *zbudl = TAKE(n1 * 21), *zbudi = TAKE(n1 * 17);
+  /* FSD arrays (:581-586), initialised at :942-954 */
+  double *zlfsd = TAKE(n2), *zanewp = TAKE(n2), *zratfsd = TAKE(n2), *zicef = TAKE(n2), *zliqf = TAKE(n2);
   int *llrainliq = (int *)TAKE(n1); /* n1 doubles >= n1 ints */
 
   double *ztp1 = TAKE(n2), *zli = TAKE(n2), *za = TAKE(n2), *zaorig = TAKE(n2);
@@ -277,6 +298,8 @@ int oracle_cloudsc(
 #undef TAKE
 
   int jl, jk, jm, jn, jo, ik;
+  for (jk = 1; jk <= klev; jk++) /* :942-954 (the zero arrays are zero from calloc) */
+    for (jl = kidia; jl <= kfdia; jl++) A2(zlfsd, jl, jk) = p->rcloud_frac_std;
 
   /* cloudsc.F90:696-703 */
   for (jl = kidia; jl <= kfdia; jl++) {
@@ -556,6 +579,8 @@ int oracle_cloudsc(
     /* 3.4 erosion, ITURBEROSION=3 (:1689-1754) */
     for (jl = kidia; jl <= kfdia; jl++) {
       A1(zldifdt, jl) = p->rcldiff * ptsphy;
+      if (SPP_ON(CLOUDSC_SPP_RCLDIFF))
+        A1(zldifdt, jl) = p->rcldiff * ptsphy * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_RCLDIFF, 0, 0);
       if (A1(ktype, jl) >= 2 && A2(plude, jl, jk) > zepsec && A1(peis, jl) < 10.0) {
         A1(zldifdt, jl) = 20.0 * p->rcldiff_convi * A1(zldifdt, jl);
       } else if (A1(ktype, jl) == 1 && A2(plude, jl, jk) > zepsec) {
@@ -592,6 +617,9 @@ int oracle_cloudsc(
       double zrlambda = pow(A1(zrho, jl) * ztemp / p->rcl_lam1r, p->rcl_lam2r);
       L2(zfallspeed, jl, NCLDQR) =
           p->rxfallspeedrain * zfallcorr * p->rcl_const7r * pow(zrlambda, p->rcl_dr);
+      if (SPP_ON(CLOUDSC_SPP_FALLSPEED)) /* :1806-1808 */
+        L2(zfallspeed, jl, NCLDQI) =
+            L2(zfallspeed, jl, NCLDQI) * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_FALLSPEED, 0, 0);
     }
     /* sedimentation source/sink (:1852-1877) */
     for (jm = 1; jm <= NCLV; jm++) {
@@ -635,6 +663,24 @@ int oracle_cloudsc(
     /* 4.3 warm rain, IWARMRAIN=3, IRAINACC=1 (:1930-2259) */
     for (jl = kidia; jl <= kfdia; jl++) {
       if (A1(zliqcld, jl) > zepsec) {
+        /* inhomogeneity (:1937-1971) */
+        double zgridlen = 0.0, zcldraincorr = 0.0;
+        if (linhom) {
+          double zqtot = fmin_((A3(zqx, jl, jk, NCLDQV, klev) + A3(zqx, jl, jk, NCLDQL, klev)) * 1000.0, 30.0);
+          zgridlen = 2 * p->ra * sqrt(p->rpi * A1(pgaw, jl)) * 0.001;
+          zcldraincorr = 1.0 - 0.8 * A2(za, jl, jk);
+          double zphip1 = .2 + .01 * zqtot + .0027 * (zqtot * zqtot) - .00008 * (zqtot * zqtot * zqtot);
+          double zphip2 = zphip1 - 0.2;
+          double zphip3 = 0.123 * exp(-zphip1 * 0.55);
+          double zanew2 = fmax_(A2(za, jl, jk), 0.1);
+          double zphic = pow(zgridlen * zanew2, 1.0 / 3.0) *
+                         pow(pow(zphip3 * zgridlen * zanew2, 1.5) + 3.0 * zphip3, -0.17);
+          double zfracsdc = (zphip1 - zphip2 * zanew2) * zphic;
+          if (A2(za, jl, jk) > 0.95) zfracsdc = 0.17 * zphic;
+          A2(zlfsd, jl, jk) = 1.3 * zfracsdc; /* ZR12 */
+        } else {
+          A2(zlfsd, jl, jk) = p->rcloud_frac_std;
+        }
         double zconst, zlcrit;
         if (A1(plsm, jl) > 0.5) {
           zconst = p->rcl_kk_cloud_num_land;
@@ -643,8 +689,24 @@ int oracle_cloudsc(
           zconst = p->rcl_kk_cloud_num_sea;
           zlcrit = p->rclcrit_sea;
         }
-        (void)zlcrit;
+        (void)zlcrit; /* IWARMRAIN=3 reads no threshold: the RCLCRIT perturbation (:2052-2062) has no effect */
         double zeaut = p->rcl_inhomogaut, zeacc = p->rcl_inhomogacc;
+        if (p->lcloud_inhomog) { /* :2075-2098 */
+          double zfracsdc = A2(zlfsd, jl, jk);
+          double zaa = A2(za, jl, jk);
+          zeaut = pow(1.0 + pow(zfracsdc, 2.0), (p->rcl_kkbauq - 1.0) * p->rcl_kkbauq / 2.0);
+          double zphir = pow(zgridlen * zaa, 1.0 / 3.0) * pow(pow(0.11 * zgridlen * zaa, 1.14) + 1.0, -0.22);
+          double zfracsdr = (1.1 - 0.8 * zaa) * zphir;
+          if (zaa > 0.95) zfracsdr = 0.3 * zphir;
+          zeacc = pow(1.0 + pow(zfracsdc, 2.0), (p->rcl_kkbac - 1.0) * p->rcl_kkbac / 2.0) *
+                  pow(1.0 + pow(zfracsdr, 2.0), (p->rcl_kkbac - 1.0) * p->rcl_kkbac / 2.0) *
+                  exp(zcldraincorr * p->rcl_kkbac * p->rcl_kkbac *
+                      sqrt(log(1.0 + pow(zfracsdc, 2.0)) * log(1.0 + pow(zfracsdr, 2.0))));
+        }
+        if (SPP_ON(CLOUDSC_SPP_CLOUDINHOM)) { /* :2106-2109 */
+          zeaut = zeaut * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_CLOUDINHOM, 0, 0);
+          zeacc = zeacc * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_CLOUDINHOM, 1, 1);
+        }
         A1(zrainaut, jl) = zeaut * ptsphy * p->rcl_kkaau * pow(A1(zliqcld, jl), p->rcl_kkbauq - 1.0) *
                            pow(zconst, p->rcl_kkbaun);
         L3(zsolqb, jl, NCLDQR, NCLDQL) = L3(zsolqb, jl, NCLDQR, NCLDQL) + A1(zrainaut, jl);
@@ -662,6 +724,10 @@ int oracle_cloudsc(
       double zzrh = p->rprecrhmax + (1.0 - p->rprecrhmax) * A1(zcovpmax, jl) / fmax_(zepsec, 1.0 - zaa);
       zzrh = fmin_(fmax_(zzrh, p->rprecrhmax), 1.0);
       double zxramid = p->ramid;
+      if (SPP_ON(CLOUDSC_SPP_RAMID)) { /* :2282-2287 */
+        zxramid = p->ramid * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_RAMID, 0, 0);
+        if (p->spp_lramidlimit1) zxramid = fmin_(1.0, zxramid);
+      }
       double zrhc = zxramid;
       double zsigk = A2(pap, jl, jk) / A2(paph, jl, klev + 1);
       if (zsigk > 0.8) {
@@ -689,6 +755,8 @@ int oracle_cloudsc(
                             (pow(zcorr2, 0.5) * pow(zlambda, p->rcl_const3r)));
         double zdenom = 1.0 + zbeta * ptsphy * A1(zcorqsliq, jl);
         double zdpevap = A1(zcovpclr, jl) * zbeta * ptsphy * zsubsat / zdenom;
+        if (SPP_ON(CLOUDSC_SPP_RAINEVAP)) /* :2346-2348 */
+          zdpevap = zdpevap * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_RAINEVAP, 0, 0);
         double zevap = fmin_(zdpevap, L2(zqxfg, jl, NCLDQR));
         L3(zsolqa, jl, NCLDQV, NCLDQR) = L3(zsolqa, jl, NCLDQV, NCLDQR) + zevap;
         L3(zsolqa, jl, NCLDQR, NCLDQV) = L3(zsolqa, jl, NCLDQR, NCLDQV) - zevap;
@@ -772,6 +840,8 @@ int oracle_cloudsc(
         if (A1(zicecld, jl) > zepsec) {
           double zzco = ptsphy * p->rsnowlin1 * exp(p->rsnowlin2 * (t - p->rtt));
           double zlcrit = p->rlcritsnow;
+          if (SPP_ON(CLOUDSC_SPP_RLCRITSNOW)) /* :2781-2783 */
+            zlcrit = p->rlcritsnow * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_RLCRITSNOW, 0, 0);
           double r = A1(zicecld, jl) / zlcrit;
           double ztemp = -1. * (r * r);
           if (ztemp < 50.0) {
@@ -949,6 +1019,8 @@ int oracle_cloudsc(
         double zdenom = 1.0 + zbeta * ptsphy * A1(zcorqsice, jl);
         double zdpr = A1(zcovpclr, jl) * zbeta * (zqsi - zqe) / zdenom * A1(zdp, jl) * zrg_r;
         double zdpevap = zdpr * A1(zdtgdp, jl);
+        if (SPP_ON(CLOUDSC_SPP_SNOWSUBLIM)) /* :3288-3290 */
+          zdpevap = zdpevap * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_SNOWSUBLIM, 0, 0);
         double zevap = fmin_(zdpevap, L2(zqxfg, jl, NCLDQS));
         L3(zsolqa, jl, NCLDQV, NCLDQS) = L3(zsolqa, jl, NCLDQV, NCLDQS) + zevap;
         L3(zsolqa, jl, NCLDQS, NCLDQV) = L3(zsolqa, jl, NCLDQS, NCLDQV) - zevap;
@@ -1160,7 +1232,10 @@ int oracle_cloudsc(
       }
     }
     for (jl = kidia; jl <= kfdia; jl++) A2(pcovptot, jl, jk) = A1(zcovptot, jl);
-    /* ZANEWP (:3819-3823) feeds only the FSD diagnostic (off) */
+    /* ZANEWP (:3819-3823): cloud fraction with precipitation fraction, for the ice FSD */
+    for (jl = kidia; jl <= kfdia; jl++)
+      if (A2(pa, jl, jk) + A1(zda, jl) > 0.001)
+        A2(zanewp, jl, jk) = fmax_(fmax_(A2(pa, jl, jk) + A1(zda, jl), A2(pcovptot, jl, jk)), 0.1);
 
     /* 7. cloud budget diagnostics (:3832-4110).  ZPIEVAP, ZPRACS and ZPRACI
        are zero in this configuration (ISUBLICE=0, PRACS/PRACI off). */
@@ -1312,7 +1387,49 @@ int oracle_cloudsc(
         is = is + 13;
       }
     }
+
+    if (p->lrad_cloud_inhomog) /* :4112-4125 */
+      for (jl = kidia; jl <= kfdia; jl++) {
+        if (A3(zqx0, jl, jk, NCLDQL, klev) + A3(zqx0, jl, jk, NCLDQI, klev) + A2(plude, jl, jk) > p->rlmin) {
+          A2(zratfsd, jl, jk) =
+              A2(plude, jl, jk) / (A2(plude, jl, jk) + A3(zqx0, jl, jk, NCLDQL, klev) + A3(zqx0, jl, jk, NCLDQI, klev));
+          A2(zratfsd, jl, jk) = fmax_(0.0, fmin_(1.0, A2(zratfsd, jl, jk)));
+        }
+        A2(zicef, jl, jk) = L2(zqxn, jl, NCLDQI);
+        A2(zliqf, jl, jk) = L2(zqxn, jl, NCLDQL);
+      }
   }
+  /* ice FSD (:4307-4359); default-REAL (binary32) literals as written at
+     :4321-4322 and the 0.00001 at :4316 */
+  if (p->lrad_cloud_inhomog) {
+    const double f_p5 = (double)0.5f, f_p001 = (double)0.001f, f_p24 = (double)0.24f, f_p11 = (double)0.11f;
+    const double f_10 = (double)10.f, f_p03 = (double)0.03f, f_1em5 = (double)0.00001f;
+    for (jk = 1; jk <= klev; jk++)
+      for (jl = kidia; jl <= kfdia; jl++) {
+        double zgridlen = 2 * p->ra * sqrt(p->rpi * A1(pgaw, jl)) * 0.001;
+        double zifsdback = 0.446585 * pow(zgridlen, 1.0 / 3.0) * pow(pow(0.308061 * zgridlen, 0.395736) + 1.0, -0.744527);
+        double zqtot = fmax_(fmin_((A3(zqx, jl, jk, NCLDQV, klev) + A3(zqx, jl, jk, NCLDQI, klev)) * 1000.0, 30.0), f_1em5);
+        double zdp_ = A2(paph, jl, jk + 1) - A2(paph, jl, jk);
+        double zrho_ = A2(pap, jl, jk) / (p->rd * A2(ztp1, jl, jk));
+        double zdelz = 1.0 / (p->rg * zrho_) * zdp_ * 0.001;
+        zdelz = fmax_(fmin_(zdelz, f_p5), f_p001);
+        double zphi = pow(zdelz / f_p24, f_p11) * pow(zqtot / f_10, f_p03);
+        double zifsd = p->rcloud_frac_std;
+        if (A2(zanewp, jl, jk) > 0.95) {
+          zifsd = zifsdback * zphi;
+          zifsd = 1.3 * (zifsd + A2(zratfsd, jl, jk) * 1.5);
+        } else if (A2(zanewp, jl, jk) > 0.001 && A2(zanewp, jl, jk) <= 0.95) {
+          zifsd = zifsdback * zphi * 1.5;
+          zifsd = 1.3 * (zifsd + A2(zratfsd, jl, jk) * 1.5);
+        }
+        double zfsd = p->rcloud_frac_std;
+        if (A2(zicef, jl, jk) > zepsec) zfsd = zifsd;
+        if (A2(zliqf, jl, jk) > 0.0 && A2(zicef, jl, jk) <= zepsec) zfsd = A2(zlfsd, jl, jk);
+        zfsd = fmin_(fmax_(0.1, zfsd), 3.575);
+        A2(pfsd, jl, jk) = zfsd;
+      }
+  }
+
   /* PCOVPTOT above the cloud top: left undefined by the reference, zero here */
   for (jk = 1; jk < ncldtop; jk++)
     for (jl = kidia; jl <= kfdia; jl++) A2(pcovptot, jl, jk) = 0.0;
@@ -1771,9 +1888,10 @@ int oracle_sltend_supersat_batched(
   return err;
 }
 
-/* The block loop of oracle_cloudsc_batched with the arrays the cloud budget
- * diagnostics read (PVFA, PDYNA/L/I/S, PHRSW, PHRLW, KCTOP, KPBLTYPE) and
- * PEXTRA (NPROMA, KLEV, KFLDX, NGPBLKS), INOUT. */
+/* The block loop of oracle_cloudsc_batched with the arrays the optional
+ * configurations read or write (PVFA, PDYNA/L/I/S, PHRSW, PHRLW, PGAW, KCTOP,
+ * KPBLTYPE, PGP2DSPP (NPROMA, NRFTOTAL, NGPBLKS), PFSD, PEXTRA (NPROMA, KLEV,
+ * KFLDX, NGPBLKS), INOUT). */
 int oracle_cloudsc_batched_diag(
     const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
     double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
@@ -1789,7 +1907,8 @@ int oracle_cloudsc_batched_diag(
     double *pfsqltur, double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
     double *pfhpsn, const double *pvfa, const double *pdyna, const double *pdynl,
     const double *pdyni, const double *pdyns, const double *phrsw, const double *phrlw,
-    const int32_t *kctop, const int32_t *kpbltype, double *pextra, int kfldx, int nthreads) {
+    const double *pgaw, const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp,
+    double *pfsd, double *pextra, int kfldx, int nthreads) {
   if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
       ngptot <= nproma * (ngpblks - 1))
     return CLOUDSC_E_SHAPE;
@@ -1812,10 +1931,11 @@ int oracle_cloudsc_batched_diag(
         ptendency_loc_a + o, ptendency_loc_cld + o * NCLV, pvfa ? pvfa + o : NULL, pvfl + o, pvfi + o,
         pdyna ? pdyna + o : NULL, pdynl ? pdynl + o : NULL, pdyni ? pdyni + o : NULL, NULL,
         pdyns ? pdyns + o : NULL, phrsw ? phrsw + o : NULL, phrlw ? phrlw + o : NULL, NULL, pap + o,
-        paph + ib * s2h, NULL, plsm + o1, NULL, ldcum + o1, kctop ? kctop + o1 : NULL, ktype + o1,
+        paph + ib * s2h, NULL, plsm + o1, pgaw ? pgaw + o1 : NULL, ldcum + o1, kctop ? kctop + o1 : NULL, ktype + o1,
         kpbltype ? kpbltype + o1 : NULL, (double *)(peis + o1), plu + o, plude + o, pludeli + o * 4,
-        psnde + o * 2, pmfu + o, pmfd + o, NULL, 0, pa + o, pclv + o * NCLV, NULL, NULL, NULL, NULL, NULL,
-        pcovptot + o, NULL, prainfrac_toprfz + o1, pfsqlf + ib * s2h, pfsqif + ib * s2h,
+        psnde + o * 2, pmfu + o, pmfd + o,
+        pgp2dspp ? pgp2dspp + o1 * (size_t)(p->spp_nrftotal > 0 ? p->spp_nrftotal : 0) : NULL, 0, pa + o,
+        pclv + o * NCLV, NULL, NULL, NULL, NULL, NULL, pcovptot + o, pfsd ? pfsd + o : NULL, prainfrac_toprfz + o1, pfsqlf + ib * s2h, pfsqif + ib * s2h,
         pfcqnng + ib * s2h, pfcqlng + ib * s2h, pfsqrf + ib * s2h, pfsqsf + ib * s2h, pfcqrng + ib * s2h,
         pfcqsng + ib * s2h, pfsqltur + ib * s2h, pfsqitur + ib * s2h, pfplsl + ib * s2h,
         pfplsn + ib * s2h, pfhpsl + ib * s2h, pfhpsn + ib * s2h, pextra ? pextra + ib * sx : NULL, kfldx);

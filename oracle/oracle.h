@@ -108,7 +108,8 @@ int oracle_cloudsc_batched_diag(
     double *pfsqltur, double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl,
     double *pfhpsn, const double *pvfa, const double *pdyna, const double *pdynl,
     const double *pdyni, const double *pdyns, const double *phrsw, const double *phrlw,
-    const int32_t *kctop, const int32_t *kpbltype, double *pextra, int kfldx, int nthreads);
+    const double *pgaw, const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp,
+    double *pfsd, double *pextra, int kfldx, int nthreads);
 
 /* The supersaturation adjustment of SLTEND (sltend.F90:380-410), one block
  * and batched over (NPROMA,...,NGPBLKS) blocks. */

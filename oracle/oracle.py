@@ -50,7 +50,7 @@ def lib(libm="glibc"):
                                                   [vp] * len(SATADJ_FIELDS) + [i32])
         L.oracle_cloud_satadj_batched.restype = i32
         L.oracle_cloudsc_batched_diag.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
-                                                  [vp] * (len(BATCHED_FIELDS) + 10) + [i32, i32])
+                                                  [vp] * (len(BATCHED_FIELDS) + 13) + [i32, i32])
         L.oracle_cloudsc_batched_diag.restype = i32
         from openifs_b200.fields import SLTEND_FIELDS
         L.oracle_sltend_supersat_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
@@ -137,7 +137,7 @@ def cloudsc_batched_diag(params, arrays, diag, nproma, klev, ngpblks, ngptot, pt
     for n, *_ in DIAG_FIELDS:
         a = diag.get(n)
         ptrs.append(None if a is None else a.ctypes.data)
-    kfldx = diag["pextra"].shape[1]
+    kfldx = diag["pextra"].shape[1] if diag.get("pextra") is not None else 0
     rc = lib(libm).oracle_cloudsc_batched_diag(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
                                                int(ngptot), float(ptsphy), *ptrs, int(kfldx), int(nthreads))
     if rc < 0:

@@ -161,9 +161,8 @@ extern "C" int hostemu_sltend_batched(const cloudsc_params *p, int nproma, int k
   return 0;
 }
 
-// CLOUDSC with the cloud budget diagnostics (the kernel's BUD form): the
-// BATCHED_FIELDS arrays in `a`, then PVFA, PDYNA, PDYNL, PDYNI, PDYNS, PHRSW,
-// PHRLW, KCTOP, KPBLTYPE, PEXTRA (fields.DIAG_FIELDS order) in `b`.
+// CLOUDSC with the optional configurations (the kernel's BUD and OPT forms):
+// the BATCHED_FIELDS arrays in `a`, the fields.DIAG_FIELDS arrays in `b`.
 extern "C" int hostemu_batched_diag(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
                                     double ptsphy, void **a, void **b, int kfldx) {
   Derived d;
@@ -196,14 +195,22 @@ extern "C" int hostemu_batched_diag(const cloudsc_params *p, int nproma, int kle
   f.ncounters = &nwarn;
   const double **bd = (const double **)b;
   f.pvfa = bd[0]; f.pdyna = bd[1]; f.pdynl = bd[2]; f.pdyni = bd[3]; f.pdyns = bd[4];
-  f.phrsw = bd[5]; f.phrlw = bd[6]; f.kctop = (const int32_t *)b[7]; f.kpbltype = (const int32_t *)b[8];
-  f.pextra = (double *)b[9];
+  f.phrsw = bd[5]; f.phrlw = bd[6]; f.pgaw = bd[7]; f.kctop = (const int32_t *)b[8];
+  f.kpbltype = (const int32_t *)b[9]; f.pgp2dspp = bd[10]; f.pfsd = (double *)b[11];
+  f.pextra = (double *)b[12];
   f.kfldx = kfldx;
+  f.nrftotal = p->spp_nrftotal;
+  const bool bud = p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint;
+  const bool opt = p->lspp || p->lcloud_inhomog || p->lrad_cloud_inhomog;
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
   for (int ib = 0; ib < ngpblks; ++ib) {
     int icend = ngptot - ib * nproma;
     if (icend > nproma) icend = nproma;
-    for (int jl = 0; jl < icend; ++jl) cloudsc_column<double, false, true>(f, sh, ib, jl);
+    for (int jl = 0; jl < icend; ++jl) {
+      if (bud && opt) cloudsc_column<double, false, true, true>(f, sh, ib, jl);
+      else if (opt) cloudsc_column<double, false, false, true>(f, sh, ib, jl);
+      else cloudsc_column<double, false, true>(f, sh, ib, jl);
+    }
   }
   return (int)nwarn;
 }

@@ -64,3 +64,57 @@ def test_block_entry_budgets(cuda):
     for n in util.COMPARED:
         g, o = util.defined(n, blk[n][None]), util.defined(n, ref[n])
         assert np.array_equal(g[..., cols], o[..., cols]), n
+
+
+@pytest.mark.parametrize("case", util.OPT_CASES)
+def test_spp_inhomogeneity_batched(cuda, case):
+    """SPP perturbations and the cloud-inhomogeneity paths (PFSD) through
+    cloudsc_b200_batched_diag, bit for bit with the oracle."""
+    import torch
+    p0, po0 = util.params()
+    p, po = util.opt_params(p0, case), util.opt_params(po0, case)
+    nproma, nblk = 64, 5
+    ngptot = nproma * nblk - 9
+    arrs = inputs.generate(nblk, nproma, p, seed=47)
+    diag = inputs.generate_diag(arrs, nproma, fields.budget_fields_needed(p) + 1, seed=47)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot)
+    try:
+        cloudsc.setup(p)
+        d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
+        g = {k: torch.from_numpy(v).cuda() for k, v in diag.items()}
+        cloudsc.cloudsc_batched_diag(p, d, g, nproma, util.KLEV, nblk, ngptot, util.PTSPHY)
+        torch.cuda.synchronize()
+        for n in util.COMPARED:
+            assert np.array_equal(util.defined(n, d[n].cpu().numpy()), util.defined(n, ref[n])), n
+        assert np.array_equal(g["pfsd"].cpu().numpy(), dref["pfsd"])
+        assert np.array_equal(g["pextra"].cpu().numpy(), dref["pextra"])
+        with pytest.raises(cloudsc.CloudscError):  # no PGAW/PGP2DSPP in the plain entry
+            cloudsc.cloudsc_batched(p, d, nproma, util.KLEV, nblk, ngptot, util.PTSPHY)
+    finally:
+        cloudsc.setup(p0)
+
+
+def test_block_entry_spp_inhomogeneity(cuda):
+    """cloudsc_b200_block with SPP, both inhomogeneity paths and the budgets:
+    PFSD and every output over KIDIA..KFDIA as the oracle."""
+    p0, po0 = util.params()
+    p, po = util.opt_params(p0, "all+budgets"), util.opt_params(po0, "all+budgets")
+    nproma = 40
+    arrs = inputs.generate(1, nproma, p, seed=53)
+    kf = fields.budget_fields_needed(p)
+    diag = inputs.generate_diag(arrs, nproma, kf, seed=53)
+    ref, dref, _ = util.run_oracle_diag(po, arrs, diag, nproma, 1, nproma)
+    blk = {k: np.ascontiguousarray(v[0]) for k, v in arrs.items()}
+    blk.update({k: np.ascontiguousarray(v[0]) for k, v in diag.items()})
+    kidia, kfdia = 2, 39
+    try:
+        cloudsc.setup(p)
+        cloudsc.cloudsc_block(p, kidia, kfdia, nproma, util.KLEV, util.PTSPHY, blk, kfldx=kf)
+    finally:
+        cloudsc.setup(p0)
+    cols = slice(kidia - 1, kfdia)
+    assert np.array_equal(blk["pfsd"][..., cols], dref["pfsd"][0][..., cols])
+    assert np.array_equal(blk["pextra"][..., cols], dref["pextra"][0][..., cols])
+    for n in util.COMPARED:
+        g, o = util.defined(n, blk[n][None]), util.defined(n, ref[n])
+        assert np.array_equal(g[..., cols], o[..., cols]), n

@@ -154,3 +154,30 @@ def test_budget_diagnostics_bit_exact(pp, flags):
     for n in util.COMPARED:
         assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), n
         assert np.array_equal(util.defined(n, ref[n]), util.defined(n, plain[n])), n
+
+
+@pytest.mark.parametrize("case", util.OPT_CASES)
+def test_spp_inhomogeneity_bit_exact(pp, case):
+    """SPP perturbations, LCLOUD_INHOMOG and LRAD_CLOUD_INHOMOG (PFSD), alone
+    and together with the budgets: the kernel's OPT form on the host against
+    the oracle, every output and PFSD/PEXTRA bit for bit, both libms."""
+    p0, po0 = pp
+    p, po = util.opt_params(p0, case), util.opt_params(po0, case)
+    nproma, nblk = 32, 6
+    ngptot = nproma * nblk - 3
+    arrs = inputs.generate(nblk, nproma, p, seed=43)
+    diag = inputs.generate_diag(arrs, nproma, util.fields.budget_fields_needed(p) + 1, seed=43)
+    for libm in ("plibm", "glibc"):
+        ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot, libm=libm)
+        emu, demu, nwe = util.run_hostemu_diag(p, arrs, diag, nproma, nblk, ngptot, libm=libm)
+        assert nw == nwe
+        for n in util.COMPARED:
+            assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), (libm, n)
+        assert np.array_equal(demu["pfsd"], dref["pfsd"]), libm
+        assert np.array_equal(demu["pextra"], dref["pextra"]), libm
+    plain, _ = util.run_oracle(po0, arrs, nproma, nblk, ngptot, libm="plibm")
+    if case != "radinhomog":  # the options change the physics
+        assert any(not np.array_equal(util.defined(n, ref[n]), util.defined(n, plain[n])) for n in util.COMPARED)
+    if "rad" in case or case.startswith("all"):
+        fsd = dref["pfsd"][:-1]  # full blocks (the last block's padding is not written)
+        assert (fsd >= 0.1).all() and (fsd <= 3.575).all() and len(np.unique(fsd)) > 10

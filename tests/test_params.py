@@ -81,9 +81,12 @@ def test_ncldtop_l137():
 
 
 def test_unsupported_switches_rejected(pp, built):
+    """The aerosol switches (NAERCLD > 0) are the only ones the kernels do
+    not implement; every other CLOUDSC switch is accepted."""
     p, _ = pp
-    q = p.copy()
-    q.lspp = 1
-    with pytest.raises(cloudsc.CloudscError) as e:
-        cloudsc.setup(q)
-    assert e.value.code == -3
+    for name in ("laericeauto", "laericesed", "laerliqautolsp", "laerliqcoll"):
+        q = p.copy()
+        setattr(q, name, 1)
+        with pytest.raises(cloudsc.CloudscError) as e:
+            cloudsc.setup(q)
+        assert e.value.code == -3, name

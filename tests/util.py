@@ -259,3 +259,37 @@ def with_flags(p, flags):
     for k, v in flags.items():
         setattr(q, k, v)
     return q
+
+
+def with_spp(p, lramidlimit1=1, nrftotal=10):
+    """A copy of ``p`` with LSPP and all eight perturbations on: fields
+    MP = 1..8 (CLOUDINHOM also reads MP+1 = 9), MU(i) = -0.05 (n+1) i and
+    XMAG(i) = 0.3 + 0.05 n."""
+    q = type(p).from_buffer_copy(p)
+    q.lspp = 1
+    q.spp_nrftotal = nrftotal
+    q.spp_lramidlimit1 = lramidlimit1
+    for n in range(8):
+        q.spp_on[n] = 1
+        q.spp_mp[n] = n + 1
+        for i in range(2):
+            q.spp_mu[2 * n + i] = -0.05 * (n + 1) * (i + 1)
+            q.spp_xmag[2 * n + i] = 0.3 + 0.05 * n
+    return q
+
+
+OPT_CASES = ["spp", "inhomog", "radinhomog", "all", "all+budgets"]
+
+
+def opt_params(p, case):
+    """``p`` with the optional configuration ``case`` of OPT_CASES."""
+    if case == "spp":
+        return with_spp(p)
+    if case == "inhomog":
+        return with_flags(p, {"lcloud_inhomog": 1})
+    if case == "radinhomog":
+        return with_flags(p, {"lrad_cloud_inhomog": 1})
+    q = with_flags(with_spp(p, lramidlimit1=0), {"lcloud_inhomog": 1, "lrad_cloud_inhomog": 1})
+    if case == "all+budgets":
+        q = with_flags(q, BUDGET_CASES[-1])
+    return q
