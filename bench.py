@@ -135,28 +135,27 @@ def _dist():
     return world, rank, local
 
 
-def cpu_baseline(p_oracle, nblocks=64, threads=0):
+def cpu_baseline(p_oracle, nblocks=64, threads=0, nproma=NPROMA, seed=SEED, seconds=10.0):
     """The oracle (the reference algorithm restated in C, system libm) on a
-    bounded sample of the workload: ``nblocks`` NPROMA blocks of 128, OpenMP
-    over blocks (ec_phys_drv.F90:438).  Returns columns/s."""
+    bounded sample of the workload: ``nblocks`` NPROMA blocks of ``nproma``,
+    OpenMP over blocks (ec_phys_drv.F90:438), warm runs for about
+    ``seconds``.  Returns (best columns/s, runs, median columns/s)."""
     from openifs_b200 import inputs
     from oracle import oracle
-    arrs = inputs.generate(nblocks, NPROMA, p_oracle, seed=SEED)
+    arrs = inputs.generate(nblocks, nproma, p_oracle, seed=seed)
     work = {k: v.copy() for k, v in arrs.items()}
-    oracle.cloudsc_batched(p_oracle, work, NPROMA, KLEV, nblocks, nblocks * NPROMA, PTSPHY,
+    oracle.cloudsc_batched(p_oracle, work, nproma, KLEV, nblocks, nblocks * nproma, PTSPHY,
                            threads, libm="glibc")  # warm
-    best = None
-    reps = 0
-    t_end = time.perf_counter() + 10.0
-    while reps < 2 or time.perf_counter() < t_end:
+    times = []
+    t_end = time.perf_counter() + seconds
+    while len(times) < 2 or time.perf_counter() < t_end:
         work = {k: v.copy() for k, v in arrs.items()}
         t = time.perf_counter()
-        oracle.cloudsc_batched(p_oracle, work, NPROMA, KLEV, nblocks, nblocks * NPROMA, PTSPHY,
+        oracle.cloudsc_batched(p_oracle, work, nproma, KLEV, nblocks, nblocks * nproma, PTSPHY,
                                threads, libm="glibc")
-        dt = time.perf_counter() - t
-        best = dt if best is None else min(best, dt)
-        reps += 1
-    return nblocks * NPROMA / best, reps
+        times.append(time.perf_counter() - t)
+    cols = nblocks * nproma
+    return cols / min(times), len(times), cols / statistics.median(times)
 
 
 def run_reference(a):
@@ -262,6 +261,36 @@ def satadj_form(a, p, host, dev, world, rank, stream):
                            "sample": f"{nb} NPROMA blocks of 128, best of 3, OpenMP over blocks"}}
 
 
+def _diag_timed(a, pb, d, plude0, diag, dev, world, stream):
+    """Mean device time of cloudsc_batched_diag under the parameters ``pb``
+    (PLUDE restored outside the events), max over ranks."""
+    import torch
+    from openifs_b200 import cloudsc
+    cloudsc.setup(pb)
+    try:
+        def step():
+            d["plude"].copy_(plude0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cloudsc.cloudsc_batched_diag(pb, d, diag, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, stream=stream)
+            e1.record(stream)
+            return e0, e1
+        for _ in range(a.warmup):
+            step()
+        torch.cuda.synchronize(dev)
+        ev = [step() for _ in range(a.steps)]
+        torch.cuda.synchronize(dev)
+        ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    finally:
+        d["plude"].copy_(plude0)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
 def budget_form(a, p, d, plude0, dev, world, stream, ms64):
     """The FP64 kernel with every cloud budget section on (LCLDBUDC/L/I/T,
     the vertical integral, LCLDBUD_TIMEINT; cloudsc.F90:3832-4110) on the same
@@ -283,33 +312,54 @@ def budget_form(a, p, d, plude0, dev, world, stream, ms64):
     diag["kctop"] = torch.zeros((NGPBLKS, NPROMA), device=dev, dtype=torch.int32)
     diag["kpbltype"] = torch.zeros((NGPBLKS, NPROMA), device=dev, dtype=torch.int32)
     diag["pextra"] = torch.zeros((NGPBLKS, kf, KLEV, NPROMA), device=dev, dtype=torch.float64)
-    cloudsc.setup(pb)
     try:
-        def step():
-            d["plude"].copy_(plude0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            cloudsc.cloudsc_batched_diag(pb, d, diag, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, stream=stream)
-            e1.record(stream)
-            return e0, e1
-        for _ in range(a.warmup):
-            step()
-        torch.cuda.synchronize(dev)
-        ev = [step() for _ in range(a.steps)]
-        torch.cuda.synchronize(dev)
-        ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+        ms = _diag_timed(a, pb, d, plude0, diag, dev, world, stream)
     finally:
         cloudsc.setup(p)
-        d["plude"].copy_(plude0)
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
     del diag
     torch.cuda.empty_cache()
     return {"ms": ms, "columns_per_s": world * NCOL / (ms * 1e-3), "overhead_vs_fp64": ms / ms64 - 1.0,
             "sections": sorted(flags), "pextra_fields": kf}
+
+
+def spp_form(a, p, d, plude0, dev, world, stream, ms64):
+    """The FP64 kernel with the stochastically perturbed parametrisations
+    (LSPP, all eight perturbations; cloudsc.F90:850-939) and the cloud
+    inhomogeneity / fractional-standard-deviation path (LCLOUD_INHOMOG,
+    LRAD_CLOUD_INHOMOG; :1937-2110, 4307-4359) on the same columns: device
+    time and its overhead over the plain FP64 kernel.  The pattern fields
+    PGP2DSPP are seeded N(0,1), PGAW is U(1e-7, 3e-6); parity of this form is
+    in the tests."""
+    import torch
+    from openifs_b200 import cloudsc
+    nrf = 10
+    pb = type(p).from_buffer_copy(p)
+    pb.lspp = 1
+    pb.spp_nrftotal = nrf
+    pb.spp_lramidlimit1 = 1
+    for n in range(8):
+        pb.spp_on[n] = 1
+        pb.spp_mp[n] = n + 1
+        for i in range(2):
+            pb.spp_mu[2 * n + i] = -0.05 * (n + 1) * (i + 1)
+            pb.spp_xmag[2 * n + i] = 0.3 + 0.05 * n
+    pb.lcloud_inhomog = 1
+    pb.lrad_cloud_inhomog = 1
+    g = torch.Generator(device=dev).manual_seed(SEED + 17)
+    diag = {"pgaw": torch.rand((NGPBLKS, NPROMA), device=dev, dtype=torch.float64, generator=g) * 2.9e-6 + 1e-7,
+            "pgp2dspp": torch.randn((NGPBLKS, nrf, NPROMA), device=dev, dtype=torch.float64, generator=g),
+            "pfsd": torch.zeros((NGPBLKS, KLEV, NPROMA), device=dev, dtype=torch.float64)}
+    try:
+        ms = _diag_timed(a, pb, d, plude0, diag, dev, world, stream)
+    finally:
+        cloudsc.setup(p)
+    fsd = diag["pfsd"]
+    out = {"ms": ms, "columns_per_s": world * NCOL / (ms * 1e-3), "overhead_vs_fp64": ms / ms64 - 1.0,
+           "switches": ["lspp (8 perturbations)", "lcloud_inhomog", "lrad_cloud_inhomog"],
+           "pfsd_range": [float(fsd.min()), float(fsd.max())]}
+    del diag
+    torch.cuda.empty_cache()
+    return out
 
 
 def sltend_form(a, p, host, dev, world, rank, stream):
@@ -582,6 +632,7 @@ def run_ours(a):
         errs[name] = err
 
     bud = budget_form(a, p, d, plude0, dev, world, stream, results["fp64"]["ms"])
+    spp = spp_form(a, p, d, plude0, dev, world, stream, results["fp64"]["ms"])
     sat = satadj_form(a, p, host, dev, world, rank, stream)
     slt = sltend_form(a, p, host, dev, world, rank, stream)
 
@@ -643,7 +694,9 @@ def run_ours(a):
 
     from oracle import oracle
     po = oracle.params_default(PTSPHY, p.ncldtop)
-    cpu_val, reps = cpu_baseline(po)
+    cpu_val, reps, cpu_med = cpu_baseline(po)
+    # the reference's CPU-scale case: 3,200 columns = 100 NPROMA blocks of 32, seed 1
+    c1_best, c1_reps, c1_med = cpu_baseline(po, nblocks=100, nproma=32, seed=1, seconds=3.0)
     ncores = os.cpu_count() or 1
 
     value = world * NCOL / (ms64 * 1e-3)
@@ -671,12 +724,17 @@ def run_ours(a):
             "surrogate": sur,
         },
         "budget_diagnostics": bud,
+        "spp_inhomogeneity": spp,
         "satadj": sat,
         "sltend_supersat": slt,
         "roofline": roofline,
         "cpu_baseline": {"value": cpu_val, "unit": "columns/s", "cores": ncores, "kind": "port",
                          "sample": f"64 NPROMA blocks of 128 (8,192 columns) of the workload, "
-                                   f"best of {reps} warm runs, OpenMP over blocks"},
+                                   f"best of {reps} warm runs, OpenMP over blocks",
+                         "median": cpu_med,
+                         "cpu_case_3200_columns": {"nproma": 32, "blocks": 100, "seed": 1,
+                                                   "columns_per_s_best": c1_best,
+                                                   "columns_per_s_median": c1_med, "runs": c1_reps}},
         "e2e": e2e,
         "clocks": clocks,
         "gpu_launches": a.steps,

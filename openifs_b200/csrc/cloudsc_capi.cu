@@ -375,7 +375,7 @@ int cloudsc_b200_setup(const cloudsc_params *p) {
     return fail(CLOUDSC_E_PARAMS, "bad params magic or version");
   if (!params_supported(*p))
     return fail(CLOUDSC_E_UNSUPPORTED,
-                "a switch this build does not implement is on (aerosol, inhomogeneity, SPP or budgets)");
+                "an aerosol switch (LAERICEAUTO, LAERICESED, LAERLIQAUTOLSP, LAERLIQCOLL) is on; this build does not implement them");
   if (p->ncldtop < 2) return fail(CLOUDSC_E_SHAPE, "ncldtop must be >= 2");
   {
     std::lock_guard<std::mutex> lk(g_mu);

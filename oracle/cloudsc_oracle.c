@@ -8,7 +8,10 @@
  *   ifs-source/arpifs/function/fcttre.func.h:37-184   (saturation functions)
  *   ifs-source/arpifs/function/fccld.func.h:26-27     (FOKOOP)
  * in the reference's default configuration (options hard-wired at
- * cloudsc.F90:727-793; LSPP, aerosol, inhomogeneity and budget switches off).
+ * cloudsc.F90:727-793), plus the optional paths the switches turn on: the
+ * cloud budget diagnostics (LCLDBUD*, :3832-4110), the SPP perturbations
+ * (LSPP, :850-939) and the cloud-inhomogeneity/FSD paths (LCLOUD_INHOMOG,
+ * LRAD_CLOUD_INHOMOG, :1937-2110, 4307-4359); the aerosol switches are off.
  * Loop order (JK outer, JL inner), local arrays and the order of every
  * floating-point operation follow the Fortran source; it is compiled with
  * -O2 -ffp-contract=off (no FMA contraction, like the reference's -no-fma
