@@ -53,6 +53,14 @@
 #define PLIBM_FN static inline
 #define PLIBM_FN_HEAVY static inline
 #endif
+/* The rarely taken full paths (extreme arguments, special values) are kept
+ * out of line on the device, so each inlined call site carries only the
+ * common path. */
+#if defined(__CUDACC__)
+#define PLIBM_FN_COLD static __host__ __device__ __noinline__
+#else
+#define PLIBM_FN_COLD static
+#endif
 
 /* The tables: one copy for host code, one in device global memory (read
  * through the read-only data cache). */
@@ -140,8 +148,8 @@ PLIBM_FN double plibm_sqrt(double x) {
 /* 2^k for -1022 <= k <= 1023 */
 PLIBM_FN double plibm_pow2i(int k) { return plibm_from_bits((uint64_t)(int64_t)(k + 1023) << 52); }
 
-/* exp(hi + lo) for |lo| <= ~1e-15 |hi|; the kernel of both exp and pow. */
-PLIBM_FN_HEAVY double plibm_exp_dd(double hi, double lo) {
+/* exp(hi + lo) for |lo| <= ~1e-15 |hi|, every hi (the full path). */
+PLIBM_FN_COLD double plibm_exp_dd_full(double hi, double lo) {
   /* clamp so the main path stays finite; results overflow / underflow naturally */
   double hc = hi > 709.9 ? 709.9 : hi;
   hc = hc < -746.0 ? -746.0 : hc;
@@ -165,15 +173,43 @@ PLIBM_FN_HEAVY double plibm_exp_dd(double hi, double lo) {
   return hi != hi ? hi : res;
 }
 
+/* exp(hi + lo) for |lo| <= ~1e-15 |hi|; the kernel of both exp and pow.
+ * For -700 < hi < 700 the full path's clamps do nothing and 2^m e (m the
+ * scale, -1010 <= m <= 1010, e in [2^(-1/256), 2^(255/256))) is a normal
+ * number, so adding m to e's exponent field gives exactly the full path's
+ * two-step product: both paths return the same bits.  NaN and the ends go
+ * through the full path. */
+PLIBM_FN_HEAVY double plibm_exp_dd(double hi, double lo) {
+  if (!(hi > -700.0 && hi < 700.0)) return plibm_exp_dd_full(hi, lo);
+  double kd = plibm_fma(hi, PLIBM_INV_LN2_128, PLIBM_SHIFT);
+  int64_t ki = (int64_t)(plibm_bits(kd) & 0xfffffffffffffULL) - (int64_t)(1LL << 51);
+  kd = kd - PLIBM_SHIFT;
+  double r = plibm_fma(-kd, PLIBM_LN2_128_HI, hi);
+  r = plibm_fma(-kd, PLIBM_LN2_128_LO, r);
+  r = r + lo;
+  int j = (int)(ki & 127);
+  int m = (int)(ki >> 7);
+  double thi = plibm_exp_t(2 * j), tlo = plibm_exp_t(2 * j + 1);
+  double p = plibm_fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5); /* 1/120, 1/24 */
+  p = plibm_fma(p, r, 0x1.5555555555555p-3);                          /* 1/6 */
+  p = plibm_fma(p, r, 0x1.0000000000000p-1);                          /* 1/2 */
+  p = plibm_fma(p, r * r, r);                                         /* expm1(r) */
+  double s = plibm_fma(thi, p, tlo);
+  double e = thi + s;
+  return plibm_from_bits(plibm_bits(e) + ((uint64_t)(int64_t)m << 52));
+}
+
 PLIBM_FN double plibm_exp(double x) { return plibm_exp_dd(x, 0.0); }
 
 /* ln(x) as hi + lo for finite x > 0. */
 PLIBM_FN_HEAVY void plibm_log_dd(double x, double *hi, double *lo) {
   uint64_t u = plibm_bits(x);
-  int sub = (u >> 52) == 0;
-  double xs = sub ? x * 0x1p54 : x;
-  u = plibm_bits(xs);
-  int e = (int)(u >> 52) - 1023 - (sub ? 54 : 0);
+  int e = -1023;
+  if ((u >> 52) == 0) { /* subnormal (or zero): scale into the normal range */
+    u = plibm_bits(x * 0x1p54);
+    e -= 54;
+  }
+  e += (int)(u >> 52);
   uint64_t mant = u & 0xfffffffffffffULL;
   int j = (int)(mant >> 45);
   double m = plibm_from_bits(mant | 0x3ff0000000000000ULL);
@@ -218,14 +254,21 @@ PLIBM_FN void plibm_log_base(double x, double *lhi, double *llo) {
 
 /* x^y given plibm_log_base(x) = lhi + llo; pow(x, y) is exactly this, so
  * calls that share a base can share its logarithm. */
+PLIBM_FN_COLD double plibm_pow_special(double x, double y, double res);
 PLIBM_FN double plibm_pow_with_log(double x, double y, double lhi, double llo) {
   /* exponents with exact-operation forms (uniform branches for constant y) */
   if (y == 0.5) return plibm_sqrt(x);
   if (y == 1.5) return x * plibm_sqrt(x);
   if (y == 2.0) return x * x;
   if (y == 3.0) return (x * x) * x;
-  int ok = (x > 0.0) && (x < PLIBM_INF);
   double res = plibm_pow_log(lhi, llo, y);
+  if (x > 0.0 && x < PLIBM_INF && y != 0.0 && y == y) return res;
+  return plibm_pow_special(x, y, res);
+}
+
+/* pow's special values: x = 0, +inf, negative or NaN; y = 0 or NaN. */
+PLIBM_FN_COLD double plibm_pow_special(double x, double y, double res) {
+  int ok = (x > 0.0) && (x < PLIBM_INF);
   double spec_zero = y > 0.0 ? 0.0 : (y < 0.0 ? PLIBM_INF : 1.0);
   double spec_inf = y > 0.0 ? PLIBM_INF : (y < 0.0 ? 0.0 : 1.0);
   double spec = x == 0.0 ? spec_zero : (x == PLIBM_INF ? spec_inf : PLIBM_NAN);
