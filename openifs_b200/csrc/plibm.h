@@ -179,14 +179,14 @@ PLIBM_FN_COLD double plibm_exp_dd_full(double hi, double lo) {
  * number, so adding m to e's exponent field gives exactly the full path's
  * two-step product: both paths return the same bits.  NaN and the ends go
  * through the full path. */
-PLIBM_FN_HEAVY double plibm_exp_dd(double hi, double lo) {
+PLIBM_FN_HEAVY double plibm_exp_core(double hi, double lo, int use_lo) {
   if (!(hi > -700.0 && hi < 700.0)) return plibm_exp_dd_full(hi, lo);
   double kd = plibm_fma(hi, PLIBM_INV_LN2_128, PLIBM_SHIFT);
   int64_t ki = (int64_t)(plibm_bits(kd) & 0xfffffffffffffULL) - (int64_t)(1LL << 51);
   kd = kd - PLIBM_SHIFT;
   double r = plibm_fma(-kd, PLIBM_LN2_128_HI, hi);
   r = plibm_fma(-kd, PLIBM_LN2_128_LO, r);
-  r = r + lo;
+  if (use_lo) r = r + lo;
   int j = (int)(ki & 127);
   int m = (int)(ki >> 7);
   double thi = plibm_exp_t(2 * j), tlo = plibm_exp_t(2 * j + 1);
@@ -198,8 +198,11 @@ PLIBM_FN_HEAVY double plibm_exp_dd(double hi, double lo) {
   double e = thi + s;
   return plibm_from_bits(plibm_bits(e) + ((uint64_t)(int64_t)m << 52));
 }
+PLIBM_FN double plibm_exp_dd(double hi, double lo) { return plibm_exp_core(hi, lo, 1); }
 
-PLIBM_FN double plibm_exp(double x) { return plibm_exp_dd(x, 0.0); }
+/* exp(x): lo = 0 needs no addition (r + 0 differs from r only for r = -0,
+ * and expm1(-0) and expm1(+0) give the same sum s below). */
+PLIBM_FN double plibm_exp(double x) { return plibm_exp_core(x, 0.0, 0); }
 
 /* ln(x) as hi + lo for finite x > 0. */
 PLIBM_FN_HEAVY void plibm_log_dd(double x, double *hi, double *lo) {
@@ -226,9 +229,10 @@ PLIBM_FN_HEAVY void plibm_log_dd(double x, double *hi, double *lo) {
   double corr = plibm_fma(-perr, r1, perr);
   double ed = (double)e;
   double a = ed * PLIBM_LN2_HI42; /* exact */
-  double s1 = a + lchi;           /* two-sum */
-  double b1 = s1 - a;
-  double err1 = (a - (s1 - b1)) + (lchi - b1);
+  /* a + lchi exactly as s1 + err1: |a| >= ln2 > lchi for e != 0 and a = 0
+   * for e = 0, so the fast two-sum is exact (and equal to the full one) */
+  double s1 = a + lchi;
+  double err1 = lchi - (s1 - a);
   double s2 = s1 + r1; /* two-sum */
   double b2 = s2 - s1;
   double err2 = (s1 - (s2 - b2)) + (r1 - b2);
