@@ -10,8 +10,9 @@ rebuild a sample of the blocks of the full-size bench input).
 Per column (all choices are this generator's, documented here):
 
 * pressure: PAPH = A + B * p_s on the operational L137 hybrid half levels
-  (data/l137_ab.txt, copied from ifs-test/tests/scm/common/namelists:90-366),
-  p_s ~ U(98, 103) kPa, PAP = (PAPH_k + PAPH_k+1)/2;
+  (data/l137_ab.txt, copied from ifs-test/tests/scm/common/namelists:90-366;
+  coarser test grids take a subset of them, hybrid_ab), p_s ~ U(98, 103)
+  kPa, PAP = (PAPH_k + PAPH_k+1)/2;
 * temperature: T_s ~ U(280, 300) K, constant-lapse-rate profile
   T = T_s (p/p_s)^(R_d G/g) with G = 6.5 K/km, floored at a 216.65 K
   tropopause, plus N(0, 1.5 K) noise;
@@ -58,20 +59,42 @@ def l137_ab():
     return _AB
 
 
-def standard_full_level_pressure(p_surf=101325.0):
+def hybrid_ab(klev=KLEV_L137):
+    """Half-level A (Pa) and B of a KLEV-level hybrid grid: the L137 grid
+    itself, or for 2 <= KLEV < 137 the L137 half levels at the KLEV + 1
+    indices round(i * 137 / KLEV), i = 0..KLEV (model top and surface kept).
+    The coarser grids stand in for the operational L60/L91 tables, which the
+    reference tree does not carry; they exercise the scheme at other
+    vertical resolutions."""
     a, b = l137_ab()
+    if klev == KLEV_L137:
+        return a, b
+    if not 2 <= klev < KLEV_L137:
+        raise ValueError("the generator builds grids of 2..137 levels")
+    idx = np.round(np.arange(klev + 1) * KLEV_L137 / klev).astype(int)
+    return a[idx], b[idx]
+
+
+def standard_full_level_pressure(p_surf=101325.0, klev=KLEV_L137):
+    a, b = hybrid_ab(klev)
     ph = a + b * p_surf
     return 0.5 * (ph[:-1] + ph[1:])
 
 
-def ncldtop_l137(rcldtopp=100.0):
-    """NCLDTOP of sucldp.F90:631-634 for the L137 standard atmosphere."""
-    stpre = standard_full_level_pressure()
+def ncldtop_for(klev=KLEV_L137, rcldtopp=100.0):
+    """NCLDTOP of sucldp.F90:631-634 for the standard atmosphere on the
+    KLEV-level grid of hybrid_ab."""
+    stpre = standard_full_level_pressure(klev=klev)
     nc = 2
     for jlev in range(len(stpre), 1, -1):
         if stpre[jlev - 1] > rcldtopp:
             nc = jlev
     return nc
+
+
+def ncldtop_l137(rcldtopp=100.0):
+    """NCLDTOP of sucldp.F90:631-634 for the L137 standard atmosphere."""
+    return ncldtop_for(KLEV_L137, rcldtopp)
 
 
 def _qsat_mix(t, p, c):
@@ -85,9 +108,7 @@ def _qsat_mix(t, p, c):
 
 
 def _block(rng, nproma, klev, ncldtop, c):
-    a_h, b_h = l137_ab()
-    if klev != len(a_h) - 1:
-        raise ValueError("the generator builds the L137 grid: klev must be 137")
+    a_h, b_h = hybrid_ab(klev)
     np_ = nproma
     ps = rng.uniform(98000.0, 103000.0, np_)
     paph = a_h[:, None] + b_h[:, None] * ps[None, :]                  # (klev+1, np)

@@ -55,6 +55,23 @@ def test_cross_libm_config1(cuda):
         assert rep_gpu[n] <= 1e-8, (n, rep_gpu[n])
 
 
+@pytest.mark.parametrize("klev", [60, 91])
+def test_other_vertical_grids(cuda, klev):
+    """60 and 91 levels (NCLDTOP from their own standard atmosphere), odd
+    NPROMA, ragged last block: bit-exact against the oracle."""
+    p, po = util.params(inputs.ncldtop_for(klev))
+    nproma, nblk = 48, 9
+    ngptot = nproma * nblk - 11
+    arrs = inputs.generate(nblk, nproma, p, klev=klev, seed=29)
+    ref, nw_ref = util.run_oracle(po, arrs, nproma, nblk, ngptot, klev=klev)
+    gpu, nw_gpu = util.run_gpu(p, arrs, nproma, nblk, ngptot, klev=klev)
+    for n in util.COMPARED:
+        a = util.defined(n, util._valid_cols(gpu[n], ngptot, nproma))
+        b = util.defined(n, util._valid_cols(ref[n], ngptot, nproma))
+        assert np.array_equal(a, b), (klev, n)
+    assert nw_gpu == nw_ref
+
+
 def test_partial_last_block_and_odd_nproma(cuda):
     """NPROMA not a multiple of 32 and NGPTOT ending inside the last block."""
     p, po = util.params()

@@ -38,6 +38,24 @@ def test_edge_cases_bit_exact(pp, case):
         assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), (case, n)
 
 
+@pytest.mark.parametrize("klev", [60, 91])
+def test_other_vertical_grids_bit_exact(klev):
+    """Other vertical resolutions (60 and 91 levels, NCLDTOP from their own
+    standard atmosphere): the kernel's column code against the oracle, bit for
+    bit, with a ragged last block."""
+    p, po = util.params(inputs.ncldtop_for(klev))
+    arrs = inputs.generate(6, 33, p, klev=klev, seed=23)
+    ngptot = 6 * 33 - 4
+    ref, nw = util.run_oracle(po, arrs, 33, 6, ngptot, klev=klev)
+    emu, nwe = util.run_hostemu(p, arrs, 33, 6, ngptot, klev=klev)
+    for n in util.COMPARED:
+        a = util.defined(n, util._valid_cols(emu[n], ngptot, 33))
+        b = util.defined(n, util._valid_cols(ref[n], ngptot, 33))
+        assert np.array_equal(a, b), (klev, n)
+    assert nw == nwe
+    assert np.abs(ref["tendency_loc_t"]).max() > 0
+
+
 def test_libm_sensitivity_of_the_reference(pp):
     """The reference algorithm with two correct libms (glibc and plibm, within
     1 ulp of each other) -- the spread any GPU build is measured against."""

@@ -1,5 +1,6 @@
 """The seeded input generator: per-block determinism and physical ranges."""
 import numpy as np
+import pytest
 
 from openifs_b200 import cloudsc, fields, inputs
 
@@ -41,3 +42,18 @@ def test_l137_table():
     assert len(a) == 138 and len(b) == 138
     assert a[0] == 0.0 and b[0] == 0.0 and b[-1] == 1.0
     assert np.all(np.diff(a[:60]) > 0)
+
+
+@pytest.mark.parametrize("klev", [2, 60, 91, 136, 137])
+def test_coarser_grids_are_subsets_of_l137(klev):
+    """The coarser test grids keep the L137 model top and surface and take
+    strictly increasing half levels of it."""
+    a137, b137 = inputs.l137_ab()
+    a, b = inputs.hybrid_ab(klev)
+    assert len(a) == len(b) == klev + 1
+    assert a[0] == a137[0] and b[-1] == b137[-1] and a[-1] == a137[-1]
+    ph = a + b * 101325.0
+    assert np.all(np.diff(ph) > 0)
+    assert set(zip(a, b)) <= set(zip(a137, b137))
+    nc = inputs.ncldtop_for(klev)
+    assert 2 <= nc <= klev

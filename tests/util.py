@@ -65,13 +65,13 @@ def _valid_cols(a, ngptot, nproma):
     return a
 
 
-def run_oracle(po, arrs, nproma, ngpblks, ngptot, nthreads=0, libm="plibm"):
+def run_oracle(po, arrs, nproma, ngpblks, ngptot, nthreads=0, libm="plibm", klev=KLEV):
     ref = {k: v.copy() for k, v in arrs.items()}
-    nwarn = oracle.cloudsc_batched(po, ref, nproma, KLEV, ngpblks, ngptot, PTSPHY, nthreads, libm=libm)
+    nwarn = oracle.cloudsc_batched(po, ref, nproma, klev, ngpblks, ngptot, PTSPHY, nthreads, libm=libm)
     return ref, nwarn
 
 
-def run_hostemu(p, arrs, nproma, ngpblks, ngptot, precision=0, libm="plibm"):
+def run_hostemu(p, arrs, nproma, ngpblks, ngptot, precision=0, libm="plibm", klev=KLEV):
     """The kernel's own column code built for the host (tests/hostemu)."""
     import ctypes
     import os
@@ -85,7 +85,7 @@ def run_hostemu(p, arrs, nproma, ngpblks, ngptot, precision=0, libm="plibm"):
     out = {k: v.copy() for k, v in arrs.items()}
     ptrs = (ctypes.c_void_p * len(fields.BATCHED_FIELDS))(
         *[out[n].ctypes.data for n, *_ in fields.BATCHED_FIELDS])
-    nw = L.hostemu_batched(ctypes.byref(p), int(nproma), KLEV, int(ngpblks), int(ngptot),
+    nw = L.hostemu_batched(ctypes.byref(p), int(nproma), int(klev), int(ngpblks), int(ngptot),
                            ctypes.c_double(PTSPHY), ptrs, int(precision))
     return out, nw
 
@@ -155,12 +155,12 @@ def mixed_error_stats(g, o):
     return out
 
 
-def run_gpu(p, arrs, nproma, ngpblks, ngptot, precision=cloudsc.FP64, device="cuda:0"):
+def run_gpu(p, arrs, nproma, ngpblks, ngptot, precision=cloudsc.FP64, device="cuda:0", klev=KLEV):
     import torch
     cloudsc.setup(p)
     dev = {k: torch.from_numpy(v).to(device) for k, v in arrs.items()}
     cnt = torch.zeros(1, dtype=torch.int32, device=device)
-    cloudsc.cloudsc_batched(p, dev, nproma, KLEV, ngpblks, ngptot, PTSPHY, precision=precision,
+    cloudsc.cloudsc_batched(p, dev, nproma, klev, ngpblks, ngptot, PTSPHY, precision=precision,
                             counter=cnt)
     torch.cuda.synchronize()
     out = {k: v.cpu().numpy() for k, v in dev.items()}
