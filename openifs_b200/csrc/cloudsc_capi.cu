@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -59,6 +60,14 @@ int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
     t_last_error += cudaGetErrorString(e);
   }
   return code;
+}
+
+// After an error in an entry point that has queued copies or kernels on
+// `streams`: wait for them, so that nothing still reads or writes the
+// caller's host arrays once the call has returned.  Returns `rc`.
+int drained(int rc, std::initializer_list<cudaStream_t> streams) {
+  for (cudaStream_t st : streams) cudaStreamSynchronize(st);
+  return rc;
 }
 
 bool params_supported(const cloudsc_params &p) {
@@ -824,7 +833,7 @@ int cloudsc_b200_block(
   for (int i = 0; i < 42 && e == cudaSuccess; ++i)
     if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, 0, 1, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "host-to-device copy", e), {s});
   Fields f = fields_from(d, t_ws.counter);
   double *dx = nullptr;
   if (bud) {
@@ -845,7 +854,7 @@ int cloudsc_b200_block(
     if (e == cudaSuccess) e = cudaMemcpyAsync(dx, pextra, nx * s2b, cudaMemcpyHostToDevice, s);
     f.pextra = dx;
     f.kfldx = kfldx;
-    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+    if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "host-to-device copy", e), {s});
   }
   double *dfsd = nullptr;
   if (opt) {
@@ -859,11 +868,11 @@ int cloudsc_b200_block(
     dfsd = pfsd ? (double *)b : nullptr;
     f.pfsd = dfsd;
     f.nrftotal = p->spp_nrftotal;
-    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+    if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "host-to-device copy", e), {s});
   }
   Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
   rc = launch_checked(0, f, sh, s);
-  if (rc) return rc;
+  if (rc) return drained(rc, {s});
   // copy back only columns KIDIA..KFDIA of every output row
   const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
   for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
@@ -879,7 +888,7 @@ int cloudsc_b200_block(
   uint32_t nwarn = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "device-to-host copy", e), {s});
   return (int)nwarn;
 }
 
@@ -945,7 +954,7 @@ int cloudsc_b200_batched_host(
     if (ngptot_c > nb * nproma) ngptot_c = nb * nproma;
     Shape sh = {nproma, klev, nb, ngptot_c, 0, ptsphy};
     rc = launch_checked(precision, f, sh, t_ws.st[1]);
-    if (rc) return rc;
+    if (rc) return drained(rc, {t_ws.st[0], t_ws.st[1], t_ws.st[2]});
     e = cudaEventRecord(t_ws.ev_done[slot], t_ws.st[1]);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[slot], 0);
     // Whole blocks are copied back in one piece; a partial last block (columns
@@ -973,7 +982,8 @@ int cloudsc_b200_batched_host(
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, t_ws.st[2]);
   if (e == cudaSuccess) e = cudaStreamSynchronize(t_ws.st[2]);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "pipelined host path", e);
+  if (e != cudaSuccess)
+    return drained(fail(CLOUDSC_E_CUDA, "pipelined host path", e), {t_ws.st[0], t_ws.st[1], t_ws.st[2]});
   return (int)nwarn;
 }
 
@@ -1060,11 +1070,11 @@ int cloudsc_b200_block_noalloc(
   for (int i = 0; i < 42 && e == cudaSuccess; ++i)
     if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, 0, 1, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "host-to-device copy", e), {s});
   Fields f = fields_from(d, counter);
   Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
   rc = launch_checked(0, f, sh, s);
-  if (rc) return rc;
+  if (rc) return drained(rc, {s});
   const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
   for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
     if (!kArrs[i].out) continue;
@@ -1075,7 +1085,7 @@ int cloudsc_b200_block_noalloc(
   uint32_t nwarn = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "device-to-host copy", e), {s});
   return (int)nwarn;
 }
 
@@ -1187,13 +1197,13 @@ int cloudsc_b200_satadj_block(
       e = cudaMemcpyAsync(d_in[i], in[i], elems_of(i) * sizeof(double), cudaMemcpyHostToDevice, s);
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "host-to-device copy", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "host-to-device copy", e), {s});
   SatadjFields f = {d_in[0], d_in[1], d_in[2], d_in[3], d_in[4], d_in[5], d_in[6], d_in[7], d_in[8],
                     d_in[9], d_in[10], d_in[11], d_in[12], d_in[13], d_in[14], d_in[15], d_in[16], d_in[17],
                     d_out[0], d_out[1], d_out[2], d_out[3], d_out[4], t_ws.counter};
   Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
   e = launch_satadj(f, sh, s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "kernel launch", e), {s});
   // copy back columns KIDIA..KFDIA of every level
   const size_t c0 = kidia - 1, ncol = kfdia - kidia + 1;
   for (int i = 0; i < 5 && e == cudaSuccess; ++i)
@@ -1202,7 +1212,7 @@ int cloudsc_b200_satadj_block(
   uint32_t nwarn = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "device-to-host copy", e);
+  if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "device-to-host copy", e), {s});
   return (int)nwarn;
 }
 
