@@ -670,8 +670,7 @@ struct Workspace {
   cudaEvent_t ev_in[4], ev_done[4], ev_out[4];
   bool events = false;
   uint32_t *counter = nullptr;
-  ~Workspace() {
-    // Thread exit: release without touching a torn-down context.
+  void release() {
     if (buf) cudaFree(buf);
     if (counter) cudaFree(counter);
     for (auto &s : st)
@@ -682,18 +681,24 @@ struct Workspace {
         cudaEventDestroy(ev_done[i]);
         cudaEventDestroy(ev_out[i]);
       }
+    buf = nullptr;
+    counter = nullptr;
+    cap = 0;
+    for (auto &s : st) s = nullptr;
+    events = false;
   }
+  // Thread exit: release without touching a torn-down context.
+  ~Workspace() { release(); }
   int prepare(int device, size_t bytes) {
     cudaError_t e;
     if (dev != device) {
-      // a different device: drop everything owned on the old one
-      if (buf) cudaFree(buf);
-      if (counter) cudaFree(counter);
-      buf = nullptr;
-      counter = nullptr;
-      cap = 0;
-      for (auto &s : st) s = nullptr;
-      events = false;
+      // a different device: release what this thread owns on the old one
+      // (with the old device current), then start over on the new one
+      if (dev >= 0) {
+        cudaSetDevice(dev);
+        release();
+        cudaSetDevice(device);
+      }
       dev = device;
     }
     if (!st[0])
