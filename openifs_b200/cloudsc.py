@@ -12,6 +12,7 @@ There is no CPU fallback: if the library is missing or no GPU is present the
 calls raise.
 """
 import ctypes
+import functools
 import os
 
 import numpy as np
@@ -155,10 +156,46 @@ def _ptr(x):
     return x.data_ptr()
 
 
+@functools.lru_cache(maxsize=64)
+def _batched_spec(nproma, klev, ngpblks):
+    """(name, numpy dtype, element count) of every batched array."""
+    from .fields import DTYPE, batched_shape
+    return tuple((n, np.dtype(DTYPE[n]), int(np.prod(batched_shape(n, ngpblks, nproma, klev))))
+                 for n, *_ in BATCHED_FIELDS)
+
+
+def _check_batched(arrays, nproma, klev, ngpblks, device):
+    """Every array of fields.BATCHED_FIELDS is present with its dtype and its
+    (NGPBLKS, ..., NPROMA) element count, on the CUDA device (device=True) or
+    in host memory: the C ABI takes bare pointers and cannot check them.
+    Raises CloudscError with the C ABI's codes (-1 missing, -2 shape)."""
+    for n, dt, want in _batched_spec(int(nproma), int(klev), int(ngpblks)):
+        x = arrays.get(n)
+        if x is None:
+            raise CloudscError(-1, f"{n}: array missing")
+        if isinstance(x, np.ndarray):
+            if device:
+                raise CloudscError(-2, f"{n}: a device tensor is needed, not a numpy array")
+            ok_dtype, size = x.dtype == dt, x.size
+        else:
+            if x.is_cuda != device:
+                raise CloudscError(-2, f"{n}: tensor must be on {'the GPU' if device else 'the host'}")
+            ok_dtype = x.element_size() == dt.itemsize and x.is_floating_point() == (dt.kind == "f")
+            size = x.numel()
+        if not ok_dtype:
+            raise CloudscError(-2, f"{n}: dtype must be {dt.name}")
+        if size < want:
+            raise CloudscError(-2, f"{n}: {size} elements, the shape needs {want}")
+
+
 def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64,
-                    stream=None, counter=None):
+                    stream=None, counter=None, validate=True):
     """One persistent launch over all blocks; ``arrays`` are CUDA tensors in
-    the fields.BATCHED_FIELDS layout.  Asynchronous on ``stream``."""
+    the fields.BATCHED_FIELDS layout.  Asynchronous on ``stream``.
+    ``validate=False`` skips the Python-side array checks and leaves only
+    the C ABI's own (for callers that pass raw pointers' owners)."""
+    if validate:
+        _check_batched(arrays, nproma, klev, ngpblks, device=True)
     args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
     s = None
     if stream is not None:
@@ -169,9 +206,11 @@ def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, preci
 
 
 def cloudsc_batched_host(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64,
-                         chunk_blocks=0):
+                         chunk_blocks=0, validate=True):
     """All blocks from host arrays (numpy, or pinned torch CPU tensors), with
     transfers pipelined against compute.  Synchronous."""
+    if validate:
+        _check_batched(arrays, nproma, klev, ngpblks, device=False)
     args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
     return _check(lib().cloudsc_b200_batched_host(
         ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),

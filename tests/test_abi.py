@@ -46,23 +46,36 @@ def test_error_codes_without_device_work(built):
     # a NULL array
     with pytest.raises(cloudsc.CloudscError) as e:
         cloudsc.cloudsc_batched(p, {**arrs, **{n: np.zeros(1) for n in fields.INPUT_NAMES}},
-                                32, 137, 2, 64, 3600.0)
+                                32, 137, 2, 64, 3600.0, validate=False)
     assert e.value.code == -1
     full = {n: np.zeros(1) for n, *_ in fields.BATCHED_FIELDS}
     # NGPTOT inconsistent with NPROMA*NGPBLKS
     with pytest.raises(cloudsc.CloudscError) as e:
-        cloudsc.cloudsc_batched(p, full, 32, 137, 2, 65, 3600.0)
+        cloudsc.cloudsc_batched(p, full, 32, 137, 2, 65, 3600.0, validate=False)
     assert e.value.code == -2
     # KLEV smaller than NCLDTOP
     with pytest.raises(cloudsc.CloudscError) as e:
-        cloudsc.cloudsc_batched(p, full, 32, 10, 2, 64, 3600.0)
+        cloudsc.cloudsc_batched(p, full, 32, 10, 2, 64, 3600.0, validate=False)
     assert e.value.code == -2
     # parameters that differ from the uploaded ones
     q = p.copy()
     q.ramid = 0.9
     with pytest.raises(cloudsc.CloudscError) as e:
-        cloudsc.cloudsc_batched(q, full, 32, 137, 2, 64, 3600.0)
+        cloudsc.cloudsc_batched(q, full, 32, 137, 2, 64, 3600.0, validate=False)
     assert e.value.code == -5
+    # the Python mirror checks presence, dtype, size and placement first
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc.cloudsc_batched(p, full, 32, 137, 2, 64, 3600.0)
+    assert e.value.code == -2
+    host = fields.alloc(2, 32, 137)
+    cloudsc._check_batched(host, 32, 137, 2, device=False)  # the right shapes pass
+    bad = dict(host, pt=host["pt"].astype(np.float32))
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc._check_batched(bad, 32, 137, 2, device=False)
+    assert e.value.code == -2
+    with pytest.raises(cloudsc.CloudscError) as e:
+        cloudsc._check_batched({k: v for k, v in host.items() if k != "ktype"}, 32, 137, 2, device=False)
+    assert e.value.code == -1
     # bad launch shape
     with pytest.raises(cloudsc.CloudscError):
         cloudsc.set_launch(0, 48, 0)
