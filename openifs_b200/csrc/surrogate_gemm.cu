@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(128, 1)
         if (!in_range) continue;
         const size_t o = (size_t)row * BN + c0;
         if (EPI == CS_EPI_SILU) {
-          __align__(16) __nv_bfloat16 h[32], z[32];
+          __align__(32) __nv_bfloat16 h[32], z[32];
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
             float zz = v[i] + (a.bias ? a.bias[c0 + i] : 0.0f);
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(128, 1)
             d[i] = w;
           }
         } else {  // CS_EPI_BWD: g = acc (+ residual gradient); dz = g * SiLU'(zprev)
-          __align__(16) __nv_bfloat16 g[32], dz[32];
+          __align__(32) __nv_bfloat16 g[32], dz[32];
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
             float gg = v[i];
@@ -231,13 +231,33 @@ __global__ void __launch_bounds__(128, 1)
 
 // ------------------------------------------------------------------ epilogue
 // 32 accumulator columns c0..c0+31 of output row `row` (fused epilogue).
-// 32 bf16 of row-major storage as 4 x 16-byte loads.
+// Each thread owns 64 (bf16) or 128 (f32) contiguous bytes of one row and
+// moves them with 32-byte accesses (sm_100 256-bit loads and stores): a warp
+// access then fills whole 32-byte sectors.  Every address is a multiple of
+// 32 bytes: rows are 128 or 256 bytes, c0 is a multiple of 32 elements, and
+// cs_conv_gemm requires 32-byte aligned epilogue arrays.
+__device__ __forceinline__ void st256(void *p, const uint32_t *w) {
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(w[0]), "r"(w[1]), "r"(w[2]),
+               "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+               : "memory");
+}
+__device__ __forceinline__ void ld256_nc(const void *p, uint32_t *w) {
+  asm volatile("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+               : "l"(p));
+}
+// 32 bf16 of row-major storage as 2 x 32-byte loads.
 __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16 *p, float (&f)[32]) {
-  __align__(16) __nv_bfloat16 t[32];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) ((uint4 *)t)[q] = __ldg((const uint4 *)p + q);
+  __align__(32) __nv_bfloat16 t[32];
+  ld256_nc(p, (uint32_t *)t);
+  ld256_nc(p + 16, (uint32_t *)t + 8);
 #pragma unroll
   for (int i = 0; i < 32; ++i) f[i] = __bfloat162float(t[i]);
+}
+// 32 bf16 as 2 x 32-byte stores.
+__device__ __forceinline__ void store_bf16x32(__nv_bfloat16 *p, const __nv_bfloat16 (&h)[32]) {
+  st256(p, (const uint32_t *)h);
+  st256(p + 16, (const uint32_t *)h + 8);
 }
 
 template <int BN, int EPI>
@@ -247,7 +267,7 @@ __device__ __forceinline__ void epilogue32(const Args &a, const float (&v)[32], 
   if (EPI == CS_EPI_SILU) {
     float r[32];
     if (a.resid) load_bf16x32(a.resid + o, r);
-    __align__(16) __nv_bfloat16 h[32], z[32];
+    __align__(32) __nv_bfloat16 h[32], z[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
       float zz = v[i] + bias[c0 + i];
@@ -260,30 +280,22 @@ __device__ __forceinline__ void epilogue32(const Args &a, const float (&v)[32], 
       z[i] = __float2bfloat16(zz);
       h[i] = __float2bfloat16(hh);
     }
-    uint4 *dh = (uint4 *)(a.out + o);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) dh[i] = ((uint4 *)h)[i];
-    if (a.out_pre) {
-      uint4 *dz = (uint4 *)(a.out_pre + o);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) dz[i] = ((uint4 *)z)[i];
-    }
+    store_bf16x32(a.out + o, h);
+    if (a.out_pre) store_bf16x32(a.out_pre + o, z);
   } else if (EPI == CS_EPI_LINEAR_F32) {
-    float4 *d = (float4 *)(a.outf + o);
+    float *d = a.outf + o;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float4 w;
-      w.x = valid ? v[4 * i + 0] + bias[c0 + 4 * i + 0] : 0.0f;
-      w.y = valid ? v[4 * i + 1] + bias[c0 + 4 * i + 1] : 0.0f;
-      w.z = valid ? v[4 * i + 2] + bias[c0 + 4 * i + 2] : 0.0f;
-      w.w = valid ? v[4 * i + 3] + bias[c0 + 4 * i + 3] : 0.0f;
-      d[i] = w;
+    for (int i = 0; i < 4; ++i) {
+      uint32_t w[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) w[j] = __float_as_uint(valid ? v[8 * i + j] + bias[c0 + 8 * i + j] : 0.0f);
+      st256(d + 8 * i, w);
     }
   } else {  // CS_EPI_BWD
     float r[32], zp[32];
     if (a.resid) load_bf16x32(a.resid + o, r);
     load_bf16x32(a.zprev + o, zp);
-    __align__(16) __nv_bfloat16 g[32], dz[32];
+    __align__(32) __nv_bfloat16 g[32], dz[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
       float gg = v[i];
@@ -296,14 +308,8 @@ __device__ __forceinline__ void epilogue32(const Args &a, const float (&v)[32], 
       g[i] = __float2bfloat16(gg);
       dz[i] = __float2bfloat16(d);
     }
-    uint4 *dd = (uint4 *)(a.out + o);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) dd[i] = ((uint4 *)dz)[i];
-    if (a.gout) {
-      uint4 *dg = (uint4 *)(a.gout + o);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) dg[i] = ((uint4 *)g)[i];
-    }
+    store_bf16x32(a.out + o, dz);
+    if (a.gout) store_bf16x32(a.gout + o, g);
   }
 }
 
@@ -572,9 +578,12 @@ extern "C" int cs_conv_gemm(const cs_gemm_desc *g, void *stream) {
   if (g->epi < CS_EPI_SILU || g->epi > CS_EPI_BWD) return CS_E_ARG;
   if (g->epi == CS_EPI_LINEAR_F32 ? !g->outf : !g->out) return CS_E_ARG;
   if (g->epi == CS_EPI_BWD && !g->zprev) return CS_E_ARG;
-  if (((uintptr_t)g->a | (uintptr_t)g->w | (uintptr_t)g->out | (uintptr_t)g->out_pre | (uintptr_t)g->gout |
-       (uintptr_t)g->outf) &
-      15)
+  // TMA operands on 16 bytes; the epilogue's 32-byte accesses need every
+  // array it reads or writes on 32 bytes
+  if (((uintptr_t)g->a | (uintptr_t)g->w) & 15) return CS_E_ARG;
+  if (((uintptr_t)g->out | (uintptr_t)g->out_pre | (uintptr_t)g->gout | (uintptr_t)g->outf |
+       (uintptr_t)g->resid | (uintptr_t)g->zprev) &
+      31)
     return CS_E_ARG;
   // warp-specialised kernel: all weights resident in shared memory plus at
   // least two A stages of BM + halo rows
