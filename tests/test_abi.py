@@ -98,3 +98,29 @@ def test_block_entry_argument_checks(built):
 def test_bytes_per_column():
     rb, wb = fields.bytes_per_column()
     assert (rb, wb) == (28528, 25328)
+
+
+def test_gemm_rejects_misaligned_epilogue_arrays(built):
+    """cs_conv_gemm checks its arrays before any device work: TMA operands on
+    16 bytes, the epilogue's arrays on 32 bytes (its 256-bit accesses);
+    anything else returns CS_E_ARG without a launch."""
+    import ctypes
+    import torch
+    from openifs_b200 import tcgemm
+    a = torch.zeros(256, 128, dtype=torch.bfloat16)
+    w = torch.zeros(1, 128, 128, dtype=torch.bfloat16)
+    out = torch.zeros(256 * 128 + 16, dtype=torch.bfloat16)
+    fn = tcgemm._lib_fn()
+
+    def call(out_ptr, resid_ptr=None):
+        d = tcgemm.GemmDesc(a.data_ptr(), w.data_ptr(), 256, 128, 128, 1, 0, 0, tcgemm.EPI_SILU, None,
+                            out_ptr, None, resid_ptr, None, None, None, None)
+        return fn(ctypes.byref(d), None)
+
+    base = out.data_ptr()
+    assert base % 32 == 0
+    assert call(base + 16) == -2            # 16-byte aligned output: rejected
+    assert call(base, a.data_ptr() + 16) == -2  # residual off by 16 bytes
+    d = tcgemm.GemmDesc(a.data_ptr() + 8, w.data_ptr(), 256, 128, 128, 1, 0, 0, tcgemm.EPI_SILU, None,
+                        base, None, None, None, None, None, None)
+    assert fn(ctypes.byref(d), None) == -2  # TMA operand off by 8 bytes
