@@ -484,7 +484,11 @@ def _surrogate_run(a, path, p, batches, d, ref, dev, world, ms64):
             r, g = r[:, :4], g[:, :4]
         if n in ("pfplsl", "pfplsn"):
             r, g = r[:, -1], g[:, -1]
-        err[n] = {"rms_over_rms": float((g - r).pow(2).mean().sqrt() / r.pow(2).mean().sqrt())}
+        # the method without a network: each level's mean FP64 value over the batch
+        clim = r.mean(dim=(0, r.dim() - 1), keepdim=True).expand_as(r)
+        rr = r.pow(2).mean().sqrt()
+        err[n] = {"rms_over_rms": float((g - r).pow(2).mean().sqrt() / rr),
+                  "level_mean_baseline_rms_over_rms": float((clim - r).pow(2).mean().sqrt() / rr)}
     nf = min(flagged[0], runner.cap)
     closure = _closure(p, d, states[0].plude_in, states[0].flagged[:nf])
     # the FP64 kernel's own non-closure on the same columns (CLOUDSC applies

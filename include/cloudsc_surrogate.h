@@ -146,8 +146,9 @@ typedef struct cs_guard {
   int32_t capacity;      /* length of the flagged-column list                   */
 } cs_guard;
 
-/* Turn the network output y ([rows][64] f32, head h at column 32h) into CLOUDSC
- * outputs: mean of the heads, de-normalised; condensates that the step would
+/* Turn the network output y ([rows][64] f32, head h at column 32h, 16-byte
+ * aligned: CS_E_ARG otherwise) into CLOUDSC outputs: mean of the heads,
+ * de-normalised; condensates that the step would
  * drive negative are refilled from vapour with their latent heat (as
  * CLOUDSC's own clean-up does, cloudsc.F90:3779-3809); LOC_Q is then shifted
  * by a column constant so that the water budget closes with the predicted

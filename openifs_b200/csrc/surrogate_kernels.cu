@@ -123,7 +123,8 @@ __global__ void raw_features_kernel(Cols C, float *feat) {
 // Input preparation in two passes: (1) the normalised features of every
 // (column, level) once, bf16 [ncol*lp][32] (threads level-major: a warp reads
 // one level of 32 neighbouring columns); (2) the 5-level im2col window of every
-// row (threads row-major: a warp writes 32 consecutive 256-byte rows).
+// row, 16 threads per 256-byte row, each storing one 16-byte chunk (8 of the
+// 128 slots), so that a warp writes two whole consecutive rows per store.
 __global__ void features_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *fb) {
   const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
   const long long n = (long long)ncol * lp;
@@ -144,29 +145,26 @@ __global__ void features_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *fb) {
   }
 }
 
+// Slot e = tap * CS_NIN + ch of row r (level k = r % lp - 2) holds feature ch
+// of level k + tap - 2; slots 125..127, padding rows and levels outside the
+// column are zero.  Only in-column rows of fb are read.
 __global__ void im2col_kernel(const __nv_bfloat16 *__restrict__ fb, long long rows, int lp, int klev,
                               __nv_bfloat16 *x0) {
-  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows; r += (long long)gridDim.x * blockDim.x) {
+  const long long n = rows * 16;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const long long r = t >> 4;
+    const int j = (int)(t & 15);
     const int k = (int)(r % lp) - 2;
-    __align__(16) __nv_bfloat16 row[128];
+    const bool kin = k >= 0 && k < klev;
+    __align__(16) __nv_bfloat16 v[8];
 #pragma unroll
-    for (int i = 0; i < 128; ++i) row[i] = __float2bfloat16(0.0f);
-    if (k >= 0 && k < klev) {
-#pragma unroll
-      for (int tap = 0; tap < 5; ++tap) {
-        const int ks = k + tap - 2;
-        if (ks < 0 || ks >= klev) continue;
-        __align__(16) __nv_bfloat16 f[32];
-        const uint4 *s4 = (const uint4 *)(fb + (r + tap - 2) * 32);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) ((uint4 *)f)[q] = __ldg(s4 + q);
-#pragma unroll
-        for (int ch = 0; ch < CS_NIN; ++ch) row[tap * CS_NIN + ch] = f[ch];
-      }
+    for (int i = 0; i < 8; ++i) {
+      const int e = 8 * j + i;
+      const int tap = e / CS_NIN, ch = e - tap * CS_NIN;
+      const int ks = k + tap - 2;
+      v[i] = (kin && tap < 5 && ks >= 0 && ks < klev) ? fb[(r + tap - 2) * 32 + ch] : __float2bfloat16(0.0f);
     }
-    uint4 *d = (uint4 *)(x0 + r * 128);
-#pragma unroll
-    for (int i = 0; i < 16; ++i) d[i] = ((uint4 *)row)[i];
+    ((uint4 *)(x0 + r * 128))[j] = *(const uint4 *)v;
   }
 }
 
@@ -389,12 +387,21 @@ __global__ void post_kernel(Cols C, const float *__restrict__ y, int nheads, cs_
     double pr = 0.0, ps = 0.0;
     for (int k = 0; k < klev; ++k) {
       const size_t r = (size_t)col * lp + 2 + k;
+      // channels 0..11 of each head as three 16-byte loads (rows are 256 bytes)
+      __align__(16) float ya[12], yb[12];
+      const float4 *yr = (const float4 *)(y + r * ys);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) ((float4 *)ya)[q] = __ldg(yr + q);
+      if (nheads == 2) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) ((float4 *)yb)[q] = __ldg(yr + 8 + q);
+      }
       float yv[CS_NOUT];
 #pragma unroll
       for (int i = 0; i < CS_NOUT; ++i) {
-        float a = y[r * ys + i];
+        float a = ya[i];
         if (nheads == 2) {
-          const float b = y[r * ys + 32 + i];
+          const float b = yb[i];
           if (i < 7) {
             spread2 += (double)(a - b) * (double)(a - b);
             ++spread_n;
@@ -559,8 +566,8 @@ int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *fbuf, void *x0
   Cols C{*c};
   const long long n = (long long)c->nproma * c->ngpblks * c->lp;
   features_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)fbuf);
-  im2col_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)fbuf, n, c->lp, c->klev,
-                                                                    (__nv_bfloat16 *)x0);
+  im2col_kernel<<<grid_1d(n * 16, 256), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)fbuf, n, c->lp,
+                                                                         c->klev, (__nv_bfloat16 *)x0);
   return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
 }
 
@@ -624,7 +631,8 @@ int cs_adamw(float *p, float *g, float *m, float *v, int32_t taps, int32_t n, in
 int cs_post(const cs_columns *c, const float *y, int32_t nheads, const cs_guard *g, int32_t *nflagged,
             int32_t *flagged, float *diag, void *stream) {
   using namespace sk;
-  if (!cols_ok(c) || !y || !g || !nflagged || (g->capacity > 0 && !flagged) || nheads < 1 || nheads > 2)
+  if (!cols_ok(c) || !y || (uintptr_t)y % 16 || !g || !nflagged || (g->capacity > 0 && !flagged) || nheads < 1 ||
+      nheads > 2)
     return CS_E_ARG;
   Cols C{*c};
   const int ncol = c->nproma * c->ngpblks;

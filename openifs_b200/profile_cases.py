@@ -11,6 +11,10 @@ ends by itself in a minute or two.  Run the same command without ncu first.
     python -m openifs_b200.profile_cases conv5 --columns 8192 --repeat 2
         the surrogate's 5-tap level convolution (width 128, SiLU and
         residual epilogue) on 8,192 columns x 144 rows, called twice
+    python -m openifs_b200.profile_cases surrogate --blocks 256 --repeat 2
+        the guarded surrogate (committed width-128 weights: input
+        preparation, network, guard, FP64 fallback of the flagged columns)
+        over 256 NPROMA blocks of 128 (32,768 columns), seed 2, run twice
 
 Each prints "ok" and exits 0 when the case ran.
 """
@@ -59,9 +63,24 @@ def run_conv5(columns, repeat, width=128, lp=144):
     torch.cuda.synchronize()
 
 
+def run_surrogate(blocks, repeat, nproma=128):
+    import torch
+    from . import cloudsc, inputs, surrogate as S
+    p = cloudsc.default_params()
+    cloudsc.setup(p)
+    host = inputs.generate(blocks, nproma, p, seed=SEED)
+    d = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    net = S.Net.load(S.WEIGHTS)
+    run = S.Runner(net, p, nproma, blocks, capacity=nproma * blocks // 16)
+    b = run.prepare(d)
+    for _ in range(repeat):
+        run.run(b)
+    torch.cuda.synchronize()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("case", choices=["cloudsc", "satadj", "conv5"])
+    ap.add_argument("case", choices=["cloudsc", "satadj", "conv5", "surrogate"])
     ap.add_argument("--blocks", type=int, default=None)
     ap.add_argument("--columns", type=int, default=8192)
     ap.add_argument("--precision", type=int, default=0)
@@ -71,6 +90,8 @@ def main(argv=None):
         run_cloudsc(a.blocks or 518, a.precision)
     elif a.case == "satadj":
         run_satadj(a.blocks or 256, a.repeat or 3)
+    elif a.case == "surrogate":
+        run_surrogate(a.blocks or 256, a.repeat or 2)
     else:
         run_conv5(a.columns, a.repeat or 2)
     print("ok")

@@ -124,3 +124,27 @@ def test_gemm_rejects_misaligned_epilogue_arrays(built):
     d = tcgemm.GemmDesc(a.data_ptr() + 8, w.data_ptr(), 256, 128, 128, 1, 0, 0, tcgemm.EPI_SILU, None,
                         base, None, None, None, None, None, None)
     assert fn(ctypes.byref(d), None) == -2  # TMA operand off by 8 bytes
+
+
+def test_post_rejects_misaligned_network_output(built):
+    """cs_post reads the network output 16 bytes at a time: an output array
+    that is not 16-byte aligned returns CS_E_ARG before any launch."""
+    import ctypes
+    import torch
+    from openifs_b200 import surrogate as S
+    p = cloudsc.default_params()
+    nproma, nblk = 32, 1
+    tdt = lambda dt: torch.float64 if np.dtype(dt) == np.float64 else torch.int32
+    dev = fields.alloc(nblk, nproma, S.KLEV, alloc_fn=lambda shape, dt: torch.zeros(shape, dtype=tdt(dt)))
+    colsum = torch.zeros(nproma * nblk, S.KLEV, 2)
+    c = S.columns(dev, nproma, nblk, colsum, p)
+    y = torch.zeros(nproma * nblk * S.LP * 64 + 8)
+    assert y.data_ptr() % 16 == 0
+    g = S.Guard()
+    g.capacity = 0
+    nflag = torch.zeros(1, dtype=torch.int32)
+    L = S._lib()
+    rc = L.cs_post(ctypes.byref(c), y.data_ptr() + 4, 2, ctypes.byref(g), nflag.data_ptr(), None, None, None)
+    assert rc == -2
+    rc = L.cs_post(ctypes.byref(c), y.data_ptr() + 8, 2, ctypes.byref(g), nflag.data_ptr(), None, None, None)
+    assert rc == -2

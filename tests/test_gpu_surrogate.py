@@ -132,3 +132,81 @@ def test_guarded_inference_closes_budgets(small_data):
     assert er.max() < 1e-10, er.max()
     # PLUDE as CLOUDSC writes it, on every column
     assert np.array_equal(out["plude"], r["plude"])
+
+
+def test_inference_inputs_match_training_inputs(cuda):
+    """The inference input x0 (cs_prep_inputs: normalised features, then the
+    5-level window) is bit-identical to the training input built from the raw
+    features of the same columns (cs_raw_features + cs_prep_batch), and every
+    window slot holds the feature of the level it names."""
+    import ctypes
+    import torch
+    p, _ = util.params()
+    nproma, nblk = 64, 3
+    ncol, rows = nproma * nblk, nproma * nblk * S.LP
+    host = inputs.generate(nblk, nproma, p, seed=5)
+    dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    colsum = torch.empty(ncol, S.KLEV, 2, device="cuda")
+    c = S.columns(dev, nproma, nblk, colsum, p)
+    L, s = S._lib(), S._stream()
+    net = S.Net.load(S.WEIGHTS)
+    S._ok(L.cs_column_sums(ctypes.byref(c), S._p(colsum), s), "cs_column_sums")
+    fbuf = torch.empty(rows, 32, dtype=torch.bfloat16, device="cuda")
+    x0 = torch.full((rows, 128), float("nan"), dtype=torch.bfloat16, device="cuda")
+    S._ok(L.cs_prep_inputs(ctypes.byref(c), ctypes.byref(net.norm), S._p(fbuf), S._p(x0), s), "cs_prep_inputs")
+    feat = torch.empty(rows, S.FSTRIDE, device="cuda")
+    S._ok(L.cs_raw_features(ctypes.byref(c), S._p(feat), s), "cs_raw_features")
+    tgt = torch.zeros(rows, 16, device="cuda")
+    order = torch.arange(ncol, dtype=torch.int32, device="cuda")
+    x0t = torch.full_like(x0, float("nan"))
+    tb = torch.empty(rows, 16, device="cuda")
+    S._ok(L.cs_prep_batch(S._p(feat), S._p(tgt), S._p(order), ncol, S.LP, S.KLEV, ctypes.byref(net.norm),
+                          S._p(x0t), S._p(tb), s), "cs_prep_batch")
+    torch.cuda.synchronize()
+    assert torch.equal(x0.view(torch.int16), x0t.view(torch.int16))
+    fb = fbuf.view(ncol, S.LP, 32)[..., :25]
+    want = torch.zeros(ncol, S.LP, 128, dtype=torch.bfloat16, device="cuda")
+    for tap in range(5):
+        lo, hi = max(0, 2 - tap), min(S.KLEV, S.KLEV + 2 - tap)  # levels k whose k + tap - 2 exists
+        want[:, 2 + lo:2 + hi, 25 * tap:25 * tap + 25] = fb[:, lo + tap:hi + tap]
+    assert torch.equal(x0.view(ncol, S.LP, 128).view(torch.int16), want.view(torch.int16))
+
+
+def test_trained_network_beats_the_methods_without_it(cuda):
+    """What training buys, on 1,024 columns of a seed no training chunk used:
+    the committed width-128 network (no column flagged, so every output is the
+    network's, after the guard's closure shifts) against the same network
+    untrained and against each level's mean FP64 tendency over these very
+    columns (a climatology that has seen the answers).  Relative RMS errors
+    against the FP64 kernel; the climatology scores about 0.94-0.99 here."""
+    import torch
+    p, _ = util.params()
+    nproma, nblk = 128, 8
+    host = inputs.generate(nblk, nproma, p, seed=4242)
+    cloudsc.setup(p)
+    ref = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    cloudsc.cloudsc_batched(p, ref, nproma, S.KLEV, nblk, nproma * nblk, util.PTSPHY)
+    trained = S.Net.load(S.WEIGHTS)
+    untrained = S.Net(trained.width, seed=3)
+    untrained.norm, untrained.out_scale = trained.norm, trained.out_scale
+
+    def predict(net):
+        dev = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+        run = S.Runner(net, p, nproma, nblk, capacity=nproma, neg_tol=1e30, closure_tol=1e30, spread_tol=1e30)
+        b = run.prepare(dev)
+        run.run(b)
+        torch.cuda.synchronize()
+        assert int(b.nflag.item()) == 0
+        return dev
+
+    def rel(g, r):
+        return float((g - r).pow(2).mean().sqrt() / r.pow(2).mean().sqrt())
+
+    out_t, out_u = predict(trained), predict(untrained)
+    for n, m in [("tendency_loc_t", None), ("tendency_loc_q", None), ("tendency_loc_a", None),
+                 ("tendency_loc_cld", 0), ("tendency_loc_cld", 1), ("tendency_loc_cld", 2), ("tendency_loc_cld", 3)]:
+        pick = (lambda a: a) if m is None else (lambda a, m=m: a[:, m])
+        r = pick(ref[n])
+        clim = r.mean(dim=(0, 2), keepdim=True).expand_as(r)
+        e_t, e_u, e_c = rel(pick(out_t[n]), r), rel(pick(out_u[n]), r), rel(clim, r)
+        assert e_t < 0.5 * e_c and e_t < 0.5 * e_u, (n, m, e_t, e_u, e_c)
