@@ -147,24 +147,52 @@ __global__ void features_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *fb) {
 
 // Slot e = tap * CS_NIN + ch of row r (level k = r % lp - 2) holds feature ch
 // of level k + tap - 2; slots 125..127, padding rows and levels outside the
-// column are zero.  Only in-column rows of fb are read.
-__global__ void im2col_kernel(const __nv_bfloat16 *__restrict__ fb, long long rows, int lp, int klev,
-                              __nv_bfloat16 *x0) {
-  const long long n = rows * 16;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const long long r = t >> 4;
-    const int j = (int)(t & 15);
-    const int k = (int)(r % lp) - 2;
-    const bool kin = k >= 0 && k < klev;
-    __align__(16) __nv_bfloat16 v[8];
+// column are zero.  A CTA takes IM_ROWS consecutive rows: it stages their
+// feature rows and two on either side in shared memory (16-byte loads), then
+// assembles each 16-byte chunk of the window there.
+constexpr int IM_ROWS = 64;
+constexpr int IM_THREADS = 256;  // a multiple of 16: each thread keeps one chunk j of every row it writes
+
+__global__ void __launch_bounds__(IM_THREADS) im2col_kernel(const __nv_bfloat16 *__restrict__ fb, long long rows,
+                                                            int lp, int klev, __nv_bfloat16 *x0) {
+  __shared__ __align__(16) __nv_bfloat16 st[(IM_ROWS + 4) * 32];
+  // this thread's chunk j and, per slot q of it, the tap and the staged offset tap * 32 + ch
+  const int j = threadIdx.x & 15;
+  int tapq[8], offq[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int e = 8 * j + i;
-      const int tap = e / CS_NIN, ch = e - tap * CS_NIN;
-      const int ks = k + tap - 2;
-      v[i] = (kin && tap < 5 && ks >= 0 && ks < klev) ? fb[(r + tap - 2) * 32 + ch] : __float2bfloat16(0.0f);
+  for (int q = 0; q < 8; ++q) {
+    const int e = 8 * j + q, tap = e / CS_NIN;
+    tapq[q] = tap;
+    offq[q] = tap * 32 + (e - tap * CS_NIN);
+  }
+  const long long ntiles = (rows + IM_ROWS - 1) / IM_ROWS;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long r0 = tile * IM_ROWS;
+    for (int i = threadIdx.x; i < (IM_ROWS + 4) * 4; i += IM_THREADS) {
+      const long long rs = r0 - 2 + i / 4;  // staged row i / 4 is feature row rs
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (rs >= 0 && rs < rows) v = __ldg((const uint4 *)(fb + rs * 32) + (i & 3));
+      ((uint4 *)st)[i] = v;
     }
-    ((uint4 *)(x0 + r * 128))[j] = *(const uint4 *)v;
+    const int rr0 = (int)(r0 % lp);  // row of r0 within its column
+    __syncthreads();
+    for (int lr = threadIdx.x >> 4; lr < IM_ROWS; lr += IM_THREADS / 16) {
+      const long long r = r0 + lr;
+      if (r >= rows) break;
+      int rr = rr0 + lr;  // row r within its column
+      while (rr >= lp) rr -= lp;
+      const int k = rr - 2;
+      const bool kin = k >= 0 && k < klev;
+      __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int ks = k + tapq[q] - 2;
+        // feature row r + tap - 2 is staged row lr + tap
+        v[q] = (kin && tapq[q] < 5 && ks >= 0 && ks < klev) ? st[lr * 32 + offq[q]] : __float2bfloat16(0.0f);
+      }
+      ((uint4 *)(x0 + r * 128))[j] = *(const uint4 *)v;
+    }
+    __syncthreads();
   }
 }
 
@@ -566,8 +594,10 @@ int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *fbuf, void *x0
   Cols C{*c};
   const long long n = (long long)c->nproma * c->ngpblks * c->lp;
   features_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)fbuf);
-  im2col_kernel<<<grid_1d(n * 16, 256), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)fbuf, n, c->lp,
-                                                                         c->klev, (__nv_bfloat16 *)x0);
+  const long long tiles = (n + IM_ROWS - 1) / IM_ROWS;
+  const int im_grid = (int)(tiles < 148LL * 8 ? tiles : 148LL * 8);
+  im2col_kernel<<<im_grid, IM_THREADS, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)fbuf, n, c->lp, c->klev,
+                                                           (__nv_bfloat16 *)x0);
   return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
 }
 

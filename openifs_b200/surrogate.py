@@ -469,11 +469,30 @@ class Runner:
         ga, na = b.gather
         _ok(L.cs_move_columns(_p(ga), na, self.nproma, self.nproma, _p(b.flagged), _p(b.nflag), self.cap,
                               0, s), "cs_move_columns")
-        cloudsc.cloudsc_batched(self.params, self.compact, self.nproma, KLEV, self.cap // self.nproma, self.cap,
-                                self.ptsphy, stream=s)
+        self._fallback(s)
         sa, nsa = b.scatter
         _ok(L.cs_move_columns(_p(sa), nsa, self.nproma, self.nproma, _p(b.flagged), _p(b.nflag), self.cap,
                               1, s), "cs_move_columns")
+
+    def _fallback(self, s):
+        """FP64 CLOUDSC on the compact batch of flagged columns.  The batch is
+        under one wave of the full-size schedule, so its time is one column's
+        walk down the levels: it runs in CTAs of about capacity / SMs columns
+        (a multiple of 32, at most 256) on the variant with the most registers
+        that holds them, which spreads the columns over every SM and leaves
+        one or two warps per scheduler.  The process-wide FP64 schedule is
+        restored afterwards (a concurrent FP64 call from another thread may
+        run with either schedule; every schedule gives the same bits)."""
+        import torch
+        nsm = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+        threads = min(256, max(32, -(-self.cap // (nsm * 32)) * 32))
+        prev = cloudsc.get_schedule(cloudsc.FP64)
+        cloudsc.set_launch(cloudsc.FP64, threads, 0)
+        try:
+            cloudsc.cloudsc_batched(self.params, self.compact, self.nproma, KLEV, self.cap // self.nproma, self.cap,
+                                    self.ptsphy, stream=s)
+        finally:
+            cloudsc.set_schedule(cloudsc.FP64, *prev)
 
     def flops_per_batch(self):
         """Multiply-add FLOPs of the network's GEMMs for one batch (padded rows included)."""
