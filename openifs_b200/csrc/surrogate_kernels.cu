@@ -121,27 +121,45 @@ __global__ void raw_features_kernel(Cols C, float *feat) {
 }
 
 // Input preparation in two passes: (1) the normalised features of every
-// (column, level) once, bf16 [ncol*lp][32] (threads level-major: a warp reads
-// one level of 32 neighbouring columns); (2) the 5-level im2col window of every
-// row, 16 threads per 256-byte row, each storing one 16-byte chunk (8 of the
-// 128 slots), so that a warp writes two whole consecutive rows per store.
-__global__ void features_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *fb) {
+// (column, level) once, bf16 [ncol*lp][32]; (2) the 5-level im2col window of
+// every row.
+// A CTA takes tiles of 32 consecutive columns x FT_ROWS consecutive rows:
+// warp w computes row r0 + w of the 32 columns (a warp reads one level of 32
+// neighbouring columns), the rows meet in shared memory, and each warp then
+// stores one column's FT_ROWS rows, FT_ROWS x 64 contiguous bytes.
+constexpr int FT_ROWS = 8;
+
+__global__ void __launch_bounds__(32 * FT_ROWS) features_kernel(Cols C, cs_norm nrm, __nv_bfloat16 *fb) {
+  __shared__ __align__(16) __nv_bfloat16 st[FT_ROWS][32][32];
   const int ncol = C.c.nproma * C.c.ngpblks, lp = C.c.lp, klev = C.c.klev;
-  const long long n = (long long)ncol * lp;
-  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-    const int r = (int)(t / ncol), col = (int)(t - (long long)r * ncol);
-    const int k = r - 2;
-    __align__(16) __nv_bfloat16 row[32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ctiles = (ncol + 31) / 32, rtiles = (lp + FT_ROWS - 1) / FT_ROWS;
+  const long long ntiles = (long long)ctiles * rtiles;
+  for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int r0 = (int)(tile / ctiles) * FT_ROWS, col0 = (int)(tile % ctiles) * 32;
+    {
+      const int r = r0 + w, col = col0 + lane, k = r - 2;
+      __align__(16) __nv_bfloat16 row[32];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) row[i] = __float2bfloat16(0.0f);
-    if (k >= 0 && k < klev) {
-      float f[CS_NIN];
-      raw_features(C, col, k, f);
-      norm_features(nrm, f, row);
+      for (int i = 0; i < 32; ++i) row[i] = __float2bfloat16(0.0f);
+      if (col < ncol && k >= 0 && k < klev) {
+        float f[CS_NIN];
+        raw_features(C, col, k, f);
+        norm_features(nrm, f, row);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) ((uint4 *)st[w][lane])[i] = ((uint4 *)row)[i];
     }
-    uint4 *d = (uint4 *)(fb + ((size_t)col * lp + r) * 32);
-#pragma unroll
-    for (int i = 0; i < 4; ++i) d[i] = ((uint4 *)row)[i];
+    __syncthreads();
+    // 32 columns x FT_ROWS rows x 4 chunks of 16 bytes; 32 consecutive
+    // chunks are one column's FT_ROWS rows
+    for (int i = threadIdx.x; i < 32 * FT_ROWS * 4; i += 32 * FT_ROWS) {
+      const int c = i / (FT_ROWS * 4), q = i - c * (FT_ROWS * 4), rr = q >> 2, part = q & 3;
+      const int col = col0 + c, r = r0 + rr;
+      if (col < ncol && r < lp)
+        ((uint4 *)(fb + ((size_t)col * lp + r) * 32))[part] = ((const uint4 *)st[rr][c])[part];
+    }
+    __syncthreads();
   }
 }
 
@@ -595,7 +613,9 @@ int cs_prep_inputs(const cs_columns *c, const cs_norm *nrm, void *fbuf, void *x0
   if (!cols_ok(c) || !nrm || !x0 || !fbuf || !c->colsum) return CS_E_ARG;
   Cols C{*c};
   const long long n = (long long)c->nproma * c->ngpblks * c->lp;
-  features_kernel<<<grid_1d(n, 128), 128, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)fbuf);
+  const long long ftiles = (long long)((c->nproma * c->ngpblks + 31) / 32) * ((c->lp + FT_ROWS - 1) / FT_ROWS);
+  const int ft_grid = (int)(ftiles < 148LL * 8 ? ftiles : 148LL * 8);
+  features_kernel<<<ft_grid, 32 * FT_ROWS, 0, (cudaStream_t)stream>>>(C, *nrm, (__nv_bfloat16 *)fbuf);
   const long long tiles = (n + IM_ROWS - 1) / IM_ROWS;
   const int im_grid = (int)(tiles < 148LL * 8 ? tiles : 148LL * 8);
   im2col_kernel<<<im_grid, IM_THREADS, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)fbuf, n, c->lp, c->klev,
