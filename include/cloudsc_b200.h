@@ -270,9 +270,11 @@ int cloudsc_b200_batched_host(
  * the shared array; to prevent that, calls are serialised by a lock inside
  * the library and each returns only after its stream has finished.  After a
  * call the array keeps that call's inputs and outputs until the next call
- * (the warning counter is cleared at the start of each call).  The first call
- * on each device looks the array's address up and should come before any
- * stream capture.
+ * (the warning counter is cleared at the start of each call).  The array's
+ * 16 MiB are reserved on a device when cloudsc_b200_setup uploads the
+ * parameters there (for another device: at the first call of any entry on
+ * it), so a caller that reserves its own GPU memory pool should call
+ * cloudsc_b200_setup first and leave room for them.
  */
 int cloudsc_b200_block_noalloc(
     const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,

@@ -53,6 +53,16 @@ struct Schedule {
 };
 Schedule g_sched[3] = {{default_variant(), 448, 0}, {default_variant(), 448, 0}, {default_variant(), 448, 0}};
 
+// The fixed device array of cloudsc_b200_block_noalloc (see that entry).  It
+// is the only device object of this file, so this file's device module --
+// and with it the array's 16 MiB -- is loaded on a device when something
+// first asks for the array's address.  ensure_params() does that when it
+// uploads the parameters to a device, so the array is reserved at
+// cloudsc_b200_setup (or at the first call on another device), not at the
+// first cloudsc_b200_block_noalloc call.
+constexpr size_t kNoAllocBytes = size_t(16) << 20;  // 16 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
 int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
   t_last_error = what;
   if (e != cudaSuccess) {
@@ -95,11 +105,6 @@ int opt_args_ok(const cloudsc_params &p, const void *pgaw, const void *pgp2dspp,
   return CLOUDSC_OK;
 }
 
-bool current_opt_on() {
-  std::lock_guard<std::mutex> lk(g_mu);
-  return g_have_params && opt_on(g_params);
-}
-
 // The cloud budget diagnostics (LCLDBUD*, cloudsc.F90:3832-4110) are on: the
 // FP64 kernel form that writes PEXTRA runs.
 bool budgets_on(const cloudsc_params &p) {
@@ -127,11 +132,6 @@ int budget_args_ok(const cloudsc_params &p, int klev, int kfldx, const void *pex
   return CLOUDSC_OK;
 }
 
-bool current_budgets_on() {
-  std::lock_guard<std::mutex> lk(g_mu);
-  return g_have_params && budgets_on(g_params);
-}
-
 Derived make_derived(const cloudsc_params &p) {
   Derived d;
   // ZCONST**RCL_KKBAUN (cloudsc.F90:2179-2181) takes one of two values; it is
@@ -155,6 +155,10 @@ int ensure_params(int *dev_out) {
   if (g_dev_gen[dev] != g_gen) {
     e = upload_params(g_params, make_derived(g_params));
     if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "parameter upload", e);
+    // load this file's module (the no-allocation entry's fixed array) now
+    void *scratch = nullptr;
+    e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaGetSymbolAddress(no-allocation array)", e);
     g_dev_gen[dev] = g_gen;
   }
   return CLOUDSC_OK;
@@ -466,19 +470,33 @@ int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t 
 // With the budget diagnostics on, the FP64 form that writes PEXTRA (kernel
 // form 3, launched with the FP64 schedule) runs instead of the plain one.
 static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaStream_t stream) {
+  // One snapshot of the schedule and the switches: the kernel form is chosen
+  // from the same parameters whose arrays are checked here, even if another
+  // thread calls cloudsc_b200_setup meanwhile.
   Schedule sc;
+  bool bud = false, opt = false, need_gaw = false, need_spp = false, need_fsd = false;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     sc = g_sched[precision];
+    if (g_have_params) {
+      bud = budgets_on(g_params);
+      opt = opt_on(g_params);
+      need_gaw = g_params.lcloud_inhomog || g_params.lrad_cloud_inhomog;
+      need_fsd = g_params.lrad_cloud_inhomog;
+      if (g_params.lspp)
+        for (int n = 0; n < 8; ++n) need_spp = need_spp || g_params.spp_on[n];
+    }
   }
   int form = precision;
-  const bool bud = current_budgets_on(), opt = current_opt_on();
   if (bud || opt) {
     if (precision != 0)
       return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics, SPP and the inhomogeneity paths are FP64 only");
     if (bud && !f.pextra)
       return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_batched_diag "
                                          "or cloudsc_b200_block");
+    if ((need_gaw && !f.pgaw) || (need_spp && !f.pgp2dspp) || (need_fsd && !f.pfsd))
+      return fail(CLOUDSC_E_UNSUPPORTED, "SPP and the inhomogeneity paths need PGP2DSPP, PGAW and PFSD: use "
+                                         "cloudsc_b200_batched_diag or cloudsc_b200_block");
     form = bud && opt ? 5 : (opt ? 4 : 3);
   }
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + sc.threads - 1) / sc.threads);
@@ -997,19 +1015,17 @@ int cloudsc_b200_batched_host(
 // ---------------------------------------------------------------------------
 // cloudsc_b200_block_noalloc: the per-block drop-in without any device
 // allocation.  Its device memory is one file-scope array, g_noalloc_scratch,
-// of kNoAllocBytes, shared by every call in the process; its address is
-// looked up once per device with cudaGetSymbolAddress.  Calls are serialised
-// by g_noalloc_mu (the array holds one block at a time).  After a call
-// returns, the array still holds that call's inputs and outputs until the
-// next call overwrites them.
+// of kNoAllocBytes, shared by every call in the process.  The array is
+// reserved on a device when cloudsc_b200_setup (or the first call of any
+// entry on that device) uploads the parameters there; every call looks its
+// device address up again with cudaGetSymbolAddress (cheap, and never stale
+// after a context reset).  Calls are serialised by g_noalloc_mu (the array
+// holds one block at a time).  After a call returns, the array still holds
+// that call's inputs and outputs until the next call overwrites them.
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr size_t kNoAllocBytes = size_t(16) << 20;  // 16 MiB
-static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
-
 std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[kMaxDev] = {nullptr};
 
 }  // namespace
 
@@ -1056,17 +1072,15 @@ int cloudsc_b200_block_noalloc(
                    " (reduce KLON or use cloudsc_b200_block)";
     return CLOUDSC_E_TOO_LARGE;
   }
-  int dev = 0;
-  rc = ensure_params(&dev);
+  rc = ensure_params(nullptr);
   if (rc) return rc;
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void *a = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
-    if (e != cudaSuccess || !a) return fail(CLOUDSC_E_CUDA, "cudaGetSymbolAddress(scratch)", e);
-    g_noalloc_ptr[dev] = a;
+  void *scratch = nullptr;
+  {
+    cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+    if (e != cudaSuccess || !scratch) return fail(CLOUDSC_E_CUDA, "cudaGetSymbolAddress(scratch)", e);
   }
-  char *base = (char *)g_noalloc_ptr[dev];
+  char *base = (char *)scratch;
   uint32_t *counter = (uint32_t *)base;
   void *d[42];
   carve(base + 256, np, kl, 1, d);

@@ -26,7 +26,9 @@
  *   log(x) = the high part of that double-double (for the one LOG CLOUDSC calls).
  *   pow(x,y) = exp(y ln x) with y ln x a double-double whose low part enters
  *           the reduced exp argument; exponents 0.5, 1.5, 2 and 3 are
- *           evaluated as sqrt(x), x*sqrt(x), x*x, x*x*x.
+ *           evaluated from sqrt(x) and products, the last two with their
+ *           rounding errors carried (fused multiply-adds) so that each
+ *           result is rounded once.
  * The code paths are branch-free (special inputs are fixed up with selects),
  * so a compiler can interleave independent calls.
  * Accuracy (tests/test_plibm.py, against glibc): exp within 1 ulp, pow within
@@ -256,15 +258,49 @@ PLIBM_FN void plibm_log_base(double x, double *lhi, double *llo) {
   plibm_log_dd(ok ? x : 1.0, lhi, llo);
 }
 
+/* x^3 rounded once: x*x = h + l and h*x = p + pe exactly (fused
+ * multiply-adds), so p + (pe + l*x) carries the exact cube to within
+ * 2^-104 relative before its one rounding -- the correctly rounded cube
+ * except at near-ties, as a correctly rounded pow(x, 3) gives.  (x*x)*x,
+ * two roundings, differs from that in about a quarter of all arguments.
+ * Outside 1e-90 < |x| < 1e90 (where the exact splits could under- or
+ * overflow) and for NaN the plain product. */
+PLIBM_FN double plibm_cube(double x) {
+  double ax = x < 0.0 ? -x : x;
+  if (!(ax > 1e-90 && ax < 1e90)) return (x * x) * x;
+  double h = x * x;
+  double l = plibm_fma(x, x, -h);
+  double p = h * x;
+  double pe = plibm_fma(h, x, -p);
+  return p + (pe + l * x);
+}
+
+/* x^1.5 rounded once: s = sqrt(x) (correctly rounded) and x - s^2 = e
+ * exactly, so sqrt(x) = s + e/(2s) to 2^-105 relative; x*s = p + pe exactly,
+ * and p + (pe + x*(e/(2s))) rounds the product with the exact root once.
+ * x*sqrt(x) rounds twice and differs from the correctly rounded x^1.5 in
+ * about a quarter of all arguments.  Outside 1e-290 < x < 1e300 (and for
+ * x <= 0 or NaN) the plain product. */
+PLIBM_FN double plibm_pow1p5(double x) {
+  double s = plibm_sqrt(x);
+  if (!(x > 1e-290 && x < 1e300)) return x * s;
+  double e = plibm_fma(-s, s, x);
+  double slo = e / (s + s);
+  double p = x * s;
+  double pe = plibm_fma(x, s, -p);
+  return p + (pe + x * slo);
+}
+
 /* x^y given plibm_log_base(x) = lhi + llo; pow(x, y) is exactly this, so
  * calls that share a base can share its logarithm. */
 PLIBM_FN_COLD double plibm_pow_special(double x, double y, double res);
 PLIBM_FN double plibm_pow_with_log(double x, double y, double lhi, double llo) {
-  /* exponents with exact-operation forms (uniform branches for constant y) */
+  /* exponents with exact-operation forms (uniform branches for constant y):
+   * sqrt and x*x are correctly rounded, the cube and x^1.5 as good as */
   if (y == 0.5) return plibm_sqrt(x);
-  if (y == 1.5) return x * plibm_sqrt(x);
+  if (y == 1.5) return plibm_pow1p5(x);
   if (y == 2.0) return x * x;
-  if (y == 3.0) return (x * x) * x;
+  if (y == 3.0) return plibm_cube(x);
   double res = plibm_pow_log(lhi, llo, y);
   if (x > 0.0 && x < PLIBM_INF && y != 0.0 && y == y) return res;
   return plibm_pow_special(x, y, res);

@@ -1,8 +1,9 @@
 """cloudsc_b200_block_noalloc, the per-block call that allocates no device
 memory (one fixed array inside the library), against the allocating
 per-block entry cloudsc_b200_block: bit-identical outputs on two calls in a
-row (the second on a different block and column range), and the size limit
-reported as CLOUDSC_E_TOO_LARGE before any device work.  This file is
+row (the second on a different block and column range), the device's free
+memory unchanged by a call, and the size limit reported as
+CLOUDSC_E_TOO_LARGE before any device work.  This file is
 collected last so that it also runs after every other GPU test."""
 import numpy as np
 import pytest
@@ -33,6 +34,40 @@ def test_noalloc_matches_block_entry_two_calls(cuda):
         assert nw == nw_ref
         for n in fields.OUTPUT_NAMES:
             assert np.array_equal(ref[n], out[n]), (ib, n)
+
+
+@pytest.mark.gpu
+def test_noalloc_takes_no_device_memory(cuda):
+    """In a thread of its own (no per-thread workspace of the allocating
+    entries), a second call of another shape leaves the device's free memory
+    exactly where the first call left it: the entry allocates nothing, and its
+    fixed array was reserved when the parameters were set up."""
+    import threading
+
+    import torch
+
+    p, _ = util.params()
+    cloudsc.setup(p)
+    got = {}
+
+    def run():
+        try:
+            for shape, (kidia, kfdia) in [(48, (1, 48)), (96, (3, 90))]:
+                blk = _block(inputs.generate(1, shape, p, seed=44 + shape), 0)
+                nw = cloudsc.cloudsc_block_noalloc(p, kidia, kfdia, shape, util.KLEV, util.PTSPHY, blk)
+                torch.cuda.synchronize()
+                got.setdefault("free", []).append(torch.cuda.mem_get_info()[0])
+                got.setdefault("nw", []).append(nw)
+        except Exception as e:  # reported in the main thread
+            got["error"] = e
+
+    t = threading.Thread(target=run)
+    t.start()
+    t.join()
+    assert "error" not in got, got.get("error")
+    first, second = got["free"]
+    assert second == first, (first, second)
+    assert got["nw"][0] >= 0 and got["nw"][1] >= 0
 
 
 def test_noalloc_rejects_blocks_above_capacity(built):
