@@ -51,6 +51,12 @@ def _args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--case", default=None, choices=sorted(CASES),
+                    help="run one small profiling case instead of the benchmark (see profile_case)")
+    ap.add_argument("--blocks", type=int, default=None, help="--case: NPROMA blocks of 128")
+    ap.add_argument("--columns", type=int, default=8192, help="--case conv5: columns")
+    ap.add_argument("--precision", type=int, default=0, help="--case cloudsc: kernel form")
+    ap.add_argument("--repeat", type=int, default=None, help="--case: calls of the kernel")
     return ap.parse_args()
 
 
@@ -135,58 +141,66 @@ def _dist():
     return world, rank, local
 
 
-def cpu_baseline(p_oracle, nblocks=64, threads=0, nproma=NPROMA, seed=SEED, seconds=10.0):
-    """The oracle (the reference algorithm restated in C, system libm) on a
-    bounded sample of the workload: ``nblocks`` NPROMA blocks of ``nproma``,
-    OpenMP over blocks (ec_phys_drv.F90:438), warm runs for about
-    ``seconds``.  Returns (best columns/s, runs, median columns/s)."""
-    from openifs_b200 import inputs
+def cpu_baseline(p_oracle, arrs, nblocks, nproma=NPROMA, seconds=10.0):
+    """The oracle (the reference algorithm restated in C, system libm) over
+    ``nblocks`` NPROMA blocks of ``arrs`` with every host thread, OpenMP over
+    blocks (ec_phys_drv.F90:438): warm runs for about ``seconds`` (at least
+    two).  The inputs are shared read-only, PLUDE (INOUT) is restored before
+    each run outside the timing, outputs go to arrays of their own.  Returns
+    (best columns/s, runs, median columns/s, outputs of the last run)."""
+    from openifs_b200 import fields
     from oracle import oracle
-    arrs = inputs.generate(nblocks, nproma, p_oracle, seed=seed)
-    work = {k: v.copy() for k, v in arrs.items()}
-    oracle.cloudsc_batched(p_oracle, work, nproma, KLEV, nblocks, nblocks * nproma, PTSPHY,
-                           threads, libm="glibc")  # warm
+    work = {k: (np.empty_like(v) if k in fields.OUTPUT_NAMES else v) for k, v in arrs.items()}
+    plude0 = arrs["plude"]
+    cols = nblocks * nproma
+
+    def once():
+        np.copyto(work["plude"], plude0)
+        t = time.perf_counter()
+        oracle.cloudsc_batched(p_oracle, work, nproma, KLEV, nblocks, cols, PTSPHY, 0, libm="glibc")
+        return time.perf_counter() - t
+
+    once()  # warm
     times = []
     t_end = time.perf_counter() + seconds
     while len(times) < 2 or time.perf_counter() < t_end:
-        work = {k: v.copy() for k, v in arrs.items()}
-        t = time.perf_counter()
-        oracle.cloudsc_batched(p_oracle, work, nproma, KLEV, nblocks, nblocks * nproma, PTSPHY,
-                               threads, libm="glibc")
-        times.append(time.perf_counter() - t)
-    cols = nblocks * nproma
-    return cols / min(times), len(times), cols / statistics.median(times)
+        times.append(once())
+    return cols / min(times), len(times), cols / statistics.median(times), work
 
 
 def run_reference(a):
+    """The reference arm: the oracle (the reference algorithm restated in C,
+    glibc libm; the Fortran cannot be compiled here) on the bench's whole
+    workload, 262,144 columns, every host thread, OpenMP over NPROMA blocks
+    (ec_phys_drv.F90:438).  One step = one call over every column; PLUDE
+    (INOUT) is restored before each step outside the timing."""
     world, rank, _ = _dist()
     if rank != 0:
         return 0
-    from openifs_b200 import cloudsc, inputs
+    from openifs_b200 import fields, inputs
     from oracle import oracle
     nc = inputs.ncldtop_l137()
     p = oracle.params_default(PTSPHY, nc)
     ncores = os.cpu_count() or 1
-    nblocks = 64
-    arrs = inputs.generate(nblocks, NPROMA, p, seed=SEED)
+    arrs = inputs.generate(NGPBLKS, NPROMA, p, seed=SEED)
+    work = {k: (np.empty_like(v) if k in fields.OUTPUT_NAMES else v) for k, v in arrs.items()}
     times = []
     for i in range(a.warmup + a.steps):
-        work = {k: v.copy() for k, v in arrs.items()}
+        np.copyto(work["plude"], arrs["plude"])
         t = time.perf_counter()
-        oracle.cloudsc_batched(p, work, NPROMA, KLEV, nblocks, nblocks * NPROMA, PTSPHY, 0,
-                               libm="glibc")
+        oracle.cloudsc_batched(p, work, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, 0, libm="glibc")
         if i >= a.warmup:
             times.append(time.perf_counter() - t)
     ms = 1e3 * statistics.mean(times)
-    val = nblocks * NPROMA / (ms * 1e-3)
-    sample = f"{nblocks} NPROMA blocks of 128 ({nblocks * NPROMA} columns) of the workload per step"
+    val = NCOL / (ms * 1e-3)
+    sample = f"the whole workload ({NGPBLKS} NPROMA blocks of {NPROMA}, {NCOL} columns) per step"
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "columns/s",
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, openifs_b200/inputs.py)",
         "config": {"workload": WORKLOAD, "columns": NCOL, "nproma": NPROMA, "klev": KLEV,
-                   "sample_columns_per_step": nblocks * NPROMA},
+                   "columns_per_step": NCOL},
         "cpu_baseline": {"value": val, "unit": "columns/s", "cores": ncores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": val, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -560,6 +574,41 @@ def _closure_cols(p, d):
     return ((w_l - w_r).abs() / w_s).reshape(-1), ((e_l - e_r).abs() / e_s).reshape(-1)
 
 
+def parity_vs_glibc(p, d, plude0, cpu_out, dev):
+    """The FP64 kernel against the CPU oracle linked with glibc (the
+    reference algorithm as a Linux build runs it) on every column of the
+    workload: the largest relative error over the defined outputs
+    (|gpu - ref| / max(|ref|, 1e-6 max|ref| of the field)) and the number of
+    branch-flip columns, columns with an element beyond 1e-12.  The kernel is
+    bit-identical to the oracle built with its own exp/log/pow (GPU tests);
+    against glibc, whose exp and pow round about 0.1 % of their results
+    differently, CLOUDSC's sort and limiters switch branches in a few
+    columns."""
+    import torch
+    from openifs_b200 import cloudsc, fields
+    d["plude"].copy_(plude0)
+    cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.FP64)
+    torch.cuda.synchronize(dev)
+    colmax = torch.zeros((NGPBLKS, NPROMA), dtype=torch.float64, device=dev)
+    per_field = {}
+    for n in fields.OUTPUT_NAMES:
+        g = d[n]
+        o = torch.from_numpy(cpu_out[n]).to(dev)
+        if n == "tendency_loc_cld":  # species NCLV is left undefined by the reference
+            g, o = g[:, :4], o[:, :4]
+        den = torch.maximum(o.abs(), 1e-6 * o.abs().max())
+        e = torch.where(den > 0, (g - o).abs() / den, torch.where(g == o, 0.0, float("inf")))
+        per_field[n] = float(e.max())
+        colmax = torch.maximum(colmax, e.reshape(NGPBLKS, -1, NPROMA).amax(dim=1))
+        del o, e, den
+    return {"oracle": "oracle/cloudsc_oracle.c linked against glibc", "columns": NCOL,
+            "max_rel": max(per_field.values()),
+            "flip_columns_over_1e-12": int((colmax > 1e-12).sum()),
+            "columns_over_1e-15": int((colmax > 1e-15).sum()),
+            "max_rel_per_field": per_field,
+            "vs_oracle_with_kernel_libm": "bit-identical (GPU tests)"}
+
+
 def run_ours(a):
     import torch
     from openifs_b200 import cloudsc, fields, inputs
@@ -725,12 +774,16 @@ def run_ours(a):
     from oracle import oracle
     po = oracle.params_default(PTSPHY, p.ncldtop)
     ncores = os.cpu_count() or 1
+    parity = None
     if world == 1:
-        cpu_val, reps, cpu_med = cpu_baseline(po)
+        cpu_val, reps, cpu_med, cpu_out = cpu_baseline(po, host, NGPBLKS)
+        parity = parity_vs_glibc(p, d, plude0, cpu_out, dev)
+        del cpu_out
         # the reference's CPU-scale case: 3,200 columns = 100 NPROMA blocks of 32, seed 1
-        c1_best, c1_reps, c1_med = cpu_baseline(po, nblocks=100, nproma=32, seed=1, seconds=3.0)
+        small = inputs.generate(100, 32, po, seed=1)
+        c1_best, c1_reps, c1_med, _ = cpu_baseline(po, small, 100, nproma=32, seconds=3.0)
         cpu_line = {"value": cpu_val, "unit": "columns/s", "cores": ncores, "kind": "port",
-                    "sample": f"64 NPROMA blocks of 128 (8,192 columns) of the workload, "
+                    "sample": f"the whole workload ({NCOL} columns = {NGPBLKS} NPROMA blocks of {NPROMA}), "
                               f"best of {reps} warm runs, OpenMP over blocks",
                     "median": cpu_med,
                     "cpu_case_3200_columns": {"nproma": 32, "blocks": 100, "seed": 1,
@@ -769,11 +822,25 @@ def run_ours(a):
         "satadj": sat,
         "sltend_supersat": slt,
         "roofline": roofline,
+        "parity_vs_glibc_oracle": parity,
         "cpu_baseline": cpu_line,
         "e2e": e2e,
         "clocks": clocks,
         "gpu_launches": a.steps,
     }
+    # the per-field errors of the reduced-precision forms and the parity
+    # summary on short lines of their own, ahead of the JSON line
+    short = {"tendency_loc_t": "T", "tendency_loc_q": "q", "tendency_loc_cld_l": "l",
+             "tendency_loc_cld_i": "i", "tendency_loc_cld_r": "r", "tendency_loc_cld_s": "s",
+             "pfplsl": "rain", "pfplsn": "snow", "tendency_loc_a": "a"}
+    for name in ("mixed", "phys32"):
+        e = errs[name]
+        print(f"# {name} vs fp64 (max|err|/max|ref| rms/rms): " +
+              " ".join(f"{short[k]} {v['max_abs_over_max']:.1e}/{v['rms_over_rms']:.1e}" for k, v in e.items()),
+              flush=True)
+    if parity:
+        print(f"# fp64 vs glibc oracle on {parity['columns']} columns: max {parity['max_rel']:.2e}, "
+              f"flip columns (>1e-12) {parity['flip_columns_over_1e-12']}", flush=True)
     print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -781,8 +848,87 @@ def run_ours(a):
     return 0
 
 
+def _case_cloudsc(a):
+    import torch
+    from openifs_b200 import cloudsc, inputs
+    blocks = a.blocks or 518
+    p = cloudsc.default_params()
+    cloudsc.setup(p)
+    arrs = inputs.generate(blocks, NPROMA, p, seed=SEED)
+    d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
+    for _ in range(a.repeat or 1):
+        cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, blocks, NPROMA * blocks, PTSPHY, precision=a.precision)
+    torch.cuda.synchronize()
+
+
+def _case_satadj(a):
+    import torch
+    from openifs_b200 import cloudsc, inputs
+    blocks = a.blocks or 256
+    p = cloudsc.default_params(PTSPHY, inputs.ncldtop_l137())
+    host = inputs.generate_satadj(blocks, NPROMA, p, seed=SEED)
+    d = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    cloudsc.setup(p)
+    for _ in range(a.repeat or 3):
+        cloudsc.satadj_batched(p, d, NPROMA, KLEV, blocks, NPROMA * blocks, PTSPHY)
+    torch.cuda.synchronize()
+
+
+def _case_conv5(a, width=128, lp=144):
+    import torch
+    from openifs_b200 import tcgemm
+    rows = a.columns * lp
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(rows, width, device="cuda", generator=g).bfloat16()
+    w5 = (torch.randn(5, width, width, device="cuda", generator=g) * 0.02).bfloat16()
+    out = torch.empty(rows, width, device="cuda", dtype=torch.bfloat16)
+    b = torch.zeros(width, device="cuda")
+    tcgemm.set_impl(0)
+    for _ in range(a.repeat or 2):
+        tcgemm.conv_gemm(x, w5, tcgemm.EPI_SILU, width, 5, lp, KLEV, b, out, None, x)
+    torch.cuda.synchronize()
+
+
+def _case_surrogate(a):
+    import torch
+    from openifs_b200 import cloudsc, inputs, surrogate as S
+    blocks = a.blocks or 256
+    p = cloudsc.default_params()
+    cloudsc.setup(p)
+    host = inputs.generate(blocks, NPROMA, p, seed=SEED)
+    d = {k: torch.from_numpy(v).cuda() for k, v in host.items()}
+    net = S.Net.load(S.WEIGHTS)
+    run = S.Runner(net, p, NPROMA, blocks, capacity=NPROMA * blocks // 16)
+    b = run.prepare(d)
+    for _ in range(a.repeat or 2):
+        run.run(b)
+    torch.cuda.synchronize()
+
+
+# Small GPU cases of the kernels, sized for an ncu capture: a few GB on the
+# device at most (inputs larger than the 126 MB L2, so DRAM counters mean
+# something) and a handful of launches, so that a capture of one launch ends
+# by itself in a minute or two; seed 2, NPROMA 128, L137 throughout.
+#   --case cloudsc [--blocks 518] [--precision 0] [--repeat 1]
+#       batched CLOUDSC over 518 blocks (66,304 columns: one wave of 148 CTAs
+#       x 448 columns) in form --precision
+#   --case satadj [--blocks 256] [--repeat 3]     CLOUD_SATADJ
+#   --case conv5 [--columns 8192] [--repeat 2]    the surrogate's 5-tap level
+#       convolution (width 128, SiLU and residual epilogue), 144 rows a column
+#   --case surrogate [--blocks 256] [--repeat 2]  the guarded surrogate with
+#       the committed width-128 weights (preparation, network, guard, FP64
+#       fallback of the flagged columns)
+# Each prints "ok" and exits 0 when the case ran.
+CASES = {"cloudsc": _case_cloudsc, "satadj": _case_satadj, "conv5": _case_conv5,
+         "surrogate": _case_surrogate}
+
+
 def main():
     a = _args()
+    if a.case:
+        CASES[a.case](a)
+        print("ok")
+        return 0
     if a.impl == "reference":
         return run_reference(a)
     return run_ours(a)

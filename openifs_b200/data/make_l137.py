@@ -28,7 +28,9 @@ def extract(namelist_text):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_l137.py <root of the OpenIFS source tree>")
+    root = sys.argv[1]
     src = os.path.join(root, "ifs-test/tests/scm/common/namelists")
     a, b = extract(open(src).read())
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "l137_ab.txt")
