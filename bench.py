@@ -245,6 +245,36 @@ def satadj_form(a, p, host, dev, world, rank, stream):
         t = torch.tensor([ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
+
+    # the same with the STATE_INCREMENT of the cumulative tendencies fused
+    # in (callpar.F90:1253-1280); the five CML arrays are restored before
+    # each step, outside the timed events
+    cml = {n: d[n].clone() for n in ("tendency_cml_t", "tendency_cml_q", "tendency_cml_a",
+                                      "tendency_cml_l", "tendency_cml_i")}
+
+    def step_inc():
+        for n, v in cml.items():
+            d[n].copy_(v)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloudsc.satadj_increment_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, stream=stream)
+        e1.record(stream)
+        return e0, e1
+
+    for _ in range(a.warmup):
+        step_inc()
+    torch.cuda.synchronize(dev)
+    ev = [step_inc() for _ in range(a.steps)]
+    torch.cuda.synchronize(dev)
+    ms_inc = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    if world > 1:
+        t = torch.tensor([ms_inc], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_inc = float(t.item())
+    for n, v in cml.items():
+        d[n].copy_(v)
+    del cml
     q, l, i, tt = (d[f"tendency_loc_{c}"] for c in "qlit")
     water = float((q + l + i).abs().max() / q.abs().max())
     enth = float((tt - p.ralvdcp * l - p.ralsdcp * i).abs().max() / tt.abs().max())
@@ -272,6 +302,8 @@ def satadj_form(a, p, host, dev, world, rank, stream):
                "sample": f"{nb} NPROMA blocks of 128, best of 3, OpenMP over blocks"}
     return {"columns_per_s": world * NCOL / (ms * 1e-3), "ms": ms,
             "parity": "bit-identical to the oracle (GPU tests)",
+            "with_state_increment": {"ms": ms_inc, "extra_ms": ms_inc - ms,
+                                     "what": "CML T/q/a/l/i += SATADJ tendencies in the same kernel"},
             "closure_max_rel": {"water": water, "enthalpy": enth},
             "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": algo / (ms * 1e-3) / 1e9 / peak, "algorithmic_bytes_per_launch": algo,
@@ -378,6 +410,55 @@ def spp_form(a, p, d, plude0, dev, world, stream, ms64):
     del diag
     torch.cuda.empty_cache()
     return out
+
+
+def state_increment_form(a, d, dev, world, stream):
+    """STATE_INCREMENT after CLOUDSC (callpar.F90:1308-1311): the cumulative
+    T, q and cloud-fraction tendencies and the four condensate species of
+    TENDENCY_CML%CLD incremented by CLOUDSC's tendencies, every column and
+    level; device time and HBM roofline (7 fields read twice and written
+    once).  The cumulative tendencies are restored before each step outside
+    the timed events."""
+    import torch
+    from openifs_b200 import cloudsc
+    cml_cld = d["tendency_cml_cld"]
+    state = {"t": d["tendency_cml_t"], "q": d["tendency_cml_q"], "a": d["tendency_cml_a"], "cld": cml_cld}
+    inc = {"t": d["tendency_loc_t"], "q": d["tendency_loc_q"], "a": d["tendency_loc_a"],
+           "cld": d["tendency_loc_cld"]}
+    keep = {n: v.clone() for n, v in state.items()}
+
+    def step():
+        for n, v in keep.items():
+            state[n].copy_(v)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        cloudsc.state_increment_batched(state, inc, NPROMA, KLEV, NGPBLKS, NCOL, stream=stream)
+        e1.record(stream)
+        return e0, e1
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ev = [step() for _ in range(a.steps)]
+    torch.cuda.synchronize(dev)
+    ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    for n, v in keep.items():
+        state[n].copy_(v)
+    del keep
+    torch.cuda.empty_cache()
+    algo = NCOL * 7 * 3 * 8 * KLEV
+    peaks = _peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    return {"ms": ms, "columns_per_s": world * NCOL / (ms * 1e-3), "fields": "T, q, a, CLD l/i/r/s",
+            "parity": "bit-identical to the oracle (GPU tests)",
+            "roofline": {"bound": "hbm", "achieved": algo / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": algo / (ms * 1e-3) / 1e9 / peak, "algorithmic_bytes_per_launch": algo,
+                         "kernel": "state_increment_kernel"}}
 
 
 def sltend_form(a, p, host, dev, world, rank, stream):
@@ -712,6 +793,7 @@ def run_ours(a):
 
     bud = budget_form(a, p, d, plude0, dev, world, stream, results["fp64"]["ms"])
     spp = spp_form(a, p, d, plude0, dev, world, stream, results["fp64"]["ms"])
+    inc = state_increment_form(a, d, dev, world, stream)
     sat = satadj_form(a, p, host, dev, world, rank, stream)
     slt = sltend_form(a, p, host, dev, world, rank, stream)
 
@@ -820,6 +902,7 @@ def run_ours(a):
         "budget_diagnostics": bud,
         "spp_inhomogeneity": spp,
         "satadj": sat,
+        "state_increment": inc,
         "sltend_supersat": slt,
         "roofline": roofline,
         "parity_vs_glibc_oracle": parity,

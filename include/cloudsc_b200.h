@@ -361,6 +361,77 @@ int cloudsc_b200_sltend_supersat_batched(
     double *padji, void *stream);
 
 /*
+ * STATE_INCREMENT (ifs-source/arpifs/phys_ec/state_increment.F90:9-105):
+ * POSTATE%X(KIDIA:KFDIA,:) = POSTATE%X(KIDIA:KFDIA,:) + PA_X(KIDIA:KFDIA,:)
+ * for every increment PA_X that is present.  CALLPAR calls it on the cloud
+ * path after CLOUD_SATADJ (callpar.F90:1278-1280: T, Q, A, QL, QI) and after
+ * CLOUDSC (:1308-1311: T, Q, A, QL, QI, QR, QS) to add the tendencies into
+ * the cumulative ones (TENDENCY_CML) that the next scheme reads.
+ *
+ * POSTATE: the state's fields (KLON, KLEV) and CLD (KLON, KLEV, NCLV), NULL
+ * where the state does not carry the field; KEYMASK: its switches as
+ * CLOUDSC_KEY_* bits -- Q, O3, A, TKE and the four condensate species are
+ * incremented only when their bit is set, U, V and T whenever their increment
+ * is present (state_increment.F90:42-103).  An increment given for a field
+ * the state lacks is an error (CLOUDSC_E_NULL).
+ */
+#define CLOUDSC_KEY_Q 0x01u
+#define CLOUDSC_KEY_O3 0x02u
+#define CLOUDSC_KEY_A 0x04u
+#define CLOUDSC_KEY_TKE 0x08u
+#define CLOUDSC_KEY_QL 0x10u
+#define CLOUDSC_KEY_QI 0x20u
+#define CLOUDSC_KEY_QR 0x40u
+#define CLOUDSC_KEY_QS 0x80u
+typedef struct cloudsc_state {
+  double *u, *v, *t, *o3, *q, *a, *cld, *tke;
+  uint32_t keymask;
+  int32_t nclv; /* species of CLD (CLOUDSC_NCLV in the default configuration) */
+} cloudsc_state;
+typedef struct cloudsc_increments {
+  const double *pa_u, *pa_v, *pa_t, *pa_o3, *pa_q, *pa_a, *pa_ql, *pa_qi, *pa_qr, *pa_qs, *pa_tke;
+  /* 0: PA_QL..PA_QS are (KLON, KLEV) arrays of their own; n > 0: each points
+   * to its species slice of one (KLON, KLEV, n) array, e.g. the four
+   * condensate slices of CLOUDSC's PTENDENCY_LOC_CLD (n = NCLV) */
+  int32_t nclv_pa;
+} cloudsc_increments;
+
+/*
+ * STATE_INCREMENT over NGPBLKS blocks with DEVICE pointers, every field
+ * stored (NPROMA, KLEV[, NCLV], NGPBLKS) like cloudsc_b200_batched: columns
+ * KIDIA..MIN(NPROMA, NGPTOT - (block-1)*NPROMA) of every block (one block of
+ * the reference's call: ngpblks = 1, ngptot = KFDIA).  One GPU thread per
+ * (column, level) point adds every present increment (one addition each,
+ * bit-identical to the reference).  Returns without synchronising.
+ */
+int cloudsc_b200_state_increment_batched(int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+                                         int32_t kidia, const cloudsc_state *postate,
+                                         const cloudsc_increments *inc, void *stream);
+
+/*
+ * CLOUD_SATADJ followed by the STATE_INCREMENT of its tendencies
+ * (callpar.F90:1253-1280) in one kernel: the arguments of
+ * cloudsc_b200_satadj_batched, with the five cumulative tendencies
+ * TENDENCY_CML%T, %Q, %A, %CLD(:,:,NCLDQL), %CLD(:,:,NCLDQI) updated in place
+ * (each point reads them once for the adjustment and writes them once,
+ * incremented, as STATE_INCREMENT does; Q, A, QL and QI only when `keymask`
+ * has their CLOUDSC_KEY_* bit).  The five TENDENCY_LOC outputs are written as
+ * by cloudsc_b200_satadj_batched.  Results bit-identical to the two calls.
+ * No reference counterpart as one routine: it fuses two consecutive calls of
+ * CALLPAR.
+ */
+int cloudsc_b200_satadj_increment_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+    double ptsphy, const double *pap, const double *paph, const double *pt, const double *pq,
+    const double *pa, const double *pl, const double *pi, double *ptendency_cml_t,
+    double *ptendency_cml_q, double *ptendency_cml_a, double *ptendency_cml_l,
+    double *ptendency_cml_i, const double *phrsw, const double *phrlw,
+    const double *ptendency_vdf_t, const double *ptendency_vdf_q, const double *pludeli,
+    const double *pvervel, double *ptendency_loc_t, double *ptendency_loc_q,
+    double *ptendency_loc_a, double *ptendency_loc_l, double *ptendency_loc_i,
+    uint32_t keymask, uint32_t *ncounters, void *stream);
+
+/*
  * cloudsc_b200_batched (FP64) with the optional configurations: the cloud
  * budget diagnostics (cloudsc.F90:3832-4110) that LCLDBUDC, LCLDBUDL,
  * LCLDBUDI, LCLDBUDT and LCLDBUD_VERTINT switch on, with LCLDBUD_TIMEINT and

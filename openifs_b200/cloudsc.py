@@ -70,6 +70,11 @@ def lib():
         ns = len(SATADJ_FIELDS)
         L.cloudsc_b200_satadj_batched.argtypes = [P, i32, i32, i32, i32, ctypes.c_double] + [vp] * ns + [vp, vp]
         L.cloudsc_b200_satadj_batched.restype = ctypes.c_int
+        L.cloudsc_b200_satadj_increment_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
+                                                            [vp] * ns + [ctypes.c_uint32, vp, vp])
+        L.cloudsc_b200_satadj_increment_batched.restype = ctypes.c_int
+        L.cloudsc_b200_state_increment_batched.argtypes = [i32] * 5 + [vp] * 3
+        L.cloudsc_b200_state_increment_batched.restype = ctypes.c_int
         L.cloudsc_b200_satadj_block.argtypes = ([P, i32, i32, i32, i32, vp, i32, ctypes.c_double] + [vp] * 16 +
                                                 [vp, vp, vp, vp, vp] + [vp] * 5 + [vp, i32])
         L.cloudsc_b200_satadj_block.restype = ctypes.c_int
@@ -334,3 +339,44 @@ def cloudsc_batched_diag(params, arrays, diag, nproma, klev, ngpblks, ngptot, pt
     st = stream.cuda_stream if stream is not None else None
     return _check(lib().cloudsc_b200_batched_diag(ctypes.byref(params), int(nproma), int(klev), int(ngpblks),
                                                   int(ngptot), float(ptsphy), *ptrs, *dptrs, kfldx, cnt, st))
+
+
+def _species_ptr(x, m):
+    """Address of species m of a (NGPBLKS, N, KLEV, NPROMA) array."""
+    return _ptr(x) + m * x.shape[2] * x.shape[3] * x.element_size()
+
+
+def state_increment_batched(state, increments, nproma, klev, ngpblks, ngptot, kidia=1, keymask=None,
+                            stream=None):
+    """STATE_INCREMENT (state_increment.F90) over every block: each field of
+    ``state`` (torch CUDA tensors, keys u, v, t, o3, q, a, cld, tke; CLD
+    (NGPBLKS, NCLV, KLEV, NPROMA)) is incremented in place by the increment
+    of the same name in ``increments`` (keys u, v, t, o3, q, a, ql, qi, qr,
+    qs, tke, or cld for a CLD-shaped array whose four condensate species are
+    added), over columns KIDIA..ICEND; Q, O3, A, TKE and the condensates only
+    where ``keymask`` (params.KEY_* bits, default all) has their bit.
+    Asynchronous on ``stream``."""
+    from .params import KEY_ALL, make_increments, make_state
+    st = make_state(state, KEY_ALL if keymask is None else keymask, _ptr)
+    inc = make_increments(increments, _ptr, _species_ptr)
+    s = stream.cuda_stream if stream is not None else None
+    f = lib().cloudsc_b200_state_increment_batched
+    return _check(f(int(nproma), int(klev), int(ngpblks), int(ngptot), int(kidia), ctypes.byref(st),
+                    ctypes.byref(inc), s))
+
+
+def satadj_increment_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, keymask=None, counter=None,
+                             stream=None):
+    """CLOUD_SATADJ followed by the STATE_INCREMENT of its five tendencies
+    into the cumulative ones (callpar.F90:1253-1280), one kernel: as
+    satadj_batched, and the tendency_cml_t/q/a/l/i tensors of ``arrays`` are
+    incremented in place (q, a, l, i only where ``keymask`` has KEY_Q,
+    KEY_A, KEY_QL, KEY_QI; default all)."""
+    from .fields import SATADJ_FIELDS
+    from .params import KEY_ALL
+    ptrs = [_ptr(arrays[n]) for n, *_ in SATADJ_FIELDS]
+    cnt = _ptr(counter) if counter is not None else None
+    st = stream.cuda_stream if stream is not None else None
+    f = lib().cloudsc_b200_satadj_increment_batched
+    return _check(f(ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
+                    *ptrs, int(KEY_ALL if keymask is None else keymask), cnt, st))

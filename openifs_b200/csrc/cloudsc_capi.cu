@@ -32,6 +32,7 @@ cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int t
                    cudaStream_t stream);
 cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream);
 cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaStream_t stream);
+cudaError_t launch_state_increment(const IncFields &f, const Shape &sh, cudaStream_t stream);
 }  // namespace cloudsc
 
 using namespace cloudsc;
@@ -1263,6 +1264,98 @@ int cloudsc_b200_sltend_supersat_batched(
                     padja, padjl, padji};
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, tsphy};
   cudaError_t e = launch_sltend_supersat(f, sh, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+// STATE_INCREMENT (state_increment.F90:9-105), batched.
+int cloudsc_b200_state_increment_batched(int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+                                         int32_t kidia, const cloudsc_state *st, const cloudsc_increments *inc,
+                                         void *stream) {
+  if (!st || !inc) return fail(CLOUDSC_E_NULL, "postate or the increments are NULL");
+  if (nproma < 1 || klev < 1 || ngpblks < 1 || ngptot < 1 || kidia < 1 || kidia > nproma ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT/KIDIA");
+  const bool any_cld = inc->pa_ql || inc->pa_qi || inc->pa_qr || inc->pa_qs;
+  if (any_cld && st->nclv < 4) return fail(CLOUDSC_E_SHAPE, "NCLV of the state's CLD must be at least 4");
+  if (inc->nclv_pa < 0 || (any_cld && inc->nclv_pa > 0 && inc->nclv_pa < 4))
+    return fail(CLOUDSC_E_SHAPE, "the increments' NCLV must be 0 or at least 4");
+  const unsigned long long s2 = (unsigned long long)nproma * klev;
+  const unsigned long long cs = (unsigned long long)(st->nclv > 0 ? st->nclv : 0) * s2;
+  const unsigned long long ps = inc->nclv_pa > 0 ? (unsigned long long)inc->nclv_pa * s2 : s2;
+  // (state field, its KEYMASK bit or 0 for always, increment, strides), in
+  // the reference's order (state_increment.F90:42-103)
+  struct Pair {
+    double *dst;
+    uint32_t key;
+    const double *src;
+    unsigned long long dbs, sbs;
+  };
+  const Pair pairs[11] = {
+      {st->u, 0, inc->pa_u, s2, s2},
+      {st->v, 0, inc->pa_v, s2, s2},
+      {st->t, 0, inc->pa_t, s2, s2},
+      {st->q, CLOUDSC_KEY_Q, inc->pa_q, s2, s2},
+      {st->o3, CLOUDSC_KEY_O3, inc->pa_o3, s2, s2},
+      {st->a, CLOUDSC_KEY_A, inc->pa_a, s2, s2},
+      {st->tke, CLOUDSC_KEY_TKE, inc->pa_tke, s2, s2},
+      {st->cld ? st->cld + 0 * s2 : nullptr, CLOUDSC_KEY_QL, inc->pa_ql, cs, ps},
+      {st->cld ? st->cld + 1 * s2 : nullptr, CLOUDSC_KEY_QI, inc->pa_qi, cs, ps},
+      {st->cld ? st->cld + 2 * s2 : nullptr, CLOUDSC_KEY_QR, inc->pa_qr, cs, ps},
+      {st->cld ? st->cld + 3 * s2 : nullptr, CLOUDSC_KEY_QS, inc->pa_qs, cs, ps}};
+  IncFields f{};
+  for (const Pair &q : pairs) {
+    if (!q.src) continue;                              // PRESENT(PA_X) false
+    if (q.key && !(st->keymask & q.key)) continue;     // KEYMASK off
+    if (!q.dst) return fail(CLOUDSC_E_NULL, "an increment is given for a field the state does not carry");
+    f.dst[f.n] = q.dst;
+    f.src[f.n] = q.src;
+    f.dst_bs[f.n] = q.dbs;
+    f.src_bs[f.n] = q.sbs;
+    ++f.n;
+  }
+  if (f.n == 0) return CLOUDSC_OK;
+  Shape sh = {nproma, klev, ngpblks, ngptot, kidia - 1, 0.0};
+  cudaError_t e = launch_state_increment(f, sh, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+// CLOUD_SATADJ + STATE_INCREMENT of its tendencies (callpar.F90:1253-1280).
+int cloudsc_b200_satadj_increment_batched(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot, double ptsphy,
+    const double *pap, const double *paph, const double *pt, const double *pq, const double *pa,
+    const double *pl, const double *pi, double *ptendency_cml_t, double *ptendency_cml_q,
+    double *ptendency_cml_a, double *ptendency_cml_l, double *ptendency_cml_i, const double *phrsw,
+    const double *phrlw, const double *ptendency_vdf_t, const double *ptendency_vdf_q, const double *pludeli,
+    const double *pvervel, double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
+    double *ptendency_loc_l, double *ptendency_loc_i, uint32_t keymask, uint32_t *ncounters,
+    void *stream) {
+  int rc = satadj_shape_ok(p, ptsphy);
+  if (rc) return rc;
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  const void *req[] = {pap, paph, pt, pq, pa, pl, pi, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a,
+                       ptendency_cml_l, ptendency_cml_i, phrsw, phrlw, ptendency_vdf_t, ptendency_vdf_q,
+                       pludeli, pvervel, ptendency_loc_t, ptendency_loc_q, ptendency_loc_a,
+                       ptendency_loc_l, ptendency_loc_i};
+  for (const void *q : req)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  rc = ensure_params(nullptr);
+  if (rc) return rc;
+  SatadjFields f = {pap, paph, pt, pq, pa, pl, pi, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a,
+                    ptendency_cml_l, ptendency_cml_i, phrsw, phrlw, ptendency_vdf_t, ptendency_vdf_q,
+                    pludeli, pvervel, ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_l,
+                    ptendency_loc_i, ncounters};
+  f.inc_t = ptendency_cml_t;  // T is incremented whatever the mask
+  f.inc_q = (keymask & CLOUDSC_KEY_Q) ? ptendency_cml_q : nullptr;
+  f.inc_a = (keymask & CLOUDSC_KEY_A) ? ptendency_cml_a : nullptr;
+  f.inc_l = (keymask & CLOUDSC_KEY_QL) ? ptendency_cml_l : nullptr;
+  f.inc_i = (keymask & CLOUDSC_KEY_QI) ? ptendency_cml_i : nullptr;
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
+  cudaError_t e = launch_satadj(f, sh, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
   return CLOUDSC_OK;
 }

@@ -53,6 +53,20 @@ struct SatadjFields {
   const double *phrsw, *phrlw, *vdf_t, *vdf_q, *pludeli, *pvervel;
   double *loc_t, *loc_q, *loc_a, *loc_l, *loc_i;
   uint32_t *ncounters;
+  // the fused STATE_INCREMENT (callpar.F90:1278-1280): where not NULL, the
+  // cumulative tendency written back incremented by SATADJ's (these alias
+  // cml_t .. cml_i; NULL for a field the state's KEYMASK leaves out)
+  double *inc_t, *inc_q, *inc_a, *inc_l, *inc_i;
+};
+
+// STATE_INCREMENT's fields (state_increment.F90): n pairs dst += src, each an
+// (NPROMA, KLEV) slab per block with its own block stride in elements (a
+// species slice of a (NPROMA, KLEV, NCLV) array has stride NCLV*KLEV*NPROMA).
+struct IncFields {
+  double *dst[11];
+  const double *src[11];
+  unsigned long long dst_bs[11], src_bs[11];
+  int n;
 };
 
 // Pointers of the batched arrays of SLTEND's supersaturation adjustment

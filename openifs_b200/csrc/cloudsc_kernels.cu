@@ -105,7 +105,12 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
 // registers (4 CTAs, 32 warps per SM) and up to 64 CTAs per SM in the grid:
 // 2.42 ms at 262,144 columns, against 2.55 ms at 80 registers with 16 CTAs
 // per SM and 2.61 ms at 48 registers.
+// INC: STATE_INCREMENT of the cumulative tendencies fused in
+// (callpar.F90:1278-1280): each point writes CML + LOC back into the CML
+// arrays it has just read (inc_* not NULL), one addition each, as the
+// separate call does.
 constexpr int kSatadjThreads = 256;
+template <bool INC>
 __global__ void __launch_bounds__(kSatadjThreads, 4) satadj_kernel(SatadjFields F, Shape sh) {
   plibm_load_tables();
   const KParams<double> &k = KP<double>();
@@ -129,16 +134,27 @@ __global__ void __launch_bounds__(kSatadjThreads, 4) satadj_kernel(SatadjFields 
       F.loc_a[idx] = 0.0;
       F.loc_l[idx] = 0.0;
       F.loc_i[idx] = 0.0;
+      if constexpr (INC) {  // + 0.0 as STATE_INCREMENT adds it (turns -0 into +0)
+        if (F.inc_t) F.inc_t[idx] = F.inc_t[idx] + 0.0;
+        if (F.inc_q) F.inc_q[idx] = F.inc_q[idx] + 0.0;
+        if (F.inc_a) F.inc_a[idx] = F.inc_a[idx] + 0.0;
+        if (F.inc_l) F.inc_l[idx] = F.inc_l[idx] + 0.0;
+        if (F.inc_i) F.inc_i[idx] = F.inc_i[idx] + 0.0;
+      }
       continue;
     }
     const size_t oh = (size_t)(ib * (kl + 1) + jk) * np + jl;  // PAPH(jl, jk)
     const size_t o4 = (size_t)(ib * 4 * kl + jk) * np + jl;     // PLUDELI(jl, jk, 1)
     const size_t sl = (size_t)kl * np;                          // one PLUDELI component
     double lt, lq, la, ll, li;
+    // the cumulative tendencies are read through the read-only path only
+    // when this kernel does not write them back
+    const double ct = INC ? F.cml_t[idx] : ld(F.cml_t + idx), cq = INC ? F.cml_q[idx] : ld(F.cml_q + idx),
+                 ca = INC ? F.cml_a[idx] : ld(F.cml_a + idx), cl = INC ? F.cml_l[idx] : ld(F.cml_l + idx),
+                 ci = INC ? F.cml_i[idx] : ld(F.cml_i + idx);
     satadj_point(k, dt, zqtmst, ld(F.pap + idx), ld(F.paph + oh), ld(F.paph + oh + np),
                  ld(F.paph + (size_t)(ib * (kl + 1) + kl) * np + jl), ld(F.pt + idx), ld(F.pq + idx),
-                 ld(F.pa + idx), ld(F.pl + idx), ld(F.pi + idx), ld(F.cml_t + idx), ld(F.cml_q + idx),
-                 ld(F.cml_a + idx), ld(F.cml_l + idx), ld(F.cml_i + idx), ld(F.phrsw + idx),
+                 ld(F.pa + idx), ld(F.pl + idx), ld(F.pi + idx), ct, cq, ca, cl, ci, ld(F.phrsw + idx),
                  ld(F.phrlw + idx), ld(F.vdf_t + idx), ld(F.vdf_q + idx), ld(F.pludeli + o4 + 2 * sl),
                  ld(F.pludeli + o4 + 3 * sl), ld(F.pvervel + idx), lt, lq, la, ll, li, nwarn);
     F.loc_t[idx] = lt;
@@ -146,6 +162,13 @@ __global__ void __launch_bounds__(kSatadjThreads, 4) satadj_kernel(SatadjFields 
     F.loc_a[idx] = la;
     F.loc_l[idx] = ll;
     F.loc_i[idx] = li;
+    if constexpr (INC) {
+      if (F.inc_t) F.inc_t[idx] = ct + lt;
+      if (F.inc_q) F.inc_q[idx] = cq + lq;
+      if (F.inc_a) F.inc_a[idx] = ca + la;
+      if (F.inc_l) F.inc_l[idx] = cl + ll;
+      if (F.inc_i) F.inc_i[idx] = ci + li;
+    }
   }
   if (nwarn && F.ncounters) atomic_add(F.ncounters, (uint32_t)nwarn);
 }
@@ -186,6 +209,28 @@ __global__ void __launch_bounds__(kSatadjThreads, 4) sltend_supersat_kernel(Slte
     if (F.padja) F.padja[idx] = aa * zrtsphy;
     if (F.padjl) F.padjl[idx] = la * zrtsphy;
     if (F.padji) F.padji[idx] = ia * zrtsphy;
+  }
+}
+
+// STATE_INCREMENT (state_increment.F90:42-103): one thread per (column,
+// level) point, numbered like satadj_kernel, adds each of the n increments
+// to its state field (coalesced: a warp covers 32 neighbouring columns of
+// one level of every field).
+__global__ void __launch_bounds__(kSatadjThreads) state_increment_kernel(IncFields F, Shape sh) {
+  const unsigned long long np = sh.nproma, kl = sh.klev;
+  const unsigned long long npts = (unsigned long long)sh.ngpblks * kl * np;
+  for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < npts;
+       idx += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long row = idx / np;
+    const int jl = (int)(idx - row * np);
+    const unsigned long long ib = row / kl;
+    const unsigned long long within = idx - ib * kl * np;  // jk * NPROMA + jl
+    const long long icend = (long long)sh.ngptot - (long long)ib * (long long)np;
+    if (jl < sh.kidia0 || jl >= icend) continue;
+    for (int f = 0; f < F.n; ++f) {
+      double *d = F.dst[f] + ib * F.dst_bs[f] + within;
+      *d = *d + ld(F.src[f] + ib * F.src_bs[f] + within);
+    }
   }
 }
 
@@ -283,6 +328,7 @@ cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int t
 
 // Launch CLOUD_SATADJ over every point of the batched arrays: a grid of
 // 256-thread CTAs, at most 64 per SM, striding over the points.
+// With any inc_* pointer set, the form with the fused STATE_INCREMENT runs.
 cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream) {
   const unsigned long long npts = (unsigned long long)sh.ngpblks * sh.klev * sh.nproma;
   int dev = 0, sms = 148;
@@ -292,7 +338,25 @@ cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t s
   const unsigned long long cap = (unsigned long long)sms * 64;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
-  satadj_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
+  if (f.inc_t || f.inc_q || f.inc_a || f.inc_l || f.inc_i)
+    satadj_kernel<true><<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
+  else
+    satadj_kernel<false><<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
+  return cudaGetLastError();
+}
+
+// STATE_INCREMENT over every point: a grid of 256-thread CTAs, at most 16
+// per SM, striding over the points.
+cudaError_t launch_state_increment(const IncFields &f, const Shape &sh, cudaStream_t stream) {
+  const unsigned long long npts = (unsigned long long)sh.ngpblks * sh.klev * sh.nproma;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  unsigned long long blocks = (npts + kSatadjThreads - 1) / kSatadjThreads;
+  const unsigned long long cap = (unsigned long long)sms * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  state_increment_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
   return cudaGetLastError();
 }
 

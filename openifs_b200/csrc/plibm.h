@@ -276,8 +276,10 @@ PLIBM_FN double plibm_cube(double x) {
 }
 
 /* x^1.5 rounded once: s = sqrt(x) (correctly rounded) and x - s^2 = e
- * exactly, so sqrt(x) = s + e/(2s) to 2^-105 relative; x*s = p + pe exactly,
- * and p + (pe + x*(e/(2s))) rounds the product with the exact root once.
+ * exactly, so sqrt(x) = s + e/(2s) to 2^-105 relative, and
+ * x*e/(2s) = (s^2 + e)*e/(2s) = e*s/2 + e^2/(2s), whose last term is below
+ * 2^-104 of the result; x*s = p + pe exactly.  p + (pe + (e*s)*0.5) thus
+ * rounds the product with the exact root once, without a division.
  * x*sqrt(x) rounds twice and differs from the correctly rounded x^1.5 in
  * about a quarter of all arguments.  Outside 1e-290 < x < 1e300 (and for
  * x <= 0 or NaN) the plain product. */
@@ -285,10 +287,9 @@ PLIBM_FN double plibm_pow1p5(double x) {
   double s = plibm_sqrt(x);
   if (!(x > 1e-290 && x < 1e300)) return x * s;
   double e = plibm_fma(-s, s, x);
-  double slo = e / (s + s);
   double p = x * s;
   double pe = plibm_fma(x, s, -p);
-  return p + (pe + x * slo);
+  return p + (pe + (e * s) * 0.5);
 }
 
 /* x^y given plibm_log_base(x) = lhi + llo; pow(x, y) is exactly this, so

@@ -60,3 +60,55 @@ class CloudscParams(ctypes.Structure):
 # Species index order of the (KLON,KLEV,NCLV) arrays (yoecldp.F90:102-107).
 NCLV = 5
 NCLDQL, NCLDQI, NCLDQR, NCLDQS, NCLDQV = 1, 2, 3, 4, 5
+
+
+# STATE_INCREMENT (state_increment.F90): the state's KEYMASK switches as the
+# CLOUDSC_KEY_* bits of include/cloudsc_b200.h, and ctypes mirrors of
+# cloudsc_state / cloudsc_increments.
+KEY_Q, KEY_O3, KEY_A, KEY_TKE, KEY_QL, KEY_QI, KEY_QR, KEY_QS = 0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x40, 0x80
+KEY_ALL = 0xFF
+STATE_FIELDS = ("u", "v", "t", "o3", "q", "a", "cld", "tke")
+INCREMENT_FIELDS = ("u", "v", "t", "o3", "q", "a", "ql", "qi", "qr", "qs", "tke")
+
+
+class CloudscState(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in STATE_FIELDS] + [("keymask", ctypes.c_uint32),
+                                                                ("nclv", ctypes.c_int32)]
+
+
+class CloudscIncrements(ctypes.Structure):
+    _fields_ = [("pa_" + n, ctypes.c_void_p) for n in INCREMENT_FIELDS] + [("nclv_pa", ctypes.c_int32)]
+
+
+def make_state(state, keymask, ptr):
+    """cloudsc_state from a dict of the state's arrays (keys of STATE_FIELDS;
+    CLD shaped (NGPBLKS, NCLV, KLEV, NPROMA)); ``ptr`` gives an array's
+    address."""
+    s = CloudscState()
+    for n in STATE_FIELDS:
+        x = state.get(n)
+        setattr(s, n, None if x is None else ptr(x))
+    s.keymask = int(keymask)
+    cld = state.get("cld")
+    s.nclv = 0 if cld is None else int(cld.shape[1])
+    return s
+
+
+def make_increments(inc, ptr, species_stride):
+    """cloudsc_increments from a dict of increments (keys of
+    INCREMENT_FIELDS), or with key "cld" a (NGPBLKS, N, KLEV, NPROMA) array
+    whose first four species give PA_QL..PA_QS; ``species_stride(x, m)`` is
+    the address of species m of such an array."""
+    c = CloudscIncrements()
+    for n in INCREMENT_FIELDS:
+        x = inc.get(n)
+        setattr(c, "pa_" + n, None if x is None else ptr(x))
+    c.nclv_pa = 0
+    cld = inc.get("cld")
+    if cld is not None:
+        for m, n in enumerate(("ql", "qi", "qr", "qs")):
+            if n in inc:
+                raise ValueError(f"give {n} either alone or through cld, not both")
+            setattr(c, "pa_" + n, species_stride(cld, m))
+        c.nclv_pa = int(cld.shape[1])
+    return c

@@ -1947,3 +1947,71 @@ int oracle_cloudsc_batched_diag(
   }
   return err < 0 ? err : total;
 }
+
+/* STATE_INCREMENT (state_increment.F90:9-105) for one block: each field the
+ * state carries is incremented over columns KIDIA..KFDIA of every level by
+ * its increment when that is present (PA_X != NULL) and, for Q, O3, A, TKE
+ * and the condensate species, when the state's KEYMASK switch is on
+ * (CLOUDSC_KEY_* bits in st->keymask).  CLD is (KLON, KLEV, st->nclv); the
+ * condensate increments are (KLON, KLEV) arrays, or species slices of one
+ * (KLON, KLEV, inc->nclv_pa) array.  Same order of fields as the reference. */
+int oracle_state_increment(int kidia, int kfdia, int klon, int klev, const cloudsc_state *st,
+                           const cloudsc_increments *inc) {
+  const size_t s2 = (size_t)klon * klev;
+#define INC2(DST, SRC)                                   \
+  for (int jk = 0; jk < klev; jk++)                      \
+    for (int jl = kidia - 1; jl < kfdia; jl++) {         \
+      size_t o = (size_t)jk * klon + jl;                 \
+      (DST)[o] = (DST)[o] + (SRC)[o];                    \
+    }
+  const uint32_t km = st->keymask;
+  if (inc->pa_u) { if (!st->u) return CLOUDSC_E_NULL; INC2(st->u, inc->pa_u) }
+  if (inc->pa_v) { if (!st->v) return CLOUDSC_E_NULL; INC2(st->v, inc->pa_v) }
+  if (inc->pa_t) { if (!st->t) return CLOUDSC_E_NULL; INC2(st->t, inc->pa_t) }
+  if (inc->pa_q && (km & CLOUDSC_KEY_Q)) { if (!st->q) return CLOUDSC_E_NULL; INC2(st->q, inc->pa_q) }
+  if (inc->pa_o3 && (km & CLOUDSC_KEY_O3)) { if (!st->o3) return CLOUDSC_E_NULL; INC2(st->o3, inc->pa_o3) }
+  if (inc->pa_a && (km & CLOUDSC_KEY_A)) { if (!st->a) return CLOUDSC_E_NULL; INC2(st->a, inc->pa_a) }
+  if (inc->pa_tke && (km & CLOUDSC_KEY_TKE)) { if (!st->tke) return CLOUDSC_E_NULL; INC2(st->tke, inc->pa_tke) }
+  const double *pcld[4] = {inc->pa_ql, inc->pa_qi, inc->pa_qr, inc->pa_qs};
+  const uint32_t kcld[4] = {CLOUDSC_KEY_QL, CLOUDSC_KEY_QI, CLOUDSC_KEY_QR, CLOUDSC_KEY_QS};
+  for (int m = 0; m < 4; m++) {
+    if (!pcld[m] || !(km & kcld[m])) continue;
+    if (!st->cld) return CLOUDSC_E_NULL;
+    double *dst = st->cld + (size_t)m * s2; /* CLD(:,:,NCLDQL+m) */
+    INC2(dst, pcld[m])
+  }
+#undef INC2
+  return 0;
+}
+
+/* STATE_INCREMENT over NPROMA blocks stored (NPROMA, ..., NGPBLKS); columns
+ * KIDIA..ICEND of each block, ICEND = MIN(NPROMA, NGPTOT - (block-1)*NPROMA). */
+int oracle_state_increment_batched(int nproma, int klev, int ngpblks, int ngptot, int kidia,
+                                   const cloudsc_state *st, const cloudsc_increments *inc) {
+  if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
+      ngptot <= nproma * (ngpblks - 1) || kidia < 1 || kidia > nproma)
+    return CLOUDSC_E_SHAPE;
+  const size_t s2 = (size_t)nproma * klev;
+  const size_t cs = (size_t)(st->nclv > 0 ? st->nclv : 0) * s2;
+  const size_t ps = inc->nclv_pa > 0 ? (size_t)inc->nclv_pa * s2 : s2;
+  int err = 0;
+  for (int ib = 0; ib < ngpblks; ib++) {
+    int icend = ngptot - ib * nproma;
+    if (icend > nproma) icend = nproma;
+    if (kidia > icend) continue;
+    cloudsc_state sb = *st;
+    cloudsc_increments ib_inc = *inc;
+#define OFF(P, STRIDE) ((P) ? (P) + ib * (STRIDE) : NULL)
+    sb.u = OFF(st->u, s2); sb.v = OFF(st->v, s2); sb.t = OFF(st->t, s2); sb.o3 = OFF(st->o3, s2);
+    sb.q = OFF(st->q, s2); sb.a = OFF(st->a, s2); sb.tke = OFF(st->tke, s2); sb.cld = OFF(st->cld, cs);
+    ib_inc.pa_u = OFF(inc->pa_u, s2); ib_inc.pa_v = OFF(inc->pa_v, s2); ib_inc.pa_t = OFF(inc->pa_t, s2);
+    ib_inc.pa_o3 = OFF(inc->pa_o3, s2); ib_inc.pa_q = OFF(inc->pa_q, s2); ib_inc.pa_a = OFF(inc->pa_a, s2);
+    ib_inc.pa_tke = OFF(inc->pa_tke, s2);
+    ib_inc.pa_ql = OFF(inc->pa_ql, ps); ib_inc.pa_qi = OFF(inc->pa_qi, ps);
+    ib_inc.pa_qr = OFF(inc->pa_qr, ps); ib_inc.pa_qs = OFF(inc->pa_qs, ps);
+#undef OFF
+    int r = oracle_state_increment(kidia, icend, nproma, klev, &sb, &ib_inc);
+    if (r < 0) err = r;
+  }
+  return err;
+}

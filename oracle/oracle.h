@@ -124,6 +124,15 @@ int oracle_sltend_supersat_batched(
     const double *pcenq, const double *pcena, double *ptent, double *ptenq, double *ptena, double *ptencld,
     double *padja, double *padjl, double *padji, int nthreads);
 
+/* STATE_INCREMENT (state_increment.F90:9-105), one block (columns
+ * KIDIA..KFDIA of (KLON, KLEV) fields) and batched over (NPROMA, ...,
+ * NGPBLKS) blocks; the cloudsc_state / cloudsc_increments conventions of
+ * cloudsc_b200_state_increment_batched. */
+int oracle_state_increment(int kidia, int kfdia, int klon, int klev, const cloudsc_state *st,
+                           const cloudsc_increments *inc);
+int oracle_state_increment_batched(int nproma, int klev, int ngpblks, int ngptot, int kidia,
+                                   const cloudsc_state *st, const cloudsc_increments *inc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -143,3 +143,28 @@ def cloudsc_batched_diag(params, arrays, diag, nproma, klev, ngpblks, ngptot, pt
     if rc < 0:
         raise RuntimeError(f"oracle_cloudsc_batched_diag returned {rc}")
     return rc
+
+
+def state_increment_batched(state, increments, nproma, klev, ngpblks, ngptot, kidia=1, keymask=None):
+    """STATE_INCREMENT over every block of numpy arrays, in place; the
+    conventions of openifs_b200.cloudsc.state_increment_batched."""
+    from openifs_b200.params import KEY_ALL, make_increments, make_state
+
+    def ptr(x):
+        if not (isinstance(x, np.ndarray) and x.flags["C_CONTIGUOUS"] and x.dtype == np.float64):
+            raise ValueError("need C-contiguous float64 numpy arrays")
+        return x.ctypes.data
+
+    def species(x, m):
+        return ptr(x) + m * x.shape[2] * x.shape[3] * 8
+
+    st = make_state(state, KEY_ALL if keymask is None else keymask, ptr)
+    inc = make_increments(increments, ptr, species)
+    L = lib()
+    f = L.oracle_state_increment_batched
+    f.argtypes = [ctypes.c_int] * 5 + [ctypes.c_void_p] * 2
+    f.restype = ctypes.c_int
+    rc = f(int(nproma), int(klev), int(ngpblks), int(ngptot), int(kidia), ctypes.byref(st), ctypes.byref(inc))
+    if rc < 0:
+        raise RuntimeError(f"oracle_state_increment_batched returned {rc}")
+    return rc
