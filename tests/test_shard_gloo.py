@@ -3,9 +3,11 @@
 CLOUDSC columns are independent (the recurrence is only vertical), so the
 multi-GPU form shards NPROMA blocks across ranks with no data-path
 collective; only scalars (timings, warning counts) are reduced.  Here two
-gloo ranks each run the oracle on their contiguous block range
-[g*N/G, (g+1)*N/G) and the gathered result must equal the single-process
-run bit for bit; the MAX reduction of step times and the SUM of warning
+gloo ranks each run the product's own column code -- the kernels'
+cloudsc_body.cuh built for the host (tests/hostemu), the code each GPU rank
+runs -- on their contiguous block range [g*N/G, (g+1)*N/G) of a ragged
+workload, and the gathered result must equal the single-process run and the
+oracle bit for bit; the MAX reduction of step times and the SUM of warning
 counts follow the bench's rules.
 """
 import os
@@ -20,7 +22,7 @@ import torch.multiprocessing as mp
 from openifs_b200 import fields, inputs, shard
 from tests import util
 
-NB, NPROMA = 6, 16
+NB, NPROMA, CUT = 7, 16, 5  # the last block holds NPROMA - CUT columns
 
 
 def _free_port():
@@ -39,9 +41,10 @@ def _worker(rank, world, port, outdir):
         p, po = util.params()
         b0, b1 = shard.block_range(NB, rank, world)
         arrs = inputs.generate(NB, NPROMA, p, seed=8, blocks=range(b0, b1))
-        ngptot = (b1 - b0) * NPROMA
-        ref, nw = util.run_oracle(po, arrs, NPROMA, b1 - b0, ngptot, libm="glibc")
-        np.savez(os.path.join(outdir, f"rank{rank}.npz"), **{n: ref[n] for n in fields.OUTPUT_NAMES})
+        # this rank's share of NGPTOT: the ragged last block is the last rank's
+        ngptot = (b1 - b0) * NPROMA - (CUT if b1 == NB else 0)
+        out, nw = util.run_hostemu(p, arrs, NPROMA, b1 - b0, ngptot)
+        np.savez(os.path.join(outdir, f"rank{rank}.npz"), **{n: out[n] for n in fields.OUTPUT_NAMES})
         t = torch.tensor([float(rank + 1)])
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         w = torch.tensor([nw])
@@ -65,10 +68,16 @@ def test_two_rank_gloo_shards_match_single_process(tmp_path, built):
                        start_method="spawn")
     p, po = util.params()
     arrs = inputs.generate(NB, NPROMA, p, seed=8)
-    ref, _ = util.run_oracle(po, arrs, NPROMA, NB, NB * NPROMA, libm="glibc")
+    ngptot = NB * NPROMA - CUT
+    single, nw1 = util.run_hostemu(p, arrs, NPROMA, NB, ngptot)
+    ref, nw_ref = util.run_oracle(po, arrs, NPROMA, NB, ngptot, libm="plibm")
     parts = [np.load(tmp_path / f"rank{r}.npz") for r in range(2)]
     for n in fields.OUTPUT_NAMES:
         got = np.concatenate([parts[0][n], parts[1][n]], axis=0)
-        assert np.array_equal(got, ref[n]), n
+        assert np.array_equal(util.defined(n, got), util.defined(n, single[n])), n
+        a = util.defined(n, util._valid_cols(got, ngptot, NPROMA))
+        b = util.defined(n, util._valid_cols(ref[n], ngptot, NPROMA))
+        assert np.array_equal(a, b), n
     red = np.load(tmp_path / "red0.npy")
     assert red[0] == 2.0
+    assert red[1] == nw1 == nw_ref
