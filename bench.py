@@ -412,6 +412,78 @@ def spp_form(a, p, d, plude0, dev, world, stream, ms64):
     return out
 
 
+def single_precision_form(a, p, host, ref, dev, world, stream, ms64):
+    """The single-precision interface (JPRB = REAL(4): every real array
+    float) on the same 262,144 columns, rounded to float: device time of the
+    three arithmetic forms, their per-field error against the FP64 kernel on
+    the double inputs, and end to end through cloudsc_b200_batched_host_sp
+    (page-locked float arrays, copies in the timed region)."""
+    import torch
+    from openifs_b200 import cloudsc, fields
+    sp = fields.to_single(host)
+    d = {k: torch.from_numpy(v).to(dev) for k, v in sp.items()}
+    plude0 = d["plude"].clone()
+    out = {}
+    for prec, name in ((cloudsc.FP64, "fp64"), (cloudsc.MIXED, "mixed"), (cloudsc.PHYS32, "phys32")):
+        ev = []
+        for i in range(a.warmup + a.steps):
+            d["plude"].copy_(plude0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            cloudsc.cloudsc_batched_sp(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=prec, stream=stream)
+            e1.record(stream)
+            if i >= a.warmup:
+                ev.append((e0, e1))
+        torch.cuda.synchronize(dev)
+        ms = statistics.mean(x.elapsed_time(y) for x, y in ev)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        err = {}
+        for n, sl in [("tendency_loc_t", None), ("tendency_loc_q", None), ("tendency_loc_cld", 0),
+                      ("tendency_loc_cld", 1), ("tendency_loc_cld", 2), ("tendency_loc_cld", 3),
+                      ("pfplsl", -1), ("pfplsn", -1)]:
+            r, g = ref[n], d[n].double()
+            label = n
+            if n == "tendency_loc_cld":
+                r, g = r[:, sl], g[:, sl]
+                label = f"{n}_{'lirs'[sl]}"
+            elif sl is not None:
+                r, g = r[:, sl], g[:, sl]
+            diff = (g - r).abs()
+            err[label] = {"max_abs_over_max": float(diff.max() / r.abs().max().clamp_min(1e-300)),
+                          "rms_over_rms": float(diff.pow(2).mean().sqrt() / r.pow(2).mean().sqrt().clamp_min(1e-300))}
+        out[name] = {"ms": ms, "columns_per_s": world * NCOL / (ms * 1e-3), "speedup_vs_fp64_interface": ms64 / ms,
+                     "error_vs_fp64_on_double_inputs": err}
+    del d
+    torch.cuda.empty_cache()
+    e2e = None
+    if not a.no_e2e:
+        pin = {k: torch.from_numpy(v).pin_memory() for k, v in sp.items()}
+        plude_h = pin["plude"].clone()
+        h2d, d2h = fields.host_copy_bytes_sp(NPROMA, KLEV, NGPBLKS, NCOL)
+        tt = []
+        for i in range(max(1, a.warmup) + a.steps):
+            pin["plude"].copy_(plude_h)
+            t = time.perf_counter()
+            cloudsc.cloudsc_batched_host_sp(p, pin, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY)
+            if i >= max(1, a.warmup):
+                tt.append(time.perf_counter() - t)
+        e2e_s = statistics.mean(tt)
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": world * NCOL / e2e_s, "unit": "columns/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": 1e3 * e2e_s,
+               "api": "cloudsc_b200_batched_host_sp (FP64 arithmetic), page-locked float host arrays"}
+        del pin
+    out["e2e"] = e2e
+    out["interface"] = "float arrays (JPRB = REAL(4)); precision 0 = FP64 arithmetic on the widened inputs"
+    return out
+
+
 def state_increment_form(a, d, dev, world, stream):
     """STATE_INCREMENT after CLOUDSC (callpar.F90:1308-1311): the cumulative
     T, q and cloud-fraction tendencies and the four condensate species of
@@ -797,11 +869,12 @@ def run_ours(a):
     sat = satadj_form(a, p, host, dev, world, rank, stream)
     slt = sltend_form(a, p, host, dev, world, rank, stream)
 
+    d["plude"].copy_(plude0)
+    cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.FP64)
+    ref = {n: d[n].clone() for n in outs}
+    spi = single_precision_form(a, p, host, ref, dev, world, stream, results["fp64"]["ms"])
     sur = None
     if not a.no_surrogate:
-        d["plude"].copy_(plude0)
-        cloudsc.cloudsc_batched(p, d, NPROMA, KLEV, NGPBLKS, NCOL, PTSPHY, precision=cloudsc.FP64)
-        ref = {n: d[n].clone() for n in outs}
         sur = surrogate_form(a, p, d, plude0, ref, dev, world, rank, results["fp64"]["ms"])
     del ref
 
@@ -898,6 +971,7 @@ def run_ours(a):
                                      "solve, saturation adjustment and budgets FP64",
                        "error_vs_fp64": errs["phys32"]},
             "surrogate": sur,
+            "single_precision_interface": spi,
         },
         "budget_diagnostics": bud,
         "spp_inhomogeneity": spp,
@@ -919,6 +993,12 @@ def run_ours(a):
     for name in ("mixed", "phys32"):
         e = errs[name]
         print(f"# {name} vs fp64 (max|err|/max|ref| rms/rms): " +
+              " ".join(f"{short[k]} {v['max_abs_over_max']:.1e}/{v['rms_over_rms']:.1e}" for k, v in e.items()),
+              flush=True)
+    for name in ("fp64", "mixed", "phys32"):
+        e = spi[name]["error_vs_fp64_on_double_inputs"]
+        print(f"# float interface, {name} arithmetic, {spi[name]['ms']:.2f} ms, vs fp64 on double inputs "
+              "(max|err|/max|ref| rms/rms): " +
               " ".join(f"{short[k]} {v['max_abs_over_max']:.1e}/{v['rms_over_rms']:.1e}" for k, v in e.items()),
               flush=True)
     if parity:

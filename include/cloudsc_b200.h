@@ -251,6 +251,56 @@ int cloudsc_b200_batched_host(
     int32_t precision, int32_t chunk_blocks);
 
 /*
+ * The single-precision interface: the OpenIFS single-precision build
+ * (JPRB = REAL(4); contrib/fiat/src/parkind/parkind1.F90:41-44, bundle.yml's
+ * single-precision option) passes every REAL array of CLOUDSC's argument
+ * list as float.  These two entries take the arrays of cloudsc_b200_batched /
+ * cloudsc_b200_batched_host in float (LDCUM and KTYPE stay int32, the
+ * parameters stay the double cloudsc_params, filled from the build's float
+ * constants) and run the same kernels: each float input is widened to double
+ * when it is read and each output rounded to float when it is written, so
+ * `precision` 0 gives exactly the FP64 kernel's results on the widened
+ * inputs, rounded to float; 1 and 2 select the FP32-mixed and FP32-physics
+ * arithmetic.  Half the bytes of the double interface cross HBM and PCIe.
+ * No reference counterpart beyond CLOUDSC itself in that build.
+ */
+int cloudsc_b200_batched_sp(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks,
+    int32_t ngptot, float ptsphy, const float *pt, const float *pq,
+    const float *ptendency_cml_t, const float *ptendency_cml_q,
+    const float *ptendency_cml_a, const float *ptendency_cml_cld,
+    float *ptendency_loc_t, float *ptendency_loc_q, float *ptendency_loc_a,
+    float *ptendency_loc_cld, const float *pvfl, const float *pvfi,
+    const float *pap, const float *paph, const float *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const float *peis,
+    const float *plu, float *plude, const float *pludeli, const float *psnde,
+    const float *pmfu, const float *pmfd, const float *pa, const float *pclv,
+    float *pcovptot, float *prainfrac_toprfz, float *pfsqlf, float *pfsqif,
+    float *pfcqnng, float *pfcqlng, float *pfsqrf, float *pfsqsf,
+    float *pfcqrng, float *pfcqsng, float *pfsqltur, float *pfsqitur,
+    float *pfplsl, float *pfplsn, float *pfhpsl, float *pfhpsn,
+    uint32_t *ncounters, int32_t precision, void *stream);
+
+/* The single-precision interface with host pointers, pipelined like
+ * cloudsc_b200_batched_host. */
+int cloudsc_b200_batched_host_sp(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks,
+    int32_t ngptot, float ptsphy, const float *pt, const float *pq,
+    const float *ptendency_cml_t, const float *ptendency_cml_q,
+    const float *ptendency_cml_a, const float *ptendency_cml_cld,
+    float *ptendency_loc_t, float *ptendency_loc_q, float *ptendency_loc_a,
+    float *ptendency_loc_cld, const float *pvfl, const float *pvfi,
+    const float *pap, const float *paph, const float *plsm,
+    const int32_t *ldcum, const int32_t *ktype, const float *peis,
+    const float *plu, float *plude, const float *pludeli, const float *psnde,
+    const float *pmfu, const float *pmfd, const float *pa, const float *pclv,
+    float *pcovptot, float *prainfrac_toprfz, float *pfsqlf, float *pfsqif,
+    float *pfcqnng, float *pfcqlng, float *pfsqrf, float *pfsqsf,
+    float *pfcqrng, float *pfcqsng, float *pfsqltur, float *pfsqitur,
+    float *pfplsl, float *pfplsn, float *pfhpsl, float *pfhpsn,
+    int32_t precision, int32_t chunk_blocks);
+
+/*
  * Per-block call that allocates no device memory.  No reference counterpart:
  * the reference has no device memory at all.  This entry is for callers that
  * cannot call cudaMalloc: a model run whose GPU memory is fully reserved up

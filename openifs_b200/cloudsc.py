@@ -94,6 +94,10 @@ def lib():
                                          [vp] * len(BLOCK_ARRAYS_1) + [i32] +
                                          [vp] * len(BLOCK_ARRAYS_2) + [i32])
         L.cloudsc_b200_block.restype = ctypes.c_int
+        L.cloudsc_b200_batched_sp.argtypes = [P, i32, i32, i32, i32, ctypes.c_float] + [vp] * nf + [vp, i32, vp]
+        L.cloudsc_b200_batched_sp.restype = ctypes.c_int
+        L.cloudsc_b200_batched_host_sp.argtypes = [P, i32, i32, i32, i32, ctypes.c_float] + [vp] * nf + [i32, i32]
+        L.cloudsc_b200_batched_host_sp.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -208,6 +212,58 @@ def cloudsc_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, preci
     return _check(lib().cloudsc_b200_batched(
         ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
         *args, _ptr(counter), int(precision), s))
+
+
+def _check_sp(arrays, nproma, klev, ngpblks, device):
+    """The single-precision interface's arrays: present, float32 (int32 for
+    LDCUM and KTYPE), large enough, on the device or the host."""
+    from .fields import DTYPE_SP, batched_shape
+    for n, *_ in BATCHED_FIELDS:
+        x = arrays.get(n)
+        if x is None:
+            raise CloudscError(-1, f"{n}: array missing")
+        want = int(np.prod(batched_shape(n, ngpblks, nproma, klev)))
+        dt = np.dtype(DTYPE_SP[n])
+        if isinstance(x, np.ndarray):
+            if device:
+                raise CloudscError(-2, f"{n}: a device tensor is needed, not a numpy array")
+            ok, size = x.dtype == dt, x.size
+        else:
+            if x.is_cuda != device:
+                raise CloudscError(-2, f"{n}: tensor must be on {'the GPU' if device else 'the host'}")
+            ok = x.element_size() == dt.itemsize and x.is_floating_point() == (dt.kind == "f")
+            size = x.numel()
+        if not ok:
+            raise CloudscError(-2, f"{n}: dtype must be {dt.name}")
+        if size < want:
+            raise CloudscError(-2, f"{n}: {size} elements, the shape needs {want}")
+
+
+def cloudsc_batched_sp(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64, stream=None,
+                       counter=None):
+    """The single-precision interface (float arrays, fields.DTYPE_SP) on
+    the device: one launch over every block, asynchronous on ``stream``;
+    ``precision`` selects the arithmetic (FP64, MIXED, PHYS32)."""
+    _check_sp(arrays, nproma, klev, ngpblks, device=True)
+    args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
+    s = None
+    if stream is not None:
+        s = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+    return _check(lib().cloudsc_b200_batched_sp(
+        ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
+        *args, _ptr(counter), int(precision), s))
+
+
+def cloudsc_batched_host_sp(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64,
+                            chunk_blocks=0):
+    """The single-precision interface from host arrays (numpy float32, or
+    pinned torch CPU tensors), pipelined like cloudsc_batched_host.
+    Synchronous."""
+    _check_sp(arrays, nproma, klev, ngpblks, device=False)
+    args = [_ptr(arrays[n]) for n, *_ in BATCHED_FIELDS]
+    return _check(lib().cloudsc_b200_batched_host_sp(
+        ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
+        *args, int(precision), int(chunk_blocks)))
 
 
 def cloudsc_batched_host(params, arrays, nproma, klev, ngpblks, ngptot, ptsphy, precision=FP64,

@@ -310,8 +310,15 @@ CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double
 // paths (LCLOUD_INHOMOG, LRAD_CLOUD_INHOMOG -> PFSD), FP64 only
 // (cloudsc.F90:850-939, 1937-2110, 2282-2348, 2781-2783, 3288-3290,
 // 3819-3823, 4112-4125, 4307-4359).  Without OPT none of this code exists.
-template <typename Real, bool F32M, bool BUD = false, bool OPT = false>
-CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bool active = true) {
+// FT: the pointer set, Fields (double arrays) or FieldsSP (float arrays of the
+// single-precision interface: every load is widened to double and every store
+// rounded to float, the arithmetic is the same).
+// GEN: every pow whose exponent is a parameter (mpowp, mpowbp) skips the
+// tests for the exponents 0.5, 1.5, 2 and 3, which the host has ruled out
+// for the uploaded parameters (gen_exponents_ok); same results, fewer
+// branches.
+template <typename Real, bool F32M, bool BUD = false, bool OPT = false, typename FT = Fields, bool GEN = false>
+CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool active = true) {
   const KParams<Real> &P = KP<Real>();
   const KParamsD &PD = c_kd;
   typedef double D;
@@ -690,8 +697,8 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         Real ztemp = C(0.5) * (qr + qxnm1_r);
         if (ztemp != C(0.0)) {
           Real zfallcorr = mpowb<F32M>(b_dens, C(0.4));
-          Real zrlambda = mpow<F32M>(zrho * ztemp / P.rcl_lam1r, P.rcl_lam2r);
-          fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpow<F32M>(zrlambda, P.rcl_dr);
+          Real zrlambda = mpowp<F32M, GEN>(zrho * ztemp / P.rcl_lam1r, P.rcl_lam2r);
+          fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpowp<F32M, GEN>(zrlambda, P.rcl_dr);
         }
       }
       if (k > ncldtop0) {
@@ -771,12 +778,12 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
             zeacc = zeacc * Real(sppf[8]);
           }
         }
-        Real zrainaut = zeaut * rdt * P.rcl_kkaau * mpowb<F32M>(b_liq, P.kkbauq_m1) * zconstpow;
+        Real zrainaut = zeaut * rdt * P.rcl_kkaau * mpowbp<F32M, GEN>(b_liq, P.kkbauq_m1) * zconstpow;
         qb_rl = qb_rl + zrainaut;
         Real zrainacc = C(0.0);
         if (zraincld > zepsec) {
-          zrainacc = zeacc * rdt * P.rcl_kkaac * mpowb<F32M>(b_liq, P.kkbac_m1) *
-                     mpow<F32M>(zraincld, P.rcl_kkbac);
+          zrainacc = zeacc * rdt * P.rcl_kkaac * mpowbp<F32M, GEN>(b_liq, P.kkbac_m1) *
+                     mpowp<F32M, GEN>(zraincld, P.rcl_kkbac);
         }
         qb_rl = qb_rl + zrainacc;
         if constexpr (BUD) {
@@ -805,18 +812,18 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         Real zqe = mx(C(0.0), mn(qv, zqsliq));
         if (zcovpclr > zepsec && zraincldm1 > zepsec && zqe < zzrh * zqsliq) {
           Real zpreclr = zraincldm1;
-          Real zfallcorr = mpowb<F32M>(b_dens, P.flt_0p4);
+          Real zfallcorr = mpowbp<F32M, GEN>(b_dens, P.flt_0p4);
           Real zesatliq = P.rv / P.rd * (P.r2es * el_e);
-          Real zlambda = mpow<F32M>(P.rcl_lam1r / (zrho * zpreclr), P.rcl_lam2r);
+          Real zlambda = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * zpreclr), P.rcl_lam2r);
           const PowBase b_lam = mbase<F32M>(zlambda);
           Real zevap_denom = P.rcl_cdenom1 * zesatliq - P.rcl_cdenom2 * t * zesatliq +
                              P.rcl_cdenom3 * mpow<F32M>(t, C(3.0)) * pap_k;
           Real zcorr2 = mpow<F32M>(t / C(273.), C(1.5)) * C(393.) / (t + C(120.));
           Real zsubsat = mx(zzrh * zqsliq - zqe, C(0.0));
           Real zbeta = (C(0.15) / zqsliq) * (t * t) * zesatliq * P.rcl_const1r * (zcorr2 / zevap_denom) *
-                       (C(0.78) / (mpowb<F32M>(b_lam, P.rcl_const4r)) +
+                       (C(0.78) / (mpowbp<F32M, GEN>(b_lam, P.rcl_const4r)) +
                         P.rcl_const2r * mpow<F32M>(zrho * zfallcorr, C(0.5)) /
-                            (mpow<F32M>(zcorr2, C(0.5)) * mpowb<F32M>(b_lam, P.rcl_const3r)));
+                            (mpow<F32M>(zcorr2, C(0.5)) * mpowbp<F32M, GEN>(b_lam, P.rcl_const3r)));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
           Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
           if (spp && P.spp_on[CLOUDSC_SPP_RAINEVAP]) zdpevap = zdpevap * Real(sppf[CLOUDSC_SPP_RAINEVAP]);
@@ -870,9 +877,9 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
           const PowBase b_pr02 = mbase<F32M>(zpr02);
           Real zterm1 = zsupersatice * (t * t) * zvpice * zcorrfac2 * P.rcl_const2s / (zrho * zaplusb);
-          Real zterm2 = C(0.65) * P.rcl_const6s * mpowb<F32M>(b_pr02, P.rcl_const4s) +
+          Real zterm2 = C(0.65) * P.rcl_const6s * mpowbp<F32M, GEN>(b_pr02, P.rcl_const4s) +
                         P.rcl_const3s * mpow<F32M>(zcorrfac, C(0.5)) * mpow<F32M>(zrho, C(0.5)) *
-                            mpowb<F32M>(b_pr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
+                            mpowbp<F32M, GEN>(b_pr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
           Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
           zpsdep = mn(zpsdep, qv - zqsmix) / zcorqsmix;
           QADD(SV, zpsdep);  // (S,V) += zpsdep, (V,S) -= zpsdep
@@ -936,9 +943,9 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
         if (t < P.rtt) {
           Real zfrzmax;
           if (llrainliq) {
-            Real zlambda = mpow<F32M>(P.rcl_lam1r / (zrho * qr), P.rcl_lam2r);
+            Real zlambda = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * qr), P.rcl_lam2r);
             Real ztemp = mn(P.rcl_fzrab * (t - P.rtt), C(50.));
-            Real zfrz = rdt * (P.rcl_const5r / zrho) * (mexp<F32M>(ztemp) - C(1.)) * mpow<F32M>(zlambda, P.rcl_const6r);
+            Real zfrz = rdt * (P.rcl_const5r / zrho) * (mexp<F32M>(ztemp) - C(1.)) * mpowp<F32M, GEN>(zlambda, P.rcl_const6r);
             zfrzmax = mx(zfrz, C(0.0));
           } else {
             Real zcons1 = xabs(rdt * (C(1.0) + C(0.5) * (P.rtt - t)) / P.rtaumel);
@@ -964,9 +971,9 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
 
       // 4.9 riming (:2973-3017)
       if (t <= P.rtt && zliqcld > zepsec && zsnowcld > zepsec && zcovptot > C(0.01)) {
-        Real zfallcorr = mpowb<F32M>(b_dens, P.flt_0p4);
+        Real zfallcorr = mpowbp<F32M, GEN>(b_dens, P.flt_0p4);
         Real zsnowrime = P.rcl_effrime * zcovptot * rdt * P.rcl_const7s * zfallcorr *
-                         mpow<F32M>(zrho * zsnowcld * P.rcl_const1s, P.rcl_const8s);
+                         mpowp<F32M, GEN>(zrho * zsnowcld * P.rcl_const1s, P.rcl_const8s);
         zsnowrime = mn(zsnowrime, C(1.0));
         qb_sl = qb_sl + zsnowrime;
         if constexpr (BUD) b_snowrime = zsnowrime;
@@ -974,11 +981,11 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
 
       // PSD slopes (:3026-3069), PSACR (:3084-3115), PIACR (:3171-3198)
       if (t <= P.rtt && prainfrac < zepsec && zraincld > zepsec) {
-        Real zlamr = mpow<F32M>(P.rcl_lam1r / (zrho * zraincld), P.rcl_lam2r);
-        Real zn0r = P.rcl_x1r * mpow<F32M>(zlamr, P.rcl_x2r);
+        Real zlamr = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * zraincld), P.rcl_lam2r);
+        Real zn0r = P.rcl_x1r * mpowp<F32M, GEN>(zlamr, P.rcl_x2r);
         Real zlamr3 = zlamr * zlamr * zlamr;
         if (zsnowcld > zepsec) {
-          Real zlams = mpow<F32M>(P.rcl_lam1s / (zrho * zsnowcld), P.rcl_lam2s);
+          Real zlams = mpowp<F32M, GEN>(P.rcl_lam1s / (zrho * zsnowcld), P.rcl_lam2s);
           Real zn0s = P.rcl_x1s;
           Real zfalldiff = mx(xabs(fs_r - fs_s), (fs_r + fs_s) / C(8.));
           Real zfac = P.rpi * P.rpi * P.rdenswat * zrho * zn0r * zn0s / (zlams * zlamr3);
@@ -989,7 +996,7 @@ CSC_DEV void cloudsc_column(const Fields &F, const Shape &sh, int ib, int jl, bo
           if constexpr (BUD) b_psacr = zpsacr;
         }
         if (zicecld > zepsec) {
-          Real zlami = mpow<F32M>(P.rcl_lam1s / (zrho * zicecld), P.rcl_lam2s);
+          Real zlami = mpowp<F32M, GEN>(P.rcl_lam1s / (zrho * zicecld), P.rcl_lam2s);
           Real zn0i = P.rcl_x1s;
           Real zfalldiff = mx(xabs(fs_r - fs_i), (fs_r + fs_i) / C(8.));
           Real zfac = P.rpi * P.rpi * P.rdenswat * C(0.1) * zrho * zn0r * zn0i / (zlami * zlamr3);

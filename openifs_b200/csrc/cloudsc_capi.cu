@@ -29,10 +29,13 @@ int default_variant();
 void variant_bounds(int v, int *maxt, int *minb);
 cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes);
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
-                   cudaStream_t stream);
+                   cudaStream_t stream, bool gen);
+bool params_allow_gen(const cloudsc_params &p, const Derived &d);
 cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream);
 cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaStream_t stream);
 cudaError_t launch_state_increment(const IncFields &f, const Shape &sh, cudaStream_t stream);
+cudaError_t launch_sp(int precision, int v, const FieldsSP &f, const Shape &sh, int threads, int grid,
+                      cudaStream_t stream, bool gen);
 }  // namespace cloudsc
 
 using namespace cloudsc;
@@ -44,7 +47,8 @@ thread_local std::string t_last_error;
 std::mutex g_mu;
 cloudsc_params g_params;
 bool g_have_params = false;
-unsigned long long g_gen = 0;
+bool g_gen = true;  // the uploaded parameters allow the GEN kernels
+unsigned long long g_gen_count = 0;  // parameter uploads so far
 constexpr int kMaxDev = 64;
 unsigned long long g_dev_gen[kMaxDev] = {0};
 // Launch schedule per precision (0 FP64, 1 FP32-mixed, 2 FP32 physics): compiled variant,
@@ -153,14 +157,14 @@ int ensure_params(int *dev_out) {
   if (dev_out) *dev_out = dev;
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_have_params) return fail(CLOUDSC_E_PARAMS, "cloudsc_b200_setup has not been called");
-  if (g_dev_gen[dev] != g_gen) {
+  if (g_dev_gen[dev] != g_gen_count) {
     e = upload_params(g_params, make_derived(g_params));
     if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "parameter upload", e);
     // load this file's module (the no-allocation entry's fixed array) now
     void *scratch = nullptr;
     e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
     if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaGetSymbolAddress(no-allocation array)", e);
-    g_dev_gen[dev] = g_gen;
+    g_dev_gen[dev] = g_gen_count;
   }
   return CLOUDSC_OK;
 }
@@ -391,11 +395,13 @@ int cloudsc_b200_setup(const cloudsc_params *p) {
     return fail(CLOUDSC_E_UNSUPPORTED,
                 "an aerosol switch (LAERICEAUTO, LAERICESED, LAERLIQAUTOLSP, LAERLIQCOLL) is on; this build does not implement them");
   if (p->ncldtop < 2) return fail(CLOUDSC_E_SHAPE, "ncldtop must be >= 2");
+  const bool gen = params_allow_gen(*p, make_derived(*p));
   {
     std::lock_guard<std::mutex> lk(g_mu);
     g_params = *p;
     g_have_params = true;
-    ++g_gen;
+    g_gen = gen;
+    ++g_gen_count;
   }
   return ensure_params(nullptr);
 }
@@ -475,10 +481,11 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
   // from the same parameters whose arrays are checked here, even if another
   // thread calls cloudsc_b200_setup meanwhile.
   Schedule sc;
-  bool bud = false, opt = false, need_gaw = false, need_spp = false, need_fsd = false;
+  bool bud = false, opt = false, need_gaw = false, need_spp = false, need_fsd = false, gen = true;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     sc = g_sched[precision];
+    gen = g_gen;
     if (g_have_params) {
       bud = budgets_on(g_params);
       opt = opt_on(g_params);
@@ -500,9 +507,12 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
                                          "cloudsc_b200_batched_diag or cloudsc_b200_block");
     form = bud && opt ? 5 : (opt ? 4 : 3);
   }
-  const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + sc.threads - 1) / sc.threads);
+  // parameters that rule out the GEN kernels: forms 0-2 run the (512, 1)
+  // kernel without GEN, at most 512 columns per CTA
+  const int threads = (!gen && form <= 2 && sc.threads > 512) ? 512 : sc.threads;
+  const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
-  cudaError_t e = launch(form, sc.variant, f, sh, sc.threads, grid, stream);
+  cudaError_t e = launch(form, sc.variant, f, sh, threads, grid, stream, gen);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
   return CLOUDSC_OK;
 }
@@ -668,12 +678,14 @@ size_t in_rows(int i, size_t klev) {
   if (i == kPludeli) return 2 * klev;
   return rows(kArrs[i].kind, klev);
 }
-size_t elem_size(int i) { return (i == 15 || i == 16) ? 4 : 8; }
+// Bytes of an element of array i: the integer arrays (LDCUM, KTYPE) 4, the
+// real ones fb (8 in the double-precision interface, 4 in the single one).
+size_t elem_size(int i, size_t fb = 8) { return (i == 15 || i == 16) ? 4 : fb; }
 // Host-to-device copy of blocks b0 .. b0+nb-1 of input array i (the rows the
 // kernels read) into a device slab of nb blocks.
 cudaError_t copy_in(void *dst, const void *host, int i, size_t np, size_t kl, size_t b0, size_t nb,
-                    cudaStream_t s) {
-  const size_t esz = elem_size(i);
+                    cudaStream_t s, size_t fb = 8) {
+  const size_t esz = elem_size(i, fb);
   const size_t per = elems(kArrs[i].kind, np, kl) * esz;  // one block's slab
   const size_t used = in_rows(i, kl) * np * esz;
   const char *src = (const char *)host + b0 * per;
@@ -756,10 +768,10 @@ thread_local Workspace t_ws;
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Carve the device arrays of `nblk` blocks out of `base`; returns bytes used.
-size_t carve(char *base, size_t np, size_t klev, size_t nblk, void *dptr[42]) {
+size_t carve(char *base, size_t np, size_t klev, size_t nblk, void *dptr[42], size_t fb = 8) {
   size_t off = 0;
   for (int i = 0; i < 42; ++i) {
-    size_t esz = (kArrs[i].kind == K1 && (i == 15 || i == 16)) ? 4 : 8;
+    size_t esz = elem_size(i, fb);
     size_t n = elems(kArrs[i].kind, np, klev) * nblk * esz;
     if (dptr) dptr[i] = base ? base + off : nullptr;
     off += align256(n);
@@ -785,6 +797,132 @@ Fields fields_from(void *d[42], uint32_t *counter) {
   f.pfhpsl = (double *)d[40]; f.pfhpsn = (double *)d[41];
   f.ncounters = counter;
   return f;
+}
+
+FieldsSP fields_sp_from(void *d[42], uint32_t *counter) {
+  FieldsSP f{};
+  f.pt = (const float *)d[0]; f.pq = (const float *)d[1]; f.cml_t = (const float *)d[2];
+  f.cml_q = (const float *)d[3]; f.cml_a = (const float *)d[4]; f.cml_cld = (const float *)d[5];
+  f.loc_t = (float *)d[6]; f.loc_q = (float *)d[7]; f.loc_a = (float *)d[8]; f.loc_cld = (float *)d[9];
+  f.pvfl = (const float *)d[10]; f.pvfi = (const float *)d[11]; f.pap = (const float *)d[12];
+  f.paph = (const float *)d[13]; f.plsm = (const float *)d[14]; f.ldcum = (const int32_t *)d[15];
+  f.ktype = (const int32_t *)d[16]; f.peis = (const float *)d[17]; f.plu = (const float *)d[18];
+  f.plude = (float *)d[19]; f.pludeli = (const float *)d[20]; f.psnde = (const float *)d[21];
+  f.pmfu = (const float *)d[22]; f.pmfd = (const float *)d[23]; f.pa = (const float *)d[24];
+  f.pclv = (const float *)d[25]; f.pcovptot = (float *)d[26]; f.prainfrac_toprfz = (float *)d[27];
+  f.pfsqlf = (float *)d[28]; f.pfsqif = (float *)d[29]; f.pfcqnng = (float *)d[30];
+  f.pfcqlng = (float *)d[31]; f.pfsqrf = (float *)d[32]; f.pfsqsf = (float *)d[33];
+  f.pfcqrng = (float *)d[34]; f.pfcqsng = (float *)d[35]; f.pfsqltur = (float *)d[36];
+  f.pfsqitur = (float *)d[37]; f.pfplsl = (float *)d[38]; f.pfplsn = (float *)d[39];
+  f.pfhpsl = (float *)d[40]; f.pfhpsn = (float *)d[41];
+  f.ncounters = counter;
+  return f;
+}
+
+// Launch the single-precision interface's kernel of `precision` with that
+// precision's schedule.
+int launch_sp_checked(int precision, const FieldsSP &f, const Shape &sh, cudaStream_t stream) {
+  Schedule sc;
+  bool gen = true;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    sc = g_sched[precision];
+    gen = g_gen;
+  }
+  int threads = sc.threads;
+  if ((sc.variant != 0 || !gen) && threads > 512) threads = 512;
+  const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
+  const int grid = grid_for(sc.ctas_per_sm, tiles);
+  cudaError_t e = launch_sp(precision, sc.variant, f, sh, threads, grid, stream, gen);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+// The host-pointer pipeline of cloudsc_b200_batched_host(_sp): chunks of
+// blocks through three device slots, H2D on stream 0, the kernel on stream 1,
+// D2H on stream 2; fb = bytes of a real element (8 or 4); `launch_fn(d, sh,
+// stream)` launches the kernel on the slot's arrays d.
+template <typename LaunchFn>
+int host_pipeline(const void *host[42], int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+                  double ptsphy, int32_t chunk_blocks, size_t fb, LaunchFn launch_fn) {
+  int dev = 0;
+  int rc = ensure_params(&dev);
+  if (rc) return rc;
+  const size_t np = nproma, kl = klev;
+  int cb = chunk_blocks > 0 ? chunk_blocks : 64;
+  if (cb > ngpblks) cb = ngpblks;
+  const int nslot = 3;
+  const size_t slot_bytes = carve(nullptr, np, kl, cb, nullptr, fb);
+  rc = t_ws.prepare(dev, slot_bytes * nslot);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), t_ws.st[1]);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaMemsetAsync", e);
+  const int nchunk = (ngpblks + cb - 1) / cb;
+  for (int c = 0; c < nchunk && e == cudaSuccess; ++c) {
+    const int slot = c % nslot;
+    const int b0 = c * cb, nb = (b0 + cb <= ngpblks) ? cb : ngpblks - b0;
+    void *d[42];
+    carve(t_ws.buf + slot * slot_bytes, np, kl, cb, d, fb);
+    // the slot is free once its previous D2H has finished
+    if (c >= nslot) e = cudaStreamWaitEvent(t_ws.st[0], t_ws.ev_out[slot], 0);
+    for (int i = 0; i < 42 && e == cudaSuccess; ++i)
+      if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, b0, nb, t_ws.st[0], fb);
+    if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_in[slot], t_ws.st[0]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[1], t_ws.ev_in[slot], 0);
+    if (e != cudaSuccess) break;
+    int ngptot_c = ngptot - b0 * nproma;
+    if (ngptot_c > nb * nproma) ngptot_c = nb * nproma;
+    Shape sh = {nproma, klev, nb, ngptot_c, 0, ptsphy};
+    rc = launch_fn(d, sh, t_ws.st[1]);
+    if (rc) return drained(rc, {t_ws.st[0], t_ws.st[1], t_ws.st[2]});
+    e = cudaEventRecord(t_ws.ev_done[slot], t_ws.st[1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[slot], 0);
+    // Whole blocks are copied back in one piece; a partial last block (columns
+    // beyond NGPTOT) returns only its computed columns, leaving the padding
+    // of the caller's array untouched as the reference does.
+    const int icend_last = ngptot_c - (nb - 1) * nproma;
+    const int nfull = (icend_last == nproma) ? nb : nb - 1;
+    for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
+      if (!kArrs[i].out) continue;
+      const size_t esz = elem_size(i, fb);
+      size_t per = elems(kArrs[i].kind, np, kl) * esz;
+      char *hb = (char *)host[i] + (size_t)b0 * per;
+      if (nfull > 0 && i == kLocCld)
+        e = cudaMemcpy2DAsync(hb, per, d[i], per, out_rows(i, kl) * np * esz, nfull, cudaMemcpyDeviceToHost,
+                              t_ws.st[2]);
+      else if (nfull > 0)
+        e = cudaMemcpyAsync(hb, d[i], per * nfull, cudaMemcpyDeviceToHost, t_ws.st[2]);
+      if (e == cudaSuccess && nfull < nb)
+        e = cudaMemcpy2DAsync(hb + per * nfull, np * esz, (char *)d[i] + per * nfull, np * esz,
+                              (size_t)icend_last * esz, out_rows(i, kl), cudaMemcpyDeviceToHost, t_ws.st[2]);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_out[slot], t_ws.st[2]);
+  }
+  uint32_t nwarn = 0;
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[(nchunk - 1) % nslot], 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, t_ws.st[2]);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t_ws.st[2]);
+  if (e != cudaSuccess)
+    return drained(fail(CLOUDSC_E_CUDA, "pipelined host path", e), {t_ws.st[0], t_ws.st[1], t_ws.st[2]});
+  return (int)nwarn;
+}
+
+// Argument checks shared by the batched entries of both interfaces.
+int batched_args_ok(const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot,
+                    double ptsphy, int32_t precision) {
+  int rc = check_params_match(p);
+  if (rc) return rc;
+  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
+  if (budgets_on(*p) || opt_on(*p))
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_block "
+                                       "or cloudsc_b200_batched_diag");
+  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
+      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
+    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
+  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
+  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
+  return CLOUDSC_OK;
 }
 
 }  // namespace
@@ -929,17 +1067,8 @@ int cloudsc_b200_batched_host(
     double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
     double *pfplsn, double *pfhpsl, double *pfhpsn, int32_t precision, int32_t chunk_blocks) {
-  int rc = check_params_match(p);
+  int rc = batched_args_ok(p, nproma, klev, ngpblks, ngptot, ptsphy, precision);
   if (rc) return rc;
-  if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
-  if (budgets_on(*p) || opt_on(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_block "
-                                       "or cloudsc_b200_batched_diag");
-  if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
-      (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
-    return fail(CLOUDSC_E_SHAPE, "inconsistent NPROMA/KLEV/NGPBLKS/NGPTOT");
-  if (p->ncldtop > klev) return fail(CLOUDSC_E_SHAPE, "NCLDTOP > KLEV");
-  if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
   const void *host[42] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
                           ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
                           pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
@@ -948,67 +1077,69 @@ int cloudsc_b200_batched_host(
                           pfhpsn};
   for (const void *q : host)
     if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
-  int dev = 0;
-  rc = ensure_params(&dev);
+  return host_pipeline(host, nproma, klev, ngpblks, ngptot, ptsphy, chunk_blocks, 8,
+                       [&](void *d[42], const Shape &sh, cudaStream_t st) {
+                         return launch_checked(precision, fields_from(d, t_ws.counter), sh, st);
+                       });
+}
+
+// The single-precision interface (JPRB = REAL(4)), device pointers.
+int cloudsc_b200_batched_sp(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot, float ptsphy,
+    const float *pt, const float *pq, const float *ptendency_cml_t, const float *ptendency_cml_q,
+    const float *ptendency_cml_a, const float *ptendency_cml_cld, float *ptendency_loc_t,
+    float *ptendency_loc_q, float *ptendency_loc_a, float *ptendency_loc_cld, const float *pvfl,
+    const float *pvfi, const float *pap, const float *paph, const float *plsm, const int32_t *ldcum,
+    const int32_t *ktype, const float *peis, const float *plu, float *plude, const float *pludeli,
+    const float *psnde, const float *pmfu, const float *pmfd, const float *pa, const float *pclv,
+    float *pcovptot, float *prainfrac_toprfz, float *pfsqlf, float *pfsqif, float *pfcqnng, float *pfcqlng,
+    float *pfsqrf, float *pfsqsf, float *pfcqrng, float *pfcqsng, float *pfsqltur, float *pfsqitur,
+    float *pfplsl, float *pfplsn, float *pfhpsl, float *pfhpsn, uint32_t *ncounters, int32_t precision,
+    void *stream) {
+  int rc = batched_args_ok(p, nproma, klev, ngpblks, ngptot, ptsphy, precision);
   if (rc) return rc;
-  const size_t np = nproma, kl = klev;
-  int cb = chunk_blocks > 0 ? chunk_blocks : 64;
-  if (cb > ngpblks) cb = ngpblks;
-  const int nslot = 3;
-  const size_t slot_bytes = carve(nullptr, np, kl, cb, nullptr);
-  rc = t_ws.prepare(dev, slot_bytes * nslot);
+  void *d[42] = {(void *)pt, (void *)pq, (void *)ptendency_cml_t, (void *)ptendency_cml_q,
+                 (void *)ptendency_cml_a, (void *)ptendency_cml_cld, ptendency_loc_t, ptendency_loc_q,
+                 ptendency_loc_a, ptendency_loc_cld, (void *)pvfl, (void *)pvfi, (void *)pap, (void *)paph,
+                 (void *)plsm, (void *)ldcum, (void *)ktype, (void *)peis, (void *)plu, plude,
+                 (void *)pludeli, (void *)psnde, (void *)pmfu, (void *)pmfd, (void *)pa, (void *)pclv,
+                 pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng, pfsqrf, pfsqsf, pfcqrng,
+                 pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl, pfhpsn};
+  for (void *q : d)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  rc = ensure_params(nullptr);
   if (rc) return rc;
-  cudaError_t e = cudaMemsetAsync(t_ws.counter, 0, sizeof(uint32_t), t_ws.st[1]);
-  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaMemsetAsync", e);
-  const int nchunk = (ngpblks + cb - 1) / cb;
-  for (int c = 0; c < nchunk && e == cudaSuccess; ++c) {
-    const int slot = c % nslot;
-    const int b0 = c * cb, nb = (b0 + cb <= ngpblks) ? cb : ngpblks - b0;
-    void *d[42];
-    carve(t_ws.buf + slot * slot_bytes, np, kl, cb, d);
-    // the slot is free once its previous D2H has finished
-    if (c >= nslot) e = cudaStreamWaitEvent(t_ws.st[0], t_ws.ev_out[slot], 0);
-    for (int i = 0; i < 42 && e == cudaSuccess; ++i)
-      if (kArrs[i].in) e = copy_in(d[i], host[i], i, np, kl, b0, nb, t_ws.st[0]);
-    if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_in[slot], t_ws.st[0]);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[1], t_ws.ev_in[slot], 0);
-    if (e != cudaSuccess) break;
-    Fields f = fields_from(d, t_ws.counter);
-    int ngptot_c = ngptot - b0 * nproma;
-    if (ngptot_c > nb * nproma) ngptot_c = nb * nproma;
-    Shape sh = {nproma, klev, nb, ngptot_c, 0, ptsphy};
-    rc = launch_checked(precision, f, sh, t_ws.st[1]);
-    if (rc) return drained(rc, {t_ws.st[0], t_ws.st[1], t_ws.st[2]});
-    e = cudaEventRecord(t_ws.ev_done[slot], t_ws.st[1]);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[slot], 0);
-    // Whole blocks are copied back in one piece; a partial last block (columns
-    // beyond NGPTOT) returns only its computed columns, leaving the padding
-    // of the caller's array untouched as the reference does.
-    const int icend_last = ngptot_c - (nb - 1) * nproma;
-    const int nfull = (icend_last == nproma) ? nb : nb - 1;
-    for (int i = 0; i < 42 && e == cudaSuccess; ++i) {
-      if (!kArrs[i].out) continue;
-      size_t per = elems(kArrs[i].kind, np, kl) * 8;
-      char *hb = (char *)host[i] + (size_t)b0 * per;
-      if (nfull > 0 && i == kLocCld)
-        e = cudaMemcpy2DAsync(hb, per, d[i], per, out_rows(i, kl) * np * 8, nfull, cudaMemcpyDeviceToHost,
-                              t_ws.st[2]);
-      else if (nfull > 0)
-        e = cudaMemcpyAsync(hb, d[i], per * nfull, cudaMemcpyDeviceToHost, t_ws.st[2]);
-      if (e == cudaSuccess && nfull < nb)
-        e = cudaMemcpy2DAsync(hb + per * nfull, np * 8, (char *)d[i] + per * nfull, np * 8,
-                              (size_t)icend_last * 8, out_rows(i, kl), cudaMemcpyDeviceToHost, t_ws.st[2]);
-    }
-    if (e == cudaSuccess) e = cudaEventRecord(t_ws.ev_out[slot], t_ws.st[2]);
-  }
-  uint32_t nwarn = 0;
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(t_ws.st[2], t_ws.ev_done[(nchunk - 1) % nslot], 0);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&nwarn, t_ws.counter, sizeof(uint32_t), cudaMemcpyDeviceToHost, t_ws.st[2]);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(t_ws.st[2]);
-  if (e != cudaSuccess)
-    return drained(fail(CLOUDSC_E_CUDA, "pipelined host path", e), {t_ws.st[0], t_ws.st[1], t_ws.st[2]});
-  return (int)nwarn;
+  Shape sh = {nproma, klev, ngpblks, ngptot, 0, (double)ptsphy};
+  return launch_sp_checked(precision, fields_sp_from(d, ncounters), sh, (cudaStream_t)stream);
+}
+
+// The single-precision interface, host pointers, pipelined like
+// cloudsc_b200_batched_host (half the bytes cross PCIe).
+int cloudsc_b200_batched_host_sp(
+    const cloudsc_params *p, int32_t nproma, int32_t klev, int32_t ngpblks, int32_t ngptot, float ptsphy,
+    const float *pt, const float *pq, const float *ptendency_cml_t, const float *ptendency_cml_q,
+    const float *ptendency_cml_a, const float *ptendency_cml_cld, float *ptendency_loc_t,
+    float *ptendency_loc_q, float *ptendency_loc_a, float *ptendency_loc_cld, const float *pvfl,
+    const float *pvfi, const float *pap, const float *paph, const float *plsm, const int32_t *ldcum,
+    const int32_t *ktype, const float *peis, const float *plu, float *plude, const float *pludeli,
+    const float *psnde, const float *pmfu, const float *pmfd, const float *pa, const float *pclv,
+    float *pcovptot, float *prainfrac_toprfz, float *pfsqlf, float *pfsqif, float *pfcqnng, float *pfcqlng,
+    float *pfsqrf, float *pfsqsf, float *pfcqrng, float *pfcqsng, float *pfsqltur, float *pfsqitur,
+    float *pfplsl, float *pfplsn, float *pfhpsl, float *pfhpsn, int32_t precision, int32_t chunk_blocks) {
+  int rc = batched_args_ok(p, nproma, klev, ngpblks, ngptot, ptsphy, precision);
+  if (rc) return rc;
+  const void *host[42] = {pt, pq, ptendency_cml_t, ptendency_cml_q, ptendency_cml_a, ptendency_cml_cld,
+                          ptendency_loc_t, ptendency_loc_q, ptendency_loc_a, ptendency_loc_cld, pvfl,
+                          pvfi, pap, paph, plsm, ldcum, ktype, peis, plu, plude, pludeli, psnde, pmfu,
+                          pmfd, pa, pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng,
+                          pfsqrf, pfsqsf, pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl,
+                          pfhpsn};
+  for (const void *q : host)
+    if (!q) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  return host_pipeline(host, nproma, klev, ngpblks, ngptot, (double)ptsphy, chunk_blocks, 4,
+                       [&](void *d[42], const Shape &sh, cudaStream_t st) {
+                         return launch_sp_checked(precision, fields_sp_from(d, t_ws.counter), sh, st);
+                       });
 }
 
 }  // extern "C"

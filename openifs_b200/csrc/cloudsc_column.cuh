@@ -132,6 +132,39 @@ CSC_DEV double mpowb(const PowBase &b, double y) {
   return plibm_pow_with_log(b.x, y, b.lhi, b.llo);
 #endif
 }
+// pow with a parameter as exponent.  With GEN the host has checked that the
+// exponent is none of 0.5, 1.5, 2 and 3, in double and rounded to float
+// (gen_exponents_ok), so the tests for those exponents are left out: the
+// same results as mpow / mpowb with fewer branches.
+CSC_DEV float xpow_gen(float x, float y) {
+#if defined(__CUDA_ARCH__)
+  return __powf(x, y);
+#else
+  return powf(x, y);
+#endif
+}
+template <bool F32, bool GEN>
+CSC_DEV double mpowp(double x, double y) {
+  if (!GEN) return mpow<F32>(x, y);
+  if (F32) return (double)xpow_gen((float)x, (float)y);
+#if defined(CLOUDSC_HOST_LIBM_GLIBC) && !defined(__CUDA_ARCH__)
+  return pow(x, y);
+#else
+  double lhi, llo;
+  plibm_log_base(x, &lhi, &llo);
+  return plibm_pow_with_log_gen(x, y, lhi, llo);
+#endif
+}
+template <bool F32, bool GEN>
+CSC_DEV double mpowbp(const PowBase &b, double y) {
+  if (!GEN) return mpowb<F32>(b, y);
+  if (F32) return (double)xpow_gen((float)b.x, (float)y);
+#if defined(CLOUDSC_HOST_LIBM_GLIBC) && !defined(__CUDA_ARCH__)
+  return pow(b.x, y);
+#else
+  return plibm_pow_with_log_gen(b.x, y, b.lhi, b.llo);
+#endif
+}
 CSC_DEV double xsqrt(double x) { return sqrt(x); }
 CSC_DEV float xsqrt(float x) { return sqrtf(x); }
 

@@ -46,6 +46,25 @@ struct Fields {
   int nrftotal;
 };
 
+// Pointers of the batched arrays of the single-precision interface
+// (JPRB = REAL(4), the OpenIFS single-precision build: parkind1.F90:41-44):
+// the arrays the default configuration reads and writes, in float, with the
+// member names of Fields so that the column body reads them unchanged (each
+// load widened to double, each store rounded to float).
+struct FieldsSP {
+  const float *pt, *pq, *cml_t, *cml_q, *cml_a, *cml_cld;
+  float *loc_t, *loc_q, *loc_a, *loc_cld;
+  const float *pvfl, *pvfi, *pap, *paph, *plsm;
+  const int32_t *ldcum, *ktype;
+  const float *peis, *plu;
+  float *plude;
+  const float *pludeli, *psnde, *pmfu, *pmfd, *pa, *pclv;
+  float *pcovptot, *prainfrac_toprfz;
+  float *pfsqlf, *pfsqif, *pfcqnng, *pfcqlng, *pfsqrf, *pfsqsf, *pfcqrng, *pfcqsng;
+  float *pfsqltur, *pfsqitur, *pfplsl, *pfplsn, *pfhpsl, *pfhpsn;
+  uint32_t *ncounters;
+};
+
 // Pointers of the batched CLOUD_SATADJ arrays (same block layout).
 struct SatadjFields {
   const double *pap, *paph, *pt, *pq, *pa, *pl, *pi;

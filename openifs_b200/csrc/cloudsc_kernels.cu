@@ -68,8 +68,12 @@ namespace cloudsc {
 //      leaves residues above CLOUDSC's 1e-14 kg/kg thresholds that switch
 //      precipitation processes on and off down the column, so this form is
 //      faster but further from FP64 (measured tendency errors of 0.3-4 %).
-template <int FORM, int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh) {
+// FT: Fields (the double-precision interface) or FieldsSP (float arrays,
+// forms 0-2 only).  GEN: the parameter-exponent pows without their tests for
+// the exponents 0.5, 1.5, 2 and 3 (forms 0-2; the host launches it when the
+// uploaded parameters have none of these, gen_exponents_ok).
+template <int FORM, int MAXT, int MINB, typename FT = Fields, bool GEN = false>
+__global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(FT F, Shape sh) {
   // Let ptxas place part of the register spills in shared memory instead of
   // local memory (a PTX pragma; the spill slots it moves no longer go
   // through L1/L2).  With the shared-memory tables, FP64: 15.29 ms vs
@@ -89,11 +93,11 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(Fields F, Shape sh)
       jl = sh.kidia0;
     }
     if constexpr (FORM == 2)
-      cloudsc_column<float, true>(F, sh, ib, jl, active);
+      cloudsc_column<float, true, false, false, FT, GEN>(F, sh, ib, jl, active);
     else if constexpr (FORM >= 3)
-      cloudsc_column<double, false, FORM == 3 || FORM == 5, FORM >= 4>(F, sh, ib, jl, active);
+      cloudsc_column<double, false, FORM == 3 || FORM == 5, FORM >= 4, FT, false>(F, sh, ib, jl, active);
     else
-      cloudsc_column<double, FORM == 1>(F, sh, ib, jl, active);
+      cloudsc_column<double, FORM == 1, false, false, FT, GEN>(F, sh, ib, jl, active);
   }
 }
 
@@ -241,6 +245,13 @@ __global__ void __launch_bounds__(kSatadjThreads) state_increment_kernel(IncFiel
 // ---------------------------------------------------------------------------
 namespace cloudsc {
 
+// Whether the parameters allow the GEN kernels (gen_exponents_ok).
+bool params_allow_gen(const cloudsc_params &p, const Derived &d) {
+  KParams<double> kd;
+  fill_kparams(p, d, kd);
+  return gen_exponents_ok(kd);
+}
+
 // Upload the parameters to this device's constant memory (all three blocks).
 cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
   KParams<double> kd;
@@ -276,34 +287,68 @@ void variant_bounds(int v, int *maxt, int *minb) {
   *minb = kVariants[v].minb;
 }
 
-template <int FORM>
+template <int FORM, bool GEN>
 static const void *kernel_ptr_form(int v) {
   switch (v) {
-    case 0: return (const void *)cloudsc_kernel<FORM, kVariants[0].maxt, kVariants[0].minb>;
-    case 1: return (const void *)cloudsc_kernel<FORM, kVariants[1].maxt, kVariants[1].minb>;
-    case 2: return (const void *)cloudsc_kernel<FORM, kVariants[2].maxt, kVariants[2].minb>;
-    case 3: return (const void *)cloudsc_kernel<FORM, kVariants[3].maxt, kVariants[3].minb>;
-    case 4: return (const void *)cloudsc_kernel<FORM, kVariants[4].maxt, kVariants[4].minb>;
-    case 5: return (const void *)cloudsc_kernel<FORM, kVariants[5].maxt, kVariants[5].minb>;
+    case 0: return (const void *)cloudsc_kernel<FORM, kVariants[0].maxt, kVariants[0].minb, Fields, GEN>;
+    case 1: return (const void *)cloudsc_kernel<FORM, kVariants[1].maxt, kVariants[1].minb, Fields, GEN>;
+    case 2: return (const void *)cloudsc_kernel<FORM, kVariants[2].maxt, kVariants[2].minb, Fields, GEN>;
+    case 3: return (const void *)cloudsc_kernel<FORM, kVariants[3].maxt, kVariants[3].minb, Fields, GEN>;
+    case 4: return (const void *)cloudsc_kernel<FORM, kVariants[4].maxt, kVariants[4].minb, Fields, GEN>;
+    case 5: return (const void *)cloudsc_kernel<FORM, kVariants[5].maxt, kVariants[5].minb, Fields, GEN>;
     default: return nullptr;
   }
 }
 static_assert(kNumVariants == 6, "kernel_ptr_form lists every variant");
-static const void *kernel_ptr(int precision, int v) {
+// Forms 0-2 exist in every variant with GEN (the parameters of every known
+// configuration allow it) and, for parameters that do not, in the (512, 1)
+// variant without it (`launch` then runs that one).  Forms 3-5 (budgets,
+// SPP, inhomogeneity) keep the tests.
+static const void *kernel_ptr(int precision, int v, bool gen) {
+  if (!gen && precision <= 2) {
+    switch (precision) {
+      case 0: return (const void *)cloudsc_kernel<0, 512, 1, Fields, false>;
+      case 1: return (const void *)cloudsc_kernel<1, 512, 1, Fields, false>;
+      case 2: return (const void *)cloudsc_kernel<2, 512, 1, Fields, false>;
+    }
+  }
   switch (precision) {
-    case 0: return kernel_ptr_form<0>(v);
-    case 1: return kernel_ptr_form<1>(v);
-    case 2: return kernel_ptr_form<2>(v);
-    case 3: return kernel_ptr_form<3>(v);
-    case 4: return kernel_ptr_form<4>(v);
-    case 5: return kernel_ptr_form<5>(v);
+    case 0: return kernel_ptr_form<0, true>(v);
+    case 1: return kernel_ptr_form<1, true>(v);
+    case 2: return kernel_ptr_form<2, true>(v);
+    case 3: return kernel_ptr_form<3, false>(v);
+    case 4: return kernel_ptr_form<4, false>(v);
+    case 5: return kernel_ptr_form<5, false>(v);
+    default: return nullptr;
+  }
+}
+
+// The single-precision interface's kernels: forms 0-2 in the two variants
+// the tuned schedules use, (640, 1) and (512, 1), with GEN; without GEN in
+// the (512, 1) variant.  Other variants map to the (512, 1) kernel (see
+// launch_sp).
+static const void *kernel_ptr_sp(int precision, int v, bool gen) {
+  const bool big = v == 0 && gen;
+  switch (precision) {
+    case 0:
+      return big ? (const void *)cloudsc_kernel<0, 640, 1, FieldsSP, true>
+                 : gen ? (const void *)cloudsc_kernel<0, 512, 1, FieldsSP, true>
+                       : (const void *)cloudsc_kernel<0, 512, 1, FieldsSP, false>;
+    case 1:
+      return big ? (const void *)cloudsc_kernel<1, 640, 1, FieldsSP, true>
+                 : gen ? (const void *)cloudsc_kernel<1, 512, 1, FieldsSP, true>
+                       : (const void *)cloudsc_kernel<1, 512, 1, FieldsSP, false>;
+    case 2:
+      return big ? (const void *)cloudsc_kernel<2, 640, 1, FieldsSP, true>
+                 : gen ? (const void *)cloudsc_kernel<2, 512, 1, FieldsSP, true>
+                       : (const void *)cloudsc_kernel<2, 512, 1, FieldsSP, false>;
     default: return nullptr;
   }
 }
 
 // Registers and local (spill) bytes per thread of variant v (needs a device).
 cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes) {
-  const void *k = kernel_ptr(precision, v);
+  const void *k = kernel_ptr(precision, v, true);
   if (!k) return cudaErrorInvalidValue;
   cudaFuncAttributes a;
   cudaError_t e = cudaFuncGetAttributes(&a, k);
@@ -314,13 +359,31 @@ cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes
 }
 
 // Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed,
-// 2 = FP32 physics.
+// 2 = FP32 physics, 3-5 the FP64 forms with budgets / SPP and inhomogeneity;
+// gen: the parameters allow the GEN kernels (forms 0-2 otherwise run the
+// (512, 1) kernel without GEN, at most 512 columns per CTA).
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
-                   cudaStream_t stream) {
+                   cudaStream_t stream, bool gen) {
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  const void *k = kernel_ptr(precision, v);
+  if (!gen && precision <= 2 && threads > 512) return cudaErrorInvalidConfiguration;
+  const void *k = kernel_ptr(precision, v, gen);
   if (!k) return cudaErrorInvalidValue;
   Fields fa = f;
+  Shape sa = sh;
+  void *args[] = {&fa, &sa};
+  return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, 0, stream);
+}
+
+// Launch form `precision` (0-2) of the single-precision interface with the
+// schedule of variant v: variant 0 keeps its (640, 1) kernel; every other
+// variant runs the (512, 1) kernel with at most 512 columns per CTA.
+cudaError_t launch_sp(int precision, int v, const FieldsSP &f, const Shape &sh, int threads, int grid,
+                      cudaStream_t stream, bool gen) {
+  if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
+  if ((v != 0 || !gen) && threads > 512) return cudaErrorInvalidConfiguration;
+  const void *k = kernel_ptr_sp(precision, v, gen);
+  if (!k) return cudaErrorInvalidValue;
+  FieldsSP fa = f;
   Shape sa = sh;
   void *args[] = {&fa, &sa};
   return cudaLaunchKernel(k, dim3(grid), dim3(threads), args, 0, stream);

@@ -61,6 +61,23 @@ inline void fill_kparams(const cloudsc_params &p, const Derived &d, KParams<Real
 }
 
 
+// The kernels' pows whose exponent is a parameter (mpowp / mpowbp in
+// cloudsc_body.cuh) may skip their tests for the exponents 0.5, 1.5, 2 and 3
+// (the GEN kernels) when none of these parameters is such an exponent, in
+// double or rounded to float.  This list names every exponent those call
+// sites use.
+inline bool gen_exponents_ok(const KParams<double> &k) {
+  const double ex[] = {k.flt_0p4,     k.kkbac_m1,    k.kkbauq_m1,   k.rcl_const3r, k.rcl_const4r,
+                       k.rcl_const4s, k.rcl_const5s, k.rcl_const6r, k.rcl_const8s, k.rcl_dr,
+                       k.rcl_kkbac,   k.rcl_lam2r,   k.rcl_lam2s,   k.rcl_x2r};
+  for (double y : ex) {
+    const float yf = (float)y;
+    if (y == 0.5 || y == 1.5 || y == 2.0 || y == 3.0) return false;
+    if (yf == 0.5f || yf == 1.5f || yf == 2.0f || yf == 3.0f) return false;
+  }
+  return true;
+}
+
 inline void fill_kparams_d(const cloudsc_params &p, KParamsD &dd) {
   dd.rg = p.rg; dd.retv = p.retv; dd.rtt = p.rtt; dd.rtice = p.rtice; dd.rtwat = p.rtwat;
   dd.rtwat_rtice_r = p.rtwat_rtice_r; dd.r2es = p.r2es; dd.r3les = p.r3les; dd.r3ies = p.r3ies;

@@ -150,9 +150,18 @@ PLIBM_FN double plibm_sqrt(double x) {
 /* 2^k for -1022 <= k <= 1023 */
 PLIBM_FN double plibm_pow2i(int k) { return plibm_from_bits((uint64_t)(int64_t)(k + 1023) << 52); }
 
-/* exp(hi + lo) for |lo| <= ~1e-15 |hi|, every hi (the full path). */
-PLIBM_FN_COLD double plibm_exp_dd_full(double hi, double lo) {
-  /* clamp so the main path stays finite; results overflow / underflow naturally */
+/* exp(hi + lo) for |lo| <= ~1e-15 |hi|, every hi; the kernel of both exp and
+ * pow.  Straight-line code (no branch), so that a compiler can interleave
+ * independent calls: the argument is clamped to [-746, 709.9] (the result
+ * then overflows or underflows as it should) and the scale 2^m is applied as
+ * two exact factors 2^(m>>1) 2^(m-(m>>1)), each a normal number for every m
+ * the clamped argument gives; NaN is passed through by a select.  The table
+ * index j is in [0, 127] for every input, NaN included.  (For -700 < hi <
+ * 700, 2^m e is normal and the two factors give exactly the bits of adding m
+ * to e's exponent field.)  use_lo = 0 skips the addition of lo = 0, which
+ * changes r only for r = -0, where expm1(-0) and expm1(+0) give the same
+ * sum s. */
+PLIBM_FN_HEAVY double plibm_exp_core(double hi, double lo, int use_lo) {
   double hc = hi > 709.9 ? 709.9 : hi;
   hc = hc < -746.0 ? -746.0 : hc;
   double kd = plibm_fma(hc, PLIBM_INV_LN2_128, PLIBM_SHIFT);
@@ -160,7 +169,7 @@ PLIBM_FN_COLD double plibm_exp_dd_full(double hi, double lo) {
   kd = kd - PLIBM_SHIFT;
   double r = plibm_fma(-kd, PLIBM_LN2_128_HI, hc);
   r = plibm_fma(-kd, PLIBM_LN2_128_LO, r);
-  r = r + lo;
+  if (use_lo) r = r + lo;
   int j = (int)(ki & 127);
   int m = (int)(ki >> 7);
   double thi = plibm_exp_t(2 * j), tlo = plibm_exp_t(2 * j + 1);
@@ -174,36 +183,9 @@ PLIBM_FN_COLD double plibm_exp_dd_full(double hi, double lo) {
   double res = (e * plibm_pow2i(m1)) * plibm_pow2i(m2);
   return hi != hi ? hi : res;
 }
-
-/* exp(hi + lo) for |lo| <= ~1e-15 |hi|; the kernel of both exp and pow.
- * For -700 < hi < 700 the full path's clamps do nothing and 2^m e (m the
- * scale, -1010 <= m <= 1010, e in [2^(-1/256), 2^(255/256))) is a normal
- * number, so adding m to e's exponent field gives exactly the full path's
- * two-step product: both paths return the same bits.  NaN and the ends go
- * through the full path. */
-PLIBM_FN_HEAVY double plibm_exp_core(double hi, double lo, int use_lo) {
-  if (!(hi > -700.0 && hi < 700.0)) return plibm_exp_dd_full(hi, lo);
-  double kd = plibm_fma(hi, PLIBM_INV_LN2_128, PLIBM_SHIFT);
-  int64_t ki = (int64_t)(plibm_bits(kd) & 0xfffffffffffffULL) - (int64_t)(1LL << 51);
-  kd = kd - PLIBM_SHIFT;
-  double r = plibm_fma(-kd, PLIBM_LN2_128_HI, hi);
-  r = plibm_fma(-kd, PLIBM_LN2_128_LO, r);
-  if (use_lo) r = r + lo;
-  int j = (int)(ki & 127);
-  int m = (int)(ki >> 7);
-  double thi = plibm_exp_t(2 * j), tlo = plibm_exp_t(2 * j + 1);
-  double p = plibm_fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5); /* 1/120, 1/24 */
-  p = plibm_fma(p, r, 0x1.5555555555555p-3);                          /* 1/6 */
-  p = plibm_fma(p, r, 0x1.0000000000000p-1);                          /* 1/2 */
-  p = plibm_fma(p, r * r, r);                                         /* expm1(r) */
-  double s = plibm_fma(thi, p, tlo);
-  double e = thi + s;
-  return plibm_from_bits(plibm_bits(e) + ((uint64_t)(int64_t)m << 52));
-}
 PLIBM_FN double plibm_exp_dd(double hi, double lo) { return plibm_exp_core(hi, lo, 1); }
 
-/* exp(x): lo = 0 needs no addition (r + 0 differs from r only for r = -0,
- * and expm1(-0) and expm1(+0) give the same sum s below). */
+/* exp(x): lo = 0 needs no addition. */
 PLIBM_FN double plibm_exp(double x) { return plibm_exp_core(x, 0.0, 0); }
 
 /* ln(x) as hi + lo for finite x > 0. */
@@ -302,6 +284,16 @@ PLIBM_FN double plibm_pow_with_log(double x, double y, double lhi, double llo) {
   if (y == 1.5) return plibm_pow1p5(x);
   if (y == 2.0) return x * x;
   if (y == 3.0) return plibm_cube(x);
+  double res = plibm_pow_log(lhi, llo, y);
+  if (x > 0.0 && x < PLIBM_INF && y != 0.0 && y == y) return res;
+  return plibm_pow_special(x, y, res);
+}
+
+/* x^y given plibm_log_base(x) = lhi + llo, for an exponent that is none of
+ * 0.5, 1.5, 2 and 3: the same bits as plibm_pow_with_log without its tests
+ * of the exponent (the kernels use it where the exponent is a parameter the
+ * host has checked). */
+PLIBM_FN double plibm_pow_with_log_gen(double x, double y, double lhi, double llo) {
   double res = plibm_pow_log(lhi, llo, y);
   if (x > 0.0 && x < PLIBM_INF && y != 0.0 && y == y) return res;
   return plibm_pow_special(x, y, res);

@@ -58,6 +58,9 @@ BATCHED_FIELDS = [
     ("pfhpsn", "hl", np.float64, "out"),
 ]
 FIELD_INDEX = {f[0]: i for i, f in enumerate(BATCHED_FIELDS)}
+# element type of each array in the single-precision interface (JPRB =
+# REAL(4)): every real array float32, the integer ones unchanged
+DTYPE_SP = {f[0]: (np.float32 if f[2] == np.float64 else f[2]) for f in BATCHED_FIELDS}
 INPUT_NAMES = [f[0] for f in BATCHED_FIELDS if f[3] in ("in", "inout")]
 OUTPUT_NAMES = [f[0] for f in BATCHED_FIELDS if f[3] in ("out", "inout")]
 KIND = {f[0]: f[1] for f in BATCHED_FIELDS}
@@ -236,3 +239,24 @@ def budget_fields_needed(params):
     """PEXTRA fields the budget sections of ``params`` write (cloudsc.F90:3832-4110)."""
     return ((26 if params.lbud23 else 0) + (1 if params.lcldbud_vertint else 0) + (12 if params.lcldbudc else 0) +
             (22 if params.lcldbudl else 0) + (20 if params.lcldbudi else 0) + (13 if params.lcldbudt else 0))
+
+
+def to_single(arrays):
+    """The arrays of the single-precision interface: each real array of
+    ``arrays`` (numpy or torch, fields.BATCHED_FIELDS names) rounded to
+    float32, the integer arrays as they are."""
+    out = {}
+    for n, v in arrays.items():
+        if n in DTYPE_SP and DTYPE_SP[n] == np.float32:
+            out[n] = v.astype(np.float32) if isinstance(v, np.ndarray) else v.float()
+        else:
+            out[n] = v
+    return out
+
+
+def host_copy_bytes_sp(nproma, klev, ngpblks, ngptot):
+    """Bytes per call crossing PCIe in cloudsc_b200_batched_host_sp: those of
+    host_copy_bytes with every real element 4 bytes instead of 8."""
+    h2d, d2h = host_copy_bytes(nproma, klev, ngpblks, ngptot)
+    ints = 2 * 4 * nproma * ngpblks  # LDCUM and KTYPE
+    return (h2d - ints) // 2 + ints, d2h // 2

@@ -75,10 +75,23 @@ extern "C" int hostemu_batched(const cloudsc_params *p, int nproma, int klev, in
     int icend = ngptot - ib * nproma;
     if (icend > nproma) icend = nproma;
     for (int jl = 0; jl < icend; ++jl) {
-      if (precision == 0)
-        cloudsc_column<double, false>(f, sh, ib, jl);
-      else
-        cloudsc_column<double, true>(f, sh, ib, jl);
+      // precision: the form (0 FP64, 1 FP32-mixed, 2 FP32 physics), plus
+      // 0x100 for the GEN column code (parameter-exponent pows untested)
+      const bool gen = (precision & 0x100) != 0;
+      switch (precision & 0xff) {
+        case 0:
+          if (gen) cloudsc_column<double, false, false, false, Fields, true>(f, sh, ib, jl);
+          else cloudsc_column<double, false>(f, sh, ib, jl);
+          break;
+        case 1:
+          if (gen) cloudsc_column<double, true, false, false, Fields, true>(f, sh, ib, jl);
+          else cloudsc_column<double, true>(f, sh, ib, jl);
+          break;
+        default:
+          if (gen) cloudsc_column<float, true, false, false, Fields, true>(f, sh, ib, jl);
+          else cloudsc_column<float, true>(f, sh, ib, jl);
+          break;
+      }
     }
   }
   return (int)nwarn;

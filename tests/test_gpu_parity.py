@@ -263,3 +263,19 @@ def test_phys32_form(cuda):
         assert np.isfinite(v["normwise_max"]), k
     for k in ("tendency_loc_t", "tendency_loc_q"):
         assert stats[k]["rms_ratio"] < 0.1, (k, stats[k])
+
+
+@pytest.mark.parametrize("name,value", [("rcl_x2r", 2.0), ("rcl_lam2s", 0.5)])
+def test_direct_parameter_exponent(cuda, name, value):
+    """A parameter used as a pow exponent set to one of 0.5, 1.5, 2 and 3:
+    the host then launches the kernels that keep plibm's tests for those
+    exponents (sqrt and products instead of exp(y ln x)), still bit-identical
+    to the oracle; setting the default back returns to the faster kernels."""
+    p, po = util.params()
+    q, qo = util.with_flags(p, {name: value}), util.with_flags(po, {name: value})
+    arrs = inputs.generate(6, 64, p, seed=83)
+    try:
+        _check(q, qo, arrs, 64, 6, 6 * 64 - 5)
+    finally:
+        cloudsc.setup(p)
+    _check(p, po, arrs, 64, 6, 6 * 64 - 5)

@@ -47,11 +47,11 @@ def test_satadj_with_increment_bit_exact(cuda, keymask):
                                                 np.zeros_like(ref["tendency_cml_l"])], axis=1))}
     incs = {"t": ref["tendency_loc_t"], "q": ref["tendency_loc_q"], "a": ref["tendency_loc_a"],
             "ql": ref["tendency_loc_l"], "qi": ref["tendency_loc_i"]}
-    oracle.state_increment_batched(st, incs, nproma, KLEV, nblk, ngptot, 1, keymask)
+    oracle.state_increment_batched(st, incs, nproma, util.KLEV, nblk, ngptot, 1, keymask)
     cloudsc.setup(p)
     d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
     cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
-    cloudsc.satadj_increment_batched(p, d, nproma, KLEV, nblk, ngptot, util.PTSPHY, keymask, counter=cnt)
+    cloudsc.satadj_increment_batched(p, d, nproma, util.KLEV, nblk, ngptot, util.PTSPHY, keymask, counter=cnt)
     torch.cuda.synchronize()
     g = {k: v.cpu().numpy() for k, v in d.items()}
     for n in fields.SATADJ_OUTPUTS:

@@ -199,3 +199,22 @@ def test_spp_inhomogeneity_bit_exact(pp, case):
     if "rad" in case or case.startswith("all"):
         fsd = dref["pfsd"][:-1]  # full blocks (the last block's padding is not written)
         assert (fsd >= 0.1).all() and (fsd <= 3.575).all() and len(np.unique(fsd)) > 10
+
+
+@pytest.mark.parametrize("form", [0, 1, 2])
+def test_gen_column_code_identical(pp, form):
+    """The GEN column code (parameter-exponent pows without their tests for
+    the exponents 0.5, 1.5, 2 and 3, which the default parameters never use)
+    gives the same bits as the tested code, in every form; the FP64 form also
+    equals the oracle."""
+    p, po = pp
+    arrs = inputs.generate(100, 32, p, seed=1)
+    a, nwa = util.run_hostemu(p, arrs, 32, 100, 3200, precision=form)
+    b, nwb = util.run_hostemu(p, arrs, 32, 100, 3200, precision=form | 0x100)
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, a[n]), util.defined(n, b[n])), (form, n)
+    assert nwa == nwb
+    if form == 0:
+        ref, _ = util.run_oracle(po, arrs, 32, 100, 3200)
+        for n in util.COMPARED:
+            assert np.array_equal(util.defined(n, b[n]), util.defined(n, ref[n])), n
