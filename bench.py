@@ -656,8 +656,33 @@ def _surrogate_run(a, path, p, batches, d, ref, dev, world, ms64):
         rr = r.pow(2).mean().sqrt()
         err[n] = {"rms_over_rms": float((g - r).pow(2).mean().sqrt() / rr),
                   "level_mean_baseline_rms_over_rms": float((clim - r).pow(2).mean().sqrt() / rr)}
+    # per level band: upper (levels 1-45), middle (46-91), lower (92-137)
+    bands = {"levels_1_45": slice(0, 45), "levels_46_91": slice(45, 91), "levels_92_137": slice(91, KLEV)}
+    for n in ["tendency_loc_t", "tendency_loc_q", "tendency_loc_cld"]:
+        r, g = ref[n], d[n]
+        if n == "tendency_loc_cld":
+            r, g = r[:, :4], g[:, :4]
+        err[n]["rms_over_rms_by_band"] = {
+            b: float((g[..., sl, :] - r[..., sl, :]).pow(2).mean().sqrt() / r[..., sl, :].pow(2).mean().sqrt().clamp_min(1e-300))
+            for b, sl in bands.items()}
     nf = min(flagged[0], runner.cap)
     closure = _closure(p, d, states[0].plude_in, states[0].flagged[:nf])
+    # the guard's own per-column diagnostics of batch 0 (an eager run): the
+    # network's raw water and enthalpy non-closure before the column shifts
+    # that close both budgets exactly, the head spread and the refilled
+    # condensate; their distribution and how often each criterion flags
+    runner.run(states[0])
+    torch.cuda.synchronize(dev)
+    dg = runner.diag.double()
+    qs = torch.tensor([0.5, 0.9, 0.99, 0.999], device=dg.device, dtype=torch.float64)
+    names = ["water_nonclosure_raw", "enthalpy_nonclosure_raw", "head_spread", "refilled_condensate_rel"]
+    tols = [runner.guard.closure_tol, runner.guard.closure_tol, runner.guard.spread_tol, runner.guard.neg_tol]
+    guard_diag = {}
+    for i, (nm, tol) in enumerate(zip(names, tols)):
+        v = dg[:, i]
+        qv = torch.quantile(v[:1_000_000], qs).tolist()
+        guard_diag[nm] = {"p50": qv[0], "p90": qv[1], "p99": qv[2], "p99.9": qv[3], "max": float(v.max()),
+                          "threshold": float(tol), "fraction_above_threshold": float((v > tol).double().mean())}
     # the FP64 kernel's own non-closure on the same columns (CLOUDSC applies
     # detrainment with its own phase split, so its water budget closes only
     # to ~1e-10 relative in some columns by this measure)
@@ -672,7 +697,7 @@ def _surrogate_run(a, path, p, batches, d, ref, dev, world, ms64):
         "ms_per_262144_columns": ms / SUR_BATCHES, "speedup_vs_fp64": ms64 / (ms / SUR_BATCHES),
         "flagged_per_batch": flagged, "flagged_fraction": sum(flagged) / ncols,
         "fallback_capacity_per_batch": runner.cap,
-        "error_vs_fp64_batch0": err, "closure_batch0": closure,
+        "error_vs_fp64_batch0": err, "closure_batch0": closure, "guard_diagnostics_batch0": guard_diag,
         "network": {"width": net.width, "gemm_flop_per_column": flops / NCOL,
                     "prep_plus_network_ms": fw_ms, "gemm_ms": gemm_ms,
                     "gemm_tflops": flops / (gemm_ms * 1e-3) / 1e12,
