@@ -114,8 +114,9 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp,
   double x = (mx(k.rtice, mn(k.rtwat, zt)) - k.rtice) * k.rtwat_rtice_r;
   double alfa = mn(1.0, x * x);
   bool delta = copysign(1.0, zt - k.rtt) > 0.0;  // FOEDELTA = 1
-  double ei = 0.0;
-  if (!delta || alfa < 1.0) ei = xexp(k.r3ies * (zt - k.rtt) / (zt - k.r4ies));
+  // computed whether or not a term needs it: without the branch the two
+  // exponentials overlap (the same bits where it is used)
+  double ei = xexp(k.r3ies * (zt - k.rtt) / (zt - k.r4ies));
   double zfoeeliq = mn((k.r2es * el) * zp_r, 0.5);
   double foeew = delta ? k.r2es * el : k.r2es * ei;
   double zfoeeice = mn(foeew * zp_r, 0.5);
@@ -437,8 +438,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       alfa = mn(C(1.0), x * x);
       el_e = mexp<F32M>(P.r3les * (t - P.rtt) / (t - P.r4les));
       bool delta = xsign(C(1.0), t - P.rtt) > C(0.0);
-      ei_e = C(0.0);
-      if (!delta || alfa < C(1.0)) ei_e = mexp<F32M>(P.r3ies * (t - P.rtt) / (t - P.r4ies));
+      // the ice exponential whether or not a term needs it (no branch: the
+      // two exponentials overlap)
+      ei_e = mexp<F32M>(P.r3ies * (t - P.rtt) / (t - P.r4ies));
       Real wsum = (alfa < C(1.0)) ? alfa * el_e + (C(1.0) - alfa) * ei_e : el_e;
       zfoeewm = mn((P.r2es * wsum) / pap_k, C(0.5));
       zqsmix = zfoeewm;
@@ -546,6 +548,12 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       const Real zrho = pap_k / (P.rd * t);
       // (RDENSREF/ZRHO)**0.4 appears in three processes: one shared logarithm
       const PowBase b_dens = mbase<F32M>(P.rdensref / zrho);
+      // its two powers (0.4 in the rain fall speed, the binary32 0.4 in rain
+      // evaporation and riming), computed here for every point so that they
+      // overlap with the code around them instead of waiting inside their
+      // processes' branches
+      const Real fallcorr_r = mpowb<F32M>(b_dens, C(0.4));
+      const Real fallcorr_f = mpowbp<F32M, GEN>(b_dens, P.flt_0p4);
       const Real zdtgdp = rdt * zgdp;
       const Real zrdtgdp = zdp * zrdtgdp_f;
       Real zcorqsliq, zcorqsice, zcorqsmix, zdqsmixdt, zevaplimmix;
@@ -696,7 +704,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       {
         Real ztemp = C(0.5) * (qr + qxnm1_r);
         if (ztemp != C(0.0)) {
-          Real zfallcorr = mpowb<F32M>(b_dens, C(0.4));
+          Real zfallcorr = fallcorr_r;
           Real zrlambda = mpowp<F32M, GEN>(zrho * ztemp / P.rcl_lam1r, P.rcl_lam2r);
           fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpowp<F32M, GEN>(zrlambda, P.rcl_dr);
         }
@@ -812,7 +820,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         Real zqe = mx(C(0.0), mn(qv, zqsliq));
         if (zcovpclr > zepsec && zraincldm1 > zepsec && zqe < zzrh * zqsliq) {
           Real zpreclr = zraincldm1;
-          Real zfallcorr = mpowbp<F32M, GEN>(b_dens, P.flt_0p4);
+          Real zfallcorr = fallcorr_f;
           Real zesatliq = P.rv / P.rd * (P.r2es * el_e);
           Real zlambda = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * zpreclr), P.rcl_lam2r);
           const PowBase b_lam = mbase<F32M>(zlambda);
@@ -971,7 +979,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // 4.9 riming (:2973-3017)
       if (t <= P.rtt && zliqcld > zepsec && zsnowcld > zepsec && zcovptot > C(0.01)) {
-        Real zfallcorr = mpowbp<F32M, GEN>(b_dens, P.flt_0p4);
+        Real zfallcorr = fallcorr_f;
         Real zsnowrime = P.rcl_effrime * zcovptot * rdt * P.rcl_const7s * zfallcorr *
                          mpowp<F32M, GEN>(zrho * zsnowcld * P.rcl_const1s, P.rcl_const8s);
         zsnowrime = mn(zsnowrime, C(1.0));

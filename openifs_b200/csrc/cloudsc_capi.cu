@@ -507,9 +507,9 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
                                          "cloudsc_b200_batched_diag or cloudsc_b200_block");
     form = bud && opt ? 5 : (opt ? 4 : 3);
   }
-  // parameters that rule out the GEN kernels: forms 0-2 run the (512, 1)
-  // kernel without GEN, at most 512 columns per CTA
-  const int threads = (!gen && form <= 2 && sc.threads > 512) ? 512 : sc.threads;
+  // parameters that rule out the GEN kernels: forms 0-2 run the (448, 1)
+  // kernel without GEN, at most 448 columns per CTA
+  const int threads = (!gen && form <= 2 && sc.threads > 448) ? 448 : sc.threads;
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
   cudaError_t e = launch(form, sc.variant, f, sh, threads, grid, stream, gen);
@@ -830,7 +830,7 @@ int launch_sp_checked(int precision, const FieldsSP &f, const Shape &sh, cudaStr
     gen = g_gen;
   }
   int threads = sc.threads;
-  if ((sc.variant != 0 || !gen) && threads > 512) threads = 512;
+  if ((sc.variant != 0 || !gen) && threads > 448) threads = 448;
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
   cudaError_t e = launch_sp(precision, sc.variant, f, sh, threads, grid, stream, gen);

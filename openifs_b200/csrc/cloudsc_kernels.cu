@@ -271,14 +271,17 @@ cudaError_t upload_params(const cloudsc_params &p, const Derived &d) {
 // registers, so each pair fixes the register budget per thread (and with it
 // the spills) and the CTA size it is meant for; the autotuner picks a
 // variant, a CTA size up to its MAXT and the persistence at run time.
-// Measured at 262,144 columns, FP64: (448,1) 15.98 ms with 128 registers;
-// (384,1) 17.77 ms with 168; three 128-thread CTAs per SM 21.7 ms.
+// 448 columns per CTA fill 148 SMs 3.96 times at 262,144 columns; the
+// (448, 1) bound gives them 144 registers (0.8 % faster than the 128 of a
+// (512, 1) bound, same bits).  Earlier measurements at 262,144 columns, FP64:
+// 384 columns per CTA at 168 registers 17.77 ms against 15.98 ms at 448;
+// three 128-thread CTAs per SM 21.7 ms.
 struct Variant {
   int maxt, minb;
 };
-constexpr Variant kVariants[] = {{640, 1}, {512, 1}, {384, 1}, {256, 1}, {256, 2}, {128, 3}};
+constexpr Variant kVariants[] = {{640, 1}, {448, 1}, {384, 1}, {256, 1}, {256, 2}, {128, 3}};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
-constexpr int kDefaultVariant = 1;  // (512, 1), run with 448 columns per CTA
+constexpr int kDefaultVariant = 1;  // (448, 1), run with 448 columns per CTA
 
 int num_variants() { return kNumVariants; }
 int default_variant() { return kDefaultVariant; }
@@ -301,15 +304,15 @@ static const void *kernel_ptr_form(int v) {
 }
 static_assert(kNumVariants == 6, "kernel_ptr_form lists every variant");
 // Forms 0-2 exist in every variant with GEN (the parameters of every known
-// configuration allow it) and, for parameters that do not, in the (512, 1)
+// configuration allow it) and, for parameters that do not, in the (448, 1)
 // variant without it (`launch` then runs that one).  Forms 3-5 (budgets,
 // SPP, inhomogeneity) keep the tests.
 static const void *kernel_ptr(int precision, int v, bool gen) {
   if (!gen && precision <= 2) {
     switch (precision) {
-      case 0: return (const void *)cloudsc_kernel<0, 512, 1, Fields, false>;
-      case 1: return (const void *)cloudsc_kernel<1, 512, 1, Fields, false>;
-      case 2: return (const void *)cloudsc_kernel<2, 512, 1, Fields, false>;
+      case 0: return (const void *)cloudsc_kernel<0, 448, 1, Fields, false>;
+      case 1: return (const void *)cloudsc_kernel<1, 448, 1, Fields, false>;
+      case 2: return (const void *)cloudsc_kernel<2, 448, 1, Fields, false>;
     }
   }
   switch (precision) {
@@ -324,24 +327,24 @@ static const void *kernel_ptr(int precision, int v, bool gen) {
 }
 
 // The single-precision interface's kernels: forms 0-2 in the two variants
-// the tuned schedules use, (640, 1) and (512, 1), with GEN; without GEN in
-// the (512, 1) variant.  Other variants map to the (512, 1) kernel (see
+// the tuned schedules use, (640, 1) and (448, 1), with GEN; without GEN in
+// the (448, 1) variant.  Other variants map to the (448, 1) kernel (see
 // launch_sp).
 static const void *kernel_ptr_sp(int precision, int v, bool gen) {
   const bool big = v == 0 && gen;
   switch (precision) {
     case 0:
       return big ? (const void *)cloudsc_kernel<0, 640, 1, FieldsSP, true>
-                 : gen ? (const void *)cloudsc_kernel<0, 512, 1, FieldsSP, true>
-                       : (const void *)cloudsc_kernel<0, 512, 1, FieldsSP, false>;
+                 : gen ? (const void *)cloudsc_kernel<0, 448, 1, FieldsSP, true>
+                       : (const void *)cloudsc_kernel<0, 448, 1, FieldsSP, false>;
     case 1:
       return big ? (const void *)cloudsc_kernel<1, 640, 1, FieldsSP, true>
-                 : gen ? (const void *)cloudsc_kernel<1, 512, 1, FieldsSP, true>
-                       : (const void *)cloudsc_kernel<1, 512, 1, FieldsSP, false>;
+                 : gen ? (const void *)cloudsc_kernel<1, 448, 1, FieldsSP, true>
+                       : (const void *)cloudsc_kernel<1, 448, 1, FieldsSP, false>;
     case 2:
       return big ? (const void *)cloudsc_kernel<2, 640, 1, FieldsSP, true>
-                 : gen ? (const void *)cloudsc_kernel<2, 512, 1, FieldsSP, true>
-                       : (const void *)cloudsc_kernel<2, 512, 1, FieldsSP, false>;
+                 : gen ? (const void *)cloudsc_kernel<2, 448, 1, FieldsSP, true>
+                       : (const void *)cloudsc_kernel<2, 448, 1, FieldsSP, false>;
     default: return nullptr;
   }
 }
@@ -361,11 +364,11 @@ cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes
 // Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed,
 // 2 = FP32 physics, 3-5 the FP64 forms with budgets / SPP and inhomogeneity;
 // gen: the parameters allow the GEN kernels (forms 0-2 otherwise run the
-// (512, 1) kernel without GEN, at most 512 columns per CTA).
+// (448, 1) kernel without GEN, at most 448 columns per CTA).
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream, bool gen) {
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  if (!gen && precision <= 2 && threads > 512) return cudaErrorInvalidConfiguration;
+  if (!gen && precision <= 2 && threads > 448) return cudaErrorInvalidConfiguration;
   const void *k = kernel_ptr(precision, v, gen);
   if (!k) return cudaErrorInvalidValue;
   Fields fa = f;
@@ -376,11 +379,11 @@ cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int t
 
 // Launch form `precision` (0-2) of the single-precision interface with the
 // schedule of variant v: variant 0 keeps its (640, 1) kernel; every other
-// variant runs the (512, 1) kernel with at most 512 columns per CTA.
+// variant runs the (448, 1) kernel with at most 448 columns per CTA.
 cudaError_t launch_sp(int precision, int v, const FieldsSP &f, const Shape &sh, int threads, int grid,
                       cudaStream_t stream, bool gen) {
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  if ((v != 0 || !gen) && threads > 512) return cudaErrorInvalidConfiguration;
+  if ((v != 0 || !gen) && threads > 448) return cudaErrorInvalidConfiguration;
   const void *k = kernel_ptr_sp(precision, v, gen);
   if (!k) return cudaErrorInvalidValue;
   FieldsSP fa = f;
