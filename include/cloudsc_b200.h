@@ -547,7 +547,7 @@ size_t cloudsc_b200_params_size(void);
  * cloudsc_b200_set_schedule(): variant, columns per CTA (a multiple of 32 up
  * to the variant's max_threads) and ctas_per_sm, the persistent CTAs resident
  * per SM (0 = one CTA per tile of columns, a grid over all tiles).  Default:
- * the (512, 1) variant, 448 columns per CTA, ctas_per_sm 0.
+ * the (448, 1) variant, 448 columns per CTA, ctas_per_sm 0.
  * cloudsc_b200_set_launch(): the same with the variant chosen as the one-CTA-
  * per-SM variant with the most registers that holds threads_per_cta.
  * Return CLOUDSC_E_SHAPE for values outside these limits.
@@ -560,6 +560,21 @@ int cloudsc_b200_set_schedule(int32_t precision, int32_t variant, int32_t thread
 int cloudsc_b200_get_schedule(int32_t precision, int32_t *variant, int32_t *threads_per_cta,
                               int32_t *ctas_per_sm);
 int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t ctas_per_sm);
+
+/*
+ * Self-check of the division the column kernels use (no reference
+ * counterpart).  The kernels of forms 0-2 divide in double precision with a
+ * branch-free reciprocal-and-residual sequence that returns IEEE a/b exactly
+ * for 2^-256 <= |b| < 2^256 and a = 0 or 2^-256 <= |a| < 2^256, and records
+ * every operand outside that window; a column with such an operand is run
+ * again with IEEE division, so the kernels' results are those of IEEE
+ * division throughout.  This entry runs that division alone on n device
+ * operand pairs: q[i] = its quotient, bad[i] = 1 where an operand lies outside
+ * the window (0 otherwise).  Device pointers; stream may be NULL.
+ * CLOUDSC_E_SHAPE for n < 0, CLOUDSC_E_NULL for a NULL array with n > 0.
+ */
+int cloudsc_b200_division_check(const double *a, const double *b, int64_t n, double *q, int32_t *bad,
+                                void *stream);
 
 /* Last CUDA error string recorded by this library on the calling thread. */
 const char *cloudsc_b200_last_error(void);

@@ -61,14 +61,21 @@ def build(force=False, verbose=False):
     nvcc = _nvcc()
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s)[:-3] + ".o")
-        cmd = [nvcc] + ARCH + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", s, "-o", o]
+        cmds.append([nvcc] + ARCH + NVCC_FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", s, "-o", o])
+        objs.append(o)
+    # the translation units compile independently: one nvcc per source, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-        objs.append(o)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(run, cmds))
     tmp = LIB + ".tmp"
     # static CUDA runtime: the library does not depend on whichever libcudart
     # another component of the process (e.g. torch) brings along

@@ -82,6 +82,8 @@ def lib():
         L.cloudsc_b200_sltend_supersat_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
                                                            [vp] * len(SLTEND_FIELDS) + [vp])
         L.cloudsc_b200_sltend_supersat_batched.restype = ctypes.c_int
+        L.cloudsc_b200_division_check.argtypes = [vp, vp, ctypes.c_int64, vp, vp, vp]
+        L.cloudsc_b200_division_check.restype = ctypes.c_int
         L.cloudsc_b200_last_error.restype = ctypes.c_char_p
         L.cloudsc_b200_version.restype = ctypes.c_char_p
         L.cloudsc_b200_params_size.restype = ctypes.c_size_t
@@ -436,3 +438,20 @@ def satadj_increment_batched(params, arrays, nproma, klev, ngpblks, ngptot, ptsp
     f = lib().cloudsc_b200_satadj_increment_batched
     return _check(f(ctypes.byref(params), int(nproma), int(klev), int(ngpblks), int(ngptot), float(ptsphy),
                     *ptrs, int(KEY_ALL if keymask is None else keymask), cnt, st))
+
+
+def division_check(a, b, stream=None):
+    """The column kernels' division on the pairs of two equal-length float64
+    CUDA tensors: returns (q, bad), the quotients and an int32 flag, 1 where
+    an operand lies outside the division's exact window (the kernels then run
+    the column again with IEEE division).  Inside the window q equals IEEE
+    a / b bit for bit."""
+    import torch
+    if a.dtype != torch.float64 or b.dtype != torch.float64 or a.shape != b.shape or not a.is_cuda:
+        raise CloudscError(-2, "division_check wants two float64 CUDA tensors of one shape")
+    a, b = a.contiguous(), b.contiguous()
+    q = torch.empty_like(a)
+    bad = torch.empty(a.shape, dtype=torch.int32, device=a.device)
+    st = stream.cuda_stream if stream is not None else None
+    _check(lib().cloudsc_b200_division_check(_ptr(a), _ptr(b), a.numel(), _ptr(q), _ptr(bad), st))
+    return q, bad

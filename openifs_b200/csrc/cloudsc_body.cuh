@@ -14,6 +14,11 @@
 #define CSC_LEVEL_SYNC()
 #endif
 
+// Every division of the column code: fast_div when FAST_ (the fast pass),
+// recording in divbad_ the operands outside its exact window; IEEE division
+// otherwise (cdiv, cloudsc_column.cuh).
+#define DIV(...) cdiv<FAST_>(__VA_ARGS__, divbad_)
+
 namespace cloudsc {
 
 // ZSOLQA(a,b) of the reference ("+" is a source of a and a sink of b).  Every
@@ -56,12 +61,13 @@ CSC_DEV double sink_sum(int jo, const QA &q) {
   }
 #define SCL1(F, A) \
   if (F) A = A * zr;
-CSC_DEV void scale_row(int jo, QA &q, const double qx[5]) {
+template <bool FAST_>
+CSC_DEV void scale_row(int jo, QA &q, const double qx[5], DivCheck &divbad_) {
   const double zepsec = 1.E-14;
   const double ss = sink_sum(jo, q);
   const double zmm = mx(qx[jo], zepsec);
   if (!(ss > zmm)) return;
-  const double zr = zmm / ss;
+  const double zr = DIV(zmm, ss);
   switch (jo) {
     case L: {
       bool fLL = q.LL < 0.0, fLI = q.LI < 0.0, fLV = q.LV < 0.0;
@@ -89,45 +95,46 @@ CSC_DEV void scale_row(int jo, QA &q, const double qx[5]) {
 #undef SCL2
 
 // ZRATIO for every species from the current ZSOLQA (cloudsc.F90:3455-3474).
-CSC_DEV void sink_ratios(const QA &q, const double qx[5], double r[5]) {
+template <bool FAST_>
+CSC_DEV void sink_ratios(const QA &q, const double qx[5], double r[5], DivCheck &divbad_) {
   const double zepsec = 1.E-14;
 #pragma unroll
   for (int jm = 0; jm < 5; ++jm) {
     double zmax = mx(qx[jm], zepsec);
-    r[jm] = zmax / mx(sink_sum(jm, q), zmax);
+    r[jm] = DIV(zmax, mx(sink_sum(jm, q), zmax));
   }
 }
 
 // ---------------------------------------------------------------------------
 // CLOUD_SUPERSATCHECK (cloud_supersatcheck.F90:111-226, KFTLIQICE=1), double.
 // ---------------------------------------------------------------------------
-CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp,
-                                              double &t_adj, double &q_adj, double &a_adj,
-                                              double &l_adj, double &i_adj) {
+template <bool FAST_>
+CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp, double &t_adj, double &q_adj,
+                           double &a_adj, double &l_adj, double &i_adj, DivCheck &divbad_) {
   const KParamsD &k = c_kd;
   const double zepsec = 1.E-14;
   double zda = 0.0;
   double zt = mx(pt, 160.0);
   double za = mx(mn(pa, 1.0), 0.0);
-  double zp_r = 1.0 / pp;
-  double el = xexp(k.r3les * (zt - k.rtt) / (zt - k.r4les));
+  double zp_r = DIV(1.0, pp);
+  double el = xexp(DIV(k.r3les * (zt - k.rtt), (zt - k.r4les)));
   double x = (mx(k.rtice, mn(k.rtwat, zt)) - k.rtice) * k.rtwat_rtice_r;
   double alfa = mn(1.0, x * x);
   bool delta = copysign(1.0, zt - k.rtt) > 0.0;  // FOEDELTA = 1
   // computed whether or not a term needs it: without the branch the two
   // exponentials overlap (the same bits where it is used)
-  double ei = xexp(k.r3ies * (zt - k.rtt) / (zt - k.r4ies));
+  double ei = xexp(DIV(k.r3ies * (zt - k.rtt), (zt - k.r4ies)));
   double zfoeeliq = mn((k.r2es * el) * zp_r, 0.5);
   double foeew = delta ? k.r2es * el : k.r2es * ei;
   double zfoeeice = mn(foeew * zp_r, 0.5);
   double zfokoop = mn(zfoeeice * (k.rkoop1 - k.rkoop2 * zt), zfoeeliq);
-  double zqsliqk = zfokoop / (1.0 - k.retv * zfokoop);
+  double zqsliqk = DIV(zfokoop, (1.0 - k.retv * zfokoop));
   double wsum = (alfa < 1.0) ? alfa * el + (1.0 - alfa) * ei : el;
   double zfoeemix = mn((k.r2es * wsum) * zp_r, 0.5);
-  double zcor = 1.0 / (1.0 - k.retv * zfoeemix);
+  double zcor = DIV(1.0, (1.0 - k.retv * zfoeemix));
   double zqsmix = zfoeemix * zcor;
   double xl = zt - k.r4les, xi = zt - k.r4ies;
-  double foedem = alfa * k.r5alvcp * (1.0 / (xl * xl)) + (1.0 - alfa) * k.r5alscp * (1.0 / (xi * xi));
+  double foedem = alfa * k.r5alvcp * (DIV(1.0, (xl * xl))) + (1.0 - alfa) * k.r5alscp * (DIV(1.0, (xi * xi)));
   double zcorqsmix = 1.0 + zqsmix * zcor * foedem;
   zqsliqk = 0.5 * (zqsliqk + zqsmix);
   double zqslim = za * zqsmix + (1.0 - za) * zqsliqk;
@@ -137,7 +144,7 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp,
     zda = (1.0 - za) * zfaci;
     double za_upd = za + zda;
     zqslim = za_upd * zqsmix + (1.0 - za_upd) * zqsliqk;
-    zcond = (pq - zqslim) / zcorqsmix;
+    zcond = DIV((pq - zqslim), zcorqsmix);
   }
   double foeldcpm = alfa * k.ralvdcp + (1.0 - alfa) * k.ralsdcp;
   t_adj = foeldcpm * zcond;
@@ -318,12 +325,23 @@ CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double
 // tests for the exponents 0.5, 1.5, 2 and 3, which the host has ruled out
 // for the uploaded parameters (gen_exponents_ok); same results, fewer
 // branches.
-template <typename Real, bool F32M, bool BUD = false, bool OPT = false, typename FT = Fields, bool GEN = false>
-CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool active = true) {
+// PASS (kPassPlain, kPassFast, kPassRedo; cloudsc_column.cuh): the fast pass
+// divides with fast_div, sets *bad when an operand of one of its divisions
+// fell outside that division's exact window, and saves the PLUDE input of every level in
+// plude_in[0..KLEV-1]; the redo pass, the column run again with IEEE division,
+// reads PLUDE from plude_in.  A column whose fast pass sets *bad must be rerun
+// (its outputs, stored in the same places by both passes, are then final) and
+// leaves its warning count to the rerun.
+template <typename Real, bool F32M, bool BUD = false, bool OPT = false, typename FT = Fields, bool GEN = false,
+          int PASS = kPassPlain>
+CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool active = true, bool *bad = nullptr,
+                            double *plude_in = nullptr) {
   const KParams<Real> &P = KP<Real>();
   const KParamsD &PD = c_kd;
   typedef double D;
 #define C(x) Real(x)
+  constexpr bool FAST_ = PASS == kPassFast;
+  DivCheck divbad_;
   const int np = sh.nproma, klev = sh.klev;
   const size_t s2 = (size_t)np * klev, s2h = (size_t)np * (klev + 1);
   const size_t o2 = (size_t)ib * s2 + jl, o2h = (size_t)ib * s2h + jl, o1 = (size_t)ib * np + jl;
@@ -414,7 +432,15 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       pmfd_k1 = Real(ld(F.pmfd + ok + np));
       plu_k1 = Real(ld(F.plu + ok + np));
     }
-    D plude_k = F.plude[ok];
+    // PLUDE is read and written in place: the fast pass keeps each level's
+    // input for a rerun of the column, which reads it back from there
+    D plude_k;
+    if constexpr (PASS == kPassRedo) {
+      plude_k = plude_in[k];
+    } else {
+      plude_k = F.plude[ok];
+      if constexpr (PASS == kPassFast) plude_in[k] = plude_k;
+    }
     const Real pap_k = Real(pap_kd);
 
     // ---------------- first guess (:982-1002) ----------------
@@ -436,22 +462,22 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
     if (k >= ncldtop0) {
       Real x = (mx(P.rtice, mn(P.rtwat, t)) - P.rtice) * P.rtwat_rtice_r;
       alfa = mn(C(1.0), x * x);
-      el_e = mexp<F32M>(P.r3les * (t - P.rtt) / (t - P.r4les));
+      el_e = mexp<F32M>(DIV(P.r3les * (t - P.rtt), (t - P.r4les)));
       bool delta = xsign(C(1.0), t - P.rtt) > C(0.0);
       // the ice exponential whether or not a term needs it (no branch: the
       // two exponentials overlap)
-      ei_e = mexp<F32M>(P.r3ies * (t - P.rtt) / (t - P.r4ies));
+      ei_e = mexp<F32M>(DIV(P.r3ies * (t - P.rtt), (t - P.r4ies)));
       Real wsum = (alfa < C(1.0)) ? alfa * el_e + (C(1.0) - alfa) * ei_e : el_e;
-      zfoeewm = mn((P.r2es * wsum) / pap_k, C(0.5));
+      zfoeewm = mn(DIV((P.r2es * wsum), pap_k), C(0.5));
       zqsmix = zfoeewm;
-      zqsmix = zqsmix / (C(1.0) - P.retv * zqsmix);
+      zqsmix = DIV(zqsmix, (C(1.0) - P.retv * zqsmix));
       Real eew = delta ? P.r2es * el_e : P.r2es * ei_e;
-      zfoeew = mn(eew / pap_k, C(0.5));
+      zfoeew = mn(DIV(eew, pap_k), C(0.5));
       zfoeew = mn(C(0.5), zfoeew);
-      zqsice = zfoeew / (C(1.0) - P.retv * zfoeew);
-      zfoeeliqt = mn((P.r2es * el_e) / pap_k, C(0.5));
+      zqsice = DIV(zfoeew, (C(1.0) - P.retv * zfoeew));
+      zfoeeliqt = mn(DIV((P.r2es * el_e), pap_k), C(0.5));
       zqsliq = zfoeeliqt;
-      zqsliq = zqsliq / (C(1.0) - P.retv * zqsliq);
+      zqsliq = DIV(zqsliq, (C(1.0) - P.retv * zqsliq));
     }
 
     // ---------------- tidy up (:1127-1199), double ----------------
@@ -493,7 +519,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
     const Real zli = ql + qi;
     Real liqfrac = C(0.0), icefrac = C(0.0);
     if (zli > P.rlmin) {
-      liqfrac = ql / zli;
+      liqfrac = DIV(ql, zli);
       icefrac = C(1.0) - liqfrac;
     }
 
@@ -544,10 +570,10 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // derived variables (:1281-1324)
       const Real zdp = Real(paph_k1 - paph_k);
-      const Real zgdp = P.rg / zdp;
-      const Real zrho = pap_k / (P.rd * t);
+      const Real zgdp = DIV(P.rg, zdp);
+      const Real zrho = DIV(pap_k, (P.rd * t));
       // (RDENSREF/ZRHO)**0.4 appears in three processes: one shared logarithm
-      const PowBase b_dens = mbase<F32M>(P.rdensref / zrho);
+      const PowBase b_dens = mbase<F32M>(DIV(P.rdensref, zrho));
       // its two powers (0.4 in the rain fall speed, the binary32 0.4 in rain
       // evaporation and riming), computed here for every point so that they
       // overlap with the code around them instead of waiting inside their
@@ -559,22 +585,22 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       Real zcorqsliq, zcorqsice, zcorqsmix, zdqsmixdt, zevaplimmix;
       {
         Real xl = t - P.r4les, xi = t - P.r4ies;
-        Real zfacw = P.r5les / (xl * xl);
-        Real zcor = C(1.0) / (C(1.0) - P.retv * zfoeeliqt);
+        Real zfacw = DIV(P.r5les, (xl * xl));
+        Real zcor = DIV(C(1.0), (C(1.0) - P.retv * zfoeeliqt));
         Real zdqsliqdt = zfacw * zcor * zqsliq;
         zcorqsliq = C(1.0) + P.ralvdcp * zdqsliqdt;
-        Real zfaci = P.r5ies / (xi * xi);
-        zcor = C(1.0) / (C(1.0) - P.retv * zfoeew);
+        Real zfaci = DIV(P.r5ies, (xi * xi));
+        zcor = DIV(C(1.0), (C(1.0) - P.retv * zfoeew));
         Real zdqsicedt = zfaci * zcor * zqsice;
         zcorqsice = C(1.0) + P.ralsdcp * zdqsicedt;
         Real zfac = alfa * zfacw + (C(1.0) - alfa) * zfaci;
-        zcor = C(1.0) / (C(1.0) - P.retv * zfoeewm);
+        zcor = DIV(C(1.0), (C(1.0) - P.retv * zfoeewm));
         zdqsmixdt = zfac * zcor * zqsmix;
         Real foeldcpm = alfa * P.ralvdcp + (C(1.0) - alfa) * P.ralsdcp;
         zcorqsmix = C(1.0) + foeldcpm * zdqsmixdt;
-        zevaplimmix = mx((zqsmix - qv) / zcorqsmix, C(0.0));
+        zevaplimmix = mx(DIV((zqsmix - qv), zcorqsmix), C(0.0));
       }
-      const Real ztmpa = C(1.0) / mx(a, C(0.01));
+      const Real ztmpa = DIV(C(1.0), mx(a, C(0.01)));
       Real zliqcld = ql * ztmpa;
       Real zicecld = qi * ztmpa;
       const Real zlicld = zliqcld + zicecld;
@@ -591,7 +617,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       if (!last) {
         plude_k = plude_k * D(zdtgdp);
         if (ldcum && Real(plude_k) > zepsec && plu_k1 > zepsec) {
-          solac = solac + Real(plude_k) / plu_k1;
+          solac = solac + DIV(Real(plude_k), plu_k1);
           convsrce_l = Real(pludeli1) * zdtgdp;
           convsrce_i = Real(pludeli2) * zdtgdp;
           QADD(LL, convsrce_l);
@@ -599,7 +625,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           if constexpr (BUD) {  // :1378-1380
             bd.l[3] = convsrce_l * zqtmst;
             bd.i[3] = convsrce_i * zqtmst;
-            bd.cc[3] = zqtmst * plude_k / plu_k1;
+            bd.cc[3] = DIV(zqtmst * plude_k, plu_k1);
           }
         } else {
           plude_k = 0.0;
@@ -621,8 +647,8 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         Real lcust_i = zmf * qxnm1_i;
         convsrce_l = convsrce_l + lcust_l;
         convsrce_i = convsrce_i + lcust_i;
-        Real zdtdp = P.zrdcp * C(0.5) * (t_prev + t) / Real(paph_k);
-        Real zwtot = mn(P.rg * (pmfu_k * zadvw + pmfd_k * zadvwd), (pap_k - pap_prev) / rdt);
+        Real zdtdp = DIV(P.zrdcp * C(0.5) * (t_prev + t), Real(paph_k));
+        Real zwtot = mn(P.rg * (pmfu_k * zadvw + pmfd_k * zadvwd), DIV((pap_k - pap_prev), rdt));
         Real zdtforc = zdtdp * rdt * zwtot;
         Real zdqs = zanewm1 * zdtforc * zdqsmixdt;
         Real lfinalsum = C(0.0);
@@ -679,12 +705,12 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           zldifdt = C(2.0) * P.rcldiff_convi * zldifdt;
         }
         if (zli > zepsec) {
-          Real zqe = (qv - a * zqsmix) / mx(zepsec, C(1.0) - a);
+          Real zqe = DIV((qv - a * zqsmix), mx(zepsec, C(1.0) - a));
           Real ze = mx(zqsmix - zqe, C(0.0));
           Real zleros = C(0.333) * a * (C(1.) - a) * zldifdt * ze;
           zleros = mn(zleros, zevaplimmix);
           zleros = mn(zleros, zli);
-          Real zaeros = C(0.5) * zleros / zlicld;
+          Real zaeros = DIV(C(0.5) * zleros, zlicld);
           solac = solac - zaeros;
           QSUB(LV, liqfrac * zleros);  // (V,L) +=, (L,V) -=
           QSUB(IV, icefrac * zleros);  // (V,I) +=, (I,V) -=
@@ -705,7 +731,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         Real ztemp = C(0.5) * (qr + qxnm1_r);
         if (ztemp != C(0.0)) {
           Real zfallcorr = fallcorr_r;
-          Real zrlambda = mpowp<F32M, GEN>(zrho * ztemp / P.rcl_lam1r, P.rcl_lam2r);
+          Real zrlambda = mpowp<F32M, GEN>(DIV(zrho * ztemp, P.rcl_lam1r), P.rcl_lam2r);
           fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpowp<F32M, GEN>(zrlambda, P.rcl_dr);
         }
       }
@@ -731,13 +757,12 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       // 4.2 precipitation fraction (:1898-1919)
       Real zcovpclr, zraincld, zraincldm1, zsnowcld;
       if (qpretot > zepsec) {
-        zcovptot = C(1.0) - ((C(1.0) - zcovptot) * (C(1.0) - mx(a, za_prev)) /
-                             (C(1.0) - mn(za_prev, C(1.0) - C(1.E-06))));
+        zcovptot = C(1.0) - (DIV((C(1.0) - zcovptot) * (C(1.0) - mx(a, za_prev)), (C(1.0) - mn(za_prev, C(1.0) - C(1.E-06)))));
         zcovptot = mx(zcovptot, P.rcovpmin);
         zcovpclr = mx(C(0.0), zcovptot - a);
-        zraincld = C(0.5) * (qr + qr_prev) / zcovptot;
-        zraincldm1 = C(0.5) * (qr + qxnm1_r) / zcovptot;
-        zsnowcld = C(0.5) * (qs + qs_prev) / zcovptot;
+        zraincld = DIV(C(0.5) * (qr + qr_prev), zcovptot);
+        zraincldm1 = DIV(C(0.5) * (qr + qxnm1_r), zcovptot);
+        zsnowcld = DIV(C(0.5) * (qs + qs_prev), zcovptot);
         zcovpmax = mx(zcovptot, zcovpmax);
       } else {
         zraincld = C(0.0);
@@ -761,7 +786,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
             const double zphip2 = zphip1 - 0.2;
             const double zphip3 = 0.123 * xexp(-zphip1 * 0.55);
             const double zanew2 = mx(double(a), 0.1);
-            const double zphic = xpow(zgridlen * zanew2, 1.0 / 3.0) *
+            const double zphic = xpow(zgridlen * zanew2, DIV(1.0, 3.0)) *
                                  xpow(xpow(zphip3 * zgridlen * zanew2, 1.5) + 3.0 * zphip3, -0.17);
             double zfracsdc = (zphip1 - zphip2 * zanew2) * zphic;
             if (double(a) > 0.95) zfracsdc = 0.17 * zphic;
@@ -770,13 +795,13 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           if (P.lcloud_inhomog) {  // :2075-2098
             const double aa = double(a);
             const double fc2 = xpow(lfsd, 2.0);
-            const double zea = xpow(1.0 + fc2, (double(P.rcl_kkbauq) - 1.0) * double(P.rcl_kkbauq) / 2.0);
-            const double zphir = xpow(zgridlen * aa, 1.0 / 3.0) * xpow(xpow(0.11 * zgridlen * aa, 1.14) + 1.0, -0.22);
+            const double zea = xpow(1.0 + fc2, DIV((double(P.rcl_kkbauq) - 1.0) * double(P.rcl_kkbauq), 2.0));
+            const double zphir = xpow(zgridlen * aa, DIV(1.0, 3.0)) * xpow(xpow(0.11 * zgridlen * aa, 1.14) + 1.0, -0.22);
             double zfracsdr = (1.1 - 0.8 * aa) * zphir;
             if (aa > 0.95) zfracsdr = 0.3 * zphir;
             const double fr2 = xpow(zfracsdr, 2.0);
             const double kb = double(P.rcl_kkbac);
-            const double zec = xpow(1.0 + fc2, (kb - 1.0) * kb / 2.0) * xpow(1.0 + fr2, (kb - 1.0) * kb / 2.0) *
+            const double zec = xpow(1.0 + fc2, DIV((kb - 1.0) * kb, 2.0)) * xpow(1.0 + fr2, DIV((kb - 1.0) * kb, 2.0)) *
                                xexp(zcldraincorr * kb * kb * xsqrt(xlog(1.0 + fc2) * xlog(1.0 + fr2)));
             zeaut = Real(zea);
             zeacc = Real(zec);
@@ -802,7 +827,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // 4.4 rain evaporation (:2271-2378)
       {
-        Real zzrh = P.rprecrhmax + (C(1.0) - P.rprecrhmax) * zcovpmax / mx(zepsec, C(1.0) - a);
+        Real zzrh = P.rprecrhmax + DIV((C(1.0) - P.rprecrhmax) * zcovpmax, mx(zepsec, C(1.0) - a));
         zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
         Real zxramid = P.ramid;
         if (spp && P.spp_on[CLOUDSC_SPP_RAMID]) {  // :2282-2287
@@ -810,9 +835,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           if (P.spp_lramidlimit1) zxramid = mn(C(1.0), zxramid);
         }
         Real zrhc = zxramid;
-        Real zsigk = pap_k / Real(paph_surf);
+        Real zsigk = DIV(pap_k, Real(paph_surf));
         if (zsigk > C(0.8)) {
-          Real s = (zsigk - C(0.8)) / C(0.2);
+          Real s = DIV((zsigk - C(0.8)), C(0.2));
           zrhc = zxramid + (C(1.0) - zxramid) * (s * s);
         }
         zzrh = mn(zrhc, zzrh);
@@ -821,19 +846,18 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (zcovpclr > zepsec && zraincldm1 > zepsec && zqe < zzrh * zqsliq) {
           Real zpreclr = zraincldm1;
           Real zfallcorr = fallcorr_f;
-          Real zesatliq = P.rv / P.rd * (P.r2es * el_e);
-          Real zlambda = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * zpreclr), P.rcl_lam2r);
+          Real zesatliq = DIV(P.rv, P.rd) * (P.r2es * el_e);
+          Real zlambda = mpowp<F32M, GEN>(DIV(P.rcl_lam1r, (zrho * zpreclr)), P.rcl_lam2r);
           const PowBase b_lam = mbase<F32M>(zlambda);
           Real zevap_denom = P.rcl_cdenom1 * zesatliq - P.rcl_cdenom2 * t * zesatliq +
                              P.rcl_cdenom3 * mpow<F32M>(t, C(3.0)) * pap_k;
-          Real zcorr2 = mpow<F32M>(t / C(273.), C(1.5)) * C(393.) / (t + C(120.));
+          Real zcorr2 = DIV(mpow<F32M>(DIV(t, C(273.)), C(1.5)) * C(393.), (t + C(120.)));
           Real zsubsat = mx(zzrh * zqsliq - zqe, C(0.0));
-          Real zbeta = (C(0.15) / zqsliq) * (t * t) * zesatliq * P.rcl_const1r * (zcorr2 / zevap_denom) *
-                       (C(0.78) / (mpowbp<F32M, GEN>(b_lam, P.rcl_const4r)) +
-                        P.rcl_const2r * mpow<F32M>(zrho * zfallcorr, C(0.5)) /
-                            (mpow<F32M>(zcorr2, C(0.5)) * mpowbp<F32M, GEN>(b_lam, P.rcl_const3r)));
+          Real zbeta = (DIV(C(0.15), zqsliq)) * (t * t) * zesatliq * P.rcl_const1r * (DIV(zcorr2, zevap_denom)) *
+                       (DIV(C(0.78), (mpowbp<F32M, GEN>(b_lam, P.rcl_const4r))) +
+                        DIV(P.rcl_const2r * mpow<F32M>(zrho * zfallcorr, C(0.5)), (mpow<F32M>(zcorr2, C(0.5)) * mpowbp<F32M, GEN>(b_lam, P.rcl_const3r))));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsliq;
-          Real zdpevap = zcovpclr * zbeta * rdt * zsubsat / zdenom;
+          Real zdpevap = DIV(zcovpclr * zbeta * rdt * zsubsat, zdenom);
           if (spp && P.spp_on[CLOUDSC_SPP_RAINEVAP]) zdpevap = zdpevap * Real(sppf[CLOUDSC_SPP_RAINEVAP]);
           D zevap = mn(D(zdpevap), qxfg_r);
           QSUB(RV, zevap);  // (V,R) += zevap, (R,V) -= zevap
@@ -847,22 +871,22 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (za_prev < P.rcldtopcf && a >= P.rcldtopcf) {
           zcldtopdist = C(0.0);
         } else {
-          zcldtopdist = zcldtopdist + zdp / (zrho * P.rg);
+          zcldtopdist = zcldtopdist + DIV(zdp, (zrho * P.rg));
         }
         if (t < (P.rtt - C(5.)) && qxfg_l > P.rlmin) {
-          Real zsupersatice = (zqsliq - zqsice) / zqsice;
-          Real zvpice = (P.r2es * ei_e) * P.rv / P.rd;
+          Real zsupersatice = DIV((zqsliq - zqsice), zqsice);
+          Real zvpice = DIV((P.r2es * ei_e) * P.rv, P.rd);
           Real zicenuclei = C(1000.0) * mexp<F32M>(C(12.96) * zsupersatice - C(0.639));
-          Real zadd = P.rlstt * (P.rlstt / (P.rv * t) - C(1.0)) / (C(2.4E-2) * t);
-          Real zbdd = P.rv * t * pap_k / (C(2.21) * zvpice);
-          Real zcvds = C(7.8) * mpow<F32M>(zicenuclei / zrho, C(0.666)) * zsupersatice / (C(8.87) * (zadd + zbdd));
-          Real zice0 = mx(zicecld, zicenuclei * P.riceinit / zrho);
+          Real zadd = DIV(P.rlstt * (DIV(P.rlstt, (P.rv * t)) - C(1.0)), (C(2.4E-2) * t));
+          Real zbdd = DIV(P.rv * t * pap_k, (C(2.21) * zvpice));
+          Real zcvds = DIV(C(7.8) * mpow<F32M>(DIV(zicenuclei, zrho), C(0.666)) * zsupersatice, (C(8.87) * (zadd + zbdd)));
+          Real zice0 = mx(zicecld, DIV(zicenuclei * P.riceinit, zrho));
           Real zinew = mpow<F32M>(C(0.666) * zcvds * rdt + mpow<F32M>(zice0, C(0.666)), C(1.5));
           D zdepos = D(mx(P.rcl_overlapliqice * a * (zinew - zice0), C(0.0)));
           zdepos = mn(zdepos, qxfg_l);
-          Real zinfactor = mn(zicenuclei / C(15000.), C(1.0));
+          Real zinfactor = mn(DIV(zicenuclei, C(15000.)), C(1.0));
           zdepos = zdepos * D(mn(zinfactor + (C(1.0) - zinfactor) *
-                                               (P.rdepliqrefrate + zcldtopdist / P.rdepliqrefdepth),
+                                               (P.rdepliqrefrate + DIV(zcldtopdist, P.rdepliqrefdepth)),
                                C(1.0)));
           QSUB(LI, zdepos);  // (I,L) += zdepos, (L,I) -= zdepos
           qxfg_i = qxfg_i + zdepos;
@@ -876,20 +900,20 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // 4.7 snow deposition, IDEPSNOW=1 (:2698-2745)
       {
-        Real zsupersatice = mx((qv - zqsmix) / zqsmix, C(0.0));
+        Real zsupersatice = mx(DIV((qv - zqsmix), zqsmix), C(0.0));
         if (t < P.rtt && zsnowcld > zepsec && zsupersatice > C(0.0)) {
-          Real zvpice = (P.r2es * ei_e) * P.rv / P.rd;
+          Real zvpice = DIV((P.r2es * ei_e) * P.rv, P.rd);
           Real zaplusb = P.rcl_apb1 * zvpice - P.rcl_apb2 * zvpice * t + pap_k * P.rcl_apb3 * (t * t * t);
-          Real zcorrfac = mpow<F32M>(C(1.0) / zrho, C(0.5));
-          Real zcorrfac2 = (mpow<F32M>(t / C(273.0), C(1.5))) * (C(393.0) / (t + C(120.0)));
+          Real zcorrfac = mpow<F32M>(DIV(C(1.0), zrho), C(0.5));
+          Real zcorrfac2 = (mpow<F32M>(DIV(t, C(273.0)), C(1.5))) * (DIV(C(393.0), (t + C(120.0))));
           Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
           const PowBase b_pr02 = mbase<F32M>(zpr02);
-          Real zterm1 = zsupersatice * (t * t) * zvpice * zcorrfac2 * P.rcl_const2s / (zrho * zaplusb);
+          Real zterm1 = DIV(zsupersatice * (t * t) * zvpice * zcorrfac2 * P.rcl_const2s, (zrho * zaplusb));
           Real zterm2 = C(0.65) * P.rcl_const6s * mpowbp<F32M, GEN>(b_pr02, P.rcl_const4s) +
-                        P.rcl_const3s * mpow<F32M>(zcorrfac, C(0.5)) * mpow<F32M>(zrho, C(0.5)) *
-                            mpowbp<F32M, GEN>(b_pr02, P.rcl_const5s) / mpow<F32M>(zcorrfac2, C(0.5));
+                        DIV(P.rcl_const3s * mpow<F32M>(zcorrfac, C(0.5)) * mpow<F32M>(zrho, C(0.5)) *
+                            mpowbp<F32M, GEN>(b_pr02, P.rcl_const5s), mpow<F32M>(zcorrfac2, C(0.5)));
           Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
-          zpsdep = mn(zpsdep, qv - zqsmix) / zcorqsmix;
+          zpsdep = DIV(mn(zpsdep, qv - zqsmix), zcorqsmix);
           QADD(SV, zpsdep);  // (S,V) += zpsdep, (V,S) -= zpsdep
           if constexpr (BUD) b_psdep = zpsdep;
         }
@@ -904,7 +928,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         Real zzco = rdt * P.rsnowlin1 * mexp<F32M>(P.rsnowlin2 * (t - P.rtt));
         Real zlcrit = P.rlcritsnow;
         if (spp && P.spp_on[CLOUDSC_SPP_RLCRITSNOW]) zlcrit = P.rlcritsnow * Real(sppf[CLOUDSC_SPP_RLCRITSNOW]);
-        Real r = zicecld / zlcrit;
+        Real r = DIV(zicecld, zlcrit);
         Real ztemp = C(-1.) * (r * r);
         Real zsnowaut = (ztemp < C(50.0)) ? zzco * (C(1.0) - mexp<F32M>(ztemp)) : zzco;
         qb_si = qb_si + zsnowaut;
@@ -919,11 +943,11 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           Real zsubsat = mx(zqsice - qv, C(0.0));
           Real ztdmtw0 = t - P.rtt -
                          zsubsat * (C(1329.31) + C(0.0074615) * (pap_k - C(0.85E5)) - C(40.637) * (t - C(275.0)));
-          Real zcons1 = xabs(rdt * (C(1.0) + C(0.5) * ztdmtw0) / P.rtaumel);
+          Real zcons1 = xabs(DIV(rdt * (C(1.0) + C(0.5) * ztdmtw0), P.rtaumel));
           zmeltmax = mx(ztdmtw0 * zcons1 * P.zrldcp, C(0.0));
         }
         if (zmeltmax > zepsec && zicetot > zepsec) {
-          D zalfa = qxfg_i / zicetot;
+          D zalfa = DIV(qxfg_i, zicetot);
           D zmelt = mn(qxfg_i, zalfa * D(zmeltmax));
           qxfg_i = qxfg_i - zmelt;
           qxfg_r = qxfg_r + zmelt;
@@ -932,7 +956,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
             bd.i[15] = -zmelt * zqtmst;
             bd.l[17] = zmelt * zqtmst;
           }
-          zalfa = qxfg_s / zicetot;
+          zalfa = DIV(qxfg_s, zicetot);
           zmelt = mn(qxfg_s, zalfa * D(zmeltmax));
           qxfg_s = qxfg_s - zmelt;
           qxfg_r = qxfg_r + zmelt;
@@ -945,18 +969,18 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       if (qr > zepsec) {
         if (t <= P.rtt && t_prev > P.rtt) {
           Real zqpre = mx(qs + qr, zepsec);
-          prainfrac = qr / zqpre;
+          prainfrac = DIV(qr, zqpre);
           llrainliq = prainfrac > P.flt_0p8;
         }
         if (t < P.rtt) {
           Real zfrzmax;
           if (llrainliq) {
-            Real zlambda = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * qr), P.rcl_lam2r);
+            Real zlambda = mpowp<F32M, GEN>(DIV(P.rcl_lam1r, (zrho * qr)), P.rcl_lam2r);
             Real ztemp = mn(P.rcl_fzrab * (t - P.rtt), C(50.));
-            Real zfrz = rdt * (P.rcl_const5r / zrho) * (mexp<F32M>(ztemp) - C(1.)) * mpowp<F32M, GEN>(zlambda, P.rcl_const6r);
+            Real zfrz = rdt * (DIV(P.rcl_const5r, zrho)) * (mexp<F32M>(ztemp) - C(1.)) * mpowp<F32M, GEN>(zlambda, P.rcl_const6r);
             zfrzmax = mx(zfrz, C(0.0));
           } else {
-            Real zcons1 = xabs(rdt * (C(1.0) + C(0.5) * (P.rtt - t)) / P.rtaumel);
+            Real zcons1 = xabs(DIV(rdt * (C(1.0) + C(0.5) * (P.rtt - t)), P.rtaumel));
             zfrzmax = mx((P.rtt - t) * zcons1 * P.zrldcp, C(0.0));
           }
           if (zfrzmax > zepsec) {
@@ -989,28 +1013,28 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // PSD slopes (:3026-3069), PSACR (:3084-3115), PIACR (:3171-3198)
       if (t <= P.rtt && prainfrac < zepsec && zraincld > zepsec) {
-        Real zlamr = mpowp<F32M, GEN>(P.rcl_lam1r / (zrho * zraincld), P.rcl_lam2r);
+        Real zlamr = mpowp<F32M, GEN>(DIV(P.rcl_lam1r, (zrho * zraincld)), P.rcl_lam2r);
         Real zn0r = P.rcl_x1r * mpowp<F32M, GEN>(zlamr, P.rcl_x2r);
         Real zlamr3 = zlamr * zlamr * zlamr;
         if (zsnowcld > zepsec) {
-          Real zlams = mpowp<F32M, GEN>(P.rcl_lam1s / (zrho * zsnowcld), P.rcl_lam2s);
+          Real zlams = mpowp<F32M, GEN>(DIV(P.rcl_lam1s, (zrho * zsnowcld)), P.rcl_lam2s);
           Real zn0s = P.rcl_x1s;
-          Real zfalldiff = mx(xabs(fs_r - fs_s), (fs_r + fs_s) / C(8.));
-          Real zfac = P.rpi * P.rpi * P.rdenswat * zrho * zn0r * zn0s / (zlams * zlamr3);
-          Real zrat = zlamr / zlams;
+          Real zfalldiff = mx(xabs(fs_r - fs_s), DIV((fs_r + fs_s), C(8.)));
+          Real zfac = DIV(P.rpi * P.rpi * P.rdenswat * zrho * zn0r * zn0s, (zlams * zlamr3));
+          Real zrat = DIV(zlamr, zlams);
           Real zpsacr =
-              zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
+              DIV(zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)), zlamr3);
           QSUB(RS, zpsacr);  // (S,R) += zpsacr, (R,S) -= zpsacr
           if constexpr (BUD) b_psacr = zpsacr;
         }
         if (zicecld > zepsec) {
-          Real zlami = mpowp<F32M, GEN>(P.rcl_lam1s / (zrho * zicecld), P.rcl_lam2s);
+          Real zlami = mpowp<F32M, GEN>(DIV(P.rcl_lam1s, (zrho * zicecld)), P.rcl_lam2s);
           Real zn0i = P.rcl_x1s;
-          Real zfalldiff = mx(xabs(fs_r - fs_i), (fs_r + fs_i) / C(8.));
-          Real zfac = P.rpi * P.rpi * P.rdenswat * C(0.1) * zrho * zn0r * zn0i / (zlami * zlamr3);
-          Real zrat = zlamr / zlami;
+          Real zfalldiff = mx(xabs(fs_r - fs_i), DIV((fs_r + fs_i), C(8.)));
+          Real zfac = DIV(P.rpi * P.rpi * P.rdenswat * C(0.1) * zrho * zn0r * zn0i, (zlami * zlamr3));
+          Real zrat = DIV(zlamr, zlami);
           Real zpiacr =
-              zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)) / zlamr3;
+              DIV(zcovptot * rdt * zfac * zfalldiff * ((C(0.5) * zrat + C(2.)) * zrat + C(5.)), zlamr3);
           QADD(IR, zpiacr);  // (I,R) += zpiacr, (R,I) -= zpiacr
           if constexpr (BUD) b_piacr = zpiacr;
         }
@@ -1018,23 +1042,23 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // 4.15 snow sublimation, ISUBLSNOW=1 (:3254-3318)
       {
-        Real zzrh = P.rprecrhmax + (C(1.0) - P.rprecrhmax) * zcovpmax / mx(zepsec, C(1.0) - a);
+        Real zzrh = P.rprecrhmax + DIV((C(1.0) - P.rprecrhmax) * zcovpmax, mx(zepsec, C(1.0) - a));
         zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
-        Real zqe = (qv - a * zqsice) / mx(zepsec, C(1.0) - a);
+        Real zqe = DIV((qv - a * zqsice), mx(zepsec, C(1.0) - a));
         zqe = mx(C(0.0), mn(zqe, zqsice));
         if (zcovpclr > zepsec && qxfg_s > zepsec && zqe < zzrh * zqsice) {
           Real aa = zcovptot * zdtgdp;
-          Real zpreclr = Real(qxfg_s) * zcovpclr / xsign(mx(xabs(aa), zepsilon), aa);
-          Real zbeta1 = xsqrt(pap_k / Real(paph_surf)) / P.rvrfactor * zpreclr / mx(zcovpclr, zepsec);
+          Real zpreclr = DIV(Real(qxfg_s) * zcovpclr, xsign(mx(xabs(aa), zepsilon), aa));
+          Real zbeta1 = DIV(DIV(xsqrt(DIV(pap_k, Real(paph_surf))), P.rvrfactor) * zpreclr, mx(zcovpclr, zepsec));
           Real zbeta = P.rg * P.rpecons * mpow<F32M>(zbeta1, C(0.5777));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsice;
-          Real zdpr = zcovpclr * zbeta * (zqsice - zqe) / zdenom * zdp * P.zrg_r;
+          Real zdpr = DIV(zcovpclr * zbeta * (zqsice - zqe), zdenom) * zdp * P.zrg_r;
           Real zdpevap = zdpr * zdtgdp;
           if (spp && P.spp_on[CLOUDSC_SPP_SNOWSUBLIM]) zdpevap = zdpevap * Real(sppf[CLOUDSC_SPP_SNOWSUBLIM]);
           D zevap = mn(D(zdpevap), qxfg_s);
           QSUB(SV, zevap);  // (V,S) += zevap, (S,V) -= zevap
           if constexpr (BUD) bd.i[17] = -zevap * zqtmst;  // :3304
-          zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), Real(D(zcovptot - a) * zevap / qxfg_s)));
+          zcovptot = mx(P.rcovpmin, zcovptot - mx(C(0.0), Real(DIV(D(zcovptot - a) * zevap, qxfg_s))));
           qxfg_s = qxfg_s - zevap;
         }
       }
@@ -1049,7 +1073,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       // 5.1 cloud cover (:3429-3438)
       D zda;
       {
-        Real zanew = (a + solac) / (C(1.0) + solab);
+        Real zanew = DIV((a + solac), (C(1.0) + solab));
         zanew = mn(zanew, C(1.0));
         if (zanew < P.ramin) zanew = C(0.0);
         zda = D(zanew) - aorig;
@@ -1061,7 +1085,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       const double qx[5] = {qlD, qiD, qrD, qsD, qvD};
       {
         double ratio[5];
-        sink_ratios(q, qx, ratio);
+        sink_ratios<FAST_>(q, qx, ratio, divbad_);
         double sr[5];
         int ord[5];
         sr[0] = ratio[0];
@@ -1093,7 +1117,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 #pragma unroll
         for (int jm = 0; jm < 5; ++jm) code |= (unsigned)ord[jm] << (3 * jm);
 #pragma unroll 1
-        for (int jm = 0; jm < 5; ++jm) scale_row((int)((code >> (3 * jm)) & 7u), q, qx);
+        for (int jm = 0; jm < 5; ++jm) scale_row<FAST_>((int)((code >> (3 * jm)) & 7u), q, qx, divbad_);
       }
 
       // 5.2.2 solve (:3546-3628), double, lower-triangular form
@@ -1108,16 +1132,16 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         const double d_i = ((1.0 + double(fallsink_i)) + double(qb_ii)) + double(qb_si);
         const double d_r = 1.0 + double(fallsink_r);
         const double d_s = 1.0 + double(fallsink_s);
-        const double m_rl = (-double(qb_rl)) / d_l;
-        const double m_sl = (-double(qb_sl)) / d_l;
-        const double m_si = (-double(qb_si)) / d_i;
+        const double m_rl = DIV((-double(qb_rl)), d_l);
+        const double m_sl = DIV((-double(qb_sl)), d_l);
+        const double m_si = DIV((-double(qb_si)), d_i);
         x_r = x_r - m_rl * x_l;
         x_s = x_s - m_sl * x_l;
         x_s = x_s - m_si * x_i;
-        x_s = x_s / d_s;
-        x_r = x_r / d_r;
-        x_i = x_i / d_i;
-        x_l = x_l / d_l;
+        x_s = DIV(x_s, d_s);
+        x_r = DIV(x_r, d_r);
+        x_i = DIV(x_i, d_i);
+        x_l = DIV(x_l, d_l);
         // clip (:3633-3640)
         if (x_l < zepsecd) { x_v = x_v + x_l; x_l = 0.0; }
         if (x_i < zepsecd) { x_v = x_v + x_i; x_i = 0.0; }
@@ -1171,7 +1195,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         D t_upd = pt_k + dt * (loc_t + cml_t);
         D a_upd = pa_k + dt * (loc_a + cml_a);
         D t_adj, q_adj, a_adj, l_adj, i_adj;
-        supersatcheck(t_upd, q_upd, a_upd, pap_kd, t_adj, q_adj, a_adj, l_adj, i_adj);
+        supersatcheck<FAST_>(t_upd, q_upd, a_upd, pap_kd, t_adj, q_adj, a_adj, l_adj, i_adj, divbad_);
         loc_q = loc_q + q_adj * zqtmst;
         loc_t = loc_t + t_adj * zqtmst;
         loc_a = loc_a + a_adj * zqtmst;
@@ -1203,7 +1227,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           const double pda = pa_k + zda;  // :3819-3823
           if (pda > 0.001) anewp = mx(mx(pda, double(covp_out)), 0.1);
           if (q0_l + q0_i + plude_k > double(P.rlmin)) {  // :4112-4125
-            ratfsd = plude_k / (plude_k + q0_l + q0_i);
+            ratfsd = DIV(plude_k, (plude_k + q0_l + q0_i));
             ratfsd = mx(0.0, mn(1.0, ratfsd));
           }
           icef = x_i;
@@ -1227,12 +1251,12 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
     // literals written as such at :4316,4321-4322 are their float values
     if constexpr (OPT) {
       if (P.lrad_cloud_inhomog) {
-        const double zifsdback = 0.446585 * xpow(zgridlen, 1.0 / 3.0) * xpow(xpow(0.308061 * zgridlen, 0.395736) + 1.0, -0.744527);
+        const double zifsdback = 0.446585 * xpow(zgridlen, DIV(1.0, 3.0)) * xpow(xpow(0.308061 * zgridlen, 0.395736) + 1.0, -0.744527);
         const double zqtot = mx(mn((qvD + qiD) * 1000.0, 30.0), double(0.00001f));
-        const double zrho_f = pap_kd / (double(P.rd) * tD);
-        double zdelz = 1.0 / (double(P.rg) * zrho_f) * (paph_k1 - paph_k) * 0.001;
+        const double zrho_f = DIV(pap_kd, (double(P.rd) * tD));
+        double zdelz = DIV(1.0, (double(P.rg) * zrho_f)) * (paph_k1 - paph_k) * 0.001;
         zdelz = mx(mn(zdelz, double(0.5f)), double(0.001f));
-        const double zphi = xpow(zdelz / double(0.24f), double(0.11f)) * xpow(zqtot / double(10.f), double(0.03f));
+        const double zphi = xpow(DIV(zdelz, double(0.24f)), double(0.11f)) * xpow(DIV(zqtot, double(10.f)), double(0.03f));
         double zifsd = double(P.rcloud_frac_std);
         if (anewp > 0.95) {
           zifsd = zifsdback * zphi;
@@ -1326,8 +1350,11 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
     }
   }
   if (active) F.prainfrac_toprfz[o1] = D(prainfrac);
-  if (active && nwarn && F.ncounters) atomic_add(F.ncounters, nwarn);
+  if (active && nwarn && F.ncounters && !(FAST_ && divbad_.bad())) atomic_add(F.ncounters, nwarn);
+  if constexpr (FAST_) *bad = active && divbad_.bad();
 #undef C
 }
+
+#undef DIV
 
 }  // namespace cloudsc

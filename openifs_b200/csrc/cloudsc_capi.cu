@@ -34,6 +34,8 @@ bool params_allow_gen(const cloudsc_params &p, const Derived &d);
 cudaError_t launch_satadj(const SatadjFields &f, const Shape &sh, cudaStream_t stream);
 cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaStream_t stream);
 cudaError_t launch_state_increment(const IncFields &f, const Shape &sh, cudaStream_t stream);
+cudaError_t launch_division_check(const double *a, const double *b, long long n, double *q, int *bad,
+                                  cudaStream_t stream);
 cudaError_t launch_sp(int precision, int v, const FieldsSP &f, const Shape &sh, int threads, int grid,
                       cudaStream_t stream, bool gen);
 }  // namespace cloudsc
@@ -507,9 +509,10 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
                                          "cloudsc_b200_batched_diag or cloudsc_b200_block");
     form = bud && opt ? 5 : (opt ? 4 : 3);
   }
-  // parameters that rule out the GEN kernels: forms 0-2 run the (448, 1)
-  // kernel without GEN, at most 448 columns per CTA
-  const int threads = (!gen && form <= 2 && sc.threads > 448) ? 448 : sc.threads;
+  // parameters that rule out the GEN kernels, and more than kMaxLevFast
+  // levels: forms 0-2 run a (448, 1) kernel, at most 448 columns per CTA
+  const bool small = !gen || sh.klev > kMaxLevFast;
+  const int threads = (small && form <= 2 && sc.threads > 448) ? 448 : sc.threads;
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
   cudaError_t e = launch(form, sc.variant, f, sh, threads, grid, stream, gen);
@@ -830,7 +833,7 @@ int launch_sp_checked(int precision, const FieldsSP &f, const Shape &sh, cudaStr
     gen = g_gen;
   }
   int threads = sc.threads;
-  if ((sc.variant != 0 || !gen) && threads > 448) threads = 448;
+  if ((sc.variant != 0 || !gen || sh.klev > kMaxLevFast) && threads > 448) threads = 448;
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
   cudaError_t e = launch_sp(precision, sc.variant, f, sh, threads, grid, stream, gen);
@@ -1487,6 +1490,16 @@ int cloudsc_b200_satadj_increment_batched(
   f.inc_i = (keymask & CLOUDSC_KEY_QI) ? ptendency_cml_i : nullptr;
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
   cudaError_t e = launch_satadj(f, sh, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+int cloudsc_b200_division_check(const double *a, const double *b, int64_t n, double *q, int32_t *bad,
+                                void *stream) {
+  if (n < 0) return fail(CLOUDSC_E_SHAPE, "n < 0");
+  if (n == 0) return CLOUDSC_OK;
+  if (!a || !b || !q || !bad) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  cudaError_t e = launch_division_check(a, b, (long long)n, q, bad, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
   return CLOUDSC_OK;
 }

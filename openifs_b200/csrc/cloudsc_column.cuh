@@ -42,6 +42,8 @@
 // result: with an FP32 state the scheme's thresholds and MIN() limiters flip
 // (a measured 5-7 % RMS error on the T tendency).
 #pragma once
+#include <type_traits>
+
 #include "cloudsc_common.cuh"
 #include "plibm.h"
 
@@ -55,6 +57,91 @@ template <typename T>
 CSC_DEV T mn(T a, T b) { return a < b ? a : b; }
 template <typename T>
 CSC_DEV T mx(T a, T b) { return a > b ? a : b; }
+
+// What the fast division reports, accumulated over every division of a
+// column.  acc ORs, for each dividend a and divisor b, the offsets
+// (2 * hi(x)) - kDivBase, whose top bits are clear exactly when x's biased
+// exponent lies in [767, 1278], i.e. 2^-256 <= |x| < 2^256 (a zero dividend
+// adds 0).  bad(): some operand left that window.
+constexpr unsigned kDivBase = 767u << 21, kDivRange = 1u << 30;
+struct DivCheck {
+  unsigned acc = 0u;
+  CSC_DEV bool bad() const { return acc >= kDivRange; }
+};
+
+// Branch-free double division for the column code.  A reciprocal estimate
+// (rcp.approx.ftz.f64) is refined by three Newton-Raphson steps
+// y <- y + y(1 - by), each error term and update one fused multiply-add; the
+// last step returns y = RN(1/b), the correctly rounded reciprocal, for every
+// divisor whose significand is not all ones (Markstein, IBM J. Res. Dev.
+// 34(1), 1990; Muller et al., Handbook of Floating-Point Arithmetic, ch. 5).
+// For b = (2 - 2^-52) 2^E the step ends on the tie 2^(-E-1) while
+// 1/b = 2^(-E-1) (1 + 2^-53 + 2^-106 + ...): the low significand bit of y is
+// then set, which gives RN(1/b) = 2^(-E-1) (1 + 2^-52).  The quotient of |a|,
+// q0 = RN(|a| y), within 1.5 ulp of |a|/b, is corrected twice with its
+// residual, q <- RN(q + RN(|a| - b q) y): the first correction brings it
+// within one ulp, where the residual is exact, and by Markstein's theorem the
+// second then returns RN(|a|/b).  The sign of a is put back by flipping the
+// sign bit, so that the result equals IEEE a/b bit for bit, zeros included,
+// when no step under- or overflows: that holds for 2^-256 <= |b| < 2^256 and
+// a = 0 or 2^-256 <= |a| < 2^256 (the quotient and every residual then stay
+// normal).  Operands outside that window (zeros, subnormals, infinities and
+// NaNs among them, a zero dividend excepted) are recorded in dc, and a column
+// with any is rerun with IEEE division.  The GPU tests compare it with IEEE
+// division on random operands and on hard ones (significands of all ones or
+// all zeros, quotients next to a rounding tie).  The host build divides with
+// IEEE division (CLOUDSC_HOST_FORCE_REDO makes every call report, to drive
+// the caller's rerun in host tests).
+CSC_DEV double fast_div(double a, double b, DivCheck &dc) {
+#if defined(__CUDA_ARCH__)
+  const int ha = __double2hiint(a), hb = __double2hiint(b);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  // all-ones significand of b: w == 0, and the clamped shift gives 1 (else 0)
+  const unsigned w = ~(((unsigned)hb | 0xfff00000u) & (unsigned)__double2loint(b));
+  y = __hiloint2double(__double2hiint(y), __double2loint(y) | (int)__funnelshift_rc(1u, 0u, w));
+  const double aa = fabs(a);
+  const double q0 = __dmul_rn(aa, y);
+  double r = __fma_rn(-b, q0, aa);
+  const double q1 = __fma_rn(r, y, q0);
+  r = __fma_rn(-b, q1, aa);
+  const double q = __fma_rn(r, y, q1);
+  const unsigned da = a == 0.0 ? 0u : (unsigned)ha * 2u - kDivBase;
+  dc.acc |= da | ((unsigned)hb * 2u - kDivBase);
+  return __hiloint2double(__double2hiint(q) ^ (ha & (int)0x80000000), __double2loint(q));
+#else
+#if defined(CLOUDSC_HOST_FORCE_REDO)
+  dc.acc = ~0u;
+#else
+  (void)dc;
+#endif
+  return a / b;
+#endif
+}
+
+// Passes of the column code (cloudsc_column's PASS): plain, IEEE division
+// throughout; fast, the branch-free fast_div, recording operands outside its
+// exact window; redo, the rerun with IEEE division of a column whose fast
+// pass recorded one.
+enum { kPassPlain = 0, kPassFast = 1, kPassRedo = 2 };
+
+// a / b, by fast_div when FAST and the quotient is a double; IEEE otherwise.
+template <bool FAST, typename A, typename B>
+CSC_DEV auto cdiv(A a, B b, DivCheck &dc) -> decltype(a / b) {
+  typedef decltype(a / b) T;
+  if constexpr (FAST && std::is_same<T, double>::value) {
+    return fast_div(double(a), double(b), dc);
+  } else {
+    (void)dc;
+    return a / b;
+  }
+}
 
 // Double precision uses the portable exp/pow of plibm.h (bit-identical on the
 // host and the GPU).

@@ -18,6 +18,8 @@
 // warps of the CTA run the same stretch of the (very long) level code at the
 // same time and share the instruction cache.
 #define CSC_LEVEL_SYNC() __syncthreads()
+#include <type_traits>
+
 #include "cloudsc_column.cuh"
 
 #include "cloudsc_kparams.h"
@@ -71,8 +73,12 @@ namespace cloudsc {
 // FT: Fields (the double-precision interface) or FieldsSP (float arrays,
 // forms 0-2 only).  GEN: the parameter-exponent pows without their tests for
 // the exponents 0.5, 1.5, 2 and 3 (forms 0-2; the host launches it when the
-// uploaded parameters have none of these, gen_exponents_ok).
-template <int FORM, int MAXT, int MINB, typename FT = Fields, bool GEN = false>
+// uploaded parameters have none of these, gen_exponents_ok).  FAST (forms
+// 0-2, KLEV <= kMaxLevFast): every column runs the fast pass (the branch-free
+// division, fast_div); a column whose pass reported an operand outside that
+// division's exact window is run again with IEEE division, so that the
+// outputs are those of IEEE division for every input.
+template <int FORM, int MAXT, int MINB, typename FT = Fields, bool GEN = false, bool FAST = false>
 __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(FT F, Shape sh) {
   // Let ptxas place part of the register spills in shared memory instead of
   // local memory (a PTX pragma; the spill slots it moves no longer go
@@ -92,12 +98,21 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(FT F, Shape sh) {
       ib = 0;
       jl = sh.kidia0;
     }
-    if constexpr (FORM == 2)
-      cloudsc_column<float, true, false, false, FT, GEN>(F, sh, ib, jl, active);
-    else if constexpr (FORM >= 3)
-      cloudsc_column<double, false, FORM == 3 || FORM == 5, FORM >= 4, FT, false>(F, sh, ib, jl, active);
-    else
-      cloudsc_column<double, FORM == 1, false, false, FT, GEN>(F, sh, ib, jl, active);
+    if constexpr (FORM >= 3) {
+      cloudsc_column<double, false, FORM == 3 || FORM == 5, FORM >= 4, FT>(F, sh, ib, jl, active);
+    } else if constexpr (FAST) {
+      typedef std::conditional_t<FORM == 2, float, double> Real;
+      double plude_in[kMaxLevFast];
+      bool bad = false;
+      cloudsc_column<Real, FORM != 0, false, false, FT, GEN, kPassFast>(F, sh, ib, jl, active, &bad, plude_in);
+      // The rerun takes the whole CTA (the column code holds a CTA barrier
+      // at every level); only the columns that reported store anything.
+      if (__syncthreads_or(bad))
+        cloudsc_column<Real, FORM != 0, false, false, FT, GEN, kPassRedo>(F, sh, ib, jl, bad, nullptr, plude_in);
+    } else {
+      typedef std::conditional_t<FORM == 2, float, double> Real;
+      cloudsc_column<Real, FORM != 0, false, false, FT, GEN>(F, sh, ib, jl, active);
+    }
   }
 }
 
@@ -238,6 +253,19 @@ __global__ void __launch_bounds__(kSatadjThreads) state_increment_kernel(IncFiel
   }
 }
 
+// The column kernels' fast division on n operand pairs: q[i] = fast_div(a[i],
+// b[i]) and bad[i] = 1 where an operand fell outside its exact window (a
+// column kernel then reruns the column with IEEE division).  A self-check of
+// the division alone.
+__global__ void __launch_bounds__(kSatadjThreads) division_check_kernel(const double *a, const double *b,
+                                                                       long long n, double *q, int *bad) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    DivCheck dc;
+    q[i] = fast_div(a[i], b[i], dc);
+    bad[i] = dc.bad() ? 1 : 0;
+  }
+}
+
 }  // namespace cloudsc
 
 // ---------------------------------------------------------------------------
@@ -290,68 +318,74 @@ void variant_bounds(int v, int *maxt, int *minb) {
   *minb = kVariants[v].minb;
 }
 
-template <int FORM, bool GEN>
+template <int FORM, bool GEN, bool FAST>
 static const void *kernel_ptr_form(int v) {
   switch (v) {
-    case 0: return (const void *)cloudsc_kernel<FORM, kVariants[0].maxt, kVariants[0].minb, Fields, GEN>;
-    case 1: return (const void *)cloudsc_kernel<FORM, kVariants[1].maxt, kVariants[1].minb, Fields, GEN>;
-    case 2: return (const void *)cloudsc_kernel<FORM, kVariants[2].maxt, kVariants[2].minb, Fields, GEN>;
-    case 3: return (const void *)cloudsc_kernel<FORM, kVariants[3].maxt, kVariants[3].minb, Fields, GEN>;
-    case 4: return (const void *)cloudsc_kernel<FORM, kVariants[4].maxt, kVariants[4].minb, Fields, GEN>;
-    case 5: return (const void *)cloudsc_kernel<FORM, kVariants[5].maxt, kVariants[5].minb, Fields, GEN>;
+    case 0: return (const void *)cloudsc_kernel<FORM, kVariants[0].maxt, kVariants[0].minb, Fields, GEN, FAST>;
+    case 1: return (const void *)cloudsc_kernel<FORM, kVariants[1].maxt, kVariants[1].minb, Fields, GEN, FAST>;
+    case 2: return (const void *)cloudsc_kernel<FORM, kVariants[2].maxt, kVariants[2].minb, Fields, GEN, FAST>;
+    case 3: return (const void *)cloudsc_kernel<FORM, kVariants[3].maxt, kVariants[3].minb, Fields, GEN, FAST>;
+    case 4: return (const void *)cloudsc_kernel<FORM, kVariants[4].maxt, kVariants[4].minb, Fields, GEN, FAST>;
+    case 5: return (const void *)cloudsc_kernel<FORM, kVariants[5].maxt, kVariants[5].minb, Fields, GEN, FAST>;
     default: return nullptr;
   }
 }
 static_assert(kNumVariants == 6, "kernel_ptr_form lists every variant");
-// Forms 0-2 exist in every variant with GEN (the parameters of every known
-// configuration allow it) and, for parameters that do not, in the (448, 1)
-// variant without it (`launch` then runs that one).  Forms 3-5 (budgets,
-// SPP, inhomogeneity) keep the tests.
-static const void *kernel_ptr(int precision, int v, bool gen) {
+// Forms 0-2 exist in every variant with GEN and FAST (the parameters of every
+// known configuration allow GEN); for parameters that do not, in the (448, 1)
+// variant with FAST only; for KLEV above kMaxLevFast, in the (448, 1) variant
+// without either (`launch` then runs that one, at most 448 columns per CTA).
+// Forms 3-5 (budgets, SPP, inhomogeneity) keep the exponent tests and IEEE
+// division.
+static const void *kernel_ptr(int precision, int v, bool gen, bool fast) {
+  if (precision <= 2 && !fast) {
+    switch (precision) {
+      case 0: return (const void *)cloudsc_kernel<0, 448, 1, Fields, false, false>;
+      case 1: return (const void *)cloudsc_kernel<1, 448, 1, Fields, false, false>;
+      case 2: return (const void *)cloudsc_kernel<2, 448, 1, Fields, false, false>;
+    }
+  }
   if (!gen && precision <= 2) {
     switch (precision) {
-      case 0: return (const void *)cloudsc_kernel<0, 448, 1, Fields, false>;
-      case 1: return (const void *)cloudsc_kernel<1, 448, 1, Fields, false>;
-      case 2: return (const void *)cloudsc_kernel<2, 448, 1, Fields, false>;
+      case 0: return (const void *)cloudsc_kernel<0, 448, 1, Fields, false, true>;
+      case 1: return (const void *)cloudsc_kernel<1, 448, 1, Fields, false, true>;
+      case 2: return (const void *)cloudsc_kernel<2, 448, 1, Fields, false, true>;
     }
   }
   switch (precision) {
-    case 0: return kernel_ptr_form<0, true>(v);
-    case 1: return kernel_ptr_form<1, true>(v);
-    case 2: return kernel_ptr_form<2, true>(v);
-    case 3: return kernel_ptr_form<3, false>(v);
-    case 4: return kernel_ptr_form<4, false>(v);
-    case 5: return kernel_ptr_form<5, false>(v);
+    case 0: return kernel_ptr_form<0, true, true>(v);
+    case 1: return kernel_ptr_form<1, true, true>(v);
+    case 2: return kernel_ptr_form<2, true, true>(v);
+    case 3: return kernel_ptr_form<3, false, false>(v);
+    case 4: return kernel_ptr_form<4, false, false>(v);
+    case 5: return kernel_ptr_form<5, false, false>(v);
     default: return nullptr;
   }
 }
 
 // The single-precision interface's kernels: forms 0-2 in the two variants
-// the tuned schedules use, (640, 1) and (448, 1), with GEN; without GEN in
-// the (448, 1) variant.  Other variants map to the (448, 1) kernel (see
-// launch_sp).
-static const void *kernel_ptr_sp(int precision, int v, bool gen) {
-  const bool big = v == 0 && gen;
+// the tuned schedules use, (640, 1) and (448, 1), with GEN and FAST; in the
+// (448, 1) variant with FAST only, and without either for KLEV above
+// kMaxLevFast.  Other variants map to the (448, 1) kernel (see launch_sp).
+template <int FORM>
+static const void *kernel_ptr_sp_form(int v, bool gen, bool fast) {
+  if (!fast) return (const void *)cloudsc_kernel<FORM, 448, 1, FieldsSP, false, false>;
+  if (!gen) return (const void *)cloudsc_kernel<FORM, 448, 1, FieldsSP, false, true>;
+  if (v == 0) return (const void *)cloudsc_kernel<FORM, 640, 1, FieldsSP, true, true>;
+  return (const void *)cloudsc_kernel<FORM, 448, 1, FieldsSP, true, true>;
+}
+static const void *kernel_ptr_sp(int precision, int v, bool gen, bool fast) {
   switch (precision) {
-    case 0:
-      return big ? (const void *)cloudsc_kernel<0, 640, 1, FieldsSP, true>
-                 : gen ? (const void *)cloudsc_kernel<0, 448, 1, FieldsSP, true>
-                       : (const void *)cloudsc_kernel<0, 448, 1, FieldsSP, false>;
-    case 1:
-      return big ? (const void *)cloudsc_kernel<1, 640, 1, FieldsSP, true>
-                 : gen ? (const void *)cloudsc_kernel<1, 448, 1, FieldsSP, true>
-                       : (const void *)cloudsc_kernel<1, 448, 1, FieldsSP, false>;
-    case 2:
-      return big ? (const void *)cloudsc_kernel<2, 640, 1, FieldsSP, true>
-                 : gen ? (const void *)cloudsc_kernel<2, 448, 1, FieldsSP, true>
-                       : (const void *)cloudsc_kernel<2, 448, 1, FieldsSP, false>;
+    case 0: return kernel_ptr_sp_form<0>(v, gen, fast);
+    case 1: return kernel_ptr_sp_form<1>(v, gen, fast);
+    case 2: return kernel_ptr_sp_form<2>(v, gen, fast);
     default: return nullptr;
   }
 }
 
 // Registers and local (spill) bytes per thread of variant v (needs a device).
 cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes) {
-  const void *k = kernel_ptr(precision, v, true);
+  const void *k = kernel_ptr(precision, v, true, true);
   if (!k) return cudaErrorInvalidValue;
   cudaFuncAttributes a;
   cudaError_t e = cudaFuncGetAttributes(&a, k);
@@ -364,12 +398,14 @@ cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes
 // Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed,
 // 2 = FP32 physics, 3-5 the FP64 forms with budgets / SPP and inhomogeneity;
 // gen: the parameters allow the GEN kernels (forms 0-2 otherwise run the
-// (448, 1) kernel without GEN, at most 448 columns per CTA).
+// (448, 1) kernel without GEN, at most 448 columns per CTA, as they do for
+// KLEV above kMaxLevFast).
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream, bool gen) {
+  const bool fast = sh.klev <= kMaxLevFast;
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  if (!gen && precision <= 2 && threads > 448) return cudaErrorInvalidConfiguration;
-  const void *k = kernel_ptr(precision, v, gen);
+  if ((!gen || !fast) && precision <= 2 && threads > 448) return cudaErrorInvalidConfiguration;
+  const void *k = kernel_ptr(precision, v, gen, fast);
   if (!k) return cudaErrorInvalidValue;
   Fields fa = f;
   Shape sa = sh;
@@ -382,9 +418,10 @@ cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int t
 // variant runs the (448, 1) kernel with at most 448 columns per CTA.
 cudaError_t launch_sp(int precision, int v, const FieldsSP &f, const Shape &sh, int threads, int grid,
                       cudaStream_t stream, bool gen) {
+  const bool fast = sh.klev <= kMaxLevFast;
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  if ((v != 0 || !gen) && threads > 448) return cudaErrorInvalidConfiguration;
-  const void *k = kernel_ptr_sp(precision, v, gen);
+  if ((v != 0 || !gen || !fast) && threads > 448) return cudaErrorInvalidConfiguration;
+  const void *k = kernel_ptr_sp(precision, v, gen, fast);
   if (!k) return cudaErrorInvalidValue;
   FieldsSP fa = f;
   Shape sa = sh;
@@ -436,6 +473,15 @@ cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaS
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
   sltend_supersat_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(f, sh);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_division_check(const double *a, const double *b, long long n, double *q, int *bad,
+                                  cudaStream_t stream) {
+  long long blocks = (n + kSatadjThreads - 1) / kSatadjThreads;
+  if (blocks > 148LL * 16) blocks = 148LL * 16;
+  if (blocks < 1) blocks = 1;
+  division_check_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(a, b, n, q, bad);
   return cudaGetLastError();
 }
 

@@ -38,6 +38,29 @@ inline float xsign(float a, float b) { return std::copysign(a, b); }
 
 using namespace cloudsc;
 
+// FD: the kernels' fast pass and, for a column it reported, the rerun with
+// IEEE division reading PLUDE from the fast pass's copy (on the host every
+// division is IEEE; the redo build reports every one, so every column runs
+// twice).
+template <typename Real, bool F32M, bool GEN, bool FD>
+static void column(const Fields &f, const Shape &sh, int ib, int jl) {
+  if (FD && sh.klev <= kMaxLevFast) {
+    double plude_in[kMaxLevFast];
+    bool bad = false;
+    cloudsc_column<Real, F32M, false, false, Fields, GEN, kPassFast>(f, sh, ib, jl, true, &bad, plude_in);
+    if (bad) cloudsc_column<Real, F32M, false, false, Fields, GEN, kPassRedo>(f, sh, ib, jl, true, nullptr, plude_in);
+  } else {
+    cloudsc_column<Real, F32M, false, false, Fields, GEN>(f, sh, ib, jl);
+  }
+}
+typedef void (*ColumnFn)(const Fields &, const Shape &, int, int);
+// indexed by form + 3 * GEN + 6 * FASTDIV
+static const ColumnFn kColumn[12] = {
+    column<double, false, false, false>, column<double, true, false, false>, column<float, true, false, false>,
+    column<double, false, true, false>,  column<double, true, true, false>,  column<float, true, true, false>,
+    column<double, false, false, true>,  column<double, true, false, true>,  column<float, true, false, true>,
+    column<double, false, true, true>,   column<double, true, true, true>,   column<float, true, true, true>};
+
 extern "C" int hostemu_batched(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
                                double ptsphy, void **a, int precision) {
   Derived d;
@@ -76,22 +99,11 @@ extern "C" int hostemu_batched(const cloudsc_params *p, int nproma, int klev, in
     if (icend > nproma) icend = nproma;
     for (int jl = 0; jl < icend; ++jl) {
       // precision: the form (0 FP64, 1 FP32-mixed, 2 FP32 physics), plus
-      // 0x100 for the GEN column code (parameter-exponent pows untested)
-      const bool gen = (precision & 0x100) != 0;
-      switch (precision & 0xff) {
-        case 0:
-          if (gen) cloudsc_column<double, false, false, false, Fields, true>(f, sh, ib, jl);
-          else cloudsc_column<double, false>(f, sh, ib, jl);
-          break;
-        case 1:
-          if (gen) cloudsc_column<double, true, false, false, Fields, true>(f, sh, ib, jl);
-          else cloudsc_column<double, true>(f, sh, ib, jl);
-          break;
-        default:
-          if (gen) cloudsc_column<float, true, false, false, Fields, true>(f, sh, ib, jl);
-          else cloudsc_column<float, true>(f, sh, ib, jl);
-          break;
-      }
+      // 0x100 for the GEN column code (parameter-exponent pows untested) and
+      // 0x200 for the kernels' fast pass with its rerun (column, FD)
+      const int form = (precision & 0xff) > 2 ? 2 : (precision & 0xff);
+      const int gen = (precision & 0x100) ? 1 : 0, fd = (precision & 0x200) ? 1 : 0;
+      kColumn[form + 3 * gen + 6 * fd](f, sh, ib, jl);
     }
   }
   return (int)nwarn;

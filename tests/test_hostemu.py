@@ -218,3 +218,34 @@ def test_gen_column_code_identical(pp, form):
         ref, _ = util.run_oracle(po, arrs, 32, 100, 3200)
         for n in util.COMPARED:
             assert np.array_equal(util.defined(n, b[n]), util.defined(n, ref[n])), n
+
+
+@pytest.mark.parametrize("form,gen", [(0, False), (0, True), (1, True), (2, True)])
+def test_column_rerun_leaves_results_unchanged(pp, form, gen):
+    """The kernels' fast pass with its rerun (flag 0x200: the fast pass keeps
+    each level's PLUDE input, a column it reports runs again with IEEE
+    division reading PLUDE from that copy) gives the plain column code's
+    bits, both when no column reruns and when every column runs twice (the
+    redo build, whose divisions all report): the rerun sees the inputs as
+    they were, although the fast pass has already written PLUDE in place, and
+    the warning count is the rerun's alone.  The FP64 form also equals the
+    oracle."""
+    p, po = pp
+    arrs = util.apply_case(inputs.generate(100, 32, p, seed=1), "all_convection")
+    ngptot = 3193
+    flags = form | (0x100 if gen else 0)
+    a, nwa = util.run_hostemu(p, arrs, 32, 100, ngptot, precision=flags)
+    assert np.abs(util.defined("plude", a["plude"])).max() > 0
+    for libm in ("plibm", "redo"):
+        b, nwb = util.run_hostemu(p, arrs, 32, 100, ngptot, precision=flags | 0x200, libm=libm)
+        for n in util.COMPARED:
+            x = util.defined(n, util._valid_cols(a[n], ngptot, 32))
+            y = util.defined(n, util._valid_cols(b[n], ngptot, 32))
+            assert np.array_equal(x, y), (form, gen, libm, n)
+        assert nwa == nwb, libm
+    if form == 0:
+        ref, _ = util.run_oracle(po, arrs, 32, 100, ngptot)
+        for n in util.COMPARED:
+            x = util.defined(n, util._valid_cols(b[n], ngptot, 32))
+            y = util.defined(n, util._valid_cols(ref[n], ngptot, 32))
+            assert np.array_equal(x, y), n

@@ -76,7 +76,10 @@ def run_hostemu(p, arrs, nproma, ngpblks, ngptot, precision=0, libm="plibm", kle
     import ctypes
     import os
     here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hostemu")
-    name = "libcloudsc_hostemu.so" if libm == "plibm" else "libcloudsc_hostemu_glibc.so"
+    # "redo": every fast division of a FASTDIV column reports bad, so each
+    # level also runs its IEEE-division pass
+    name = {"plibm": "libcloudsc_hostemu.so", "glibc": "libcloudsc_hostemu_glibc.so",
+            "redo": "libcloudsc_hostemu_redo.so"}[libm]
     path = os.path.join(here, name)
     if not os.path.exists(path):
         import subprocess
