@@ -118,10 +118,19 @@ int cs_prep_batch(const float *feat, const float *tgt, const int32_t *cols, int3
 int cs_loss(const float *y, const float *t, int32_t rows, int32_t lp, int32_t klev, const float *w16,
             int32_t nheads, void *dy, double *loss_sum, void *stream);
 
-/* dw[t][n][k] += sum_r dz[r][n] * x[r + t - taps/2][k] (f32, CUDA cores);
- * db[n] += sum_r dz[r][n] when db is not NULL. */
+/* dw[t][n][k] += sum_r dz[r][n] * x[r + t - taps/2][k] (bf16 products, f32
+ * accumulation on the tcgen05 tensor cores, cs_wgrad_tc); db[n] += sum_r
+ * dz[r][n] when db is not NULL.  n and k are 64 or 128, taps 1 or 5; rows of
+ * x outside [0, rows) count as zero. */
 int cs_wgrad(const void *dz, const void *x, int32_t rows, int32_t n, int32_t k, int32_t taps, float *dw,
              float *db, void *stream);
+
+/* The weight-gradient GEMM alone: dw[t][n][k] += sum_r dz[r][n] *
+ * x[r + t - taps/2][k] on the tensor cores.  dz [rows][n] and x [rows][k] bf16
+ * row-major, dw f32 [taps][n][k], all 16-byte aligned; n, k in {64, 128}.
+ * err (or NULL): bit 1 or 2 set when a bounded wait in the kernel ran out. */
+int cs_wgrad_tc(const void *dz, const void *x, int32_t rows, int32_t n, int32_t k, int32_t taps, float *dw,
+                unsigned *err, void *stream);
 
 typedef struct cs_adam {
   float lr, beta1, beta2, eps, weight_decay, bc1, bc2; /* bc = 1 - beta^step */

@@ -489,6 +489,166 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   if (warp == 1) tcg::tmem_dealloc(tmem, TMEM_COLS);
 }
 
+// ------------------------------------------------------------------ weight gradients
+// dW[t][n][k] += sum_r dZ[r][n] * X[r + t - taps/2][k]: one GEMM per tap whose
+// reduction runs over the rows, the outer dimension of both operands.  Both
+// are therefore read MN-major: TMA fetches boxes of 64 features x 64 rows
+// (128 bytes per row, 128-byte swizzle), a row per K index, and the
+// descriptor walks them with 8-row groups 1024 bytes apart (SBO) and the
+// second 64 features one box further (LBO).  M = 128 covers dZ's features
+// (the upper half zero when n = 64), N = X's features (64 or 128).  Each CTA
+// reduces one chunk of rows of one tap into a TMEM accumulator, then adds it
+// to dW (f32 vector reductions).  Rows outside [0, rows) read as zero, as do
+// X rows shifted past either end.
+constexpr int WG_RK = 64;                    // rows (K) per stage
+constexpr int WG_STAGES = 4;
+constexpr int WG_HALF = WG_RK * 128;         // one box of 64 features: 8 KB
+constexpr int WG_STAGE = 4 * WG_HALF;        // dZ (two halves) + X (two halves)
+constexpr int WG_SMEM = WG_STAGES * WG_STAGE + 1024 + 256;
+
+__device__ __forceinline__ uint64_t sdesc_mn_sw128(uint32_t saddr, uint32_t lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu)          // start address / 16
+         | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16)  // leading byte offset: the next 64 features
+         | ((uint64_t)(1024 >> 4) << 32)             // stride byte offset: 8-row groups along K
+         | ((uint64_t)1 << 46)                       // descriptor version
+         | ((uint64_t)2 << 61);                      // swizzle: 128 B
+}
+__device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
+               : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(128, 1)
+    wgrad_tc_kernel(const __grid_constant__ CUtensorMap tmD, const __grid_constant__ CUtensorMap tmX, int rows,
+                    int chunk, int n, int taps, float *dw, unsigned *err) {
+  // transpose bits 15 and 16: both operands MN-major
+  constexpr uint32_t IDESC = tcg::idesc_bf16_f32(128, BN) | (1u << 15) | (1u << 16);
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *bars = (uint64_t *)(smem + WG_STAGES * WG_STAGE);
+  uint64_t *full = bars, *empty = bars + WG_STAGES, *tfull = empty + WG_STAGES, *drain = tfull + 1;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+  volatile uint32_t *issued = (volatile uint32_t *)(tmem_slot + 2);
+  volatile uint32_t *consumed = (volatile uint32_t *)(tmem_slot + 3);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int t = blockIdx.y, shift = t - taps / 2;
+  const int r0 = blockIdx.x * chunk;
+  const int r1 = min(rows, r0 + chunk);
+  const int nkb = (r1 - r0 + WG_RK - 1) / WG_RK;
+  const int nh = n / 64;
+  constexpr int KH = BN / 64;
+  // the dZ half TMA never writes (n = 64) stays zero: M is always 128
+  if (nh == 1) {
+    for (int i = tid; i < WG_STAGES * WG_HALF / 16; i += blockDim.x) {
+      const int s = i / (WG_HALF / 16), j = i % (WG_HALF / 16);
+      reinterpret_cast<uint4 *>(smem + s * WG_STAGE + WG_HALF)[j] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int s = 0; s < WG_STAGES; ++s) {
+      tcg::mbar_init(&full[s], 1);
+      tcg::mbar_init(&empty[s], 1);
+    }
+    tcg::mbar_init(tfull, 1);
+    tcg::mbar_init(drain, 1);
+    *abort_flag = 0;
+    *issued = 0;
+    *consumed = 0;
+    tcg::mbar_fence_init();
+    tcg::tma_prefetch_desc(&tmD);
+    tcg::tma_prefetch_desc(&tmX);
+  }
+  if (warp == 1) {
+    tcg::tmem_alloc(tmem_slot, BN);
+    tcg::tmem_relinquish();
+  }
+  tcg::tc_fence_before();
+  __syncthreads();
+  tcg::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- producer
+    for (int kb = 0; kb < nkb && !*abort_flag; ++kb) {
+      const int s = kb % WG_STAGES;
+      if (kb >= WG_STAGES && !tcg::mbar_wait(&empty[s], ((kb / WG_STAGES) - 1) & 1)) {
+        flag(err, 1u);
+        *abort_flag = 1;
+        break;
+      }
+      uint8_t *st = smem + s * WG_STAGE;
+      const int r = r0 + kb * WG_RK;
+      tcg::mbar_arrive_expect_tx(&full[s], (uint32_t)((nh + KH) * WG_HALF));
+      for (int h = 0; h < nh; ++h) tcg::tma_load_2d(st + h * WG_HALF, &tmD, &full[s], h * 64, r);
+      for (int h = 0; h < KH; ++h) tcg::tma_load_2d(st + (2 + h) * WG_HALF, &tmX, &full[s], h * 64, r + shift);
+      *issued = (uint32_t)(kb + 1);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    bool ok = true;
+    for (int kb = 0; kb < nkb && !*abort_flag; ++kb) {
+      const int s = kb % WG_STAGES;
+      ok = tcg::mbar_wait(&full[s], (kb / WG_STAGES) & 1);
+      if (!ok) break;
+      tcg::tc_fence_after();
+      const uint32_t sa = tcg::smem_u32(smem + s * WG_STAGE);
+      const uint64_t da = sdesc_mn_sw128(sa, WG_HALF);
+      const uint64_t db = sdesc_mn_sw128(sa + 2 * WG_HALF, WG_HALF);
+#pragma unroll
+      for (int kk = 0; kk < WG_RK / 16; ++kk)  // 16 rows = two 1024-byte groups per instruction
+        tcg::mma_bf16(tmem, da + (uint64_t)(kk * (2048 >> 4)), db + (uint64_t)(kk * (2048 >> 4)), IDESC,
+                      (kb > 0 || kk > 0) ? 1u : 0u);
+      tcg::mma_commit(&empty[s]);
+      *consumed = (uint32_t)(kb + 1);
+    }
+    if (ok && !*abort_flag) {
+      tcg::mma_commit(tfull);
+    } else {
+      flag(err, 1u);
+      *abort_flag = 1;
+    }
+  }
+  __syncwarp();
+  // ---------------- epilogue: warp w holds TMEM lanes 32w.. = features n of dZ
+  int ok = 1;
+  if (lane == 0) ok = (!*abort_flag && tcg::mbar_wait(tfull, 0)) ? 1 : 0;
+  ok = __shfl_sync(0xffffffffu, ok, 0);
+  if (ok) {
+    tcg::tc_fence_after();
+    const int m0 = warp * 32;
+    if (m0 < n) {
+#pragma unroll
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        float v[32];
+        tcg::tmem_ld32(tmem + ((uint32_t)m0 << 16) + (uint32_t)c0, v);
+        float *d = dw + ((size_t)t * n + m0 + lane) * BN + c0;
+#pragma unroll
+        for (int i = 0; i < 32; i += 4) red_add_v4(d + i, v[i], v[i + 1], v[i + 2], v[i + 3]);
+      }
+    }
+  } else if (lane == 0) {
+    flag(err, 2u);
+    *abort_flag = 1;
+  }
+  __syncthreads();
+  // On an abort, let every copy and MMA this CTA issued land before shared
+  // memory and TMEM are released (bounded waits).
+  if (tid == 0 && *abort_flag) {
+    for (uint32_t q = *consumed; q < *issued; ++q)
+      (void)tcg::mbar_wait(&full[q % WG_STAGES], (q / WG_STAGES) & 1);
+  }
+  if (tid == 32 && *abort_flag) {
+    tcg::mma_commit(drain);
+    (void)tcg::mbar_wait(drain, 0);
+  }
+  tcg::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tcg::tmem_dealloc(tmem, BN);
+}
+
 // ------------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -557,6 +717,19 @@ cudaError_t launch_ws_n(const CUtensorMap &ma, const CUtensorMap &mb, const Args
   if (a.epi == CS_EPI_SILU) return launch_ws_t<BN, CS_EPI_SILU, 1>(ma, mb, a, grid, nst, st);
   if (a.epi == CS_EPI_BWD) return launch_ws_t<BN, CS_EPI_BWD, 1>(ma, mb, a, grid, nst, st);
   return launch_ws_t<BN, CS_EPI_LINEAR_F32, 1>(ma, mb, a, grid, nst, st);
+}
+
+template <int BN>
+cudaError_t launch_wgrad_t(const CUtensorMap &md, const CUtensorMap &mx, int rows, int chunk, int nchunks, int n,
+                           int taps, float *dw, unsigned *err, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(wgrad_tc_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, WG_SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  wgrad_tc_kernel<BN><<<dim3(nchunks, taps), 128, WG_SMEM, st>>>(md, mx, rows, chunk, n, taps, dw, err);
+  return cudaGetLastError();
 }
 
 int g_impl = 0;  // 0: warp-specialised kernel, 1: the single-thread pipeline
@@ -634,5 +807,34 @@ extern "C" int cs_conv_gemm(const cs_gemm_desc *g, void *stream) {
     else if (g->epi == CS_EPI_BWD) e = launch_t<64, CS_EPI_BWD>(ma, mb, a, grid, st);
     else e = launch_t<64, CS_EPI_LINEAR_F32>(ma, mb, a, grid, st);
   }
+  return e == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+// dW[t][n][k] += sum over rows of dZ[r][n] X[r + t - taps/2][k] on the tensor
+// cores (wgrad_tc_kernel): dZ [rows][n], X [rows][k] bf16 row-major, dW f32.
+extern "C" int cs_wgrad_tc(const void *dz, const void *x, int32_t rows, int32_t n, int32_t k, int32_t taps,
+                           float *dw, unsigned *err, void *stream) {
+  using namespace sg;
+  if (!dz || !x || !dw || rows <= 0 || (n != 64 && n != 128) || (k != 64 && k != 128) || (taps != 1 && taps != 5))
+    return CS_E_ARG;
+  if (((uintptr_t)dz | (uintptr_t)x | (uintptr_t)dw) & 15) return CS_E_ARG;
+  CUtensorMap md, mx;
+  if (!make_map(&md, dz, (uint64_t)rows, (uint64_t)n, (uint32_t)WG_RK)) return CS_E_CUDA;
+  if (!make_map(&mx, x, (uint64_t)rows, (uint64_t)k, (uint32_t)WG_RK)) return CS_E_CUDA;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // about two CTAs per SM over all taps, chunks of at least 512 rows (each
+  // chunk adds its n x k partial to dW)
+  int nchunks = (2 * sms + taps - 1) / taps;
+  const int maxchunks = (rows + 511) / 512;
+  if (nchunks > maxchunks) nchunks = maxchunks;
+  if (nchunks < 1) nchunks = 1;
+  int chunk = (rows + nchunks - 1) / nchunks;
+  chunk = (chunk + WG_RK - 1) / WG_RK * WG_RK;
+  nchunks = (rows + chunk - 1) / chunk;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = k == 128 ? launch_wgrad_t<128>(md, mx, rows, chunk, nchunks, n, taps, dw, err, st)
+                           : launch_wgrad_t<64>(md, mx, rows, chunk, nchunks, n, taps, dw, err, st);
   return e == cudaSuccess ? CS_OK : CS_E_CUDA;
 }

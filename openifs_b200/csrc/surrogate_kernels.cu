@@ -330,58 +330,20 @@ __global__ void loss_kernel(const float *__restrict__ y, const float *__restrict
 }
 
 // ---------------------------------------------------------------- gradients
-// One CTA: tap t, a 64 x 64 tile of (n, k), a chunk of rows; 256 threads with
-// 4 x 4 outputs each, rows staged 32 at a time in shared memory.
-constexpr int WG_CHUNK = 2048;
-__global__ void __launch_bounds__(256) wgrad_kernel(const __nv_bfloat16 *__restrict__ dz,
-                                                    const __nv_bfloat16 *__restrict__ x, int rows, int n, int k,
-                                                    int taps, float *dw) {
-  __shared__ float sd[32][64 + 4];
-  __shared__ float sx[32][64 + 4];
-  const int t = blockIdx.z;
-  const int ktiles = k / 64;
-  const int n0 = (blockIdx.y / ktiles) * 64, k0 = (blockIdx.y % ktiles) * 64;
-  const int r0 = blockIdx.x * WG_CHUNK, r1 = min(rows, r0 + WG_CHUNK);
-  const int shift = t - taps / 2;
-  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
-  float acc[4][4] = {};
-  for (int rr = r0; rr < r1; rr += 32) {
-    for (int e = tid; e < 32 * 64; e += 256) {
-      const int i = e >> 6, j = e & 63;
-      const int r = rr + i;
-      sd[i][j] = r < r1 ? __bfloat162float(dz[(size_t)r * n + n0 + j]) : 0.0f;
-      const int rx = r + shift;
-      sx[i][j] = (r < r1 && rx >= 0 && rx < rows) ? __bfloat162float(x[(size_t)rx * k + k0 + j]) : 0.0f;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int i = 0; i < 32; ++i) {
-      float a[4], b[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = sd[i][ty * 4 + q];
-        b[q] = sx[i][tx * 4 + q];
-      }
-#pragma unroll
-      for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] += a[p] * b[q];
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int p = 0; p < 4; ++p)
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      atomicAdd(&dw[((size_t)t * n + n0 + ty * 4 + p) * k + k0 + tx * 4 + q], acc[p][q]);
-}
-
+// The weight gradients run on the tensor cores (cs_wgrad_tc, surrogate_gemm.cu);
+// the bias gradient is a column sum of dz over chunks of rows.
+constexpr int BG_CHUNK = 128;
 __global__ void bgrad_kernel(const __nv_bfloat16 *__restrict__ dz, int rows, int n, float *db) {
-  const int r0 = blockIdx.x * WG_CHUNK, r1 = min(rows, r0 + WG_CHUNK);
+  const int r0 = blockIdx.x * BG_CHUNK, r1 = min(rows, r0 + BG_CHUNK);
   for (int j = threadIdx.x; j < n; j += blockDim.x) {
-    float s = 0.0f;
-    for (int r = r0; r < r1; ++r) s += __bfloat162float(dz[(size_t)r * n + j]);
-    atomicAdd(&db[j], s);
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};  // four independent sums: the loads overlap
+    int r = r0;
+    for (; r + 4 <= r1; r += 4) {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s[q] += __bfloat162float(dz[(size_t)(r + q) * n + j]);
+    }
+    for (; r < r1; ++r) s[0] += __bfloat162float(dz[(size_t)r * n + j]);
+    atomicAdd(&db[j], (s[0] + s[1]) + (s[2] + s[3]));
   }
 }
 
@@ -661,11 +623,11 @@ int cs_loss(const float *y, const float *t, int32_t rows, int32_t lp, int32_t kl
 int cs_wgrad(const void *dz, const void *x, int32_t rows, int32_t n, int32_t k, int32_t taps, float *dw,
              float *db, void *stream) {
   using namespace sk;
-  if (!dz || !x || !dw || rows <= 0 || n % 64 || k % 64 || (taps != 1 && taps != 5)) return CS_E_ARG;
-  dim3 grid((rows + WG_CHUNK - 1) / WG_CHUNK, (n / 64) * (k / 64), taps);
-  wgrad_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)dz, (const __nv_bfloat16 *)x, rows,
-                                                        n, k, taps, dw);
-  if (db) bgrad_kernel<<<(rows + WG_CHUNK - 1) / WG_CHUNK, 128, 0, (cudaStream_t)stream>>>(
+  if (!dz || !x || !dw || rows <= 0 || (n != 64 && n != 128) || (k != 64 && k != 128) || (taps != 1 && taps != 5))
+    return CS_E_ARG;
+  const int rc = cs_wgrad_tc(dz, x, rows, n, k, taps, dw, nullptr, stream);
+  if (rc != CS_OK) return rc;
+  if (db) bgrad_kernel<<<(rows + BG_CHUNK - 1) / BG_CHUNK, 128, 0, (cudaStream_t)stream>>>(
       (const __nv_bfloat16 *)dz, rows, n, db);
   return cudaGetLastError() == cudaSuccess ? CS_OK : CS_E_CUDA;
 }

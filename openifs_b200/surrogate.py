@@ -104,11 +104,12 @@ def _lib():
         L.cs_prep_batch.argtypes = [vp, vp, vp, i32, i32, i32, ctypes.POINTER(Norm), vp, vp, vp]
         L.cs_loss.argtypes = [vp, vp, i32, i32, i32, vp, i32, vp, vp, vp]
         L.cs_wgrad.argtypes = [vp, vp, i32, i32, i32, i32, vp, vp, vp]
+        L.cs_wgrad_tc.argtypes = [vp, vp, i32, i32, i32, i32, vp, vp, vp]
         L.cs_adamw.argtypes = [vp, vp, vp, vp, i32, i32, i32, ctypes.POINTER(Adam), vp, vp, vp]
         L.cs_post.argtypes = [ctypes.POINTER(Columns), vp, i32, ctypes.POINTER(Guard), vp, vp, vp, vp]
         L.cs_move_columns.argtypes = [vp, i32, i32, i32, vp, vp, i32, i32, vp]
         for f in ["cs_raw_features", "cs_column_sums", "cs_prep_inputs", "cs_prep_targets", "cs_prep_batch", "cs_loss",
-                  "cs_wgrad", "cs_adamw", "cs_post", "cs_move_columns"]:
+                  "cs_wgrad", "cs_wgrad_tc", "cs_adamw", "cs_post", "cs_move_columns"]:
             getattr(L, f).restype = ctypes.c_int
         _L = L
     return _L

@@ -1,5 +1,5 @@
 """The surrogate's GPU kernels: gradients of the whole network (tcgen05
-forward and backward-data GEMMs, CUDA-core weight gradients, loss kernel)
+forward, backward-data and weight-gradient GEMMs, loss kernel)
 against the float64 CPU reference (tests/surrogate_ref.py, itself checked
 against finite differences) on identical bf16-rounded weights and inputs;
 a short training run that must lower the loss; and the guarded inference
@@ -60,6 +60,52 @@ def test_gradients_match_cpu_reference(cuda, width):
         gb = net.gb[i].double().cpu().numpy()
         relb = np.linalg.norm(gb - G[f"b{i}"]) / np.linalg.norm(G[f"b{i}"])
         assert relb < 5e-2, (i, relb)
+
+
+@pytest.mark.parametrize("n,k,taps,rows", [(128, 128, 5, 20_000), (128, 128, 1, 7_777), (64, 128, 1, 9_000),
+                                           (64, 64, 5, 12_345), (128, 64, 5, 3_001), (64, 64, 1, 100)])
+def test_weight_gradient_gemm(cuda, n, k, taps, rows):
+    """The tensor-core weight gradient dW[t][n][k] += sum_r dZ[r][n] X[r+t-taps/2][k]
+    (MN-major operands, split over row chunks, f32 reductions into dW)
+    against float64 sums of the same bf16 values: rows shifted past either
+    end count as zero, dW accumulates onto what it holds, the error flag
+    stays clear."""
+    import torch
+    rng = np.random.default_rng(rows + n + k + taps)
+    dz = torch.from_numpy(rng.standard_normal((rows, n)).astype(np.float32)).bfloat16().cuda()
+    x = torch.from_numpy(rng.standard_normal((rows, k)).astype(np.float32)).bfloat16().cuda()
+    init = rng.standard_normal((taps, n, k)).astype(np.float32)
+    dw = torch.from_numpy(init).cuda()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    L = S._lib()
+    rc = L.cs_wgrad_tc(dz.data_ptr(), x.data_ptr(), rows, n, k, taps, dw.data_ptr(), err.data_ptr(), S._stream())
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    D = dz.double().cpu().numpy()
+    X = x.double().cpu().numpy()
+    ref = init.astype(np.float64)
+    for t in range(taps):
+        s = t - taps // 2
+        xs = np.zeros_like(X)
+        if s >= 0:
+            xs[:rows - s] = X[s:]
+        else:
+            xs[-s:] = X[:rows + s]
+        ref[t] += D.T @ xs
+    got = dw.double().cpu().numpy()
+    scale = np.sqrt(rows)
+    assert np.abs(got - ref).max() <= 1e-4 * scale, np.abs(got - ref).max()
+
+
+def test_weight_gradient_rejects_bad_shapes(cuda):
+    import torch
+    L = S._lib()
+    a = torch.zeros(256, 128, dtype=torch.bfloat16, device="cuda")
+    dw = torch.zeros(128, 128, device="cuda")
+    assert L.cs_wgrad_tc(a.data_ptr(), a.data_ptr(), 256, 96, 128, 1, dw.data_ptr(), None, None) != 0
+    assert L.cs_wgrad_tc(a.data_ptr(), a.data_ptr(), 256, 128, 128, 3, dw.data_ptr(), None, None) != 0
+    assert L.cs_wgrad_tc(a.data_ptr() + 2, a.data_ptr(), 256, 128, 128, 1, dw.data_ptr(), None, None) != 0
 
 
 @pytest.fixture(scope="module")
