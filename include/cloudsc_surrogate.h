@@ -50,6 +50,16 @@ typedef struct cs_gemm_desc {
  * (tcgen05, one persistent CTA per SM). */
 int cs_conv_gemm(const cs_gemm_desc *g, void *stream);
 
+/* The network's MLP layer and output head in one kernel (inference):
+ * h = SiLU(a w1^T + b1) kept on chip as bf16, y = h w2^T + b2 (f32); rows
+ * outside the levels of the lp/klev layout written as zero, as
+ * cs_conv_gemm's CS_EPI_SILU then CS_EPI_LINEAR_F32 would (same bits).
+ * a [rows][k] and w1 [k][k], w2 [64][k] bf16 (16-byte aligned), y f32
+ * [rows][64] (32-byte aligned); k 64 or 128; b1, b2 or NULL; err as in
+ * cs_gemm_desc. */
+int cs_mlp_head(const void *a, const void *w1, const float *b1, const void *w2, const float *b2, int32_t rows,
+                int32_t k, int32_t lp, int32_t klev, float *y, uint32_t *err, void *stream);
+
 /* Which kernel cs_conv_gemm runs: 0 (default) the warp-specialised one
  * (weights resident in shared memory, one halo tile per K block for the 5
  * taps, double-buffered TMEM accumulator), 1 the simple single-thread

@@ -489,6 +489,272 @@ __global__ void __launch_bounds__(WS_THREADS, 1)
   if (warp == 1) tcg::tmem_dealloc(tmem, TMEM_COLS);
 }
 
+// ------------------------------------------------------------------ fused MLP layer + output head
+// Inference only: h = SiLU(A W1^T + b1) (padding rows zero) and
+// y = h W2^T + b2 (f32, padding rows zero) in one kernel, h never leaving
+// the SM: the epilogue warps write it as bf16 into a shared-memory tile in
+// the same 128-byte-swizzled K-major layout TMA writes, and the second
+// layer's MMAs read it from there.  Warp 0 streams the 128-row tiles of A
+// (a 3-stage ring; both weight matrices resident), warp 1 issues the MMAs
+// (tile i's first layer, then tile i-1's second layer, so the tensor core
+// works while the epilogue drains), warps 2-17 drain TMEM.  The first
+// layer's accumulator and h are double-buffered; the arithmetic is the
+// unfused epilogues' (SiLU then bf16; bias add), so y equals the two-kernel
+// result bit for bit.
+constexpr int MH_WARPS = 16;
+constexpr int MH_THREADS = 64 + 32 * MH_WARPS;
+template <int W>
+struct MhLayout {
+  static constexpr int KB = W / 64;
+  static constexpr int NST = 3;
+  static constexpr int TILE = KB * 16384;        // 128 rows x W bf16, KB blocks of 128 x 64
+  static constexpr int W1_BYTES = KB * W * 128;   // W x W
+  static constexpr int W2_BYTES = KB * 64 * 128;  // 64 x W
+  static constexpr int OFF_W1 = 0;
+  static constexpr int OFF_W2 = OFF_W1 + W1_BYTES;
+  static constexpr int OFF_A = OFF_W2 + W2_BYTES;
+  static constexpr int OFF_H = OFF_A + NST * TILE;
+  static constexpr int OFF_BIAS = OFF_H + 2 * TILE;
+  static constexpr int OFF_BAR = OFF_BIAS + (W + 64) * 4;
+  static constexpr int SMEM = OFF_BAR + 256 + 1024;
+  static constexpr int TMEM_COLS = 2 * W + 128 <= 256 ? 256 : 512;
+};
+
+template <int W>
+__global__ void __launch_bounds__(MH_THREADS, 1)
+    mlp_head_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmW1,
+                    const __grid_constant__ CUtensorMap tmW2, const float *b1, const float *b2, int rows, int lp,
+                    int klev, float *y, unsigned *err) {
+  using L = MhLayout<W>;
+  constexpr uint32_t ID1 = tcg::idesc_bf16_f32(BM, W), ID2 = tcg::idesc_bf16_f32(BM, 64);
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  float *sb1 = (float *)(smem + L::OFF_BIAS), *sb2 = sb1 + W;
+  uint64_t *bars = (uint64_t *)(smem + L::OFF_BAR);
+  uint64_t *wfull = bars, *full = bars + 1, *empty = full + L::NST;
+  uint64_t *t1full = empty + L::NST, *t1empty = t1full + 2, *hfull = t1empty + 2, *t2full = hfull + 2,
+           *t2empty = t2full + 2, *drain = t2empty + 2;
+  uint32_t *tmem_slot = (uint32_t *)(drain + 1);
+  volatile int *abort_flag = (volatile int *)(tmem_slot + 1);
+  volatile uint32_t *issued = (volatile uint32_t *)(tmem_slot + 2);
+  volatile uint32_t *consumed = (volatile uint32_t *)(tmem_slot + 3);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntiles = (rows + BM - 1) / BM;
+  if (tid == 0) {
+    tcg::mbar_init(wfull, 1);
+    for (int s = 0; s < L::NST; ++s) {
+      tcg::mbar_init(&full[s], 1);
+      tcg::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tcg::mbar_init(&t1full[b], 1);
+      tcg::mbar_init(&t1empty[b], MH_WARPS);
+      tcg::mbar_init(&hfull[b], MH_WARPS);
+      tcg::mbar_init(&t2full[b], 1);
+      tcg::mbar_init(&t2empty[b], MH_WARPS);
+    }
+    tcg::mbar_init(drain, 1);
+    *abort_flag = 0;
+    *issued = 0;
+    *consumed = 0;
+    tcg::mbar_fence_init();
+    tcg::tma_prefetch_desc(&tmA);
+    tcg::tma_prefetch_desc(&tmW1);
+    tcg::tma_prefetch_desc(&tmW2);
+  }
+  if (warp == 1) {
+    tcg::tmem_alloc(tmem_slot, L::TMEM_COLS);
+    tcg::tmem_relinquish();
+  }
+  for (int c = tid; c < W; c += blockDim.x) sb1[c] = b1 ? b1[c] : 0.0f;
+  for (int c = tid; c < 64; c += blockDim.x) sb2[c] = b2 ? b2[c] : 0.0f;
+  tcg::tc_fence_before();
+  __syncthreads();
+  tcg::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------- producer
+    tcg::mbar_arrive_expect_tx(wfull, (uint32_t)(L::W1_BYTES + L::W2_BYTES));
+    for (int kb = 0; kb < L::KB; ++kb) tcg::tma_load_2d(smem + L::OFF_W1 + kb * W * 128, &tmW1, wfull, kb * BK, 0);
+    for (int kb = 0; kb < L::KB; ++kb) tcg::tma_load_2d(smem + L::OFF_W2 + kb * 64 * 128, &tmW2, wfull, kb * BK, 0);
+    uint32_t it = 0;
+    for (int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x, ++it) {
+      const int s = it % L::NST;
+      if (it >= (uint32_t)L::NST && !tcg::mbar_wait(&empty[s], ((it / L::NST) - 1) & 1)) {
+        flag(err, 1u);
+        *abort_flag = 1;
+        break;
+      }
+      tcg::mbar_arrive_expect_tx(&full[s], (uint32_t)L::TILE);
+      for (int kb = 0; kb < L::KB; ++kb)
+        tcg::tma_load_2d(smem + L::OFF_A + s * L::TILE + kb * 16384, &tmA, &full[s], kb * BK, tile * BM);
+      *issued = it + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---------------- MMA issuer
+    // second layer of local tile j: h (shared memory) x W2^T into the second accumulator
+    auto layer2 = [&](uint32_t j) -> bool {
+      const int b = j & 1;
+      if (!tcg::mbar_wait(&hfull[b], (j >> 1) & 1)) return false;
+      if (j >= 2 && !tcg::mbar_wait(&t2empty[b], ((j >> 1) - 1) & 1)) return false;
+      tcg::tc_fence_after();
+      const uint32_t acc = tmem + (uint32_t)(2 * W + b * 64);
+      const uint32_t sh = tcg::smem_u32(smem + L::OFF_H + b * L::TILE);
+#pragma unroll
+      for (int kb = 0; kb < L::KB; ++kb) {
+        const uint64_t da = tcg::sdesc_k_sw128(sh + kb * 16384);
+        const uint64_t db = tcg::sdesc_k_sw128(tcg::smem_u32(smem + L::OFF_W2 + kb * 64 * 128));
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk)
+          tcg::mma_bf16(acc, da + 2 * kk, db + 2 * kk, ID2, (kb > 0 || kk > 0) ? 1u : 0u);
+      }
+      tcg::mma_commit(&t2full[b]);
+      return true;
+    };
+    bool ok = tcg::mbar_wait(wfull, 0);
+    uint32_t i = 0;
+    for (int tile = blockIdx.x; ok && tile < ntiles && !*abort_flag; tile += gridDim.x, ++i) {
+      const int b = i & 1, s = i % L::NST;
+      if (i >= 2) ok = tcg::mbar_wait(&t1empty[b], ((i >> 1) - 1) & 1);
+      if (ok) ok = tcg::mbar_wait(&full[s], (i / L::NST) & 1);
+      if (!ok) break;
+      tcg::tc_fence_after();
+      const uint32_t acc = tmem + (uint32_t)(b * W);
+      const uint32_t sa = tcg::smem_u32(smem + L::OFF_A + s * L::TILE);
+#pragma unroll
+      for (int kb = 0; kb < L::KB; ++kb) {
+        const uint64_t da = tcg::sdesc_k_sw128(sa + kb * 16384);
+        const uint64_t db = tcg::sdesc_k_sw128(tcg::smem_u32(smem + L::OFF_W1 + kb * W * 128));
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk)
+          tcg::mma_bf16(acc, da + 2 * kk, db + 2 * kk, ID1, (kb > 0 || kk > 0) ? 1u : 0u);
+      }
+      tcg::mma_commit(&empty[s]);
+      tcg::mma_commit(&t1full[b]);
+      *consumed = i + 1;
+      if (i >= 1 && !layer2(i - 1)) {
+        ok = false;
+        break;
+      }
+    }
+    if (ok && i >= 1 && !*abort_flag) ok = layer2(i - 1);
+    if (!ok) {
+      flag(err, 1u);
+      *abort_flag = 1;
+    }
+  } else if (warp >= 2) {
+    // ---------------- epilogue, software-pipelined: the first layer of tile
+    // i, then the output head of tile i-1 (its MMAs long finished), so no
+    // warp waits for the second layer of the tile it has just handed over.
+    // The head's 64 columns go to slices 0-1 at width 128 and to the slices
+    // the first layer leaves idle (2-3) at width 64.
+    const int quarter = warp & 3, slice = (warp - 2) >> 2;
+    const int hslice = W == 64 ? slice - 2 : slice;  // head column slice of this warp, 0 or 1 if any
+    // drain the output head of local tile j (rows of `tile`) into y
+    auto head = [&](uint32_t j, int tile) -> bool {
+      const int b = j & 1;
+      int ok = 1;
+      if (lane == 0) ok = tcg::mbar_wait(&t2full[b], (j >> 1) & 1) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) return false;
+      __syncwarp();
+      tcg::tc_fence_after();
+      if (hslice >= 0 && hslice < 2) {
+        const int row = tile * BM + quarter * 32 + lane;
+        const int pos = lp > 0 ? row % lp : 2;
+        const bool valid = row < rows && (lp <= 0 || (pos >= 2 && pos < 2 + klev));
+        float v[32];
+        tcg::tmem_ld32(tmem + (uint32_t)(2 * W + b * 64) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(hslice * 32),
+                       v);
+        if (row < rows) {
+          float *d = y + (size_t)row * 64 + hslice * 32;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            uint32_t w8[8];
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj)
+              w8[jj] = __float_as_uint(valid ? v[8 * q + jj] + sb2[hslice * 32 + 8 * q + jj] : 0.0f);
+            st256(d + 8 * q, w8);
+          }
+        }
+      }
+      tcg::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tcg::mbar_arrive(&t2empty[b]);
+      return true;
+    };
+    uint32_t i = 0;
+    bool ok_all = true;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++i) {
+      const int b = i & 1;
+      int ok = 1;
+      if (lane == 0) ok = tcg::mbar_wait(&t1full[b], (i >> 1) & 1) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) {
+        ok_all = false;
+        break;
+      }
+      __syncwarp();
+      tcg::tc_fence_after();
+      if (slice * 32 < W) {
+        const int rt = quarter * 32 + lane, row = tile * BM + rt;
+        const int pos = lp > 0 ? row % lp : 2;
+        const bool valid = row < rows && (lp <= 0 || (pos >= 2 && pos < 2 + klev));
+        float v[32];
+        tcg::tmem_ld32(tmem + (uint32_t)(b * W) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(slice * 32), v);
+        __align__(16) __nv_bfloat16 h[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+          float hh = silu(v[q] + sb1[slice * 32 + q]);
+          if (!valid) hh = 0.0f;
+          h[q] = __float2bfloat16(hh);
+        }
+        uint8_t *hb = smem + L::OFF_H + b * L::TILE;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int chunk = slice * 4 + j, kb = chunk >> 3, c = chunk & 7;  // 16-byte chunk of the row
+          *reinterpret_cast<uint4 *>(hb + kb * 16384 + rt * 128 + ((c ^ (rt & 7)) << 4)) =
+              reinterpret_cast<const uint4 *>(h)[j];
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      }
+      tcg::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        tcg::mbar_arrive(&t1empty[b]);
+        tcg::mbar_arrive(&hfull[b]);
+      }
+      if (i >= 1 && !head(i - 1, tile - (int)gridDim.x)) {
+        ok_all = false;
+        break;
+      }
+      if (__shfl_sync(0xffffffffu, lane == 0 ? *abort_flag : 0, 0)) {
+        ok_all = false;
+        break;
+      }
+    }
+    if (ok_all && i >= 1 && !head(i - 1, blockIdx.x + (int)(i - 1) * (int)gridDim.x)) ok_all = false;
+    if (!ok_all && lane == 0) {
+      flag(err, 2u);
+      *abort_flag = 1;
+    }
+  }
+  __syncthreads();
+  // On an abort, let every copy and MMA this CTA issued land before shared
+  // memory and TMEM are released (bounded waits).
+  if (tid == 0 && *abort_flag) {
+    for (uint32_t q = *consumed; q < *issued; ++q) (void)tcg::mbar_wait(&full[q % L::NST], (q / L::NST) & 1);
+  }
+  if (tid == 32 && *abort_flag) {
+    tcg::mma_commit(drain);
+    (void)tcg::mbar_wait(drain, 0);
+  }
+  tcg::tc_fence_before();
+  __syncthreads();
+  if (warp == 1) tcg::tmem_dealloc(tmem, L::TMEM_COLS);
+}
+
 // ------------------------------------------------------------------ weight gradients
 // dW[t][n][k] += sum_r dZ[r][n] * X[r + t - taps/2][k]: one GEMM per tap whose
 // reduction runs over the rows, the outer dimension of both operands.  Both
@@ -732,6 +998,22 @@ cudaError_t launch_wgrad_t(const CUtensorMap &md, const CUtensorMap &mx, int row
   return cudaGetLastError();
 }
 
+template <int W>
+cudaError_t launch_mh_t(const CUtensorMap &ma, const CUtensorMap &m1, const CUtensorMap &m2, const float *b1,
+                        const float *b2, int rows, int lp, int klev, float *y, unsigned *err, int grid,
+                        cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e =
+        cudaFuncSetAttribute(mlp_head_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, MhLayout<W>::SMEM);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  mlp_head_kernel<W><<<grid, MH_THREADS, MhLayout<W>::SMEM, st>>>(ma, m1, m2, b1, b2, rows, lp, klev, y, err);
+  return cudaGetLastError();
+}
+static_assert(MhLayout<128>::SMEM <= WS_SMEM, "the fused kernel fits in shared memory");
+
 int g_impl = 0;  // 0: warp-specialised kernel, 1: the single-thread pipeline
 
 }  // namespace sg
@@ -836,5 +1118,32 @@ extern "C" int cs_wgrad_tc(const void *dz, const void *x, int32_t rows, int32_t 
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = k == 128 ? launch_wgrad_t<128>(md, mx, rows, chunk, nchunks, n, taps, dw, err, st)
                            : launch_wgrad_t<64>(md, mx, rows, chunk, nchunks, n, taps, dw, err, st);
+  return e == cudaSuccess ? CS_OK : CS_E_CUDA;
+}
+
+// The network's MLP layer and output head in one kernel (inference):
+// y = (SiLU(a w1^T + b1)) w2^T + b2, the hidden activation kept on chip
+// (mlp_head_kernel).  a [rows][k] bf16, w1 [k][k], w2 [64][k] bf16, y f32
+// [rows][64]; k 64 or 128; rows outside the levels of the lp/klev column
+// layout written as zero.
+extern "C" int cs_mlp_head(const void *a, const void *w1, const float *b1, const void *w2, const float *b2,
+                           int32_t rows, int32_t k, int32_t lp, int32_t klev, float *y, unsigned *err,
+                           void *stream) {
+  using namespace sg;
+  if (!a || !w1 || !w2 || !y || rows <= 0 || (k != 64 && k != 128)) return CS_E_ARG;
+  if (((uintptr_t)a | (uintptr_t)w1 | (uintptr_t)w2) & 15) return CS_E_ARG;
+  if ((uintptr_t)y & 31) return CS_E_ARG;
+  CUtensorMap ma, m1, m2;
+  if (!make_map(&ma, a, (uint64_t)rows, (uint64_t)k, (uint32_t)BM)) return CS_E_CUDA;
+  if (!make_map(&m1, w1, (uint64_t)k, (uint64_t)k, (uint32_t)k)) return CS_E_CUDA;
+  if (!make_map(&m2, w2, 64, (uint64_t)k, 64)) return CS_E_CUDA;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ntiles = (rows + BM - 1) / BM;
+  const int grid = ntiles < sms ? ntiles : sms;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = k == 128 ? launch_mh_t<128>(ma, m1, m2, b1, b2, rows, lp, klev, y, err, grid, st)
+                           : launch_mh_t<64>(ma, m1, m2, b1, b2, rows, lp, klev, y, err, grid, st);
   return e == cudaSuccess ? CS_OK : CS_E_CUDA;
 }

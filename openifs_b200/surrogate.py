@@ -223,8 +223,9 @@ class Net:
             G(B["x0"][:rows], self.wbf[1], E.EPI_SILU, W, 1, LP, KLEV, self.b[1], ha, stream=stream)
             G(ha[:rows], self.wbf[2], E.EPI_SILU, W, 5, LP, KLEV, self.b[2], hb, resid=ha, stream=stream)
             G(hb[:rows], self.wbf[3], E.EPI_SILU, W, 5, LP, KLEV, self.b[3], ha, resid=hb, stream=stream)
-            G(ha[:rows], self.wbf[4], E.EPI_SILU, W, 1, LP, KLEV, self.b[4], hb, stream=stream)
-            G(hb[:rows], self.wbf[5], E.EPI_LINEAR_F32, 64, 1, LP, KLEV, self.b[5], outf=B["y"], stream=stream)
+            # the MLP layer and the output head in one kernel: h4 stays on chip
+            E.mlp_head(ha[:rows], self.wbf[4], self.b[4], self.wbf[5], self.b[5], B["y"], LP, KLEV,
+                       stream=stream)
         return B["y"]
 
     def backward(self, B, rows):

@@ -56,3 +56,28 @@ def conv_gemm(a, w, epi, n, taps=1, lp=0, klev=0, bias=None, out=None, out_pre=N
     rc = _lib_fn()(ctypes.byref(d), s)
     if rc != 0:
         raise RuntimeError(f"cs_conv_gemm failed ({rc})")
+
+
+_mh = None
+
+
+def mlp_head(a, w1, b1, w2, b2, y, lp=0, klev=0, err=None, stream=None):
+    """y = SiLU(a @ w1.T + b1) @ w2.T + b2 in one kernel (cs_mlp_head): the
+    hidden activation stays on chip.  a: [rows, k] bf16; w1: [k, k] (or
+    [1, k, k]) and w2: [64, k] (or [1, 64, k]) bf16; b1 [k], b2 [64] f32 or
+    None; y: f32 with at least rows rows of 64."""
+    global _mh
+    import torch
+    if _mh is None:
+        L = cloudsc.lib()
+        vp, i32 = ctypes.c_void_p, ctypes.c_int32
+        L.cs_mlp_head.argtypes = [vp, vp, vp, vp, vp, i32, i32, i32, i32, vp, vp, vp]
+        L.cs_mlp_head.restype = ctypes.c_int
+        _mh = L.cs_mlp_head
+    rows, k = a.shape
+    if y.shape[-1] != 64 or y.numel() < rows * 64:
+        raise ValueError("y must hold rows x 64 floats")
+    s = torch.cuda.current_stream().cuda_stream if stream is None else stream
+    rc = _mh(_p(a), _p(w1), _p(b1), _p(w2), _p(b2), rows, k, lp, klev, _p(y), _p(err), s)
+    if rc != 0:
+        raise RuntimeError(f"cs_mlp_head failed ({rc})")

@@ -108,6 +108,35 @@ def test_weight_gradient_rejects_bad_shapes(cuda):
     assert L.cs_wgrad_tc(a.data_ptr() + 2, a.data_ptr(), 256, 128, 128, 1, dw.data_ptr(), None, None) != 0
 
 
+@pytest.mark.parametrize("width,rows", [(128, 5 * 144 + 37), (64, 3 * 144), (128, 64)])
+def test_fused_mlp_head_equals_two_kernels(cuda, width, rows):
+    """cs_mlp_head (the MLP layer's SiLU output kept in shared memory and fed
+    to the output head's MMAs) gives the two-kernel result bit for bit:
+    cs_conv_gemm with the SiLU epilogue, then with the linear f32 one; the
+    padding rows of the column layout zero in both; the error word clear."""
+    import torch
+    from openifs_b200 import tcgemm as E
+    rng = np.random.default_rng(width + rows)
+    a = torch.from_numpy(rng.standard_normal((rows, width)).astype(np.float32)).bfloat16().cuda()
+    w1 = torch.from_numpy(0.1 * rng.standard_normal((1, width, width)).astype(np.float32)).bfloat16().cuda()
+    w2 = torch.from_numpy(0.1 * rng.standard_normal((1, 64, width)).astype(np.float32)).bfloat16().cuda()
+    b1 = torch.from_numpy(rng.standard_normal(width).astype(np.float32)).cuda()
+    b2 = torch.from_numpy(rng.standard_normal(64).astype(np.float32)).cuda()
+    h = torch.empty(rows, width, dtype=torch.bfloat16, device="cuda")
+    y_ref = torch.full((rows, 64), 7.0, device="cuda")
+    E.conv_gemm(a, w1, E.EPI_SILU, width, 1, S.LP, S.KLEV, b1, h)
+    E.conv_gemm(h, w2, E.EPI_LINEAR_F32, 64, 1, S.LP, S.KLEV, b2, outf=y_ref)
+    y = torch.full((rows, 64), 7.0, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    E.mlp_head(a, w1, b1, w2, b2, y, S.LP, S.KLEV, err=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(y, y_ref)
+    pos = torch.arange(rows, device="cuda") % S.LP
+    pad = (pos < 2) | (pos >= 2 + S.KLEV)
+    assert bool((y[pad] == 0).all()) and float(y[~pad].abs().max()) > 0
+
+
 @pytest.fixture(scope="module")
 def small_data(cuda):
     p, _ = util.params()
