@@ -324,7 +324,12 @@ int cloudsc_b200_batched_host_sp(
  * 16 MiB are reserved on a device when cloudsc_b200_setup uploads the
  * parameters there (for another device: at the first call of any entry on
  * it), so a caller that reserves its own GPU memory pool should call
- * cloudsc_b200_setup first and leave room for them.
+ * cloudsc_b200_setup first and leave room for them.  The same set-up also
+ * reserves the kernels' per-thread local memory (it raises the CUDA stack
+ * size limit to the largest kernel's frame, about 2.6 KB, never lowering
+ * it): the driver holds that for every thread the device can run, which it
+ * would otherwise take at the first launch (measured on a B200: set-up takes
+ * 542 MiB with the fixed array, and the first call then none).
  */
 int cloudsc_b200_block_noalloc(
     const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,

@@ -28,6 +28,7 @@ int num_variants();
 int default_variant();
 void variant_bounds(int v, int *maxt, int *minb);
 cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes);
+cudaError_t max_local_bytes(size_t *out);
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream, bool gen);
 bool params_allow_gen(const cloudsc_params &p, const Derived &d);
@@ -166,6 +167,20 @@ int ensure_params(int *dev_out) {
     void *scratch = nullptr;
     e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
     if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaGetSymbolAddress(no-allocation array)", e);
+    // Reserve the column kernels' local memory now, not at their first
+    // launch: the driver sizes it as the per-thread stack times the threads
+    // the device can hold (about half a GB on a B200 for a 2.6 KB frame), so
+    // raise the stack limit to the largest kernel's frame (never lower it).
+    size_t need = 0, cur = 0;
+    e = max_local_bytes(&need);
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaFuncGetAttributes(column kernels)", e);
+    e = cudaDeviceGetLimit(&cur, cudaLimitStackSize);
+    if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "cudaDeviceGetLimit(stack size)", e);
+    if (cur < need) {
+      e = cudaDeviceSetLimit(cudaLimitStackSize, need);
+      if (e != cudaSuccess)
+        return fail(CLOUDSC_E_CUDA, "reserving the column kernels' local memory (cudaDeviceSetLimit, stack size)", e);
+    }
     g_dev_gen[dev] = g_gen_count;
   }
   return CLOUDSC_OK;

@@ -395,6 +395,33 @@ cudaError_t variant_attributes(int precision, int v, int *regs, int *local_bytes
   return cudaSuccess;
 }
 
+// The largest local memory (stack frame) per thread of any column kernel:
+// the spill slots and the fast pass's copy of the PLUDE inputs.
+cudaError_t max_local_bytes(size_t *out) {
+  size_t m = 0;
+  auto see = [&](const void *k) -> cudaError_t {
+    if (!k) return cudaSuccess;
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, k);
+    if (e == cudaSuccess && a.localSizeBytes > m) m = a.localSizeBytes;
+    return e;
+  };
+  for (int v = 0; v < kNumVariants; ++v)
+    for (int g = 0; g < 2; ++g)
+      for (int f = 0; f < 2; ++f) {
+        for (int prec = 0; prec <= 5; ++prec) {
+          cudaError_t e = see(kernel_ptr(prec, v, g != 0, f != 0));
+          if (e != cudaSuccess) return e;
+        }
+        for (int prec = 0; prec <= 2; ++prec) {
+          cudaError_t e = see(kernel_ptr_sp(prec, v, g != 0, f != 0));
+          if (e != cudaSuccess) return e;
+        }
+      }
+  *out = m;
+  return cudaSuccess;
+}
+
 // Launch variant v of the kernel: precision 0 = FP64, 1 = FP32-mixed,
 // 2 = FP32 physics, 3-5 the FP64 forms with budgets / SPP and inhomogeneity;
 // gen: the parameters allow the GEN kernels (forms 0-2 otherwise run the

@@ -70,6 +70,40 @@ def test_noalloc_takes_no_device_memory(cuda):
     assert got["nw"][0] >= 0 and got["nw"][1] >= 0
 
 
+@pytest.mark.gpu
+def test_noalloc_first_call_after_setup_takes_no_device_memory(cuda):
+    """In a fresh process, the device's free memory right after
+    cloudsc_b200_setup equals the free memory after the first no-allocation
+    call: set-up has already reserved the fixed array and the column kernels'
+    local memory, so a caller may reserve the rest of the GPU for its own
+    pool between the two."""
+    import os
+    import subprocess
+    import sys
+    script = """
+import numpy as np, torch
+from openifs_b200 import cloudsc, inputs
+from tests import util
+torch.cuda.init(); torch.zeros(1, device="cuda"); torch.cuda.synchronize()
+p, _ = util.params()
+blk = {k: v[0].copy() for k, v in inputs.generate(1, 64, p, seed=45).items()}
+cloudsc.setup(p)
+torch.cuda.synchronize()
+f0 = torch.cuda.mem_get_info()[0]
+nw = cloudsc.cloudsc_block_noalloc(p, 1, 64, 64, util.KLEV, util.PTSPHY, blk)
+torch.cuda.synchronize()
+f1 = torch.cuda.mem_get_info()[0]
+print("FREE", f0, f1, nw)
+"""
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", script], cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = [ln for ln in r.stdout.splitlines() if ln.startswith("FREE")][-1]
+    _, f0, f1, nw = line.split()
+    assert int(f1) == int(f0), (f0, f1)
+    assert int(nw) >= 0
+
+
 def test_noalloc_rejects_blocks_above_capacity(built):
     p = cloudsc.default_params()
     try:
