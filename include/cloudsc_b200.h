@@ -90,7 +90,11 @@ typedef struct cloudsc_params {
   int32_t ncldtop;
   /* switches that select code paths; the values the B200 kernels implement
    * are the reference defaults noted beside each (others -> CLOUDSC_E_UNSUPPORTED) */
-  int32_t laericeauto, laericesed, laerliqautolsp, laerliqcoll; /* all 0 (NAERCLD=0) */
+  int32_t laericeauto, laericesed, laerliqautolsp, laerliqcoll; /* any: LAERICESED, LAERICEAUTO FP64 (their
+                                                                  arrays required); LAERLIQAUTOLSP and
+                                                                  LAERLIQCOLL act only under IWARMRAIN = 1
+                                                                  (cloudsc.F90:1985,2020), which the
+                                                                  reference fixes at 3 (:727): no effect */
   int32_t lcloud_inhomog;                                       /* any (FP64) */
   int32_t lcldbudc, lcldbudl, lcldbudi, lcldbudt, lcldbud_vertint; /* any: budgets to PEXTRA, FP64 */
   int32_t lcldbud_timeint;                                      /* any */
@@ -163,7 +167,9 @@ int cloudsc_b200_setup(const cloudsc_params *p);
  * pgp2dspp, plcrit_aer, picrit_aer, pre_ice, pccn, pnice, pfsd, pextra.  With
  * a cloud budget switch on (LCLDBUD*), the budget diagnostics are added to
  * PEXTRA(KIDIA:KFDIA,:,1:KFLDX) and the inputs the sections that are on read
- * are required (see cloudsc_b200_batched_diag).
+ * are required (see cloudsc_b200_batched_diag); likewise PRE_ICE with
+ * LAERICESED and PICRIT_AER, PNICE with LAERICEAUTO (PLCRIT_AER and PCCN are
+ * never read: see the aerosol switches in cloudsc_params).
  */
 int cloudsc_b200_block(
     const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
@@ -494,10 +500,13 @@ int cloudsc_b200_satadj_increment_batched(
  * fields of cloudsc_params, cloudsc.F90:850-939); the cloud-inhomogeneity
  * paths (LCLOUD_INHOMOG: autoconversion/accretion enhancement from the
  * liquid FSD, :1937-2098; LRAD_CLOUD_INHOMOG: PFSD, :3819-3823, 4112-4125,
- * 4307-4359).  The same arrays as cloudsc_b200_batched, then the inputs
- * only these read: PVFA, PDYNA, PDYNL, PDYNI, PDYNS, PHRSW, PHRLW (budgets),
- * PGAW (NPROMA, NGPBLKS; inhomogeneity), KCTOP, KPBLTYPE (vertical-integral
- * budget), PGP2DSPP (NPROMA, NRFTOTAL, NGPBLKS; SPP), PFSD (NPROMA, KLEV,
+ * 4307-4359); the aerosol-aware ice fall speed (LAERICESED, :1798-1803) and
+ * ice-to-snow autoconversion (LAERICEAUTO, :2776-2779).  The same arrays as
+ * cloudsc_b200_batched, then the inputs only these read: PVFA, PDYNA, PDYNL,
+ * PDYNI, PDYNS, PHRSW, PHRLW (budgets), PGAW (NPROMA, NGPBLKS;
+ * inhomogeneity), KCTOP, KPBLTYPE (vertical-integral budget), PGP2DSPP
+ * (NPROMA, NRFTOTAL, NGPBLKS; SPP), PRE_ICE (NPROMA, KLEV, NGPBLKS;
+ * LAERICESED), PICRIT_AER and PNICE (NPROMA, KLEV, NGPBLKS; LAERICEAUTO), PFSD (NPROMA, KLEV,
  * NGPBLKS; written with LRAD_CLOUD_INHOMOG), PEXTRA (NPROMA, KLEV, KFLDX,
  * NGPBLKS, INOUT: the budgets are added to it); arrays of options that are
  * off may be NULL.  CLOUDSC_E_SHAPE when KFLDX is below the
@@ -527,7 +536,8 @@ int cloudsc_b200_batched_diag(
     double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
     const double *pvfa, const double *pdyna, const double *pdynl, const double *pdyni,
     const double *pdyns, const double *phrsw, const double *phrlw, const double *pgaw,
-    const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp, double *pfsd,
+    const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp, const double *pre_ice,
+    const double *picrit_aer, const double *pnice, double *pfsd,
     double *pextra, int32_t kfldx, uint32_t *ncounters, void *stream);
 
 /* Bytes of the fixed device array cloudsc_b200_block_noalloc works in. */

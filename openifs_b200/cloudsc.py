@@ -63,8 +63,9 @@ def lib():
         L.cloudsc_b200_set_schedule.restype = ctypes.c_int
         L.cloudsc_b200_get_schedule.argtypes = [i32, pi32, pi32, pi32]
         L.cloudsc_b200_get_schedule.restype = ctypes.c_int
+        from .fields import DIAG_FIELDS
         L.cloudsc_b200_batched_diag.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
-                                                [vp] * (len(BATCHED_FIELDS) + 13) + [i32, vp, vp])
+                                                [vp] * (len(BATCHED_FIELDS) + len(DIAG_FIELDS)) + [i32, vp, vp])
         L.cloudsc_b200_batched_diag.restype = ctypes.c_int
         from .fields import SATADJ_FIELDS
         ns = len(SATADJ_FIELDS)
@@ -385,7 +386,8 @@ def sltend_supersat_batched(params, arrays, nproma, klev, ngpblks, ngptot, tsphy
 
 def cloudsc_batched_diag(params, arrays, diag, nproma, klev, ngpblks, ngptot, ptsphy, counter=None, stream=None):
     """cloudsc_batched (FP64) with the optional configurations the params
-    switch on (budget diagnostics, SPP, cloud inhomogeneity): ``diag`` holds
+    switch on (budget diagnostics, SPP, cloud inhomogeneity, the aerosol
+    switches LAERICESED and LAERICEAUTO): ``diag`` holds
     the fields.DIAG_FIELDS device tensors (those of options that are off may
     be omitted); PEXTRA, (NGPBLKS, KFLDX, KLEV, NPROMA), is added to and PFSD
     written in place."""

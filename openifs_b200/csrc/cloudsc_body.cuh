@@ -723,8 +723,13 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       }
 
       // 4.1 fall speeds (:1783-1844), sedimentation (:1852-1877)
-      const Real fs_i = (spp && P.spp_on[CLOUDSC_SPP_FALLSPEED]) ? P.rvice * Real(sppf[CLOUDSC_SPP_FALLSPEED])
-                                                                 : P.rvice;  // :1806-1808
+      Real fs_i0 = P.rvice;
+      if constexpr (OPT) {
+        // LAERICESED: 0.002 ZRE_ICE**1.0 from the ice effective radius (:1798-1803)
+        if (P.laericesed) fs_i0 = C(0.002) * Real(ld(F.pre_ice + ok));
+      }
+      const Real fs_i = (spp && P.spp_on[CLOUDSC_SPP_FALLSPEED]) ? fs_i0 * Real(sppf[CLOUDSC_SPP_FALLSPEED])
+                                                                 : fs_i0;  // :1806-1808
       const Real fs_s = P.rvsnow;
       Real fs_r = C(0.0);
       {
@@ -927,7 +932,18 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       if (t <= P.rtt && zicecld > zepsec) {
         Real zzco = rdt * P.rsnowlin1 * mexp<F32M>(P.rsnowlin2 * (t - P.rtt));
         Real zlcrit = P.rlcritsnow;
-        if (spp && P.spp_on[CLOUDSC_SPP_RLCRITSNOW]) zlcrit = P.rlcritsnow * Real(sppf[CLOUDSC_SPP_RLCRITSNOW]);
+        bool aer = false;
+        if constexpr (OPT) {
+          // LAERICEAUTO: the aerosol's critical ice amount, the rate scaled by
+          // (RNICE/PNICE)**0.333 (:2776-2779)
+          if (P.laericeauto) {
+            zlcrit = Real(ld(F.picrit_aer + ok));
+            zzco = zzco * mpow<F32M>(DIV(P.rnice, Real(ld(F.pnice + ok))), C(0.333));
+            aer = true;
+          }
+        }
+        if (!aer && spp && P.spp_on[CLOUDSC_SPP_RLCRITSNOW])
+          zlcrit = P.rlcritsnow * Real(sppf[CLOUDSC_SPP_RLCRITSNOW]);
         Real r = DIV(zicecld, zlcrit);
         Real ztemp = C(-1.) * (r * r);
         Real zsnowaut = (ztemp < C(50.0)) ? zzco * (C(1.0) - mexp<F32M>(ztemp)) : zzco;

@@ -88,18 +88,22 @@ int drained(int rc, std::initializer_list<cudaStream_t> streams) {
   return rc;
 }
 
-bool params_supported(const cloudsc_params &p) {
-  if (p.laericeauto || p.laericesed || p.laerliqautolsp || p.laerliqcoll) return false;
-  return true;
+// SPP, a cloud-inhomogeneity path or an aerosol switch that acts is on: the
+// FP64 form with them runs.  (LAERLIQAUTOLSP and LAERLIQCOLL act only under
+// IWARMRAIN = 1, cloudsc.F90:1985-1989, 2020-2023; IWARMRAIN is 3, :727, so
+// those two change nothing and need no form of their own.)
+bool opt_on(const cloudsc_params &p) {
+  return p.lspp || p.lcloud_inhomog || p.lrad_cloud_inhomog || p.laericesed || p.laericeauto;
 }
-
-// SPP or a cloud-inhomogeneity path is on: the FP64 form with them runs.
-bool opt_on(const cloudsc_params &p) { return p.lspp || p.lcloud_inhomog || p.lrad_cloud_inhomog; }
 
 // Inputs of the SPP / inhomogeneity form: PGP2DSPP (KLON, NRFTOTAL) when a
 // perturbation is on (its MP, and MP+1 for CLOUDINHOM, within NRFTOTAL),
 // PGAW with an inhomogeneity path, PFSD with LRAD_CLOUD_INHOMOG.
-int opt_args_ok(const cloudsc_params &p, const void *pgaw, const void *pgp2dspp, const void *pfsd) {
+int opt_args_ok(const cloudsc_params &p, const void *pgaw, const void *pgp2dspp, const void *pfsd,
+                const void *pre_ice, const void *picrit_aer, const void *pnice) {
+  if (p.laericesed && !pre_ice) return fail(CLOUDSC_E_NULL, "LAERICESED is on: PRE_ICE is required");
+  if (p.laericeauto && (!picrit_aer || !pnice))
+    return fail(CLOUDSC_E_NULL, "LAERICEAUTO is on: PICRIT_AER and PNICE are required");
   if (p.lspp)
     for (int n = 0; n < 8; ++n) {
       if (!p.spp_on[n]) continue;
@@ -408,9 +412,6 @@ int cloudsc_b200_setup(const cloudsc_params *p) {
   if (!p) return fail(CLOUDSC_E_NULL, "params is NULL");
   if (p->magic != CLOUDSC_PARAMS_MAGIC || p->version != 1)
     return fail(CLOUDSC_E_PARAMS, "bad params magic or version");
-  if (!params_supported(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED,
-                "an aerosol switch (LAERICEAUTO, LAERICESED, LAERLIQAUTOLSP, LAERLIQCOLL) is on; this build does not implement them");
   if (p->ncldtop < 2) return fail(CLOUDSC_E_SHAPE, "ncldtop must be >= 2");
   const bool gen = params_allow_gen(*p, make_derived(*p));
   {
@@ -499,6 +500,7 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
   // thread calls cloudsc_b200_setup meanwhile.
   Schedule sc;
   bool bud = false, opt = false, need_gaw = false, need_spp = false, need_fsd = false, gen = true;
+  bool need_re = false, need_icrit = false;
   {
     std::lock_guard<std::mutex> lk(g_mu);
     sc = g_sched[precision];
@@ -508,6 +510,8 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
       opt = opt_on(g_params);
       need_gaw = g_params.lcloud_inhomog || g_params.lrad_cloud_inhomog;
       need_fsd = g_params.lrad_cloud_inhomog;
+      need_re = g_params.laericesed;
+      need_icrit = g_params.laericeauto;
       if (g_params.lspp)
         for (int n = 0; n < 8; ++n) need_spp = need_spp || g_params.spp_on[n];
     }
@@ -515,13 +519,15 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
   int form = precision;
   if (bud || opt) {
     if (precision != 0)
-      return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics, SPP and the inhomogeneity paths are FP64 only");
+      return fail(CLOUDSC_E_UNSUPPORTED,
+                  "the budget diagnostics, SPP, the inhomogeneity paths and the aerosol switches are FP64 only");
     if (bud && !f.pextra)
       return fail(CLOUDSC_E_UNSUPPORTED, "the budget diagnostics need PEXTRA: use cloudsc_b200_batched_diag "
                                          "or cloudsc_b200_block");
-    if ((need_gaw && !f.pgaw) || (need_spp && !f.pgp2dspp) || (need_fsd && !f.pfsd))
-      return fail(CLOUDSC_E_UNSUPPORTED, "SPP and the inhomogeneity paths need PGP2DSPP, PGAW and PFSD: use "
-                                         "cloudsc_b200_batched_diag or cloudsc_b200_block");
+    if ((need_gaw && !f.pgaw) || (need_spp && !f.pgp2dspp) || (need_fsd && !f.pfsd) || (need_re && !f.pre_ice) ||
+        (need_icrit && (!f.picrit_aer || !f.pnice)))
+      return fail(CLOUDSC_E_UNSUPPORTED, "SPP, the inhomogeneity paths and the aerosol switches need their "
+                                         "arrays: use cloudsc_b200_batched_diag or cloudsc_b200_block");
     form = bud && opt ? 5 : (opt ? 4 : 3);
   }
   // parameters that rule out the GEN kernels, and more than kMaxLevFast
@@ -553,7 +559,7 @@ int cloudsc_b200_batched(
   if (rc) return rc;
   if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   if (budgets_on(*p) || opt_on(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_batched_diag "
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP, the inhomogeneity paths and the aerosol switches: use cloudsc_b200_batched_diag "
                                        "or cloudsc_b200_block");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
@@ -594,8 +600,8 @@ int cloudsc_b200_batched_diag(
     double *pfplsn, double *pfhpsl, double *pfhpsn, const double *pvfa, const double *pdyna,
     const double *pdynl, const double *pdyni, const double *pdyns, const double *phrsw,
     const double *phrlw, const double *pgaw, const int32_t *kctop, const int32_t *kpbltype,
-    const double *pgp2dspp, double *pfsd, double *pextra, int32_t kfldx, uint32_t *ncounters,
-    void *stream) {
+    const double *pgp2dspp, const double *pre_ice, const double *picrit_aer, const double *pnice,
+    double *pfsd, double *pextra, int32_t kfldx, uint32_t *ncounters, void *stream) {
   int rc = check_params_match(p);
   if (rc) return rc;
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
@@ -617,7 +623,7 @@ int cloudsc_b200_batched_diag(
     if (rc) return rc;
   }
   if (opt_on(*p)) {
-    rc = opt_args_ok(*p, pgaw, pgp2dspp, pfsd);
+    rc = opt_args_ok(*p, pgaw, pgp2dspp, pfsd, pre_ice, picrit_aer, pnice);
     if (rc) return rc;
   }
   rc = ensure_params(nullptr);
@@ -628,7 +634,7 @@ int cloudsc_b200_batched_diag(
               pclv, pcovptot, prainfrac_toprfz, pfsqlf, pfsqif, pfcqnng, pfcqlng, pfsqrf, pfsqsf,
               pfcqrng, pfcqsng, pfsqltur, pfsqitur, pfplsl, pfplsn, pfhpsl, pfhpsn, ncounters,
               pvfa, pdyna, pdynl, pdyni, pdyns, phrsw, phrlw, kctop, kpbltype, pextra, kfldx,
-              pgaw, pgp2dspp, pfsd, p->spp_nrftotal};
+              pgaw, pgp2dspp, pfsd, p->spp_nrftotal, pre_ice, picrit_aer, pnice};
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
   return launch_checked(0, f, sh, (cudaStream_t)stream);
 }
@@ -933,7 +939,7 @@ int batched_args_ok(const cloudsc_params *p, int32_t nproma, int32_t klev, int32
   if (rc) return rc;
   if (precision < 0 || precision > 2) return fail(CLOUDSC_E_SHAPE, "precision must be 0, 1 or 2");
   if (budgets_on(*p) || opt_on(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_block "
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP, the inhomogeneity paths and the aerosol switches: use cloudsc_b200_block "
                                        "or cloudsc_b200_batched_diag");
   if (nproma < 1 || klev < 2 || ngpblks < 1 || ngptot < 1 ||
       (long long)ngptot > (long long)nproma * ngpblks || ngptot <= (long long)nproma * (ngpblks - 1))
@@ -965,8 +971,8 @@ int cloudsc_b200_block(
     double *pfsqif, double *pfcqnng, double *pfcqlng, double *pfsqrf, double *pfsqsf,
     double *pfcqrng, double *pfcqsng, double *pfsqltur, double *pfsqitur, double *pfplsl,
     double *pfplsn, double *pfhpsl, double *pfhpsn, double *pextra, int32_t kfldx) {
-  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)ldslphy; (void)plcrit_aer;
-  (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice;
+  // PLCRIT_AER and PCCN are read only under IWARMRAIN = 1 (see opt_on)
+  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)ldslphy; (void)plcrit_aer; (void)pccn;
   int rc = check_params_match(p);
   if (rc) return rc;
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
@@ -988,7 +994,7 @@ int cloudsc_b200_block(
     if (rc) return rc;
   }
   if (opt) {
-    rc = opt_args_ok(*p, pgaw, pgp2dspp, pfsd);
+    rc = opt_args_ok(*p, pgaw, pgp2dspp, pfsd, pre_ice, picrit_aer, pnice);
     if (rc) return rc;
   }
   int dev = 0;
@@ -1000,10 +1006,11 @@ int cloudsc_b200_block(
   const size_t s2b = np * kl * 8, nx = bud ? (size_t)kfldx : 0;
   const size_t base = (bytes + 255) / 256 * 256;
   const size_t extra = bud ? 7 * s2b + 2 * ((np * 4 + 255) / 256 * 256) + nx * s2b : 0;
-  // with SPP / inhomogeneity: PGAW, PGP2DSPP (KLON, NRFTOTAL), PFSD after that
+  // with SPP / inhomogeneity / aerosol: PGAW, PGP2DSPP (KLON, NRFTOTAL),
+  // PFSD, then PRE_ICE, PICRIT_AER, PNICE after that
   const size_t nrf = opt && p->lspp ? (size_t)p->spp_nrftotal : 0;
   const size_t gawb = (np * 8 + 255) / 256 * 256, sppb = (np * nrf * 8 + 255) / 256 * 256;
-  const size_t extra2 = opt ? gawb + sppb + s2b : 0;
+  const size_t extra2 = opt ? gawb + sppb + s2b + 3 * s2b : 0;
   rc = t_ws.prepare(dev, base + extra + extra2);
   if (rc) return rc;
   void *d[42];
@@ -1048,6 +1055,13 @@ int cloudsc_b200_block(
     dfsd = pfsd ? (double *)b : nullptr;
     f.pfsd = dfsd;
     f.nrftotal = p->spp_nrftotal;
+    b += s2b;
+    const double *av[3] = {pre_ice, picrit_aer, pnice};
+    const double **adst[3] = {&f.pre_ice, &f.picrit_aer, &f.pnice};
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i, b += s2b) {
+      *adst[i] = av[i] ? (const double *)b : nullptr;
+      if (av[i]) e = cudaMemcpyAsync(b, av[i], s2b, cudaMemcpyHostToDevice, s);
+    }
     if (e != cudaSuccess) return drained(fail(CLOUDSC_E_CUDA, "host-to-device copy", e), {s});
   }
   Shape sh = {klon, klev, 1, kfdia, kidia - 1, ptsphy};
@@ -1199,7 +1213,7 @@ int cloudsc_b200_block_noalloc(
   int rc = check_params_match(p);
   if (rc) return rc;
   if (budgets_on(*p) || opt_on(*p))
-    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP and the inhomogeneity paths: use cloudsc_b200_block "
+    return fail(CLOUDSC_E_UNSUPPORTED, "budgets, SPP, the inhomogeneity paths and the aerosol switches: use cloudsc_b200_block "
                                        "or cloudsc_b200_batched_diag");
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia)
     return fail(CLOUDSC_E_SHAPE, "inconsistent KIDIA/KFDIA/KLON/KLEV");
@@ -1268,7 +1282,6 @@ namespace {
 int satadj_shape_ok(const cloudsc_params *p, double ptsphy) {
   int rc = check_params_match(p);
   if (rc) return rc;
-  if (!params_supported(*p)) return fail(CLOUDSC_E_UNSUPPORTED, "a parameter switch this build lacks is on");
   if (!(ptsphy > 0.0)) return fail(CLOUDSC_E_SHAPE, "PTSPHY must be positive");
   return CLOUDSC_OK;
 }

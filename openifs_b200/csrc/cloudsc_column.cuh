@@ -286,6 +286,10 @@ struct KParams {
   Real ra, rcloud_frac_std, spp_mu[16], spp_xmag[16];
   int lspp, lcloud_inhomog, lrad_cloud_inhomog, spp_lramidlimit1, spp_on[8], spp_mp[8];
   int ncldtop, lmfdsnow;
+  // aerosol-aware ice sedimentation and ice-to-snow autoconversion
+  // (LAERICESED, LAERICEAUTO; cloudsc.F90:1798-1803, 2776-2779)
+  Real rnice;
+  int laericesed, laericeauto;
 };
 
 // Double-precision copy of the scalars the FP64 stages (solve, supersaturation

@@ -44,6 +44,10 @@ struct Fields {
   const double *pgp2dspp;  // (NPROMA, NRFTOTAL) per block
   double *pfsd;            // (NPROMA, KLEV) per block, written with LRAD_CLOUD_INHOMOG
   int nrftotal;
+  // read only with the aerosol switches (same form): (NPROMA, KLEV) per block
+  const double *pre_ice;     // LAERICESED: ice effective radius
+  const double *picrit_aer;  // LAERICEAUTO: critical ice amount
+  const double *pnice;       // LAERICEAUTO: ice number concentration
 };
 
 // Pointers of the batched arrays of the single-precision interface

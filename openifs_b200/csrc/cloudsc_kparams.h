@@ -58,6 +58,9 @@ inline void fill_kparams(const cloudsc_params &p, const Derived &d, KParams<Real
   }
   k.ncldtop = p.ncldtop;
   k.lmfdsnow = p.lmfdsnow;
+  k.rnice = Real(p.rnice);
+  k.laericesed = p.laericesed;
+  k.laericeauto = p.laericeauto;
 }
 
 

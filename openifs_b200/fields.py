@@ -230,6 +230,9 @@ DIAG_FIELDS = [
     ("kctop", "1d", np.int32, "in"),
     ("kpbltype", "1d", np.int32, "in"),
     ("pgp2dspp", "spp", np.float64, "in"),
+    ("pre_ice", "2d", np.float64, "in"),
+    ("picrit_aer", "2d", np.float64, "in"),
+    ("pnice", "2d", np.float64, "in"),
     ("pfsd", "2d", np.float64, "out"),
     ("pextra", "extra", np.float64, "inout"),
 ]

@@ -291,7 +291,10 @@ def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None, nrft
     2e-5 K/s), PHRLW ~ N(-2e-5, 1e-5 K/s); KCTOP a level index 1..KLEV on the
     convective columns, 0 elsewhere; KPBLTYPE in 0..3; PEXTRA ~ N(0, 1) (it is
     INOUT: the diagnostics add to it); PGAW ~ U(1e-7, 3e-6) (grid boxes of
-    about 7-40 km); PGP2DSPP ~ N(0, 1) on ``nrftotal`` fields; PFSD zero (an
+    about 7-40 km); PGP2DSPP ~ N(0, 1) on ``nrftotal`` fields; PRE_ICE ~
+    U(20, 120) um (ice effective radius: 0.04-0.24 m/s fall speed, around the
+    default RVICE = 0.13); PICRIT_AER ~ U(1e-5, 1e-4) kg/kg (around RLCRITSNOW
+    = 3e-5); PNICE ~ RNICE exp(N(0, 1)) (around RNICE = 0.027); PFSD zero (an
     output)."""
     nb = base["pt"].shape[0]
     ids = list(range(nb)) if blocks is None else list(blocks)
@@ -302,6 +305,9 @@ def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None, nrft
     out["pextra"] = np.zeros((nb, kfldx, klev, nproma))
     out["pgaw"] = np.zeros((nb, nproma))
     out["pgp2dspp"] = np.zeros((nb, nrftotal, nproma))
+    out["pre_ice"] = np.zeros(shp2)
+    out["picrit_aer"] = np.zeros(shp2)
+    out["pnice"] = np.zeros(shp2)
     out["pfsd"] = np.zeros(shp2)
     for j, ib in enumerate(ids):
         rng = np.random.default_rng([int(seed), int(ib), 13])
@@ -319,6 +325,10 @@ def generate_diag(base, nproma, kfldx, klev=KLEV_L137, seed=1, blocks=None, nrft
         out["pextra"][j] = rng.normal(0.0, 1.0, (kfldx, klev, nproma))
         out["pgaw"][j] = rng.uniform(1e-7, 3e-6, nproma)
         out["pgp2dspp"][j] = rng.normal(0.0, 1.0, (nrftotal, nproma))
+        ra = np.random.default_rng([int(seed), int(ib), 17])  # the aerosol inputs' own stream
+        out["pre_ice"][j] = ra.uniform(20.0, 120.0, shp)
+        out["picrit_aer"][j] = ra.uniform(1e-5, 1e-4, shp)
+        out["pnice"][j] = 0.027 * np.exp(ra.normal(0.0, 1.0, shp))
     return out
 
 

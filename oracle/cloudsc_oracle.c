@@ -155,10 +155,6 @@ static void supersatcheck(const cloudsc_params *p, int kidia, int kfdia, int kft
   }
 }
 
-static int params_supported(const cloudsc_params *p) {
-  if (p->laericeauto || p->laericesed || p->laerliqautolsp || p->laerliqcoll) return 0;
-  return 1;
-}
 
 /* SPP factor EXP(MU(i+1) + XMAG(i+1)*PGP2DSPP(JL, MP + off)) of perturbation
  * n (cloudsc.F90:1692,1807,2106-2107,2283,2347,2782,3289). */
@@ -188,11 +184,12 @@ int oracle_cloudsc(
     double *pfsqsf, double *pfcqrng, double *pfcqsng, double *pfsqltur,
     double *pfsqitur, double *pfplsl, double *pfplsn, double *pfhpsl, double *pfhpsn,
     double *pextra, int kfldx) {
-  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)ldslphy; (void)plcrit_aer;
-  (void)picrit_aer; (void)pre_ice; (void)pccn; (void)pnice;
+  /* PLCRIT_AER and PCCN are read only by LAERLIQAUTOLSP and LAERLIQCOLL,
+     whose code sits in the IWARMRAIN = 1 branch (:1985-1989, :2020-2023);
+     IWARMRAIN is 3 (:727), so those two switches change nothing. */
+  (void)lddiag; (void)pdynr; (void)pvervel; (void)pgeom; (void)ldslphy; (void)plcrit_aer; (void)pccn;
 
   if (!p || p->magic != CLOUDSC_PARAMS_MAGIC) return CLOUDSC_E_PARAMS;
-  if (!params_supported(p)) return CLOUDSC_E_UNSUPPORTED;
   if (kidia < 1 || kfdia > klon || kidia > kfdia || klev < 2) return CLOUDSC_E_SHAPE;
   const int ncldtop = p->ncldtop;
   if (ncldtop < 2 || ncldtop > klev) return CLOUDSC_E_SHAPE;
@@ -213,6 +210,8 @@ int oracle_cloudsc(
   }
   const int linhom = p->lcloud_inhomog || p->lrad_cloud_inhomog;
   if (linhom && !pgaw) return CLOUDSC_E_NULL;
+  /* aerosol-aware ice sedimentation and ice-to-snow autoconversion */
+  if ((p->laericesed && !pre_ice) || (p->laericeauto && (!picrit_aer || !pnice))) return CLOUDSC_E_NULL;
   if (p->lrad_cloud_inhomog && !pfsd) return CLOUDSC_E_NULL;
   const int lbud = p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint;
   if (lbud) {
@@ -620,6 +619,8 @@ int oracle_cloudsc(
       double zrlambda = pow(A1(zrho, jl) * ztemp / p->rcl_lam1r, p->rcl_lam2r);
       L2(zfallspeed, jl, NCLDQR) =
           p->rxfallspeedrain * zfallcorr * p->rcl_const7r * pow(zrlambda, p->rcl_dr);
+      if (p->laericesed) /* :1798-1803, ZRE_ICE**1.0 = ZRE_ICE */
+        L2(zfallspeed, jl, NCLDQI) = 0.002 * A2(pre_ice, jl, jk);
       if (SPP_ON(CLOUDSC_SPP_FALLSPEED)) /* :1806-1808 */
         L2(zfallspeed, jl, NCLDQI) =
             L2(zfallspeed, jl, NCLDQI) * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_FALLSPEED, 0, 0);
@@ -843,7 +844,10 @@ int oracle_cloudsc(
         if (A1(zicecld, jl) > zepsec) {
           double zzco = ptsphy * p->rsnowlin1 * exp(p->rsnowlin2 * (t - p->rtt));
           double zlcrit = p->rlcritsnow;
-          if (SPP_ON(CLOUDSC_SPP_RLCRITSNOW)) /* :2781-2783 */
+          if (p->laericeauto) { /* :2776-2779 */
+            zlcrit = A2(picrit_aer, jl, jk);
+            zzco = zzco * pow(p->rnice / A2(pnice, jl, jk), 0.333);
+          } else if (SPP_ON(CLOUDSC_SPP_RLCRITSNOW)) /* :2781-2783 */
             zlcrit = p->rlcritsnow * spp_fac(p, pgp2dspp, klon, jl, CLOUDSC_SPP_RLCRITSNOW, 0, 0);
           double r = A1(zicecld, jl) / zlcrit;
           double ztemp = -1. * (r * r);
@@ -1584,7 +1588,6 @@ int oracle_cloud_satadj(
     double *ptendency_loc_t, double *ptendency_loc_q, double *ptendency_loc_a,
     double *ptendency_loc_l, double *ptendency_loc_i) {
   (void)ktype; (void)lddiag; (void)pmfu; (void)pmfd;
-  if (!params_supported(p)) return CLOUDSC_E_UNSUPPORTED;
   if (klon < 1 || klev < 2 || kidia < 1 || kfdia > klon || kidia > kfdia) return CLOUDSC_E_SHAPE;
   const int ncldtop = p->ncldtop;
   const double zqtmst = 1.0 / ptsphy; /* :291 */
@@ -1893,8 +1896,9 @@ int oracle_sltend_supersat_batched(
 
 /* The block loop of oracle_cloudsc_batched with the arrays the optional
  * configurations read or write (PVFA, PDYNA/L/I/S, PHRSW, PHRLW, PGAW, KCTOP,
- * KPBLTYPE, PGP2DSPP (NPROMA, NRFTOTAL, NGPBLKS), PFSD, PEXTRA (NPROMA, KLEV,
- * KFLDX, NGPBLKS), INOUT). */
+ * KPBLTYPE, PGP2DSPP (NPROMA, NRFTOTAL, NGPBLKS), PRE_ICE, PICRIT_AER, PNICE
+ * (NPROMA, KLEV, NGPBLKS), PFSD, PEXTRA (NPROMA, KLEV, KFLDX, NGPBLKS),
+ * INOUT). */
 int oracle_cloudsc_batched_diag(
     const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
     double ptsphy, const double *pt, const double *pq, const double *ptendency_cml_t,
@@ -1911,6 +1915,7 @@ int oracle_cloudsc_batched_diag(
     double *pfhpsn, const double *pvfa, const double *pdyna, const double *pdynl,
     const double *pdyni, const double *pdyns, const double *phrsw, const double *phrlw,
     const double *pgaw, const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp,
+    const double *pre_ice, const double *picrit_aer, const double *pnice,
     double *pfsd, double *pextra, int kfldx, int nthreads) {
   if (nproma < 1 || ngpblks < 1 || ngptot < 1 || ngptot > nproma * ngpblks ||
       ngptot <= nproma * (ngpblks - 1))
@@ -1938,7 +1943,8 @@ int oracle_cloudsc_batched_diag(
         kpbltype ? kpbltype + o1 : NULL, (double *)(peis + o1), plu + o, plude + o, pludeli + o * 4,
         psnde + o * 2, pmfu + o, pmfd + o,
         pgp2dspp ? pgp2dspp + o1 * (size_t)(p->spp_nrftotal > 0 ? p->spp_nrftotal : 0) : NULL, 0, pa + o,
-        pclv + o * NCLV, NULL, NULL, NULL, NULL, NULL, pcovptot + o, pfsd ? pfsd + o : NULL, prainfrac_toprfz + o1, pfsqlf + ib * s2h, pfsqif + ib * s2h,
+        pclv + o * NCLV, NULL, picrit_aer ? picrit_aer + o : NULL, pre_ice ? pre_ice + o : NULL, NULL,
+        pnice ? pnice + o : NULL, pcovptot + o, pfsd ? pfsd + o : NULL, prainfrac_toprfz + o1, pfsqlf + ib * s2h, pfsqif + ib * s2h,
         pfcqnng + ib * s2h, pfcqlng + ib * s2h, pfsqrf + ib * s2h, pfsqsf + ib * s2h, pfcqrng + ib * s2h,
         pfcqsng + ib * s2h, pfsqltur + ib * s2h, pfsqitur + ib * s2h, pfplsl + ib * s2h,
         pfplsn + ib * s2h, pfhpsl + ib * s2h, pfhpsn + ib * s2h, pextra ? pextra + ib * sx : NULL, kfldx);

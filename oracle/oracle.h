@@ -109,6 +109,7 @@ int oracle_cloudsc_batched_diag(
     double *pfhpsn, const double *pvfa, const double *pdyna, const double *pdynl,
     const double *pdyni, const double *pdyns, const double *phrsw, const double *phrlw,
     const double *pgaw, const int32_t *kctop, const int32_t *kpbltype, const double *pgp2dspp,
+    const double *pre_ice, const double *picrit_aer, const double *pnice,
     double *pfsd, double *pextra, int kfldx, int nthreads);
 
 /* The supersaturation adjustment of SLTEND (sltend.F90:380-410), one block

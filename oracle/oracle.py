@@ -33,7 +33,7 @@ def lib(libm="glibc"):
         if not os.path.exists(LIB_PATHS[libm]):
             build()
         from openifs_b200.params import CloudscParams
-        from openifs_b200.fields import BATCHED_FIELDS
+        from openifs_b200.fields import BATCHED_FIELDS, DIAG_FIELDS
         L = ctypes.CDLL(LIB_PATHS[libm])
         P = ctypes.POINTER(CloudscParams)
         vp = ctypes.c_void_p
@@ -50,7 +50,7 @@ def lib(libm="glibc"):
                                                   [vp] * len(SATADJ_FIELDS) + [i32])
         L.oracle_cloud_satadj_batched.restype = i32
         L.oracle_cloudsc_batched_diag.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +
-                                                  [vp] * (len(BATCHED_FIELDS) + 13) + [i32, i32])
+                                                  [vp] * (len(BATCHED_FIELDS) + len(DIAG_FIELDS)) + [i32, i32])
         L.oracle_cloudsc_batched_diag.restype = i32
         from openifs_b200.fields import SLTEND_FIELDS
         L.oracle_sltend_supersat_batched.argtypes = ([P, i32, i32, i32, i32, ctypes.c_double] +

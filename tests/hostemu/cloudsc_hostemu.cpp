@@ -221,12 +221,14 @@ extern "C" int hostemu_batched_diag(const cloudsc_params *p, int nproma, int kle
   const double **bd = (const double **)b;
   f.pvfa = bd[0]; f.pdyna = bd[1]; f.pdynl = bd[2]; f.pdyni = bd[3]; f.pdyns = bd[4];
   f.phrsw = bd[5]; f.phrlw = bd[6]; f.pgaw = bd[7]; f.kctop = (const int32_t *)b[8];
-  f.kpbltype = (const int32_t *)b[9]; f.pgp2dspp = bd[10]; f.pfsd = (double *)b[11];
-  f.pextra = (double *)b[12];
+  f.kpbltype = (const int32_t *)b[9]; f.pgp2dspp = bd[10];
+  f.pre_ice = bd[11]; f.picrit_aer = bd[12]; f.pnice = bd[13];
+  f.pfsd = (double *)b[14];
+  f.pextra = (double *)b[15];
   f.kfldx = kfldx;
   f.nrftotal = p->spp_nrftotal;
   const bool bud = p->lcldbudc || p->lcldbudl || p->lcldbudi || p->lcldbudt || p->lcldbud_vertint;
-  const bool opt = p->lspp || p->lcloud_inhomog || p->lrad_cloud_inhomog;
+  const bool opt = p->lspp || p->lcloud_inhomog || p->lrad_cloud_inhomog || p->laericesed || p->laericeauto;
   Shape sh = {nproma, klev, ngpblks, ngptot, 0, ptsphy};
   for (int ib = 0; ib < ngpblks; ++ib) {
     int icend = ngptot - ib * nproma;

@@ -176,9 +176,10 @@ def test_budget_diagnostics_bit_exact(pp, flags):
 
 @pytest.mark.parametrize("case", util.OPT_CASES)
 def test_spp_inhomogeneity_bit_exact(pp, case):
-    """SPP perturbations, LCLOUD_INHOMOG and LRAD_CLOUD_INHOMOG (PFSD), alone
-    and together with the budgets: the kernel's OPT form on the host against
-    the oracle, every output and PFSD/PEXTRA bit for bit, both libms."""
+    """SPP perturbations, LCLOUD_INHOMOG and LRAD_CLOUD_INHOMOG (PFSD), the
+    aerosol switches (PRE_ICE, PICRIT_AER, PNICE), alone and together with the
+    budgets: the kernel's OPT form on the host against the oracle, every
+    output and PFSD/PEXTRA bit for bit, both libms."""
     p0, po0 = pp
     p, po = util.opt_params(p0, case), util.opt_params(po0, case)
     nproma, nblk = 32, 6

@@ -3,10 +3,12 @@ and the oracle's (oracle_params.c) agree bit for bit, and both reproduce
 hand-derived values of the SUCLDP / SUPHEC / YOMCST formulas."""
 import math
 
+import numpy as np
 import pytest
 
 from openifs_b200 import cloudsc, inputs
 from oracle import oracle
+from tests import util
 
 
 @pytest.fixture(scope="module")
@@ -80,13 +82,23 @@ def test_ncldtop_l137():
     assert lib.cloudsc_b200_ncldtop(137, np.ascontiguousarray(stpre).ctypes.data, 100.0) == nc
 
 
-def test_unsupported_switches_rejected(pp, built):
-    """The aerosol switches (NAERCLD > 0) are the only ones the kernels do
-    not implement; every other CLOUDSC switch is accepted."""
-    p, _ = pp
+def test_aerosol_switches_accepted(pp, built):
+    """Every CLOUDSC switch is accepted, the four aerosol switches (NAERCLD >
+    0) included.  LAERLIQAUTOLSP and LAERLIQCOLL act only in the IWARMRAIN = 1
+    branch (cloudsc.F90:1985-1989, 2020-2023) and IWARMRAIN is fixed at 3
+    (:727): with them on, the oracle's outputs are the default's bit for bit,
+    PLCRIT_AER and PCCN unread."""
+    p, po = pp
     for name in ("laericeauto", "laericesed", "laerliqautolsp", "laerliqcoll"):
-        q = p.copy()
-        setattr(q, name, 1)
-        with pytest.raises(cloudsc.CloudscError) as e:
+        q = util.with_flags(p, {name: 1})
+        try:
             cloudsc.setup(q)
-        assert e.value.code == -3, name
+        except cloudsc.CloudscError as e:  # without a GPU the upload fails (-4) after the checks
+            assert e.code == -4, (name, e.code)
+    arrs = inputs.generate(3, 32, p, seed=8)
+    ref, nw = util.run_oracle(po, arrs, 32, 3, 90)
+    qo = util.with_flags(po, {"laerliqautolsp": 1, "laerliqcoll": 1})
+    got, nw2 = util.run_oracle(qo, arrs, 32, 3, 90)
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, got[n]), util.defined(n, ref[n])), n
+    assert nw == nw2

@@ -289,7 +289,10 @@ def with_spp(p, lramidlimit1=1, nrftotal=10):
     return q
 
 
-OPT_CASES = ["spp", "inhomog", "radinhomog", "all", "all+budgets"]
+OPT_CASES = ["spp", "inhomog", "radinhomog", "aerosol", "all", "all+budgets"]
+# the four aerosol switches (NAERCLD > 0); LAERLIQAUTOLSP and LAERLIQCOLL act
+# only under IWARMRAIN = 1, which the reference does not use
+AEROSOL = {"laericesed": 1, "laericeauto": 1, "laerliqautolsp": 1, "laerliqcoll": 1}
 
 
 def opt_params(p, case):
@@ -300,7 +303,9 @@ def opt_params(p, case):
         return with_flags(p, {"lcloud_inhomog": 1})
     if case == "radinhomog":
         return with_flags(p, {"lrad_cloud_inhomog": 1})
-    q = with_flags(with_spp(p, lramidlimit1=0), {"lcloud_inhomog": 1, "lrad_cloud_inhomog": 1})
+    if case == "aerosol":
+        return with_flags(p, AEROSOL)
+    q = with_flags(with_spp(p, lramidlimit1=0), dict({"lcloud_inhomog": 1, "lrad_cloud_inhomog": 1}, **AEROSOL))
     if case == "all+budgets":
         q = with_flags(q, BUDGET_CASES[-1])
     return q
