@@ -18,6 +18,11 @@
 // recording in divbad_ the operands outside its exact window; IEEE division
 // otherwise (cdiv, cloudsc_column.cuh).
 #define DIV(...) cdiv<FAST_>(__VA_ARGS__, divbad_)
+// A literal divisor: its reciprocal folded at compile time (cdivk).
+#define DIVK(A, B) cdivk<FAST_>(A, B, 1.0 / (B), divbad_)
+// A power-of-two literal divisor: multiplication by its exact reciprocal,
+// the same bits as the division for every operand.
+#define DIV2(A, B) ((A) * decltype(A)(1.0 / (B)))
 
 namespace cloudsc {
 
@@ -842,7 +847,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         Real zrhc = zxramid;
         Real zsigk = DIV(pap_k, Real(paph_surf));
         if (zsigk > C(0.8)) {
-          Real s = DIV((zsigk - C(0.8)), C(0.2));
+          Real s = DIVK((zsigk - C(0.8)), 0.2);
           zrhc = zxramid + (C(1.0) - zxramid) * (s * s);
         }
         zzrh = mn(zrhc, zzrh);
@@ -856,7 +861,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           const PowBase b_lam = mbase<F32M>(zlambda);
           Real zevap_denom = P.rcl_cdenom1 * zesatliq - P.rcl_cdenom2 * t * zesatliq +
                              P.rcl_cdenom3 * mpow<F32M>(t, C(3.0)) * pap_k;
-          Real zcorr2 = DIV(mpow<F32M>(DIV(t, C(273.)), C(1.5)) * C(393.), (t + C(120.)));
+          Real zcorr2 = DIV(mpow<F32M>(DIVK(t, 273.), C(1.5)) * C(393.), (t + C(120.)));
           Real zsubsat = mx(zzrh * zqsliq - zqe, C(0.0));
           Real zbeta = (DIV(C(0.15), zqsliq)) * (t * t) * zesatliq * P.rcl_const1r * (DIV(zcorr2, zevap_denom)) *
                        (DIV(C(0.78), (mpowbp<F32M, GEN>(b_lam, P.rcl_const4r))) +
@@ -889,7 +894,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           Real zinew = mpow<F32M>(C(0.666) * zcvds * rdt + mpow<F32M>(zice0, C(0.666)), C(1.5));
           D zdepos = D(mx(P.rcl_overlapliqice * a * (zinew - zice0), C(0.0)));
           zdepos = mn(zdepos, qxfg_l);
-          Real zinfactor = mn(DIV(zicenuclei, C(15000.)), C(1.0));
+          Real zinfactor = mn(DIVK(zicenuclei, 15000.), C(1.0));
           zdepos = zdepos * D(mn(zinfactor + (C(1.0) - zinfactor) *
                                                (P.rdepliqrefrate + DIV(zcldtopdist, P.rdepliqrefdepth)),
                                C(1.0)));
@@ -910,7 +915,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           Real zvpice = DIV((P.r2es * ei_e) * P.rv, P.rd);
           Real zaplusb = P.rcl_apb1 * zvpice - P.rcl_apb2 * zvpice * t + pap_k * P.rcl_apb3 * (t * t * t);
           Real zcorrfac = mpow<F32M>(DIV(C(1.0), zrho), C(0.5));
-          Real zcorrfac2 = (mpow<F32M>(DIV(t, C(273.0)), C(1.5))) * (DIV(C(393.0), (t + C(120.0))));
+          Real zcorrfac2 = (mpow<F32M>(DIVK(t, 273.0), C(1.5))) * (DIV(C(393.0), (t + C(120.0))));
           Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
           const PowBase b_pr02 = mbase<F32M>(zpr02);
           Real zterm1 = DIV(zsupersatice * (t * t) * zvpice * zcorrfac2 * P.rcl_const2s, (zrho * zaplusb));
@@ -1035,7 +1040,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (zsnowcld > zepsec) {
           Real zlams = mpowp<F32M, GEN>(DIV(P.rcl_lam1s, (zrho * zsnowcld)), P.rcl_lam2s);
           Real zn0s = P.rcl_x1s;
-          Real zfalldiff = mx(xabs(fs_r - fs_s), DIV((fs_r + fs_s), C(8.)));
+          Real zfalldiff = mx(xabs(fs_r - fs_s), DIV2((fs_r + fs_s), C(8.)));
           Real zfac = DIV(P.rpi * P.rpi * P.rdenswat * zrho * zn0r * zn0s, (zlams * zlamr3));
           Real zrat = DIV(zlamr, zlams);
           Real zpsacr =
@@ -1046,7 +1051,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (zicecld > zepsec) {
           Real zlami = mpowp<F32M, GEN>(DIV(P.rcl_lam1s, (zrho * zicecld)), P.rcl_lam2s);
           Real zn0i = P.rcl_x1s;
-          Real zfalldiff = mx(xabs(fs_r - fs_i), DIV((fs_r + fs_i), C(8.)));
+          Real zfalldiff = mx(xabs(fs_r - fs_i), DIV2((fs_r + fs_i), C(8.)));
           Real zfac = DIV(P.rpi * P.rpi * P.rdenswat * C(0.1) * zrho * zn0r * zn0i, (zlami * zlamr3));
           Real zrat = DIV(zlamr, zlami);
           Real zpiacr =
@@ -1372,5 +1377,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 }
 
 #undef DIV
+#undef DIVK
+#undef DIV2
 
 }  // namespace cloudsc

@@ -125,6 +125,47 @@ CSC_DEV double fast_div(double a, double b, DivCheck &dc) {
 #endif
 }
 
+// fast_div for a literal divisor b, given y = RN(1/b) folded at compile
+// time (IEEE division of two constants): only the two residual corrections
+// and the dividend's window test remain.  Exact as fast_div is: every such
+// divisor lies in the window and has no all-ones significand, so y is the
+// correctly rounded reciprocal Markstein's theorem needs.
+CSC_DEV double fast_div_k(double a, double b, double y, DivCheck &dc) {
+#if defined(__CUDA_ARCH__)
+  const int ha = __double2hiint(a);
+  const double aa = fabs(a);
+  const double q0 = __dmul_rn(aa, y);
+  double r = __fma_rn(-b, q0, aa);
+  const double q1 = __fma_rn(r, y, q0);
+  r = __fma_rn(-b, q1, aa);
+  const double q = __fma_rn(r, y, q1);
+  dc.acc |= a == 0.0 ? 0u : (unsigned)ha * 2u - kDivBase;
+  return __hiloint2double(__double2hiint(q) ^ (ha & (int)0x80000000), __double2loint(q));
+#else
+  (void)y;
+#if defined(CLOUDSC_HOST_FORCE_REDO)
+  dc.acc = ~0u;
+#else
+  (void)dc;
+#endif
+  return a / b;
+#endif
+}
+
+// a / b for a literal b (y = 1/b folded): fast_div_k when FAST and the
+// quotient is a double; IEEE otherwise.
+template <bool FAST, typename A>
+CSC_DEV auto cdivk(A a, double b, double y, DivCheck &dc) -> decltype(a / A(b)) {
+  typedef decltype(a / A(b)) T;
+  if constexpr (FAST && std::is_same<T, double>::value) {
+    return fast_div_k(double(a), b, y, dc);
+  } else {
+    (void)dc;
+    (void)y;
+    return a / A(b);
+  }
+}
+
 // Passes of the column code (cloudsc_column's PASS): plain, IEEE division
 // throughout; fast, the branch-free fast_div, recording operands outside its
 // exact window; redo, the rerun with IEEE division of a column whose fast
