@@ -23,6 +23,8 @@
 // A power-of-two literal divisor: multiplication by its exact reciprocal,
 // the same bits as the division for every operand.
 #define DIV2(A, B) ((A) * decltype(A)(1.0 / (B)))
+// A parameter divisor with its reciprocal computed on the host (KParams rcp_*).
+#define DIVP(A, B, Y) cdivk<FAST_>(A, B, Y, divbad_)
 
 namespace cloudsc {
 
@@ -347,6 +349,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 #define C(x) Real(x)
   constexpr bool FAST_ = PASS == kPassFast;
   DivCheck divbad_;
+  if constexpr (FAST_) {
+    if (P.rcp_force) divbad_.acc = ~0u;  // a parameter divisor fast_div_k cannot take: rerun
+  }
   const int np = sh.nproma, klev = sh.klev;
   const size_t s2 = (size_t)np * klev, s2h = (size_t)np * (klev + 1);
   const size_t o2 = (size_t)ib * s2 + jl, o2h = (size_t)ib * s2h + jl, o1 = (size_t)ib * np + jl;
@@ -741,7 +746,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         Real ztemp = C(0.5) * (qr + qxnm1_r);
         if (ztemp != C(0.0)) {
           Real zfallcorr = fallcorr_r;
-          Real zrlambda = mpowp<F32M, GEN>(DIV(zrho * ztemp, P.rcl_lam1r), P.rcl_lam2r);
+          Real zrlambda = mpowp<F32M, GEN>(DIVP(zrho * ztemp, P.rcl_lam1r, P.rcp_rcl_lam1r), P.rcl_lam2r);
           fs_r = P.rxfallspeedrain * zfallcorr * P.rcl_const7r * mpowp<F32M, GEN>(zrlambda, P.rcl_dr);
         }
       }
@@ -856,7 +861,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (zcovpclr > zepsec && zraincldm1 > zepsec && zqe < zzrh * zqsliq) {
           Real zpreclr = zraincldm1;
           Real zfallcorr = fallcorr_f;
-          Real zesatliq = DIV(P.rv, P.rd) * (P.r2es * el_e);
+          Real zesatliq = P.rv_rd * (P.r2es * el_e);
           Real zlambda = mpowp<F32M, GEN>(DIV(P.rcl_lam1r, (zrho * zpreclr)), P.rcl_lam2r);
           const PowBase b_lam = mbase<F32M>(zlambda);
           Real zevap_denom = P.rcl_cdenom1 * zesatliq - P.rcl_cdenom2 * t * zesatliq +
@@ -885,7 +890,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         }
         if (t < (P.rtt - C(5.)) && qxfg_l > P.rlmin) {
           Real zsupersatice = DIV((zqsliq - zqsice), zqsice);
-          Real zvpice = DIV((P.r2es * ei_e) * P.rv, P.rd);
+          Real zvpice = DIVP((P.r2es * ei_e) * P.rv, P.rd, P.rcp_rd);
           Real zicenuclei = C(1000.0) * mexp<F32M>(C(12.96) * zsupersatice - C(0.639));
           Real zadd = DIV(P.rlstt * (DIV(P.rlstt, (P.rv * t)) - C(1.0)), (C(2.4E-2) * t));
           Real zbdd = DIV(P.rv * t * pap_k, (C(2.21) * zvpice));
@@ -896,7 +901,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           zdepos = mn(zdepos, qxfg_l);
           Real zinfactor = mn(DIVK(zicenuclei, 15000.), C(1.0));
           zdepos = zdepos * D(mn(zinfactor + (C(1.0) - zinfactor) *
-                                               (P.rdepliqrefrate + DIV(zcldtopdist, P.rdepliqrefdepth)),
+                                               (P.rdepliqrefrate + DIVP(zcldtopdist, P.rdepliqrefdepth, P.rcp_rdepliqrefdepth)),
                                C(1.0)));
           QSUB(LI, zdepos);  // (I,L) += zdepos, (L,I) -= zdepos
           qxfg_i = qxfg_i + zdepos;
@@ -912,7 +917,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       {
         Real zsupersatice = mx(DIV((qv - zqsmix), zqsmix), C(0.0));
         if (t < P.rtt && zsnowcld > zepsec && zsupersatice > C(0.0)) {
-          Real zvpice = DIV((P.r2es * ei_e) * P.rv, P.rd);
+          Real zvpice = DIVP((P.r2es * ei_e) * P.rv, P.rd, P.rcp_rd);
           Real zaplusb = P.rcl_apb1 * zvpice - P.rcl_apb2 * zvpice * t + pap_k * P.rcl_apb3 * (t * t * t);
           Real zcorrfac = mpow<F32M>(DIV(C(1.0), zrho), C(0.5));
           Real zcorrfac2 = (mpow<F32M>(DIVK(t, 273.0), C(1.5))) * (DIV(C(393.0), (t + C(120.0))));
@@ -964,7 +969,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           Real zsubsat = mx(zqsice - qv, C(0.0));
           Real ztdmtw0 = t - P.rtt -
                          zsubsat * (C(1329.31) + C(0.0074615) * (pap_k - C(0.85E5)) - C(40.637) * (t - C(275.0)));
-          Real zcons1 = xabs(DIV(rdt * (C(1.0) + C(0.5) * ztdmtw0), P.rtaumel));
+          Real zcons1 = xabs(DIVP(rdt * (C(1.0) + C(0.5) * ztdmtw0), P.rtaumel, P.rcp_rtaumel));
           zmeltmax = mx(ztdmtw0 * zcons1 * P.zrldcp, C(0.0));
         }
         if (zmeltmax > zepsec && zicetot > zepsec) {
@@ -1001,7 +1006,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
             Real zfrz = rdt * (DIV(P.rcl_const5r, zrho)) * (mexp<F32M>(ztemp) - C(1.)) * mpowp<F32M, GEN>(zlambda, P.rcl_const6r);
             zfrzmax = mx(zfrz, C(0.0));
           } else {
-            Real zcons1 = xabs(DIV(rdt * (C(1.0) + C(0.5) * (P.rtt - t)), P.rtaumel));
+            Real zcons1 = xabs(DIVP(rdt * (C(1.0) + C(0.5) * (P.rtt - t)), P.rtaumel, P.rcp_rtaumel));
             zfrzmax = mx((P.rtt - t) * zcons1 * P.zrldcp, C(0.0));
           }
           if (zfrzmax > zepsec) {
@@ -1070,7 +1075,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (zcovpclr > zepsec && qxfg_s > zepsec && zqe < zzrh * zqsice) {
           Real aa = zcovptot * zdtgdp;
           Real zpreclr = DIV(Real(qxfg_s) * zcovpclr, xsign(mx(xabs(aa), zepsilon), aa));
-          Real zbeta1 = DIV(DIV(xsqrt(DIV(pap_k, Real(paph_surf))), P.rvrfactor) * zpreclr, mx(zcovpclr, zepsec));
+          Real zbeta1 = DIV(DIVP(xsqrt(DIV(pap_k, Real(paph_surf))), P.rvrfactor, P.rcp_rvrfactor) * zpreclr, mx(zcovpclr, zepsec));
           Real zbeta = P.rg * P.rpecons * mpow<F32M>(zbeta1, C(0.5777));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsice;
           Real zdpr = DIV(zcovpclr * zbeta * (zqsice - zqe), zdenom) * zdp * P.zrg_r;
@@ -1379,5 +1384,6 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 #undef DIV
 #undef DIVK
 #undef DIV2
+#undef DIVP
 
 }  // namespace cloudsc

@@ -331,6 +331,13 @@ struct KParams {
   // (LAERICESED, LAERICEAUTO; cloudsc.F90:1798-1803, 2776-2779)
   Real rnice;
   int laericesed, laericeauto;
+  // Divisions by parameters: RV/RD in the working precision, and the
+  // correctly rounded reciprocals of the parameter divisors, for fast_div_k.
+  // rcp_force: one of those divisors is outside fast_div's window or has an
+  // all-ones significand, and every column takes the IEEE rerun.
+  Real rv_rd;
+  double rcp_rd, rcp_rtaumel, rcp_rcl_lam1r, rcp_rdepliqrefdepth, rcp_rvrfactor;
+  int rcp_force;
 };
 
 // Double-precision copy of the scalars the FP64 stages (solve, supersaturation

@@ -1,5 +1,7 @@
 // Host-side conversion of cloudsc_params into the kernels' constant blocks.
 #pragma once
+#include <cstdint>
+#include <cstring>
 #include "cloudsc_column.cuh"
 
 namespace cloudsc {
@@ -61,6 +63,26 @@ inline void fill_kparams(const cloudsc_params &p, const Derived &d, KParams<Real
   k.rnice = Real(p.rnice);
   k.laericesed = p.laericesed;
   k.laericeauto = p.laericeauto;
+  // RV/RD with the division the kernels would perform (IEEE, in Real)
+  k.rv_rd = Real(p.rv) / Real(p.rd);
+  // 1/b correctly rounded (IEEE on the host) for each parameter divisor;
+  // usable by fast_div_k only inside its window and without an all-ones
+  // significand (the conditions of fast_div)
+  bool ok = true;
+  auto rcp = [&ok](double b) {
+    uint64_t u;
+    std::memcpy(&u, &b, 8);
+    const unsigned e = (unsigned)((u >> 52) & 0x7ff);
+    const bool ones = (u & ((1ull << 52) - 1)) == ((1ull << 52) - 1);
+    ok = ok && e >= 767u && e <= 1278u && !ones;
+    return 1.0 / b;
+  };
+  k.rcp_rd = rcp(p.rd);
+  k.rcp_rtaumel = rcp(p.rtaumel);
+  k.rcp_rcl_lam1r = rcp(p.rcl_lam1r);
+  k.rcp_rdepliqrefdepth = rcp(p.rdepliqrefdepth);
+  k.rcp_rvrfactor = rcp(p.rvrfactor);
+  k.rcp_force = ok ? 0 : 1;
 }
 
 

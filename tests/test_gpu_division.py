@@ -220,3 +220,27 @@ def test_kernel_reruns_columns_with_reported_divisions(cuda, nproma, nblk, cut):
         assert np.array_equal(a, b), n
         assert np.isfinite(b).all(), n
     assert nwg == nw
+
+
+@pytest.mark.parametrize("name,value", [("rtaumel", float(np.nextafter(8192.0, 0.0))),
+                                        ("rd", float(np.nextafter(256.0, 0.0))),
+                                        ("rdepliqrefdepth", float(np.nextafter(512.0, 0.0)))])
+def test_kernel_parameter_divisor_outside_fast_path(cuda, name, value):
+    """The kernels divide by five parameters with reciprocals computed on the
+    host.  A parameter they cannot take that way (here an all-ones
+    significand, near the parameter's physical value) makes every column take
+    the IEEE rerun: the FP64 kernel still equals the oracle bit for bit."""
+    p, po = util.params()
+    p = util.with_flags(p, {name: value})
+    po = util.with_flags(po, {name: value})
+    nproma, nblk = 32, 6
+    arrs = inputs.generate(nblk, nproma, p, seed=29)
+    ngptot = nproma * nblk - 5
+    ref, nw = util.run_oracle(po, arrs, nproma, nblk, ngptot)
+    gpu, nwg = util.run_gpu(p, arrs, nproma, nblk, ngptot)
+    for n in util.COMPARED:
+        a = util.defined(n, util._valid_cols(gpu[n], ngptot, nproma))
+        b = util.defined(n, util._valid_cols(ref[n], ngptot, nproma))
+        assert np.array_equal(a, b), n
+        assert np.isfinite(b).all(), n
+    assert nwg == nw
