@@ -170,7 +170,35 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp, double &t
 // one field.  ZPIEVAP, ZPRACS and ZPRACI are zero in this configuration
 // (ISUBLICE = 0, PRACS and PRACI off); the KTYPE/KPBLTYPE == IS+1 tests are
 // as written at :3925,3929.
+//
+// Every slot one level updates is distinct (the entry points require KLEV >=
+// 84 with the vertical integral, so IK never reaches the next field), and a
+// slot is updated at most once per level.  Each group of updates therefore
+// loads all its old values before it stores any: the compiler cannot move a
+// load above the store before it by itself (the slots lie a run-time
+// multiple of NPROMA apart), and one update after another would wait a full
+// memory round trip each.  The additions and their operands are the
+// reference's, one rounding each, so the values are unchanged.
 // ---------------------------------------------------------------------------
+template <int N>
+CSC_DEV void px_add(double *px, const size_t (&o)[N], const double (&v)[N]) {
+  double old[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) old[n] = px[o[n]];
+#pragma unroll
+  for (int n = 0; n < N; ++n) px[o[n]] = old[n] + v[n];
+}
+// the same where update n happens only when c[n] holds
+template <int N>
+CSC_DEV void px_add_if(double *px, const size_t (&o)[N], const double (&v)[N], const bool (&c)[N]) {
+  double old[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) old[n] = px[o[n]];
+#pragma unroll
+  for (int n = 0; n < N; ++n)
+    if (c[n]) px[o[n]] = old[n] + v[n];
+}
+
 template <typename Real>
 CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double *cc, const double *bl,
                            const double *bi, size_t base, int np, int klev, int k, double dt, double zqtmst,
@@ -180,135 +208,136 @@ CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double
                            int kpbltype, int kctop, double peis) {
   double *px = F.pextra + base;
   const size_t sk = (size_t)np, sf = (size_t)np * klev;
-  // PEXTRA(JL, IK, IS) with 1-based IK and IS
-  auto X = [&](int ik, int is) -> double & { return px[(size_t)(is - 1) * sf + (size_t)(ik - 1) * sk]; };
+  // offset of PEXTRA(JL, IK, IS) with 1-based IK and IS
+  auto S = [&](int ik, int is) -> size_t { return (size_t)(is - 1) * sf + (size_t)(ik - 1) * sk; };
   int is = P.lbud23 ? 26 : 0;
   const double zdt = P.lcldbud_timeint ? dt : 1.0;
   const int jk = k + 1;
   if (P.lcldbud_vertint) {
     const double zdz = zdp / (zrho * double(P.rg));
-    X(4, is + 1) = X(4, is + 1) + cc[2] * zdz * zdt;
-    X(6, is + 1) = X(6, is + 1) + cc[3] * zdz * zdt;
-    X(7, is + 1) = X(7, is + 1) + (cc[4] + cc[6]) * zdz * zdt;
-    X(8, is + 1) = X(8, is + 1) + cc[5] * zdz * zdt;
-    X(9, is + 1) = X(9, is + 1) + cc[7] * zdz * zdt;
-    X(10, is + 1) = X(10, is + 1) + cc[12] * zdz * zdt;
-    X(11, is + 1) = X(11, is + 1) + pvfa * zdz * zdt;
-    X(12, is + 1) = X(12, is + 1) + pdyna * zdz * zdt;
-    X(14 + 5, is + 1) = X(14 + 5, is + 1) + bl[2] * zdz * zdt;
-    X(14 + 7, is + 1) = X(14 + 7, is + 1) + bl[3] * zdz * zdt;
-    X(14 + 8, is + 1) = X(14 + 8, is + 1) + (bl[4] + bl[6]) * zdz * zdt;
-    X(14 + 9, is + 1) = X(14 + 9, is + 1) + bl[5] * zdz * zdt;
-    X(14 + 10, is + 1) = X(14 + 10, is + 1) + bl[7] * zdz * zdt;
-    X(14 + 11, is + 1) = X(14 + 11, is + 1) + bl[11] * zdz * zdt;
-    X(14 + 12, is + 1) = X(14 + 12, is + 1) + bl[14] * zdz * zdt;
-    X(14 + 13, is + 1) = X(14 + 13, is + 1) + bl[15] * zdz * zdt;
-    X(14 + 14, is + 1) = X(14 + 14, is + 1) + bl[12] * zdz * zdt;
-    X(14 + 15, is + 1) = X(14 + 15, is + 1) + bl[13] * zdz * zdt;
-    X(14 + 16, is + 1) = X(14 + 16, is + 1) + bl[17] * zdz * zdt;
-    X(14 + 17, is + 1) = X(14 + 17, is + 1) + (bl[18] + bl[19]) * zdz * zdt;
-    X(14 + 18, is + 1) = X(14 + 18, is + 1) + bl[20] * zdz * zdt;
-    X(14 + 19, is + 1) = X(14 + 19, is + 1) + bl[21] * zdz * zdt;
-    X(14 + 20, is + 1) = X(14 + 20, is + 1) + 0.0 * zdz * zdt * zqtmst;
-    X(14 + 21, is + 1) = X(14 + 21, is + 1) + psacr * zdz * zdt * zqtmst;
-    X(14 + 22, is + 1) = X(14 + 22, is + 1) + 0.0 * zdz * zdt * zqtmst;
-    X(14 + 23, is + 1) = X(14 + 23, is + 1) + piacr * zdz * zdt * zqtmst;
-    X(14 + 24, is + 1) = X(14 + 24, is + 1) + pvfl * zdz * zdt;
-    X(14 + 25, is + 1) = X(14 + 25, is + 1) + pdynl * zdz * zdt;
-    X(39 + 5, is + 1) = X(39 + 5, is + 1) + bi[2] * zdz * zdt;
-    X(39 + 7, is + 1) = X(39 + 7, is + 1) + bi[3] * zdz * zdt;
-    X(39 + 8, is + 1) = X(39 + 8, is + 1) + (bi[4] + bi[6]) * zdz * zdt;
-    X(39 + 9, is + 1) = X(39 + 9, is + 1) + bi[5] * zdz * zdt;
-    X(39 + 10, is + 1) = X(39 + 10, is + 1) + bi[7] * zdz * zdt;
-    X(39 + 11, is + 1) = X(39 + 11, is + 1) + bi[11] * zdz * zdt;
-    X(39 + 12, is + 1) = X(39 + 12, is + 1) + (bi[12] + bi[13]) * zdz * zdt;
-    X(39 + 13, is + 1) = X(39 + 13, is + 1) + bi[14] * zdz * zdt;
-    X(39 + 14, is + 1) = X(39 + 14, is + 1) + bi[16] * zdz * zdt;
-    X(39 + 15, is + 1) = X(39 + 15, is + 1) + bi[17] * zdz * zdt;
-    X(39 + 16, is + 1) = X(39 + 16, is + 1) + psdep * zqtmst * zdz * zdt;
-    X(39 + 17, is + 1) = X(39 + 17, is + 1) + pvfi * zdz * zdt;
-    X(39 + 18, is + 1) = X(39 + 18, is + 1) + pdyni * zdz * zdt;
-    X(39 + 19, is + 1) = X(39 + 19, is + 1) + pdyns * zdz * zdt;
-    X(60, is + 1) = prainfrac;
-    if (ktype == 0) X(70, is + 1) = X(70, is + 1) + 1.0;
-    if (ktype == is + 1) X(71, is + 1) = X(71, is + 1) + 1.0;
-    if (ktype == 2) X(72, is + 1) = X(72, is + 1) + 1.0;
-    if (ktype == 3) X(73, is + 1) = X(73, is + 1) + 1.0;
-    if (kpbltype == 0) X(74, is + 1) = X(74, is + 1) + 1.0;
-    if (kpbltype == is + 1) X(75, is + 1) = X(75, is + 1) + 1.0;
-    if (kpbltype == 2) X(76, is + 1) = X(76, is + 1) + 1.0;
-    if (kpbltype == 3) X(77, is + 1) = X(77, is + 1) + 1.0;
-    X(78, is + 1) = X(78, is + 1) + peis;
-    if (peis > 6.0) X(79, is + 1) = X(79, is + 1) + 1.0;
-    if (peis > 8.0) X(80, is + 1) = X(80, is + 1) + 1.0;
-    if (peis > 10.0) X(81, is + 1) = X(81, is + 1) + 1.0;
-    if (ktype >= 2 && peis < double(P.reisthsc)) X(82, is + 1) = X(82, is + 1) + 1.0;
-    if (ktype > 0) X(83, is + 1) = double(kctop);
+    const int f = is + 1;
+    {
+      const size_t o[8] = {S(4, f), S(6, f), S(7, f), S(8, f), S(9, f), S(10, f), S(11, f), S(12, f)};
+      const double v[8] = {cc[2] * zdz * zdt,          cc[3] * zdz * zdt, (cc[4] + cc[6]) * zdz * zdt,
+                           cc[5] * zdz * zdt,          cc[7] * zdz * zdt, cc[12] * zdz * zdt,
+                           pvfa * zdz * zdt,           pdyna * zdz * zdt};
+      px_add(px, o, v);
+    }
+    {
+      const size_t o[11] = {S(14 + 5, f),  S(14 + 7, f),  S(14 + 8, f),  S(14 + 9, f),  S(14 + 10, f), S(14 + 11, f),
+                            S(14 + 12, f), S(14 + 13, f), S(14 + 14, f), S(14 + 15, f), S(14 + 16, f)};
+      const double v[11] = {bl[2] * zdz * zdt,  bl[3] * zdz * zdt,  (bl[4] + bl[6]) * zdz * zdt,
+                            bl[5] * zdz * zdt,  bl[7] * zdz * zdt,  bl[11] * zdz * zdt,
+                            bl[14] * zdz * zdt, bl[15] * zdz * zdt, bl[12] * zdz * zdt,
+                            bl[13] * zdz * zdt, bl[17] * zdz * zdt};
+      px_add(px, o, v);
+    }
+    {
+      const size_t o[9] = {S(14 + 17, f), S(14 + 18, f), S(14 + 19, f), S(14 + 20, f), S(14 + 21, f),
+                           S(14 + 22, f), S(14 + 23, f), S(14 + 24, f), S(14 + 25, f)};
+      const double v[9] = {(bl[18] + bl[19]) * zdz * zdt, bl[20] * zdz * zdt,
+                           bl[21] * zdz * zdt,            0.0 * zdz * zdt * zqtmst,
+                           psacr * zdz * zdt * zqtmst,    0.0 * zdz * zdt * zqtmst,
+                           piacr * zdz * zdt * zqtmst,    pvfl * zdz * zdt,
+                           pdynl * zdz * zdt};
+      px_add(px, o, v);
+    }
+    px[S(60, f)] = prainfrac;
+    {
+      const size_t o[15] = {S(39 + 5, f),  S(39 + 7, f),  S(39 + 8, f),  S(39 + 9, f),  S(39 + 10, f),
+                            S(39 + 11, f), S(39 + 12, f), S(39 + 13, f), S(39 + 14, f), S(39 + 15, f),
+                            S(39 + 16, f), S(39 + 17, f), S(39 + 18, f), S(39 + 19, f), S(78, f)};
+      const double v[15] = {bi[2] * zdz * zdt,           bi[3] * zdz * zdt,  (bi[4] + bi[6]) * zdz * zdt,
+                            bi[5] * zdz * zdt,           bi[7] * zdz * zdt,  bi[11] * zdz * zdt,
+                            (bi[12] + bi[13]) * zdz * zdt, bi[14] * zdz * zdt, bi[16] * zdz * zdt,
+                            bi[17] * zdz * zdt,          psdep * zqtmst * zdz * zdt,
+                            pvfi * zdz * zdt,            pdyni * zdz * zdt,  pdyns * zdz * zdt,
+                            peis};
+      px_add(px, o, v);
+    }
+    {
+      const size_t o[12] = {S(70, f), S(71, f), S(72, f), S(73, f), S(74, f), S(75, f),
+                            S(76, f), S(77, f), S(79, f), S(80, f), S(81, f), S(82, f)};
+      const double v[12] = {1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1.0};
+      const bool c[12] = {ktype == 0,     ktype == is + 1,     ktype == 2,     ktype == 3,
+                          kpbltype == 0,  kpbltype == is + 1,  kpbltype == 2,  kpbltype == 3,
+                          peis > 6.0,     peis > 8.0,          peis > 10.0,
+                          ktype >= 2 && peis < double(P.reisthsc)};
+      px_add_if(px, o, v, c);
+    }
+    if (ktype > 0) px[S(83, f)] = double(kctop);
     is = is + 1;
   }
   if (P.lcldbudc) {  // :3948-3970
-    X(jk, is + 4) = X(jk, is + 4) + cc[2] * zdt;
-    X(jk, is + 6) = X(jk, is + 6) + cc[3] * zdt;
-    X(jk, is + 7) = X(jk, is + 7) + (cc[4] + cc[6]) * zdt;
-    X(jk, is + 8) = X(jk, is + 8) + cc[5] * zdt;
-    X(jk, is + 9) = X(jk, is + 9) + cc[7] * zdt;
-    X(jk, is + 11) = X(jk, is + 11) + pvfa * zdt;
-    X(jk, is + 12) = X(jk, is + 12) + pdyna * zdt;
+    const size_t o[7] = {S(jk, is + 4), S(jk, is + 6), S(jk, is + 7), S(jk, is + 8),
+                         S(jk, is + 9), S(jk, is + 11), S(jk, is + 12)};
+    const double v[7] = {cc[2] * zdt, cc[3] * zdt, (cc[4] + cc[6]) * zdt, cc[5] * zdt,
+                         cc[7] * zdt, pvfa * zdt,  pdyna * zdt};
+    px_add(px, o, v);
     is = is + 12;
   }
   if (P.lcldbudl) {  // :3972-4007
-    X(jk, is + 5) = X(jk, is + 5) + bl[2] * zdt;
-    X(jk, is + 7) = X(jk, is + 7) + bl[3] * zdt;
-    X(jk, is + 8) = X(jk, is + 8) + (bl[4] + bl[6]) * zdt;
-    X(jk, is + 9) = X(jk, is + 9) + bl[5] * zdt;
-    X(jk, is + 10) = X(jk, is + 10) + bl[7] * zdt;
-    X(jk, is + 11) = X(jk, is + 11) + bl[11] * zdt;
-    X(jk, is + 12) = X(jk, is + 12) + bl[12] * zdt;
-    X(jk, is + 13) = X(jk, is + 13) + bl[13] * zdt;
-    X(jk, is + 14) = X(jk, is + 14) + bl[14] * zdt;
-    X(jk, is + 15) = X(jk, is + 15) + bl[15] * zdt;
-    X(jk, is + 16) = X(jk, is + 16) + bl[17] * zdt;
-    X(jk, is + 17) = X(jk, is + 17) + (bl[18] + bl[19]) * zdt;
-    X(jk, is + 18) = X(jk, is + 18) + bl[20] * zdt;
-    X(jk, is + 19) = X(jk, is + 19) + bl[21] * zdt;
-    X(jk, is + 20) = X(jk, is + 20) + pvfl * zdt;
-    X(jk, is + 21) = X(jk, is + 21) + pdynl * zdt;
-    X(jk, is + 22) = X(jk, is + 22) + xl;
+    {
+      const size_t o[9] = {S(jk, is + 5),  S(jk, is + 7),  S(jk, is + 8),  S(jk, is + 9), S(jk, is + 10),
+                           S(jk, is + 11), S(jk, is + 12), S(jk, is + 13), S(jk, is + 14)};
+      const double v[9] = {bl[2] * zdt,  bl[3] * zdt,  (bl[4] + bl[6]) * zdt, bl[5] * zdt, bl[7] * zdt,
+                           bl[11] * zdt, bl[12] * zdt, bl[13] * zdt,          bl[14] * zdt};
+      px_add(px, o, v);
+    }
+    {
+      const size_t o[8] = {S(jk, is + 15), S(jk, is + 16), S(jk, is + 17), S(jk, is + 18),
+                           S(jk, is + 19), S(jk, is + 20), S(jk, is + 21), S(jk, is + 22)};
+      const double v[8] = {bl[15] * zdt, bl[17] * zdt, (bl[18] + bl[19]) * zdt, bl[20] * zdt,
+                           bl[21] * zdt, pvfl * zdt,   pdynl * zdt,             xl};
+      px_add(px, o, v);
+    }
     is = is + 22;
   }
   if (P.lcldbudi) {  // :4009-4048
-    X(jk, is + 5) = X(jk, is + 5) + bi[2] * zdt;
-    X(jk, is + 7) = X(jk, is + 7) + bi[3] * zdt;
-    X(jk, is + 8) = X(jk, is + 8) + (bi[4] + bi[6]) * zdt;
-    X(jk, is + 9) = X(jk, is + 9) + bi[5] * zdt;
-    X(jk, is + 10) = X(jk, is + 10) + bi[7] * zdt;
-    X(jk, is + 11) = X(jk, is + 11) + bi[11] * zdt;
-    X(jk, is + 12) = X(jk, is + 12) + (bi[12] + bi[13]) * zdt;
-    X(jk, is + 13) = X(jk, is + 13) + bi[14] * zdt;
-    X(jk, is + 14) = X(jk, is + 14) + (bi[15] + bi[16]) * zdt;
-    X(jk, is + 15) = X(jk, is + 15) + psdep * zqtmst * zdt;
-    X(jk, is + 16) = X(jk, is + 16) + bi[17] * zdt;
-    X(jk, is + 17) = X(jk, is + 17) + pvfi * zdt;
-    X(jk, is + 18) = X(jk, is + 18) + 0.0 * zqtmst * zdt;
-    X(jk, is + 19) = X(jk, is + 19) + pdyni * zdt;
-    X(jk, is + 20) = X(jk, is + 20) + xi;
+    {
+      const size_t o[8] = {S(jk, is + 5), S(jk, is + 7),  S(jk, is + 8),  S(jk, is + 9),
+                           S(jk, is + 10), S(jk, is + 11), S(jk, is + 12), S(jk, is + 13)};
+      const double v[8] = {bi[2] * zdt, bi[3] * zdt,  (bi[4] + bi[6]) * zdt,   bi[5] * zdt,
+                           bi[7] * zdt, bi[11] * zdt, (bi[12] + bi[13]) * zdt, bi[14] * zdt};
+      px_add(px, o, v);
+    }
+    {
+      const size_t o[7] = {S(jk, is + 14), S(jk, is + 15), S(jk, is + 16), S(jk, is + 17),
+                           S(jk, is + 18), S(jk, is + 19), S(jk, is + 20)};
+      const double v[7] = {(bi[15] + bi[16]) * zdt, psdep * zqtmst * zdt, bi[17] * zdt, pvfi * zdt,
+                           0.0 * zqtmst * zdt,      pdyni * zdt,          xi};
+      px_add(px, o, v);
+    }
     is = is + 20;
   }
   if (P.lcldbudt) {  // :4051-4106
     const double lv = double(P.ralvdcp), ls = double(P.ralsdcp), lf = double(P.ralfdcp);
-    X(jk, is + 1) = X(jk, is + 1) + phrsw;
-    X(jk, is + 2) = X(jk, is + 2) + phrlw;
-    X(jk, is + 3) = X(jk, is + 3) + ((bl[1] + bl[2] + bl[9] + bl[10]) * lv - bi[11] * lv) * zdt;
-    X(jk, is + 4) = X(jk, is + 4) + (bi[1] + bi[2] + bi[9] + bi[10] + bi[11]) * ls * zdt;
-    X(jk, is + 5) = X(jk, is + 5) + bi[11] * lf * zdt;
-    X(jk, is + 6) = X(jk, is + 6) + (bl[7] + bl[8] + bl[5]) * lv * zdt;
-    X(jk, is + 7) = X(jk, is + 7) + (bi[7] + bi[8] + bi[5]) * ls * zdt;
-    X(jk, is + 8) = X(jk, is + 8) + bl[20] * lv * zdt;
-    X(jk, is + 9) = X(jk, is + 9) + bi[17] * ls * zdt;
-    X(jk, is + 10) = X(jk, is + 10) + bi[15] * lf * zdt;
-    X(jk, is + 11) = X(jk, is + 11) + bi[16] * lf * zdt;
-    X(jk, is + 12) = X(jk, is + 12) - (bl[12] + bl[13] + bl[18] + bl[19]) * lf * zdt;
-    X(jk, is + 13) = X(jk, is + 13) + bl[21] * lf * zdt;
+    {
+      const size_t o[7] = {S(jk, is + 1), S(jk, is + 2), S(jk, is + 3), S(jk, is + 4),
+                           S(jk, is + 5), S(jk, is + 6), S(jk, is + 7)};
+      const double v[7] = {phrsw,
+                           phrlw,
+                           ((bl[1] + bl[2] + bl[9] + bl[10]) * lv - bi[11] * lv) * zdt,
+                           (bi[1] + bi[2] + bi[9] + bi[10] + bi[11]) * ls * zdt,
+                           bi[11] * lf * zdt,
+                           (bl[7] + bl[8] + bl[5]) * lv * zdt,
+                           (bi[7] + bi[8] + bi[5]) * ls * zdt};
+      px_add(px, o, v);
+    }
+    {
+      const size_t o[6] = {S(jk, is + 8),  S(jk, is + 9),  S(jk, is + 10),
+                           S(jk, is + 11), S(jk, is + 12), S(jk, is + 13)};
+      // X(JK, IS+12) is decremented (:4100): the subtraction is kept as such
+      double old[6];
+#pragma unroll
+      for (int n = 0; n < 6; ++n) old[n] = px[o[n]];
+      px[o[0]] = old[0] + bl[20] * lv * zdt;
+      px[o[1]] = old[1] + bi[17] * ls * zdt;
+      px[o[2]] = old[2] + bi[15] * lf * zdt;
+      px[o[3]] = old[3] + bi[16] * lf * zdt;
+      px[o[4]] = old[4] - (bl[12] + bl[13] + bl[18] + bl[19]) * lf * zdt;
+      px[o[5]] = old[5] + bl[21] * lf * zdt;
+    }
   }
 }
 
@@ -339,10 +368,16 @@ CSC_DEV void write_budgets(const Fields &F, const KParams<Real> &P, const double
 // reads PLUDE from plude_in.  A column whose fast pass sets *bad must be rerun
 // (its outputs, stored in the same places by both passes, are then final) and
 // leaves its warning count to the rerun.
+// With BUD, PEXTRA is accumulated in place, so the two passes share its
+// levels: the fast pass adds a level's budget terms only while no division
+// has reported (everything it computed up to there is IEEE's), and records
+// in *kbud the first level it left out; the redo pass adds the terms of the
+// levels from *kbud on.  Every slot then receives IEEE's terms once each, in
+// level order, as in one IEEE run.
 template <typename Real, bool F32M, bool BUD = false, bool OPT = false, typename FT = Fields, bool GEN = false,
           int PASS = kPassPlain>
 CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool active = true, bool *bad = nullptr,
-                            double *plude_in = nullptr) {
+                            double *plude_in = nullptr, int *kbud = nullptr) {
   const KParams<Real> &P = KP<Real>();
   const KParamsD &PD = c_kd;
   typedef double D;
@@ -411,6 +446,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
   Real pfplsx_i = C(0.0), pfplsx_r = C(0.0), pfplsx_s = C(0.0);  // ZPFPLSX(JK)
   D fsqlf = 0.0, fsqif = 0.0, fcqlng = 0.0, fcqnng = 0.0, fsqltur = 0.0, fsqitur = 0.0;
   unsigned nwarn = 0;
+  // first level whose budget terms the fast pass leaves to the redo pass
+  int kbud_l = klev;
+  if constexpr (BUD && PASS == kPassRedo) kbud_l = *kbud;
 
   // flux index 1 (:4231-4241)
   if (active) {
@@ -1264,7 +1302,15 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         // inputs a section that is off does not read may be NULL
         auto opt = [&](const double *q) { return q ? ld(q + ok) : 0.0; };
         auto opti = [&](const int32_t *q) { return q ? ld(q + o1) : 0; };
-        if (active)
+        bool wr = active;
+        if constexpr (FAST_) {
+          if (divbad_.bad()) {
+            wr = false;
+            kbud_l = k < kbud_l ? k : kbud_l;
+          }
+        }
+        if constexpr (PASS == kPassRedo) wr = wr && k >= kbud_l;
+        if (wr)
           write_budgets(F, P, bd.cc, bd.l, bd.i, (size_t)ib * np * klev * F.kfldx + jl, np, klev, k, dt,
                         zqtmst, double(zdp), double(zrho), opt(F.pvfa), opt(F.pdyna), double(pvfl),
                         opt(F.pdynl), double(pvfi), opt(F.pdyni), opt(F.pdyns), opt(F.phrsw), opt(F.phrlw),
@@ -1378,6 +1424,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
   if (active) F.prainfrac_toprfz[o1] = D(prainfrac);
   if (active && nwarn && F.ncounters && !(FAST_ && divbad_.bad())) atomic_add(F.ncounters, nwarn);
   if constexpr (FAST_) *bad = active && divbad_.bad();
+  if constexpr (FAST_ && BUD) *kbud = kbud_l;
 #undef C
 }
 

@@ -530,10 +530,10 @@ static int launch_checked(int precision, const Fields &f, const Shape &sh, cudaS
                                          "arrays: use cloudsc_b200_batched_diag or cloudsc_b200_block");
     form = bud && opt ? 5 : (opt ? 4 : 3);
   }
-  // parameters that rule out the GEN kernels, and more than kMaxLevFast
-  // levels: forms 0-2 run a (448, 1) kernel, at most 448 columns per CTA
-  const bool small = !gen || sh.klev > kMaxLevFast;
-  const int threads = (small && form <= 2 && sc.threads > 448) ? 448 : sc.threads;
+  // parameters that rule out the GEN kernels, more than kMaxLevFast levels
+  // and forms 3-5: a (448, 1) kernel, at most 448 columns per CTA
+  const bool small = !gen || sh.klev > kMaxLevFast || form > 2;
+  const int threads = (small && sc.threads > 448) ? 448 : sc.threads;
   const int tiles = (int)(((long long)sh.ngpblks * sh.nproma + threads - 1) / threads);
   const int grid = grid_for(sc.ctas_per_sm, tiles);
   cudaError_t e = launch(form, sc.variant, f, sh, threads, grid, stream, gen);

@@ -42,6 +42,8 @@
 // result: with an FP32 state the scheme's thresholds and MIN() limiters flip
 // (a measured 5-7 % RMS error on the T tendency).
 #pragma once
+#include <cstdint>
+#include <cstring>
 #include <type_traits>
 
 #include "cloudsc_common.cuh"
@@ -69,6 +71,16 @@ struct DivCheck {
   CSC_DEV bool bad() const { return acc >= kDivRange; }
 };
 
+#if !defined(__CUDA_ARCH__)
+// The window offset of x on the host (the GPU code takes hi(x) with
+// __double2hiint): host builds report the operands the GPU kernels report.
+inline unsigned div_offset_host(double x) {
+  uint64_t u;
+  std::memcpy(&u, &x, sizeof u);
+  return (unsigned)(u >> 32) * 2u - kDivBase;
+}
+#endif
+
 // Branch-free double division for the column code.  A reciprocal estimate
 // (rcp.approx.ftz.f64) is refined by three Newton-Raphson steps
 // y <- y + y(1 - by), each error term and update one fused multiply-add; the
@@ -90,8 +102,9 @@ struct DivCheck {
 // with any is rerun with IEEE division.  The GPU tests compare it with IEEE
 // division on random operands and on hard ones (significands of all ones or
 // all zeros, quotients next to a rounding tie).  The host build divides with
-// IEEE division (CLOUDSC_HOST_FORCE_REDO makes every call report, to drive
-// the caller's rerun in host tests).
+// IEEE division and reports the operands the GPU would report
+// (CLOUDSC_HOST_FORCE_REDO makes every call report, to drive the caller's
+// rerun in host tests).
 CSC_DEV double fast_div(double a, double b, DivCheck &dc) {
 #if defined(__CUDA_ARCH__)
   const int ha = __double2hiint(a), hb = __double2hiint(b);
@@ -119,7 +132,7 @@ CSC_DEV double fast_div(double a, double b, DivCheck &dc) {
 #if defined(CLOUDSC_HOST_FORCE_REDO)
   dc.acc = ~0u;
 #else
-  (void)dc;
+  dc.acc |= (a == 0.0 ? 0u : div_offset_host(a)) | div_offset_host(b);
 #endif
   return a / b;
 #endif
@@ -146,7 +159,7 @@ CSC_DEV double fast_div_k(double a, double b, double y, DivCheck &dc) {
 #if defined(CLOUDSC_HOST_FORCE_REDO)
   dc.acc = ~0u;
 #else
-  (void)dc;
+  dc.acc |= a == 0.0 ? 0u : div_offset_host(a);
 #endif
   return a / b;
 #endif

@@ -72,12 +72,13 @@ namespace cloudsc {
 //      faster but further from FP64 (measured tendency errors of 0.3-4 %).
 // FT: Fields (the double-precision interface) or FieldsSP (float arrays,
 // forms 0-2 only).  GEN: the parameter-exponent pows without their tests for
-// the exponents 0.5, 1.5, 2 and 3 (forms 0-2; the host launches it when the
-// uploaded parameters have none of these, gen_exponents_ok).  FAST (forms
-// 0-2, KLEV <= kMaxLevFast): every column runs the fast pass (the branch-free
-// division, fast_div); a column whose pass reported an operand outside that
-// division's exact window is run again with IEEE division, so that the
-// outputs are those of IEEE division for every input.
+// the exponents 0.5, 1.5, 2 and 3 (the host launches it when the uploaded
+// parameters have none of these, gen_exponents_ok).  FAST (KLEV <=
+// kMaxLevFast): every column runs the fast pass (the branch-free division,
+// fast_div); a column whose pass reported an operand outside that division's
+// exact window is run again with IEEE division, so that the outputs are
+// those of IEEE division for every input (with the budgets, the two passes
+// split PEXTRA's levels between them: cloudsc_column, kbud).
 template <int FORM, int MAXT, int MINB, typename FT = Fields, bool GEN = false, bool FAST = false>
 __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(FT F, Shape sh) {
   // Let ptxas place part of the register spills in shared memory instead of
@@ -99,7 +100,18 @@ __global__ void __launch_bounds__(MAXT, MINB) cloudsc_kernel(FT F, Shape sh) {
       jl = sh.kidia0;
     }
     if constexpr (FORM >= 3) {
-      cloudsc_column<double, false, FORM == 3 || FORM == 5, FORM >= 4, FT>(F, sh, ib, jl, active);
+      constexpr bool BUD = FORM == 3 || FORM == 5, OPT = FORM >= 4;
+      if constexpr (FAST) {
+        double plude_in[kMaxLevFast];
+        bool bad = false;
+        int kbud = sh.klev;
+        cloudsc_column<double, false, BUD, OPT, FT, GEN, kPassFast>(F, sh, ib, jl, active, &bad, plude_in, &kbud);
+        if (__syncthreads_or(bad))
+          cloudsc_column<double, false, BUD, OPT, FT, GEN, kPassRedo>(F, sh, ib, jl, bad, nullptr, plude_in,
+                                                                       &kbud);
+      } else {
+        cloudsc_column<double, false, BUD, OPT, FT, GEN>(F, sh, ib, jl, active);
+      }
     } else if constexpr (FAST) {
       typedef std::conditional_t<FORM == 2, float, double> Real;
       double plude_in[kMaxLevFast];
@@ -335,8 +347,14 @@ static_assert(kNumVariants == 6, "kernel_ptr_form lists every variant");
 // known configuration allow GEN); for parameters that do not, in the (448, 1)
 // variant with FAST only; for KLEV above kMaxLevFast, in the (448, 1) variant
 // without either (`launch` then runs that one, at most 448 columns per CTA).
-// Forms 3-5 (budgets, SPP, inhomogeneity) keep the exponent tests and IEEE
-// division.
+// Forms 3-5 (budgets, SPP, inhomogeneity, aerosols) exist in the (448, 1)
+// variant only, in the same three builds; every variant maps to it.
+template <int FORM>
+static const void *kernel_ptr_opt_form(bool gen, bool fast) {
+  if (!fast) return (const void *)cloudsc_kernel<FORM, 448, 1, Fields, false, false>;
+  if (!gen) return (const void *)cloudsc_kernel<FORM, 448, 1, Fields, false, true>;
+  return (const void *)cloudsc_kernel<FORM, 448, 1, Fields, true, true>;
+}
 static const void *kernel_ptr(int precision, int v, bool gen, bool fast) {
   if (precision <= 2 && !fast) {
     switch (precision) {
@@ -356,9 +374,9 @@ static const void *kernel_ptr(int precision, int v, bool gen, bool fast) {
     case 0: return kernel_ptr_form<0, true, true>(v);
     case 1: return kernel_ptr_form<1, true, true>(v);
     case 2: return kernel_ptr_form<2, true, true>(v);
-    case 3: return kernel_ptr_form<3, false, false>(v);
-    case 4: return kernel_ptr_form<4, false, false>(v);
-    case 5: return kernel_ptr_form<5, false, false>(v);
+    case 3: return kernel_ptr_opt_form<3>(gen, fast);
+    case 4: return kernel_ptr_opt_form<4>(gen, fast);
+    case 5: return kernel_ptr_opt_form<5>(gen, fast);
     default: return nullptr;
   }
 }
@@ -426,12 +444,12 @@ cudaError_t max_local_bytes(size_t *out) {
 // 2 = FP32 physics, 3-5 the FP64 forms with budgets / SPP and inhomogeneity;
 // gen: the parameters allow the GEN kernels (forms 0-2 otherwise run the
 // (448, 1) kernel without GEN, at most 448 columns per CTA, as they do for
-// KLEV above kMaxLevFast).
+// KLEV above kMaxLevFast; forms 3-5 always run a (448, 1) kernel).
 cudaError_t launch(int precision, int v, const Fields &f, const Shape &sh, int threads, int grid,
                    cudaStream_t stream, bool gen) {
   const bool fast = sh.klev <= kMaxLevFast;
   if (v < 0 || v >= kNumVariants || threads > kVariants[v].maxt) return cudaErrorInvalidConfiguration;
-  if ((!gen || !fast) && precision <= 2 && threads > 448) return cudaErrorInvalidConfiguration;
+  if ((!gen || !fast || precision > 2) && threads > 448) return cudaErrorInvalidConfiguration;
   const void *k = kernel_ptr(precision, v, gen, fast);
   if (!k) return cudaErrorInvalidValue;
   Fields fa = f;

@@ -186,10 +186,35 @@ extern "C" int hostemu_sltend_batched(const cloudsc_params *p, int nproma, int k
   return 0;
 }
 
+// The kernels' forms 3-5 on one column: the plain column code, or (FD) the
+// fast pass and, for a column it reported, the rerun, the two passes
+// splitting PEXTRA's levels as the kernels do.
+template <bool BUD, bool OPT, bool GEN, bool FD>
+static void column_opt(const Fields &f, const Shape &sh, int ib, int jl) {
+  if (FD && sh.klev <= kMaxLevFast) {
+    double plude_in[kMaxLevFast];
+    bool bad = false;
+    int kbud = sh.klev;
+    cloudsc_column<double, false, BUD, OPT, Fields, GEN, kPassFast>(f, sh, ib, jl, true, &bad, plude_in, &kbud);
+    if (bad)
+      cloudsc_column<double, false, BUD, OPT, Fields, GEN, kPassRedo>(f, sh, ib, jl, true, nullptr, plude_in,
+                                                                      &kbud);
+  } else {
+    cloudsc_column<double, false, BUD, OPT, Fields, GEN>(f, sh, ib, jl);
+  }
+}
+// indexed by (BUD && OPT ? 2 : OPT ? 1 : 0) + 3 * GEN + 6 * FD
+static const ColumnFn kColumnOpt[12] = {
+    column_opt<true, false, false, false>, column_opt<false, true, false, false>, column_opt<true, true, false, false>,
+    column_opt<true, false, true, false>,  column_opt<false, true, true, false>,  column_opt<true, true, true, false>,
+    column_opt<true, false, false, true>,  column_opt<false, true, false, true>,  column_opt<true, true, false, true>,
+    column_opt<true, false, true, true>,   column_opt<false, true, true, true>,   column_opt<true, true, true, true>};
+
 // CLOUDSC with the optional configurations (the kernel's BUD and OPT forms):
-// the BATCHED_FIELDS arrays in `a`, the fields.DIAG_FIELDS arrays in `b`.
+// the BATCHED_FIELDS arrays in `a`, the fields.DIAG_FIELDS arrays in `b`;
+// flags 0x100 for the GEN column code, 0x200 for the fast pass with its rerun.
 extern "C" int hostemu_batched_diag(const cloudsc_params *p, int nproma, int klev, int ngpblks, int ngptot,
-                                    double ptsphy, void **a, void **b, int kfldx) {
+                                    double ptsphy, void **a, void **b, int kfldx, int flags) {
   Derived d;
 #ifdef CLOUDSC_HOST_LIBM_GLIBC
   d.zconst_pow_land = std::pow(p->rcl_kk_cloud_num_land, p->rcl_kkbaun);
@@ -234,9 +259,8 @@ extern "C" int hostemu_batched_diag(const cloudsc_params *p, int nproma, int kle
     int icend = ngptot - ib * nproma;
     if (icend > nproma) icend = nproma;
     for (int jl = 0; jl < icend; ++jl) {
-      if (bud && opt) cloudsc_column<double, false, true, true>(f, sh, ib, jl);
-      else if (opt) cloudsc_column<double, false, false, true>(f, sh, ib, jl);
-      else cloudsc_column<double, false, true>(f, sh, ib, jl);
+      const int form = bud && opt ? 2 : (opt ? 1 : 0);
+      kColumnOpt[form + ((flags & 0x100) ? 3 : 0) + ((flags & 0x200) ? 6 : 0)](f, sh, ib, jl);
     }
   }
   return (int)nwarn;

@@ -118,3 +118,41 @@ def test_block_entry_spp_inhomogeneity(cuda):
     for n in util.COMPARED:
         g, o = util.defined(n, blk[n][None]), util.defined(n, ref[n])
         assert np.array_equal(g[..., cols], o[..., cols]), n
+
+
+@pytest.mark.parametrize("case", ["budgets", "spp", "all+budgets"])
+def test_optional_forms_rerun_mid_column(cuda, case):
+    """Forms 3-5 run the fast pass with its rerun.  Three columns get a
+    pressure of 1e80 Pa at levels 60, 90 and 120, outside the fast division's
+    window: they report there and run again with IEEE division, the fast pass
+    having added PEXTRA's terms of the levels above.  Every output, PFSD and
+    PEXTRA equal the oracle's bit for bit, and the warning count is counted
+    once."""
+    import torch
+    p0, po0 = util.params()
+    if case == "budgets":
+        p, po = util.with_flags(p0, util.BUDGET_CASES[-1]), util.with_flags(po0, util.BUDGET_CASES[-1])
+    else:
+        p, po = util.opt_params(p0, case), util.opt_params(po0, case)
+    nproma, nblk = 32, 6
+    ngptot = nproma * nblk - 3
+    arrs = util.with_out_of_window_pressure(inputs.generate(nblk, nproma, p, seed=43))
+    diag = inputs.generate_diag(arrs, nproma, fields.budget_fields_needed(p) + 1, seed=43)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot)
+    try:
+        cloudsc.setup(p)
+        d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
+        g = {k: torch.from_numpy(v).cuda() for k, v in diag.items()}
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        cloudsc.cloudsc_batched_diag(p, d, g, nproma, util.KLEV, nblk, ngptot, util.PTSPHY, counter=cnt)
+        torch.cuda.synchronize()
+        for n in util.COMPARED:
+            a = util.defined(n, util._valid_cols(d[n].cpu().numpy(), ngptot, nproma))
+            b = util.defined(n, util._valid_cols(ref[n], ngptot, nproma))
+            assert np.array_equal(a, b), n
+            assert np.isfinite(b).all(), n
+        assert np.array_equal(g["pfsd"].cpu().numpy(), dref["pfsd"])
+        assert np.array_equal(g["pextra"].cpu().numpy(), dref["pextra"])
+        assert int(cnt.item()) == nw
+    finally:
+        cloudsc.setup(p0)

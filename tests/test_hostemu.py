@@ -174,6 +174,37 @@ def test_budget_diagnostics_bit_exact(pp, flags):
         assert np.array_equal(util.defined(n, ref[n]), util.defined(n, plain[n])), n
 
 
+@pytest.mark.parametrize("case", ["budgets", "spp", "all+budgets"])
+def test_optional_forms_rerun_leaves_results_unchanged(pp, case):
+    """The kernels' fast pass with its rerun in the budget and SPP/
+    inhomogeneity forms: with no column rerunning, with every column
+    rerunning (the redo build, whose divisions all report) and with three
+    columns reporting in mid-column (an out-of-window pressure at levels 60,
+    90 and 120), the outputs, PFSD and PEXTRA equal the plain column code's
+    and the oracle's bit for bit.  PEXTRA is accumulated in place, so the
+    fast pass leaves a reporting column's levels from the report on to the
+    rerun: a level added twice, or not at all, would show here."""
+    p0, po0 = pp
+    if case == "budgets":
+        p, po = util.with_flags(p0, util.BUDGET_CASES[-1]), util.with_flags(po0, util.BUDGET_CASES[-1])
+    else:
+        p, po = util.opt_params(p0, case), util.opt_params(po0, case)
+    nproma, nblk = 32, 6
+    ngptot = nproma * nblk - 3
+    arrs = util.with_out_of_window_pressure(inputs.generate(nblk, nproma, p, seed=43))
+    diag = inputs.generate_diag(arrs, nproma, util.fields.budget_fields_needed(p) + 1, seed=43)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot)
+    for n in util.COMPARED:
+        assert np.isfinite(util.defined(n, ref[n])).all(), n
+    for libm, flags in (("plibm", 0), ("plibm", 0x200), ("plibm", 0x300), ("redo", 0x300)):
+        emu, demu, nwe = util.run_hostemu_diag(p, arrs, diag, nproma, nblk, ngptot, libm=libm, flags=flags)
+        assert nw == nwe, (libm, flags)
+        for n in util.COMPARED:
+            assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), (libm, flags, n)
+        assert np.array_equal(demu["pfsd"], dref["pfsd"]), (libm, flags)
+        assert np.array_equal(demu["pextra"], dref["pextra"]), (libm, flags)
+
+
 @pytest.mark.parametrize("case", util.OPT_CASES)
 def test_spp_inhomogeneity_bit_exact(pp, case):
     """SPP perturbations, LCLOUD_INHOMOG and LRAD_CLOUD_INHOMOG (PFSD), the

@@ -226,14 +226,17 @@ def run_oracle_sltend(po, arrs, nproma, ngpblks, ngptot, libm="plibm"):
 
 
 
-def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm"):
-    """The kernel's column code with the budget diagnostics, on the host."""
+def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm", flags=0):
+    """The kernel's column code with the budget diagnostics, on the host;
+    flags 0x100 for the GEN column code, 0x200 for the kernels' fast pass with
+    its rerun."""
     import ctypes
     import os
     import subprocess
     here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hostemu")
     subprocess.run(["make", "-s", "-C", here], check=True)
-    name = "libcloudsc_hostemu.so" if libm == "plibm" else "libcloudsc_hostemu_glibc.so"
+    name = {"plibm": "libcloudsc_hostemu.so", "glibc": "libcloudsc_hostemu_glibc.so",
+            "redo": "libcloudsc_hostemu_redo.so"}[libm]
     L = ctypes.CDLL(os.path.join(here, name))
     out = {k: v.copy() for k, v in arrs.items()}
     dout = {k: v.copy() for k, v in diag.items()}
@@ -241,7 +244,7 @@ def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm"):
     b = (ctypes.c_void_p * len(fields.DIAG_FIELDS))(
         *[(dout[n].ctypes.data if dout.get(n) is not None else None) for n, *_ in fields.DIAG_FIELDS])
     nw = L.hostemu_batched_diag(ctypes.byref(p), int(nproma), KLEV, int(ngpblks), int(ngptot),
-                                ctypes.c_double(PTSPHY), a, b, int(dout["pextra"].shape[1]))
+                                ctypes.c_double(PTSPHY), a, b, int(dout["pextra"].shape[1]), int(flags))
     return out, dout, nw
 
 
@@ -290,6 +293,21 @@ def with_spp(p, lramidlimit1=1, nrftotal=10):
 
 
 OPT_CASES = ["spp", "inhomog", "radinhomog", "aerosol", "all", "all+budgets"]
+
+# (block, column, level) points given a pressure of 1e80 Pa, outside the fast
+# division's window: those columns' fast pass reports at that level (the
+# first division by PAP) and they run again with IEEE division; the scheme's
+# outputs stay finite
+OUT_OF_WINDOW_PAP = [(0, 3, 90), (2, 17, 60), (5, 1, 120)]
+
+
+def with_out_of_window_pressure(arrs, points=OUT_OF_WINDOW_PAP):
+    """A copy of ``arrs`` with PAP = 1e80 at ``points``."""
+    out = dict(arrs)
+    out["pap"] = arrs["pap"].copy()
+    for ib, jl, k in points:
+        out["pap"][ib, k, jl] = 1e80
+    return out
 # the four aerosol switches (NAERCLD > 0); LAERLIQAUTOLSP and LAERLIQCOLL act
 # only under IWARMRAIN = 1, which the reference does not use
 AEROSOL = {"laericesed": 1, "laericeauto": 1, "laerliqautolsp": 1, "laerliqcoll": 1}
