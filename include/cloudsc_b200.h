@@ -578,7 +578,7 @@ int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t 
 
 /*
  * Self-check of the division the column kernels use (no reference
- * counterpart).  The kernels of forms 0-2 divide in double precision with a
+ * counterpart).  The column kernels divide in double precision with a
  * branch-free reciprocal-and-residual sequence that returns IEEE a/b exactly
  * for 2^-256 <= |b| < 2^256 and a = 0 or 2^-256 <= |a| < 2^256, and records
  * every operand outside that window; a column with such an operand is run
@@ -590,6 +590,16 @@ int cloudsc_b200_set_launch(int32_t precision, int32_t threads_per_cta, int32_t 
  */
 int cloudsc_b200_division_check(const double *a, const double *b, int64_t n, double *q, int32_t *bad,
                                 void *stream);
+
+/*
+ * The reciprocal half of that division on its own (no reference
+ * counterpart): the kernels take 1/b this way, and the reciprocal of a
+ * divisor shared by several quotients once.  y[i] = the reciprocal of b[i],
+ * IEEE 1/b bit for bit for 2^-256 <= |b| < 2^256; bad[i] = 1 where b lies
+ * outside that window (0 otherwise).  Device pointers; stream may be NULL.
+ * CLOUDSC_E_SHAPE for n < 0, CLOUDSC_E_NULL for a NULL array with n > 0.
+ */
+int cloudsc_b200_reciprocal_check(const double *b, int64_t n, double *y, int32_t *bad, void *stream);
 
 /* Last CUDA error string recorded by this library on the calling thread. */
 const char *cloudsc_b200_last_error(void);

@@ -85,6 +85,8 @@ def lib():
         L.cloudsc_b200_sltend_supersat_batched.restype = ctypes.c_int
         L.cloudsc_b200_division_check.argtypes = [vp, vp, ctypes.c_int64, vp, vp, vp]
         L.cloudsc_b200_division_check.restype = ctypes.c_int
+        L.cloudsc_b200_reciprocal_check.argtypes = [vp, ctypes.c_int64, vp, vp, vp]
+        L.cloudsc_b200_reciprocal_check.restype = ctypes.c_int
         L.cloudsc_b200_last_error.restype = ctypes.c_char_p
         L.cloudsc_b200_version.restype = ctypes.c_char_p
         L.cloudsc_b200_params_size.restype = ctypes.c_size_t
@@ -457,3 +459,19 @@ def division_check(a, b, stream=None):
     st = stream.cuda_stream if stream is not None else None
     _check(lib().cloudsc_b200_division_check(_ptr(a), _ptr(b), a.numel(), _ptr(q), _ptr(bad), st))
     return q, bad
+
+
+def reciprocal_check(b, stream=None):
+    """The column kernels' reciprocal on a float64 CUDA tensor: returns
+    (y, bad), the reciprocals and an int32 flag, 1 where b lies outside the
+    window 2^-256 <= |b| < 2^256.  Inside it y equals IEEE 1 / b bit for
+    bit."""
+    import torch
+    if b.dtype != torch.float64 or not b.is_cuda:
+        raise CloudscError(-2, "reciprocal_check wants a float64 CUDA tensor")
+    b = b.contiguous()
+    y = torch.empty_like(b)
+    bad = torch.empty(b.shape, dtype=torch.int32, device=b.device)
+    st = stream.cuda_stream if stream is not None else None
+    _check(lib().cloudsc_b200_reciprocal_check(_ptr(b), b.numel(), _ptr(y), _ptr(bad), st))
+    return y, bad

@@ -25,6 +25,13 @@
 #define DIV2(A, B) ((A) * decltype(A)(1.0 / (B)))
 // A parameter divisor with its reciprocal computed on the host (KParams rcp_*).
 #define DIVP(A, B, Y) cdivk<FAST_>(A, B, Y, divbad_)
+// The quotient 1/B (crcp): in the fast pass the reciprocal half of fast_div,
+// recording B's window.
+#define RCP(B) crcp<FAST_>(B, divbad_)
+// A / B for a divisor shared by several quotients, Y = RCP(B) computed once:
+// the same operations as DIV(A, B) (fast_div is fast_rcp followed by
+// fast_div_k's corrections), so the same bits.
+#define DIVY(A, B, Y) cdivk<FAST_>(A, B, Y, divbad_)
 
 namespace cloudsc {
 
@@ -123,7 +130,7 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp, double &t
   double zda = 0.0;
   double zt = mx(pt, 160.0);
   double za = mx(mn(pa, 1.0), 0.0);
-  double zp_r = DIV(1.0, pp);
+  double zp_r = RCP(pp);
   double el = xexp(DIV(k.r3les * (zt - k.rtt), (zt - k.r4les)));
   double x = (mx(k.rtice, mn(k.rtwat, zt)) - k.rtice) * k.rtwat_rtice_r;
   double alfa = mn(1.0, x * x);
@@ -138,10 +145,10 @@ CSC_DEV void supersatcheck(double pt, double pq, double pa, double pp, double &t
   double zqsliqk = DIV(zfokoop, (1.0 - k.retv * zfokoop));
   double wsum = (alfa < 1.0) ? alfa * el + (1.0 - alfa) * ei : el;
   double zfoeemix = mn((k.r2es * wsum) * zp_r, 0.5);
-  double zcor = DIV(1.0, (1.0 - k.retv * zfoeemix));
+  double zcor = RCP(1.0 - k.retv * zfoeemix);
   double zqsmix = zfoeemix * zcor;
   double xl = zt - k.r4les, xi = zt - k.r4ies;
-  double foedem = alfa * k.r5alvcp * (DIV(1.0, (xl * xl))) + (1.0 - alfa) * k.r5alscp * (DIV(1.0, (xi * xi)));
+  double foedem = alfa * k.r5alvcp * (RCP(xl * xl)) + (1.0 - alfa) * k.r5alscp * (RCP(xi * xi));
   double zcorqsmix = 1.0 + zqsmix * zcor * foedem;
   zqsliqk = 0.5 * (zqsliqk + zqsmix);
   double zqslim = za * zqsmix + (1.0 - za) * zqsliqk;
@@ -507,6 +514,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
     // (only the loop levels JK >= NCLDTOP read these)
     Real alfa = C(0.0), zfoeewm = C(0.0), zqsmix = C(0.0), zfoeew = C(0.0), zqsice = C(0.0);
     Real zfoeeliqt = C(0.0), zqsliq = C(0.0), el_e = C(0.0), ei_e = C(0.0);
+    // 1/(1 - RETV FOEEW) for the mixed, ice and liquid saturation pressures:
+    // the divisors of ZQSMIX/ZQSICE/ZQSLIQ and the ZCOR factors below
+    Real rmix = C(0.0), rice = C(0.0), rliq = C(0.0);
     if (k >= ncldtop0) {
       Real x = (mx(P.rtice, mn(P.rtwat, t)) - P.rtice) * P.rtwat_rtice_r;
       alfa = mn(C(1.0), x * x);
@@ -516,16 +526,23 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       // two exponentials overlap)
       ei_e = mexp<F32M>(DIV(P.r3ies * (t - P.rtt), (t - P.r4ies)));
       Real wsum = (alfa < C(1.0)) ? alfa * el_e + (C(1.0) - alfa) * ei_e : el_e;
-      zfoeewm = mn(DIV((P.r2es * wsum), pap_k), C(0.5));
+      const Real rpap = RCP(pap_k);
+      zfoeewm = mn(DIVY((P.r2es * wsum), pap_k, rpap), C(0.5));
       zqsmix = zfoeewm;
-      zqsmix = DIV(zqsmix, (C(1.0) - P.retv * zqsmix));
+      const Real dmix = C(1.0) - P.retv * zqsmix;
+      rmix = RCP(dmix);
+      zqsmix = DIVY(zqsmix, dmix, rmix);
       Real eew = delta ? P.r2es * el_e : P.r2es * ei_e;
-      zfoeew = mn(DIV(eew, pap_k), C(0.5));
+      zfoeew = mn(DIVY(eew, pap_k, rpap), C(0.5));
       zfoeew = mn(C(0.5), zfoeew);
-      zqsice = DIV(zfoeew, (C(1.0) - P.retv * zfoeew));
-      zfoeeliqt = mn(DIV((P.r2es * el_e), pap_k), C(0.5));
+      const Real dice = C(1.0) - P.retv * zfoeew;
+      rice = RCP(dice);
+      zqsice = DIVY(zfoeew, dice, rice);
+      zfoeeliqt = mn(DIVY((P.r2es * el_e), pap_k, rpap), C(0.5));
       zqsliq = zfoeeliqt;
-      zqsliq = DIV(zqsliq, (C(1.0) - P.retv * zqsliq));
+      const Real dliq = C(1.0) - P.retv * zqsliq;
+      rliq = RCP(dliq);
+      zqsliq = DIVY(zqsliq, dliq, rliq);
     }
 
     // ---------------- tidy up (:1127-1199), double ----------------
@@ -634,21 +651,21 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       {
         Real xl = t - P.r4les, xi = t - P.r4ies;
         Real zfacw = DIV(P.r5les, (xl * xl));
-        Real zcor = DIV(C(1.0), (C(1.0) - P.retv * zfoeeliqt));
+        Real zcor = rliq;  // 1/(1 - RETV ZFOEELIQT)
         Real zdqsliqdt = zfacw * zcor * zqsliq;
         zcorqsliq = C(1.0) + P.ralvdcp * zdqsliqdt;
         Real zfaci = DIV(P.r5ies, (xi * xi));
-        zcor = DIV(C(1.0), (C(1.0) - P.retv * zfoeew));
+        zcor = rice;  // 1/(1 - RETV ZFOEEW)
         Real zdqsicedt = zfaci * zcor * zqsice;
         zcorqsice = C(1.0) + P.ralsdcp * zdqsicedt;
         Real zfac = alfa * zfacw + (C(1.0) - alfa) * zfaci;
-        zcor = DIV(C(1.0), (C(1.0) - P.retv * zfoeewm));
+        zcor = rmix;  // 1/(1 - RETV ZFOEEWM)
         zdqsmixdt = zfac * zcor * zqsmix;
         Real foeldcpm = alfa * P.ralvdcp + (C(1.0) - alfa) * P.ralsdcp;
         zcorqsmix = C(1.0) + foeldcpm * zdqsmixdt;
         zevaplimmix = mx(DIV((zqsmix - qv), zcorqsmix), C(0.0));
       }
-      const Real ztmpa = DIV(C(1.0), mx(a, C(0.01)));
+      const Real ztmpa = RCP(mx(a, C(0.01)));
       Real zliqcld = ql * ztmpa;
       Real zicecld = qi * ztmpa;
       const Real zlicld = zliqcld + zicecld;
@@ -813,9 +830,10 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         zcovptot = C(1.0) - (DIV((C(1.0) - zcovptot) * (C(1.0) - mx(a, za_prev)), (C(1.0) - mn(za_prev, C(1.0) - C(1.E-06)))));
         zcovptot = mx(zcovptot, P.rcovpmin);
         zcovpclr = mx(C(0.0), zcovptot - a);
-        zraincld = DIV(C(0.5) * (qr + qr_prev), zcovptot);
-        zraincldm1 = DIV(C(0.5) * (qr + qxnm1_r), zcovptot);
-        zsnowcld = DIV(C(0.5) * (qs + qs_prev), zcovptot);
+        const Real rcov = RCP(zcovptot);
+        zraincld = DIVY(C(0.5) * (qr + qr_prev), zcovptot, rcov);
+        zraincldm1 = DIVY(C(0.5) * (qr + qxnm1_r), zcovptot, rcov);
+        zsnowcld = DIVY(C(0.5) * (qs + qs_prev), zcovptot, rcov);
         zcovpmax = mx(zcovptot, zcovpmax);
       } else {
         zraincld = C(0.0);
@@ -839,7 +857,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
             const double zphip2 = zphip1 - 0.2;
             const double zphip3 = 0.123 * xexp(-zphip1 * 0.55);
             const double zanew2 = mx(double(a), 0.1);
-            const double zphic = xpow(zgridlen * zanew2, DIV(1.0, 3.0)) *
+            const double zphic = xpow(zgridlen * zanew2, (1.0 / 3.0)) *
                                  xpow(xpow(zphip3 * zgridlen * zanew2, 1.5) + 3.0 * zphip3, -0.17);
             double zfracsdc = (zphip1 - zphip2 * zanew2) * zphic;
             if (double(a) > 0.95) zfracsdc = 0.17 * zphic;
@@ -849,7 +867,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
             const double aa = double(a);
             const double fc2 = xpow(lfsd, 2.0);
             const double zea = xpow(1.0 + fc2, DIV((double(P.rcl_kkbauq) - 1.0) * double(P.rcl_kkbauq), 2.0));
-            const double zphir = xpow(zgridlen * aa, DIV(1.0, 3.0)) * xpow(xpow(0.11 * zgridlen * aa, 1.14) + 1.0, -0.22);
+            const double zphir = xpow(zgridlen * aa, (1.0 / 3.0)) * xpow(xpow(0.11 * zgridlen * aa, 1.14) + 1.0, -0.22);
             double zfracsdr = (1.1 - 0.8 * aa) * zphir;
             if (aa > 0.95) zfracsdr = 0.3 * zphir;
             const double fr2 = xpow(zfracsdr, 2.0);
@@ -957,7 +975,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (t < P.rtt && zsnowcld > zepsec && zsupersatice > C(0.0)) {
           Real zvpice = DIVP((P.r2es * ei_e) * P.rv, P.rd, P.rcp_rd);
           Real zaplusb = P.rcl_apb1 * zvpice - P.rcl_apb2 * zvpice * t + pap_k * P.rcl_apb3 * (t * t * t);
-          Real zcorrfac = mpow<F32M>(DIV(C(1.0), zrho), C(0.5));
+          Real zcorrfac = mpow<F32M>(RCP(zrho), C(0.5));
           Real zcorrfac2 = (mpow<F32M>(DIVK(t, 273.0), C(1.5))) * (DIV(C(393.0), (t + C(120.0))));
           Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
           const PowBase b_pr02 = mbase<F32M>(zpr02);
@@ -1196,16 +1214,17 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         const double d_i = ((1.0 + double(fallsink_i)) + double(qb_ii)) + double(qb_si);
         const double d_r = 1.0 + double(fallsink_r);
         const double d_s = 1.0 + double(fallsink_s);
-        const double m_rl = DIV((-double(qb_rl)), d_l);
-        const double m_sl = DIV((-double(qb_sl)), d_l);
-        const double m_si = DIV((-double(qb_si)), d_i);
+        const double rd_l = RCP(d_l), rd_i = RCP(d_i);
+        const double m_rl = DIVY((-double(qb_rl)), d_l, rd_l);
+        const double m_sl = DIVY((-double(qb_sl)), d_l, rd_l);
+        const double m_si = DIVY((-double(qb_si)), d_i, rd_i);
         x_r = x_r - m_rl * x_l;
         x_s = x_s - m_sl * x_l;
         x_s = x_s - m_si * x_i;
         x_s = DIV(x_s, d_s);
         x_r = DIV(x_r, d_r);
-        x_i = DIV(x_i, d_i);
-        x_l = DIV(x_l, d_l);
+        x_i = DIVY(x_i, d_i, rd_i);
+        x_l = DIVY(x_l, d_l, rd_l);
         // clip (:3633-3640)
         if (x_l < zepsecd) { x_v = x_v + x_l; x_l = 0.0; }
         if (x_i < zepsecd) { x_v = x_v + x_i; x_i = 0.0; }
@@ -1323,10 +1342,10 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
     // literals written as such at :4316,4321-4322 are their float values
     if constexpr (OPT) {
       if (P.lrad_cloud_inhomog) {
-        const double zifsdback = 0.446585 * xpow(zgridlen, DIV(1.0, 3.0)) * xpow(xpow(0.308061 * zgridlen, 0.395736) + 1.0, -0.744527);
+        const double zifsdback = 0.446585 * xpow(zgridlen, (1.0 / 3.0)) * xpow(xpow(0.308061 * zgridlen, 0.395736) + 1.0, -0.744527);
         const double zqtot = mx(mn((qvD + qiD) * 1000.0, 30.0), double(0.00001f));
         const double zrho_f = DIV(pap_kd, (double(P.rd) * tD));
-        double zdelz = DIV(1.0, (double(P.rg) * zrho_f)) * (paph_k1 - paph_k) * 0.001;
+        double zdelz = RCP(double(P.rg) * zrho_f) * (paph_k1 - paph_k) * 0.001;
         zdelz = mx(mn(zdelz, double(0.5f)), double(0.001f));
         const double zphi = xpow(DIV(zdelz, double(0.24f)), double(0.11f)) * xpow(DIV(zqtot, double(10.f)), double(0.03f));
         double zifsd = double(P.rcloud_frac_std);
@@ -1432,5 +1451,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 #undef DIVK
 #undef DIV2
 #undef DIVP
+#undef RCP
+#undef DIVY
 
 }  // namespace cloudsc

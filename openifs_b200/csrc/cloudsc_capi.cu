@@ -37,6 +37,7 @@ cudaError_t launch_sltend_supersat(const SltendFields &f, const Shape &sh, cudaS
 cudaError_t launch_state_increment(const IncFields &f, const Shape &sh, cudaStream_t stream);
 cudaError_t launch_division_check(const double *a, const double *b, long long n, double *q, int *bad,
                                   cudaStream_t stream);
+cudaError_t launch_reciprocal_check(const double *b, long long n, double *y, int *bad, cudaStream_t stream);
 cudaError_t launch_sp(int precision, int v, const FieldsSP &f, const Shape &sh, int threads, int grid,
                       cudaStream_t stream, bool gen);
 }  // namespace cloudsc
@@ -1528,6 +1529,15 @@ int cloudsc_b200_division_check(const double *a, const double *b, int64_t n, dou
   if (n == 0) return CLOUDSC_OK;
   if (!a || !b || !q || !bad) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
   cudaError_t e = launch_division_check(a, b, (long long)n, q, bad, (cudaStream_t)stream);
+  if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
+  return CLOUDSC_OK;
+}
+
+int cloudsc_b200_reciprocal_check(const double *b, int64_t n, double *y, int32_t *bad, void *stream) {
+  if (n < 0) return fail(CLOUDSC_E_SHAPE, "n < 0");
+  if (n == 0) return CLOUDSC_OK;
+  if (!b || !y || !bad) return fail(CLOUDSC_E_NULL, "a required array pointer is NULL");
+  cudaError_t e = launch_reciprocal_check(b, (long long)n, y, bad, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(CLOUDSC_E_CUDA, "kernel launch", e);
   return CLOUDSC_OK;
 }

@@ -138,6 +138,35 @@ CSC_DEV double fast_div(double a, double b, DivCheck &dc) {
 #endif
 }
 
+// The reciprocal half of fast_div on its own: y = RN(1/b), the correctly
+// rounded reciprocal (IEEE 1/b), for 2^-256 <= |b| < 2^256; b outside that
+// window is recorded in dc.  Used for the quotients 1/b and, through
+// fast_div_k, for several dividends over one divisor.
+CSC_DEV double fast_rcp(double b, DivCheck &dc) {
+#if defined(__CUDA_ARCH__)
+  const int hb = __double2hiint(b);
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  e = __fma_rn(-b, y, 1.0);
+  y = __fma_rn(y, e, y);
+  const unsigned w = ~(((unsigned)hb | 0xfff00000u) & (unsigned)__double2loint(b));
+  y = __hiloint2double(__double2hiint(y), __double2loint(y) | (int)__funnelshift_rc(1u, 0u, w));
+  dc.acc |= (unsigned)hb * 2u - kDivBase;
+  return y;
+#else
+#if defined(CLOUDSC_HOST_FORCE_REDO)
+  dc.acc = ~0u;
+#else
+  dc.acc |= div_offset_host(b);
+#endif
+  return 1.0 / b;
+#endif
+}
+
 // fast_div for a literal divisor b, given y = RN(1/b) folded at compile
 // time (IEEE division of two constants): only the two residual corrections
 // and the dividend's window test remain.  Exact as fast_div is: every such
@@ -176,6 +205,17 @@ CSC_DEV auto cdivk(A a, double b, double y, DivCheck &dc) -> decltype(a / A(b)) 
     (void)dc;
     (void)y;
     return a / A(b);
+  }
+}
+
+// 1 / b: fast_rcp when FAST and b is a double; IEEE otherwise.
+template <bool FAST, typename B>
+CSC_DEV B crcp(B b, DivCheck &dc) {
+  if constexpr (FAST && std::is_same<B, double>::value) {
+    return fast_rcp(b, dc);
+  } else {
+    (void)dc;
+    return B(1) / b;
   }
 }
 

@@ -278,6 +278,16 @@ __global__ void __launch_bounds__(kSatadjThreads) division_check_kernel(const do
   }
 }
 
+// fast_rcp on n divisors: y[i] and the window report bad[i].
+__global__ void __launch_bounds__(kSatadjThreads) reciprocal_check_kernel(const double *b, long long n, double *y,
+                                                                         int *bad) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    DivCheck dc;
+    y[i] = fast_rcp(b[i], dc);
+    bad[i] = dc.bad() ? 1 : 0;
+  }
+}
+
 }  // namespace cloudsc
 
 // ---------------------------------------------------------------------------
@@ -527,6 +537,14 @@ cudaError_t launch_division_check(const double *a, const double *b, long long n,
   if (blocks > 148LL * 16) blocks = 148LL * 16;
   if (blocks < 1) blocks = 1;
   division_check_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(a, b, n, q, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reciprocal_check(const double *b, long long n, double *y, int *bad, cudaStream_t stream) {
+  long long blocks = (n + kSatadjThreads - 1) / kSatadjThreads;
+  if (blocks > 148LL * 16) blocks = 148LL * 16;
+  if (blocks < 1) blocks = 1;
+  reciprocal_check_kernel<<<(unsigned)blocks, kSatadjThreads, 0, stream>>>(b, n, y, bad);
   return cudaGetLastError();
 }
 

@@ -130,6 +130,47 @@ def test_hard_operands(cuda):
         assert good.mean() > 0.99, (name, good.mean())
 
 
+def test_reciprocal(cuda):
+    """The reciprocal the kernels take for 1/b and for a divisor shared by
+    several quotients (fast_rcp, the first half of fast_div): equal to IEEE
+    1 / b bit for bit inside the window 2^-256 <= |b| < 2^256 and reported
+    outside it.  Random significands over exponents of +-1000, all-ones and
+    power-of-two significands and a few ulps from them, lognormal values, and
+    every special value."""
+    import torch
+    rng = np.random.default_rng(13)
+    n = 2_000_000
+    ones = np.nextafter(2.0, 0.0)
+    e = rng.integers(-300, 301, n)
+    sgn = rng.choice([-1.0, 1.0], n)
+    b = np.concatenate([
+        rng.uniform(1, 2, n) * np.ldexp(1.0, rng.integers(-1000, 1001, n)) * sgn,
+        ones * np.ldexp(1.0, e) * sgn,
+        _near(ones * np.ldexp(1.0, e), rng) * sgn,
+        np.ldexp(1.0, e) * sgn,
+        _near(np.ldexp(1.0, e), rng) * sgn,
+        np.nextafter(1.0, 0.0) * np.ldexp(1.0, e),
+        np.exp(rng.normal(0, 12, n)) * sgn,
+        np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 5e-324, -1e-310, 2.0 ** -256, 2.0 ** 256,
+                  np.nextafter(2.0 ** -256, 0.0), np.nextafter(2.0 ** 256, 0.0)]),
+    ])
+    tb = torch.from_numpy(b).cuda()
+    y, bad = cloudsc.reciprocal_check(tb)
+    torch.cuda.synchronize()
+    y, bad = y.cpu().numpy(), bad.cpu().numpy()
+    with np.errstate(all="ignore"):
+        ref = 1.0 / b
+    good = bad == 0
+    assert (good == _in_window(b)).all(), b[good != _in_window(b)][:4]
+    same = _bits(y) == _bits(ref)
+    assert same[good].all(), b[good & ~same][:4]
+    assert good.mean() > 0.75  # a quarter of the first set and 15 % of the next five lie outside
+    yz, badz = cloudsc.reciprocal_check(torch.empty(0, dtype=torch.float64, device="cuda"))
+    assert yz.numel() == 0 and badz.numel() == 0
+    with pytest.raises(cloudsc.CloudscError):
+        cloudsc.reciprocal_check(torch.ones(3, device="cuda"))
+
+
 def test_zero_dividend_keeps_the_sign(cuda):
     """+-0 / b is the zero of sign(a) xor sign(b) for every divisor inside
     the window, all-ones significands included, without a report; divisors
