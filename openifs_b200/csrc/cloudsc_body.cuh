@@ -412,6 +412,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
   const int ktype = ld(F.ktype + o1);
   const Real peis = Real(ld(F.peis + o1));
   const D paph_surf = ld(F.paph + o2h + (size_t)klev * np);
+  // reciprocals of the column's constant divisors (time step, surface
+  // pressure), taken once
+  const Real rrdt = RCP(rdt), rpsurf = RCP(Real(paph_surf));
   Real zadvw = C(1.0), zadvwd = C(1.0);
   if (ktype == 1 && P.rmfadvw > C(0.0)) {
     zadvw = C(1.0) - P.rmfadvw;
@@ -637,8 +640,9 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       const Real zdp = Real(paph_k1 - paph_k);
       const Real zgdp = DIV(P.rg, zdp);
       const Real zrho = DIV(pap_k, (P.rd * t));
+      const Real rrho = RCP(zrho);
       // (RDENSREF/ZRHO)**0.4 appears in three processes: one shared logarithm
-      const PowBase b_dens = mbase<F32M>(DIV(P.rdensref, zrho));
+      const PowBase b_dens = mbase<F32M>(DIVY(P.rdensref, zrho, rrho));
       // its two powers (0.4 in the rain fall speed, the binary32 0.4 in rain
       // evaporation and riming), computed here for every point so that they
       // overlap with the code around them instead of waiting inside their
@@ -647,7 +651,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
       const Real fallcorr_f = mpowbp<F32M, GEN>(b_dens, P.flt_0p4);
       const Real zdtgdp = rdt * zgdp;
       const Real zrdtgdp = zdp * zrdtgdp_f;
-      Real zcorqsliq, zcorqsice, zcorqsmix, zdqsmixdt, zevaplimmix;
+      Real zcorqsliq, zcorqsice, zcorqsmix, zdqsmixdt, zevaplimmix, rcqsmix;
       {
         Real xl = t - P.r4les, xi = t - P.r4ies;
         Real zfacw = DIV(P.r5les, (xl * xl));
@@ -663,9 +667,13 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         zdqsmixdt = zfac * zcor * zqsmix;
         Real foeldcpm = alfa * P.ralvdcp + (C(1.0) - alfa) * P.ralsdcp;
         zcorqsmix = C(1.0) + foeldcpm * zdqsmixdt;
-        zevaplimmix = mx(DIV((zqsmix - qv), zcorqsmix), C(0.0));
+        rcqsmix = RCP(zcorqsmix);
+        zevaplimmix = mx(DIVY((zqsmix - qv), zcorqsmix, rcqsmix), C(0.0));
       }
       const Real ztmpa = RCP(mx(a, C(0.01)));
+      // MAX(ZEPSEC, 1 - ZA), the divisor of the clear-sky humidity and of
+      // the precipitation's relative-humidity threshold
+      const Real d1ma = mx(zepsec, C(1.0) - a), r1ma = RCP(d1ma);
       Real zliqcld = ql * ztmpa;
       Real zicecld = qi * ztmpa;
       const Real zlicld = zliqcld + zicecld;
@@ -713,7 +721,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         convsrce_l = convsrce_l + lcust_l;
         convsrce_i = convsrce_i + lcust_i;
         Real zdtdp = DIV(P.zrdcp * C(0.5) * (t_prev + t), Real(paph_k));
-        Real zwtot = mn(P.rg * (pmfu_k * zadvw + pmfd_k * zadvwd), DIV((pap_k - pap_prev), rdt));
+        Real zwtot = mn(P.rg * (pmfu_k * zadvw + pmfd_k * zadvwd), DIVY((pap_k - pap_prev), rdt, rrdt));
         Real zdtforc = zdtdp * rdt * zwtot;
         Real zdqs = zanewm1 * zdtforc * zdqsmixdt;
         Real lfinalsum = C(0.0);
@@ -770,7 +778,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           zldifdt = C(2.0) * P.rcldiff_convi * zldifdt;
         }
         if (zli > zepsec) {
-          Real zqe = DIV((qv - a * zqsmix), mx(zepsec, C(1.0) - a));
+          Real zqe = DIVY((qv - a * zqsmix), d1ma, r1ma);
           Real ze = mx(zqsmix - zqe, C(0.0));
           Real zleros = C(0.333) * a * (C(1.) - a) * zldifdt * ze;
           zleros = mn(zleros, zevaplimmix);
@@ -898,7 +906,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // 4.4 rain evaporation (:2271-2378)
       {
-        Real zzrh = P.rprecrhmax + DIV((C(1.0) - P.rprecrhmax) * zcovpmax, mx(zepsec, C(1.0) - a));
+        Real zzrh = P.rprecrhmax + DIVY((C(1.0) - P.rprecrhmax) * zcovpmax, d1ma, r1ma);
         zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
         Real zxramid = P.ramid;
         if (spp && P.spp_on[CLOUDSC_SPP_RAMID]) {  // :2282-2287
@@ -906,7 +914,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           if (P.spp_lramidlimit1) zxramid = mn(C(1.0), zxramid);
         }
         Real zrhc = zxramid;
-        Real zsigk = DIV(pap_k, Real(paph_surf));
+        Real zsigk = DIVY(pap_k, Real(paph_surf), rpsurf);
         if (zsigk > C(0.8)) {
           Real s = DIVK((zsigk - C(0.8)), 0.2);
           zrhc = zxramid + (C(1.0) - zxramid) * (s * s);
@@ -950,8 +958,8 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           Real zicenuclei = C(1000.0) * mexp<F32M>(C(12.96) * zsupersatice - C(0.639));
           Real zadd = DIV(P.rlstt * (DIV(P.rlstt, (P.rv * t)) - C(1.0)), (C(2.4E-2) * t));
           Real zbdd = DIV(P.rv * t * pap_k, (C(2.21) * zvpice));
-          Real zcvds = DIV(C(7.8) * mpow<F32M>(DIV(zicenuclei, zrho), C(0.666)) * zsupersatice, (C(8.87) * (zadd + zbdd)));
-          Real zice0 = mx(zicecld, DIV(zicenuclei * P.riceinit, zrho));
+          Real zcvds = DIV(C(7.8) * mpow<F32M>(DIVY(zicenuclei, zrho, rrho), C(0.666)) * zsupersatice, (C(8.87) * (zadd + zbdd)));
+          Real zice0 = mx(zicecld, DIVY(zicenuclei * P.riceinit, zrho, rrho));
           Real zinew = mpow<F32M>(C(0.666) * zcvds * rdt + mpow<F32M>(zice0, C(0.666)), C(1.5));
           D zdepos = D(mx(P.rcl_overlapliqice * a * (zinew - zice0), C(0.0)));
           zdepos = mn(zdepos, qxfg_l);
@@ -975,7 +983,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
         if (t < P.rtt && zsnowcld > zepsec && zsupersatice > C(0.0)) {
           Real zvpice = DIVP((P.r2es * ei_e) * P.rv, P.rd, P.rcp_rd);
           Real zaplusb = P.rcl_apb1 * zvpice - P.rcl_apb2 * zvpice * t + pap_k * P.rcl_apb3 * (t * t * t);
-          Real zcorrfac = mpow<F32M>(RCP(zrho), C(0.5));
+          Real zcorrfac = mpow<F32M>(rrho, C(0.5));
           Real zcorrfac2 = (mpow<F32M>(DIVK(t, 273.0), C(1.5))) * (DIV(C(393.0), (t + C(120.0))));
           Real zpr02 = zrho * zsnowcld * P.rcl_const1s;
           const PowBase b_pr02 = mbase<F32M>(zpr02);
@@ -984,7 +992,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
                         DIV(P.rcl_const3s * mpow<F32M>(zcorrfac, C(0.5)) * mpow<F32M>(zrho, C(0.5)) *
                             mpowbp<F32M, GEN>(b_pr02, P.rcl_const5s), mpow<F32M>(zcorrfac2, C(0.5)));
           Real zpsdep = mx(zcovptot * zterm1 * zterm2 * rdt, C(0.0));
-          zpsdep = DIV(mn(zpsdep, qv - zqsmix), zcorqsmix);
+          zpsdep = DIVY(mn(zpsdep, qv - zqsmix), zcorqsmix, rcqsmix);
           QADD(SV, zpsdep);  // (S,V) += zpsdep, (V,S) -= zpsdep
           if constexpr (BUD) b_psdep = zpsdep;
         }
@@ -1029,7 +1037,8 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           zmeltmax = mx(ztdmtw0 * zcons1 * P.zrldcp, C(0.0));
         }
         if (zmeltmax > zepsec && zicetot > zepsec) {
-          D zalfa = DIV(qxfg_i, zicetot);
+          const D rit = RCP(D(zicetot));
+          D zalfa = DIVY(qxfg_i, D(zicetot), rit);
           D zmelt = mn(qxfg_i, zalfa * D(zmeltmax));
           qxfg_i = qxfg_i - zmelt;
           qxfg_r = qxfg_r + zmelt;
@@ -1038,7 +1047,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
             bd.i[15] = -zmelt * zqtmst;
             bd.l[17] = zmelt * zqtmst;
           }
-          zalfa = DIV(qxfg_s, zicetot);
+          zalfa = DIVY(qxfg_s, D(zicetot), rit);
           zmelt = mn(qxfg_s, zalfa * D(zmeltmax));
           qxfg_s = qxfg_s - zmelt;
           qxfg_r = qxfg_r + zmelt;
@@ -1059,7 +1068,7 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
           if (llrainliq) {
             Real zlambda = mpowp<F32M, GEN>(DIV(P.rcl_lam1r, (zrho * qr)), P.rcl_lam2r);
             Real ztemp = mn(P.rcl_fzrab * (t - P.rtt), C(50.));
-            Real zfrz = rdt * (DIV(P.rcl_const5r, zrho)) * (mexp<F32M>(ztemp) - C(1.)) * mpowp<F32M, GEN>(zlambda, P.rcl_const6r);
+            Real zfrz = rdt * (DIVY(P.rcl_const5r, zrho, rrho)) * (mexp<F32M>(ztemp) - C(1.)) * mpowp<F32M, GEN>(zlambda, P.rcl_const6r);
             zfrzmax = mx(zfrz, C(0.0));
           } else {
             Real zcons1 = xabs(DIVP(rdt * (C(1.0) + C(0.5) * (P.rtt - t)), P.rtaumel, P.rcp_rtaumel));
@@ -1124,14 +1133,14 @@ CSC_DEV void cloudsc_column(const FT &F, const Shape &sh, int ib, int jl, bool a
 
       // 4.15 snow sublimation, ISUBLSNOW=1 (:3254-3318)
       {
-        Real zzrh = P.rprecrhmax + DIV((C(1.0) - P.rprecrhmax) * zcovpmax, mx(zepsec, C(1.0) - a));
+        Real zzrh = P.rprecrhmax + DIVY((C(1.0) - P.rprecrhmax) * zcovpmax, d1ma, r1ma);
         zzrh = mn(mx(zzrh, P.rprecrhmax), C(1.0));
-        Real zqe = DIV((qv - a * zqsice), mx(zepsec, C(1.0) - a));
+        Real zqe = DIVY((qv - a * zqsice), d1ma, r1ma);
         zqe = mx(C(0.0), mn(zqe, zqsice));
         if (zcovpclr > zepsec && qxfg_s > zepsec && zqe < zzrh * zqsice) {
           Real aa = zcovptot * zdtgdp;
           Real zpreclr = DIV(Real(qxfg_s) * zcovpclr, xsign(mx(xabs(aa), zepsilon), aa));
-          Real zbeta1 = DIV(DIVP(xsqrt(DIV(pap_k, Real(paph_surf))), P.rvrfactor, P.rcp_rvrfactor) * zpreclr, mx(zcovpclr, zepsec));
+          Real zbeta1 = DIV(DIVP(xsqrt(DIVY(pap_k, Real(paph_surf), rpsurf)), P.rvrfactor, P.rcp_rvrfactor) * zpreclr, mx(zcovpclr, zepsec));
           Real zbeta = P.rg * P.rpecons * mpow<F32M>(zbeta1, C(0.5777));
           Real zdenom = C(1.0) + zbeta * rdt * zcorqsice;
           Real zdpr = DIV(zcovpclr * zbeta * (zqsice - zqe), zdenom) * zdp * P.zrg_r;
