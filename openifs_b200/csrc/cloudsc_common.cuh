@@ -106,8 +106,8 @@ struct Shape {
 };
 
 // Levels whose PLUDE input the kernels' fast pass keeps for a rerun of the
-// column (a per-thread array); with more levels (KLEV above this) forms 0-2
-// run their plain kernel, IEEE division throughout.
+// column (a per-thread array); with more levels (KLEV above this) every form
+// runs its plain kernel, IEEE division throughout.
 constexpr int kMaxLevFast = 256;
 
 }  // namespace cloudsc
