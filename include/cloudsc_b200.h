@@ -332,10 +332,11 @@ int cloudsc_b200_batched_host_sp(
  * it), so a caller that reserves its own GPU memory pool should call
  * cloudsc_b200_setup first and leave room for them.  The same set-up also
  * reserves the kernels' per-thread local memory (it raises the CUDA stack
- * size limit to the largest kernel's frame, about 2.6 KB, never lowering
+ * size limit to the largest kernel's frame, about 3 KB, never lowering
  * it): the driver holds that for every thread the device can run, which it
- * would otherwise take at the first launch (measured on a B200: set-up takes
- * 542 MiB with the fixed array, and the first call then none).
+ * would otherwise take at the first launch (measured on a B200 with a 2.6 KB
+ * frame: set-up took 542 MiB with the fixed array, and the first call then
+ * none).
  */
 int cloudsc_b200_block_noalloc(
     const cloudsc_params *p, int32_t kidia, int32_t kfdia, int32_t klon, int32_t klev,
