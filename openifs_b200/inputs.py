@@ -61,18 +61,24 @@ def l137_ab():
 
 def hybrid_ab(klev=KLEV_L137):
     """Half-level A (Pa) and B of a KLEV-level hybrid grid: the L137 grid
-    itself, or for 2 <= KLEV < 137 the L137 half levels at the KLEV + 1
-    indices round(i * 137 / KLEV), i = 0..KLEV (model top and surface kept).
-    The coarser grids stand in for the operational L60/L91 tables, which the
-    reference tree does not carry; they exercise the scheme at other
-    vertical resolutions."""
+    itself; for 2 <= KLEV < 137 the L137 half levels at the KLEV + 1
+    indices round(i * 137 / KLEV), i = 0..KLEV (model top and surface kept);
+    for 137 < KLEV <= 1000 A and B interpolated linearly in the L137 half-level
+    index at i * 137 / KLEV.  The coarser grids stand in for the operational
+    L60/L91 tables, which the reference tree does not carry; they and the
+    finer ones exercise the scheme at other vertical resolutions."""
     a, b = l137_ab()
     if klev == KLEV_L137:
         return a, b
-    if not 2 <= klev < KLEV_L137:
-        raise ValueError("the generator builds grids of 2..137 levels")
-    idx = np.round(np.arange(klev + 1) * KLEV_L137 / klev).astype(int)
-    return a[idx], b[idx]
+    if not 2 <= klev <= 1000:
+        raise ValueError("the generator builds grids of 2..1000 levels")
+    if klev < KLEV_L137:
+        idx = np.round(np.arange(klev + 1) * KLEV_L137 / klev).astype(int)
+        return a[idx], b[idx]
+    x = np.arange(klev + 1) * KLEV_L137 / klev
+    i = np.minimum(np.floor(x).astype(int), KLEV_L137 - 1)
+    w = x - i
+    return a[i] * (1.0 - w) + a[i + 1] * w, b[i] * (1.0 - w) + b[i + 1] * w
 
 
 def standard_full_level_pressure(p_surf=101325.0, klev=KLEV_L137):

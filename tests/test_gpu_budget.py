@@ -120,6 +120,37 @@ def test_block_entry_spp_inhomogeneity(cuda):
         assert np.array_equal(g[..., cols], o[..., cols]), n
 
 
+def test_optional_forms_more_levels_than_the_fast_pass_keeps(cuda):
+    """300 levels: the budget, SPP and inhomogeneity form runs its plain
+    kernel (no fast pass beyond 256 levels).  Outputs, PFSD and PEXTRA
+    bit for bit with the oracle."""
+    import torch
+    klev = 300
+    p0, po0 = util.params(inputs.ncldtop_for(klev))
+    p, po = util.opt_params(p0, "all+budgets"), util.opt_params(po0, "all+budgets")
+    nproma, nblk = 32, 4
+    ngptot = nproma * nblk - 3
+    arrs = inputs.generate(nblk, nproma, p, klev=klev, seed=37)
+    diag = inputs.generate_diag(arrs, nproma, fields.budget_fields_needed(p) + 1, klev=klev, seed=37)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, nproma, nblk, ngptot, klev=klev)
+    try:
+        cloudsc.setup(p)
+        d = {k: torch.from_numpy(v).cuda() for k, v in arrs.items()}
+        g = {k: torch.from_numpy(v).cuda() for k, v in diag.items()}
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        cloudsc.cloudsc_batched_diag(p, d, g, nproma, klev, nblk, ngptot, util.PTSPHY, counter=cnt)
+        torch.cuda.synchronize()
+        for n in util.COMPARED:
+            a = util.defined(n, util._valid_cols(d[n].cpu().numpy(), ngptot, nproma))
+            b = util.defined(n, util._valid_cols(ref[n], ngptot, nproma))
+            assert np.array_equal(a, b), n
+        assert np.array_equal(g["pfsd"].cpu().numpy(), dref["pfsd"])
+        assert np.array_equal(g["pextra"].cpu().numpy(), dref["pextra"])
+        assert int(cnt.item()) == nw
+    finally:
+        cloudsc.setup(p0)
+
+
 @pytest.mark.parametrize("case", ["budgets", "spp", "all+budgets"])
 def test_optional_forms_rerun_mid_column(cuda, case):
     """Forms 3-5 run the fast pass with its rerun.  Three columns get a

@@ -93,6 +93,34 @@ def test_other_vertical_grids(cuda, klev):
     assert nw_gpu == nw_ref
 
 
+def test_more_levels_than_the_fast_pass_keeps(cuda):
+    """300 levels, above the 256 whose PLUDE inputs the fast pass keeps: the
+    plain (448, 1) kernels run (at most 448 columns per CTA, whatever the
+    schedule says).  FP64 bit-exact against the oracle with a ragged last
+    block; the FP32-mixed form runs and stays close to it."""
+    klev = 300
+    p, po = util.params(inputs.ncldtop_for(klev))
+    nproma, nblk = 32, 5
+    ngptot = nproma * nblk - 7
+    arrs = inputs.generate(nblk, nproma, p, klev=klev, seed=31)
+    ref, nw_ref = util.run_oracle(po, arrs, nproma, nblk, ngptot, klev=klev)
+    before = cloudsc.get_schedule(cloudsc.FP64)
+    try:
+        cloudsc.set_schedule(cloudsc.FP64, 0, 640, 0)  # clamped to 448 beyond the fast pass's levels
+        gpu, nw_gpu = util.run_gpu(p, arrs, nproma, nblk, ngptot, klev=klev)
+    finally:
+        cloudsc.set_schedule(cloudsc.FP64, *before)
+    for n in util.COMPARED:
+        a = util.defined(n, util._valid_cols(gpu[n], ngptot, nproma))
+        b = util.defined(n, util._valid_cols(ref[n], ngptot, nproma))
+        assert np.array_equal(a, b), n
+    assert nw_gpu == nw_ref
+    mixed, _ = util.run_gpu(p, arrs, nproma, nblk, ngptot, precision=cloudsc.MIXED, klev=klev)
+    t, tm = ref["tendency_loc_t"], mixed["tendency_loc_t"]
+    assert np.isfinite(tm).all()
+    assert np.sqrt(np.mean((tm - t) ** 2)) <= 1e-3 * np.sqrt(np.mean(t ** 2))
+
+
 def test_partial_last_block_and_odd_nproma(cuda):
     """NPROMA not a multiple of 32 and NGPTOT ending inside the last block."""
     p, po = util.params()

@@ -56,6 +56,34 @@ def test_other_vertical_grids_bit_exact(klev):
     assert np.abs(ref["tendency_loc_t"]).max() > 0
 
 
+def test_more_levels_than_the_fast_pass_keeps():
+    """300 levels, above the 256 whose PLUDE inputs the kernels' fast pass
+    keeps: the kernels then run their plain column code.  The host build of
+    that path (the fast-pass flag is ignored there, as on the GPU) against
+    the oracle, bit for bit, in the plain FP64 form and with every budget
+    section, SPP and the inhomogeneity paths on."""
+    klev = 300
+    p, po = util.params(inputs.ncldtop_for(klev))
+    arrs = inputs.generate(3, 32, p, klev=klev, seed=31)
+    ngptot = 3 * 32 - 5
+    ref, nw = util.run_oracle(po, arrs, 32, 3, ngptot, klev=klev)
+    emu, nwe = util.run_hostemu(p, arrs, 32, 3, ngptot, klev=klev, precision=0x300)
+    for n in util.COMPARED:
+        a = util.defined(n, util._valid_cols(emu[n], ngptot, 32))
+        b = util.defined(n, util._valid_cols(ref[n], ngptot, 32))
+        assert np.array_equal(a, b), n
+    assert nw == nwe
+    q, qo = util.opt_params(p, "all+budgets"), util.opt_params(po, "all+budgets")
+    diag = inputs.generate_diag(arrs, 32, util.fields.budget_fields_needed(q) + 1, klev=klev, seed=31)
+    ref, dref, nw = util.run_oracle_diag(qo, arrs, diag, 32, 3, ngptot, klev=klev)
+    emu, demu, nwe = util.run_hostemu_diag(q, arrs, diag, 32, 3, ngptot, flags=0x300, klev=klev)
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), n
+    assert np.array_equal(demu["pextra"], dref["pextra"])
+    assert np.array_equal(demu["pfsd"], dref["pfsd"])
+    assert nw == nwe
+
+
 def test_libm_sensitivity_of_the_reference(pp):
     """The reference algorithm with two correct libms (glibc and plibm, within
     1 ulp of each other) -- the spread any GPU build is measured against."""

@@ -44,6 +44,26 @@ def test_l137_table():
     assert np.all(np.diff(a[:60]) > 0)
 
 
+@pytest.mark.parametrize("klev", [138, 300, 1000])
+def test_finer_grids_interpolate_l137(klev):
+    """The finer test grids keep the L137 model top and surface, increase
+    strictly, and pass through every L137 half level whose index i * 137 /
+    KLEV is whole."""
+    a137, b137 = inputs.l137_ab()
+    a, b = inputs.hybrid_ab(klev)
+    assert len(a) == len(b) == klev + 1
+    assert a[0] == a137[0] and b[0] == b137[0] and a[-1] == a137[-1] and b[-1] == b137[-1]
+    assert np.all(np.diff(a + b * 101325.0) > 0)
+    assert np.all(np.diff(a + b * 50000.0) > 0)
+    for i in range(klev + 1):
+        if (i * 137) % klev == 0:
+            assert a[i] == a137[i * 137 // klev] and b[i] == b137[i * 137 // klev]
+    nc = inputs.ncldtop_for(klev)
+    assert 2 <= nc <= klev
+    with pytest.raises(ValueError):
+        inputs.hybrid_ab(1001)
+
+
 @pytest.mark.parametrize("klev", [2, 60, 91, 136, 137])
 def test_coarser_grids_are_subsets_of_l137(klev):
     """The coarser test grids keep the L137 model top and surface and take

@@ -226,7 +226,7 @@ def run_oracle_sltend(po, arrs, nproma, ngpblks, ngptot, libm="plibm"):
 
 
 
-def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm", flags=0):
+def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm", flags=0, klev=KLEV):
     """The kernel's column code with the budget diagnostics, on the host;
     flags 0x100 for the GEN column code, 0x200 for the kernels' fast pass with
     its rerun."""
@@ -243,16 +243,16 @@ def run_hostemu_diag(p, arrs, diag, nproma, ngpblks, ngptot, libm="plibm", flags
     a = (ctypes.c_void_p * len(fields.BATCHED_FIELDS))(*[out[n].ctypes.data for n, *_ in fields.BATCHED_FIELDS])
     b = (ctypes.c_void_p * len(fields.DIAG_FIELDS))(
         *[(dout[n].ctypes.data if dout.get(n) is not None else None) for n, *_ in fields.DIAG_FIELDS])
-    nw = L.hostemu_batched_diag(ctypes.byref(p), int(nproma), KLEV, int(ngpblks), int(ngptot),
+    nw = L.hostemu_batched_diag(ctypes.byref(p), int(nproma), int(klev), int(ngpblks), int(ngptot),
                                 ctypes.c_double(PTSPHY), a, b, int(dout["pextra"].shape[1]), int(flags))
     return out, dout, nw
 
 
-def run_oracle_diag(po, arrs, diag, nproma, ngpblks, ngptot, libm="plibm"):
+def run_oracle_diag(po, arrs, diag, nproma, ngpblks, ngptot, libm="plibm", klev=KLEV):
     from oracle import oracle
     out = {k: v.copy() for k, v in arrs.items()}
     dout = {k: v.copy() for k, v in diag.items()}
-    nw = oracle.cloudsc_batched_diag(po, out, dout, nproma, KLEV, ngpblks, ngptot, PTSPHY, libm=libm)
+    nw = oracle.cloudsc_batched_diag(po, out, dout, nproma, klev, ngpblks, ngptot, PTSPHY, libm=libm)
     return out, dout, nw
 
 
