@@ -134,8 +134,7 @@ def test_single_column(cuda):
     _check(p, po, arrs, 1, 3, 3)
 
 
-@pytest.mark.parametrize("case", ["clear", "overcast", "warm", "cold", "no_convection",
-                                  "all_convection", "land", "sea", "tiny_condensate"])
+@pytest.mark.parametrize("case", util.EDGE_CASES)
 def test_edge_columns(cuda, case):
     """Edge-case columns the reference's branches single out."""
     p, po = util.params()

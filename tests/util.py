@@ -94,7 +94,7 @@ def run_hostemu(p, arrs, nproma, ngpblks, ngptot, precision=0, libm="plibm", kle
 
 
 EDGE_CASES = ["clear", "overcast", "warm", "cold", "no_convection", "all_convection", "land",
-              "sea", "tiny_condensate"]
+              "sea", "tiny_condensate", "supersaturated", "tiny_cloud_fraction", "negative_condensate"]
 
 
 def apply_case(arrs, case):
@@ -123,6 +123,21 @@ def apply_case(arrs, case):
         arrs["plsm"][:] = 0.0
     elif case == "tiny_condensate":
         cl[:, :4] = np.where(cl[:, :4] > 0, 5e-9, 0.0)
+    elif case == "supersaturated":
+        # 40 % more vapour: most cloudy levels above saturation, so that
+        # CLOUD_SUPERSATCHECK and the condensation branches act everywhere
+        arrs["pq"][:] = arrs["pq"] * 1.4
+    elif case == "tiny_cloud_fraction":
+        # cloud fraction below RAMIN (1e-8) wherever there is cloud: the
+        # tidy-up evaporates the condensate of every such level
+        arrs["pa"][:] = np.where(arrs["pa"] > 0, 5e-9, 0.0)
+    elif case == "negative_condensate":
+        # negative liquid and ice of about -1e-6 kg/kg on every 7th level
+        # (as a dynamics step can leave them): the tidy-up moves them to the
+        # vapour, and the tendencies are taken against the negative first
+        # guess
+        cl[:, 0, ::7] = -np.abs(cl[:, 0, ::7]) * 0.01 - 1e-6
+        cl[:, 1, ::7] = -np.abs(cl[:, 1, ::7]) * 0.01 - 1e-6
     else:
         raise ValueError(case)
     return arrs
