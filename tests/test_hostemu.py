@@ -56,6 +56,25 @@ def test_other_vertical_grids_bit_exact(klev):
     assert np.abs(ref["tendency_loc_t"]).max() > 0
 
 
+@pytest.mark.parametrize("case", ["clear", "supersaturated", "tiny_cloud_fraction", "negative_condensate"])
+def test_optional_forms_edge_cases(pp, case):
+    """The budget, SPP and inhomogeneity form on edge-case columns, with the
+    kernels' fast pass and rerun: outputs, PFSD and PEXTRA bit for bit with
+    the oracle."""
+    p0, po0 = pp
+    p, po = util.opt_params(p0, "all+budgets"), util.opt_params(po0, "all+budgets")
+    arrs = util.apply_case(inputs.generate(3, 32, p, seed=47), case)
+    ngptot = 3 * 32 - 2
+    diag = inputs.generate_diag(arrs, 32, util.fields.budget_fields_needed(p) + 1, seed=47)
+    ref, dref, nw = util.run_oracle_diag(po, arrs, diag, 32, 3, ngptot)
+    emu, demu, nwe = util.run_hostemu_diag(p, arrs, diag, 32, 3, ngptot, flags=0x300)
+    assert nw == nwe
+    for n in util.COMPARED:
+        assert np.array_equal(util.defined(n, emu[n]), util.defined(n, ref[n])), n
+    assert np.array_equal(demu["pextra"], dref["pextra"])
+    assert np.array_equal(demu["pfsd"], dref["pfsd"])
+
+
 def test_more_levels_than_the_fast_pass_keeps():
     """300 levels, above the 256 whose PLUDE inputs the kernels' fast pass
     keeps: the kernels then run their plain column code.  The host build of
